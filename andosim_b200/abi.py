@@ -1,0 +1,332 @@
+"""ctypes binding of the C ABI declared in ``include/ando_gpu.h``.
+
+This is the binding any non-pybind11 host would write against
+``libando_gpu.so`` (it mirrors the header's structs field for field). The GPU
+parity tests call the library through it, and it is the ctypes stub shown in
+the integration notes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libando_gpu.so"
+
+ANDO_OK = 0
+ANDO_ERR_CAPACITY = 6
+SEMANTICS = {"reference": 0, "corrected": 1}
+PRECOND = {"block_jacobi": 0, "learned": 1}
+
+# Every symbol the header declares (checked by the CPU test suite).
+EXPORTED = [
+    "ando_abi_version", "ando_status_string", "ando_last_error", "ando_ctx_create", "ando_ctx_destroy",
+    "ando_mesh_upload", "ando_mesh_set_vertices", "ando_state_upload", "ando_state_download",
+    "ando_apply_gravity", "ando_step", "ando_compute_contacts", "ando_last_system", "ando_eval_system",
+    "ando_last_gradient",
+]
+
+
+class Material(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("youngs_modulus", "poisson_ratio", "density", "thickness", "bending_stiffness")]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double), ("beta_max", C.c_double),
+        ("min_newton_steps", C.c_int32), ("max_newton_steps", C.c_int32), ("friction_min_newton_steps", C.c_int32),
+        ("pcg_tol", C.c_double), ("pcg_max_iters", C.c_int32),
+        ("contact_gap_max", C.c_double), ("wall_gap", C.c_double), ("enable_ccd", C.c_int32),
+        ("contact_normal_epsilon", C.c_double), ("barrier_tolerance", C.c_double),
+        ("enable_friction", C.c_int32), ("friction_mu", C.c_double), ("friction_epsilon", C.c_double),
+        ("friction_tangent_threshold", C.c_double), ("velocity_damping", C.c_double), ("contact_restitution", C.c_double),
+        ("enable_strain_limiting", C.c_int32), ("strain_limit", C.c_double), ("strain_tau", C.c_double),
+        ("strain_epsilon", C.c_double), ("strain_svd_epsilon", C.c_double), ("hessian_epsilon", C.c_double),
+        ("min_gap", C.c_double), ("semantics", C.c_int32), ("precond", C.c_int32),
+    ]
+
+
+class Pin(C.Structure):
+    _fields_ = [("vertex", C.c_int32), ("active", C.c_int32), ("target", C.c_double * 3)]
+
+
+class Wall(C.Structure):
+    _fields_ = [("normal", C.c_double * 3), ("offset", C.c_double), ("gap", C.c_double), ("active", C.c_int32), ("pad_", C.c_int32)]
+
+
+class Rigid(C.Structure):
+    _fields_ = [
+        ("num_vertices", C.c_int32), ("num_triangles", C.c_int32),
+        ("local_vertices", C.POINTER(C.c_double)), ("triangles", C.POINTER(C.c_int32)),
+        ("mass", C.c_double), ("inertia_body_inv", C.c_double * 9), ("position", C.c_double * 3),
+        ("rotation", C.c_double * 9), ("linear_velocity", C.c_double * 3), ("angular_velocity", C.c_double * 3),
+    ]
+
+
+class Contact(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("idx0", C.c_int32), ("idx1", C.c_int32), ("idx2", C.c_int32), ("idx3", C.c_int32),
+        ("rigid_body_index", C.c_int32), ("vertex_count", C.c_int32), ("pad_", C.c_int32),
+        ("gap", C.c_double), ("normal", C.c_double * 3), ("witness_p", C.c_double * 3), ("witness_q", C.c_double * 3),
+        ("barycentric", C.c_double * 3), ("weights", C.c_double * 4),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("newton_iters", C.c_int32), ("pcg_iters", C.c_int32), ("pcg_max_per_newton", C.c_int32),
+        ("pcg_not_converged", C.c_int32), ("line_search_fail", C.c_int32), ("contacts", C.c_int32),
+        ("strain_active", C.c_int32), ("status", C.c_int32), ("precond_fallbacks", C.c_int32), ("pad_", C.c_int32),
+        ("beta", C.c_double), ("last_alpha", C.c_double), ("device_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad_"}
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Load libando_gpu.so and declare the prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    L = C.CDLL(str(LIB_PATH))
+    P, I32, D = C.c_void_p, C.c_int32, C.c_double
+    pd, pi, pf = C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_float)
+    L.ando_abi_version.restype = I32
+    L.ando_status_string.restype = C.c_char_p; L.ando_status_string.argtypes = [I32]
+    L.ando_last_error.restype = C.c_char_p
+    L.ando_ctx_create.restype = I32; L.ando_ctx_create.argtypes = [I32, C.POINTER(P)]
+    L.ando_ctx_destroy.restype = None; L.ando_ctx_destroy.argtypes = [P]
+    L.ando_mesh_upload.restype = I32; L.ando_mesh_upload.argtypes = [P, pd, I32, pi, I32, pd, pd, C.POINTER(Material)]
+    L.ando_mesh_set_vertices.restype = I32; L.ando_mesh_set_vertices.argtypes = [P, pd, I32]
+    L.ando_state_upload.restype = I32; L.ando_state_upload.argtypes = [P, pd, pd, pd, pd, I32]
+    L.ando_state_download.restype = I32; L.ando_state_download.argtypes = [P, pd, pd, I32]
+    L.ando_apply_gravity.restype = I32; L.ando_apply_gravity.argtypes = [P, pd, D]
+    L.ando_step.restype = I32
+    L.ando_step.argtypes = [P, C.POINTER(Params), C.POINTER(Pin), I32, C.POINTER(Wall), I32, C.POINTER(Rigid), I32, C.POINTER(StepStats)]
+    L.ando_eval_system.restype = I32
+    L.ando_eval_system.argtypes = [P, C.POINTER(Params), C.POINTER(Pin), I32, C.POINTER(Wall), I32, C.POINTER(Rigid), I32]
+    L.ando_compute_contacts.restype = I32
+    L.ando_compute_contacts.argtypes = [P, C.POINTER(Rigid), I32, C.POINTER(Contact), I32, pi]
+    L.ando_last_system.restype = I32; L.ando_last_system.argtypes = [P, pi, pi, pi, pi, pf, pf, pf]
+    L.ando_last_gradient.restype = I32; L.ando_last_gradient.argtypes = [P, pd, I32]
+    _lib = L
+    return L
+
+
+class AbiError(RuntimeError):
+    pass
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != ANDO_OK:
+        L = lib()
+        raise AbiError(f"{what}: {L.ando_status_string(rc).decode()} ({L.ando_last_error().decode()})")
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def rest_state(vertices: np.ndarray, triangles: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Per-face rest area and Dm_inv (row-major 2x2) in the local 2D frame (mesh.cpp:18-75)."""
+    v = np.asarray(vertices, dtype=np.float64)
+    t = np.asarray(triangles, dtype=np.int64)
+    e1 = v[t[:, 1]] - v[t[:, 0]]
+    e2 = v[t[:, 2]] - v[t[:, 0]]
+    l1 = (e1 * e1).sum(1)
+    l2 = (e2 * e2).sum(1)
+    n = np.cross(e1, e2)
+    nl = np.linalg.norm(n, axis=1)
+    ok = (l1 >= 1e-12) & (l2 >= 1e-12) & (nl >= 1e-12)
+    area = np.where(ok, nl * 0.5, 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        nu = n / nl[:, None]
+        t1 = e1 / np.sqrt(l1)[:, None]
+        t2 = np.cross(nu, t1)
+        a = (e1 * t1).sum(1); b = (e2 * t1).sum(1); c = (e1 * t2).sum(1); d = (e2 * t2).sum(1)
+        det = a * d - b * c
+        inv = 1.0 / det
+        dm = np.stack([d * inv, -b * inv, -c * inv, a * inv], axis=1)
+    dm[~ok] = 0.0
+    return np.ascontiguousarray(area), np.ascontiguousarray(dm)
+
+
+def lumped_masses(num_vertices: int, triangles: np.ndarray, area: np.ndarray, thickness: float, density: float) -> np.ndarray:
+    """m_i = sum over incident faces of area * thickness * density / 3 (state.cpp:18-32)."""
+    m = np.zeros(num_vertices)
+    fm = area * thickness * density / 3.0
+    for k in range(3):
+        np.add.at(m, triangles[:, k], fm)
+    return m
+
+
+def make_params(params: dict, semantics: str = "reference", precond: str = "block_jacobi") -> Params:
+    """Params with the reference's SimParams defaults (types.h:60-100), overridden by `params`."""
+    d = dict(dt=0.002, beta_max=0.25, min_newton_steps=2, max_newton_steps=8, friction_min_newton_steps=32,
+             pcg_tol=1e-3, pcg_max_iters=1000, contact_gap_max=0.001, wall_gap=0.001, enable_ccd=1,
+             contact_normal_epsilon=1e-8, barrier_tolerance=1e-12, enable_friction=0, friction_mu=0.1,
+             friction_epsilon=1e-5, friction_tangent_threshold=1e-6, velocity_damping=0.0, contact_restitution=0.0,
+             enable_strain_limiting=0, strain_limit=0.05, strain_tau=0.05, strain_epsilon=0.0, strain_svd_epsilon=1e-6,
+             hessian_epsilon=1e-8, min_gap=1e-8)
+    d.update({k: v for k, v in params.items()})
+    p = Params()
+    for name, typ in Params._fields_:
+        if name in ("semantics", "precond"):
+            continue
+        val = d[name]
+        setattr(p, name, int(val) if typ is C.c_int32 else float(val))
+    p.semantics = SEMANTICS[semantics]
+    p.precond = PRECOND[precond]
+    return p
+
+
+class Scene:
+    """One device context holding a mesh and its state."""
+
+    def __init__(self, vertices, triangles, material: dict, device: int = 0):
+        L = lib()
+        self.V = int(len(vertices))
+        self.T = int(len(triangles))
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
+        self.triangles = np.ascontiguousarray(triangles, dtype=np.int32)
+        mat = dict(youngs_modulus=1e6, poisson_ratio=0.3, density=1000.0, thickness=0.001, bending_stiffness=0.0)
+        mat.update(material)
+        self.material = Material(**mat)
+        self.area, self.dm_inv = rest_state(self.vertices, self.triangles)
+        self.masses = lumped_masses(self.V, self.triangles, self.area, mat["thickness"], mat["density"])
+        self.ctx = C.c_void_p()
+        _check(L.ando_ctx_create(device, C.byref(self.ctx)), "ando_ctx_create")
+        _check(L.ando_mesh_upload(self.ctx, _dptr(self.vertices), self.V, _iptr(self.triangles), self.T,
+                                  _dptr(self.area), _dptr(self.dm_inv), C.byref(self.material)), "ando_mesh_upload")
+        zeros = np.zeros((self.V, 3))
+        self.upload(self.vertices, zeros, self.vertices, self.masses)
+
+    def close(self):
+        if self.ctx:
+            lib().ando_ctx_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, x=None, v=None, x_prev=None, masses=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x, v, x_prev, masses)]
+        ptrs = [None if a is None else _dptr(a) for a in arrs]
+        _check(lib().ando_state_upload(self.ctx, *ptrs, self.V), "ando_state_upload")
+
+    def download(self) -> Tuple[np.ndarray, np.ndarray]:
+        x = np.empty((self.V, 3)); v = np.empty((self.V, 3))
+        _check(lib().ando_state_download(self.ctx, _dptr(x), _dptr(v), self.V), "ando_state_download")
+        return x, v
+
+    def apply_gravity(self, g, dt: float):
+        ga = np.ascontiguousarray(g, dtype=np.float64)
+        _check(lib().ando_apply_gravity(self.ctx, _dptr(ga), float(dt)), "ando_apply_gravity")
+
+    @staticmethod
+    def _constraints(pins, walls):
+        pa = (Pin * max(1, len(pins)))()
+        for k, (i, t) in enumerate(pins):
+            pa[k].vertex = int(i); pa[k].active = 1
+            for q in range(3):
+                pa[k].target[q] = float(t[q])
+        wa = (Wall * max(1, len(walls)))()
+        for k, (n, off, gap) in enumerate(walls):
+            n = np.asarray(n, dtype=np.float64)
+            nn = np.linalg.norm(n)
+            n = n / nn if nn > 0 else n
+            for q in range(3):
+                wa[k].normal[q] = float(n[q])
+            wa[k].offset = float(off); wa[k].gap = float(gap); wa[k].active = 1
+        return pa, wa
+
+    def step(self, params: Params, pins: Sequence = (), walls: Sequence = (), rigids: Optional[List[Rigid]] = None) -> dict:
+        pa, wa = self._constraints(list(pins), list(walls))
+        st = StepStats()
+        nr = len(rigids) if rigids else 0
+        ra = (Rigid * max(1, nr))(*(rigids or []))
+        _check(lib().ando_step(self.ctx, C.byref(params), pa, len(pins), wa, len(walls), ra, nr, C.byref(st)), "ando_step")
+        if rigids:
+            for k in range(nr):
+                C.pointer(rigids[k])[0] = ra[k]
+        return st.as_dict()
+
+    def eval_system(self, params: Params, pins: Sequence = (), walls: Sequence = (), rigids: Optional[List[Rigid]] = None):
+        pa, wa = self._constraints(list(pins), list(walls))
+        nr = len(rigids) if rigids else 0
+        ra = (Rigid * max(1, nr))(*(rigids or []))
+        _check(lib().ando_eval_system(self.ctx, C.byref(params), pa, len(pins), wa, len(walls), ra, nr), "ando_eval_system")
+
+    def last_gradient(self) -> np.ndarray:
+        g = np.empty(3 * self.V)
+        _check(lib().ando_last_gradient(self.ctx, _dptr(g), self.V), "ando_last_gradient")
+        return g
+
+    def last_system(self):
+        V = C.c_int32(); nnzb = C.c_int32()
+        _check(lib().ando_last_system(self.ctx, C.byref(V), C.byref(nnzb), None, None, None, None, None), "ando_last_system")
+        rowptr = np.empty(V.value + 1, dtype=np.int32)
+        cols = np.empty(nnzb.value, dtype=np.int32)
+        vals = np.empty(9 * nnzb.value, dtype=np.float32)
+        rhs = np.empty(3 * V.value, dtype=np.float32)
+        sol = np.empty(3 * V.value, dtype=np.float32)
+        _check(lib().ando_last_system(self.ctx, C.byref(V), C.byref(nnzb), _iptr(rowptr), _iptr(cols), _fptr(vals),
+                                      _fptr(rhs), _fptr(sol)), "ando_last_system")
+        return rowptr, cols, vals.reshape(-1, 3, 3), rhs, sol
+
+    def contacts(self, rigids: Optional[List[Rigid]] = None) -> List[Contact]:
+        nr = len(rigids) if rigids else 0
+        ra = (Rigid * max(1, nr))(*(rigids or []))
+        n = C.c_int32()
+        buf = (Contact * 1)()
+        rc = lib().ando_compute_contacts(self.ctx, ra, nr, buf, 0, C.byref(n))
+        if rc not in (ANDO_OK, ANDO_ERR_CAPACITY):
+            _check(rc, "ando_compute_contacts")
+        if n.value == 0:
+            return []
+        buf = (Contact * n.value)()
+        _check(lib().ando_compute_contacts(self.ctx, ra, nr, buf, n.value, C.byref(n)), "ando_compute_contacts")
+        return list(buf)
+
+
+def make_rigid(vertices, triangles, density: float, keep: list) -> Rigid:
+    """Rigid body as RigidBody::initialize builds it (rigid_body.cpp:11-91); `keep` holds the arrays alive."""
+    v = np.asarray(vertices, dtype=np.float64)
+    c = v.mean(axis=0)
+    local = np.ascontiguousarray(v - c)
+    tris = np.ascontiguousarray(triangles, dtype=np.int32)
+    ext = v.max(0) - v.min(0)
+    vol = max(ext[0], 1e-6) * max(ext[1], 1e-6) * max(ext[2], 1e-6)
+    mass = max(density * vol, 1e-3)
+    I = np.array([(mass / 12.0) * (ext[1] ** 2 + ext[2] ** 2), (mass / 12.0) * (ext[0] ** 2 + ext[2] ** 2),
+                  (mass / 12.0) * (ext[0] ** 2 + ext[1] ** 2)])
+    I = np.maximum(I, 1e-6)
+    keep.extend([local, tris])
+    r = Rigid()
+    r.num_vertices = len(local); r.num_triangles = len(tris)
+    r.local_vertices = _dptr(local); r.triangles = _iptr(tris)
+    r.mass = mass
+    for k in range(9):
+        r.inertia_body_inv[k] = 0.0
+        r.rotation[k] = 1.0 if k in (0, 4, 8) else 0.0
+    r.inertia_body_inv[0], r.inertia_body_inv[4], r.inertia_body_inv[8] = 1 / I[0], 1 / I[1], 1 / I[2]
+    for q in range(3):
+        r.position[q] = c[q]; r.linear_velocity[q] = 0.0; r.angular_velocity[q] = 0.0
+    return r

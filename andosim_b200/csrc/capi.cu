@@ -1,0 +1,709 @@
+// capi.cu -- host orchestration of the implicit step behind the C ABI of
+// include/ando_gpu.h.
+//
+// The control flow of Integrator::step / inner_newton_step
+// (integrator.cpp:70-236) runs here on the host; every numerical stage runs on
+// the device. One Newton iteration is a fixed launch sequence whose later
+// kernels are predicated on a device flag (gradient-norm test), so the host
+// reads back one small control block per Newton iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+
+#include "../../include/ando_gpu.h"
+#include "kernels.cuh"
+
+using namespace ando;
+
+namespace {
+
+thread_local std::string g_last_error = "";
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail(ANDO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t reserve(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    if (p) { cudaFree(p); p = nullptr; n = 0; }
+    size_t c = count ? count : 1;
+    cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+    if (e == cudaSuccess) n = c;
+    return e;
+  }
+  cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
+    cudaError_t e = reserve(count);
+    if (e != cudaSuccess || count == 0) return e;
+    return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+}  // namespace
+
+struct ando_ctx_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int V = 0, T = 0, nnzb = 0;
+  double mu = 0, thickness = 0, density = 0;
+  int el_semantics = -1;
+  bool mesh_ready = false, state_ready = false;
+  int pcg_grid = 1;
+
+  DevBuf<int> tris, rowptr, cols, slot_row, diag_slot, face_slot, slot_cptr, slot_contrib, vf_ptr, vf;
+  DevBuf<double> rest_area, dm_inv, mass, el_a, el_b, g_el, mesh_x;
+  DevBuf<double> x, v, x_prev, x_old, x_hat, g, g_const, diag_const, diag_extra;
+  DevBuf<float> b, d, r, z, p0, p1, Ap, val, precond;
+  DevBuf<unsigned char> sflags;
+  DevBuf<StrainSV> sv;
+  DevBuf<Ctrl> ctrl;
+  DevBuf<double> partials;
+  Ctrl* ctrl_host = nullptr;
+
+  // contacts
+  DevBuf<int> det_counts, det_offsets;
+  DevBuf<ContactDev> contacts;
+  int ncontacts = 0, n_pe = 0;
+  DevBuf<int> ekeys, ekeys_sorted, ebegin, eend, xflags, xkeys, xcols, xbegin, xend, nsel;
+  DevBuf<ContactEntry> ents, ents_sorted, xent;
+  DevBuf<float> xval;
+  int nx = 0, nent = 0;
+  DevBuf<unsigned char> cub_tmp;
+
+  // constraints
+  DevBuf<int> pin_vertex;
+  DevBuf<double> pin_target;
+  DevBuf<WallDev> walls;
+  int num_pins = 0, num_walls = 0;
+  WallDev first_wall_host{};
+
+  // rigid bodies
+  DevBuf<RigidDev> bodies_dev;
+  std::vector<RigidDev> bodies_host;
+  std::vector<DevBuf<double>*> body_local, body_world;
+  std::vector<DevBuf<int>*> body_tris;
+
+  ~ando_ctx_s() {
+    for (auto* b : body_local) delete b;
+    for (auto* b : body_world) delete b;
+    for (auto* b : body_tris) delete b;
+    if (ctrl_host) cudaFreeHost(ctrl_host);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  MeshDev mesh_dev() const {
+    MeshDev m;
+    m.V = V; m.T = T; m.nnzb = nnzb; m.mu = mu; m.thickness = thickness; m.density = density;
+    m.tris = tris.p; m.rest_area = rest_area.p; m.dm_inv = dm_inv.p; m.mass = mass.p;
+    m.rowptr = rowptr.p; m.cols = cols.p; m.slot_row = slot_row.p; m.diag_slot = diag_slot.p;
+    m.face_slot = face_slot.p; m.slot_cptr = slot_cptr.p; m.slot_contrib = slot_contrib.p;
+    m.vf_ptr = vf_ptr.p; m.vf = vf.p; m.el_a = el_a.p; m.el_b = el_b.p; m.g_elastic = g_el.p;
+    return m;
+  }
+
+  cudaError_t cub_reserve(size_t bytes) { return cub_tmp.reserve(bytes); }
+};
+
+namespace {
+
+int check_ctx(ando_ctx c) {
+  if (!c) return fail(ANDO_ERR_INVALID, "null context");
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return fail(ANDO_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return ANDO_OK;
+}
+
+double to_fraction(double v) { return v > 1.0 ? v * 0.01 : v; }
+
+StepParams make_step_params(const ando_params& p, int num_walls, int first_wall) {
+  StepParams s;
+  s.dt = p.dt; s.dt2inv = 1.0 / (p.dt * p.dt);
+  s.contact_gap_max = p.contact_gap_max; s.wall_gap = p.wall_gap; s.normal_eps = p.contact_normal_epsilon;
+  s.barrier_tol = p.barrier_tolerance; s.min_gap = p.min_gap;
+  s.friction_mu = p.friction_mu; s.friction_eps = p.friction_epsilon; s.friction_thresh = p.friction_tangent_threshold;
+  s.enable_friction = p.enable_friction; s.enable_strain = p.enable_strain_limiting; s.semantics = p.semantics;
+  double tau = to_fraction(p.strain_tau);
+  double eps = p.strain_epsilon > 0.0 ? to_fraction(p.strain_epsilon) : tau;
+  s.strain_tau = tau; s.strain_eps = eps; s.svd_eps = std::max(p.strain_svd_epsilon, 1e-8);
+  s.num_walls = num_walls; s.first_wall = first_wall;
+  return s;
+}
+
+// Contact detection at the current positions into ctx->contacts (order of
+// Collision::detect_all_collisions: vertex-triangle by vertex, then rigid
+// contacts by body, vertex and triangle).
+int detect(ando_ctx c, int nb) {
+  MeshDev m = c->mesh_dev();
+  long long units = (long long)c->V * (1 + nb);
+  int literal_pt = (c->T == 1) ? 1 : 0;
+  CK(c->det_counts.reserve(units + 1));
+  CK(c->det_offsets.reserve(units + 1));
+  launch_detect_count(m, c->x.p, c->bodies_dev.p, nb, literal_pt, c->det_counts.p, c->stream);
+  CK(cudaMemsetAsync(c->det_counts.p + units, 0, sizeof(int), c->stream));
+  size_t bytes = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->det_counts.p, c->det_offsets.p, (int)(units + 1), c->stream));
+  CK(c->cub_reserve(bytes));
+  CK(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, bytes, c->det_counts.p, c->det_offsets.p, (int)(units + 1), c->stream));
+  int total = 0;
+  CK(cudaMemcpyAsync(&total, c->det_offsets.p + units, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->ncontacts = total;
+  CK(c->contacts.reserve(total));
+  if (total) launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, literal_pt, c->det_offsets.p, c->contacts.p, c->stream);
+  c->n_pe = literal_pt ? total : 0;  // only the literal vertex-triangle case produces PT contacts
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+
+// Per-step contact constants: k_bar and barrier derivatives at the frozen
+// gap, the per-vertex constant gradient/diagonal, and the extra off-diagonal
+// block segment sorted by row.
+int prepare_contacts(ando_ctx c, const StepParams& sp) {
+  MeshDev m = c->mesh_dev();
+  int nc = c->ncontacts, V = c->V;
+  launch_contact_prep(m, c->contacts.p, nc, sp, c->stream);
+  int ne = 16 * nc;
+  c->nent = ne;
+  CK(c->ekeys.reserve(ne + 1)); CK(c->ekeys_sorted.reserve(ne + 1));
+  CK(c->ents.reserve(ne + 1)); CK(c->ents_sorted.reserve(ne + 1));
+  CK(c->ebegin.reserve(V)); CK(c->eend.reserve(V));
+  CK(c->xflags.reserve(ne + 1)); CK(c->xkeys.reserve(ne + 1)); CK(c->xent.reserve(ne + 1));
+  CK(c->xcols.reserve(ne + 1)); CK(c->xval.reserve(9ull * (ne + 1))); CK(c->xbegin.reserve(V)); CK(c->xend.reserve(V));
+  CK(c->nsel.reserve(1));
+  if (ne == 0) {
+    CK(cudaMemsetAsync(c->ebegin.p, 0, sizeof(int) * V, c->stream));
+    CK(cudaMemsetAsync(c->eend.p, 0, sizeof(int) * V, c->stream));
+    c->nx = 0;
+    launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, c->g_const.p, c->diag_const.p, c->stream);
+    CK(cudaGetLastError());
+    return ANDO_OK;
+  }
+  launch_contact_entries(c->contacts.p, nc, V, sp.enable_friction && sp.friction_mu > 0.0, c->ekeys.p, c->ents.p, c->stream);
+  int bits = 1;
+  while ((1ll << bits) <= (long long)V) ++bits;
+  size_t bytes = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, c->ekeys.p, c->ekeys_sorted.p, c->ents.p, c->ents_sorted.p, ne, 0, bits, c->stream));
+  CK(c->cub_reserve(bytes));
+  CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, c->ekeys.p, c->ekeys_sorted.p, c->ents.p, c->ents_sorted.p, ne, 0, bits, c->stream));
+  launch_vertex_ranges(c->ekeys_sorted.p, ne, V, c->ebegin.p, c->eend.p, c->stream);
+  launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, c->g_const.p, c->diag_const.p, c->stream);
+  // extra segment: off-diagonal barrier blocks, kept in row order
+  launch_extra_flags(c->ents_sorted.p, c->ekeys_sorted.p, ne, c->xflags.p, c->stream);
+  bytes = 0;
+  CK(cub::DeviceSelect::Flagged(nullptr, bytes, c->ents_sorted.p, c->xflags.p, c->xent.p, c->nsel.p, ne, c->stream));
+  CK(c->cub_reserve(bytes));
+  CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, c->ents_sorted.p, c->xflags.p, c->xent.p, c->nsel.p, ne, c->stream));
+  CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, c->ekeys_sorted.p, c->xflags.p, c->xkeys.p, c->nsel.p, ne, c->stream));
+  int nx = 0;
+  CK(cudaMemcpyAsync(&nx, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->nx = nx;
+  launch_extra_values(c->contacts.p, c->xent.p, c->xcols.p, nx, sp, c->xval.p, c->stream);
+  launch_vertex_ranges(c->xkeys.p, nx, V, c->xbegin.p, c->xend.p, c->stream);
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+
+int upload_rigids(ando_ctx c, const ando_rigid* rigids, int nb) {
+  while ((int)c->body_local.size() < nb) {
+    c->body_local.push_back(new DevBuf<double>());
+    c->body_world.push_back(new DevBuf<double>());
+    c->body_tris.push_back(new DevBuf<int>());
+  }
+  c->bodies_host.resize(nb);
+  for (int i = 0; i < nb; ++i) {
+    const ando_rigid& r = rigids[i];
+    if (r.num_vertices < 0 || r.num_triangles < 0 || (r.num_vertices && !r.local_vertices) || (r.num_triangles && !r.triangles))
+      return fail(ANDO_ERR_INVALID, "rigid body arrays");
+    for (int t = 0; t < 3 * r.num_triangles; ++t)
+      if (r.triangles[t] < 0 || r.triangles[t] >= r.num_vertices) return fail(ANDO_ERR_INVALID, "rigid triangle index out of range");
+    CK(c->body_local[i]->upload(r.local_vertices, 3ull * r.num_vertices, c->stream));
+    CK(c->body_world[i]->reserve(3ull * r.num_vertices));
+    CK(c->body_tris[i]->upload(r.triangles, 3ull * r.num_triangles, c->stream));
+    RigidDev& B = c->bodies_host[i];
+    B.nv = r.num_vertices; B.nt = r.num_triangles;
+    B.local = c->body_local[i]->p; B.world = c->body_world[i]->p; B.tris = c->body_tris[i]->p;
+    std::memcpy(B.pos, r.position, sizeof(B.pos)); std::memcpy(B.R, r.rotation, sizeof(B.R));
+    std::memcpy(B.Iinv_body, r.inertia_body_inv, sizeof(B.Iinv_body)); B.mass = r.mass;
+    std::memcpy(B.lin, r.linear_velocity, sizeof(B.lin)); std::memcpy(B.ang, r.angular_velocity, sizeof(B.ang));
+  }
+  CK(c->bodies_dev.upload(c->bodies_host.data(), nb, c->stream));
+  if (nb) launch_rigid_world(c->bodies_dev.p, c->bodies_host.data(), nb, c->stream);
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+
+struct NewtonOut { double ret; };
+
+// Integrator::inner_newton_step (integrator.cpp:152-236).
+int inner_newton(ando_ctx c, const ando_params& p, const StepParams& sp, ando_step_stats& st, double& ret) {
+  MeshDev m = c->mesh_dev();
+  int max_it = p.max_newton_steps;
+  if (p.enable_friction) max_it = std::max(max_it, p.friction_min_newton_steps);
+  // the line search takes the first active wall's stored normal unchanged and
+  // tests squaredNorm > 0.5 (integrator.cpp:204-213, line_search.cpp:132)
+  WallDev first_wall = c->first_wall_host;
+  bool ls_wall = sp.first_wall >= 0 &&
+                 first_wall.n[0] * first_wall.n[0] + first_wall.n[1] * first_wall.n[1] + first_wall.n[2] * first_wall.n[2] > 0.5;
+  PcgArgs pa;
+  pa.V = c->V; pa.rowptr = c->rowptr.p; pa.cols = c->cols.p; pa.val = c->val.p;
+  pa.xbegin = c->nx ? c->xbegin.p : nullptr; pa.xend = c->nx ? c->xend.p : nullptr; pa.xcols = c->xcols.p; pa.xval = c->xval.p;
+  pa.P = c->precond.p; pa.b = c->b.p; pa.x = c->d.p; pa.r = c->r.p; pa.z = c->z.p; pa.p0 = c->p0.p; pa.p1 = c->p1.p; pa.Ap = c->Ap.p;
+  pa.partials = c->partials.p; pa.ctrl = c->ctrl.p; pa.tol = float(p.pcg_tol); pa.max_iters = p.pcg_max_iters;
+  for (int it = 0; it < max_it; ++it) {
+    launch_ctrl_reset(c->ctrl.p, c->stream);
+    if (sp.enable_strain) launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, c->stream);
+    launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
+                    c->pin_vertex.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
+                    c->ebegin.p, c->eend.p, sp, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, c->stream);
+    launch_check(c->ctrl.p, p.pcg_tol, c->stream);
+    launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->val.p, c->precond.p, c->ctrl.p, c->stream);
+    CK(launch_pcg(pa, c->pcg_grid, c->stream));
+    if (ls_wall) launch_ls_wall(c->V, c->x.p, c->d.p, first_wall, c->ctrl.p, c->stream);
+    if (c->n_pe) launch_ls_contacts(c->contacts.p, c->ncontacts, c->x.p, c->d.p, c->ctrl.p, c->stream);
+    launch_update(c->V, c->x.p, c->d.p, c->ctrl.p, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const Ctrl& h = *c->ctrl_host;
+    st.strain_active = h.strain_active;
+    if (h.converged) { ret = 1.0; return ANDO_OK; }
+    if (h.pcg_status == PCG_TIMEOUT || h.bar_err) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
+    st.newton_iters++;
+    st.pcg_iters += h.pcg_iters;
+    st.pcg_max_per_newton = std::max(st.pcg_max_per_newton, h.pcg_iters);
+    if (!h.pcg_converged) st.pcg_not_converged++;
+    st.last_alpha = h.alpha;
+    if (h.alpha < 1e-8) { ret = 0.0; return ANDO_OK; }
+    if (h.alpha > 0.99) { ret = 1.0; return ANDO_OK; }
+  }
+  ret = 0.5;
+  return ANDO_OK;
+}
+
+// Upload this step's pins (active ones, stably sorted by vertex), walls and
+// rigid bodies, and refresh the elastic blocks when the semantics changed.
+int upload_constraints(ando_ctx c, const ando_params& p, const ando_pin* pins, int num_pins, const ando_wall* walls, int num_walls,
+                       ando_rigid* rigids, int num_rigids, StepParams& sp) {
+  cudaStream_t s = c->stream;
+  if (c->el_semantics != p.semantics) {
+    launch_elastic_slots(c->mesh_dev(), c->mu, c->thickness, p.semantics, c->el_a.p, c->el_b.p, s);
+    c->el_semantics = p.semantics;
+  }
+  std::vector<int> order;
+  for (int k = 0; k < num_pins; ++k) {
+    if (!pins[k].active) continue;
+    if (pins[k].vertex < 0 || pins[k].vertex >= c->V) return fail(ANDO_ERR_INVALID, "pin vertex out of range");
+    order.push_back(k);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pins[a].vertex < pins[b].vertex; });
+  std::vector<int> pv(order.size());
+  std::vector<double> pt(3 * order.size());
+  for (size_t k = 0; k < order.size(); ++k) {
+    pv[k] = pins[order[k]].vertex;
+    for (int q = 0; q < 3; ++q) pt[3 * k + q] = pins[order[k]].target[q];
+  }
+  c->num_pins = (int)order.size();
+  CK(c->pin_vertex.upload(pv.data(), pv.size(), s));
+  CK(c->pin_target.upload(pt.data(), pt.size(), s));
+  std::vector<WallDev> wd(num_walls);
+  int first_wall = -1;
+  for (int k = 0; k < num_walls; ++k) {
+    for (int q = 0; q < 3; ++q) wd[k].n[q] = walls[k].normal[q];
+    wd[k].offset = walls[k].offset; wd[k].gap = walls[k].gap; wd[k].active = walls[k].active;
+    if (walls[k].active && first_wall < 0) { first_wall = k; c->first_wall_host = wd[k]; }
+  }
+  c->num_walls = num_walls;
+  CK(c->walls.upload(wd.data(), wd.size(), s));
+  int rc = upload_rigids(c, rigids, num_rigids);
+  if (rc) return rc;
+  sp = make_step_params(p, num_walls, first_wall);
+  return ANDO_OK;
+}
+
+// beta accumulation, error-reduction pass, velocity update, damping,
+// restitution and rigid coupling (integrator.cpp:98-149).
+int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_rigids, int num_walls, ando_step_stats& st) {
+  cudaStream_t s = c->stream;
+  int rc;
+  double beta = 0.0;
+  int bi = 0;
+  while (beta < p.beta_max && bi < 20) {
+    double alpha = 0.0;
+    rc = inner_newton(c, p, sp, st, alpha);
+    if (rc) return rc;
+    beta = beta + (1.0 - beta) * alpha;
+    ++bi;
+    if (alpha < 1e-6) { st.line_search_fail++; break; }
+  }
+  if (beta > 1e-6) {
+    double a2 = 0.0;
+    rc = inner_newton(c, p, sp, st, a2);
+    if (rc) return rc;
+  }
+  st.beta = beta;
+  if (beta > 1e-6) {
+    double damp = p.velocity_damping > 0.0 ? 1.0 - std::min(std::max(p.velocity_damping, 0.0), 1.0) : 1.0;
+    launch_velocity(c->V, c->x.p, c->x_old.p, beta * p.dt, damp, c->v.p, s);
+    if (p.contact_restitution > 0.0) {
+      double e = std::min(std::max(p.contact_restitution, 0.0), 1.0);
+      rc = detect(c, num_rigids);
+      if (rc) return rc;
+      launch_restitution_contacts(c->contacts.p, c->ncontacts, c->mass.p, c->V, e, std::max(p.contact_gap_max, 1e-5),
+                                  c->bodies_dev.p, num_rigids, c->v.p, s);
+      launch_restitution_walls(c->V, c->x.p, c->walls.p, num_walls, e, p.contact_gap_max, c->v.p, s);
+    }
+  }
+  if (num_rigids > 0) {
+    rc = detect(c, num_rigids);
+    if (rc) return rc;
+    long long units = (long long)c->V * (1 + num_rigids);
+    launch_rigid_coupling(c->mesh_dev(), c->contacts.p, c->ncontacts, sp, c->bodies_dev.p, num_rigids, c->det_offsets.p, units, p.dt, s);
+    CK(cudaMemcpyAsync(c->bodies_host.data(), c->bodies_dev.p, sizeof(RigidDev) * num_rigids, cudaMemcpyDeviceToHost, s));
+  }
+  return ANDO_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int32_t ando_abi_version(void) { return ANDO_ABI_VERSION; }
+
+const char* ando_status_string(int32_t s) {
+  switch (s) {
+    case ANDO_OK: return "ok";
+    case ANDO_ERR_INVALID: return "invalid argument";
+    case ANDO_ERR_CUDA: return "CUDA error";
+    case ANDO_ERR_STATE: return "call out of order";
+    case ANDO_ERR_TIMEOUT: return "device wait timed out";
+    case ANDO_ERR_NO_DEVICE: return "no usable CUDA device";
+    case ANDO_ERR_CAPACITY: return "buffer too small";
+    default: return "unknown status";
+  }
+}
+
+const char* ando_last_error(void) { return g_last_error.c_str(); }
+
+int32_t ando_ctx_create(int32_t device, ando_ctx* out) {
+  if (!out) return fail(ANDO_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(ANDO_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= n) return fail(ANDO_ERR_INVALID, "device index out of range");
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(ANDO_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
+  CK(cudaSetDevice(device));
+  ando_ctx c = new ando_ctx_s();
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e == cudaSuccess) e = cudaMallocHost(&c->ctrl_host, sizeof(Ctrl));
+  if (e == cudaSuccess) e = c->ctrl.reserve(1);
+  if (e == cudaSuccess) e = cudaMemset(c->ctrl.p, 0, sizeof(Ctrl));
+  if (e != cudaSuccess) { delete c; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
+  c->pcg_grid = pcg_grid_size(device);
+  e = c->partials.reserve(3ull * std::max(c->pcg_grid, 1));
+  if (e != cudaSuccess) { delete c; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
+  *out = c;
+  return ANDO_OK;
+}
+
+void ando_ctx_destroy(ando_ctx c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete c;
+}
+
+int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const int32_t* tris, int32_t T,
+                         const double* rest_areas, const double* dm_inv, const ando_material* mat) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (V <= 0 || T < 0 || !vertices || (T && (!tris || !rest_areas || !dm_inv)) || !mat)
+    return fail(ANDO_ERR_INVALID, "mesh arrays");
+  for (long long k = 0; k < 3ll * T; ++k)
+    if (tris[k] < 0 || tris[k] >= V) return fail(ANDO_ERR_INVALID, "triangle index out of range");
+  // Static block pattern: self blocks plus every (a, b) vertex pair of every face.
+  std::vector<std::vector<int>> adj(V);
+  for (int i = 0; i < V; ++i) adj[i].push_back(i);
+  for (int f = 0; f < T; ++f)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) adj[tris[3 * f + a]].push_back(tris[3 * f + b]);
+  std::vector<int> rowptr(V + 1, 0), cols, slot_row, diag_slot(V);
+  for (int i = 0; i < V; ++i) {
+    auto& r = adj[i];
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    for (int cidx : r) { if (cidx == i) diag_slot[i] = (int)cols.size(); cols.push_back(cidx); slot_row.push_back(i); }
+    rowptr[i + 1] = (int)cols.size();
+    std::vector<int>().swap(r);
+  }
+  const int nnzb = (int)cols.size();
+  auto slot_of = [&](int r, int col) {
+    auto b = cols.begin() + rowptr[r], e = cols.begin() + rowptr[r + 1];
+    return int(std::lower_bound(b, e, col) - cols.begin());
+  };
+  std::vector<int> face_slot(9ull * T), cptr(nnzb + 1, 0), contrib(9ull * T), vfp(V + 1, 0), vfl(3ull * T);
+  for (int f = 0; f < T; ++f)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        int s = slot_of(tris[3 * f + a], tris[3 * f + b]);
+        face_slot[9ull * f + 3 * a + b] = s;
+        cptr[s + 1]++;
+      }
+  for (int s = 0; s < nnzb; ++s) cptr[s + 1] += cptr[s];
+  {
+    std::vector<int> pos(cptr.begin(), cptr.end() - 1);
+    for (int f = 0; f < T; ++f)
+      for (int k = 0; k < 9; ++k) contrib[pos[face_slot[9ull * f + k]]++] = 9 * f + k;
+  }
+  for (int f = 0; f < T; ++f) for (int a = 0; a < 3; ++a) vfp[tris[3 * f + a] + 1]++;
+  for (int i = 0; i < V; ++i) vfp[i + 1] += vfp[i];
+  {
+    std::vector<int> pos(vfp.begin(), vfp.end() - 1);
+    for (int f = 0; f < T; ++f) for (int a = 0; a < 3; ++a) vfl[pos[tris[3 * f + a]]++] = 3 * f + a;
+  }
+  cudaStream_t s = c->stream;
+  c->V = V; c->T = T; c->nnzb = nnzb;
+  c->mu = mat->youngs_modulus / (2.0 * (1.0 + mat->poisson_ratio));
+  c->thickness = mat->thickness; c->density = mat->density;
+  CK(c->tris.upload(tris, 3ull * T, s));
+  CK(c->rest_area.upload(rest_areas, T, s));
+  CK(c->dm_inv.upload(dm_inv, 4ull * T, s));
+  CK(c->rowptr.upload(rowptr.data(), V + 1, s));
+  CK(c->cols.upload(cols.data(), nnzb, s));
+  CK(c->slot_row.upload(slot_row.data(), nnzb, s));
+  CK(c->diag_slot.upload(diag_slot.data(), V, s));
+  CK(c->face_slot.upload(face_slot.data(), 9ull * T, s));
+  CK(c->slot_cptr.upload(cptr.data(), nnzb + 1, s));
+  CK(c->slot_contrib.upload(contrib.data(), 9ull * T, s));
+  CK(c->vf_ptr.upload(vfp.data(), V + 1, s));
+  CK(c->vf.upload(vfl.data(), 3ull * T, s));
+  CK(c->mesh_x.upload(vertices, 3ull * V, s));
+  CK(c->el_a.reserve(nnzb)); CK(c->el_b.reserve(nnzb)); CK(c->g_el.reserve(3ull * V));
+  // per-vertex / per-slot work buffers
+  CK(c->x.reserve(3ull * V)); CK(c->v.reserve(3ull * V)); CK(c->x_prev.reserve(3ull * V)); CK(c->mass.reserve(V));
+  CK(c->x_old.reserve(3ull * V)); CK(c->x_hat.reserve(3ull * V)); CK(c->g.reserve(3ull * V));
+  CK(c->g_const.reserve(3ull * V)); CK(c->diag_const.reserve(9ull * V)); CK(c->diag_extra.reserve(9ull * V));
+  CK(c->b.reserve(3ull * V)); CK(c->d.reserve(3ull * V)); CK(c->r.reserve(3ull * V)); CK(c->z.reserve(3ull * V));
+  CK(c->p0.reserve(3ull * V)); CK(c->p1.reserve(3ull * V)); CK(c->Ap.reserve(3ull * V));
+  CK(c->val.reserve(9ull * nnzb)); CK(c->precond.reserve(9ull * V));
+  CK(c->sflags.reserve(std::max(T, 1))); CK(c->sv.reserve(2ull * std::max(T, 1)));
+  CK(cudaMemsetAsync(c->sflags.p, 0, std::max(T, 1), s));
+  CK(cudaMemsetAsync(c->d.p, 0, sizeof(float) * 3ull * V, s));
+  c->el_semantics = -1;
+  c->mesh_ready = true;
+  c->state_ready = false;
+  MeshDev m = c->mesh_dev();
+  launch_elastic_gradient(m, c->mesh_x.p, c->mu, c->thickness, c->g_el.p, s);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  return ANDO_OK;
+}
+
+int32_t ando_mesh_set_vertices(ando_ctx c, const double* vertices, int32_t V) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready) return fail(ANDO_ERR_STATE, "mesh not uploaded");
+  if (!vertices || V != c->V) return fail(ANDO_ERR_INVALID, "vertex count mismatch");
+  CK(c->mesh_x.upload(vertices, 3ull * V, c->stream));
+  launch_elastic_gradient(c->mesh_dev(), c->mesh_x.p, c->mu, c->thickness, c->g_el.p, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return ANDO_OK;
+}
+
+int32_t ando_state_upload(ando_ctx c, const double* x, const double* v, const double* xp, const double* mass, int32_t V) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready) return fail(ANDO_ERR_STATE, "mesh not uploaded");
+  if (V != c->V) return fail(ANDO_ERR_INVALID, "vertex count mismatch");
+  if (!c->state_ready && (!x || !v || !xp || !mass)) return fail(ANDO_ERR_INVALID, "first state upload needs every array");
+  if (x) CK(cudaMemcpyAsync(c->x.p, x, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
+  if (v) CK(cudaMemcpyAsync(c->v.p, v, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
+  if (xp) CK(cudaMemcpyAsync(c->x_prev.p, xp, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
+  if (mass) CK(cudaMemcpyAsync(c->mass.p, mass, sizeof(double) * V, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->state_ready = true;
+  return ANDO_OK;
+}
+
+int32_t ando_state_download(ando_ctx c, double* x, double* v, int32_t V) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->state_ready) return fail(ANDO_ERR_STATE, "state not uploaded");
+  if (V != c->V) return fail(ANDO_ERR_INVALID, "vertex count mismatch");
+  if (x) CK(cudaMemcpyAsync(x, c->x.p, sizeof(double) * 3ull * V, cudaMemcpyDeviceToHost, c->stream));
+  if (v) CK(cudaMemcpyAsync(v, c->v.p, sizeof(double) * 3ull * V, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ANDO_OK;
+}
+
+int32_t ando_apply_gravity(ando_ctx c, const double g[3], double dt) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->state_ready) return fail(ANDO_ERR_STATE, "state not uploaded");
+  if (!g) return fail(ANDO_ERR_INVALID, "null gravity");
+  launch_gravity(c->V, c->x.p, c->v.p, g[0], g[1], g[2], dt, c->stream);
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+
+int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, int32_t num_pins,
+                  const ando_wall* walls, int32_t num_walls, ando_rigid* rigids, int32_t num_rigids,
+                  ando_step_stats* stats) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  if (!params || num_pins < 0 || num_walls < 0 || num_rigids < 0 || (num_pins && !pins) || (num_walls && !walls) || (num_rigids && !rigids))
+    return fail(ANDO_ERR_INVALID, "step arguments");
+  const ando_params& p = *params;
+  if (p.semantics != ANDO_SEMANTICS_REFERENCE) return fail(ANDO_ERR_INVALID, "only REFERENCE semantics is implemented");
+  if (p.precond != ANDO_PRECOND_BLOCK_JACOBI) return fail(ANDO_ERR_INVALID, "preconditioner not available");
+  ando_step_stats st;
+  std::memset(&st, 0, sizeof(st));
+  cudaStream_t s = c->stream;
+  CK(cudaEventRecord(c->ev0, s));
+  StepParams sp;
+  rc = upload_constraints(c, p, pins, num_pins, walls, num_walls, rigids, num_rigids, sp);
+  if (rc) return rc;
+  launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
+  rc = detect(c, num_rigids);
+  if (rc) return rc;
+  st.contacts = c->ncontacts;
+  rc = prepare_contacts(c, sp);
+  if (rc) return rc;
+  rc = step_body(c, p, sp, num_rigids, num_walls, st);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev1, s));
+  CK(cudaEventSynchronize(c->ev1));
+  for (int i = 0; i < num_rigids; ++i) {
+    const RigidDev& B = c->bodies_host[i];
+    std::memcpy(rigids[i].position, B.pos, sizeof(B.pos)); std::memcpy(rigids[i].rotation, B.R, sizeof(B.R));
+    std::memcpy(rigids[i].linear_velocity, B.lin, sizeof(B.lin)); std::memcpy(rigids[i].angular_velocity, B.ang, sizeof(B.ang));
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  st.device_ms = ms;
+  st.status = ANDO_OK;
+  if (stats) *stats = st;
+  return ANDO_OK;
+}
+
+int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* pins, int32_t num_pins,
+                         const ando_wall* walls, int32_t num_walls, const ando_rigid* rigids, int32_t num_rigids) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  if (!params || num_pins < 0 || num_walls < 0 || num_rigids < 0 || (num_pins && !pins) || (num_walls && !walls) || (num_rigids && !rigids))
+    return fail(ANDO_ERR_INVALID, "system arguments");
+  const ando_params& p = *params;
+  if (p.semantics != ANDO_SEMANTICS_REFERENCE) return fail(ANDO_ERR_INVALID, "only REFERENCE semantics is implemented");
+  std::vector<ando_rigid> copy(rigids, rigids + num_rigids);
+  StepParams sp;
+  rc = upload_constraints(c, p, pins, num_pins, walls, num_walls, copy.data(), num_rigids, sp);
+  if (rc) return rc;
+  cudaStream_t s = c->stream;
+  launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
+  rc = detect(c, num_rigids);
+  if (rc) return rc;
+  rc = prepare_contacts(c, sp);
+  if (rc) return rc;
+  MeshDev m = c->mesh_dev();
+  launch_ctrl_reset(c->ctrl.p, s);
+  if (sp.enable_strain) launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, s);
+  launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
+                  c->pin_vertex.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
+                  c->ebegin.p, c->eend.p, sp, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, s);
+  launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->val.p, c->precond.p, c->ctrl.p, s);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  return ANDO_OK;
+}
+
+int32_t ando_compute_contacts(ando_ctx c, const ando_rigid* rigids, int32_t num_rigids, ando_contact* out, int32_t capacity, int32_t* num_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  if (!num_out || capacity < 0 || (capacity && !out) || num_rigids < 0 || (num_rigids && !rigids)) return fail(ANDO_ERR_INVALID, "contact arguments");
+  // rigid bodies are read-only here (a copy of the caller's structs)
+  std::vector<ando_rigid> copy(rigids, rigids + num_rigids);
+  rc = upload_rigids(c, copy.data(), num_rigids);
+  if (rc) return rc;
+  rc = detect(c, num_rigids);
+  if (rc) return rc;
+  *num_out = c->ncontacts;
+  if (c->ncontacts == 0) return ANDO_OK;
+  std::vector<ContactDev> h(c->ncontacts);
+  CK(cudaMemcpyAsync(h.data(), c->contacts.p, sizeof(ContactDev) * c->ncontacts, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int n = std::min(capacity, c->ncontacts);
+  for (int k = 0; k < n; ++k) {
+    const ContactDev& C = h[k];
+    ando_contact& o = out[k];
+    std::memset(&o, 0, sizeof(o));
+    o.type = C.type; o.idx0 = C.idx[0]; o.idx1 = C.idx[1]; o.idx2 = C.idx[2]; o.idx3 = C.idx[3];
+    o.rigid_body_index = C.rigid; o.vertex_count = C.count; o.gap = C.gap;
+    for (int q = 0; q < 3; ++q) { o.normal[q] = C.n[q]; o.witness_p[q] = C.wp[q]; o.witness_q[q] = C.wq[q]; o.barycentric[q] = C.bary[q]; }
+    for (int q = 0; q < 4; ++q) o.weights[q] = C.w[q];
+  }
+  return c->ncontacts > capacity ? fail(ANDO_ERR_CAPACITY, "contact buffer too small") : ANDO_OK;
+}
+
+int32_t ando_last_system(ando_ctx c, int32_t* V, int32_t* nnzb, int32_t* rowptr, int32_t* cols, float* vals, float* rhs, float* sol) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready) return fail(ANDO_ERR_STATE, "mesh not uploaded");
+  if (V) *V = c->V;
+  if (nnzb) *nnzb = c->nnzb;
+  cudaStream_t s = c->stream;
+  if (rowptr) CK(cudaMemcpyAsync(rowptr, c->rowptr.p, sizeof(int) * (c->V + 1), cudaMemcpyDeviceToHost, s));
+  if (cols) CK(cudaMemcpyAsync(cols, c->cols.p, sizeof(int) * c->nnzb, cudaMemcpyDeviceToHost, s));
+  if (vals) CK(cudaMemcpyAsync(vals, c->val.p, sizeof(float) * 9ull * c->nnzb, cudaMemcpyDeviceToHost, s));
+  if (rhs) CK(cudaMemcpyAsync(rhs, c->b.p, sizeof(float) * 3ull * c->V, cudaMemcpyDeviceToHost, s));
+  if (sol) CK(cudaMemcpyAsync(sol, c->d.p, sizeof(float) * 3ull * c->V, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return ANDO_OK;
+}
+
+int32_t ando_last_gradient(ando_ctx c, double* g, int32_t V) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready || !g || V != c->V) return fail(ANDO_ERR_INVALID, "gradient arguments");
+  CK(cudaMemcpyAsync(g, c->g.p, sizeof(double) * 3ull * V, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ANDO_OK;
+}
+
+}  // extern "C"

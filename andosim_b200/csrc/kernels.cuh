@@ -1,0 +1,73 @@
+// kernels.cuh -- kernel entry points of the step (definitions in kernels.cu / pcg.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace ando {
+
+struct RigidDev {
+  int nv, nt;
+  const double* local;  // 3nv
+  const int* tris;      // 3nt
+  double* world;        // 3nv (written per step)
+  double pos[3], R[9], Iinv_body[9], mass, lin[3], ang[3];
+};
+
+// setup
+void launch_elastic_slots(const MeshDev& m, double mu, double thickness, int semantics, double* el_a, double* el_b, cudaStream_t s);
+void launch_elastic_gradient(const MeshDev& m, const double* mesh_vertices, double mu, double thickness, double* g_el, cudaStream_t s);
+
+// per step
+void launch_predict(int V, const double* x, const double* v, double dt, double* x_old, double* x_hat, cudaStream_t s);
+void launch_gravity(int V, double* x, double* v, double gx, double gy, double gz, double dt, cudaStream_t s);
+void launch_rigid_world(RigidDev* bodies_dev, const RigidDev* bodies_host, int nb, cudaStream_t s);
+// contact detection: count per (PT vertex) + (rigid body, vertex); literal PT only when T == 1.
+void launch_detect_count(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, int* counts, cudaStream_t s);
+void launch_detect_write(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, const int* offsets, ContactDev* out, cudaStream_t s);
+void launch_contact_prep(const MeshDev& m, ContactDev* c, int nc, const StepParams& p, cudaStream_t s);
+void launch_contact_entries(const ContactDev* c, int nc, int V, int friction, int* keys, ContactEntry* ents, cudaStream_t s);
+void launch_vertex_ranges(const int* sorted_keys, int n, int V, int* begin, int* end, cudaStream_t s);
+void launch_contact_vertex(const MeshDev& m, const ContactDev* c, const ContactEntry* ents, const int* begin, const int* end,
+                           const StepParams& p, double* g_const, double* diag_const, cudaStream_t s);
+void launch_extra_flags(const ContactEntry* ents, const int* keys, int n, int* flags, cudaStream_t s);
+void launch_extra_values(const ContactDev* c, const ContactEntry* xent, int* xcols, int nx, const StepParams& p, float* xval, cudaStream_t s);
+
+// Newton iteration
+void launch_ctrl_reset(Ctrl* ctrl, cudaStream_t s);
+void launch_strain_face(const MeshDev& m, const double* x, const StepParams& p, unsigned char* flags, StrainSV* sv, Ctrl* ctrl, cudaStream_t s);
+void launch_gradient(const MeshDev& m, const double* x, const double* x_hat, const double* x_prev, const double* g_const,
+                     const double* diag_const, const unsigned char* sflags, const StrainSV* sv,
+                     const int* pin_vertex, const double* pin_target, int num_pins, const WallDev* walls,
+                     const ContactDev* contacts, const ContactEntry* ents, const int* ebegin, const int* eend,
+                     const StepParams& p, double* g, float* b, double* diag_extra, Ctrl* ctrl, cudaStream_t s);
+void launch_check(Ctrl* ctrl, double tol, cudaStream_t s);
+void launch_assemble(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                     float* val, float* precond, const Ctrl* ctrl, cudaStream_t s);
+void launch_ls_wall(int V, const double* x, const float* d, WallDev w, Ctrl* ctrl, cudaStream_t s);
+void launch_ls_contacts(const ContactDev* c, int nc, const double* x, const float* d, Ctrl* ctrl, cudaStream_t s);
+void launch_update(int V, double* x, const float* d, Ctrl* ctrl, cudaStream_t s);
+
+// end of step
+void launch_velocity(int V, const double* x, const double* x_old, double beta_dt, double damp_scale, double* v, cudaStream_t s);
+void launch_restitution_contacts(const ContactDev* c, int nc, const double* mass, int V, double e, double gap_limit,
+                                 RigidDev* bodies, int nb, double* v, cudaStream_t s);
+void launch_restitution_walls(int V, const double* x, const WallDev* walls, int nw, double e, double gap_max, double* v, cudaStream_t s);
+void launch_rigid_coupling(const MeshDev& m, const ContactDev* c, int nc, const StepParams& p, RigidDev* bodies, int nb,
+                           const int* offsets, long long units, double dt, cudaStream_t s);
+
+// PCG (pcg.cu)
+struct PcgArgs {
+  int V;
+  const int* rowptr; const int* cols; const float* val;
+  const int* xbegin; const int* xend; const int* xcols; const float* xval;  // extra contact segment
+  const float* P;     // block-Jacobi inverse, 9V
+  const float* b;
+  float *x, *r, *z, *p0, *p1, *Ap;
+  double* partials;   // 3 * grid
+  Ctrl* ctrl;
+  float tol; int max_iters;
+};
+int pcg_grid_size(int device);
+cudaError_t launch_pcg(const PcgArgs& a, int grid, cudaStream_t s);
+
+}  // namespace ando

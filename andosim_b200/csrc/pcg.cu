@@ -1,0 +1,222 @@
+// pcg.cu -- block-Jacobi preconditioned conjugate gradients as one persistent
+// cooperative kernel (replaces PCGSolver::solve, pcg_solver.cpp:8-146).
+//
+// Same iteration as the reference: x0 = 0, r = b, block-Jacobi z = P r,
+// stop when |r|_inf / |b|_inf < tol (or |r|_inf when |b|_inf < 1e-16), fail
+// when |p^T A p| < 1e-16. Vectors and the BSR matrix are FP32; every dot
+// product and norm is accumulated in FP64 and reduced in a fixed order, so
+// results are bitwise reproducible run to run.
+//
+// Per iteration there are two grid barriers:
+//   A: p_new = z + beta p_old (recomputed on the fly for gathered columns),
+//      Ap = A p_new with one warp per block row, partial p^T Ap
+//   B: x += alpha p, r -= alpha Ap, z = P r, partial r^T z and |r|_inf
+// The barrier is bounded (common.cuh): on timeout the kernel reports
+// PCG_TIMEOUT instead of spinning forever.
+#include "kernels.cuh"
+
+namespace ando {
+
+namespace {
+
+constexpr int PCG_TPB = 512;
+constexpr int PCG_WARPS = PCG_TPB / 32;
+
+__device__ inline double block_sum(double v, double* sh) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = l < PCG_WARPS ? sh[l] : 0.0;
+    for (int o = 16; o; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (l == 0) sh[0] = r;
+  }
+  __syncthreads();
+  r = sh[0];
+  __syncthreads();
+  return r;
+}
+__device__ inline double block_max(double v, double* sh) {
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = l < PCG_WARPS ? sh[l] : 0.0;
+    for (int o = 16; o; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+    if (l == 0) sh[0] = r;
+  }
+  __syncthreads();
+  r = sh[0];
+  __syncthreads();
+  return r;
+}
+// Every CTA reduces the per-CTA partials in the same order -> identical scalars everywhere.
+__device__ inline double grid_sum(const double* part, int n, double* sh) {
+  double v = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) v += part[k];
+  return block_sum(v, sh);
+}
+__device__ inline double grid_max(const double* part, int n, double* sh) {
+  double v = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) v = fmax(v, part[k]);
+  return block_max(v, sh);
+}
+
+__device__ inline void p_at(const float* z, const float* pold, float beta, bool first, int j, float& p0, float& p1, float& p2) {
+  float z0 = z[3 * j], z1 = z[3 * j + 1], z2 = z[3 * j + 2];
+  if (first) { p0 = z0; p1 = z1; p2 = z2; return; }
+  p0 = z0 + beta * pold[3 * j]; p1 = z1 + beta * pold[3 * j + 1]; p2 = z2 + beta * pold[3 * j + 2];
+}
+
+__global__ void __launch_bounds__(PCG_TPB) k_pcg(PcgArgs a) {
+  Ctrl* ctrl = a.ctrl;
+  if (ctrl->converged) return;
+  __shared__ double sh[PCG_WARPS + 1];
+  const int V = a.V;
+  const unsigned nb = gridDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  double* part_pap = a.partials;
+  double* part_rz = a.partials + nb;
+  double* part_rinf = a.partials + 2 * nb;
+
+  // init: x = 0, r = b, z = P r
+  double rz_loc = 0.0, binf_loc = 0.0;
+  for (int i = tid; i < V; i += nthreads) {
+    float r0 = a.b[3 * i], r1 = a.b[3 * i + 1], r2 = a.b[3 * i + 2];
+    const float* P = a.P + 9 * (long long)i;
+    float z0 = P[0] * r0 + P[1] * r1 + P[2] * r2, z1 = P[3] * r0 + P[4] * r1 + P[5] * r2, z2 = P[6] * r0 + P[7] * r1 + P[8] * r2;
+    a.x[3 * i] = 0.f; a.x[3 * i + 1] = 0.f; a.x[3 * i + 2] = 0.f;
+    a.r[3 * i] = r0; a.r[3 * i + 1] = r1; a.r[3 * i + 2] = r2;
+    a.z[3 * i] = z0; a.z[3 * i + 1] = z1; a.z[3 * i + 2] = z2;
+    rz_loc += double(r0) * z0 + double(r1) * z1 + double(r2) * z2;
+    binf_loc = fmax(binf_loc, fmax(fabs(double(r0)), fmax(fabs(double(r1)), fabs(double(r2)))));
+  }
+  rz_loc = block_sum(rz_loc, sh);
+  binf_loc = block_max(binf_loc, sh);
+  if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz_loc; part_rinf[blockIdx.x] = binf_loc; }
+  bool ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+  int status = PCG_MAXIT, iters = 0;
+  double rel = 0.0;
+  if (!ok) status = PCG_TIMEOUT;
+  double rz = ok ? grid_sum(part_rz, nb, sh) : 0.0;
+  double binf = ok ? grid_max(part_rinf, nb, sh) : 0.0;
+  if (ok) {
+    rel = binf < 1e-16 ? binf : 1.0;
+    if (rel < double(a.tol)) status = PCG_OK;
+  }
+  float* pold = a.p0;
+  float* pnew = a.p1;
+  float beta = 0.f;
+  bool first = true;
+  const int lane = threadIdx.x & 31;
+  const int gwarp = tid >> 5, nwarps = nthreads >> 5;
+  const int comp = lane >> 3, bi = lane & 7;
+  for (int it = 0; ok && status == PCG_MAXIT && it < a.max_iters; ++it) {
+    // ---- phase A: p_new, Ap = A p_new, p^T Ap
+    double pap_loc = 0.0;
+    for (int row = gwarp; row < V; row += nwarps) {
+      float acc = 0.f;
+      int s0 = a.rowptr[row], s1 = a.rowptr[row + 1];
+      for (int k0 = s0; k0 < s1; k0 += 8) {
+        int k = k0 + bi;
+        if (comp < 3 && k < s1) {
+          int col = a.cols[k];
+          const float* h = a.val + 9 * (long long)k + 3 * comp;
+          float q0, q1, q2; p_at(a.z, pold, beta, first, col, q0, q1, q2);
+          acc += h[0] * q0 + h[1] * q1 + h[2] * q2;
+        }
+      }
+      if (a.xbegin) {
+        int e0 = a.xbegin[row], e1 = a.xend[row];
+        for (int k0 = e0; k0 < e1; k0 += 8) {
+          int k = k0 + bi;
+          if (comp < 3 && k < e1) {
+            int col = a.xcols[k];
+            const float* h = a.xval + 9 * (long long)k + 3 * comp;
+            float q0, q1, q2; p_at(a.z, pold, beta, first, col, q0, q1, q2);
+            acc += h[0] * q0 + h[1] * q1 + h[2] * q2;
+          }
+        }
+      }
+      acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+      float y0 = __shfl_sync(0xffffffffu, acc, 0), y1 = __shfl_sync(0xffffffffu, acc, 8), y2 = __shfl_sync(0xffffffffu, acc, 16);
+      if (lane == 0) {
+        float q0, q1, q2; p_at(a.z, pold, beta, first, row, q0, q1, q2);
+        pnew[3 * row] = q0; pnew[3 * row + 1] = q1; pnew[3 * row + 2] = q2;
+        a.Ap[3 * row] = y0; a.Ap[3 * row + 1] = y1; a.Ap[3 * row + 2] = y2;
+        pap_loc += double(q0) * y0 + double(q1) * y1 + double(q2) * y2;
+      }
+    }
+    pap_loc = block_sum(pap_loc, sh);
+    if (threadIdx.x == 0) part_pap[blockIdx.x] = pap_loc;
+    ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+    if (!ok) { status = PCG_TIMEOUT; break; }
+    double pap = grid_sum(part_pap, nb, sh);
+    iters = it + 1;
+    if (fabs(pap) < 1e-16) { status = PCG_NOT_SPD; break; }
+    float alpha = float(rz / pap);
+    // ---- phase B: x, r, z, r^T z, |r|_inf
+    double rz_new_loc = 0.0, rinf_loc = 0.0;
+    for (int i = tid; i < V; i += nthreads) {
+      float p0 = pnew[3 * i], p1 = pnew[3 * i + 1], p2 = pnew[3 * i + 2];
+      float q0 = a.Ap[3 * i], q1 = a.Ap[3 * i + 1], q2 = a.Ap[3 * i + 2];
+      a.x[3 * i] += alpha * p0; a.x[3 * i + 1] += alpha * p1; a.x[3 * i + 2] += alpha * p2;
+      float r0 = a.r[3 * i] - alpha * q0, r1 = a.r[3 * i + 1] - alpha * q1, r2 = a.r[3 * i + 2] - alpha * q2;
+      a.r[3 * i] = r0; a.r[3 * i + 1] = r1; a.r[3 * i + 2] = r2;
+      const float* P = a.P + 9 * (long long)i;
+      float z0 = P[0] * r0 + P[1] * r1 + P[2] * r2, z1 = P[3] * r0 + P[4] * r1 + P[5] * r2, z2 = P[6] * r0 + P[7] * r1 + P[8] * r2;
+      a.z[3 * i] = z0; a.z[3 * i + 1] = z1; a.z[3 * i + 2] = z2;
+      rz_new_loc += double(r0) * z0 + double(r1) * z1 + double(r2) * z2;
+      rinf_loc = fmax(rinf_loc, fmax(fabs(double(r0)), fmax(fabs(double(r1)), fabs(double(r2)))));
+    }
+    rz_new_loc = block_sum(rz_new_loc, sh);
+    rinf_loc = block_max(rinf_loc, sh);
+    if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz_new_loc; part_rinf[blockIdx.x] = rinf_loc; }
+    ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+    if (!ok) { status = PCG_TIMEOUT; break; }
+    double rz_new = grid_sum(part_rz, nb, sh);
+    double rinf = grid_max(part_rinf, nb, sh);
+    rel = binf < 1e-16 ? rinf : rinf / binf;
+    if (rel < double(a.tol)) { status = PCG_OK; break; }
+    beta = float(rz_new / rz);
+    rz = rz_new;
+    first = false;
+    float* t = pold; pold = pnew; pnew = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctrl->pcg_iters = iters;
+    ctrl->pcg_status = status;
+    ctrl->pcg_converged = status == PCG_OK ? 1 : 0;
+    ctrl->pcg_rel = rel;
+  }
+}
+
+}  // namespace
+
+int pcg_grid_size(int device) {
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg, PCG_TPB, 0);
+  if (per_sm < 1) per_sm = 1;
+  int co = sms * per_sm;
+  int want = 2 * sms;
+  return co < want ? co : want;
+}
+
+cudaError_t launch_pcg(const PcgArgs& a, int grid, cudaStream_t s) {
+  int need = (a.V + PCG_TPB - 1) / PCG_TPB;  // enough CTAs for one vertex per thread
+  if (need < 1) need = 1;
+  if (grid > need) grid = need;
+  void* args[] = {(void*)&a};
+  return cudaLaunchCooperativeKernel((void*)k_pcg, dim3(grid), dim3(PCG_TPB), args, 0, s);
+}
+
+}  // namespace ando

@@ -1,0 +1,208 @@
+"""Seeded synthetic scenes for the five benchmark configurations.
+
+The reference ships no scene files for these workloads, so every scene is
+generated from a seed. Grids use the diagonal split of the reference demos
+(demos/demo_framework.py:528-553): quad (i0, i1, i2, i3) becomes the triangles
+(i0, i2, i1) and (i1, i2, i3).
+
+Each builder returns a :class:`Scene` holding plain numpy arrays; callers feed
+them to ``ando_barrier_core`` (the CUDA path) or to the CPU oracle.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Tuple
+
+import numpy as np
+
+
+@dataclass
+class Rigid:
+    vertices: np.ndarray
+    triangles: np.ndarray
+    density: float
+
+
+@dataclass
+class Scene:
+    name: str
+    vertices: np.ndarray                 # (V, 3) float64
+    triangles: np.ndarray                # (T, 3) int32
+    material: dict                       # Material fields
+    params: dict                         # SimParams fields
+    pins: List[Tuple[int, np.ndarray]]   # (vertex, target)
+    walls: List[Tuple[np.ndarray, float, float]]  # (normal, offset, gap)
+    gravity: np.ndarray = field(default_factory=lambda: np.array([0.0, 0.0, -9.81]))
+    frames: int = 1
+    rigids: List[Rigid] = field(default_factory=list)
+    # Optional per-frame pin targets: frame index -> list of (vertex, target).
+    pin_schedule: Optional[Callable[[int], List[Tuple[int, np.ndarray]]]] = None
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.vertices.shape[0])
+
+    @property
+    def num_triangles(self) -> int:
+        return int(self.triangles.shape[0])
+
+    def pins_at(self, frame: int) -> List[Tuple[int, np.ndarray]]:
+        return self.pin_schedule(frame) if self.pin_schedule is not None else self.pins
+
+
+def grid_triangles(nx: int, ny: int, offset: int = 0) -> np.ndarray:
+    """Diagonal-split triangles of an nx-by-ny vertex grid (row-major, x fastest)."""
+    yi, xi = np.meshgrid(np.arange(ny - 1), np.arange(nx - 1), indexing="ij")
+    i0 = (yi * nx + xi).ravel() + offset
+    i1, i2 = i0 + 1, i0 + nx
+    i3 = i2 + 1
+    tris = np.empty((2 * i0.size, 3), dtype=np.int32)
+    tris[0::2] = np.stack([i0, i2, i1], axis=1)
+    tris[1::2] = np.stack([i1, i2, i3], axis=1)
+    return tris
+
+
+def grid_plane(n: int, size: float) -> np.ndarray:
+    """n-by-n grid over [0, size]^2 in the z=0 plane (x fastest)."""
+    t = np.linspace(0.0, size, n)
+    yy, xx = np.meshgrid(t, t, indexing="ij")
+    return np.stack([xx.ravel(), yy.ravel(), np.zeros(n * n)], axis=1)
+
+
+def cloth_params(**kw) -> dict:
+    p = dict(dt=1.0 / 60.0, beta_max=0.25, max_newton_steps=8, pcg_tol=1e-3, pcg_max_iters=1000,
+             contact_gap_max=1e-3, wall_gap=1e-3, enable_strain_limiting=True, strain_limit=0.05,
+             strain_tau=0.05)
+    p.update(kw)
+    return p
+
+
+def ground() -> Tuple[np.ndarray, float, float]:
+    return (np.array([0.0, 0.0, 1.0]), 0.0, 1e-3)
+
+
+def c1(seed: int = 0, n: int = 32, frames: int = 120) -> Scene:
+    """32x32 cloth, 1 m square at z=1, +-0.1 mm in-plane jitter, top corners pinned, ground plane."""
+    rng = np.random.default_rng(seed)
+    v = grid_plane(n, 1.0)
+    v[:, :2] += rng.uniform(-1e-4, 1e-4, size=(n * n, 2))
+    v[:, 2] = 1.0
+    tris = grid_triangles(n, n)
+    top = [(n - 1) * n, n * n - 1]
+    pins = [(i, v[i].copy()) for i in top]
+    mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
+    return Scene("c1_32x32", v, tris, mat, cloth_params(), pins, [ground()], frames=frames)
+
+
+def _sheet(n: int, size: float, angle: float, z0: float, phases, lambdas, dirs) -> np.ndarray:
+    v = grid_plane(n, size) - np.array([size / 2, size / 2, 0.0])
+    c, s = math.cos(angle), math.sin(angle)
+    xy = v[:, :2] @ np.array([[c, s], [-s, c]])
+    h = np.zeros(n * n)
+    for ph, lam, d in zip(phases, lambdas, dirs):
+        h += np.sin(2 * math.pi * (xy @ d) / lam + ph)
+    v = np.stack([xy[:, 0], xy[:, 1], z0 + 0.02 * h / 3.0], axis=1)
+    return v
+
+
+def c2(seed: int = 0, n: int = 96, sheets: int = 4, frames: int = 200) -> Scene:
+    """Four 96x96 sheets stacked at 5 mm from z=0.5, seeded rotations and 2 cm height waves."""
+    rng = np.random.default_rng(seed)
+    verts, tris = [], []
+    for k in range(sheets):
+        ang = rng.uniform(0.0, math.pi / 4)
+        ph = rng.uniform(0, 2 * math.pi, 3)
+        lam = rng.uniform(0.2, 0.5, 3)
+        th = rng.uniform(0, 2 * math.pi, 3)
+        dirs = np.stack([np.cos(th), np.sin(th)], axis=1)
+        verts.append(_sheet(n, 1.0, ang, 0.5 + 0.005 * k, ph, lam, dirs))
+        tris.append(grid_triangles(n, n, offset=k * n * n))
+    mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
+    return Scene("c2_4x96x96", np.concatenate(verts), np.concatenate(tris), mat, cloth_params(), [], [ground()], frames=frames)
+
+
+def c3(seed: int = 0, scenes: int = 64, frames: int = 60) -> List[Scene]:
+    """64 independent square cloths, side drawn from 16..128, 1-4 corner pins, log-uniform E."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(scenes):
+        n = int(rng.integers(16, 129))
+        v = grid_plane(n, 1.0)
+        v[:, 2] = 1.0
+        corners = [0, n - 1, (n - 1) * n, n * n - 1]
+        k = int(rng.integers(1, 5))
+        chosen = sorted(rng.choice(4, size=k, replace=False).tolist())
+        pins = [(corners[c], v[corners[c]].copy()) for c in chosen]
+        E = float(10 ** rng.uniform(4, 6))
+        mat = dict(youngs_modulus=E, poisson_ratio=0.3, density=200.0, thickness=1e-3)
+        out.append(Scene(f"c3_scene{s}_{n}", v, grid_triangles(n, n), mat,
+                         cloth_params(enable_strain_limiting=False), pins, [ground()], frames=frames))
+    return out
+
+
+def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
+    """Two 2 m curtains (n x n each) 3 mm apart in y, top rows pinned and driven +-0.3 m along x at 0.5 Hz
+    in opposite phase. The reference has no call to move a pin, so the pin set is rebuilt every frame."""
+    rng = np.random.default_rng(seed)
+    verts, tris, top = [], [], []
+    for k in range(2):
+        g = grid_plane(n, 2.0)
+        v = np.stack([g[:, 0] - 1.0, np.full(n * n, 0.003 * k), g[:, 1] + 0.2], axis=1)
+        v[:, [0, 2]] += rng.uniform(-1e-4, 1e-4, size=(n * n, 2))
+        verts.append(v)
+        tris.append(grid_triangles(n, n, offset=k * n * n))
+        top.extend(range(k * n * n + (n - 1) * n, (k + 1) * n * n))
+    v = np.concatenate(verts)
+    base = {i: v[i].copy() for i in top}
+    half = n * n
+    dt = 1.0 / 60.0
+
+    def schedule(frame: int):
+        t = (frame + 1) * dt
+        out = []
+        for i in top:
+            sgn = 1.0 if i < half else -1.0
+            tgt = base[i].copy()
+            tgt[0] += sgn * 0.3 * math.sin(2 * math.pi * 0.5 * t)
+            out.append((i, tgt))
+        return out
+
+    mat = dict(youngs_modulus=2e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
+    return Scene(f"c4_2x{n}x{n}", v, np.concatenate(tris), mat, cloth_params(),
+                 [(i, base[i]) for i in top], [ground()], frames=frames, pin_schedule=schedule)
+
+
+def box_mesh(lo, hi) -> Tuple[np.ndarray, np.ndarray]:
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], dtype=np.float64)
+    t = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4],
+                  [1, 2, 6], [1, 6, 5], [2, 3, 7], [2, 7, 6], [3, 0, 4], [3, 4, 7]], dtype=np.int32)
+    return v, t
+
+
+def c5(seed: int = 0, n: int = 512, frames: int = 240) -> Scene:
+    """3 m cloth (n x n) over a 1 x 1 x 0.75 m static box on the ground; one edge row pulled at 1 m/s after frame 60."""
+    rng = np.random.default_rng(seed)
+    v = grid_plane(n, 3.0) - np.array([1.5, 1.5, 0.0])
+    v[:, :2] += rng.uniform(-1e-4, 1e-4, size=(n * n, 2))
+    v[:, 2] = 0.80
+    bv, bt = box_mesh((-0.5, -0.5, 0.0), (0.5, 0.5, 0.75))
+    edge = list(range(0, n))
+    base = {i: v[i].copy() for i in edge}
+    dt = 1.0 / 60.0
+
+    def schedule(frame: int):
+        t = max(0, frame + 1 - 60) * dt
+        return [(i, base[i] + np.array([-1.0 * t, 0.0, 0.0])) for i in edge]
+
+    mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
+    return Scene(f"c5_{n}x{n}_box", v, grid_triangles(n, n), mat,
+                 cloth_params(strain_limit=0.03, strain_tau=0.03),
+                 [(i, base[i]) for i in edge], [ground()], frames=frames,
+                 rigids=[Rigid(bv, bt, 1e6)], pin_schedule=schedule)
+
+
+CONFIGS = {"c1": c1, "c2": c2, "c3": c3, "c4": c4, "c5": c5}

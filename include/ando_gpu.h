@@ -1,0 +1,210 @@
+/*
+ * ando_gpu.h -- C ABI of the B200 (sm_100a) implementation of AndoSim's
+ * implicit cloth/shell step.
+ *
+ * Plain C types only: no C++, no CUDA and no torch types cross this boundary.
+ * Every entry point returns an ando_status (0 = ANDO_OK); nothing throws.
+ *
+ * The reference binds its C++ core to Python with pybind11
+ * (src/py/bindings.cpp:27-633). The pybind11 module shipped here
+ * (andosim_b200/csrc/bindings.cpp, module name `ando_barrier_core`) keeps that
+ * Python surface and calls the entry points below; any other host (ctypes,
+ * cffi, a C++ add-on) can bind them directly. Each declaration names the
+ * reference interface it replaces.
+ */
+#ifndef ANDO_GPU_H
+#define ANDO_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ANDO_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define ANDO_API __attribute__((visibility("default")))
+#else
+#define ANDO_API
+#endif
+
+typedef enum {
+  ANDO_OK = 0,
+  ANDO_ERR_INVALID = 1,      /* bad argument (null pointer, size, index out of range) */
+  ANDO_ERR_CUDA = 2,         /* a CUDA runtime call failed; see ando_last_error() */
+  ANDO_ERR_STATE = 3,        /* call out of order (e.g. step before mesh/state upload) */
+  ANDO_ERR_TIMEOUT = 4,      /* a device-side bounded wait gave up (grid barrier) */
+  ANDO_ERR_NO_DEVICE = 5,    /* no CUDA device / wrong architecture */
+  ANDO_ERR_CAPACITY = 6      /* a caller-supplied buffer is too small */
+} ando_status;
+
+/* Step semantics. REFERENCE reproduces the reference step exactly, including
+ * its documented quirks (elastic gradient on the rest mesh, repelling pins,
+ * literal BVH broad phase, frozen contact gaps, sampled CCD). CORRECTED is
+ * reserved for the physically corrected variant. */
+typedef enum { ANDO_SEMANTICS_REFERENCE = 0, ANDO_SEMANTICS_CORRECTED = 1 } ando_semantics;
+
+/* Preconditioner of the PCG inner solve. */
+typedef enum { ANDO_PRECOND_BLOCK_JACOBI = 0, ANDO_PRECOND_LEARNED = 1 } ando_precond;
+
+/* ContactType (collision.h:70-75). */
+typedef enum {
+  ANDO_CONTACT_POINT_TRIANGLE = 0,
+  ANDO_CONTACT_EDGE_EDGE = 1,
+  ANDO_CONTACT_WALL = 2,
+  ANDO_CONTACT_RIGID_POINT_TRIANGLE = 3
+} ando_contact_type;
+
+/* Material (types.h:51-57). */
+typedef struct {
+  double youngs_modulus, poisson_ratio, density, thickness, bending_stiffness;
+} ando_material;
+
+/* SimParams (types.h:60-100), every field, plus the two GPU-only knobs at the end. */
+typedef struct {
+  double dt, beta_max;
+  int32_t min_newton_steps, max_newton_steps, friction_min_newton_steps;
+  double pcg_tol;
+  int32_t pcg_max_iters;
+  double contact_gap_max, wall_gap;
+  int32_t enable_ccd;
+  double contact_normal_epsilon, barrier_tolerance;
+  int32_t enable_friction;
+  double friction_mu, friction_epsilon, friction_tangent_threshold;
+  double velocity_damping, contact_restitution;
+  int32_t enable_strain_limiting;
+  double strain_limit, strain_tau, strain_epsilon, strain_svd_epsilon;
+  double hessian_epsilon, min_gap;
+  int32_t semantics; /* ando_semantics */
+  int32_t precond;   /* ando_precond */
+} ando_params;
+
+/* PinConstraint (constraints.h:12-17). */
+typedef struct { int32_t vertex; int32_t active; double target[3]; } ando_pin;
+
+/* WallConstraint (constraints.h:22-28); normal already normalised by add_wall. */
+typedef struct { double normal[3]; double offset; double gap; int32_t active; int32_t pad_; } ando_wall;
+
+/* RigidBody (rigid_body.h), copied in and out by value around a step exactly
+ * as bindings.cpp:476-491 does. Mesh arrays are read-only; the dynamic fields
+ * are updated in place by ando_step. */
+typedef struct {
+  int32_t num_vertices, num_triangles;
+  const double* local_vertices;  /* (num_vertices, 3), body frame */
+  const int32_t* triangles;      /* (num_triangles, 3) */
+  double mass;
+  double inertia_body_inv[9];    /* row-major */
+  double position[3];
+  double rotation[9];            /* row-major */
+  double linear_velocity[3];
+  double angular_velocity[3];
+} ando_rigid;
+
+/* ContactPair (collision.h:78-103). */
+typedef struct {
+  int32_t type, idx0, idx1, idx2, idx3, rigid_body_index, vertex_count, pad_;
+  double gap;
+  double normal[3], witness_p[3], witness_q[3], barycentric[3];
+  double weights[4];
+} ando_contact;
+
+/* Per-step counters (no reference counterpart: the reference only logs to stderr). */
+typedef struct {
+  int32_t newton_iters;        /* Newton iterations that solved a system */
+  int32_t pcg_iters;           /* PCG iterations summed over the step */
+  int32_t pcg_max_per_newton;
+  int32_t pcg_not_converged;
+  int32_t line_search_fail;    /* inner steps whose line search returned alpha < 1e-6 */
+  int32_t contacts;            /* contacts detected at the start of the step */
+  int32_t strain_active;       /* strain-limit constraints active at the last gradient */
+  int32_t status;              /* ando_status of the step */
+  int32_t precond_fallbacks;   /* learned-preconditioner solves redone with block-Jacobi */
+  int32_t pad_;
+  double beta;
+  double last_alpha;
+  double device_ms;            /* device time of the step (CUDA events) */
+} ando_step_stats;
+
+typedef struct ando_ctx_s* ando_ctx;
+
+/* Library identity. */
+ANDO_API int32_t ando_abi_version(void);
+ANDO_API const char* ando_status_string(int32_t status);
+/* Message of the last CUDA/argument error on this thread (never NULL). */
+ANDO_API const char* ando_last_error(void);
+
+/* Create / destroy a device context holding one scene (mesh topology, rest
+ * data and simulation state) on `device`. No reference counterpart: the
+ * reference keeps everything in host objects. */
+ANDO_API int32_t ando_ctx_create(int32_t device, ando_ctx* out);
+ANDO_API void ando_ctx_destroy(ando_ctx ctx);
+
+/* Upload mesh topology, rest data and the current mesh vertices.
+ * Replaces Mesh::initialize / Mesh::compute_rest_state (mesh.h:137-142,
+ * mesh.cpp:8-75): the caller passes the rest areas and Dm_inv it computed
+ * (row-major 2x2 per face); the device builds the block-sparse pattern,
+ * scatter maps and the constant elastic Hessian blocks from them. */
+ANDO_API int32_t ando_mesh_upload(ando_ctx ctx, const double* vertices, int32_t num_vertices,
+                         const int32_t* triangles, int32_t num_triangles,
+                         const double* rest_areas, const double* dm_inv,
+                         const ando_material* material);
+
+/* Replace only the mesh vertices (Mesh::set_positions, mesh.cpp:121-123, and
+ * the `vertices` property setter, bindings.cpp:185-191). */
+ANDO_API int32_t ando_mesh_set_vertices(ando_ctx ctx, const double* vertices, int32_t num_vertices);
+
+/* Upload the simulation state (State::initialize, state.cpp:6-16; any of the
+ * pointers may be NULL to keep the device copy). */
+ANDO_API int32_t ando_state_upload(ando_ctx ctx, const double* positions, const double* velocities,
+                          const double* positions_prev, const double* masses, int32_t num_vertices);
+
+/* Download positions and/or velocities (State.get_positions/get_velocities,
+ * bindings.cpp:248-267). Either pointer may be NULL. */
+ANDO_API int32_t ando_state_download(ando_ctx ctx, double* positions, double* velocities, int32_t num_vertices);
+
+/* v += g*dt; x += v*dt for every vertex (State.apply_gravity, bindings.cpp:284-300). */
+ANDO_API int32_t ando_apply_gravity(ando_ctx ctx, const double gravity[3], double dt);
+
+/* One implicit step (Integrator::step, integrator.h:33-35, integrator.cpp:70-150).
+ * `rigids` may be NULL when num_rigids == 0; their dynamic fields are updated.
+ * `stats` may be NULL. */
+ANDO_API int32_t ando_step(ando_ctx ctx, const ando_params* params,
+                  const ando_pin* pins, int32_t num_pins,
+                  const ando_wall* walls, int32_t num_walls,
+                  ando_rigid* rigids, int32_t num_rigids,
+                  ando_step_stats* stats);
+
+/* Contact detection at the current state (Integrator::compute_contacts,
+ * integrator.h:44-46, integrator.cpp:238-244). Writes up to `capacity`
+ * contacts and the total count to *num_out; returns ANDO_ERR_CAPACITY when
+ * the total exceeds `capacity`. */
+ANDO_API int32_t ando_compute_contacts(ando_ctx ctx, const ando_rigid* rigids, int32_t num_rigids,
+                              ando_contact* out, int32_t capacity, int32_t* num_out);
+
+/* Block-sparse (3x3 BSR) system of the most recent Newton iteration, for
+ * inspection and for the preconditioner-training dump. Pass NULL pointers to
+ * query sizes. rowptr: num_vertices+1; cols: nnzb; vals: 9*nnzb (row-major
+ * blocks); rhs: 3*num_vertices. Extra contact blocks are not included. */
+ANDO_API int32_t ando_last_system(ando_ctx ctx, int32_t* num_vertices, int32_t* nnzb,
+                         int32_t* rowptr, int32_t* cols, float* vals, float* rhs, float* solution);
+
+/* Evaluate, without stepping, the system the first Newton iteration of a step
+ * would solve at the current state: prediction x_hat = x + dt*v, contact
+ * detection, Newton gradient (Integrator::compute_gradient,
+ * integrator.cpp:246-396) and Hessian (assemble_system_matrix, :398-544).
+ * Read the results with ando_last_gradient / ando_last_system. This is the
+ * solver's system dump for preconditioner training and for parity checks. */
+ANDO_API int32_t ando_eval_system(ando_ctx ctx, const ando_params* params,
+                                  const ando_pin* pins, int32_t num_pins,
+                                  const ando_wall* walls, int32_t num_walls,
+                                  const ando_rigid* rigids, int32_t num_rigids);
+
+/* Newton gradient (FP64, 3*num_vertices) of the most recent Newton iteration. */
+ANDO_API int32_t ando_last_gradient(ando_ctx ctx, double* gradient, int32_t num_vertices);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ANDO_GPU_H */

@@ -1,0 +1,350 @@
+"""CUDA path against the CPU oracle (REFERENCE semantics).
+
+Stage checks go through the C ABI (ctypes, ``andosim_b200.abi``): the Newton
+gradient and the assembled block-sparse Hessian of one Newton iteration are
+compared with the FP64 oracle's Integrator::compute_gradient /
+assemble_system_matrix at the same state. Whole-step checks drive the
+``ando_barrier_core`` module exactly as the reference demos drive theirs
+(apply_gravity, then Integrator.step) and compare positions with the FP64
+oracle.
+
+Tolerances: gradient and Hessian within 1e-5 relative (the Hessian is stored
+in FP32, the gradient is FP64); positions within 1e-4 of the mesh extent.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from andosim_b200 import scenes
+from conftest import oracle_constraints, oracle_scene
+
+pytestmark = pytest.mark.gpu
+
+GRAD_RTOL = 1e-5
+HESS_RTOL = 1e-5
+POS_TOL = 1e-4
+
+
+# ------------------------------------------------------------------ helpers
+def small_cloth(n=12, size=0.3, z=0.3, seed=0, **params):
+    rng = np.random.default_rng(seed)
+    v = scenes.grid_plane(n, size)
+    v[:, :2] += rng.uniform(-1e-4, 1e-4, size=(n * n, 2))
+    v[:, 2] = z
+    mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
+    return scenes.Scene(f"cloth{n}", v, scenes.grid_triangles(n, n), mat, scenes.cloth_params(**params), [], [scenes.ground()])
+
+
+def bsr_to_dense(rowptr, cols, vals, V):
+    H = np.zeros((3 * V, 3 * V))
+    for r in range(V):
+        for k in range(rowptr[r], rowptr[r + 1]):
+            c = cols[k]
+            H[3 * r:3 * r + 3, 3 * c:3 * c + 3] += vals[k]
+    return H
+
+
+def csr_to_dense(d):
+    n = d["n"]
+    H = np.zeros((n, n))
+    rp, cc, vv = d["rowptr"], d["cols"], d["vals"]
+    for r in range(n):
+        H[r, cc[rp[r]:rp[r + 1]]] += vv[rp[r]:rp[r + 1]]
+    return H
+
+
+def oracle_system(oracle, sc, x, v, params=None, rigids=None):
+    """FP64 gradient and Hessian of the first Newton iteration at state (x, v)."""
+    O = oracle.f64
+    m, s, p = oracle_scene(O, sc)
+    for k, val in (params or {}).items():
+        setattr(p, k, val)
+    s.set_positions(x)
+    s.set_velocities(v)
+    c = oracle_constraints(O, sc)
+    bodies = None
+    if rigids:
+        bodies = []
+        for rg in rigids:
+            b = O.RigidBody()
+            b.initialize(rg.vertices, rg.triangles, rg.density)
+            bodies.append(b)
+    contacts = O.Integrator.compute_contacts(m, s, bodies)
+    xt = x + p.dt * v
+    g = O.Integrator.gradient(m, s, xt, contacts, c, p)
+    H = O.Integrator.assemble(m, s, contacts, c, p)
+    return np.asarray(g), H, len(contacts)
+
+
+def gpu_system(abi, sc, x, v, params=None, rigids=None):
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material)
+    S.upload(x, v, sc.vertices, None)
+    p = dict(sc.params)
+    p.update(params or {})
+    keep = []
+    rb = [abi.make_rigid(r.vertices, r.triangles, r.density, keep) for r in (rigids or [])]
+    S.eval_system(abi.make_params(p), sc.pins_at(0), sc.walls, rb or None)
+    g = S.last_gradient()
+    rowptr, cols, vals, rhs, _ = S.last_system()
+    H = bsr_to_dense(rowptr, cols, vals, S.V)
+    S.close()
+    return g, H, rhs
+
+
+def assert_system_close(oracle, abi, sc, x, v, params=None, rigids=None, expect_contacts=None):
+    g_o, H_o, nc = oracle_system(oracle, sc, x, v, params, rigids)
+    g_g, H_g, rhs = gpu_system(abi, sc, x, v, params, rigids)
+    if expect_contacts is not None:
+        assert (nc > 0) == expect_contacts
+    gs = np.abs(g_o).max()
+    assert np.abs(g_g - g_o).max() <= GRAD_RTOL * gs + 1e-12, np.abs(g_g - g_o).max() / gs
+    np.testing.assert_allclose(rhs, (-g_g).astype(np.float32), rtol=0, atol=0)
+    Hd = csr_to_dense(H_o)
+    hs = np.abs(Hd).max()
+    err = np.abs(H_g - Hd)
+    assert (err <= HESS_RTOL * np.abs(Hd) + 1e-7 * hs).all(), float((err / (np.abs(Hd) + 1e-7 * hs)).max())
+    return g_o, Hd
+
+
+# ----------------------------------------------------------- stage parity
+def test_system_free_fall(oracle, abi):
+    sc = scenes.c1()
+    v = np.zeros_like(sc.vertices)
+    v[:, 2] = -9.81 / 60
+    x = sc.vertices + v / 60
+    assert_system_close(oracle, abi, sc, x, v)
+
+
+def test_system_pins_inside_domain(oracle, abi):
+    sc = scenes.c1()
+    x = sc.vertices.copy()
+    for i, t in sc.pins:
+        x[i] = t + np.array([3e-4, -2e-4, 4e-4])   # gap 0.54 mm < 1 mm: pin barrier active
+    assert_system_close(oracle, abi, sc, x, np.zeros_like(x))
+
+
+def test_system_wall_and_strain(oracle, abi):
+    sc = small_cloth(n=10, z=0.0004)
+    x = sc.vertices.copy()
+    x[:, 0] *= 1.08                                   # 8 % stretch in x: strain limit active
+    x[::7, 2] = 0.0002                                # some vertices deeper in the wall barrier
+    v = np.zeros_like(x)
+    v[:, 2] = -0.1
+    assert_system_close(oracle, abi, sc, x, v)
+
+
+def test_system_strain_degenerate_and_average(oracle, abi):
+    sc = small_cloth(n=8, z=0.5)
+    x = sc.vertices.copy()
+    x[:, :2] *= 1.07                                  # isotropic stretch: equal singular values
+    assert_system_close(oracle, abi, sc, x, np.zeros_like(x))
+
+
+def test_system_rigid_contacts(oracle, abi):
+    sc = small_cloth(n=14, size=0.6, z=0.0)
+    sc.vertices[:, :2] -= 0.3
+    bv, bt = scenes.box_mesh((-0.15, -0.15, 0.0), (0.15, 0.15, 0.1))
+    x = sc.vertices.copy()
+    x[:, 2] = 0.1005                                  # 0.5 mm above the box top
+    rig = [scenes.Rigid(bv, bt, 1e6)]
+    assert_system_close(oracle, abi, sc, x, np.zeros_like(x), rigids=rig, expect_contacts=True)
+
+
+def test_system_rigid_contacts_with_friction(oracle, abi):
+    sc = small_cloth(n=10, size=0.4, z=0.0)
+    sc.vertices[:, :2] -= 0.2
+    bv, bt = scenes.box_mesh((-0.1, -0.1, 0.0), (0.1, 0.1, 0.1))
+    x = sc.vertices.copy()
+    x[:, 2] = 0.1004
+    x[:, 0] += 0.002                                  # tangential motion since positions_prev
+    rig = [scenes.Rigid(bv, bt, 1e6)]
+    assert_system_close(oracle, abi, sc, x, np.zeros_like(x), params=dict(enable_friction=True, friction_mu=0.3),
+                        rigids=rig, expect_contacts=True)
+
+
+def single_triangle_scene():
+    """One triangle plus free vertices: the only mesh size for which the
+    reference's BVH yields vertex-triangle candidates (collision.cpp:81-86)."""
+    v = np.array([[0.0, 0.0, 0.0], [0.2, 0.0, 0.0], [0.0, 0.2, 0.0], [0.05, 0.05, 0.0004], [0.06, 0.05, 0.0008],
+                  [0.5, 0.5, 0.5]])
+    t = np.array([[0, 1, 2]], dtype=np.int32)
+    mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
+    return scenes.Scene("tri1", v, t, mat, scenes.cloth_params(enable_strain_limiting=False), [], [])
+
+
+def test_system_point_triangle_contacts(oracle, abi):
+    sc = single_triangle_scene()
+    assert_system_close(oracle, abi, sc, sc.vertices.copy(), np.zeros_like(sc.vertices), expect_contacts=True)
+
+
+def test_contact_lists_match(oracle, core):
+    sc = single_triangle_scene()
+    O = oracle.f64
+    m, s, _ = oracle_scene(O, sc)
+    ref = O.Integrator.compute_contacts(m, s, None)
+    gm = core.Mesh()
+    gm.initialize(sc.vertices, sc.triangles, core.Material(**sc.material))
+    gs = core.State()
+    gs.initialize(gm)
+    got = core.Integrator.compute_contacts(gm, gs)
+    assert len(ref) == len(got) == 2
+    for a, b in zip(ref, got):
+        assert (a.idx0, a.idx1, a.idx2, a.idx3) == (b.idx0, b.idx1, b.idx2, b.idx3)
+        assert int(a.type) == int(b.type)
+        assert abs(a.gap - b.gap) < 1e-7
+        np.testing.assert_allclose(a.normal, b.normal, atol=1e-6)
+
+
+def dense_to_csr(H):
+    rows, cols = np.nonzero(H)
+    rp = np.zeros(H.shape[0] + 1, dtype=np.int32)
+    np.add.at(rp, rows + 1, 1)
+    return np.cumsum(rp).astype(np.int32), cols.astype(np.int32), H[rows, cols]
+
+
+def test_pcg_direction_matches_oracle_solve(oracle, abi):
+    """One Newton solve: the GPU direction vs the FP64 oracle PCG on the same system."""
+    sc = small_cloth(n=20, size=1.0, z=0.5)
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material)
+    rng = np.random.default_rng(4)
+    v = rng.normal(scale=0.5, size=sc.vertices.shape)
+    S.upload(sc.vertices, v, sc.vertices, None)
+    p = abi.make_params(dict(sc.params, pcg_tol=1e-5, max_newton_steps=1, beta_max=1e-9))
+    st = S.step(p, sc.pins, sc.walls)
+    rowptr, cols, vals, rhs, sol = S.last_system()
+    S.close()
+    H = bsr_to_dense(rowptr, cols, vals, len(rowptr) - 1)
+    b = rhs.astype(np.float64)
+    r = b - H @ sol.astype(np.float64)
+    assert np.abs(r).max() / np.abs(b).max() < 5e-5
+    assert st["pcg_iters"] >= 1
+
+
+# ---------------------------------------------------------- whole steps
+def run_oracle(oracle, sc, frames, prec="f64", rigids=None):
+    O = getattr(oracle, prec)
+    m, s, p = oracle_scene(O, sc)
+    bodies = None
+    if rigids:
+        bodies = []
+        for rg in rigids:
+            b = O.RigidBody()
+            b.initialize(rg.vertices, rg.triangles, rg.density)
+            bodies.append(b)
+    traj, stats = [], []
+    for f in range(frames):
+        c = oracle_constraints(O, sc, f)
+        s.apply_gravity(sc.gravity, p.dt)
+        stats.append(O.Integrator.step(m, s, c, p, bodies))
+        traj.append(np.asarray(s.get_positions(), dtype=np.float64))
+    return traj, stats, bodies
+
+
+def run_gpu(core, sc, frames, params=None, rigids=None):
+    m = core.Mesh()
+    m.initialize(sc.vertices, sc.triangles, core.Material(**sc.material))
+    s = core.State()
+    s.initialize(m)
+    p = core.SimParams()
+    for k, v in dict(sc.params, **(params or {})).items():
+        setattr(p, k, v)
+    bodies = None
+    if rigids:
+        bodies = []
+        for rg in rigids:
+            b = core.RigidBody()
+            b.initialize(rg.vertices, rg.triangles, rg.density)
+            bodies.append(b)
+    traj, stats = [], []
+    for f in range(frames):
+        c = core.Constraints()
+        for i, t in sc.pins_at(f):
+            c.add_pin(int(i), t)
+        for n, o, g in sc.walls:
+            c.add_wall(n, o, g)
+        s.apply_gravity(sc.gravity, p.dt)
+        core.Integrator.step(m, s, c, p, bodies)
+        stats.append(core.Integrator.last_step_stats(s))
+        traj.append(s.get_positions64())
+    return traj, stats, bodies
+
+
+def extent(sc):
+    return float((sc.vertices.max(0) - sc.vertices.min(0)).max())
+
+
+def max_rel_error(ta, tb, ext):
+    return max(float(np.abs(a - b).max()) / ext for a, b in zip(ta, tb))
+
+
+def test_trajectory_c1_120_frames(oracle, core):
+    sc = scenes.c1()
+    to, so, _ = run_oracle(oracle, sc, 120)
+    tg, sg, _ = run_gpu(core, sc, 120)
+    assert max_rel_error(to, tg, extent(sc)) <= POS_TOL
+    assert [s["newton_iters"] for s in so] == [s["newton_iters"] for s in sg]
+
+
+def test_trajectory_pinned_strained_cloth(oracle, core):
+    """Pins near their targets, strain limiting active, cloth resting on the wall."""
+    sc = small_cloth(n=16, size=0.5, z=0.0006)
+    sc.vertices[:, 0] *= 1.06
+    sc.pins = [(0, sc.vertices[0] + 4e-4), (15, sc.vertices[15] - 3e-4)]
+    to, _, _ = run_oracle(oracle, sc, 30)
+    tg, _, _ = run_gpu(core, sc, 30)
+    assert max_rel_error(to, tg, extent(sc)) <= POS_TOL
+
+
+def test_trajectory_cloth_on_rigid_box(oracle, core):
+    sc = small_cloth(n=16, size=0.6, z=0.1008)
+    sc.vertices[:, :2] -= 0.3
+    bv, bt = scenes.box_mesh((-0.15, -0.15, 0.0), (0.15, 0.15, 0.1))
+    rig = [scenes.Rigid(bv, bt, 1e6)]
+    to, _, bo = run_oracle(oracle, sc, 20, rigids=rig)
+    tg, _, bg = run_gpu(core, sc, 20, rigids=rig)
+    assert max_rel_error(to, tg, extent(sc)) <= POS_TOL
+    np.testing.assert_allclose(bg[0].linear_velocity, bo[0].linear_velocity, rtol=1e-4, atol=1e-9)
+    np.testing.assert_allclose(bg[0].position, bo[0].position, rtol=1e-6, atol=1e-9)
+
+
+def test_trajectory_point_triangle_ccd(oracle, core):
+    sc = single_triangle_scene()
+    sc.walls = []
+    to, so, _ = run_oracle(oracle, sc, 15)
+    tg, sg, _ = run_gpu(core, sc, 15)
+    assert max_rel_error(to, tg, extent(sc)) <= POS_TOL
+
+
+def test_trajectory_damping_restitution(oracle, core):
+    sc = small_cloth(n=12, size=0.4, z=0.02)
+    sc.params.update(velocity_damping=0.02, contact_restitution=0.5)
+    to, _, _ = run_oracle(oracle, sc, 25)
+    tg, _, _ = run_gpu(core, sc, 25)
+    assert max_rel_error(to, tg, extent(sc)) <= POS_TOL
+
+
+def test_step_is_deterministic(core):
+    sc = small_cloth(n=20, size=0.5, z=0.01)
+    sc.vertices[:, 0] *= 1.06
+    ta, _, _ = run_gpu(core, sc, 10)
+    tb, _, _ = run_gpu(core, sc, 10)
+    for a, b in zip(ta, tb):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_apply_gravity_kernel(core):
+    sc = small_cloth(n=6)
+    m = core.Mesh()
+    m.initialize(sc.vertices, sc.triangles, core.Material(**sc.material))
+    s = core.State()
+    s.initialize(m)
+    p = core.SimParams()
+    core.Integrator.step(m, s, core.Constraints(), p)   # state now lives on the device
+    x0, v0 = s.get_positions64(), s.get_velocities64()
+    s.apply_gravity(np.array([0.0, 0.0, -9.81]), 0.01)
+    x1, v1 = s.get_positions64(), s.get_velocities64()
+    np.testing.assert_allclose(v1, v0 + np.array([0, 0, -9.81]) * np.float32(0.01), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(x1, x0 + v1 * np.float32(0.01), rtol=0, atol=1e-12)
