@@ -25,8 +25,11 @@ EXPORTED = [
     "ando_abi_version", "ando_status_string", "ando_last_error", "ando_ctx_create", "ando_ctx_destroy",
     "ando_mesh_upload", "ando_mesh_set_vertices", "ando_state_upload", "ando_state_download",
     "ando_apply_gravity", "ando_step", "ando_compute_contacts", "ando_last_system", "ando_eval_system",
-    "ando_last_gradient",
+    "ando_last_gradient", "ando_last_contact_blocks", "ando_profile_enable", "ando_profile_read", "ando_ctx_stream",
+    "ando_broad_phase",
 ]
+
+PHASES = ["setup", "strain", "gradient", "assemble", "pcg", "line_search", "finish"]
 
 
 class Material(C.Structure):
@@ -74,6 +77,16 @@ class Contact(C.Structure):
     ]
 
 
+class Profile(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("phase_launches", C.c_int64 * 7), ("phase_ms", C.c_double * 7),
+                ("pcg_iterations", C.c_int64), ("newton_iterations", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {"launches": self.launches, "pcg_iterations": self.pcg_iterations, "newton_iterations": self.newton_iterations,
+                "phase_ms": {p: self.phase_ms[i] for i, p in enumerate(PHASES)},
+                "phase_launches": {p: self.phase_launches[i] for i, p in enumerate(PHASES)}}
+
+
 class StepStats(C.Structure):
     _fields_ = [
         ("newton_iters", C.c_int32), ("pcg_iters", C.c_int32), ("pcg_max_per_newton", C.c_int32),
@@ -115,6 +128,11 @@ def lib() -> C.CDLL:
     L.ando_compute_contacts.argtypes = [P, C.POINTER(Rigid), I32, C.POINTER(Contact), I32, pi]
     L.ando_last_system.restype = I32; L.ando_last_system.argtypes = [P, pi, pi, pi, pi, pf, pf, pf]
     L.ando_last_gradient.restype = I32; L.ando_last_gradient.argtypes = [P, pd, I32]
+    L.ando_last_contact_blocks.restype = I32; L.ando_last_contact_blocks.argtypes = [P, pi, pi, pi, pf]
+    L.ando_profile_enable.restype = I32; L.ando_profile_enable.argtypes = [P, I32]
+    L.ando_profile_read.restype = I32; L.ando_profile_read.argtypes = [P, C.POINTER(Profile)]
+    L.ando_ctx_stream.restype = I32; L.ando_ctx_stream.argtypes = [P, C.POINTER(C.c_void_p)]
+    L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
     _lib = L
     return L
 
@@ -290,6 +308,40 @@ class Scene:
         _check(lib().ando_last_system(self.ctx, C.byref(V), C.byref(nnzb), _iptr(rowptr), _iptr(cols), _fptr(vals),
                                       _fptr(rhs), _fptr(sol)), "ando_last_system")
         return rowptr, cols, vals.reshape(-1, 3, 3), rhs, sol
+
+    def last_contact_blocks(self):
+        n = C.c_int32()
+        _check(lib().ando_last_contact_blocks(self.ctx, C.byref(n), None, None, None), "ando_last_contact_blocks")
+        rows = np.empty(n.value, dtype=np.int32); cols = np.empty(n.value, dtype=np.int32)
+        vals = np.empty(9 * n.value, dtype=np.float32)
+        if n.value:
+            _check(lib().ando_last_contact_blocks(self.ctx, C.byref(n), _iptr(rows), _iptr(cols), _fptr(vals)),
+                   "ando_last_contact_blocks")
+        return rows, cols, vals.reshape(-1, 3, 3)
+
+    def broad_phase(self, kind: int, pad: float = 0.0) -> np.ndarray:
+        """Sorted candidate pairs, shape (n, 2): kind 0 (vertex, triangle), kind 1 (edge, edge)."""
+        n = C.c_int32()
+        rc = lib().ando_broad_phase(self.ctx, kind, float(pad), None, 0, C.byref(n))
+        if rc not in (ANDO_OK, ANDO_ERR_CAPACITY):
+            _check(rc, "ando_broad_phase")
+        out = np.empty((max(n.value, 1), 2), dtype=np.int32)
+        if n.value:
+            _check(lib().ando_broad_phase(self.ctx, kind, float(pad), _iptr(out), n.value, C.byref(n)), "ando_broad_phase")
+        return out[:n.value]
+
+    def profile_enable(self, enable: bool = True):
+        _check(lib().ando_profile_enable(self.ctx, 1 if enable else 0), "ando_profile_enable")
+
+    def profile(self) -> dict:
+        pr = Profile()
+        _check(lib().ando_profile_read(self.ctx, C.byref(pr)), "ando_profile_read")
+        return pr.as_dict()
+
+    def stream(self) -> int:
+        sp = C.c_void_p()
+        _check(lib().ando_ctx_stream(self.ctx, C.byref(sp)), "ando_ctx_stream")
+        return sp.value or 0
 
     def contacts(self, rigids: Optional[List[Rigid]] = None) -> List[Contact]:
         nr = len(rigids) if rigids else 0

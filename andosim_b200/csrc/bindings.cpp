@@ -230,6 +230,7 @@ struct State {
   ~State() { if (ctx) ando_ctx_destroy(ctx); }
 
   size_t nv() const { return x.size(); }
+  static int& device() { static int d = 0; return d; }
 
   void sync_host() {
     if (!device_newer || !ctx) return;
@@ -246,7 +247,7 @@ struct State {
   // Make the device hold this mesh and this state.
   void bind(const Mesh& mesh) {
     if (mesh.nv() != nv()) throw std::runtime_error("mesh and state have different vertex counts");
-    if (!ctx) check(ando_ctx_create(0, &ctx), "GPU context");
+    if (!ctx) check(ando_ctx_create(State::device(), &ctx), "GPU context");
     if (topo != mesh.topo_version) {
       sync_host();
       std::vector<double> mv = flat(mesh.vertices);
@@ -476,6 +477,8 @@ PYBIND11_MODULE(ando_barrier_core, m) {
   m.def("version", []() { return std::string("ando_barrier_core v1.0.0"); }, "Get version string");
   m.def("backend", []() { return std::string("cuda-sm_100a"); });
   m.attr("ABI_VERSION") = ando_abi_version();
+  m.def("set_device", [](int d) { State::device() = d; }, "CUDA device for states created from now on (default 0)");
+  m.def("get_device", []() { return State::device(); });
 
   py::class_<Material>(m, "Material")
       .def(py::init<>())
@@ -591,6 +594,12 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         if (v.size() != s.nv()) throw py::value_error("positions must have one row per vertex");
         s.sync_host(); s.x = v; s.host_dirty = true;
       })
+      .def("_stream_handle", [](State& s) -> uintptr_t {
+        if (!s.ctx) return 0;
+        void* st = nullptr;
+        check(ando_ctx_stream(s.ctx, &st), "stream");
+        return reinterpret_cast<uintptr_t>(st);
+      }, "cudaStream_t of the state's device context (0 before the first GPU call)")
       .def("set_velocities64", [](State& s, py::object p) {
         auto v = to_v3(p, "velocities");
         if (v.size() != s.nv()) throw py::value_error("velocities must have one row per vertex");

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <unordered_set>
 #include <string>
 #include <vector>
 
@@ -22,6 +23,7 @@
 
 #include "../../include/ando_gpu.h"
 #include "kernels.cuh"
+#include "lbvh.cuh"
 
 using namespace ando;
 
@@ -39,28 +41,6 @@ int fail(int code, const std::string& msg) {
     cudaError_t e_ = (call);                                                                       \
     if (e_ != cudaSuccess) return fail(ANDO_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
-
-template <class T> struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() { if (p) cudaFree(p); }
-  cudaError_t reserve(size_t count) {
-    if (count <= n && p) return cudaSuccess;
-    if (p) { cudaFree(p); p = nullptr; n = 0; }
-    size_t c = count ? count : 1;
-    cudaError_t e = cudaMalloc(&p, c * sizeof(T));
-    if (e == cudaSuccess) n = c;
-    return e;
-  }
-  cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
-    cudaError_t e = reserve(count);
-    if (e != cudaSuccess || count == 0) return e;
-    return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
-  }
-};
 
 }  // namespace
 
@@ -95,11 +75,19 @@ struct ando_ctx_s {
   DevBuf<unsigned char> cub_tmp;
 
   // constraints
-  DevBuf<int> pin_vertex;
+  DevBuf<int> pin_vertex, pin_head;
   DevBuf<double> pin_target;
   DevBuf<WallDev> walls;
   int num_pins = 0, num_walls = 0;
   WallDev first_wall_host{};
+
+  // broad phase
+  DevBuf<int> edges;
+  int E = 0;
+  Lbvh bvh_tri, bvh_edge;
+  DevBuf<int2> pairs, pair_scratch;
+  DevBuf<unsigned long long> pk0, pk1;
+  DevBuf<int> pcount;
 
   // rigid bodies
   DevBuf<RigidDev> bodies_dev;
@@ -108,6 +96,7 @@ struct ando_ctx_s {
   std::vector<DevBuf<int>*> body_tris;
 
   ~ando_ctx_s() {
+    destroy_events();
     for (auto* b : body_local) delete b;
     for (auto* b : body_world) delete b;
     for (auto* b : body_tris) delete b;
@@ -128,7 +117,53 @@ struct ando_ctx_s {
   }
 
   cudaError_t cub_reserve(size_t bytes) { return cub_tmp.reserve(bytes); }
+
+  // profiling: phase events are recorded around launches and read back at the
+  // next synchronisation point
+  bool prof = false;
+  ando_profile profile{};
+  std::vector<cudaEvent_t> ev_free;
+  struct Pending { int phase; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+
+  cudaEvent_t take_event() {
+    if (!ev_free.empty()) { cudaEvent_t e = ev_free.back(); ev_free.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void collect() {
+    for (auto& q : pending) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, q.a, q.b) == cudaSuccess) profile.phase_ms[q.phase] += ms;
+      ev_free.push_back(q.a); ev_free.push_back(q.b);
+    }
+    pending.clear();
+  }
+  void destroy_events() {
+    collect();
+    for (auto e : ev_free) cudaEventDestroy(e);
+    ev_free.clear();
+  }
 };
+
+namespace {
+// Times the launches issued while it is alive (one phase) and counts them.
+struct Phase {
+  ando_ctx c; int phase; cudaEvent_t a = nullptr;
+  Phase(ando_ctx c_, int ph) : c(c_), phase(ph) {
+    if (c->prof) { a = c->take_event(); cudaEventRecord(a, c->stream); }
+  }
+  void launched(int n = 1) { c->profile.launches += n; c->profile.phase_launches[phase] += n; }
+  ~Phase() {
+    if (c->prof && a) {
+      cudaEvent_t b = c->take_event();
+      cudaEventRecord(b, c->stream);
+      c->pending.push_back({phase, a, b});
+    }
+  }
+};
+}  // namespace
 
 namespace {
 
@@ -158,13 +193,22 @@ StepParams make_step_params(const ando_params& p, int num_walls, int first_wall)
 // Contact detection at the current positions into ctx->contacts (order of
 // Collision::detect_all_collisions: vertex-triangle by vertex, then rigid
 // contacts by body, vertex and triangle).
-int detect(ando_ctx c, int nb) {
+int detect(ando_ctx c, int nb, int phase = ANDO_PHASE_SETUP) {
+  Phase ph(c, phase);
   MeshDev m = c->mesh_dev();
   long long units = (long long)c->V * (1 + nb);
   int literal_pt = (c->T == 1) ? 1 : 0;
+  if (!literal_pt && nb == 0) {
+    // The reference's BVH yields no self-contact candidate for >= 2 triangles
+    // (collision.cpp:81-86) and there is no rigid body: nothing to detect.
+    c->ncontacts = 0;
+    c->n_pe = 0;
+    return ANDO_OK;
+  }
   CK(c->det_counts.reserve(units + 1));
   CK(c->det_offsets.reserve(units + 1));
   launch_detect_count(m, c->x.p, c->bodies_dev.p, nb, literal_pt, c->det_counts.p, c->stream);
+  ph.launched();
   CK(cudaMemsetAsync(c->det_counts.p + units, 0, sizeof(int), c->stream));
   size_t bytes = 0;
   CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, c->det_counts.p, c->det_offsets.p, (int)(units + 1), c->stream));
@@ -175,7 +219,7 @@ int detect(ando_ctx c, int nb) {
   CK(cudaStreamSynchronize(c->stream));
   c->ncontacts = total;
   CK(c->contacts.reserve(total));
-  if (total) launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, literal_pt, c->det_offsets.p, c->contacts.p, c->stream);
+  if (total) { launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, literal_pt, c->det_offsets.p, c->contacts.p, c->stream); ph.launched(); }
   c->n_pe = literal_pt ? total : 0;  // only the literal vertex-triangle case produces PT contacts
   CK(cudaGetLastError());
   return ANDO_OK;
@@ -185,9 +229,10 @@ int detect(ando_ctx c, int nb) {
 // gap, the per-vertex constant gradient/diagonal, and the extra off-diagonal
 // block segment sorted by row.
 int prepare_contacts(ando_ctx c, const StepParams& sp) {
+  Phase ph(c, ANDO_PHASE_SETUP);
   MeshDev m = c->mesh_dev();
   int nc = c->ncontacts, V = c->V;
-  launch_contact_prep(m, c->contacts.p, nc, sp, c->stream);
+  if (nc) { launch_contact_prep(m, c->contacts.p, nc, sp, c->stream); ph.launched(); }
   int ne = 16 * nc;
   c->nent = ne;
   CK(c->ekeys.reserve(ne + 1)); CK(c->ekeys_sorted.reserve(ne + 1));
@@ -201,10 +246,12 @@ int prepare_contacts(ando_ctx c, const StepParams& sp) {
     CK(cudaMemsetAsync(c->eend.p, 0, sizeof(int) * V, c->stream));
     c->nx = 0;
     launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, c->g_const.p, c->diag_const.p, c->stream);
+    ph.launched();
     CK(cudaGetLastError());
     return ANDO_OK;
   }
   launch_contact_entries(c->contacts.p, nc, V, sp.enable_friction && sp.friction_mu > 0.0, c->ekeys.p, c->ents.p, c->stream);
+  ph.launched();
   int bits = 1;
   while ((1ll << bits) <= (long long)V) ++bits;
   size_t bytes = 0;
@@ -215,6 +262,7 @@ int prepare_contacts(ando_ctx c, const StepParams& sp) {
   launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, c->g_const.p, c->diag_const.p, c->stream);
   // extra segment: off-diagonal barrier blocks, kept in row order
   launch_extra_flags(c->ents_sorted.p, c->ekeys_sorted.p, ne, c->xflags.p, c->stream);
+  ph.launched(3);
   bytes = 0;
   CK(cub::DeviceSelect::Flagged(nullptr, bytes, c->ents_sorted.p, c->xflags.p, c->xent.p, c->nsel.p, ne, c->stream));
   CK(c->cub_reserve(bytes));
@@ -224,8 +272,9 @@ int prepare_contacts(ando_ctx c, const StepParams& sp) {
   CK(cudaMemcpyAsync(&nx, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->nx = nx;
-  launch_extra_values(c->contacts.p, c->xent.p, c->xcols.p, nx, sp, c->xval.p, c->stream);
+  if (nx) { launch_extra_values(c->contacts.p, c->xent.p, c->xcols.p, nx, sp, c->xval.p, c->stream); ph.launched(); }
   launch_vertex_ranges(c->xkeys.p, nx, V, c->xbegin.p, c->xend.p, c->stream);
+  ph.launched();
   CK(cudaGetLastError());
   return ANDO_OK;
 }
@@ -254,7 +303,7 @@ int upload_rigids(ando_ctx c, const ando_rigid* rigids, int nb) {
     std::memcpy(B.lin, r.linear_velocity, sizeof(B.lin)); std::memcpy(B.ang, r.angular_velocity, sizeof(B.ang));
   }
   CK(c->bodies_dev.upload(c->bodies_host.data(), nb, c->stream));
-  if (nb) launch_rigid_world(c->bodies_dev.p, c->bodies_host.data(), nb, c->stream);
+  if (nb) { Phase ph(c, ANDO_PHASE_SETUP); launch_rigid_world(c->bodies_dev.p, c->bodies_host.data(), nb, c->stream); ph.launched(); }
   CK(cudaGetLastError());
   return ANDO_OK;
 }
@@ -277,26 +326,50 @@ int inner_newton(ando_ctx c, const ando_params& p, const StepParams& sp, ando_st
   pa.P = c->precond.p; pa.b = c->b.p; pa.x = c->d.p; pa.r = c->r.p; pa.z = c->z.p; pa.p0 = c->p0.p; pa.p1 = c->p1.p; pa.Ap = c->Ap.p;
   pa.partials = c->partials.p; pa.ctrl = c->ctrl.p; pa.tol = float(p.pcg_tol); pa.max_iters = p.pcg_max_iters;
   for (int it = 0; it < max_it; ++it) {
-    launch_ctrl_reset(c->ctrl.p, c->stream);
-    if (sp.enable_strain) launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, c->stream);
-    launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
-                    c->pin_vertex.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
-                    c->ebegin.p, c->eend.p, sp, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, c->stream);
-    launch_check(c->ctrl.p, p.pcg_tol, c->stream);
-    launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->val.p, c->precond.p, c->ctrl.p, c->stream);
-    CK(launch_pcg(pa, c->pcg_grid, c->stream));
-    if (ls_wall) launch_ls_wall(c->V, c->x.p, c->d.p, first_wall, c->ctrl.p, c->stream);
-    if (c->n_pe) launch_ls_contacts(c->contacts.p, c->ncontacts, c->x.p, c->d.p, c->ctrl.p, c->stream);
-    launch_update(c->V, c->x.p, c->d.p, c->ctrl.p, c->stream);
+    if (sp.enable_strain) {
+      Phase ph(c, ANDO_PHASE_STRAIN);
+      launch_ctrl_reset(c->ctrl.p, c->stream);
+      launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, c->stream);
+      ph.launched(2);
+    }
+    {
+      Phase ph(c, ANDO_PHASE_GRADIENT);
+      if (!sp.enable_strain) { launch_ctrl_reset(c->ctrl.p, c->stream); ph.launched(); }
+      launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
+                      c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
+                      c->ebegin.p, c->eend.p, sp, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, c->stream);
+      launch_check(c->ctrl.p, p.pcg_tol, c->stream);
+      ph.launched(2);
+    }
+    {
+      Phase ph(c, ANDO_PHASE_ASSEMBLE);
+      launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->val.p, c->precond.p, c->ctrl.p, c->stream);
+      ph.launched();
+    }
+    {
+      Phase ph(c, ANDO_PHASE_PCG);
+      CK(launch_pcg(pa, c->pcg_grid, c->stream));
+      ph.launched();
+    }
+    {
+      Phase ph(c, ANDO_PHASE_LINE_SEARCH);
+      if (ls_wall) { launch_ls_wall(c->V, c->x.p, c->d.p, first_wall, c->ctrl.p, c->stream); ph.launched(); }
+      if (c->n_pe) { launch_ls_contacts(c->contacts.p, c->ncontacts, c->x.p, c->d.p, c->ctrl.p, c->stream); ph.launched(); }
+      launch_update(c->V, c->x.p, c->d.p, c->ctrl.p, c->stream);
+      ph.launched();
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    c->collect();
     const Ctrl& h = *c->ctrl_host;
     st.strain_active = h.strain_active;
     if (h.converged) { ret = 1.0; return ANDO_OK; }
     if (h.pcg_status == PCG_TIMEOUT || h.bar_err) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
     st.newton_iters++;
     st.pcg_iters += h.pcg_iters;
+    c->profile.pcg_iterations += h.pcg_iters;
+    c->profile.newton_iterations += 1;
     st.pcg_max_per_newton = std::max(st.pcg_max_per_newton, h.pcg_iters);
     if (!h.pcg_converged) st.pcg_not_converged++;
     st.last_alpha = h.alpha;
@@ -313,7 +386,9 @@ int upload_constraints(ando_ctx c, const ando_params& p, const ando_pin* pins, i
                        ando_rigid* rigids, int num_rigids, StepParams& sp) {
   cudaStream_t s = c->stream;
   if (c->el_semantics != p.semantics) {
+    Phase ph(c, ANDO_PHASE_SETUP);
     launch_elastic_slots(c->mesh_dev(), c->mu, c->thickness, p.semantics, c->el_a.p, c->el_b.p, s);
+    ph.launched();
     c->el_semantics = p.semantics;
   }
   std::vector<int> order;
@@ -332,6 +407,13 @@ int upload_constraints(ando_ctx c, const ando_params& p, const ando_pin* pins, i
   c->num_pins = (int)order.size();
   CK(c->pin_vertex.upload(pv.data(), pv.size(), s));
   CK(c->pin_target.upload(pt.data(), pt.size(), s));
+  CK(c->pin_head.reserve(c->V));
+  if (c->num_pins) {
+    Phase ph(c, ANDO_PHASE_SETUP);
+    CK(cudaMemsetAsync(c->pin_head.p, 0xff, sizeof(int) * c->V, s));
+    launch_pin_heads(c->pin_vertex.p, c->num_pins, c->pin_head.p, s);
+    ph.launched();
+  }
   std::vector<WallDev> wd(num_walls);
   int first_wall = -1;
   for (int k = 0; k < num_walls; ++k) {
@@ -368,23 +450,26 @@ int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_ri
     if (rc) return rc;
   }
   st.beta = beta;
+  Phase ph(c, ANDO_PHASE_FINISH);
   if (beta > 1e-6) {
     double damp = p.velocity_damping > 0.0 ? 1.0 - std::min(std::max(p.velocity_damping, 0.0), 1.0) : 1.0;
     launch_velocity(c->V, c->x.p, c->x_old.p, beta * p.dt, damp, c->v.p, s);
+    ph.launched();
     if (p.contact_restitution > 0.0) {
       double e = std::min(std::max(p.contact_restitution, 0.0), 1.0);
-      rc = detect(c, num_rigids);
+      rc = detect(c, num_rigids, ANDO_PHASE_FINISH);
       if (rc) return rc;
-      launch_restitution_contacts(c->contacts.p, c->ncontacts, c->mass.p, c->V, e, std::max(p.contact_gap_max, 1e-5),
-                                  c->bodies_dev.p, num_rigids, c->v.p, s);
-      launch_restitution_walls(c->V, c->x.p, c->walls.p, num_walls, e, p.contact_gap_max, c->v.p, s);
+      if (c->ncontacts) { launch_restitution_contacts(c->contacts.p, c->ncontacts, c->mass.p, c->V, e, std::max(p.contact_gap_max, 1e-5),
+                                                      c->bodies_dev.p, num_rigids, c->v.p, s); ph.launched(); }
+      if (num_walls) { launch_restitution_walls(c->V, c->x.p, c->walls.p, num_walls, e, p.contact_gap_max, c->v.p, s); ph.launched(); }
     }
   }
   if (num_rigids > 0) {
-    rc = detect(c, num_rigids);
+    rc = detect(c, num_rigids, ANDO_PHASE_FINISH);
     if (rc) return rc;
     long long units = (long long)c->V * (1 + num_rigids);
     launch_rigid_coupling(c->mesh_dev(), c->contacts.p, c->ncontacts, sp, c->bodies_dev.p, num_rigids, c->det_offsets.p, units, p.dt, s);
+    ph.launched();
     CK(cudaMemcpyAsync(c->bodies_host.data(), c->bodies_dev.p, sizeof(RigidDev) * num_rigids, cudaMemcpyDeviceToHost, s));
   }
   return ANDO_OK;
@@ -473,6 +558,19 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     auto b = cols.begin() + rowptr[r], e = cols.begin() + rowptr[r + 1];
     return int(std::lower_bound(b, e, col) - cols.begin());
   };
+  // unique edges in first-seen order (mesh.cpp:77-98)
+  std::vector<int> edges;
+  {
+    std::unordered_set<unsigned long long> seen;
+    seen.reserve(size_t(3) * T);
+    for (int f = 0; f < T; ++f)
+      for (int i = 0; i < 3; ++i) {
+        int a = tris[3 * f + i], b = tris[3 * f + (i + 1) % 3];
+        int lo = std::min(a, b), hi = std::max(a, b);
+        unsigned long long key = ((unsigned long long)(unsigned)lo << 32) | (unsigned)hi;
+        if (seen.insert(key).second) { edges.push_back(lo); edges.push_back(hi); }
+      }
+  }
   std::vector<int> face_slot(9ull * T), cptr(nnzb + 1, 0), contrib(9ull * T), vfp(V + 1, 0), vfl(3ull * T);
   for (int f = 0; f < T; ++f)
     for (int a = 0; a < 3; ++a)
@@ -510,6 +608,8 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->vf_ptr.upload(vfp.data(), V + 1, s));
   CK(c->vf.upload(vfl.data(), 3ull * T, s));
   CK(c->mesh_x.upload(vertices, 3ull * V, s));
+  c->E = int(edges.size() / 2);
+  CK(c->edges.upload(edges.data(), edges.size(), s));
   CK(c->el_a.reserve(nnzb)); CK(c->el_b.reserve(nnzb)); CK(c->g_el.reserve(3ull * V));
   // per-vertex / per-slot work buffers
   CK(c->x.reserve(3ull * V)); CK(c->v.reserve(3ull * V)); CK(c->x_prev.reserve(3ull * V)); CK(c->mass.reserve(V));
@@ -574,7 +674,11 @@ int32_t ando_apply_gravity(ando_ctx c, const double g[3], double dt) {
   if (rc) return rc;
   if (!c->state_ready) return fail(ANDO_ERR_STATE, "state not uploaded");
   if (!g) return fail(ANDO_ERR_INVALID, "null gravity");
-  launch_gravity(c->V, c->x.p, c->v.p, g[0], g[1], g[2], dt, c->stream);
+  {
+    Phase ph(c, ANDO_PHASE_FINISH);
+    launch_gravity(c->V, c->x.p, c->v.p, g[0], g[1], g[2], dt, c->stream);
+    ph.launched();
+  }
   CK(cudaGetLastError());
   return ANDO_OK;
 }
@@ -597,7 +701,11 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
   StepParams sp;
   rc = upload_constraints(c, p, pins, num_pins, walls, num_walls, rigids, num_rigids, sp);
   if (rc) return rc;
-  launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
+  {
+    Phase ph(c, ANDO_PHASE_SETUP);
+    launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
+    ph.launched();
+  }
   rc = detect(c, num_rigids);
   if (rc) return rc;
   st.contacts = c->ncontacts;
@@ -613,6 +721,7 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     std::memcpy(rigids[i].position, B.pos, sizeof(B.pos)); std::memcpy(rigids[i].rotation, B.R, sizeof(B.R));
     std::memcpy(rigids[i].linear_velocity, B.lin, sizeof(B.lin)); std::memcpy(rigids[i].angular_velocity, B.ang, sizeof(B.ang));
   }
+  c->collect();
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   st.device_ms = ms;
@@ -644,7 +753,7 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   launch_ctrl_reset(c->ctrl.p, s);
   if (sp.enable_strain) launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, s);
   launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
-                  c->pin_vertex.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
+                  c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
                   c->ebegin.p, c->eend.p, sp, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, s);
   launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->val.p, c->precond.p, c->ctrl.p, s);
   CK(cudaGetLastError());
@@ -694,6 +803,75 @@ int32_t ando_last_system(ando_ctx c, int32_t* V, int32_t* nnzb, int32_t* rowptr,
   if (rhs) CK(cudaMemcpyAsync(rhs, c->b.p, sizeof(float) * 3ull * c->V, cudaMemcpyDeviceToHost, s));
   if (sol) CK(cudaMemcpyAsync(sol, c->d.p, sizeof(float) * 3ull * c->V, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  return ANDO_OK;
+}
+
+int32_t ando_broad_phase(ando_ctx c, int32_t kind, double pad, int32_t* pairs, int32_t capacity, int32_t* count) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  if (!count || capacity < 0 || (capacity && !pairs) || (kind != 0 && kind != 1) || !(pad >= 0.0))
+    return fail(ANDO_ERR_INVALID, "broad-phase arguments");
+  cudaStream_t s = c->stream;
+  int n = 0;
+  {
+    Phase ph(c, ANDO_PHASE_SETUP);
+    Lbvh& B = kind == 0 ? c->bvh_tri : c->bvh_edge;
+    long long before = B.launches;
+    if (kind == 0) {
+      CK(B.build(c->x.p, c->tris.p, 3, c->T, float(pad), c->cub_tmp, s));
+      CK(B.query(c->x.p, 0, nullptr, c->V, float(pad), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &n, s));
+    } else {
+      CK(B.build(c->x.p, c->edges.p, 2, c->E, float(pad), c->cub_tmp, s));
+      CK(B.query(c->x.p, 1, c->edges.p, c->E, float(pad), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &n, s));
+    }
+    ph.launched(int(B.launches - before));
+  }
+  *count = n;
+  int m = std::min(n, capacity);
+  if (m) CK(cudaMemcpyAsync(pairs, c->pairs.p, sizeof(int2) * m, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return n > capacity ? fail(ANDO_ERR_CAPACITY, "pair buffer too small") : ANDO_OK;
+}
+
+int32_t ando_last_contact_blocks(ando_ctx c, int32_t* count, int32_t* rows, int32_t* cols, float* vals) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!count) return fail(ANDO_ERR_INVALID, "null count");
+  *count = c->nx;
+  cudaStream_t s = c->stream;
+  if (c->nx) {
+    if (rows) CK(cudaMemcpyAsync(rows, c->xkeys.p, sizeof(int) * c->nx, cudaMemcpyDeviceToHost, s));
+    if (cols) CK(cudaMemcpyAsync(cols, c->xcols.p, sizeof(int) * c->nx, cudaMemcpyDeviceToHost, s));
+    if (vals) CK(cudaMemcpyAsync(vals, c->xval.p, sizeof(float) * 9ull * c->nx, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  return ANDO_OK;
+}
+
+int32_t ando_profile_enable(ando_ctx c, int32_t enable) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  c->collect();
+  c->prof = enable != 0;
+  std::memset(&c->profile, 0, sizeof(c->profile));
+  return ANDO_OK;
+}
+
+int32_t ando_profile_read(ando_ctx c, ando_profile* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out) return fail(ANDO_ERR_INVALID, "null profile");
+  CK(cudaStreamSynchronize(c->stream));
+  c->collect();
+  *out = c->profile;
+  return ANDO_OK;
+}
+
+int32_t ando_ctx_stream(ando_ctx c, void** stream) {
+  if (!c || !stream) return fail(ANDO_ERR_INVALID, "null argument");
+  *stream = (void*)c->stream;
   return ANDO_OK;
 }
 

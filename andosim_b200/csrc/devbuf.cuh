@@ -1,0 +1,32 @@
+// devbuf.cuh -- owning device buffer that only grows (host-side helper).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace ando {
+
+template <class T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t reserve(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    if (p) { cudaFree(p); p = nullptr; n = 0; }
+    size_t c = count ? count : 1;
+    cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+    if (e == cudaSuccess) n = c;
+    return e;
+  }
+  cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
+    cudaError_t e = reserve(count);
+    if (e != cudaSuccess || count == 0) return e;
+    return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+}  // namespace ando

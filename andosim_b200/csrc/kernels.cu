@@ -521,9 +521,9 @@ __global__ void k_strain_face(MeshDev m, const double* x, StepParams p, unsigned
 // writes the vertex's diagonal Hessian terms (mass, pin, wall, contact,
 // friction blocks of assemble_system_matrix) for the assembly kernel, and
 // folds |g|_inf into ctrl->gnorm_bits.
-__global__ void k_gradient(MeshDev m, const double* x, const double* x_hat, const double* x_prev, const double* g_const,
+__global__ void __launch_bounds__(256, 3) k_gradient(MeshDev m, const double* x, const double* x_hat, const double* x_prev, const double* g_const,
                            const double* diag_const, const unsigned char* sflags, const StrainSV* sv,
-                           const int* pin_vertex, const double* pin_target, int num_pins, const WallDev* walls,
+                           const int* pin_vertex, const int* pin_head, const double* pin_target, int num_pins, const WallDev* walls,
                            const ContactDev* contacts, const ContactEntry* ents, const int* ebegin, const int* eend,
                            StepParams p, double* g, float* b, double* diag_extra, Ctrl* ctrl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -553,11 +553,10 @@ __global__ void k_gradient(MeshDev m, const double* x, const double* x_hat, cons
     int ds = m.diag_slot[i];
     double A = mdiag + m.el_a[ds], B = mdiag + m.el_b[ds];
     double D0 = fmax(A, 1e-8), D2 = fmax(B, 1e-8);  // enforce_spd of the diagonal H_total block
-    // pins (sorted by vertex)
+    // pins (sorted by vertex; pin_head[i] = first pin of vertex i or -1)
     if (num_pins > 0) {
-      int lo = 0, hi = num_pins;
-      while (lo < hi) { int mid = (lo + hi) >> 1; if (pin_vertex[mid] < i) lo = mid + 1; else hi = mid; }
-      for (int k = lo; k < num_pins && pin_vertex[k] == i; ++k) {
+      int lo = pin_head[i];
+      for (int k = lo; k >= 0 && k < num_pins && pin_vertex[k] == i; ++k) {
         d3 off = xi - mk(pin_target[3 * k], pin_target[3 * k + 1], pin_target[3 * k + 2]);
         double len = nrm(off);
         d3 dir = len > 1e-9 ? off / len : mk(1, 0, 0);
@@ -631,6 +630,12 @@ __global__ void k_gradient(MeshDev m, const double* x, const double* x_hat, cons
   }
   local = warp_max_d(local);
   if ((threadIdx.x & 31) == 0) atomicMax(&ctrl->gnorm_bits, (unsigned long long)__double_as_longlong(local));
+}
+
+__global__ void k_pin_heads(const int* pin_vertex, int num_pins, int* pin_head) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= num_pins) return;
+  if (k == 0 || pin_vertex[k - 1] != pin_vertex[k]) pin_head[pin_vertex[k]] = k;
 }
 
 __global__ void k_check(Ctrl* c, double tol) {
@@ -967,12 +972,15 @@ void launch_ctrl_reset(Ctrl* ctrl, cudaStream_t s) { k_ctrl_reset<<<1, 1, 0, s>>
 void launch_strain_face(const MeshDev& m, const double* x, const StepParams& p, unsigned char* flags, StrainSV* sv, Ctrl* ctrl, cudaStream_t s) {
   if (m.T) k_strain_face<<<nblk(m.T), TPB, 0, s>>>(m, x, p, flags, sv, ctrl);
 }
+void launch_pin_heads(const int* pin_vertex, int num_pins, int* pin_head, cudaStream_t s) {
+  if (num_pins) k_pin_heads<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, pin_head);
+}
 void launch_gradient(const MeshDev& m, const double* x, const double* x_hat, const double* x_prev, const double* g_const,
                      const double* diag_const, const unsigned char* sflags, const StrainSV* sv,
-                     const int* pin_vertex, const double* pin_target, int num_pins, const WallDev* walls,
+                     const int* pin_vertex, const int* pin_head, const double* pin_target, int num_pins, const WallDev* walls,
                      const ContactDev* contacts, const ContactEntry* ents, const int* ebegin, const int* eend,
                      const StepParams& p, double* g, float* b, double* diag_extra, Ctrl* ctrl, cudaStream_t s) {
-  if (m.V) k_gradient<<<nblk(m.V), TPB, 0, s>>>(m, x, x_hat, x_prev, g_const, diag_const, sflags, sv, pin_vertex, pin_target, num_pins, walls,
+  if (m.V) k_gradient<<<nblk(m.V), TPB, 0, s>>>(m, x, x_hat, x_prev, g_const, diag_const, sflags, sv, pin_vertex, pin_head, pin_target, num_pins, walls,
                                                 contacts, ents, ebegin, eend, p, g, b, diag_extra, ctrl);
 }
 void launch_check(Ctrl* ctrl, double tol, cudaStream_t s) { k_check<<<1, 1, 0, s>>>(ctrl, tol); }

@@ -37,10 +37,11 @@ void launch_ctrl_reset(Ctrl* ctrl, cudaStream_t s);
 void launch_strain_face(const MeshDev& m, const double* x, const StepParams& p, unsigned char* flags, StrainSV* sv, Ctrl* ctrl, cudaStream_t s);
 void launch_gradient(const MeshDev& m, const double* x, const double* x_hat, const double* x_prev, const double* g_const,
                      const double* diag_const, const unsigned char* sflags, const StrainSV* sv,
-                     const int* pin_vertex, const double* pin_target, int num_pins, const WallDev* walls,
+                     const int* pin_vertex, const int* pin_head, const double* pin_target, int num_pins, const WallDev* walls,
                      const ContactDev* contacts, const ContactEntry* ents, const int* ebegin, const int* eend,
                      const StepParams& p, double* g, float* b, double* diag_extra, Ctrl* ctrl, cudaStream_t s);
 void launch_check(Ctrl* ctrl, double tol, cudaStream_t s);
+void launch_pin_heads(const int* pin_vertex, int num_pins, int* pin_head, cudaStream_t s);
 void launch_assemble(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                      float* val, float* precond, const Ctrl* ctrl, cudaStream_t s);
 void launch_ls_wall(int V, const double* x, const float* d, WallDev w, Ctrl* ctrl, cudaStream_t s);

@@ -1,0 +1,320 @@
+// lbvh.cu -- linear BVH broad phase (replaces Collision::build_*_bvh and
+// broad_phase_triangles / broad_phase_edges, collision.cpp:65-276).
+//
+// Boxes are FP32, built from the FP32-rounded positions exactly as the
+// reference's Real=float AABBs are (collision.cpp:48-62), optionally inflated
+// by `pad`. The candidate predicate is the reference's inclusive overlap test
+// (collision.h:37-41) with a +-1e-4 point box, the incident-face exclusion
+// (collision.cpp:221) and, for edges, e1 < e2 and no shared vertex
+// (collision.cpp:259-266). Any correct hierarchy returns exactly the set of
+// primitive pairs whose boxes pass that test, so the result equals the
+// brute-force query bit for bit once sorted.
+//
+// Pipeline: primitive boxes -> scene bounds -> 30-bit Morton codes of box
+// centres (index appended, so keys are unique) -> radix sort -> Karras
+// hierarchy (one thread per internal node) -> bottom-up refit with arrival
+// counters -> one thread per query with an explicit stack; hits are compacted
+// with a warp ballot (one atomic per warp) and the pair list is then sorted so
+// its order does not depend on scheduling.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
+
+#include "lbvh.cuh"
+
+namespace ando {
+
+namespace {
+
+constexpr int TPB = 256;
+inline int nblk(long long n) { return int((n + TPB - 1) / TPB); }
+
+using Box = LbvhBox;
+
+__device__ inline float3 xf(const double* x, int i) { return make_float3(float(x[3 * i]), float(x[3 * i + 1]), float(x[3 * i + 2])); }
+
+__global__ void k_prim_boxes(const double* x, const int* prims, int arity, int n, float pad, Box* boxes) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float3 p = xf(x, prims[arity * i]);
+  Box b; b.lo[0] = b.hi[0] = p.x; b.lo[1] = b.hi[1] = p.y; b.lo[2] = b.hi[2] = p.z;
+  for (int k = 1; k < arity; ++k) {
+    float3 q = xf(x, prims[arity * i + k]);
+    b.lo[0] = fminf(b.lo[0], q.x); b.lo[1] = fminf(b.lo[1], q.y); b.lo[2] = fminf(b.lo[2], q.z);
+    b.hi[0] = fmaxf(b.hi[0], q.x); b.hi[1] = fmaxf(b.hi[1], q.y); b.hi[2] = fmaxf(b.hi[2], q.z);
+  }
+  if (pad > 0.f) for (int k = 0; k < 3; ++k) { b.lo[k] -= pad; b.hi[k] += pad; }
+  boxes[i] = b;
+}
+
+// Scene bounds as min/max over box centres (block reduction + float atomics
+// on the ordered-int encoding, exact for min/max).
+__device__ inline int f2ord(float f) { int i = __float_as_int(f); return i >= 0 ? i : i ^ 0x7fffffff; }
+__device__ inline float ord2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__global__ void k_bounds_init(int* b) {
+  if (threadIdx.x < 3) { b[threadIdx.x] = 0x7fffffff; b[3 + threadIdx.x] = (int)0x80000000; }
+}
+__global__ void k_bounds(const Box* boxes, int n, int* bounds) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  if (i < n) for (int k = 0; k < 3; ++k) { float c = 0.5f * (boxes[i].lo[k] + boxes[i].hi[k]); lo[k] = c; hi[k] = c; }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o; o >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) for (int k = 0; k < 3; ++k) { atomicMin(&bounds[k], f2ord(lo[k])); atomicMax(&bounds[3 + k], f2ord(hi[k])); }
+}
+
+__device__ inline unsigned expand10(unsigned v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void k_morton(const Box* boxes, int n, const int* bounds, unsigned long long* keys, int* vals) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned m = 0;
+  unsigned q[3];
+  for (int k = 0; k < 3; ++k) {
+    float lo = ord2f(bounds[k]), hi = ord2f(bounds[3 + k]);
+    float c = 0.5f * (boxes[i].lo[k] + boxes[i].hi[k]);
+    float t = hi > lo ? (c - lo) / (hi - lo) : 0.5f;
+    t = fminf(fmaxf(t, 0.f), 1.f);
+    q[k] = min(1023u, (unsigned)(t * 1024.f));
+  }
+  m = (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
+  keys[i] = ((unsigned long long)m << 32) | (unsigned)i;
+  vals[i] = i;
+}
+
+__device__ inline int delta(const unsigned long long* k, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  return __clzll(k[i] ^ k[j]);
+}
+
+// Karras 2012: internal node i covers a key range found from the common
+// prefix lengths of its neighbours. Nodes [0, n-1) are internal, leaves are
+// encoded as n-1 + sorted position.
+__global__ void k_karras(const unsigned long long* keys, int n, int* left, int* right, int* parent) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+  int dmin = delta(keys, n, i, i - d);
+  int lmax = 2;
+  while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  int j = i + l * d;
+  int dnode = delta(keys, n, i, j);
+  int s = 0;
+  int t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  int gamma = i + s * d + min(d, 0);
+  int lo = min(i, j), hi = max(i, j);
+  int lc = (lo == gamma) ? (n - 1 + gamma) : gamma;
+  int rc = (hi == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
+  left[i] = lc; right[i] = rc;
+  parent[lc] = i; parent[rc] = i;
+}
+
+// Bottom-up refit: the second child to arrive at a node computes its box.
+__global__ void k_refit(const Box* boxes, const int* order, int n, const int* left, const int* right, const int* parent,
+                        Box* nodes, int* arrive) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int leaf = n - 1 + i;
+  nodes[leaf] = boxes[order[i]];
+  if (n == 1) return;
+  int p = parent[leaf];
+  while (p >= 0) {
+    __threadfence();
+    if (atomicAdd(&arrive[p], 1) == 0) return;  // first arrival: the sibling finishes this node
+    __threadfence();
+    // the sibling's box was written by another thread: read it past L1
+    Box a, b;
+    const float* pa = reinterpret_cast<const float*>(nodes + left[p]);
+    const float* pb = reinterpret_cast<const float*>(nodes + right[p]);
+    for (int k = 0; k < 3; ++k) { a.lo[k] = __ldcg(pa + k); a.hi[k] = __ldcg(pa + 3 + k); b.lo[k] = __ldcg(pb + k); b.hi[k] = __ldcg(pb + 3 + k); }
+    Box u;
+    for (int k = 0; k < 3; ++k) { u.lo[k] = fminf(a.lo[k], b.lo[k]); u.hi[k] = fmaxf(a.hi[k], b.hi[k]); }
+    nodes[p] = u;
+    p = p == 0 ? -1 : parent[p];
+  }
+}
+
+__device__ inline bool overlap(const Box& a, const Box& b) {
+  return a.lo[0] <= b.hi[0] && a.hi[0] >= b.lo[0] && a.lo[1] <= b.hi[1] && a.hi[1] >= b.lo[1] && a.lo[2] <= b.hi[2] && a.hi[2] >= b.lo[2];
+}
+
+// Warp-ballot append: one atomic per warp per round of hits.
+__device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, int cap) {
+  unsigned mask = __ballot_sync(0xffffffffu, hit);
+  if (!mask) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (hit) {
+    int slot = base + __popc(mask & ((1u << lane) - 1u));
+    if (slot < cap) out[slot] = make_int2(q, prim);
+  }
+}
+
+// One thread per query. kind 0: query = vertex (point box +-1e-4 inflated by
+// pad), prims = triangles, skip incident triangles. kind 1: query = edge,
+// prims = edges, keep e1 < e2 without shared vertex.
+__global__ void k_query(const double* x, const int* qprims, int kind, int nq, float pad, const int* prims, int n,
+                        const int* order, const int* left, const int* right, const Box* nodes, int2* out, int* count, int cap) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = q < nq;
+  Box qb;
+  int qa = -1, qc = -1;
+  if (active) {
+    if (kind == 0) {
+      float3 p = xf(x, q);
+      float e = 1e-4f;
+      qb.lo[0] = p.x - e; qb.lo[1] = p.y - e; qb.lo[2] = p.z - e;
+      qb.hi[0] = p.x + e; qb.hi[1] = p.y + e; qb.hi[2] = p.z + e;
+      if (pad > 0.f) for (int k = 0; k < 3; ++k) { qb.lo[k] -= pad; qb.hi[k] += pad; }
+    } else {
+      qa = qprims[2 * q]; qc = qprims[2 * q + 1];
+      float3 a = xf(x, qa), b = xf(x, qc);
+      qb.lo[0] = fminf(a.x, b.x); qb.lo[1] = fminf(a.y, b.y); qb.lo[2] = fminf(a.z, b.z);
+      qb.hi[0] = fmaxf(a.x, b.x); qb.hi[1] = fmaxf(a.y, b.y); qb.hi[2] = fmaxf(a.z, b.z);
+      if (pad > 0.f) for (int k = 0; k < 3; ++k) { qb.lo[k] -= pad; qb.hi[k] += pad; }
+    }
+  }
+  // Depth-first with an explicit stack. With unique 64-bit keys the hierarchy
+  // is at most 64 levels deep, so 96 slots never overflow; an overflow would
+  // be reported through count[1] instead of dropping candidates silently.
+  constexpr int STACK = 96;
+  int stack[STACK];
+  int sp = 0;
+  const int leaf0 = n - 1;          // with one primitive the root (node 0) is its leaf
+  if (active && n > 0) stack[sp++] = 0;
+  while (__any_sync(0xffffffffu, sp > 0)) {
+    bool hit = false;
+    int prim = -1;
+    if (sp > 0) {
+      int node = stack[--sp];
+      bool is_leaf = node >= leaf0;
+      const Box& nb = nodes[node];
+      if (overlap(qb, nb)) {
+        if (is_leaf) {
+          prim = order[node - leaf0];
+          if (kind == 0) {
+            hit = prims[3 * prim] != q && prims[3 * prim + 1] != q && prims[3 * prim + 2] != q;
+          } else {
+            int pa = prims[2 * prim], pc = prims[2 * prim + 1];
+            hit = q < prim && pa != qa && pa != qc && pc != qa && pc != qc;
+          }
+        } else if (sp <= STACK - 2) {
+          stack[sp++] = left[node];
+          stack[sp++] = right[node];
+        } else {
+          atomicAdd(count + 1, 1);
+        }
+      }
+    }
+    emit(hit, q, prim, out, count, cap);
+  }
+}
+
+__global__ void k_pair_keys(const int2* pairs, int n, unsigned long long* keys) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = ((unsigned long long)(unsigned)pairs[i].x << 32) | (unsigned)pairs[i].y;
+}
+
+}  // namespace
+
+cudaError_t Lbvh::reserve_prims(int n) {
+  cudaError_t e;
+  size_t N = n > 0 ? n : 1;
+  if ((e = boxes.reserve(N))) return e;
+  if ((e = keys.reserve(N))) return e;
+  if ((e = keys_sorted.reserve(N))) return e;
+  if ((e = idx.reserve(N))) return e;
+  if ((e = order.reserve(N))) return e;
+  if ((e = left.reserve(N))) return e;
+  if ((e = right.reserve(N))) return e;
+  if ((e = parent.reserve(2 * N))) return e;
+  if ((e = nodes.reserve(2 * N))) return e;
+  if ((e = arrive.reserve(N))) return e;
+  if ((e = bounds.reserve(6))) return e;
+  return cudaSuccess;
+}
+
+// Build the hierarchy over `n` primitives of `arity` vertex indices each.
+cudaError_t Lbvh::build(const double* x, const int* prims_, int arity, int n_, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s) {
+  n = n_;
+  prims = prims_;
+  cudaError_t e = reserve_prims(n);
+  if (e) return e;
+  if (n == 0) return cudaSuccess;
+  k_prim_boxes<<<nblk(n), TPB, 0, s>>>(x, prims, arity, n, pad, boxes.p);
+  k_bounds_init<<<1, 32, 0, s>>>(bounds.p);
+  k_bounds<<<nblk(n), TPB, 0, s>>>(boxes.p, n, bounds.p);
+  k_morton<<<nblk(n), TPB, 0, s>>>(boxes.p, n, bounds.p, keys.p, idx.p);
+  size_t bytes = 0;
+  if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, keys_sorted.p, idx.p, order.p, n, 0, 64, s))) return e;
+  if ((e = tmp.reserve(bytes))) return e;
+  if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, keys.p, keys_sorted.p, idx.p, order.p, n, 0, 64, s))) return e;
+  if (n > 1) {
+    if ((e = cudaMemsetAsync(parent.p, 0xff, sizeof(int) * (2 * n - 1), s))) return e;
+    k_karras<<<nblk(n - 1), TPB, 0, s>>>(keys_sorted.p, n, left.p, right.p, parent.p);
+    if ((e = cudaMemsetAsync(arrive.p, 0, sizeof(int) * n, s))) return e;
+  }
+  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p);
+  launches += n > 1 ? 6 : 5;
+  return cudaGetLastError();
+}
+
+// Query the hierarchy; returns the sorted (query, primitive) pairs in `out`
+// (capacity grown as needed) and their number in *npairs.
+cudaError_t Lbvh::query(const double* x, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
+                        DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
+                        DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
+  cudaError_t e;
+  *npairs = 0;
+  if (n == 0 || nq == 0) return cudaSuccess;
+  if ((e = counter.reserve(2))) return e;
+  if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    int cap = int(scratch.n);
+    if ((e = cudaMemsetAsync(counter.p, 0, 2 * sizeof(int), s))) return e;
+    k_query<<<nblk(nq), TPB, 0, s>>>(x, qprims, kind, nq, pad, prims, n, order.p, left.p, right.p, nodes.p, scratch.p, counter.p, cap);
+    launches += 1;
+    int cnt2[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(cnt2, counter.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaStreamSynchronize(s))) return e;
+    if (cnt2[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
+    int cnt = cnt2[0];
+    if (cnt <= cap) { *npairs = cnt; break; }
+    if ((e = scratch.reserve(size_t(cnt) + size_t(cnt) / 4))) return e;
+  }
+  int m = *npairs;
+  if (m == 0) return cudaSuccess;
+  if ((e = k0.reserve(m))) return e;
+  if ((e = k1.reserve(m))) return e;
+  if ((e = out.reserve(m))) return e;
+  k_pair_keys<<<nblk(m), TPB, 0, s>>>(scratch.p, m, k0.p);
+  launches += 1;
+  size_t bytes = 0;
+  if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
+  if ((e = tmp.reserve(bytes))) return e;
+  if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
+  return cudaGetLastError();
+}
+
+}  // namespace ando

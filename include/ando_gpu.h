@@ -128,6 +128,27 @@ typedef struct {
 
 typedef struct ando_ctx_s* ando_ctx;
 
+/* Phases of a step timed by the profiler (no reference counterpart; the
+ * reference only times whole steps from Python, demo_framework.py:144-170). */
+typedef enum {
+  ANDO_PHASE_SETUP = 0,        /* prediction, contact detection, per-step contact constants */
+  ANDO_PHASE_STRAIN = 1,       /* per-face strain-limit SVD and barrier terms */
+  ANDO_PHASE_GRADIENT = 2,     /* per-vertex Newton gradient and diagonal terms */
+  ANDO_PHASE_ASSEMBLE = 3,     /* BSR Hessian assembly + block-Jacobi inverse */
+  ANDO_PHASE_PCG = 4,          /* persistent PCG solve */
+  ANDO_PHASE_LINE_SEARCH = 5,  /* feasibility masks and position update */
+  ANDO_PHASE_FINISH = 6,       /* velocity update, restitution, rigid coupling, gravity */
+  ANDO_PHASE_COUNT = 7
+} ando_phase;
+
+typedef struct {
+  int64_t launches;                        /* this library's kernel launches since the last reset */
+  int64_t phase_launches[ANDO_PHASE_COUNT];
+  double phase_ms[ANDO_PHASE_COUNT];       /* summed CUDA-event time of each phase (profiling on) */
+  int64_t pcg_iterations;                  /* PCG iterations inside the profiled PCG launches */
+  int64_t newton_iterations;               /* Newton iterations that assembled and solved */
+} ando_profile;
+
 /* Library identity. */
 ANDO_API int32_t ando_abi_version(void);
 ANDO_API const char* ando_status_string(int32_t status);
@@ -199,6 +220,32 @@ ANDO_API int32_t ando_eval_system(ando_ctx ctx, const ando_params* params,
                                   const ando_pin* pins, int32_t num_pins,
                                   const ando_wall* walls, int32_t num_walls,
                                   const ando_rigid* rigids, int32_t num_rigids);
+
+/* The per-step contact blocks between vertices that share no mesh face
+ * (vertex-triangle and edge-edge barrier terms), which live outside the
+ * static pattern of ando_last_system: block k sits at (rows[k], cols[k]).
+ * Pass NULL pointers to query the count. */
+ANDO_API int32_t ando_last_contact_blocks(ando_ctx ctx, int32_t* count, int32_t* rows, int32_t* cols, float* vals);
+
+/* Broad-phase candidate pairs at the current positions from the device LBVH
+ * (replaces Collision::build_*_bvh / broad_phase_*, collision.cpp:65-276, with
+ * the query the reference intends; its own BVH drops every leaf holding 2..4
+ * primitives). kind 0: (vertex, triangle) pairs, the vertex not a corner of
+ * the triangle; kind 1: (edge, edge) pairs with e1 < e2 and no shared vertex,
+ * edges numbered in Mesh::compute_edges' first-seen order. Boxes are FP32 with
+ * the reference's inclusive overlap test and +-1e-4 point box, each inflated
+ * by `pad`. Pairs (2 ints each) come sorted by (first, second); with too small
+ * a `capacity` the call returns ANDO_ERR_CAPACITY and the total in *count. */
+ANDO_API int32_t ando_broad_phase(ando_ctx ctx, int32_t kind, double pad, int32_t* pairs, int32_t capacity, int32_t* count);
+
+/* Start (enable != 0) or stop per-phase CUDA-event timing; resets the counters.
+ * Kernel launches are counted whether or not timing is on. */
+ANDO_API int32_t ando_profile_enable(ando_ctx ctx, int32_t enable);
+ANDO_API int32_t ando_profile_read(ando_ctx ctx, ando_profile* out);
+
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
+ * callers that time or order work around the library's. */
+ANDO_API int32_t ando_ctx_stream(ando_ctx ctx, void** stream);
 
 /* Newton gradient (FP64, 3*num_vertices) of the most recent Newton iteration. */
 ANDO_API int32_t ando_last_gradient(ando_ctx ctx, double* gradient, int32_t num_vertices);

@@ -815,11 +815,16 @@ template <class R> AABB<R> point_box(const V3<R>& p) {
 }
 
 // Candidate vertex-triangle pairs (v, t) and edge-edge pairs (e1 < e2).
+// `pad` inflates every box (triangle, edge and point) in the INTENDED mode;
+// the LITERAL mode is the reference's query and ignores it.
+template <class R> void inflate(AABB<R>& b, R pad) { for (int k = 0; k < 3; ++k) { b.lo[k] = b.lo[k] - pad; b.hi[k] = b.hi[k] + pad; } }
+
 template <class R> void broad_phase(const Mesh<R>& m, const std::vector<V3<R>>& x, BroadPhase mode,
-                                    std::vector<std::pair<int, int>>& vt, std::vector<std::pair<int, int>>& ee) {
+                                    std::vector<std::pair<int, int>>& vt, std::vector<std::pair<int, int>>& ee, R pad = R(0)) {
   vt.clear(); ee.clear();
   auto tb = triangle_boxes(m, x);
   auto eb = edge_boxes(m, x);
+  if (mode == BroadPhase::INTENDED && pad > R(0)) { for (auto& b : tb) inflate(b, pad); for (auto& b : eb) inflate(b, pad); }
   if (mode == BroadPhase::LITERAL) {
     BVH<R> tbvh = bvh_build(tb), ebvh = bvh_build(eb);
     if (!tbvh.nodes.empty()) {
@@ -860,6 +865,7 @@ template <class R> void broad_phase(const Mesh<R>& m, const std::vector<V3<R>>& 
   } else {
     for (size_t v = 0; v < x.size(); ++v) {
       AABB<R> pbx = point_box(x[v]);
+      if (pad > R(0)) inflate(pbx, pad);
       for (size_t t = 0; t < tb.size(); ++t) {
         if (!pbx.overlaps(tb[t])) continue;
         const auto& tri = m.triangles[t];
@@ -903,7 +909,8 @@ template <class R> void narrow_pt(const V3<R>& p, const V3<R>& a, const V3<R>& b
 }
 
 // collision.cpp:389-452 (clamped segment-segment closest points)
-template <class R> void narrow_ee(const V3<R>& p0, const V3<R>& p1, const V3<R>& q0, const V3<R>& q1, R& dist, V3<R>& normal, V3<R>& wp, V3<R>& wq) {
+template <class R> void narrow_ee(const V3<R>& p0, const V3<R>& p1, const V3<R>& q0, const V3<R>& q1, R& dist, V3<R>& normal, V3<R>& wp, V3<R>& wq,
+                                  R* s_out = nullptr, R* t_out = nullptr) {
   V3<R> d1 = p1 - p0, d2 = q1 - q0, r = p0 - q0;
   R a = d1.dot(d1), e = d2.dot(d2), f = d2.dot(r);
   R s, t; const R eps = R(1e-10);
@@ -925,6 +932,8 @@ template <class R> void narrow_ee(const V3<R>& p0, const V3<R>& p1, const V3<R>&
     wp = p0 + d1 * s; wq = q0 + d2 * t;
   }
   V3<R> df = wp - wq; dist = df.norm(); normal = dist > R(1e-10) ? df / dist : V3<R>(0, 0, 1);
+  if (s_out) *s_out = s;
+  if (t_out) *t_out = t;
 }
 
 // collision.cpp:11-43
@@ -1369,6 +1378,373 @@ template <class R> class Integrator {
       rigids[size_t(c.rigid_body_index)].apply_force(c.witness_q, -(nn * dV), R(0));
     }
     for (auto& b : rigids) b.integrate(p.dt);
+  }
+};
+
+
+// ======================================================================
+// CORRECTED semantics: the step the reference intends (its docs/dev/
+// PROJECT_SPEC.md), with the defects listed in the REFERENCE path fixed:
+//   * elasticity on the current positions; the constant Hessian is the exact
+//     Hessian of k |F - R|^2 for a fixed frame R: 2k (G G^T) (x) I3 with
+//     G = [[-1,-1],[1,0],[0,1]] Dm_inv (no SPD clamp needed, it is PSD);
+//   * kinematic pins: a pinned vertex is placed on its target at the start of
+//     the step and its degrees of freedom are removed from the solve;
+//   * self contact from the intended broad phase (boxes inflated by the
+//     barrier activation distance), vertex-triangle AND edge-edge barriers,
+//     gaps, normals and weights refreshed at every Newton iteration (edge-edge
+//     weights are the closest-point parameters [1-s, s, -(1-t), -t]);
+//   * line search: a conservative time of impact along the extended direction
+//     (conservative advancement with exact distances, FP64) over every pair
+//     whose swept boxes overlap, plus the exact linear time of impact of every
+//     active wall; the step taken is x += toi * d.
+// ======================================================================
+
+// Correct BVH query (leaves keep up to 4 primitives): the same candidate set
+// as the brute-force INTENDED broad phase in O(n log n).
+template <class R> struct QBVH {
+  struct Node { AABB<R> box; int left = -1, right = -1, start = 0, end = 0; };
+  std::vector<Node> nodes; std::vector<int> idx;
+  int build(const std::vector<AABB<R>>& pb, int s, int e) {
+    int ni = int(nodes.size()); nodes.emplace_back();
+    AABB<R> box; for (int i = s; i < e; ++i) box.expand(pb[size_t(idx[size_t(i)])]);
+    nodes[size_t(ni)].box = box; nodes[size_t(ni)].start = s; nodes[size_t(ni)].end = e;
+    if (e - s <= 4) return ni;
+    int ax = box.longest_axis();
+    std::sort(idx.begin() + s, idx.begin() + e, [&](int a, int c) { return pb[size_t(a)].center()[ax] < pb[size_t(c)].center()[ax]; });
+    int mid = s + (e - s) / 2;
+    int l = build(pb, s, mid), r = build(pb, mid, e);
+    nodes[size_t(ni)].left = l; nodes[size_t(ni)].right = r;
+    return ni;
+  }
+  void init(const std::vector<AABB<R>>& pb) {
+    nodes.clear(); idx.resize(pb.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = int(i);
+    if (!pb.empty()) build(pb, 0, int(pb.size()));
+  }
+  template <class F> void query(const AABB<R>& q, const std::vector<AABB<R>>& pb, F&& visit) const {
+    if (nodes.empty()) return;
+    std::vector<int> st = {0};
+    while (!st.empty()) {
+      int ni = st.back(); st.pop_back();
+      const Node& nd = nodes[size_t(ni)];
+      if (!q.overlaps(nd.box)) continue;
+      if (nd.left < 0) { for (int i = nd.start; i < nd.end; ++i) if (q.overlaps(pb[size_t(idx[size_t(i)])])) visit(idx[size_t(i)]); }
+      else { st.push_back(nd.right); st.push_back(nd.left); }
+    }
+  }
+};
+
+// Candidate pairs with the reference predicate over boxes spanning positions
+// x0 and x1 (x1 == nullptr: boxes at x0), inflated by pad; sorted.
+template <class R> void candidates(const Mesh<R>& m, const std::vector<V3<R>>& x0, const std::vector<V3<R>>* x1, R pad,
+                                   std::vector<std::pair<int, int>>& vt, std::vector<std::pair<int, int>>& ee) {
+  vt.clear(); ee.clear();
+  auto tb = triangle_boxes(m, x0);
+  auto eb = edge_boxes(m, x0);
+  if (x1) {
+    auto tb1 = triangle_boxes(m, *x1); auto eb1 = edge_boxes(m, *x1);
+    for (size_t i = 0; i < tb.size(); ++i) tb[i].expand(tb1[i]);
+    for (size_t i = 0; i < eb.size(); ++i) eb[i].expand(eb1[i]);
+  }
+  for (auto& b : tb) inflate(b, pad);
+  for (auto& b : eb) inflate(b, pad);
+  QBVH<R> tq, eq; tq.init(tb); eq.init(eb);
+  for (size_t v = 0; v < x0.size(); ++v) {
+    AABB<R> pbx = point_box(x0[v]);
+    if (x1) pbx.expand(point_box((*x1)[v]));
+    inflate(pbx, pad);
+    tq.query(pbx, tb, [&](int t) {
+      const auto& tri = m.triangles[size_t(t)];
+      if (tri.v[0] == int(v) || tri.v[1] == int(v) || tri.v[2] == int(v)) return;
+      vt.push_back({int(v), t});
+    });
+  }
+  for (size_t a = 0; a < eb.size(); ++a) {
+    eq.query(eb[a], eb, [&](int b) {
+      if (int(a) >= b) return;
+      const Edge &e1 = m.edges[a], &e2 = m.edges[size_t(b)];
+      if (e1.v[0] == e2.v[0] || e1.v[0] == e2.v[1] || e1.v[1] == e2.v[0] || e1.v[1] == e2.v[1]) return;
+      ee.push_back({int(a), b});
+    });
+  }
+  std::sort(vt.begin(), vt.end()); std::sort(ee.begin(), ee.end());
+}
+
+// Contacts inside the activation distance at positions x (refreshed every Newton iteration).
+template <class R> std::vector<ContactPair<R>> detect_corrected(const Mesh<R>& m, const std::vector<V3<R>>& x, const std::vector<RigidBody<R>>* rigids, R gap_max) {
+  std::vector<ContactPair<R>> out;
+  std::vector<std::pair<int, int>> vt, ee;
+  candidates(m, x, (const std::vector<V3<R>>*)nullptr, gap_max, vt, ee);
+  for (auto& pr : vt) {
+    ContactPair<R> c; c.type = ContactType::POINT_TRIANGLE; c.idx0 = pr.first;
+    const auto& t = m.triangles[size_t(pr.second)]; c.idx1 = t.v[0]; c.idx2 = t.v[1]; c.idx3 = t.v[2];
+    const auto &p = x[size_t(c.idx0)], &a = x[size_t(c.idx1)], &b = x[size_t(c.idx2)], &cc = x[size_t(c.idx3)];
+    narrow_pt(p, a, b, cc, c.gap, c.normal, c.witness_p, c.witness_q);
+    if (!(c.gap < gap_max)) continue;
+    V3<R> bc = triangle_barycentric(c.witness_q, a, b, cc); c.barycentric = bc;
+    c.weights = {R(1), -bc[0], -bc[1], -bc[2]}; c.vertex_count = 4; out.push_back(c);
+  }
+  for (auto& pr : ee) {
+    ContactPair<R> c; c.type = ContactType::EDGE_EDGE;
+    const Edge &e1 = m.edges[size_t(pr.first)], &e2 = m.edges[size_t(pr.second)];
+    c.idx0 = e1.v[0]; c.idx1 = e1.v[1]; c.idx2 = e2.v[0]; c.idx3 = e2.v[1];
+    R sp, tp;
+    narrow_ee(x[size_t(c.idx0)], x[size_t(c.idx1)], x[size_t(c.idx2)], x[size_t(c.idx3)], c.gap, c.normal, c.witness_p, c.witness_q, &sp, &tp);
+    if (!(c.gap < gap_max)) continue;
+    c.vertex_count = 4; c.weights = {R(1) - sp, sp, -(R(1) - tp), -tp}; out.push_back(c);
+  }
+  if (rigids) {
+    for (size_t rb = 0; rb < rigids->size(); ++rb) {
+      const auto& body = (*rigids)[rb];
+      auto wv = body.world_vertices();
+      for (size_t v = 0; v < x.size(); ++v)
+        for (const auto& t : body.tris) {
+          ContactPair<R> c; c.type = ContactType::RIGID_POINT_TRIANGLE; c.idx0 = Index(v);
+          c.idx1 = t.v[0]; c.idx2 = t.v[1]; c.idx3 = t.v[2]; c.rigid_body_index = int(rb);
+          narrow_pt(x[v], wv[size_t(t.v[0])], wv[size_t(t.v[1])], wv[size_t(t.v[2])], c.gap, c.normal, c.witness_p, c.witness_q);
+          if (c.gap < gap_max) { c.vertex_count = 1; c.weights[0] = R(1); out.push_back(c); }
+        }
+    }
+  }
+  return out;
+}
+
+// Constant elastic Hessian of the CORRECTED energy: per face the 3x3 vertex
+// blocks c_ab I3 with c_ab = 2k (G G^T)_ab.
+template <class R> void corrected_face_coeffs(const Mesh<R>& mesh, size_t f, R c[3][3]) {
+  R mu = R(double(mesh.material.youngs_modulus) / (2.0 * (1.0 + double(mesh.material.poisson_ratio))));
+  R k = mesh.rest_areas[f] * mesh.material.thickness * mu;
+  const M2<R>& D = mesh.Dm_inv[f];
+  R G[3][2] = {{-(D.a + D.c), -(D.b + D.d)}, {D.a, D.b}, {D.c, D.d}};
+  for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) c[a][b] = R(2) * k * (G[a][0] * G[b][0] + G[a][1] * G[b][1]);
+}
+template <class R> void corrected_elastic_triplets(const Mesh<R>& mesh, std::vector<Triplet<R>>& out) {
+  for (size_t f = 0; f < mesh.triangles.size(); ++f) {
+    const auto& t = mesh.triangles[f];
+    R c[3][3]; corrected_face_coeffs(mesh, f, c);
+    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) for (int k = 0; k < 3; ++k) out.push_back({t.v[a] * 3 + k, t.v[b] * 3 + k, c[a][b]});
+  }
+}
+template <class R> void elastic_gradient_at(const Mesh<R>& mesh, const std::vector<V3<R>>& X, std::vector<R>& g) {
+  Mesh<R> tmp; tmp.vertices = X; tmp.triangles = mesh.triangles; tmp.Dm_inv = mesh.Dm_inv; tmp.rest_areas = mesh.rest_areas; tmp.material = mesh.material;
+  elastic_gradient(tmp, g);
+}
+
+// Conservative time of impact of one pair along the motion x -> x + e: advance
+// by (d - eta) / l until the distance falls to eta = 0.1 d0 (l bounds how fast
+// the distance can shrink per unit time). Returns t in [0, 1].
+template <class R> R advance_toi(const std::function<R(R)>& dist, R l) {
+  if (!(l > R(0))) return R(1);
+  R d0 = dist(R(0));
+  if (!(d0 > R(0))) return R(0);
+  R eta = R(0.1) * d0, t = 0;
+  for (int it = 0; it < 200; ++it) {
+    R d = it == 0 ? d0 : dist(t);
+    if (d <= eta) return t;
+    t += (d - eta) / l;
+    if (t >= R(1)) return R(1);
+  }
+  return t;
+}
+
+template <class R> class CorrectedIntegrator {
+ public:
+  static void step(Mesh<R>& mesh, State<R>& st, Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>* stats = nullptr) {
+    StepStats<R> local; StepStats<R>& S = stats ? *stats : local;
+    S = StepStats<R>();
+    const size_t n = st.positions.size(); const R dt = p.dt;
+    std::vector<V3<R>> x_old = st.positions, x_target(n);
+    std::vector<char> fixed(n, 0);
+    for (const auto& pin : C.pins) if (pin.active) { st.positions[size_t(pin.vertex_idx)] = pin.target_position; fixed[size_t(pin.vertex_idx)] = 1; }
+    for (size_t i = 0; i < n; ++i) x_target[i] = x_old[i] + st.velocities[i] * dt;
+    R beta = 0; int bi = 0;
+    while (beta < p.beta_max && bi < 20) {
+      R alpha = inner_newton(mesh, st, x_target, fixed, C, p, rigids, S);
+      beta = R(double(beta) + (1.0 - double(beta)) * double(alpha));
+      ++bi;
+      if (alpha < R(1e-6)) { S.line_search_fail++; break; }
+    }
+    if (beta > R(1e-6)) inner_newton(mesh, st, x_target, fixed, C, p, rigids, S);
+    S.beta = beta;
+    if (beta > R(1e-6)) {
+      R bdt = beta * dt;
+      for (size_t i = 0; i < n; ++i) st.velocities[i] = (st.positions[i] - x_old[i]) / bdt;
+      if (p.velocity_damping > R(0)) { R sc = R(1) - std::clamp(p.velocity_damping, R(0), R(1)); for (auto& v : st.velocities) v = v * sc; }
+    }
+  }
+
+  static Csr<R> base_elastic(const Mesh<R>& mesh) { std::vector<Triplet<R>> el; corrected_elastic_triplets(mesh, el); return Csr<R>::from_triplets(Index(3 * mesh.vertices.size()), el); }
+
+  static void gradient(const Mesh<R>& mesh, const State<R>& st, const std::vector<V3<R>>& x_target, const std::vector<char>& fixed,
+                       const std::vector<ContactPair<R>>& contacts, Constraints<R>& C, const SimParams<R>& p, const Csr<R>& H_el, std::vector<R>& g) {
+    const size_t n = st.positions.size(); const R dt = p.dt;
+    g.assign(3 * n, R(0));
+    for (size_t i = 0; i < n; ++i) { R mf = st.masses[i] / (dt * dt); for (int j = 0; j < 3; ++j) g[3 * i + size_t(j)] += mf * (st.positions[i][j] - x_target[i][j]); }
+    std::vector<R> ge; elastic_gradient_at(mesh, st.positions, ge);
+    for (size_t i = 0; i < g.size(); ++i) g[i] += ge[i];
+    if (p.enable_strain_limiting) { strain_rebuild(mesh, st, p, H_el, C, Lookup::INDEXED); strain_gradient(mesh, st, C, p, g); }
+    else C.strain_limits.clear();
+    for (const auto& c : contacts) {
+      R kb = contact_stiffness(c, st.masses, dt, H_el, Lookup::INDEXED);
+      if (!in_domain(c.gap, p.contact_gap_max)) continue;
+      V3<R> nrm = normalize_or_default(c.normal, p.contact_normal_epsilon);
+      R dV = barrier_gradient(c.gap, p.contact_gap_max, kb);
+      Index ids[4] = {c.idx0, c.idx1, c.idx2, c.idx3};
+      int cnt = std::max(c.vertex_count, 1);
+      for (int i = 0; i < cnt; ++i) {
+        if (ids[i] < 0 || c.weights[size_t(i)] == R(0)) continue;
+        V3<R> add = nrm * (dV * c.weights[size_t(i)]);
+        for (int k = 0; k < 3; ++k) g[size_t(ids[i]) * 3 + size_t(k)] += add[k];
+      }
+    }
+    Csr<R> H_tot = H_el;  // walls take k_bar from the elastic + inertia diagonal block
+    for (const auto& w : C.walls) {
+      if (!w.active) continue;
+      V3<R> nrm = normalize_or_default(w.normal, p.contact_normal_epsilon);
+      for (size_t vi = 0; vi < n; ++vi) {
+        M3<R> Hb = extract_hessian_block(H_el, Index(vi), Lookup::INDEXED);
+        R md = st.masses[vi] / (dt * dt);
+        Hb(0, 0) += md; Hb(1, 1) += md; Hb(2, 2) += md;
+        R kb = wall_stiffness(st.masses[vi], p.wall_gap, w.normal, Hb, p.min_gap);
+        R gap = nrm.dot(st.positions[vi]) - w.offset;
+        if (!in_domain(gap, p.contact_gap_max)) continue;
+        R dV = barrier_gradient(gap, p.contact_gap_max, kb);
+        for (int k = 0; k < 3; ++k) g[vi * 3 + size_t(k)] += dV * nrm[k];
+      }
+    }
+    for (size_t i = 0; i < n; ++i) if (fixed[i]) for (int k = 0; k < 3; ++k) g[3 * i + size_t(k)] = R(0);
+  }
+
+  static Csr<R> assemble(const Mesh<R>& mesh, const State<R>& st, const std::vector<char>& fixed, const std::vector<ContactPair<R>>& contacts,
+                         Constraints<R>& C, const SimParams<R>& p, const Csr<R>& H_el) {
+    const Index n = Index(st.positions.size()); const R dt = p.dt;
+    std::vector<Triplet<R>> tr;
+    R dinv = R(1) / (dt * dt);
+    for (Index row = 0; row < 3 * n; ++row) { R v = st.masses[size_t(row / 3)] * dinv; if (v != R(0)) tr.push_back({row, row, v}); }
+    corrected_elastic_triplets(mesh, tr);
+    if (p.enable_strain_limiting) strain_hessian(mesh, st, C, p, tr);
+    for (const auto& c : contacts) {
+      R kb = contact_stiffness(c, st.masses, dt, H_el, Lookup::INDEXED);
+      if (!in_domain(c.gap, p.contact_gap_max)) continue;
+      V3<R> nrm = normalize_or_default(c.normal, p.contact_normal_epsilon);
+      R d2V = barrier_hessian(c.gap, p.contact_gap_max, kb);
+      Index ids[4] = {c.idx0, c.idx1, c.idx2, c.idx3};
+      int cnt = std::max(c.vertex_count, 1);
+      for (int i = 0; i < cnt; ++i) for (int j = 0; j < cnt; ++j) {
+        if (ids[i] < 0 || ids[j] < 0 || c.weights[size_t(i)] == R(0) || c.weights[size_t(j)] == R(0)) continue;
+        V3<R> gi = nrm * c.weights[size_t(i)], gj = nrm * c.weights[size_t(j)];
+        for (int r = 0; r < 3; ++r) for (int q = 0; q < 3; ++q) {
+          R v = d2V * (gi[r] * gj[q]);
+          if (std::fabs(v) < p.barrier_tolerance) continue;
+          tr.push_back({ids[i] * 3 + r, ids[j] * 3 + q, v});
+        }
+      }
+    }
+    for (const auto& w : C.walls) {
+      if (!w.active) continue;
+      V3<R> nrm = normalize_or_default(w.normal, p.contact_normal_epsilon);
+      for (Index vi = 0; vi < n; ++vi) {
+        M3<R> Hb = extract_hessian_block(H_el, vi, Lookup::INDEXED);
+        R md = st.masses[size_t(vi)] / (dt * dt);
+        Hb(0, 0) += md; Hb(1, 1) += md; Hb(2, 2) += md;
+        R kb = wall_stiffness(st.masses[size_t(vi)], p.wall_gap, w.normal, Hb, p.min_gap);
+        R gap = nrm.dot(st.positions[size_t(vi)]) - w.offset;
+        if (!in_domain(gap, p.contact_gap_max)) continue;
+        R d2V = barrier_hessian(gap, p.contact_gap_max, kb);
+        for (int r = 0; r < 3; ++r) for (int q = 0; q < 3; ++q) { R v = d2V * nrm[r] * nrm[q]; if (std::fabs(v) >= p.barrier_tolerance) tr.push_back({vi * 3 + r, vi * 3 + q, v}); }
+      }
+    }
+    // kinematic pins: drop every entry touching a fixed vertex, unit diagonal
+    std::vector<Triplet<R>> kept; kept.reserve(tr.size());
+    for (auto& t : tr) if (!fixed[size_t(t.row / 3)] && !fixed[size_t(t.col / 3)]) kept.push_back(t);
+    for (Index i = 0; i < n; ++i) if (fixed[size_t(i)]) for (int k = 0; k < 3; ++k) kept.push_back({3 * i + k, 3 * i + k, R(1)});
+    return Csr<R>::from_triplets(3 * n, kept);
+  }
+
+  // Conservative time of impact along ext (line search of the CORRECTED step).
+  static R toi(const Mesh<R>& mesh, const std::vector<V3<R>>& x, const std::vector<V3<R>>& ext, const std::vector<char>& fixed,
+               const Constraints<R>& C, const std::vector<RigidBody<R>>* rigids) {
+    const size_t n = x.size();
+    R t = 1;
+    for (const auto& w : C.walls) {
+      if (!w.active) continue;
+      V3<R> nn = w.normal.normalized();
+      for (size_t i = 0; i < n; ++i) {
+        if (fixed[i]) continue;
+        R dn = nn.dot(ext[i]);
+        if (!(dn < R(0))) continue;
+        R gap = nn.dot(x[i]) - w.offset;
+        t = std::min(t, std::max(gap, R(0)) / (-dn));
+      }
+    }
+    std::vector<V3<R>> x1(n);
+    for (size_t i = 0; i < n; ++i) x1[i] = x[i] + ext[i];
+    std::vector<std::pair<int, int>> vt, ee;
+    candidates(mesh, x, &x1, R(0), vt, ee);
+    auto L = [&](int i) { return ext[size_t(i)].norm(); };
+    for (auto& pr : vt) {
+      const auto& tri = mesh.triangles[size_t(pr.second)];
+      int v = pr.first, a = tri.v[0], b = tri.v[1], c = tri.v[2];
+      R l = L(v) + std::max(L(a), std::max(L(b), L(c)));
+      auto dist = [&](R s) { R d; V3<R> nm, wp, wq; narrow_pt(x[size_t(v)] + ext[size_t(v)] * s, x[size_t(a)] + ext[size_t(a)] * s,
+                                                              x[size_t(b)] + ext[size_t(b)] * s, x[size_t(c)] + ext[size_t(c)] * s, d, nm, wp, wq); return d; };
+      t = std::min(t, advance_toi<R>(dist, l));
+    }
+    for (auto& pr : ee) {
+      const Edge &e1 = mesh.edges[size_t(pr.first)], &e2 = mesh.edges[size_t(pr.second)];
+      int a = e1.v[0], b = e1.v[1], c = e2.v[0], d = e2.v[1];
+      R l = std::max(L(a), L(b)) + std::max(L(c), L(d));
+      auto dist = [&](R s) { R dd; V3<R> nm, wp, wq; narrow_ee(x[size_t(a)] + ext[size_t(a)] * s, x[size_t(b)] + ext[size_t(b)] * s,
+                                                               x[size_t(c)] + ext[size_t(c)] * s, x[size_t(d)] + ext[size_t(d)] * s, dd, nm, wp, wq); return dd; };
+      t = std::min(t, advance_toi<R>(dist, l));
+    }
+    if (rigids) {
+      for (const auto& body : *rigids) {
+        auto wv = body.world_vertices();
+        for (size_t v = 0; v < n; ++v) {
+          R l = L(int(v));
+          if (!(l > R(0))) continue;
+          for (const auto& tr : body.tris) {
+            AABB<R> tb; tb.expand(wv[size_t(tr.v[0])]); tb.expand(wv[size_t(tr.v[1])]); tb.expand(wv[size_t(tr.v[2])]);
+            AABB<R> pb = point_box(x[v]); pb.expand(point_box(x1[v]));
+            if (!pb.overlaps(tb)) continue;
+            auto dist = [&](R s) { R d; V3<R> nm, wp, wq; narrow_pt(x[v] + ext[v] * s, wv[size_t(tr.v[0])], wv[size_t(tr.v[1])], wv[size_t(tr.v[2])], d, nm, wp, wq); return d; };
+            t = std::min(t, advance_toi<R>(dist, l));
+          }
+        }
+      }
+    }
+    return t;
+  }
+
+  static R inner_newton(const Mesh<R>& mesh, State<R>& st, const std::vector<V3<R>>& x_target, const std::vector<char>& fixed,
+                        Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>& S) {
+    const size_t n = st.positions.size();
+    Csr<R> H_el = base_elastic(mesh);
+    for (int it = 0; it < p.max_newton_steps; ++it) {
+      auto contacts = detect_corrected(mesh, st.positions, rigids, p.contact_gap_max);
+      S.contacts = std::max(S.contacts, int(contacts.size()));
+      std::vector<R> g;
+      gradient(mesh, st, x_target, fixed, contacts, C, p, H_el, g);
+      R gn = 0; for (R e : g) gn = std::max(gn, std::fabs(e));
+      if (gn < p.pcg_tol) return R(1);
+      S.newton_iters++;
+      Csr<R> H = assemble(mesh, st, fixed, contacts, C, p, H_el);
+      std::vector<R> d(3 * n, R(0)), ng(3 * n);
+      for (size_t i = 0; i < 3 * n; ++i) ng[i] = -g[i];
+      auto pr = pcg_solve(H, ng, d, p.pcg_tol, p.pcg_max_iters);
+      S.pcg_iters += pr.iters; S.pcg_per_newton.push_back(pr.iters);
+      if (!pr.converged) S.pcg_not_converged++;
+      std::vector<V3<R>> ext(n);
+      for (size_t i = 0; i < n; ++i) ext[i] = fixed[i] ? V3<R>() : V3<R>(d[3 * i], d[3 * i + 1], d[3 * i + 2]) * R(1.25);
+      R alpha = toi(mesh, st.positions, ext, fixed, C, rigids);
+      S.alphas.push_back(alpha);
+      if (alpha < R(1e-8)) return R(0);
+      for (size_t i = 0; i < n; ++i) if (!fixed[i]) st.positions[i] = st.positions[i] + V3<R>(d[3 * i], d[3 * i + 1], d[3 * i + 2]) * alpha;
+      if (alpha > R(0.99)) return R(1);
+    }
+    return R(0.5);
   }
 };
 

@@ -269,9 +269,9 @@ template <class R> void bind(py::module_& m) {
     std::vector<R> bb = vec_of<R>(b), x(bb.size(), R(0));
     auto res = pcg_solve(A, bb, x, tol, max_iters);
     return py::make_tuple(py::array_t<R>(py::ssize_t(x.size()), x.data()), res.converged, res.iters, res.rel_res); });
-  m.def("broad_phase", [](const MeshT& me, Arr<R> x, const std::string& mode) {
-    std::vector<std::pair<int, int>> vt, ee; broad_phase(me, to_v3<R>(x), to_broad(mode), vt, ee);
-    return py::make_tuple(vt, ee); });
+  m.def("broad_phase", [](const MeshT& me, Arr<R> x, const std::string& mode, R pad) {
+    std::vector<std::pair<int, int>> vt, ee; broad_phase(me, to_v3<R>(x), to_broad(mode), vt, ee, pad);
+    return py::make_tuple(vt, ee); }, py::arg("mesh"), py::arg("positions"), py::arg("mode"), py::arg("pad") = R(0));
   m.def("bvh_node_count", [](const MeshT& me, Arr<R> x) { return bvh_build(triangle_boxes(me, to_v3<R>(x))).nodes.size(); });
 }
 

@@ -90,6 +90,9 @@ def gpu_system(abi, sc, x, v, params=None, rigids=None):
     g = S.last_gradient()
     rowptr, cols, vals, rhs, _ = S.last_system()
     H = bsr_to_dense(rowptr, cols, vals, S.V)
+    xr, xc, xv = S.last_contact_blocks()
+    for r, c, blk in zip(xr, xc, xv):
+        H[3 * r:3 * r + 3, 3 * c:3 * c + 3] += blk
     S.close()
     return g, H, rhs
 
@@ -168,7 +171,9 @@ def test_system_rigid_contacts_with_friction(oracle, abi):
 def single_triangle_scene():
     """One triangle plus free vertices: the only mesh size for which the
     reference's BVH yields vertex-triangle candidates (collision.cpp:81-86)."""
-    v = np.array([[0.0, 0.0, 0.0], [0.2, 0.0, 0.0], [0.0, 0.2, 0.0], [0.05, 0.05, 0.0004], [0.06, 0.05, 0.0008],
+    # the reference's point box is +-0.1 mm (collision.cpp:208), so the hovering
+    # vertices sit within 0.1 mm of the triangle's plane to become candidates
+    v = np.array([[0.0, 0.0, 0.0], [0.2, 0.0, 0.0], [0.0, 0.2, 0.0], [0.05, 0.05, 0.00005], [0.06, 0.05, 0.00009],
                   [0.5, 0.5, 0.5]])
     t = np.array([[0, 1, 2]], dtype=np.int32)
     mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
