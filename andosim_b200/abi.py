@@ -55,6 +55,24 @@ class Pin(C.Structure):
     _fields_ = [("vertex", C.c_int32), ("active", C.c_int32), ("target", C.c_double * 3)]
 
 
+# numpy twin of Pin (same 32-byte layout), so pin sets are built without a Python loop
+PIN_DTYPE = np.dtype([("vertex", "<i4"), ("active", "<i4"), ("target", "<f8", (3,))])
+assert PIN_DTYPE.itemsize == C.sizeof(Pin)
+
+
+def pin_array(pins) -> np.ndarray:
+    """Pins as a PIN_DTYPE array; accepts (vertex, target) pairs or an existing array."""
+    if isinstance(pins, np.ndarray) and pins.dtype == PIN_DTYPE:
+        return np.ascontiguousarray(pins)
+    pins = list(pins)
+    a = np.zeros(len(pins), PIN_DTYPE)
+    if pins:
+        a["vertex"] = [int(i) for i, _ in pins]
+        a["active"] = 1
+        a["target"] = np.asarray([t for _, t in pins], dtype=np.float64).reshape(len(pins), 3)
+    return a
+
+
 class Wall(C.Structure):
     _fields_ = [("normal", C.c_double * 3), ("offset", C.c_double), ("gap", C.c_double), ("active", C.c_int32), ("pad_", C.c_int32)]
 
@@ -91,7 +109,7 @@ class StepStats(C.Structure):
     _fields_ = [
         ("newton_iters", C.c_int32), ("pcg_iters", C.c_int32), ("pcg_max_per_newton", C.c_int32),
         ("pcg_not_converged", C.c_int32), ("line_search_fail", C.c_int32), ("contacts", C.c_int32),
-        ("strain_active", C.c_int32), ("status", C.c_int32), ("precond_fallbacks", C.c_int32), ("pad_", C.c_int32),
+        ("strain_active", C.c_int32), ("status", C.c_int32), ("precond_fallbacks", C.c_int32), ("graph_launched", C.c_int32),
         ("beta", C.c_double), ("last_alpha", C.c_double), ("device_ms", C.c_double),
     ]
 
@@ -260,11 +278,7 @@ class Scene:
 
     @staticmethod
     def _constraints(pins, walls):
-        pa = (Pin * max(1, len(pins)))()
-        for k, (i, t) in enumerate(pins):
-            pa[k].vertex = int(i); pa[k].active = 1
-            for q in range(3):
-                pa[k].target[q] = float(t[q])
+        pa = pin_array(pins)
         wa = (Wall * max(1, len(walls)))()
         for k, (n, off, gap) in enumerate(walls):
             n = np.asarray(n, dtype=np.float64)
@@ -276,21 +290,23 @@ class Scene:
         return pa, wa
 
     def step(self, params: Params, pins: Sequence = (), walls: Sequence = (), rigids: Optional[List[Rigid]] = None) -> dict:
-        pa, wa = self._constraints(list(pins), list(walls))
+        pa, wa = self._constraints(pins, list(walls))
         st = StepStats()
         nr = len(rigids) if rigids else 0
         ra = (Rigid * max(1, nr))(*(rigids or []))
-        _check(lib().ando_step(self.ctx, C.byref(params), pa, len(pins), wa, len(walls), ra, nr, C.byref(st)), "ando_step")
+        _check(lib().ando_step(self.ctx, C.byref(params), pa.ctypes.data_as(C.POINTER(Pin)), len(pa), wa, len(walls), ra, nr,
+                               C.byref(st)), "ando_step")
         if rigids:
             for k in range(nr):
                 C.pointer(rigids[k])[0] = ra[k]
         return st.as_dict()
 
     def eval_system(self, params: Params, pins: Sequence = (), walls: Sequence = (), rigids: Optional[List[Rigid]] = None):
-        pa, wa = self._constraints(list(pins), list(walls))
+        pa, wa = self._constraints(pins, list(walls))
         nr = len(rigids) if rigids else 0
         ra = (Rigid * max(1, nr))(*(rigids or []))
-        _check(lib().ando_eval_system(self.ctx, C.byref(params), pa, len(pins), wa, len(walls), ra, nr), "ando_eval_system")
+        _check(lib().ando_eval_system(self.ctx, C.byref(params), pa.ctypes.data_as(C.POINTER(Pin)), len(pa), wa, len(walls), ra, nr),
+               "ando_eval_system")
 
     def last_gradient(self) -> np.ndarray:
         g = np.empty(3 * self.V)

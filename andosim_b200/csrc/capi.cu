@@ -81,6 +81,22 @@ struct ando_ctx_s {
   int num_pins = 0, num_walls = 0;
   WallDev first_wall_host{};
 
+  // whole-frame CUDA graph (REFERENCE semantics without contact detection)
+  cudaStream_t cap2 = nullptr, cap3 = nullptr;
+  DevBuf<StepCtl> sctl;
+  StepCtl* sctl_host = nullptr;
+  cudaGraphExec_t frame_exec = nullptr;
+  std::vector<unsigned char> frame_key;
+  bool use_graphs = true;
+  long long mesh_generation = 0;
+
+  // CORRECTED semantics
+  DevBuf<unsigned char> fixed;
+  DevBuf<double> g_el_x, x1, ext;
+  DevBuf<unsigned long long> toi, emax_cap;
+  double max_move = 1e300;   // 4 x mean rest edge length: largest displacement per Newton iteration
+  DevBuf<int2> pairs_ee;
+
   // broad phase
   DevBuf<int> edges;
   int E = 0;
@@ -97,6 +113,10 @@ struct ando_ctx_s {
 
   ~ando_ctx_s() {
     destroy_events();
+    if (frame_exec) cudaGraphExecDestroy(frame_exec);
+    if (sctl_host) cudaFreeHost(sctl_host);
+    if (cap2) cudaStreamDestroy(cap2);
+    if (cap3) cudaStreamDestroy(cap3);
     for (auto* b : body_local) delete b;
     for (auto* b : body_world) delete b;
     for (auto* b : body_tris) delete b;
@@ -193,11 +213,11 @@ StepParams make_step_params(const ando_params& p, int num_walls, int first_wall)
 // Contact detection at the current positions into ctx->contacts (order of
 // Collision::detect_all_collisions: vertex-triangle by vertex, then rigid
 // contacts by body, vertex and triangle).
-int detect(ando_ctx c, int nb, int phase = ANDO_PHASE_SETUP) {
+int detect(ando_ctx c, int nb, int phase = ANDO_PHASE_SETUP, double thresh = 0.01, bool literal_allowed = true, int dst_offset = 0) {
   Phase ph(c, phase);
   MeshDev m = c->mesh_dev();
   long long units = (long long)c->V * (1 + nb);
-  int literal_pt = (c->T == 1) ? 1 : 0;
+  int literal_pt = (literal_allowed && c->T == 1) ? 1 : 0;
   if (!literal_pt && nb == 0) {
     // The reference's BVH yields no self-contact candidate for >= 2 triangles
     // (collision.cpp:81-86) and there is no rigid body: nothing to detect.
@@ -207,7 +227,7 @@ int detect(ando_ctx c, int nb, int phase = ANDO_PHASE_SETUP) {
   }
   CK(c->det_counts.reserve(units + 1));
   CK(c->det_offsets.reserve(units + 1));
-  launch_detect_count(m, c->x.p, c->bodies_dev.p, nb, literal_pt, c->det_counts.p, c->stream);
+  launch_detect_count(m, c->x.p, c->bodies_dev.p, nb, literal_pt, thresh, c->det_counts.p, c->stream);
   ph.launched();
   CK(cudaMemsetAsync(c->det_counts.p + units, 0, sizeof(int), c->stream));
   size_t bytes = 0;
@@ -218,8 +238,9 @@ int detect(ando_ctx c, int nb, int phase = ANDO_PHASE_SETUP) {
   CK(cudaMemcpyAsync(&total, c->det_offsets.p + units, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->ncontacts = total;
-  CK(c->contacts.reserve(total));
-  if (total) { launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, literal_pt, c->det_offsets.p, c->contacts.p, c->stream); ph.launched(); }
+  if (dst_offset < 0) return ANDO_OK;  // count only: the caller sizes the buffer and writes later
+  if (dst_offset == 0) CK(c->contacts.reserve(total));
+  if (total) { launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, literal_pt, thresh, c->det_offsets.p, c->contacts.p + dst_offset, c->stream); ph.launched(); }
   c->n_pe = literal_pt ? total : 0;  // only the literal vertex-triangle case produces PT contacts
   CK(cudaGetLastError());
   return ANDO_OK;
@@ -228,7 +249,7 @@ int detect(ando_ctx c, int nb, int phase = ANDO_PHASE_SETUP) {
 // Per-step contact constants: k_bar and barrier derivatives at the frozen
 // gap, the per-vertex constant gradient/diagonal, and the extra off-diagonal
 // block segment sorted by row.
-int prepare_contacts(ando_ctx c, const StepParams& sp) {
+int prepare_contacts(ando_ctx c, const StepParams& sp, const double* g_base, const unsigned char* fixed) {
   Phase ph(c, ANDO_PHASE_SETUP);
   MeshDev m = c->mesh_dev();
   int nc = c->ncontacts, V = c->V;
@@ -245,12 +266,12 @@ int prepare_contacts(ando_ctx c, const StepParams& sp) {
     CK(cudaMemsetAsync(c->ebegin.p, 0, sizeof(int) * V, c->stream));
     CK(cudaMemsetAsync(c->eend.p, 0, sizeof(int) * V, c->stream));
     c->nx = 0;
-    launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, c->g_const.p, c->diag_const.p, c->stream);
+    launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, g_base, c->g_const.p, c->diag_const.p, c->stream);
     ph.launched();
     CK(cudaGetLastError());
     return ANDO_OK;
   }
-  launch_contact_entries(c->contacts.p, nc, V, sp.enable_friction && sp.friction_mu > 0.0, c->ekeys.p, c->ents.p, c->stream);
+  launch_contact_entries(c->contacts.p, nc, V, sp.semantics == 0 && sp.enable_friction && sp.friction_mu > 0.0, c->ekeys.p, c->ents.p, c->stream);
   ph.launched();
   int bits = 1;
   while ((1ll << bits) <= (long long)V) ++bits;
@@ -259,7 +280,7 @@ int prepare_contacts(ando_ctx c, const StepParams& sp) {
   CK(c->cub_reserve(bytes));
   CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, c->ekeys.p, c->ekeys_sorted.p, c->ents.p, c->ents_sorted.p, ne, 0, bits, c->stream));
   launch_vertex_ranges(c->ekeys_sorted.p, ne, V, c->ebegin.p, c->eend.p, c->stream);
-  launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, c->g_const.p, c->diag_const.p, c->stream);
+  launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, g_base, c->g_const.p, c->diag_const.p, c->stream);
   // extra segment: off-diagonal barrier blocks, kept in row order
   launch_extra_flags(c->ents_sorted.p, c->ekeys_sorted.p, ne, c->xflags.p, c->stream);
   ph.launched(3);
@@ -272,7 +293,7 @@ int prepare_contacts(ando_ctx c, const StepParams& sp) {
   CK(cudaMemcpyAsync(&nx, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->nx = nx;
-  if (nx) { launch_extra_values(c->contacts.p, c->xent.p, c->xcols.p, nx, sp, c->xval.p, c->stream); ph.launched(); }
+  if (nx) { launch_extra_values(c->contacts.p, c->xent.p, c->xkeys.p, fixed, c->xcols.p, nx, sp, c->xval.p, c->stream); ph.launched(); }
   launch_vertex_ranges(c->xkeys.p, nx, V, c->xbegin.p, c->xend.p, c->stream);
   ph.launched();
   CK(cudaGetLastError());
@@ -337,13 +358,13 @@ int inner_newton(ando_ctx c, const ando_params& p, const StepParams& sp, ando_st
       if (!sp.enable_strain) { launch_ctrl_reset(c->ctrl.p, c->stream); ph.launched(); }
       launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
                       c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
-                      c->ebegin.p, c->eend.p, sp, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, c->stream);
+                      c->ebegin.p, c->eend.p, sp, nullptr, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, c->stream);
       launch_check(c->ctrl.p, p.pcg_tol, c->stream);
       ph.launched(2);
     }
     {
       Phase ph(c, ANDO_PHASE_ASSEMBLE);
-      launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->val.p, c->precond.p, c->ctrl.p, c->stream);
+      launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, nullptr, c->val.p, c->precond.p, c->ctrl.p, c->stream);
       ph.launched();
     }
     {
@@ -378,6 +399,284 @@ int inner_newton(ando_ctx c, const ando_params& p, const StepParams& sp, ando_st
   }
   ret = 0.5;
   return ANDO_OK;
+}
+
+// CORRECTED contact set at the current positions: LBVH vertex-triangle and
+// edge-edge candidates within the activation distance, then rigid contacts.
+int detect_corrected(ando_ctx c, int nb, double gap_max) {
+  cudaStream_t s = c->stream;
+  int nvt = 0, nee = 0;
+  {
+    Phase ph(c, ANDO_PHASE_SETUP);
+    long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
+    CK(c->bvh_tri.build(c->x.p, nullptr, c->tris.p, 3, c->T, float(gap_max), c->cub_tmp, s));
+    CK(c->bvh_tri.query(c->x.p, nullptr, 0, nullptr, c->V, float(gap_max), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
+    CK(c->bvh_edge.build(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->cub_tmp, s));
+    CK(c->bvh_edge.query(c->x.p, nullptr, 1, c->edges.p, c->E, float(gap_max), c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
+    ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
+  }
+  int nr = 0;
+  if (nb > 0) {
+    // count rigid contacts first to size the buffer, then write them after the self contacts
+    int rc = detect(c, nb, ANDO_PHASE_SETUP, gap_max, false, -1);
+    if (rc) return rc;
+    nr = c->ncontacts;
+  }
+  CK(c->contacts.reserve(size_t(nvt) + nee + nr + 1));
+  if (nb > 0 && nr) {
+    MeshDev m = c->mesh_dev();
+    Phase ph(c, ANDO_PHASE_SETUP);
+    launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, 0, gap_max, c->det_offsets.p, c->contacts.p + nvt + nee, s);
+    ph.launched();
+  }
+  if (nvt + nee) {
+    Phase ph(c, ANDO_PHASE_SETUP);
+    launch_pairs_to_contacts(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, gap_max, c->contacts.p, s);
+    ph.launched();
+  }
+  c->ncontacts = nvt + nee + nr;
+  c->n_pe = 0;
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+
+// Conservative time of impact along ext = 1.25 d: walls, swept-box LBVH
+// candidates, rigid triangles; then x += toi * d (CORRECTED line search).
+int corrected_line_search(ando_ctx c, int nb) {
+  cudaStream_t s = c->stream;
+  Phase ph(c, ANDO_PHASE_LINE_SEARCH);
+  launch_swept_end(c->V, c->x.p, c->d.p, c->fixed.p, 1.25, c->max_move, c->emax_cap.p, c->x1.p, c->ext.p, s);
+  launch_toi_reset(c->toi.p, s);
+  launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
+  ph.launched(2 + (c->num_walls ? 1 : 0));
+  int nvt = 0, nee = 0;
+  long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
+  CK(c->bvh_tri.build(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->cub_tmp, s));
+  CK(c->bvh_tri.query(c->x.p, c->x1.p, 0, nullptr, c->V, 0.f, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
+  CK(c->bvh_edge.build(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->cub_tmp, s));
+  CK(c->bvh_edge.query(c->x.p, c->x1.p, 1, c->edges.p, c->E, 0.f, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
+  ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
+  if (nvt + nee) { launch_toi_pairs(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, c->ext.p, c->toi.p, s); ph.launched(); }
+  if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
+  launch_update_toi(c->V, c->x.p, c->d.p, c->fixed.p, c->ctrl.p, c->toi.p, c->emax_cap.p, s);
+  ph.launched();
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+
+// Contacts, elastic gradient at x, contact constants, gradient, norm test.
+int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, int nb) {
+  MeshDev m = c->mesh_dev();
+  cudaStream_t s = c->stream;
+  int rc = detect_corrected(c, nb, p.contact_gap_max);
+  if (rc) return rc;
+  {
+    Phase ph(c, ANDO_PHASE_GRADIENT);
+    launch_ctrl_reset(c->ctrl.p, s);
+    launch_elastic_gradient(m, c->x.p, c->mu, c->thickness, c->g_el_x.p, s);
+    ph.launched(2);
+  }
+  rc = prepare_contacts(c, sp, c->g_el_x.p, c->fixed.p);
+  if (rc) return rc;
+  if (sp.enable_strain) {
+    Phase ph(c, ANDO_PHASE_STRAIN);
+    launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, s);
+    ph.launched();
+  }
+  Phase ph(c, ANDO_PHASE_GRADIENT);
+  launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
+                  c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
+                  c->ebegin.p, c->eend.p, sp, c->fixed.p, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, s);
+  launch_check(c->ctrl.p, p.pcg_tol, s);
+  ph.launched(2);
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+
+// inner_newton_step with the CORRECTED terms and line search.
+int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& sp, int nb, ando_step_stats& st, double& ret) {
+  MeshDev m = c->mesh_dev();
+  cudaStream_t s = c->stream;
+  PcgArgs pa;
+  pa.V = c->V; pa.rowptr = c->rowptr.p; pa.cols = c->cols.p; pa.val = c->val.p;
+  pa.P = c->precond.p; pa.b = c->b.p; pa.x = c->d.p; pa.r = c->r.p; pa.z = c->z.p; pa.p0 = c->p0.p; pa.p1 = c->p1.p; pa.Ap = c->Ap.p;
+  pa.partials = c->partials.p; pa.ctrl = c->ctrl.p; pa.tol = float(p.pcg_tol); pa.max_iters = p.pcg_max_iters;
+  for (int it = 0; it < p.max_newton_steps; ++it) {
+    int rc = corrected_gradient(c, p, sp, nb);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c->collect();
+    st.strain_active = c->ctrl_host->strain_active;
+    st.contacts = std::max(st.contacts, c->ncontacts);
+    if (c->ctrl_host->converged) { ret = 1.0; return ANDO_OK; }
+    pa.xbegin = c->nx ? c->xbegin.p : nullptr; pa.xend = c->nx ? c->xend.p : nullptr; pa.xcols = c->xcols.p; pa.xval = c->xval.p;
+    {
+      Phase ph(c, ANDO_PHASE_ASSEMBLE);
+      launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->val.p, c->precond.p, c->ctrl.p, s);
+      ph.launched();
+    }
+    {
+      Phase ph(c, ANDO_PHASE_PCG);
+      CK(launch_pcg(pa, c->pcg_grid, s));
+      ph.launched();
+    }
+    rc = corrected_line_search(c, nb);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    c->collect();
+    const Ctrl& h = *c->ctrl_host;
+    if (h.pcg_status == PCG_TIMEOUT || h.bar_err) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
+    st.newton_iters++;
+    st.pcg_iters += h.pcg_iters;
+    c->profile.pcg_iterations += h.pcg_iters;
+    c->profile.newton_iterations += 1;
+    st.pcg_max_per_newton = std::max(st.pcg_max_per_newton, h.pcg_iters);
+    if (!h.pcg_converged) st.pcg_not_converged++;
+    st.last_alpha = h.alpha;
+    if (h.alpha < 1e-8) { ret = 0.0; return ANDO_OK; }
+    if (h.alpha > 0.99) { ret = 1.0; return ANDO_OK; }
+  }
+  ret = 0.5;
+  return ANDO_OK;
+}
+
+// Kinematic pins of the CORRECTED step: pinned vertices sit on their targets.
+int apply_pins(ando_ctx c) {
+  cudaStream_t s = c->stream;
+  CK(cudaMemsetAsync(c->fixed.p, 0, c->V, s));
+  if (c->num_pins) {
+    Phase ph(c, ANDO_PHASE_SETUP);
+    launch_pin_apply(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->fixed.p, s);
+    ph.launched();
+  }
+  return ANDO_OK;
+}
+
+// One Newton iteration of the REFERENCE step as a fixed launch sequence
+// (also the body of the graph's inner loop).
+void enqueue_reference_iteration(ando_ctx c, const ando_params& p, const StepParams& sp, const PcgArgs& pa, bool ls_wall,
+                                 const WallDev& wall, cudaStream_t s, cudaError_t& err) {
+  MeshDev m = c->mesh_dev();
+  launch_ctrl_reset(c->ctrl.p, s);
+  if (sp.enable_strain) launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, s);
+  launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
+                  c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
+                  c->ebegin.p, c->eend.p, sp, nullptr, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, s);
+  launch_check(c->ctrl.p, p.pcg_tol, s);
+  launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, nullptr, c->val.p, c->precond.p, c->ctrl.p, s);
+  cudaError_t e = launch_pcg(pa, c->pcg_grid, s);
+  if (e != cudaSuccess && err == cudaSuccess) err = e;
+  if (ls_wall) launch_ls_wall(c->V, c->x.p, c->d.p, wall, c->ctrl.p, s);
+  launch_update(c->V, c->x.p, c->d.p, c->ctrl.p, s);
+}
+
+int kernels_per_iteration(const StepParams& sp, bool ls_wall) { return 7 + (sp.enable_strain ? 1 : 0) + (ls_wall ? 1 : 0); }
+
+// Capture the whole REFERENCE frame (no contacts) as one graph:
+//   predict, per-step constants, control init,
+//   WHILE(inner steps) { inner begin, WHILE(Newton) { iteration, Newton control }, beta control },
+//   velocity update, control block -> host.
+int capture_frame(ando_ctx c, const ando_params& p, const StepParams& sp, bool ls_wall, const WallDev& wall) {
+  cudaStream_t s = c->stream, s2 = c->cap2, s3 = c->cap3;
+  cudaError_t err = cudaSuccess;
+  int max_it = p.max_newton_steps;
+  if (p.enable_friction) max_it = std::max(max_it, p.friction_min_newton_steps);
+  PcgArgs pa;
+  pa.V = c->V; pa.rowptr = c->rowptr.p; pa.cols = c->cols.p; pa.val = c->val.p;
+  pa.xbegin = nullptr; pa.xend = nullptr; pa.xcols = c->xcols.p; pa.xval = c->xval.p;
+  pa.P = c->precond.p; pa.b = c->b.p; pa.x = c->d.p; pa.r = c->r.p; pa.z = c->z.p; pa.p0 = c->p0.p; pa.p1 = c->p1.p; pa.Ap = c->Ap.p;
+  pa.partials = c->partials.p; pa.ctrl = c->ctrl.p; pa.tol = float(p.pcg_tol); pa.max_iters = p.pcg_max_iters;
+  MeshDev m = c->mesh_dev();
+  cudaGraph_t full = nullptr, tmp = nullptr;
+  int depth = 0;   // open captures, closed on failure
+  auto abort_capture = [&](const char* what, cudaError_t e) {
+    cudaGraph_t g;
+    if (depth >= 3) cudaStreamEndCapture(s3, &g);
+    if (depth >= 2) cudaStreamEndCapture(s2, &g);
+    if (depth >= 1) { cudaStreamEndCapture(s, &g); if (g) cudaGraphDestroy(g); }
+    cudaGetLastError();
+    return fail(ANDO_ERR_CUDA, std::string("frame graph capture: ") + what + ": " + cudaGetErrorString(e));
+  };
+#define CAP(call, what) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return abort_capture(what, e_); } while (0)
+  CAP(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin");
+  depth = 1;
+  launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
+  CAP(cudaMemsetAsync(c->ebegin.p, 0, sizeof(int) * c->V, s), "memset");
+  CAP(cudaMemsetAsync(c->eend.p, 0, sizeof(int) * c->V, s), "memset");
+  launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, c->g_el.p, c->g_const.p, c->diag_const.p, s);
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  CAP(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd), "capture info");
+  cudaGraphConditionalHandle h_outer;
+  CAP(cudaGraphConditionalHandleCreate(&h_outer, g, 0, 0), "outer handle");
+  launch_ctl_init(c->sctl.p, p.beta_max, max_it, h_outer, s);
+  CAP(cudaGetLastError(), "ctl init");
+  CAP(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd), "capture info");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h_outer;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t n_outer;
+  CAP(cudaGraphAddNode(&n_outer, g, deps, nd, &cp), "outer node");
+  CAP(cudaStreamUpdateCaptureDependencies(s, &n_outer, 1, cudaStreamSetCaptureDependencies), "deps");
+  cudaGraph_t body_outer = cp.conditional.phGraph_out[0];
+  CAP(cudaStreamBeginCaptureToGraph(s2, body_outer, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "begin outer body");
+  depth = 2;
+  cudaGraphConditionalHandle h_newton;
+  CAP(cudaGraphConditionalHandleCreate(&h_newton, body_outer, 0, 0), "newton handle");
+  launch_inner_begin(c->sctl.p, h_newton, s2);
+  cudaGraph_t g2 = nullptr;
+  CAP(cudaStreamGetCaptureInfo(s2, &cs, nullptr, &g2, &deps, &nd), "capture info 2");
+  cudaGraphNodeParams cp2 = {};
+  cp2.type = cudaGraphNodeTypeConditional;
+  cp2.conditional.handle = h_newton;
+  cp2.conditional.type = cudaGraphCondTypeWhile;
+  cp2.conditional.size = 1;
+  cudaGraphNode_t n_newton;
+  CAP(cudaGraphAddNode(&n_newton, g2, deps, nd, &cp2), "newton node");
+  CAP(cudaStreamUpdateCaptureDependencies(s2, &n_newton, 1, cudaStreamSetCaptureDependencies), "deps 2");
+  cudaGraph_t body_newton = cp2.conditional.phGraph_out[0];
+  CAP(cudaStreamBeginCaptureToGraph(s3, body_newton, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "begin newton body");
+  depth = 3;
+  enqueue_reference_iteration(c, p, sp, pa, ls_wall, wall, s3, err);
+  CAP(err, "iteration");
+  launch_newton_ctl(c->sctl.p, c->ctrl.p, h_newton, s3);
+  CAP(cudaGetLastError(), "newton body");
+  CAP(cudaStreamEndCapture(s3, &tmp), "end newton body");
+  depth = 2;
+  launch_outer_ctl(c->sctl.p, p.beta_max, h_outer, s2);
+  CAP(cudaGetLastError(), "outer body");
+  CAP(cudaStreamEndCapture(s2, &tmp), "end outer body");
+  depth = 1;
+  double damp = p.velocity_damping > 0.0 ? 1.0 - std::min(std::max(p.velocity_damping, 0.0), 1.0) : 1.0;
+  launch_velocity_ctl(c->V, c->x.p, c->x_old.p, p.dt, damp, c->v.p, c->sctl.p, s);
+  CAP(cudaMemcpyAsync(c->sctl_host, c->sctl.p, sizeof(StepCtl), cudaMemcpyDeviceToHost, s), "ctl copy");
+  CAP(cudaGetLastError(), "epilogue");
+  CAP(cudaStreamEndCapture(s, &full), "end");
+  depth = 0;
+#undef CAP
+  if (c->frame_exec) { cudaGraphExecDestroy(c->frame_exec); c->frame_exec = nullptr; }
+  cudaError_t e = cudaGraphInstantiate(&c->frame_exec, full, 0);
+  cudaGraphDestroy(full);
+  if (e != cudaSuccess) { c->frame_exec = nullptr; cudaGetLastError(); return fail(ANDO_ERR_CUDA, std::string("frame graph instantiate: ") + cudaGetErrorString(e)); }
+  return ANDO_OK;
+}
+
+// The graph stays valid while parameters, constraint counts and every buffer
+// it references are unchanged.
+std::vector<unsigned char> frame_key(ando_ctx c, const ando_params& p, const StepParams& sp) {
+  std::vector<unsigned char> k;
+  auto put = [&](const void* d, size_t n) { const unsigned char* b = (const unsigned char*)d; k.insert(k.end(), b, b + n); };
+  put(&p, sizeof(p)); put(&sp, sizeof(sp)); put(&c->first_wall_host, sizeof(WallDev));
+  put(&c->num_pins, sizeof(int)); put(&c->num_walls, sizeof(int)); put(&c->mesh_generation, sizeof(long long));
+  const void* ptrs[] = {c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->walls.p, c->x.p, c->val.p, c->contacts.p, c->ents_sorted.p};
+  put(ptrs, sizeof(ptrs));
+  return k;
 }
 
 // Upload this step's pins (active ones, stably sorted by vertex), walls and
@@ -436,9 +735,11 @@ int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_ri
   int rc;
   double beta = 0.0;
   int bi = 0;
+  const bool corrected = p.semantics == ANDO_SEMANTICS_CORRECTED;
+  auto newton = [&](double& a) { return corrected ? inner_newton_corrected(c, p, sp, num_rigids, st, a) : inner_newton(c, p, sp, st, a); };
   while (beta < p.beta_max && bi < 20) {
     double alpha = 0.0;
-    rc = inner_newton(c, p, sp, st, alpha);
+    rc = newton(alpha);
     if (rc) return rc;
     beta = beta + (1.0 - beta) * alpha;
     ++bi;
@@ -446,7 +747,7 @@ int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_ri
   }
   if (beta > 1e-6) {
     double a2 = 0.0;
-    rc = inner_newton(c, p, sp, st, a2);
+    rc = newton(a2);
     if (rc) return rc;
   }
   st.beta = beta;
@@ -455,7 +756,7 @@ int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_ri
     double damp = p.velocity_damping > 0.0 ? 1.0 - std::min(std::max(p.velocity_damping, 0.0), 1.0) : 1.0;
     launch_velocity(c->V, c->x.p, c->x_old.p, beta * p.dt, damp, c->v.p, s);
     ph.launched();
-    if (p.contact_restitution > 0.0) {
+    if (p.contact_restitution > 0.0 && !corrected) {
       double e = std::min(std::max(p.contact_restitution, 0.0), 1.0);
       rc = detect(c, num_rigids, ANDO_PHASE_FINISH);
       if (rc) return rc;
@@ -464,7 +765,7 @@ int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_ri
       if (num_walls) { launch_restitution_walls(c->V, c->x.p, c->walls.p, num_walls, e, p.contact_gap_max, c->v.p, s); ph.launched(); }
     }
   }
-  if (num_rigids > 0) {
+  if (num_rigids > 0 && !corrected) {
     rc = detect(c, num_rigids, ANDO_PHASE_FINISH);
     if (rc) return rc;
     long long units = (long long)c->V * (1 + num_rigids);
@@ -513,6 +814,10 @@ int32_t ando_ctx_create(int32_t device, ando_ctx* out) {
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e == cudaSuccess) e = cudaMallocHost(&c->ctrl_host, sizeof(Ctrl));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->sctl_host, sizeof(StepCtl));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap3, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = c->sctl.reserve(1);
   if (e == cudaSuccess) e = c->ctrl.reserve(1);
   if (e == cudaSuccess) e = cudaMemset(c->ctrl.p, 0, sizeof(Ctrl));
   if (e != cudaSuccess) { delete c; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
@@ -619,9 +924,21 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->p0.reserve(3ull * V)); CK(c->p1.reserve(3ull * V)); CK(c->Ap.reserve(3ull * V));
   CK(c->val.reserve(9ull * nnzb)); CK(c->precond.reserve(9ull * V));
   CK(c->sflags.reserve(std::max(T, 1))); CK(c->sv.reserve(2ull * std::max(T, 1)));
+  CK(c->emax_cap.reserve(2));
+  {
+    double sum = 0.0;
+    for (size_t e = 0; e + 1 < edges.size(); e += 2) {
+      const double* a = vertices + 3ull * edges[e]; const double* b = vertices + 3ull * edges[e + 1];
+      sum += std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+    }
+    c->max_move = edges.empty() ? 1e300 : 4.0 * sum / double(edges.size() / 2);
+  }
+  CK(c->fixed.reserve(V)); CK(c->g_el_x.reserve(3ull * V)); CK(c->x1.reserve(3ull * V)); CK(c->ext.reserve(3ull * V)); CK(c->toi.reserve(1));
+  CK(cudaMemsetAsync(c->fixed.p, 0, V, s));
   CK(cudaMemsetAsync(c->sflags.p, 0, std::max(T, 1), s));
   CK(cudaMemsetAsync(c->d.p, 0, sizeof(float) * 3ull * V, s));
   c->el_semantics = -1;
+  c->mesh_generation++;
   c->mesh_ready = true;
   c->state_ready = false;
   MeshDev m = c->mesh_dev();
@@ -692,7 +1009,7 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
   if (!params || num_pins < 0 || num_walls < 0 || num_rigids < 0 || (num_pins && !pins) || (num_walls && !walls) || (num_rigids && !rigids))
     return fail(ANDO_ERR_INVALID, "step arguments");
   const ando_params& p = *params;
-  if (p.semantics != ANDO_SEMANTICS_REFERENCE) return fail(ANDO_ERR_INVALID, "only REFERENCE semantics is implemented");
+  if (p.semantics != ANDO_SEMANTICS_REFERENCE && p.semantics != ANDO_SEMANTICS_CORRECTED) return fail(ANDO_ERR_INVALID, "unknown semantics");
   if (p.precond != ANDO_PRECOND_BLOCK_JACOBI) return fail(ANDO_ERR_INVALID, "preconditioner not available");
   ando_step_stats st;
   std::memset(&st, 0, sizeof(st));
@@ -706,11 +1023,52 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
     ph.launched();
   }
-  rc = detect(c, num_rigids);
-  if (rc) return rc;
-  st.contacts = c->ncontacts;
-  rc = prepare_contacts(c, sp);
-  if (rc) return rc;
+  const bool graph_ok = c->use_graphs && !c->prof && p.semantics == ANDO_SEMANTICS_REFERENCE && num_rigids == 0 && c->T != 1 &&
+                        p.contact_restitution <= 0.0;
+  if (graph_ok) {
+    // whole frame as one graph launch; falls back to the host-driven loop if capture is refused
+    bool ls_wall = sp.first_wall >= 0 && (c->first_wall_host.n[0] * c->first_wall_host.n[0] + c->first_wall_host.n[1] * c->first_wall_host.n[1] +
+                                          c->first_wall_host.n[2] * c->first_wall_host.n[2]) > 0.5;
+    std::vector<unsigned char> key = frame_key(c, p, sp);
+    if (!c->frame_exec || key != c->frame_key) {
+      CK(c->ebegin.reserve(c->V)); CK(c->eend.reserve(c->V));
+      CK(c->contacts.reserve(1)); CK(c->ents_sorted.reserve(1)); CK(c->xcols.reserve(1)); CK(c->xval.reserve(9));
+      CK(cudaStreamSynchronize(s));
+      key = frame_key(c, p, sp);
+      if (capture_frame(c, p, sp, ls_wall, c->first_wall_host) == ANDO_OK) c->frame_key = key;
+      else { c->use_graphs = false; c->frame_key.clear(); }
+    }
+    if (c->use_graphs && c->frame_exec) {
+      CK(cudaGraphLaunch(c->frame_exec, s));
+      CK(cudaEventRecord(c->ev1, s));
+      CK(cudaEventSynchronize(c->ev1));
+      const StepCtl& h = *c->sctl_host;
+      if (h.error) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
+      st.newton_iters = h.newton_iters; st.pcg_iters = h.pcg_iters; st.pcg_max_per_newton = h.pcg_max;
+      st.pcg_not_converged = h.pcg_not_converged; st.line_search_fail = h.line_search_fail; st.strain_active = h.strain_active;
+      st.beta = h.beta; st.last_alpha = h.last_alpha; st.contacts = 0; st.graph_launched = 1;
+      long long launches = 5 + 2ll * h.inner_steps + (long long)h.iterations_run * kernels_per_iteration(sp, ls_wall);
+      c->profile.launches += launches;
+      c->profile.pcg_iterations += h.pcg_iters;
+      c->profile.newton_iterations += h.newton_iters;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+      st.device_ms = ms;
+      st.status = ANDO_OK;
+      if (stats) *stats = st;
+      return ANDO_OK;
+    }
+  }
+  if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
+    rc = apply_pins(c);
+    if (rc) return rc;
+  } else {
+    rc = detect(c, num_rigids);
+    if (rc) return rc;
+    st.contacts = c->ncontacts;
+    rc = prepare_contacts(c, sp, c->g_el.p, nullptr);
+    if (rc) return rc;
+  }
   rc = step_body(c, p, sp, num_rigids, num_walls, st);
   if (rc) return rc;
   CK(cudaGetLastError());
@@ -738,24 +1096,34 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   if (!params || num_pins < 0 || num_walls < 0 || num_rigids < 0 || (num_pins && !pins) || (num_walls && !walls) || (num_rigids && !rigids))
     return fail(ANDO_ERR_INVALID, "system arguments");
   const ando_params& p = *params;
-  if (p.semantics != ANDO_SEMANTICS_REFERENCE) return fail(ANDO_ERR_INVALID, "only REFERENCE semantics is implemented");
+  if (p.semantics != ANDO_SEMANTICS_REFERENCE && p.semantics != ANDO_SEMANTICS_CORRECTED) return fail(ANDO_ERR_INVALID, "unknown semantics");
   std::vector<ando_rigid> copy(rigids, rigids + num_rigids);
   StepParams sp;
   rc = upload_constraints(c, p, pins, num_pins, walls, num_walls, copy.data(), num_rigids, sp);
   if (rc) return rc;
   cudaStream_t s = c->stream;
   launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
+  MeshDev m = c->mesh_dev();
+  if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
+    rc = apply_pins(c);
+    if (rc) return rc;
+    rc = corrected_gradient(c, p, sp, num_rigids);
+    if (rc) return rc;
+    launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->val.p, c->precond.p, c->ctrl.p, s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return ANDO_OK;
+  }
   rc = detect(c, num_rigids);
   if (rc) return rc;
-  rc = prepare_contacts(c, sp);
+  rc = prepare_contacts(c, sp, c->g_el.p, nullptr);
   if (rc) return rc;
-  MeshDev m = c->mesh_dev();
   launch_ctrl_reset(c->ctrl.p, s);
   if (sp.enable_strain) launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, s);
   launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
                   c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
-                  c->ebegin.p, c->eend.p, sp, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, s);
-  launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->val.p, c->precond.p, c->ctrl.p, s);
+                  c->ebegin.p, c->eend.p, sp, sp.semantics ? c->fixed.p : nullptr, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, s);
+  launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, sp.semantics ? c->fixed.p : nullptr, c->val.p, c->precond.p, c->ctrl.p, s);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
   return ANDO_OK;
@@ -819,11 +1187,11 @@ int32_t ando_broad_phase(ando_ctx c, int32_t kind, double pad, int32_t* pairs, i
     Lbvh& B = kind == 0 ? c->bvh_tri : c->bvh_edge;
     long long before = B.launches;
     if (kind == 0) {
-      CK(B.build(c->x.p, c->tris.p, 3, c->T, float(pad), c->cub_tmp, s));
-      CK(B.query(c->x.p, 0, nullptr, c->V, float(pad), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &n, s));
+      CK(B.build(c->x.p, nullptr, c->tris.p, 3, c->T, float(pad), c->cub_tmp, s));
+      CK(B.query(c->x.p, nullptr, 0, nullptr, c->V, float(pad), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &n, s));
     } else {
-      CK(B.build(c->x.p, c->edges.p, 2, c->E, float(pad), c->cub_tmp, s));
-      CK(B.query(c->x.p, 1, c->edges.p, c->E, float(pad), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &n, s));
+      CK(B.build(c->x.p, nullptr, c->edges.p, 2, c->E, float(pad), c->cub_tmp, s));
+      CK(B.query(c->x.p, nullptr, 1, c->edges.p, c->E, float(pad), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &n, s));
     }
     ph.launched(int(B.launches - before));
   }

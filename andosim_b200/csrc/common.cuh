@@ -114,6 +114,16 @@ struct Ctrl {
 
 enum PcgStatus { PCG_OK = 0, PCG_MAXIT = 1, PCG_NOT_SPD = 2, PCG_TIMEOUT = 3, PCG_SKIPPED = 4 };
 
+// Device-side control of one step (integrator.cpp:98-121 and 152-236) when the
+// whole frame runs as one CUDA graph: the beta loop, the error-reduction pass
+// and the Newton loop are decided on the device between graph iterations.
+struct StepCtl {
+  double beta, ret, last_alpha;
+  int bi, phase, newton_it, max_it;   // phase 0: beta loop, 1: error-reduction pass, 2: done
+  int newton_iters, pcg_iters, pcg_max, pcg_not_converged, line_search_fail, strain_active, error;
+  int iterations_run, inner_steps;    // Newton bodies and inner steps executed (launch accounting)
+};
+
 // Bounded grid barrier for cooperative launches. All CTAs of the grid must be
 // co-resident (cudaLaunchCooperativeKernel guarantees it). A CTA that waits
 // more than `limit` polls sets *err and every CTA leaves; callers check the

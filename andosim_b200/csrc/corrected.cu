@@ -1,0 +1,298 @@
+// corrected.cu -- kernels of the CORRECTED step semantics.
+//
+// The CORRECTED step keeps the reference's algorithm (beta accumulation,
+// Newton with a block-Jacobi PCG inner solve, cubic barriers with
+// elasticity-inclusive dynamic stiffness) and fixes what the reference gets
+// wrong: elasticity is evaluated on the current positions, pins are
+// kinematic, self contact comes from a working broad phase with vertex-
+// triangle and edge-edge barriers refreshed every Newton iteration, and the
+// line search bounds the step by a conservative time of impact (FP64) instead
+// of 10 temporal samples.
+#include <cfloat>
+
+#include "kernels.cuh"
+
+namespace ando {
+
+namespace {
+
+constexpr int TPB = 256;
+inline int nblk(long long n) { return int((n + TPB - 1) / TPB); }
+
+// Segment-segment closest points (collision.cpp:389-452 scheme) with the
+// segment parameters.
+__device__ inline double ee_dist(d3 p0, d3 p1, d3 q0, d3 q1, double& s, double& t, d3& wp, d3& wq) {
+  d3 d1 = p1 - p0, d2 = q1 - q0, r = p0 - q0;
+  double a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+  const double eps = 1e-10;
+  auto cl = [](double v) { return fmin(fmax(v, 0.0), 1.0); };
+  s = 0.0; t = 0.0;
+  if (a <= eps && e <= eps) { wp = p0; wq = q0; }
+  else {
+    if (a <= eps) { s = 0; t = cl(f / e); }
+    else {
+      double c = dot(d1, r);
+      if (e <= eps) { t = 0; s = cl(-c / a); }
+      else {
+        double b = dot(d1, d2), den = a * e - b * b;
+        s = den != 0.0 ? cl((b * f - c * e) / den) : 0.0;
+        t = (b * s + f) / e;
+        if (t < 0.0) { t = 0; s = cl(-c / a); }
+        else if (t > 1.0) { t = 1; s = cl((b - c) / a); }
+      }
+    }
+    wp = p0 + d1 * s; wq = q0 + d2 * t;
+  }
+  return nrm(wp - wq);
+}
+
+// Point-triangle distance (collision.cpp:279-386 scheme).
+__device__ inline double pt_dist(d3 p, d3 a, d3 b, d3 c, d3& normal, d3& wq) {
+  d3 ab = b - a, ac = c - a, ap = p - a;
+  double d1 = dot(ab, ap), d2 = dot(ac, ap), dist;
+  auto vert = [&](d3 q) { wq = q; d3 df = p - q; double dd = nrm(df); normal = dd > 1e-10 ? df / dd : mk(0, 0, 1); return dd; };
+  if (d1 <= 0.0 && d2 <= 0.0) return vert(a);
+  d3 bp = p - b; double d3_ = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3_ >= 0.0 && d4 <= d3_) return vert(b);
+  d3 cp = p - c; double d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0.0 && d5 <= d6) return vert(c);
+  double vc = d1 * d4 - d3_ * d2;
+  if (vc <= 0.0 && d1 >= 0.0 && d3_ <= 0.0) return vert(a + ab * (d1 / (d1 - d3_)));
+  double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) return vert(a + ac * (d2 / (d2 - d6)));
+  double va = d3_ * d6 - d5 * d4;
+  if (va <= 0.0 && (d4 - d3_) >= 0.0 && (d5 - d6) >= 0.0) return vert(b + (c - b) * ((d4 - d3_) / ((d4 - d3_) + (d5 - d6))));
+  double den = 1.0 / (va + vb + vc);
+  wq = a + ab * (vb * den) + ac * (vc * den);
+  d3 df = p - wq; dist = nrm(df);
+  d3 tn = cross(ab, ac); double ta = nrm(tn);
+  if (ta > 1e-10) { tn = tn / ta; if (dot(tn, df) < 0.0) tn = -tn; normal = tn; }
+  else normal = dist > 1e-10 ? df / dist : mk(0, 0, 1);
+  return dist;
+}
+
+__device__ inline d3 bary(d3 p, d3 a, d3 b, d3 c) {
+  d3 v0 = b - a, v1 = c - a, v2 = p - a;
+  double d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
+  double den = d00 * d11 - d01 * d01, v = 0, w = 0;
+  if (fabs(den) > DBL_EPSILON) { v = (d11 * d20 - d01 * d21) / den; w = (d00 * d21 - d01 * d20) / den; }
+  v = fmin(fmax(v, 0.0), 1.0); w = fmin(fmax(w, 0.0), 1.0);
+  if (v + w > 1.0) { double sm = v + w; if (sm > DBL_EPSILON) { v /= sm; w /= sm; } }
+  return mk(1.0 - v - w, v, w);
+}
+
+__global__ void k_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= num_pins) return;
+  // several pins on one vertex: the last one in list order wins (pins arrive
+  // stably sorted by vertex)
+  int v = pin_vertex[k];
+  if (k + 1 < num_pins && pin_vertex[k + 1] == v) return;
+  x[3 * v] = pin_target[3 * k]; x[3 * v + 1] = pin_target[3 * k + 1]; x[3 * v + 2] = pin_target[3 * k + 2];
+  fixed[v] = 1;
+}
+
+// Candidate pairs -> contacts at the current positions. Every candidate gets a
+// slot; the ones outside the activation distance are marked inactive
+// (type < 0) and contribute nothing.
+__global__ void k_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges,
+                                    const double* x, double gap_max, ContactDev* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nvt + nee) return;
+  ContactDev C;
+  C.rigid = -1; C.count = 4; C.kbar = C.dV = C.d2V = 0.0; C.in_dom = 0;
+  C.nn[0] = C.nn[1] = C.nn[2] = 0.0;
+  if (k < nvt) {
+    int v = vt[k].x, t = vt[k].y;
+    C.type = 0; C.idx[0] = v; C.idx[1] = tris[3 * t]; C.idx[2] = tris[3 * t + 1]; C.idx[3] = tris[3 * t + 2];
+    d3 p = ld3(x, v), a = ld3(x, C.idx[1]), b = ld3(x, C.idx[2]), c = ld3(x, C.idx[3]);
+    d3 n, wq;
+    double d = pt_dist(p, a, b, c, n, wq);
+    d3 bc = bary(wq, a, b, c);
+    C.gap = d; C.n[0] = n.x; C.n[1] = n.y; C.n[2] = n.z;
+    C.wp[0] = p.x; C.wp[1] = p.y; C.wp[2] = p.z; C.wq[0] = wq.x; C.wq[1] = wq.y; C.wq[2] = wq.z;
+    C.bary[0] = bc.x; C.bary[1] = bc.y; C.bary[2] = bc.z;
+    C.w[0] = 1.0; C.w[1] = -bc.x; C.w[2] = -bc.y; C.w[3] = -bc.z;
+  } else {
+    int e1 = ee[k - nvt].x, e2 = ee[k - nvt].y;
+    C.type = 1; C.idx[0] = edges[2 * e1]; C.idx[1] = edges[2 * e1 + 1]; C.idx[2] = edges[2 * e2]; C.idx[3] = edges[2 * e2 + 1];
+    double s, t; d3 wp, wq;
+    double d = ee_dist(ld3(x, C.idx[0]), ld3(x, C.idx[1]), ld3(x, C.idx[2]), ld3(x, C.idx[3]), s, t, wp, wq);
+    d3 n = d > 1e-10 ? (wp - wq) / d : mk(0, 0, 1);
+    C.gap = d; C.n[0] = n.x; C.n[1] = n.y; C.n[2] = n.z;
+    C.wp[0] = wp.x; C.wp[1] = wp.y; C.wp[2] = wp.z; C.wq[0] = wq.x; C.wq[1] = wq.y; C.wq[2] = wq.z;
+    C.bary[0] = s; C.bary[1] = t; C.bary[2] = 0.0;
+    C.w[0] = 1.0 - s; C.w[1] = s; C.w[2] = -(1.0 - t); C.w[3] = -t;
+  }
+  if (!(C.gap < gap_max)) C.type = -1 - C.type;  // outside the activation distance: inactive
+  out[k] = C;
+}
+
+// Largest extended displacement |1.25 d_i| over free vertices (max-reduction on IEEE bits).
+__global__ void k_ext_max(int V, const float* d, const unsigned char* fixed, double ext_scale, unsigned long long* emax) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (i < V && !(fixed && fixed[i])) {
+    double a = d[3 * i], b = d[3 * i + 1], c = d[3 * i + 2];
+    e = ext_scale * sqrt(a * a + b * b + c * c);
+  }
+  for (int o = 16; o; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if ((threadIdx.x & 31) == 0 && e > 0.0) atomicMax(emax, (unsigned long long)__double_as_longlong(e));
+}
+
+// ext = cap * 1.25 d with cap = min(1, lmax / max|1.25 d|) (no vertex moves
+// more than lmax in one Newton iteration); x1 = x + ext. cap is stored in
+// emax_cap[1] for the position update.
+__global__ void k_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double ext_scale, double lmax,
+                            unsigned long long* emax_cap, double* x1, double* ext) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double emax = __longlong_as_double((long long)emax_cap[0]);
+  double cap = emax > lmax ? lmax / emax : 1.0;
+  if (i == 0) emax_cap[1] = (unsigned long long)__double_as_longlong(cap);
+  if (i >= 3 * V) return;
+  double e = fixed && fixed[i / 3] ? 0.0 : cap * (ext_scale * double(d[i]));
+  ext[i] = e;
+  x1[i] = x[i] + e;
+}
+
+__device__ inline void atomic_min_pos(unsigned long long* addr, double t) {
+  atomicMin(addr, (unsigned long long)__double_as_longlong(fmax(t, 0.0)));
+}
+__device__ inline double warp_min(double v) { for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
+
+// Exact linear time of impact of each vertex against every active wall.
+__global__ void k_toi_walls(int V, const double* x, const double* ext, const WallDev* walls, int nw, unsigned long long* toi) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double t = 1.0;
+  if (i < V) {
+    d3 xi = ld3(x, i), e = ld3(ext, i);
+    for (int w = 0; w < nw; ++w) {
+      if (!walls[w].active) continue;
+      d3 n = normalized(mk(walls[w].n[0], walls[w].n[1], walls[w].n[2]));
+      double dn = dot(n, e);
+      if (!(dn < 0.0)) continue;
+      double gap = dot(n, xi) - walls[w].offset;
+      t = fmin(t, fmax(gap, 0.0) / (-dn));
+    }
+  }
+  t = warp_min(t);
+  if ((threadIdx.x & 31) == 0 && t < 1.0) atomic_min_pos(toi, t);
+}
+
+// Conservative advancement: the distance of a pair cannot shrink faster than
+// l (sum of the largest displacements of either side) per unit time, so
+// stepping by (d - eta) / l never skips contact; stop at eta = d0 / 10.
+template <class F> __device__ inline double advance(F dist, double l) {
+  if (!(l > 0.0)) return 1.0;
+  double d0 = dist(0.0);
+  if (!(d0 > 0.0)) return 0.0;
+  double eta = 0.1 * d0, t = 0.0, d = d0;
+  for (int it = 0; it < 200; ++it) {
+    if (it) d = dist(t);
+    if (d <= eta) return t;
+    t += (d - eta) / l;
+    if (t >= 1.0) return 1.0;
+  }
+  return t;
+}
+
+__global__ void k_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges,
+                            const double* x, const double* ext, unsigned long long* toi) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double t = 1.0;
+  if (k < nvt + nee) {
+    int id[4];
+    if (k < nvt) { id[0] = vt[k].x; int tr = vt[k].y; id[1] = tris[3 * tr]; id[2] = tris[3 * tr + 1]; id[3] = tris[3 * tr + 2]; }
+    else { int e1 = ee[k - nvt].x, e2 = ee[k - nvt].y; id[0] = edges[2 * e1]; id[1] = edges[2 * e1 + 1]; id[2] = edges[2 * e2]; id[3] = edges[2 * e2 + 1]; }
+    d3 p[4], e[4];
+    double L[4];
+    for (int q = 0; q < 4; ++q) { p[q] = ld3(x, id[q]); e[q] = ld3(ext, id[q]); L[q] = nrm(e[q]); }
+    if (k < nvt) {
+      double l = L[0] + fmax(L[1], fmax(L[2], L[3]));
+      t = advance([&](double s) { d3 n, wq; return pt_dist(p[0] + e[0] * s, p[1] + e[1] * s, p[2] + e[2] * s, p[3] + e[3] * s, n, wq); }, l);
+    } else {
+      double l = fmax(L[0], L[1]) + fmax(L[2], L[3]);
+      t = advance([&](double s) { double a, b; d3 wp, wq; return ee_dist(p[0] + e[0] * s, p[1] + e[1] * s, p[2] + e[2] * s, p[3] + e[3] * s, a, b, wp, wq); }, l);
+    }
+  }
+  t = warp_min(t);
+  if ((threadIdx.x & 31) == 0 && t < 1.0) atomic_min_pos(toi, t);
+}
+
+// Vertices against static rigid triangles (the bodies do not move during the step).
+__global__ void k_toi_rigid(int V, const double* x, const double* ext, const RigidDev* bodies, int nb, unsigned long long* toi) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double t = 1.0;
+  if (i < V) {
+    d3 p = ld3(x, i), e = ld3(ext, i);
+    double l = nrm(e);
+    if (l > 0.0) {
+      for (int b = 0; b < nb; ++b) {
+        const RigidDev& B = bodies[b];
+        for (int tr = 0; tr < B.nt; ++tr) {
+          d3 a = ld3(B.world, B.tris[3 * tr]), bb = ld3(B.world, B.tris[3 * tr + 1]), c = ld3(B.world, B.tris[3 * tr + 2]);
+          bool overlap = true;
+          for (int k = 0; k < 3; ++k) {
+            double lo = fmin(comp(p, k), comp(p + e, k)) - 1e-4, hi = fmax(comp(p, k), comp(p + e, k)) + 1e-4;
+            double tl = fmin(fmin(comp(a, k), comp(bb, k)), comp(c, k)), th = fmax(fmax(comp(a, k), comp(bb, k)), comp(c, k));
+            if (!(lo <= th && hi >= tl)) overlap = false;
+          }
+          if (!overlap) continue;
+          t = fmin(t, advance([&](double s) { d3 n, wq; return pt_dist(p + e * s, a, bb, c, n, wq); }, l));
+        }
+      }
+    }
+  }
+  t = warp_min(t);
+  if ((threadIdx.x & 31) == 0 && t < 1.0) atomic_min_pos(toi, t);
+}
+
+// x += alpha d for free vertices, alpha = the time of impact bound (<= 1).
+__global__ void k_update_toi(int V, double* x, const float* d, const unsigned char* fixed, Ctrl* ctrl, const unsigned long long* toi,
+                             const unsigned long long* emax_cap) {
+  if (ctrl->converged) return;
+  double cap = __longlong_as_double((long long)emax_cap[1]);
+  double a = cap * fmin(1.0, __longlong_as_double((long long)*toi));
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) ctrl->alpha = a;
+  if (a < 1e-8 || i >= V || (fixed && fixed[i])) return;
+  x[3 * i] += a * double(d[3 * i]);
+  x[3 * i + 1] += a * double(d[3 * i + 1]);
+  x[3 * i + 2] += a * double(d[3 * i + 2]);
+}
+
+__global__ void k_toi_reset(unsigned long long* toi) { *toi = (unsigned long long)__double_as_longlong(1.0); }
+
+}  // namespace
+
+void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed, cudaStream_t s) {
+  if (num_pins) k_pin_apply<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, fixed);
+}
+void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
+                              double gap_max, ContactDev* out, cudaStream_t s) {
+  if (nvt + nee) k_pairs_to_contacts<<<nblk(nvt + nee), TPB, 0, s>>>(vt, nvt, ee, nee, tris, edges, x, gap_max, out);
+}
+void launch_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double scale, double lmax,
+                      unsigned long long* emax_cap, double* x1, double* ext, cudaStream_t s) {
+  if (!V) return;
+  cudaMemsetAsync(emax_cap, 0, sizeof(unsigned long long), s);
+  k_ext_max<<<nblk(V), TPB, 0, s>>>(V, d, fixed, scale, emax_cap);
+  k_swept_end<<<nblk(3ll * V), TPB, 0, s>>>(V, x, d, fixed, scale, lmax, emax_cap, x1, ext);
+}
+void launch_toi_reset(unsigned long long* toi, cudaStream_t s) { k_toi_reset<<<1, 1, 0, s>>>(toi); }
+void launch_toi_walls(int V, const double* x, const double* ext, const WallDev* walls, int nw, unsigned long long* toi, cudaStream_t s) {
+  if (V && nw) k_toi_walls<<<nblk(V), TPB, 0, s>>>(V, x, ext, walls, nw, toi);
+}
+void launch_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
+                      const double* ext, unsigned long long* toi, cudaStream_t s) {
+  if (nvt + nee) k_toi_pairs<<<nblk(nvt + nee), TPB, 0, s>>>(vt, nvt, ee, nee, tris, edges, x, ext, toi);
+}
+void launch_toi_rigid(int V, const double* x, const double* ext, const RigidDev* bodies, int nb, unsigned long long* toi, cudaStream_t s) {
+  if (V && nb) k_toi_rigid<<<nblk(V), TPB, 0, s>>>(V, x, ext, bodies, nb, toi);
+}
+void launch_update_toi(int V, double* x, const float* d, const unsigned char* fixed, Ctrl* ctrl, const unsigned long long* toi,
+                       const unsigned long long* emax_cap, cudaStream_t s) {
+  k_update_toi<<<nblk(V > 0 ? V : 1), TPB, 0, s>>>(V, x, d, fixed, ctrl, toi, emax_cap);
+}
+
+}  // namespace ando

@@ -56,10 +56,19 @@ __global__ void k_elastic_slots(MeshDev m, double mu, double thickness, int sema
   for (int k = m.slot_cptr[s]; k < m.slot_cptr[s + 1]; ++k) {
     int e = m.slot_contrib[k];
     int f = e / 9, a = (e % 9) / 3, b = e % 3;
-    double K00, K01, K11; face_K(m, f, mu, thickness, K00, K01, K11);
-    double c = face_block_coeff(K00, K01, K11, a, b);
-    if (semantics == 0) { A += fmax(c, 1e-8); B += 1e-8; }
-    else { A += c; B += c; }
+    if (semantics == 0) {
+      double K00, K01, K11; face_K(m, f, mu, thickness, K00, K01, K11);
+      double c = face_block_coeff(K00, K01, K11, a, b);
+      A += fmax(c, 1e-8); B += 1e-8;
+    } else {
+      // Hessian of k |F - R|^2 for a fixed frame R: 2k (G G^T)_ab I3 with
+      // G = [[-1,-1],[1,0],[0,1]] Dm_inv
+      double k = m.rest_area[f] * thickness * mu;
+      double da = m.dm_inv[4 * f], db = m.dm_inv[4 * f + 1], dc = m.dm_inv[4 * f + 2], dd = m.dm_inv[4 * f + 3];
+      double G[3][2] = {{-(da + dc), -(db + dd)}, {da, db}, {dc, dd}};
+      double c = 2.0 * k * (G[a][0] * G[b][0] + G[a][1] * G[b][1]);
+      A += c; B += c;
+    }
   }
   el_a[s] = A; el_b[s] = B;
 }
@@ -200,7 +209,7 @@ __device__ inline bool literal_pt_candidate(const MeshDev& m, const double* x, i
 
 // Count contacts per detection unit. Units: [0,V) vertex-vs-triangle-0 (literal
 // PT, only when T == 1), then [V + b*V + v] vertex v vs rigid body b.
-__global__ void k_detect_count(MeshDev m, const double* x, const RigidDev* bodies, int nb, int literal_pt, int* counts) {
+__global__ void k_detect_count(MeshDev m, const double* x, const RigidDev* bodies, int nb, int literal_pt, double thresh, int* counts) {
   long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long total = (long long)m.V * (1 + nb);
   if (u >= total) return;
@@ -210,7 +219,7 @@ __global__ void k_detect_count(MeshDev m, const double* x, const RigidDev* bodie
     if (literal_pt && literal_pt_candidate(m, x, v)) {
       double dist; d3 n, wq;
       narrow_pt(ld3(x, v), ld3(x, m.tris[0]), ld3(x, m.tris[1]), ld3(x, m.tris[2]), dist, n, wq);
-      cnt = dist < 0.01 ? 1 : 0;
+      cnt = dist < thresh ? 1 : 0;
     }
   } else {
     int b = int((u - m.V) / m.V), v = int((u - m.V) % m.V);
@@ -219,13 +228,13 @@ __global__ void k_detect_count(MeshDev m, const double* x, const RigidDev* bodie
     for (int t = 0; t < B.nt; ++t) {
       double dist; d3 n, wq;
       narrow_pt(p, ld3(B.world, B.tris[3 * t]), ld3(B.world, B.tris[3 * t + 1]), ld3(B.world, B.tris[3 * t + 2]), dist, n, wq);
-      cnt += dist < 0.01 ? 1 : 0;
+      cnt += dist < thresh ? 1 : 0;
     }
   }
   counts[u] = cnt;
 }
 
-__global__ void k_detect_write(MeshDev m, const double* x, const RigidDev* bodies, int nb, int literal_pt, const int* offsets, ContactDev* out) {
+__global__ void k_detect_write(MeshDev m, const double* x, const RigidDev* bodies, int nb, int literal_pt, double thresh, const int* offsets, ContactDev* out) {
   long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long total = (long long)m.V * (1 + nb);
   if (u >= total) return;
@@ -236,7 +245,7 @@ __global__ void k_detect_write(MeshDev m, const double* x, const RigidDev* bodie
     d3 p = ld3(x, v), a = ld3(x, m.tris[0]), b = ld3(x, m.tris[1]), c = ld3(x, m.tris[2]);
     double dist; d3 n, wq;
     narrow_pt(p, a, b, c, dist, n, wq);
-    if (!(dist < 0.01)) return;
+    if (!(dist < thresh)) return;
     ContactDev C;
     C.type = 0; C.idx[0] = v; C.idx[1] = m.tris[0]; C.idx[2] = m.tris[1]; C.idx[3] = m.tris[2]; C.rigid = -1; C.count = 4;
     C.gap = dist; C.n[0] = n.x; C.n[1] = n.y; C.n[2] = n.z;
@@ -252,7 +261,7 @@ __global__ void k_detect_write(MeshDev m, const double* x, const RigidDev* bodie
     for (int t = 0; t < B.nt; ++t) {
       double dist; d3 n, wq;
       narrow_pt(p, ld3(B.world, B.tris[3 * t]), ld3(B.world, B.tris[3 * t + 1]), ld3(B.world, B.tris[3 * t + 2]), dist, n, wq);
-      if (!(dist < 0.01)) continue;
+      if (!(dist < thresh)) continue;
       ContactDev C;
       C.type = 3; C.idx[0] = v; C.idx[1] = B.tris[3 * t]; C.idx[2] = B.tris[3 * t + 1]; C.idx[3] = B.tris[3 * t + 2];
       C.rigid = bi; C.count = 1; C.gap = dist; C.n[0] = n.x; C.n[1] = n.y; C.n[2] = n.z;
@@ -313,7 +322,7 @@ __global__ void k_contact_prep(MeshDev m, ContactDev* cs, int nc, StepParams p) 
   C.kbar = contact_kbar(m, C, p.dt);
   d3 nn = normalize_or_default(mk(C.n[0], C.n[1], C.n[2]), p.normal_eps);
   C.nn[0] = nn.x; C.nn[1] = nn.y; C.nn[2] = nn.z;
-  bool barrier_type = (C.type == 0 || C.type == 3);
+  bool barrier_type = (C.type == 0 || C.type == 3 || (p.semantics == 1 && C.type == 1));
   C.in_dom = barrier_type && in_domain(C.gap, p.contact_gap_max);
   C.dV = C.in_dom ? bar_grad(C.gap, p.contact_gap_max, C.kbar) : 0.0;
   C.d2V = C.in_dom ? bar_hess(C.gap, p.contact_gap_max, C.kbar) : 0.0;
@@ -332,7 +341,7 @@ __global__ void k_contact_entries(const ContactDev* cs, int nc, int V, int frict
                  C.idx[i] >= 0 && C.idx[j] >= 0 && C.idx[i] < V && C.idx[j] < V;
   // a barrier gradient entry is represented by the (i,i) entry even when d2V == 0 but dV != 0
   bool grad_only = !barrier && i == j && C.in_dom && C.dV != 0.0 && i < cnt && C.w[i] != 0.0 && C.idx[i] >= 0 && C.idx[i] < V;
-  bool fric = friction && i == 0 && j == 0 && C.idx[0] >= 0 && C.idx[0] < V;
+  bool fric = friction && C.type >= 0 && i == 0 && j == 0 && C.idx[0] >= 0 && C.idx[0] < V;
   ContactEntry E; E.contact = c; E.li = i; E.lj = j;
   if (barrier || grad_only || fric) {
     keys[e] = C.idx[i];
@@ -358,10 +367,10 @@ __global__ void k_vertex_ranges(const int* keys, int n, int V, int* begin, int* 
 // mesh, so constant) + contact barrier gradient, and the contact Hessian
 // blocks that land on the diagonal. Contact terms are summed in contact order.
 __global__ void k_contact_vertex(MeshDev m, const ContactDev* cs, const ContactEntry* ents, const int* begin, const int* end,
-                                 StepParams p, double* g_const, double* diag_const) {
+                                 StepParams p, const double* g_base, double* g_const, double* diag_const) {
   int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= m.V) return;
-  d3 g = ld3(m.g_elastic, v);
+  d3 g = ld3(g_base, v);
   double H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int k = begin[v]; k < end[v]; ++k) {
     ContactEntry E = ents[k];
@@ -391,11 +400,13 @@ __global__ void k_extra_flags(const ContactEntry* ents, const int* keys, int n, 
   flags[k] = (E.col >= 0 && E.col != keys[k] && !(E.li & 16)) ? 1 : 0;
 }
 
-__global__ void k_extra_values(const ContactDev* cs, const ContactEntry* xent, int* xcols, int nx, StepParams p, float* xval) {
+__global__ void k_extra_values(const ContactDev* cs, const ContactEntry* xent, const int* xkeys, const unsigned char* fixed, int* xcols, int nx,
+                               StepParams p, float* xval) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nx) return;
   ContactEntry E = xent[k];
   xcols[k] = E.col;
+  if (fixed && (fixed[xkeys[k]] || fixed[E.col])) { for (int q = 0; q < 9; ++q) xval[9 * k + q] = 0.f; return; }
   const ContactDev& C = cs[E.contact];
   int i = E.li & 3, j = E.lj;
   d3 n = mk(C.nn[0], C.nn[1], C.nn[2]);
@@ -525,10 +536,15 @@ __global__ void __launch_bounds__(256, 3) k_gradient(MeshDev m, const double* x,
                            const double* diag_const, const unsigned char* sflags, const StrainSV* sv,
                            const int* pin_vertex, const int* pin_head, const double* pin_target, int num_pins, const WallDev* walls,
                            const ContactDev* contacts, const ContactEntry* ents, const int* ebegin, const int* eend,
-                           StepParams p, double* g, float* b, double* diag_extra, Ctrl* ctrl) {
+                           StepParams p, const unsigned char* fixed, double* g, float* b, double* diag_extra, Ctrl* ctrl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double local = 0.0;
-  if (i < m.V) {
+  if (i < m.V && fixed && fixed[i]) {
+    // kinematic pin (CORRECTED): no degree of freedom, unit diagonal block
+    st3(g, i, mk(0, 0, 0));
+    b[3 * i] = 0.f; b[3 * i + 1] = 0.f; b[3 * i + 2] = 0.f;
+    for (int k = 0; k < 9; ++k) diag_extra[9 * i + k] = (k % 4 == 0) ? 1.0 : 0.0;
+  } else if (i < m.V) {
     double mi = m.mass[i];
     d3 xi = ld3(x, i), xh = ld3(x_hat, i);
     double mf = mi / (p.dt * p.dt);
@@ -553,8 +569,9 @@ __global__ void __launch_bounds__(256, 3) k_gradient(MeshDev m, const double* x,
     int ds = m.diag_slot[i];
     double A = mdiag + m.el_a[ds], B = mdiag + m.el_b[ds];
     double D0 = fmax(A, 1e-8), D2 = fmax(B, 1e-8);  // enforce_spd of the diagonal H_total block
-    // pins (sorted by vertex; pin_head[i] = first pin of vertex i or -1)
-    if (num_pins > 0) {
+    // pins (sorted by vertex; pin_head[i] = first pin of vertex i or -1);
+    // CORRECTED pins are kinematic and carry no barrier
+    if (num_pins > 0 && p.semantics == 0) {
       int lo = pin_head[i];
       for (int k = lo; k >= 0 && k < num_pins && pin_vertex[k] == i; ++k) {
         d3 off = xi - mk(pin_target[3 * k], pin_target[3 * k + 1], pin_target[3 * k + 2]);
@@ -650,11 +667,18 @@ __global__ void k_check(Ctrl* c, double tol) {
 // by construction, so the reference's (H + H^T)/2 leaves it unchanged. The
 // diagonal slot also yields the block-Jacobi inverse (pcg_solver.cpp:77-114).
 __global__ void k_assemble(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
-                           float* val, float* precond, const Ctrl* ctrl) {
+                           const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl) {
   if (ctrl->converged) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= m.nnzb) return;
   int row = m.slot_row[s], col = m.cols[s];
+  if (fixed && (fixed[row] || fixed[col])) {
+    // kinematic pin: decoupled row and column, unit diagonal (diag_extra holds I)
+    float one = row == col ? 1.f : 0.f;
+    for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = (k % 4 == 0) ? one : 0.f;
+    if (row == col) for (int k = 0; k < 9; ++k) precond[9 * (long long)row + k] = (k % 4 == 0) ? 1.f : 0.f;
+    return;
+  }
   double H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   H[0] = H[4] = m.el_a[s]; H[8] = m.el_b[s];
   if (enable_strain) {
@@ -921,7 +945,85 @@ __global__ void k_rigid_coupling(MeshDev m, const ContactDev* cs, StepParams p, 
   }
 }
 
+// ------------------------------------------------------- graph step control
+__global__ void k_ctl_init(StepCtl* c, double beta_max, int max_it, cudaGraphConditionalHandle outer) {
+  c->beta = 0.0; c->ret = 0.0; c->last_alpha = 0.0;
+  c->bi = 0; c->newton_it = 0; c->max_it = max_it;
+  c->newton_iters = c->pcg_iters = c->pcg_max = c->pcg_not_converged = c->line_search_fail = c->strain_active = c->error = 0;
+  c->iterations_run = c->inner_steps = 0;
+  c->phase = (0.0 < beta_max) ? 0 : 2;
+  cudaGraphSetConditional(outer, c->phase != 2 ? 1u : 0u);
+}
+
+__global__ void k_inner_begin(StepCtl* c, cudaGraphConditionalHandle newton) {
+  c->newton_it = 0;
+  c->inner_steps++;
+  cudaGraphSetConditional(newton, c->max_it > 0 ? 1u : 0u);
+}
+
+// After one Newton iteration: the decisions of inner_newton_step (integrator.cpp:169-235).
+__global__ void k_newton_ctl(StepCtl* c, const Ctrl* ctrl, cudaGraphConditionalHandle newton) {
+  bool stop = false;
+  c->iterations_run++;
+  c->strain_active = ctrl->strain_active;
+  if (ctrl->converged) { c->ret = 1.0; stop = true; }
+  else if (ctrl->pcg_status == PCG_TIMEOUT || ctrl->bar_err) { c->error = 1; c->ret = 0.0; stop = true; }
+  else {
+    c->newton_iters++;
+    c->pcg_iters += ctrl->pcg_iters;
+    c->pcg_max = max(c->pcg_max, ctrl->pcg_iters);
+    if (!ctrl->pcg_converged) c->pcg_not_converged++;
+    c->last_alpha = ctrl->alpha;
+    if (ctrl->alpha < 1e-8) { c->ret = 0.0; stop = true; }
+    else if (ctrl->alpha > 0.99) { c->ret = 1.0; stop = true; }
+    else if (++c->newton_it >= c->max_it) { c->ret = 0.5; stop = true; }
+  }
+  cudaGraphSetConditional(newton, stop ? 0u : 1u);
+}
+
+// After one inner Newton step: beta accumulation and the error-reduction pass
+// (integrator.cpp:98-121).
+__global__ void k_outer_ctl(StepCtl* c, double beta_max, cudaGraphConditionalHandle outer) {
+  if (c->error) { c->phase = 2; cudaGraphSetConditional(outer, 0u); return; }
+  if (c->phase == 0) {
+    double a = c->ret;
+    c->beta = c->beta + (1.0 - c->beta) * a;
+    c->bi++;
+    bool more = true;
+    if (a < 1e-6) { c->line_search_fail++; more = false; }
+    if (more && !(c->beta < beta_max && c->bi < 20)) more = false;
+    if (!more) c->phase = c->beta > 1e-6 ? 1 : 2;
+  } else {
+    c->phase = 2;
+  }
+  cudaGraphSetConditional(outer, c->phase != 2 ? 1u : 0u);
+}
+
+__global__ void k_velocity_ctl(int V, const double* x, const double* x_old, double dt, double damp_scale, double* v, const StepCtl* c) {
+  double beta = c->beta;
+  if (!(beta > 1e-6)) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * V) return;
+  double vi = (x[i] - x_old[i]) / (beta * dt);
+  if (damp_scale != 1.0) vi *= damp_scale;
+  v[i] = vi;
+}
+
 }  // namespace
+
+void launch_ctl_init(StepCtl* c, double beta_max, int max_it, cudaGraphConditionalHandle outer, cudaStream_t s) {
+  k_ctl_init<<<1, 1, 0, s>>>(c, beta_max, max_it, outer);
+}
+void launch_inner_begin(StepCtl* c, cudaGraphConditionalHandle newton, cudaStream_t s) { k_inner_begin<<<1, 1, 0, s>>>(c, newton); }
+void launch_newton_ctl(StepCtl* c, const Ctrl* ctrl, cudaGraphConditionalHandle newton, cudaStream_t s) {
+  k_newton_ctl<<<1, 1, 0, s>>>(c, ctrl, newton);
+}
+void launch_outer_ctl(StepCtl* c, double beta_max, cudaGraphConditionalHandle outer, cudaStream_t s) {
+  k_outer_ctl<<<1, 1, 0, s>>>(c, beta_max, outer);
+}
+void launch_velocity_ctl(int V, const double* x, const double* x_old, double dt, double damp_scale, double* v, const StepCtl* c, cudaStream_t s) {
+  if (V) k_velocity_ctl<<<nblk(3ll * V), TPB, 0, s>>>(V, x, x_old, dt, damp_scale, v, c);
+}
 
 // ------------------------------------------------------------------ launchers
 void launch_elastic_slots(const MeshDev& m, double mu, double thickness, int semantics, double* el_a, double* el_b, cudaStream_t s) {
@@ -941,13 +1043,13 @@ void launch_rigid_world(RigidDev* bodies_dev, const RigidDev* bodies_host, int n
   for (int b = 0; b < nb; ++b) maxv = bodies_host[b].nv > maxv ? bodies_host[b].nv : maxv;
   if (nb && maxv) k_rigid_world<<<dim3(nblk(maxv), nb), TPB, 0, s>>>(bodies_dev, nb);
 }
-void launch_detect_count(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, int* counts, cudaStream_t s) {
+void launch_detect_count(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, double thresh, int* counts, cudaStream_t s) {
   long long units = (long long)m.V * (1 + nb);
-  if (units) k_detect_count<<<nblk(units), TPB, 0, s>>>(m, x, bodies, nb, literal_pt, counts);
+  if (units) k_detect_count<<<nblk(units), TPB, 0, s>>>(m, x, bodies, nb, literal_pt, thresh, counts);
 }
-void launch_detect_write(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, const int* offsets, ContactDev* out, cudaStream_t s) {
+void launch_detect_write(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, double thresh, const int* offsets, ContactDev* out, cudaStream_t s) {
   long long units = (long long)m.V * (1 + nb);
-  if (units) k_detect_write<<<nblk(units), TPB, 0, s>>>(m, x, bodies, nb, literal_pt, offsets, out);
+  if (units) k_detect_write<<<nblk(units), TPB, 0, s>>>(m, x, bodies, nb, literal_pt, thresh, offsets, out);
 }
 void launch_contact_prep(const MeshDev& m, ContactDev* c, int nc, const StepParams& p, cudaStream_t s) {
   if (nc) k_contact_prep<<<nblk(nc), TPB, 0, s>>>(m, c, nc, p);
@@ -959,14 +1061,15 @@ void launch_vertex_ranges(const int* keys, int n, int V, int* begin, int* end, c
   if (V) k_vertex_ranges<<<nblk(V), TPB, 0, s>>>(keys, n, V, begin, end);
 }
 void launch_contact_vertex(const MeshDev& m, const ContactDev* c, const ContactEntry* ents, const int* begin, const int* end,
-                           const StepParams& p, double* g_const, double* diag_const, cudaStream_t s) {
-  if (m.V) k_contact_vertex<<<nblk(m.V), TPB, 0, s>>>(m, c, ents, begin, end, p, g_const, diag_const);
+                           const StepParams& p, const double* g_base, double* g_const, double* diag_const, cudaStream_t s) {
+  if (m.V) k_contact_vertex<<<nblk(m.V), TPB, 0, s>>>(m, c, ents, begin, end, p, g_base, g_const, diag_const);
 }
 void launch_extra_flags(const ContactEntry* ents, const int* keys, int n, int* flags, cudaStream_t s) {
   if (n) k_extra_flags<<<nblk(n), TPB, 0, s>>>(ents, keys, n, flags);
 }
-void launch_extra_values(const ContactDev* c, const ContactEntry* xent, int* xcols, int nx, const StepParams& p, float* xval, cudaStream_t s) {
-  if (nx) k_extra_values<<<nblk(nx), TPB, 0, s>>>(c, xent, xcols, nx, p, xval);
+void launch_extra_values(const ContactDev* c, const ContactEntry* xent, const int* xkeys, const unsigned char* fixed, int* xcols, int nx,
+                         const StepParams& p, float* xval, cudaStream_t s) {
+  if (nx) k_extra_values<<<nblk(nx), TPB, 0, s>>>(c, xent, xkeys, fixed, xcols, nx, p, xval);
 }
 void launch_ctrl_reset(Ctrl* ctrl, cudaStream_t s) { k_ctrl_reset<<<1, 1, 0, s>>>(ctrl); }
 void launch_strain_face(const MeshDev& m, const double* x, const StepParams& p, unsigned char* flags, StrainSV* sv, Ctrl* ctrl, cudaStream_t s) {
@@ -979,14 +1082,14 @@ void launch_gradient(const MeshDev& m, const double* x, const double* x_hat, con
                      const double* diag_const, const unsigned char* sflags, const StrainSV* sv,
                      const int* pin_vertex, const int* pin_head, const double* pin_target, int num_pins, const WallDev* walls,
                      const ContactDev* contacts, const ContactEntry* ents, const int* ebegin, const int* eend,
-                     const StepParams& p, double* g, float* b, double* diag_extra, Ctrl* ctrl, cudaStream_t s) {
+                     const StepParams& p, const unsigned char* fixed, double* g, float* b, double* diag_extra, Ctrl* ctrl, cudaStream_t s) {
   if (m.V) k_gradient<<<nblk(m.V), TPB, 0, s>>>(m, x, x_hat, x_prev, g_const, diag_const, sflags, sv, pin_vertex, pin_head, pin_target, num_pins, walls,
-                                                contacts, ents, ebegin, eend, p, g, b, diag_extra, ctrl);
+                                                contacts, ents, ebegin, eend, p, fixed, g, b, diag_extra, ctrl);
 }
 void launch_check(Ctrl* ctrl, double tol, cudaStream_t s) { k_check<<<1, 1, 0, s>>>(ctrl, tol); }
 void launch_assemble(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
-                     float* val, float* precond, const Ctrl* ctrl, cudaStream_t s) {
-  if (m.nnzb) k_assemble<<<nblk(m.nnzb), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, val, precond, ctrl);
+                     const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl, cudaStream_t s) {
+  if (m.nnzb) k_assemble<<<nblk(m.nnzb), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, val, precond, ctrl);
 }
 void launch_ls_wall(int V, const double* x, const float* d, WallDev w, Ctrl* ctrl, cudaStream_t s) {
   if (V) k_ls_wall<<<nblk(V), TPB, 0, s>>>(V, x, d, w, ctrl);

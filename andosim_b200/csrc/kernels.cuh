@@ -22,15 +22,16 @@ void launch_predict(int V, const double* x, const double* v, double dt, double* 
 void launch_gravity(int V, double* x, double* v, double gx, double gy, double gz, double dt, cudaStream_t s);
 void launch_rigid_world(RigidDev* bodies_dev, const RigidDev* bodies_host, int nb, cudaStream_t s);
 // contact detection: count per (PT vertex) + (rigid body, vertex); literal PT only when T == 1.
-void launch_detect_count(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, int* counts, cudaStream_t s);
-void launch_detect_write(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, const int* offsets, ContactDev* out, cudaStream_t s);
+void launch_detect_count(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, double thresh, int* counts, cudaStream_t s);
+void launch_detect_write(const MeshDev& m, const double* x, const RigidDev* bodies, int nb, int literal_pt, double thresh, const int* offsets, ContactDev* out, cudaStream_t s);
 void launch_contact_prep(const MeshDev& m, ContactDev* c, int nc, const StepParams& p, cudaStream_t s);
 void launch_contact_entries(const ContactDev* c, int nc, int V, int friction, int* keys, ContactEntry* ents, cudaStream_t s);
 void launch_vertex_ranges(const int* sorted_keys, int n, int V, int* begin, int* end, cudaStream_t s);
 void launch_contact_vertex(const MeshDev& m, const ContactDev* c, const ContactEntry* ents, const int* begin, const int* end,
-                           const StepParams& p, double* g_const, double* diag_const, cudaStream_t s);
+                           const StepParams& p, const double* g_base, double* g_const, double* diag_const, cudaStream_t s);
 void launch_extra_flags(const ContactEntry* ents, const int* keys, int n, int* flags, cudaStream_t s);
-void launch_extra_values(const ContactDev* c, const ContactEntry* xent, int* xcols, int nx, const StepParams& p, float* xval, cudaStream_t s);
+void launch_extra_values(const ContactDev* c, const ContactEntry* xent, const int* xkeys, const unsigned char* fixed, int* xcols, int nx,
+                         const StepParams& p, float* xval, cudaStream_t s);
 
 // Newton iteration
 void launch_ctrl_reset(Ctrl* ctrl, cudaStream_t s);
@@ -39,11 +40,11 @@ void launch_gradient(const MeshDev& m, const double* x, const double* x_hat, con
                      const double* diag_const, const unsigned char* sflags, const StrainSV* sv,
                      const int* pin_vertex, const int* pin_head, const double* pin_target, int num_pins, const WallDev* walls,
                      const ContactDev* contacts, const ContactEntry* ents, const int* ebegin, const int* eend,
-                     const StepParams& p, double* g, float* b, double* diag_extra, Ctrl* ctrl, cudaStream_t s);
+                     const StepParams& p, const unsigned char* fixed, double* g, float* b, double* diag_extra, Ctrl* ctrl, cudaStream_t s);
 void launch_check(Ctrl* ctrl, double tol, cudaStream_t s);
 void launch_pin_heads(const int* pin_vertex, int num_pins, int* pin_head, cudaStream_t s);
 void launch_assemble(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
-                     float* val, float* precond, const Ctrl* ctrl, cudaStream_t s);
+                     const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl, cudaStream_t s);
 void launch_ls_wall(int V, const double* x, const float* d, WallDev w, Ctrl* ctrl, cudaStream_t s);
 void launch_ls_contacts(const ContactDev* c, int nc, const double* x, const float* d, Ctrl* ctrl, cudaStream_t s);
 void launch_update(int V, double* x, const float* d, Ctrl* ctrl, cudaStream_t s);
@@ -55,6 +56,27 @@ void launch_restitution_contacts(const ContactDev* c, int nc, const double* mass
 void launch_restitution_walls(int V, const double* x, const WallDev* walls, int nw, double e, double gap_max, double* v, cudaStream_t s);
 void launch_rigid_coupling(const MeshDev& m, const ContactDev* c, int nc, const StepParams& p, RigidDev* bodies, int nb,
                            const int* offsets, long long units, double dt, cudaStream_t s);
+
+// whole-frame CUDA graph control (kernels.cu)
+void launch_ctl_init(StepCtl* c, double beta_max, int max_it, cudaGraphConditionalHandle outer, cudaStream_t s);
+void launch_inner_begin(StepCtl* c, cudaGraphConditionalHandle newton, cudaStream_t s);
+void launch_newton_ctl(StepCtl* c, const Ctrl* ctrl, cudaGraphConditionalHandle newton, cudaStream_t s);
+void launch_outer_ctl(StepCtl* c, double beta_max, cudaGraphConditionalHandle outer, cudaStream_t s);
+void launch_velocity_ctl(int V, const double* x, const double* x_old, double dt, double damp_scale, double* v, const StepCtl* c, cudaStream_t s);
+
+// CORRECTED semantics (corrected.cu)
+void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed, cudaStream_t s);
+void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
+                              double gap_max, ContactDev* out, cudaStream_t s);
+void launch_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double scale, double lmax,
+                      unsigned long long* emax_cap, double* x1, double* ext, cudaStream_t s);
+void launch_toi_reset(unsigned long long* toi, cudaStream_t s);
+void launch_toi_walls(int V, const double* x, const double* ext, const WallDev* walls, int nw, unsigned long long* toi, cudaStream_t s);
+void launch_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
+                      const double* ext, unsigned long long* toi, cudaStream_t s);
+void launch_toi_rigid(int V, const double* x, const double* ext, const RigidDev* bodies, int nb, unsigned long long* toi, cudaStream_t s);
+void launch_update_toi(int V, double* x, const float* d, const unsigned char* fixed, Ctrl* ctrl, const unsigned long long* toi,
+                       const unsigned long long* emax_cap, cudaStream_t s);
 
 // PCG (pcg.cu)
 struct PcgArgs {

@@ -32,16 +32,19 @@ using Box = LbvhBox;
 
 __device__ inline float3 xf(const double* x, int i) { return make_float3(float(x[3 * i]), float(x[3 * i + 1]), float(x[3 * i + 2])); }
 
-__global__ void k_prim_boxes(const double* x, const int* prims, int arity, int n, float pad, Box* boxes) {
+__device__ inline void grow(Box& b, float3 q) {
+  b.lo[0] = fminf(b.lo[0], q.x); b.lo[1] = fminf(b.lo[1], q.y); b.lo[2] = fminf(b.lo[2], q.z);
+  b.hi[0] = fmaxf(b.hi[0], q.x); b.hi[1] = fmaxf(b.hi[1], q.y); b.hi[2] = fmaxf(b.hi[2], q.z);
+}
+
+// Box of primitive i at positions x, or swept over x -> x1 when x1 is given.
+__global__ void k_prim_boxes(const double* x, const double* x1, const int* prims, int arity, int n, float pad, Box* boxes) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float3 p = xf(x, prims[arity * i]);
   Box b; b.lo[0] = b.hi[0] = p.x; b.lo[1] = b.hi[1] = p.y; b.lo[2] = b.hi[2] = p.z;
-  for (int k = 1; k < arity; ++k) {
-    float3 q = xf(x, prims[arity * i + k]);
-    b.lo[0] = fminf(b.lo[0], q.x); b.lo[1] = fminf(b.lo[1], q.y); b.lo[2] = fminf(b.lo[2], q.z);
-    b.hi[0] = fmaxf(b.hi[0], q.x); b.hi[1] = fmaxf(b.hi[1], q.y); b.hi[2] = fmaxf(b.hi[2], q.z);
-  }
+  for (int k = 1; k < arity; ++k) grow(b, xf(x, prims[arity * i + k]));
+  if (x1) for (int k = 0; k < arity; ++k) grow(b, xf(x1, prims[arity * i + k]));
   if (pad > 0.f) for (int k = 0; k < 3; ++k) { b.lo[k] -= pad; b.hi[k] += pad; }
   boxes[i] = b;
 }
@@ -173,7 +176,7 @@ __device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, in
 // One thread per query. kind 0: query = vertex (point box +-1e-4 inflated by
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
 // prims = edges, keep e1 < e2 without shared vertex.
-__global__ void k_query(const double* x, const int* qprims, int kind, int nq, float pad, const int* prims, int n,
+__global__ void k_query(const double* x, const double* x1, const int* qprims, int kind, int nq, float pad, const int* prims, int n,
                         const int* order, const int* left, const int* right, const Box* nodes, int2* out, int* count, int cap) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = q < nq;
@@ -185,12 +188,18 @@ __global__ void k_query(const double* x, const int* qprims, int kind, int nq, fl
       float e = 1e-4f;
       qb.lo[0] = p.x - e; qb.lo[1] = p.y - e; qb.lo[2] = p.z - e;
       qb.hi[0] = p.x + e; qb.hi[1] = p.y + e; qb.hi[2] = p.z + e;
+      if (x1) {
+        float3 p1 = xf(x1, q);
+        qb.lo[0] = fminf(qb.lo[0], p1.x - e); qb.lo[1] = fminf(qb.lo[1], p1.y - e); qb.lo[2] = fminf(qb.lo[2], p1.z - e);
+        qb.hi[0] = fmaxf(qb.hi[0], p1.x + e); qb.hi[1] = fmaxf(qb.hi[1], p1.y + e); qb.hi[2] = fmaxf(qb.hi[2], p1.z + e);
+      }
       if (pad > 0.f) for (int k = 0; k < 3; ++k) { qb.lo[k] -= pad; qb.hi[k] += pad; }
     } else {
       qa = qprims[2 * q]; qc = qprims[2 * q + 1];
       float3 a = xf(x, qa), b = xf(x, qc);
       qb.lo[0] = fminf(a.x, b.x); qb.lo[1] = fminf(a.y, b.y); qb.lo[2] = fminf(a.z, b.z);
       qb.hi[0] = fmaxf(a.x, b.x); qb.hi[1] = fmaxf(a.y, b.y); qb.hi[2] = fmaxf(a.z, b.z);
+      if (x1) { grow(qb, xf(x1, qa)); grow(qb, xf(x1, qc)); }
       if (pad > 0.f) for (int k = 0; k < 3; ++k) { qb.lo[k] -= pad; qb.hi[k] += pad; }
     }
   }
@@ -256,13 +265,13 @@ cudaError_t Lbvh::reserve_prims(int n) {
 }
 
 // Build the hierarchy over `n` primitives of `arity` vertex indices each.
-cudaError_t Lbvh::build(const double* x, const int* prims_, int arity, int n_, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s) {
+cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, int arity, int n_, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s) {
   n = n_;
   prims = prims_;
   cudaError_t e = reserve_prims(n);
   if (e) return e;
   if (n == 0) return cudaSuccess;
-  k_prim_boxes<<<nblk(n), TPB, 0, s>>>(x, prims, arity, n, pad, boxes.p);
+  k_prim_boxes<<<nblk(n), TPB, 0, s>>>(x, x1, prims, arity, n, pad, boxes.p);
   k_bounds_init<<<1, 32, 0, s>>>(bounds.p);
   k_bounds<<<nblk(n), TPB, 0, s>>>(boxes.p, n, bounds.p);
   k_morton<<<nblk(n), TPB, 0, s>>>(boxes.p, n, bounds.p, keys.p, idx.p);
@@ -282,7 +291,7 @@ cudaError_t Lbvh::build(const double* x, const int* prims_, int arity, int n_, f
 
 // Query the hierarchy; returns the sorted (query, primitive) pairs in `out`
 // (capacity grown as needed) and their number in *npairs.
-cudaError_t Lbvh::query(const double* x, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
+cudaError_t Lbvh::query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
                         DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
                         DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
   cudaError_t e;
@@ -293,13 +302,14 @@ cudaError_t Lbvh::query(const double* x, int kind, const int* qprims, int nq, fl
   for (int attempt = 0; attempt < 2; ++attempt) {
     int cap = int(scratch.n);
     if ((e = cudaMemsetAsync(counter.p, 0, 2 * sizeof(int), s))) return e;
-    k_query<<<nblk(nq), TPB, 0, s>>>(x, qprims, kind, nq, pad, prims, n, order.p, left.p, right.p, nodes.p, scratch.p, counter.p, cap);
+    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, pad, prims, n, order.p, left.p, right.p, nodes.p, scratch.p, counter.p, cap);
     launches += 1;
     int cnt2[2] = {0, 0};
     if ((e = cudaMemcpyAsync(cnt2, counter.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
     if (cnt2[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
     int cnt = cnt2[0];
+    if (cnt < 0 || cnt > (1 << 26)) return cudaErrorMemoryAllocation;  // > 64M candidate pairs: refuse instead of exhausting memory
     if (cnt <= cap) { *npairs = cnt; break; }
     if ((e = scratch.reserve(size_t(cnt) + size_t(cnt) / 4))) return e;
   }

@@ -19,9 +19,10 @@ struct Lbvh {
   long long launches = 0;
 
   cudaError_t reserve_prims(int n);
-  cudaError_t build(const double* x, const int* prims, int arity, int n, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s);
+  // x1 (may be null): boxes swept from positions x to x1
+  cudaError_t build(const double* x, const double* x1, const int* prims, int arity, int n, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s);
   // kind 0: vertices against triangles; kind 1: edges against edges.
-  cudaError_t query(const double* x, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out, DevBuf<int2>& scratch,
+  cudaError_t query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out, DevBuf<int2>& scratch,
                     DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1, DevBuf<int>& counter,
                     DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
 };

@@ -143,7 +143,9 @@ def c3(seed: int = 0, scenes: int = 64, frames: int = 60) -> List[Scene]:
 
 def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
     """Two 2 m curtains (n x n each) 3 mm apart in y, top rows pinned and driven +-0.3 m along x at 0.5 Hz
-    in opposite phase. The reference has no call to move a pin, so the pin set is rebuilt every frame."""
+    in opposite phase. The reference has no call to move a pin, so the pin set is rebuilt every frame.
+    The drive amplitude ramps in with a smoothstep over the first 0.5 s: started at full amplitude the
+    pinned rows would jump two edge lengths (1.6 cm at n = 256) in the first frame."""
     rng = np.random.default_rng(seed)
     verts, tris, top = [], [], []
     for k in range(2):
@@ -160,11 +162,13 @@ def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
 
     def schedule(frame: int):
         t = (frame + 1) * dt
+        r = min(1.0, t / 0.5)
+        ramp = r * r * (3.0 - 2.0 * r)
         out = []
         for i in top:
             sgn = 1.0 if i < half else -1.0
             tgt = base[i].copy()
-            tgt[0] += sgn * 0.3 * math.sin(2 * math.pi * 0.5 * t)
+            tgt[0] += sgn * 0.3 * ramp * math.sin(2 * math.pi * 0.5 * t)
             out.append((i, tgt))
         return out
 

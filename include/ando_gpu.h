@@ -120,7 +120,7 @@ typedef struct {
   int32_t strain_active;       /* strain-limit constraints active at the last gradient */
   int32_t status;              /* ando_status of the step */
   int32_t precond_fallbacks;   /* learned-preconditioner solves redone with block-Jacobi */
-  int32_t pad_;
+  int32_t graph_launched;      /* 1 when the whole step ran as one CUDA graph launch */
   double beta;
   double last_alpha;
   double device_ms;            /* device time of the step (CUDA events) */

@@ -1397,7 +1397,9 @@ template <class R> class Integrator {
 //   * line search: a conservative time of impact along the extended direction
 //     (conservative advancement with exact distances, FP64) over every pair
 //     whose swept boxes overlap, plus the exact linear time of impact of every
-//     active wall; the step taken is x += toi * d.
+//     active wall; the step taken is x += toi * d. The extended direction is
+//     first capped so that no vertex moves more than 4 mean rest edge lengths
+//     in one Newton iteration (bounds the swept boxes).
 // ======================================================================
 
 // Correct BVH query (leaves keep up to 4 primitives): the same candidate set
@@ -1718,10 +1720,18 @@ template <class R> class CorrectedIntegrator {
     return t;
   }
 
+  static R max_move(const Mesh<R>& mesh) {
+    if (mesh.edges.empty()) return std::numeric_limits<R>::max();
+    double sum = 0;
+    for (const auto& e : mesh.edges) sum += double((mesh.vertices[size_t(e.v[1])] - mesh.vertices[size_t(e.v[0])]).norm());
+    return R(4.0 * sum / double(mesh.edges.size()));
+  }
+
   static R inner_newton(const Mesh<R>& mesh, State<R>& st, const std::vector<V3<R>>& x_target, const std::vector<char>& fixed,
                         Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>& S) {
     const size_t n = st.positions.size();
     Csr<R> H_el = base_elastic(mesh);
+    const R lmax = max_move(mesh);
     for (int it = 0; it < p.max_newton_steps; ++it) {
       auto contacts = detect_corrected(mesh, st.positions, rigids, p.contact_gap_max);
       S.contacts = std::max(S.contacts, int(contacts.size()));
@@ -1737,8 +1747,14 @@ template <class R> class CorrectedIntegrator {
       S.pcg_iters += pr.iters; S.pcg_per_newton.push_back(pr.iters);
       if (!pr.converged) S.pcg_not_converged++;
       std::vector<V3<R>> ext(n);
-      for (size_t i = 0; i < n; ++i) ext[i] = fixed[i] ? V3<R>() : V3<R>(d[3 * i], d[3 * i + 1], d[3 * i + 2]) * R(1.25);
-      R alpha = toi(mesh, st.positions, ext, fixed, C, rigids);
+      R emax = 0;
+      for (size_t i = 0; i < n; ++i) {
+        ext[i] = fixed[i] ? V3<R>() : V3<R>(d[3 * i], d[3 * i + 1], d[3 * i + 2]) * R(1.25);
+        emax = std::max(emax, ext[i].norm());
+      }
+      R cap = emax > lmax ? lmax / emax : R(1);
+      if (cap < R(1)) for (auto& e : ext) e = e * cap;
+      R alpha = cap * toi(mesh, st.positions, ext, fixed, C, rigids);
       S.alphas.push_back(alpha);
       if (alpha < R(1e-8)) return R(0);
       for (size_t i = 0; i < n; ++i) if (!fixed[i]) st.positions[i] = st.positions[i] + V3<R>(d[3 * i], d[3 * i + 1], d[3 * i + 2]) * alpha;

@@ -193,21 +193,40 @@ template <class R> void bind(py::module_& m) {
 
   struct IntegratorTag {};
   py::class_<IntegratorTag>(m, "Integrator")
-      .def_static("step", [opts, stats_dict](MeshT& me, StateT& s, ConT& c, const ParT& p, py::object rigid, const std::string& lookup, const std::string& broad) {
+      .def_static("step", [opts, stats_dict](MeshT& me, StateT& s, ConT& c, const ParT& p, py::object rigid, const std::string& lookup,
+                                            const std::string& broad, const std::string& semantics) {
         Options<R> o = opts(lookup, broad);
         StepStats<R> S;
+        bool corrected = semantics == "corrected";
         auto t0 = std::chrono::steady_clock::now();
-        if (rigid.is_none()) Integrator<R>::step(me, s, c, p, nullptr, o, &S);
-        else {
-          std::vector<RB*> h; std::vector<RB> store;
-          for (auto it : rigid) { RB& b = it.cast<RB&>(); h.push_back(&b); store.push_back(b); }
-          Integrator<R>::step(me, s, c, p, &store, o, &S);
-          for (size_t i = 0; i < h.size(); ++i) *h[i] = store[i];
-        }
+        std::vector<RB*> h; std::vector<RB> store;
+        if (!rigid.is_none()) for (auto it : rigid) { RB& b = it.cast<RB&>(); h.push_back(&b); store.push_back(b); }
+        std::vector<RB>* rp = rigid.is_none() ? nullptr : &store;
+        if (corrected) CorrectedIntegrator<R>::step(me, s, c, p, rp, &S);
+        else Integrator<R>::step(me, s, c, p, rp, o, &S);
+        for (size_t i = 0; i < h.size(); ++i) *h[i] = store[i];
         double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         return stats_dict(S, secs);
       }, py::arg("mesh"), py::arg("state"), py::arg("constraints"), py::arg("params"), py::arg("rigid_bodies") = py::none(),
-         py::arg("lookup") = "indexed", py::arg("broad") = "literal")
+         py::arg("lookup") = "indexed", py::arg("broad") = "literal", py::arg("semantics") = "reference")
+      // CORRECTED stages at the current state: contacts, gradient, Hessian, time of impact
+      .def_static("corrected_system", [](const MeshT& me, StateT& s, Arr<R> x_target, py::object fixed_mask, ConT& c, const ParT& p) {
+        auto fm = py::array_t<int8_t, py::array::c_style | py::array::forcecast>::ensure(fixed_mask);
+        std::vector<char> fixed(fm.data(), fm.data() + fm.size());
+        auto contacts = detect_corrected(me, s.positions, (const std::vector<RB>*)nullptr, p.contact_gap_max);
+        Csr<R> H_el = CorrectedIntegrator<R>::base_elastic(me);
+        std::vector<R> g;
+        CorrectedIntegrator<R>::gradient(me, s, to_v3<R>(x_target), fixed, contacts, c, p, H_el, g);
+        Csr<R> H = CorrectedIntegrator<R>::assemble(me, s, fixed, contacts, c, p, H_el);
+        py::dict d; d["gradient"] = py::array_t<R>(py::ssize_t(g.size()), g.data()); d["hessian"] = csr_dict(H);
+        d["contacts"] = contacts;
+        return d;
+      })
+      .def_static("corrected_toi", [](const MeshT& me, Arr<R> x, Arr<R> ext, py::object fixed_mask, const ConT& c) {
+        auto fm = py::array_t<int8_t, py::array::c_style | py::array::forcecast>::ensure(fixed_mask);
+        std::vector<char> fixed(fm.data(), fm.data() + fm.size());
+        return CorrectedIntegrator<R>::toi(me, to_v3<R>(x), to_v3<R>(ext), fixed, c, (const std::vector<RB>*)nullptr);
+      })
       .def_static("compute_contacts", [opts](const MeshT& me, const StateT& s, py::object rigid, const std::string& broad) {
         Options<R> o = opts("indexed", broad);
         if (rigid.is_none()) return detect_all(me, s, (const std::vector<RB>*)nullptr, o.broad);

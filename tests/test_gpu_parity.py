@@ -353,3 +353,28 @@ def test_apply_gravity_kernel(core):
     x1, v1 = s.get_positions64(), s.get_velocities64()
     np.testing.assert_allclose(v1, v0 + np.array([0, 0, -9.81]) * np.float32(0.01), rtol=0, atol=1e-12)
     np.testing.assert_allclose(x1, x0 + v1 * np.float32(0.01), rtol=0, atol=1e-12)
+
+
+def test_frame_graph_matches_host_loop(abi):
+    """The whole step as one CUDA graph launch (device-side Newton and inner
+    loops) runs the same kernels in the same order as the host-driven loop, so
+    the two trajectories are bit-identical. Profiling forces the host loop."""
+    sc = small_cloth(n=18, size=0.5, z=0.02)
+    sc.vertices[:, 0] *= 1.06                    # strain limit active
+    p = abi.make_params(dict(sc.params, pcg_tol=1e-6))
+    runs = []
+    for profiled in (False, True):
+        S = abi.Scene(sc.vertices, sc.triangles, sc.material)
+        S.upload(sc.vertices, np.zeros_like(sc.vertices), sc.vertices, None)
+        S.profile_enable(profiled)
+        xs, graph = [], []
+        for f in range(12):
+            S.apply_gravity(sc.gravity, p.dt)
+            st = S.step(p, [(0, sc.vertices[0])], sc.walls)
+            graph.append(st["graph_launched"])
+            xs.append(S.download()[0])
+        S.close()
+        runs.append((xs, graph))
+    assert all(runs[0][1]) and not any(runs[1][1])
+    for a, b in zip(runs[0][0], runs[1][0]):
+        np.testing.assert_array_equal(a, b)
