@@ -26,7 +26,7 @@ EXPORTED = [
     "ando_mesh_upload", "ando_mesh_set_vertices", "ando_state_upload", "ando_state_download",
     "ando_apply_gravity", "ando_step", "ando_compute_contacts", "ando_last_system", "ando_eval_system",
     "ando_last_gradient", "ando_last_contact_blocks", "ando_profile_enable", "ando_profile_read", "ando_ctx_stream",
-    "ando_broad_phase",
+    "ando_broad_phase", "ando_pcg_solve_noalloc",
 ]
 
 PHASES = ["setup", "strain", "gradient", "assemble", "pcg", "line_search", "finish"]
@@ -151,6 +151,8 @@ def lib() -> C.CDLL:
     L.ando_profile_read.restype = I32; L.ando_profile_read.argtypes = [P, C.POINTER(Profile)]
     L.ando_ctx_stream.restype = I32; L.ando_ctx_stream.argtypes = [P, C.POINTER(C.c_void_p)]
     L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
+    L.ando_pcg_solve_noalloc.restype = I32
+    L.ando_pcg_solve_noalloc.argtypes = [I32, P, I32, P, P, P, P, P, P, C.c_int64, D, I32, pi, pi, pd]
     _lib = L
     return L
 

@@ -36,6 +36,18 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+}  // namespace
+
+namespace ando {
+// Error reporting for entry points defined in other translation units.
+int set_last_error(int code, const char* msg) {
+  g_last_error = msg;
+  return code;
+}
+}  // namespace ando
+
+namespace {
+
 #define CK(call)                                                                                   \
   do {                                                                                             \
     cudaError_t e_ = (call);                                                                       \

@@ -250,6 +250,38 @@ ANDO_API int32_t ando_ctx_stream(ando_ctx ctx, void** stream);
 /* Newton gradient (FP64, 3*num_vertices) of the most recent Newton iteration. */
 ANDO_API int32_t ando_last_gradient(ando_ctx ctx, double* gradient, int32_t num_vertices);
 
+/* Largest system ando_pcg_solve_noalloc accepts (3 * num_rows must fit int32). */
+#define ANDO_NOALLOC_MAX_ROWS 715827882
+
+/* Block-Jacobi PCG on a caller-owned 3x3-block BSR system that allocates no
+ * device memory. No reference counterpart: the reference's PCGSolver::solve
+ * (pcg_solver.cpp:8-146) allocates its vectors on every call. It is for
+ * callers that cannot allocate at solve time: a host that hands out all device
+ * memory from its own fixed arena, or one that cannot take the device-wide
+ * synchronisation of cudaFree between frames. The iteration is the one
+ * ando_step runs (x0 = 0, stop when |r|_inf < tol * |b|_inf, FP64 dots).
+ *
+ * Device pointers: rowptr (num_rows+1), cols (sorted per row), vals (9 floats
+ * per block, row-major), rhs (3*num_rows), x (3*num_rows, overwritten) and
+ * work (>= 24*num_rows floats, any contents; larger sizes are rejected with
+ * ANDO_ERR_CAPACITY, as are num_rows > ANDO_NOALLOC_MAX_ROWS). `stream` is a
+ * cudaStream_t of `device` (NULL = legacy default stream). Reduction partials
+ * and grid-barrier words live in a 16 KiB static device array per device
+ * (partials for up to 640 CTAs; the grid is capped there); the call zeroes its
+ * control words itself, so nothing has to start at zero.
+ *
+ * The first call on a device looks up that array's device address and the
+ * kernel's grid size (which may load the module): make it before any stream
+ * capture. Calls on one device share the scratch, so overlapping calls (other
+ * streams or threads without ordering) race; serialise them. With all three
+ * outputs NULL the call is asynchronous on `stream`; otherwise it synchronises
+ * `stream` and reports iterations, the PCG status (0 converged, 1 max
+ * iterations, 2 not SPD, 3 barrier timeout) and the final relative residual. */
+ANDO_API int32_t ando_pcg_solve_noalloc(int32_t device, void* stream, int32_t num_rows, const int32_t* rowptr,
+                                        const int32_t* cols, const float* vals, const float* rhs, float* x, float* work,
+                                        int64_t work_floats, double tol, int32_t max_iters, int32_t* iterations,
+                                        int32_t* pcg_status, double* rel_residual);
+
 #ifdef __cplusplus
 }
 #endif
