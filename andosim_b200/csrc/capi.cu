@@ -20,6 +20,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "../../include/ando_gpu.h"
 #include "kernels.cuh"
@@ -76,11 +77,22 @@ struct ando_ctx_s {
   DevBuf<double> partials;
   Ctrl* ctrl_host = nullptr;
 
+  // block-scaled system of the CORRECTED step (L = chol(A_ii), A^ = L^-1 A L^-T)
+  DevBuf<double> Linv, xh;
+  DevBuf<float> Lf, bhat, valh, xvalh, r2;
+  DevBuf<unsigned char> chol_ok;
+  int pcg_scaled_grid = 1, pcg_learned_grid = 1;
+
   // contacts
   DevBuf<int> det_counts, det_offsets;
-  DevBuf<ContactDev> contacts;
+  DevBuf<ContactDev> contacts, contacts_all;
   int ncontacts = 0, n_pe = 0;
+  int* ctrl_host_count = nullptr;  // pinned int for small device -> host counts
   DevBuf<int> ekeys, ekeys_sorted, ebegin, eend, xflags, xkeys, xcols, xbegin, xend, nsel;
+  // merged extra blocks: 64-bit row:col keys, entry indices, run heads, block rows
+  DevBuf<unsigned long long> xk0, xk1;
+  DevBuf<int> xi0, xi1, xheads, xrow;
+  int nx_raw = 0;
   DevBuf<ContactEntry> ents, ents_sorted, xent;
   DevBuf<float> xval;
   int nx = 0, nent = 0;
@@ -133,6 +145,7 @@ struct ando_ctx_s {
     for (auto* b : body_world) delete b;
     for (auto* b : body_tris) delete b;
     if (ctrl_host) cudaFreeHost(ctrl_host);
+    if (ctrl_host_count) cudaFreeHost(ctrl_host_count);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -180,6 +193,10 @@ struct ando_ctx_s {
 };
 
 namespace {
+struct ActiveContact {
+  __device__ bool operator()(const ContactDev& c) const { return c.type >= 0; }
+};
+
 // Times the launches issued while it is alive (one phase) and counts them.
 struct Phase {
   ando_ctx c; int phase; cudaEvent_t a = nullptr;
@@ -272,12 +289,12 @@ int prepare_contacts(ando_ctx c, const StepParams& sp, const double* g_base, con
   CK(c->ents.reserve(ne + 1)); CK(c->ents_sorted.reserve(ne + 1));
   CK(c->ebegin.reserve(V)); CK(c->eend.reserve(V));
   CK(c->xflags.reserve(ne + 1)); CK(c->xkeys.reserve(ne + 1)); CK(c->xent.reserve(ne + 1));
-  CK(c->xcols.reserve(ne + 1)); CK(c->xval.reserve(9ull * (ne + 1))); CK(c->xbegin.reserve(V)); CK(c->xend.reserve(V));
+  CK(c->xbegin.reserve(V)); CK(c->xend.reserve(V)); CK(c->xrow.reserve(1)); CK(c->xcols.reserve(1)); CK(c->xval.reserve(9));
   CK(c->nsel.reserve(1));
   if (ne == 0) {
     CK(cudaMemsetAsync(c->ebegin.p, 0, sizeof(int) * V, c->stream));
     CK(cudaMemsetAsync(c->eend.p, 0, sizeof(int) * V, c->stream));
-    c->nx = 0;
+    c->nx = 0; c->nx_raw = 0;
     launch_contact_vertex(m, c->contacts.p, c->ents_sorted.p, c->ebegin.p, c->eend.p, sp, g_base, c->g_const.p, c->diag_const.p, c->stream);
     ph.launched();
     CK(cudaGetLastError());
@@ -301,12 +318,37 @@ int prepare_contacts(ando_ctx c, const StepParams& sp, const double* g_base, con
   CK(c->cub_reserve(bytes));
   CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, c->ents_sorted.p, c->xflags.p, c->xent.p, c->nsel.p, ne, c->stream));
   CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, c->ekeys_sorted.p, c->xflags.p, c->xkeys.p, c->nsel.p, ne, c->stream));
-  int nx = 0;
-  CK(cudaMemcpyAsync(&nx, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->ctrl_host_count, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  c->nx = nx;
-  if (nx) { launch_extra_values(c->contacts.p, c->xent.p, c->xkeys.p, fixed, c->xcols.p, nx, sp, c->xval.p, c->stream); ph.launched(); }
-  launch_vertex_ranges(c->xkeys.p, nx, V, c->xbegin.p, c->xend.p, c->stream);
+  int nraw = *c->ctrl_host_count, nu = 0;
+  c->nx_raw = nraw;
+  if (nraw) {
+    // merge the entries of each (row, col) into one block: sort by row:col
+    // (stable, so entries stay in contact order inside a block), then one
+    // thread per run of equal keys
+    CK(c->xk0.reserve(nraw)); CK(c->xk1.reserve(nraw)); CK(c->xi0.reserve(nraw)); CK(c->xi1.reserve(nraw)); CK(c->xheads.reserve(nraw));
+    launch_extra_key64(c->xent.p, c->xkeys.p, nraw, c->xk0.p, c->xi0.p, c->stream);
+    bytes = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, c->xk0.p, c->xk1.p, c->xi0.p, c->xi1.p, nraw, 0, 32 + bits, c->stream));
+    CK(c->cub_reserve(bytes));
+    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, bytes, c->xk0.p, c->xk1.p, c->xi0.p, c->xi1.p, nraw, 0, 32 + bits, c->stream));
+    launch_run_heads(c->xk1.p, nraw, c->xflags.p, c->stream);
+    bytes = 0;
+    thrust::counting_iterator<int> iota(0);
+    CK(cub::DeviceSelect::Flagged(nullptr, bytes, iota, c->xflags.p, c->xheads.p, c->nsel.p, nraw, c->stream));
+    CK(c->cub_reserve(bytes));
+    CK(cub::DeviceSelect::Flagged(c->cub_tmp.p, bytes, iota, c->xflags.p, c->xheads.p, c->nsel.p, nraw, c->stream));
+    CK(cudaMemcpyAsync(c->ctrl_host_count, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    nu = *c->ctrl_host_count;
+    CK(c->xrow.reserve(nu)); CK(c->xcols.reserve(nu)); CK(c->xval.reserve(9ull * nu));
+    if (sp.semantics == ANDO_SEMANTICS_CORRECTED) CK(c->xvalh.reserve(9ull * nu));
+    launch_extra_merge(c->contacts.p, c->xent.p, c->xk1.p, c->xi1.p, c->xheads.p, nu, nraw, fixed, sp, nullptr, c->xrow.p, c->xcols.p,
+                       c->xval.p, nullptr, c->stream);
+    ph.launched(4);
+  }
+  c->nx = nu;
+  launch_vertex_ranges(c->xrow.p, nu, V, c->xbegin.p, c->xend.p, c->stream);
   ph.launched();
   CK(cudaGetLastError());
   return ANDO_OK;
@@ -434,19 +476,32 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
     if (rc) return rc;
     nr = c->ncontacts;
   }
+  // Candidate pairs become contacts; only those inside the activation
+  // distance carry a barrier term, so the rest are dropped here (stable
+  // compaction keeps the candidates' sorted order).
+  int na = 0;
   CK(c->contacts.reserve(size_t(nvt) + nee + nr + 1));
+  if (nvt + nee) {
+    Phase ph(c, ANDO_PHASE_SETUP);
+    CK(c->contacts_all.reserve(size_t(nvt) + nee));
+    CK(c->nsel.reserve(1));
+    launch_pairs_to_contacts(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, gap_max, c->contacts_all.p, s);
+    size_t bytes = 0;
+    CK(cub::DeviceSelect::If(nullptr, bytes, c->contacts_all.p, c->contacts.p, c->nsel.p, nvt + nee, ActiveContact(), s));
+    CK(c->cub_reserve(bytes));
+    CK(cub::DeviceSelect::If(c->cub_tmp.p, bytes, c->contacts_all.p, c->contacts.p, c->nsel.p, nvt + nee, ActiveContact(), s));
+    CK(cudaMemcpyAsync(c->ctrl_host_count, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    na = *c->ctrl_host_count;
+    ph.launched(2);
+  }
   if (nb > 0 && nr) {
     MeshDev m = c->mesh_dev();
     Phase ph(c, ANDO_PHASE_SETUP);
-    launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, 0, gap_max, c->det_offsets.p, c->contacts.p + nvt + nee, s);
+    launch_detect_write(m, c->x.p, c->bodies_dev.p, nb, 0, gap_max, c->det_offsets.p, c->contacts.p + na, s);
     ph.launched();
   }
-  if (nvt + nee) {
-    Phase ph(c, ANDO_PHASE_SETUP);
-    launch_pairs_to_contacts(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, gap_max, c->contacts.p, s);
-    ph.launched();
-  }
-  c->ncontacts = nvt + nee + nr;
+  c->ncontacts = na + nr;
   c->n_pe = 0;
   CK(cudaGetLastError());
   return ANDO_OK;
@@ -505,14 +560,32 @@ int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, i
   return ANDO_OK;
 }
 
+// Assembly of the CORRECTED Newton system: the unscaled BSR values (kept for
+// ando_last_system), the block Cholesky factors of the diagonal and the
+// scaled system A^ = L^-1 A L^-T with its right-hand side.
+void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
+  MeshDev m = c->mesh_dev();
+  launch_diag_factor(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->g.p, c->Linv.p, c->Lf.p, c->bhat.p,
+                     c->chol_ok.p, c->ctrl.p, s);
+  launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p, c->val.p,
+                         c->valh.p, c->ctrl.p, s);
+  if (c->nx) launch_extra_merge(c->contacts.p, c->xent.p, c->xk1.p, c->xi1.p, c->xheads.p, c->nx, c->nx_raw, c->fixed.p, sp, c->Linv.p,
+                                nullptr, nullptr, nullptr, c->xvalh.p, s);
+}
+
+PcgScaledArgs scaled_args(ando_ctx c, const ando_params& p) {
+  PcgScaledArgs a;
+  a.V = c->V; a.rowptr = c->rowptr.p; a.cols = c->cols.p; a.valh = c->valh.p;
+  a.xbegin = c->nx ? c->xbegin.p : nullptr; a.xend = c->nx ? c->xend.p : nullptr; a.xcols = c->xcols.p; a.xvalh = c->xvalh.p;
+  a.S = nullptr; a.Linv = c->Linv.p; a.Lf = c->Lf.p; a.bhat = c->bhat.p; a.d = c->d.p;
+  a.xh = c->xh.p; a.r = c->r.p; a.r2 = c->r2.p; a.z = c->z.p; a.p0 = c->p0.p; a.p1 = c->p1.p; a.Ap = c->Ap.p;
+  a.partials = c->partials.p; a.ctrl = c->ctrl.p; a.tol = float(p.pcg_tol); a.max_iters = p.pcg_max_iters; a.stall_window = 50;
+  return a;
+}
+
 // inner_newton_step with the CORRECTED terms and line search.
 int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& sp, int nb, ando_step_stats& st, double& ret) {
-  MeshDev m = c->mesh_dev();
   cudaStream_t s = c->stream;
-  PcgArgs pa;
-  pa.V = c->V; pa.rowptr = c->rowptr.p; pa.cols = c->cols.p; pa.val = c->val.p;
-  pa.P = c->precond.p; pa.b = c->b.p; pa.x = c->d.p; pa.r = c->r.p; pa.z = c->z.p; pa.p0 = c->p0.p; pa.p1 = c->p1.p; pa.Ap = c->Ap.p;
-  pa.partials = c->partials.p; pa.ctrl = c->ctrl.p; pa.tol = float(p.pcg_tol); pa.max_iters = p.pcg_max_iters;
   for (int it = 0; it < p.max_newton_steps; ++it) {
     int rc = corrected_gradient(c, p, sp, nb);
     if (rc) return rc;
@@ -522,15 +595,15 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
     st.strain_active = c->ctrl_host->strain_active;
     st.contacts = std::max(st.contacts, c->ncontacts);
     if (c->ctrl_host->converged) { ret = 1.0; return ANDO_OK; }
-    pa.xbegin = c->nx ? c->xbegin.p : nullptr; pa.xend = c->nx ? c->xend.p : nullptr; pa.xcols = c->xcols.p; pa.xval = c->xval.p;
     {
       Phase ph(c, ANDO_PHASE_ASSEMBLE);
-      launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->val.p, c->precond.p, c->ctrl.p, s);
-      ph.launched();
+      enqueue_scaled_assembly(c, sp, s);
+      ph.launched(c->nx ? 3 : 2);
     }
     {
       Phase ph(c, ANDO_PHASE_PCG);
-      CK(launch_pcg(pa, c->pcg_grid, s));
+      PcgScaledArgs sa = scaled_args(c, p);
+      CK(launch_pcg_scaled(sa, false, c->pcg_scaled_grid, s));
       ph.launched();
     }
     rc = corrected_line_search(c, nb);
@@ -827,6 +900,7 @@ int32_t ando_ctx_create(int32_t device, ando_ctx* out) {
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e == cudaSuccess) e = cudaMallocHost(&c->ctrl_host, sizeof(Ctrl));
   if (e == cudaSuccess) e = cudaMallocHost(&c->sctl_host, sizeof(StepCtl));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->ctrl_host_count, sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap2, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap3, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = c->sctl.reserve(1);
@@ -834,7 +908,9 @@ int32_t ando_ctx_create(int32_t device, ando_ctx* out) {
   if (e == cudaSuccess) e = cudaMemset(c->ctrl.p, 0, sizeof(Ctrl));
   if (e != cudaSuccess) { delete c; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
   c->pcg_grid = pcg_grid_size(device);
-  e = c->partials.reserve(3ull * std::max(c->pcg_grid, 1));
+  c->pcg_scaled_grid = pcg_scaled_grid_size(device, false);
+  c->pcg_learned_grid = pcg_scaled_grid_size(device, true);
+  e = c->partials.reserve(3ull * std::max(std::max(c->pcg_grid, c->pcg_scaled_grid), std::max(c->pcg_learned_grid, 1)));
   if (e != cudaSuccess) { delete c; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
   *out = c;
   return ANDO_OK;
@@ -935,6 +1011,8 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->b.reserve(3ull * V)); CK(c->d.reserve(3ull * V)); CK(c->r.reserve(3ull * V)); CK(c->z.reserve(3ull * V));
   CK(c->p0.reserve(3ull * V)); CK(c->p1.reserve(3ull * V)); CK(c->Ap.reserve(3ull * V));
   CK(c->val.reserve(9ull * nnzb)); CK(c->precond.reserve(9ull * V));
+  CK(c->Linv.reserve(6ull * V)); CK(c->Lf.reserve(6ull * V)); CK(c->bhat.reserve(3ull * V)); CK(c->chol_ok.reserve(V));
+  CK(c->valh.reserve(9ull * nnzb)); CK(c->xh.reserve(3ull * V)); CK(c->r2.reserve(3ull * V));
   CK(c->sflags.reserve(std::max(T, 1))); CK(c->sv.reserve(2ull * std::max(T, 1)));
   CK(c->emax_cap.reserve(2));
   {
@@ -1121,7 +1199,7 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
     if (rc) return rc;
     rc = corrected_gradient(c, p, sp, num_rigids);
     if (rc) return rc;
-    launch_assemble(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->val.p, c->precond.p, c->ctrl.p, s);
+    enqueue_scaled_assembly(c, sp, s);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
     return ANDO_OK;
@@ -1221,7 +1299,7 @@ int32_t ando_last_contact_blocks(ando_ctx c, int32_t* count, int32_t* rows, int3
   *count = c->nx;
   cudaStream_t s = c->stream;
   if (c->nx) {
-    if (rows) CK(cudaMemcpyAsync(rows, c->xkeys.p, sizeof(int) * c->nx, cudaMemcpyDeviceToHost, s));
+    if (rows) CK(cudaMemcpyAsync(rows, c->xrow.p, sizeof(int) * c->nx, cudaMemcpyDeviceToHost, s));
     if (cols) CK(cudaMemcpyAsync(cols, c->xcols.p, sizeof(int) * c->nx, cudaMemcpyDeviceToHost, s));
     if (vals) CK(cudaMemcpyAsync(vals, c->xval.p, sizeof(float) * 9ull * c->nx, cudaMemcpyDeviceToHost, s));
   }

@@ -99,6 +99,9 @@ struct MeshDev {
 // Strain-limit data of one face and one singular value.
 struct StrainSV { double J[9]; double dV, d2V; };
 
+// Lower-triangular 3x3 (Cholesky factor or its inverse), row-major packed.
+struct Tri3 { double l00, l10, l11, l20, l21, l22; };
+
 // -------------------------------------------------------- device control
 struct Ctrl {
   unsigned long long gnorm_bits;  // max |g| as IEEE bits (non-negative doubles order as integers)
@@ -112,7 +115,10 @@ struct Ctrl {
   int pad;
 };
 
-enum PcgStatus { PCG_OK = 0, PCG_MAXIT = 1, PCG_NOT_SPD = 2, PCG_TIMEOUT = 3, PCG_SKIPPED = 4 };
+// PCG_PRECOND: the learned preconditioner lost positive definiteness
+// (r^T z <= 0); PCG_STALL: its residual stopped improving. Both hand the
+// solve back to block-Jacobi.
+enum PcgStatus { PCG_OK = 0, PCG_MAXIT = 1, PCG_NOT_SPD = 2, PCG_TIMEOUT = 3, PCG_SKIPPED = 4, PCG_PRECOND = 5, PCG_STALL = 6 };
 
 // Device-side control of one step (integrator.cpp:98-121 and 152-236) when the
 // whole frame runs as one CUDA graph: the beta loop, the error-reduction pass

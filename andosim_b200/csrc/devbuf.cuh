@@ -1,4 +1,7 @@
 // devbuf.cuh -- owning device buffer that only grows (host-side helper).
+// A buffer that has to grow takes at least 1.5x its old capacity, so sizes
+// that creep up step by step (contacts, pairs) reallocate rarely: cudaFree
+// synchronises the whole device.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,8 +19,8 @@ template <class T> struct DevBuf {
   ~DevBuf() { if (p) cudaFree(p); }
   cudaError_t reserve(size_t count) {
     if (count <= n && p) return cudaSuccess;
-    if (p) { cudaFree(p); p = nullptr; n = 0; }
     size_t c = count ? count : 1;
+    if (p) { c = c > n + n / 2 ? c : n + n / 2; cudaFree(p); p = nullptr; n = 0; }
     cudaError_t e = cudaMalloc(&p, c * sizeof(T));
     if (e == cudaSuccess) n = c;
     return e;

@@ -400,24 +400,6 @@ __global__ void k_extra_flags(const ContactEntry* ents, const int* keys, int n, 
   flags[k] = (E.col >= 0 && E.col != keys[k] && !(E.li & 16)) ? 1 : 0;
 }
 
-__global__ void k_extra_values(const ContactDev* cs, const ContactEntry* xent, const int* xkeys, const unsigned char* fixed, int* xcols, int nx,
-                               StepParams p, float* xval) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nx) return;
-  ContactEntry E = xent[k];
-  xcols[k] = E.col;
-  if (fixed && (fixed[xkeys[k]] || fixed[E.col])) { for (int q = 0; q < 9; ++q) xval[9 * k + q] = 0.f; return; }
-  const ContactDev& C = cs[E.contact];
-  int i = E.li & 3, j = E.lj;
-  d3 n = mk(C.nn[0], C.nn[1], C.nn[2]);
-  d3 gi = n * C.w[i], gj = n * C.w[j];
-  for (int r = 0; r < 3; ++r)
-    for (int q = 0; q < 3; ++q) {
-      double val = C.d2V * (comp(gi, r) * comp(gj, q));
-      xval[9 * k + r * 3 + q] = fabs(val) < p.barrier_tol ? 0.0f : float(val);
-    }
-}
-
 // ---------------------------------------------------------- Newton iteration
 __global__ void k_ctrl_reset(Ctrl* c) {
   c->gnorm_bits = 0ull; c->ls_mask = (1u << 20) - 1u; c->converged = 0;
@@ -666,20 +648,13 @@ __global__ void k_check(Ctrl* c, double tol) {
 // diagonal slot the vertex's diagonal terms. Every contribution is symmetric
 // by construction, so the reference's (H + H^T)/2 leaves it unchanged. The
 // diagonal slot also yields the block-Jacobi inverse (pcg_solver.cpp:77-114).
-__global__ void k_assemble(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
-                           const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl) {
-  if (ctrl->converged) return;
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= m.nnzb) return;
-  int row = m.slot_row[s], col = m.cols[s];
-  if (fixed && (fixed[row] || fixed[col])) {
-    // kinematic pin: decoupled row and column, unit diagonal (diag_extra holds I)
-    float one = row == col ? 1.f : 0.f;
-    for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = (k % 4 == 0) ? one : 0.f;
-    if (row == col) for (int k = 0; k < 9; ++k) precond[9 * (long long)row + k] = (k % 4 == 0) ? 1.f : 0.f;
-    return;
-  }
-  double H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+// FP64 Hessian block of BSR slot s (row, col): the constant elastic block,
+// the strain-limit blocks of the faces sharing the slot (face order;
+// StrainLimiting::accumulate_hessian drop rules) and, for a diagonal slot, the
+// vertex's diagonal terms.
+__device__ inline void slot_block(const MeshDev& m, int s, int row, int col, const unsigned char* sflags, const StrainSV* sv,
+                                  const double* diag_extra, int enable_strain, double H[9]) {
+  for (int k = 0; k < 9; ++k) H[k] = 0.0;
   H[0] = H[4] = m.el_a[s]; H[8] = m.el_b[s];
   if (enable_strain) {
     for (int k = m.slot_cptr[s]; k < m.slot_cptr[s + 1]; ++k) {
@@ -700,6 +675,23 @@ __global__ void k_assemble(MeshDev m, const unsigned char* sflags, const StrainS
     }
   }
   if (row == col) for (int k = 0; k < 9; ++k) H[k] += diag_extra[9 * row + k];
+}
+
+__global__ void k_assemble(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                           const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl) {
+  if (ctrl->converged) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= m.nnzb) return;
+  int row = m.slot_row[s], col = m.cols[s];
+  if (fixed && (fixed[row] || fixed[col])) {
+    // kinematic pin: decoupled row and column, unit diagonal (diag_extra holds I)
+    float one = row == col ? 1.f : 0.f;
+    for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = (k % 4 == 0) ? one : 0.f;
+    if (row == col) for (int k = 0; k < 9; ++k) precond[9 * (long long)row + k] = (k % 4 == 0) ? 1.f : 0.f;
+    return;
+  }
+  double H[9];
+  slot_block(m, s, row, col, sflags, sv, diag_extra, enable_strain, H);
   float hf[9];
   for (int k = 0; k < 9; ++k) { hf[k] = float(H[k]); val[9 * (long long)s + k] = hf[k]; }
   if (row == col) {
@@ -717,6 +709,180 @@ __global__ void k_assemble(MeshDev m, const unsigned char* sflags, const StrainS
     } else {
       P[0] = 1.f; P[1] = 0.f; P[2] = 0.f; P[3] = 0.f; P[4] = 1.f; P[5] = 0.f; P[6] = 0.f; P[7] = 0.f; P[8] = 1.f;
     }
+  }
+}
+
+// ------------------------------------------------ scaled system (CORRECTED)
+// Symmetric block scaling of the Newton system: with A_ii = L_i L_i^T (FP64
+// Cholesky of the assembled diagonal block) the PCG runs on
+// A^ = L^-1 A L^-T, whose diagonal blocks are I. Block-Jacobi PCG on A and CG
+// on A^ are the same iteration in exact arithmetic. In FP32 they are not:
+// contact and strain barriers make some diagonal blocks 1e10 times stiffer
+// than the mass block next to them, FP32 sums over such a row cancel, and the
+// unscaled iteration stalls; every stored entry of A^ is O(1). The scaling is
+// applied in FP64, before the single rounding to FP32.
+__device__ inline bool chol3(const double H[9], Tri3& L) {
+  double a = H[0];
+  if (!(a > 0.0)) return false;
+  L.l00 = sqrt(a);
+  L.l10 = H[3] / L.l00; L.l20 = H[6] / L.l00;
+  double b = H[4] - L.l10 * L.l10;
+  if (!(b > 0.0)) return false;
+  L.l11 = sqrt(b);
+  L.l21 = (H[7] - L.l20 * L.l10) / L.l11;
+  double c = H[8] - L.l20 * L.l20 - L.l21 * L.l21;
+  if (!(c > 0.0)) return false;
+  L.l22 = sqrt(c);
+  return true;
+}
+__device__ inline Tri3 tri_inv(const Tri3& L) {
+  Tri3 M;
+  M.l00 = 1.0 / L.l00; M.l11 = 1.0 / L.l11; M.l22 = 1.0 / L.l22;
+  M.l10 = -L.l10 * M.l00 * M.l11;
+  M.l21 = -L.l21 * M.l11 * M.l22;
+  M.l20 = -(L.l20 * M.l00 + L.l21 * M.l10) * M.l22;
+  return M;
+}
+// R = Mr H Mc^T with Mr, Mc lower triangular.
+__device__ inline void scale_block(const Tri3& Mr, const double H[9], const Tri3& Mc, double R[9]) {
+  double T[9];
+  for (int c = 0; c < 3; ++c) {
+    T[0 + c] = Mr.l00 * H[c];
+    T[3 + c] = Mr.l10 * H[c] + Mr.l11 * H[3 + c];
+    T[6 + c] = Mr.l20 * H[c] + Mr.l21 * H[3 + c] + Mr.l22 * H[6 + c];
+  }
+  for (int r = 0; r < 3; ++r) {
+    const double* t = T + 3 * r;
+    R[3 * r + 0] = t[0] * Mc.l00;
+    R[3 * r + 1] = t[0] * Mc.l10 + t[1] * Mc.l11;
+    R[3 * r + 2] = t[0] * Mc.l20 + t[1] * Mc.l21 + t[2] * Mc.l22;
+  }
+}
+__device__ inline Tri3 ld_tri(const double* p, int i) {
+  const double* q = p + 6 * (long long)i;
+  Tri3 t; t.l00 = q[0]; t.l10 = q[1]; t.l11 = q[2]; t.l20 = q[3]; t.l21 = q[4]; t.l22 = q[5];
+  return t;
+}
+
+// Per vertex: the FP64 diagonal block, its Cholesky factor L (a shifted
+// factorisation when rounding made the block indefinite), L^-1 in FP64, L in
+// FP32 (for the unscaled residual norm) and the scaled right-hand side
+// b^ = -L^-1 g.
+__global__ void k_diag_factor(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                              const unsigned char* fixed, const double* g, double* Linv, float* Lf, float* bhat,
+                              unsigned char* chol_ok, const Ctrl* ctrl) {
+  if (ctrl->converged) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.V) return;
+  double H[9];
+  if (fixed && fixed[i]) {
+    for (int k = 0; k < 9; ++k) H[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  } else {
+    slot_block(m, m.diag_slot[i], i, i, sflags, sv, diag_extra, enable_strain, H);
+  }
+  Tri3 L;
+  bool ok = chol3(H, L);
+  if (!ok) {
+    double tr = fabs(H[0]) + fabs(H[4]) + fabs(H[8]) + 1e-300;
+    bool done = false;
+    for (int t = 0; t < 3 && !done; ++t) {
+      double Hs[9];
+      for (int k = 0; k < 9; ++k) Hs[k] = H[k];
+      double sh = tr * (t == 0 ? 1e-12 : (t == 1 ? 1e-8 : 1e-4));
+      Hs[0] += sh; Hs[4] += sh; Hs[8] += sh;
+      done = chol3(Hs, L);
+    }
+    if (!done) {
+      L.l00 = sqrt(fmax(fabs(H[0]), 1e-300)); L.l11 = sqrt(fmax(fabs(H[4]), 1e-300)); L.l22 = sqrt(fmax(fabs(H[8]), 1e-300));
+      L.l10 = L.l20 = L.l21 = 0.0;
+    }
+  }
+  Tri3 M = tri_inv(L);
+  double* q = Linv + 6 * (long long)i;
+  q[0] = M.l00; q[1] = M.l10; q[2] = M.l11; q[3] = M.l20; q[4] = M.l21; q[5] = M.l22;
+  float* lf = Lf + 6 * (long long)i;
+  lf[0] = float(L.l00); lf[1] = float(L.l10); lf[2] = float(L.l11); lf[3] = float(L.l20); lf[4] = float(L.l21); lf[5] = float(L.l22);
+  chol_ok[i] = ok ? 1 : 0;
+  d3 gi = ld3(g, i);
+  bhat[3 * i] = float(-(M.l00 * gi.x));
+  bhat[3 * i + 1] = float(-(M.l10 * gi.x + M.l11 * gi.y));
+  bhat[3 * i + 2] = float(-(M.l20 * gi.x + M.l21 * gi.y + M.l22 * gi.z));
+}
+
+// Per slot: the unscaled block (val, FP32; optional) and the scaled block
+// valh = L_row^-1 H L_col^-T (FP32, computed in FP64). Diagonal slots of
+// factored rows are exactly I.
+__global__ void k_assemble_scaled(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                                  const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
+                                  const Ctrl* ctrl) {
+  if (ctrl->converged) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= m.nnzb) return;
+  int row = m.slot_row[s], col = m.cols[s];
+  float* vh = valh + 9 * (long long)s;
+  if (fixed && (fixed[row] || fixed[col])) {
+    float one = row == col ? 1.f : 0.f;
+    for (int k = 0; k < 9; ++k) { float v = (k % 4 == 0) ? one : 0.f; vh[k] = v; if (val) val[9 * (long long)s + k] = v; }
+    return;
+  }
+  double H[9];
+  slot_block(m, s, row, col, sflags, sv, diag_extra, enable_strain, H);
+  if (val) for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = float(H[k]);
+  if (row == col && chol_ok[row]) {
+    for (int k = 0; k < 9; ++k) vh[k] = (k % 4 == 0) ? 1.f : 0.f;
+    return;
+  }
+  double R[9];
+  scale_block(ld_tri(Linv, row), H, ld_tri(Linv, col), R);
+  for (int k = 0; k < 9; ++k) vh[k] = float(R[k]);
+}
+
+// Contact blocks outside the static pattern. Entries of the same (row, col)
+// arrive adjacent (sorted by the 64-bit key row:col, stably, so in contact
+// order) and merge into one block: the FP64 sum of k_extra_values' per-entry
+// blocks, each with its |v| < barrier_tol drop rule. With Linv the merged
+// block is scaled (L_row^-1 H L_col^-T) before the rounding to FP32.
+__global__ void k_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  key[k] = ((unsigned long long)(unsigned)xkeys[k] << 32) | (unsigned long long)(unsigned)xent[k].col;
+  idx[k] = k;
+}
+__global__ void k_run_heads(const unsigned long long* key, int n, int* flags) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  flags[k] = (k == 0 || key[k] != key[k - 1]) ? 1 : 0;
+}
+__global__ void k_extra_merge(const ContactDev* cs, const ContactEntry* xent, const unsigned long long* key, const int* idx, const int* heads,
+                              int nu, int n, const unsigned char* fixed, StepParams p, const double* Linv, int* xrow, int* xcols,
+                              float* xval, float* xvalh) {
+  int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nu) return;
+  int k0 = heads[u], k1 = u + 1 < nu ? heads[u + 1] : n;
+  int row = int(key[k0] >> 32), col = int(key[k0] & 0xffffffffull);
+  if (xrow) { xrow[u] = row; xcols[u] = col; }
+  double H[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  bool zero = fixed && (fixed[row] || fixed[col]);
+  if (!zero) {
+    for (int k = k0; k < k1; ++k) {
+      ContactEntry E = xent[idx[k]];
+      const ContactDev& C = cs[E.contact];
+      int i = E.li & 3, j = E.lj;
+      d3 nn = mk(C.nn[0], C.nn[1], C.nn[2]);
+      d3 gi = nn * C.w[i], gj = nn * C.w[j];
+      for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q) {
+          double v = C.d2V * (comp(gi, r) * comp(gj, q));
+          if (!(fabs(v) < p.barrier_tol)) H[3 * r + q] += v;
+        }
+    }
+  }
+  if (xval) for (int q = 0; q < 9; ++q) xval[9 * (long long)u + q] = float(H[q]);
+  if (xvalh) {
+    double R[9];
+    if (zero) for (int q = 0; q < 9; ++q) R[q] = 0.0;
+    else scale_block(ld_tri(Linv, row), H, ld_tri(Linv, col), R);
+    for (int q = 0; q < 9; ++q) xvalh[9 * (long long)u + q] = float(R[q]);
   }
 }
 
@@ -1067,10 +1233,6 @@ void launch_contact_vertex(const MeshDev& m, const ContactDev* c, const ContactE
 void launch_extra_flags(const ContactEntry* ents, const int* keys, int n, int* flags, cudaStream_t s) {
   if (n) k_extra_flags<<<nblk(n), TPB, 0, s>>>(ents, keys, n, flags);
 }
-void launch_extra_values(const ContactDev* c, const ContactEntry* xent, const int* xkeys, const unsigned char* fixed, int* xcols, int nx,
-                         const StepParams& p, float* xval, cudaStream_t s) {
-  if (nx) k_extra_values<<<nblk(nx), TPB, 0, s>>>(c, xent, xkeys, fixed, xcols, nx, p, xval);
-}
 void launch_ctrl_reset(Ctrl* ctrl, cudaStream_t s) { k_ctrl_reset<<<1, 1, 0, s>>>(ctrl); }
 void launch_strain_face(const MeshDev& m, const double* x, const StepParams& p, unsigned char* flags, StrainSV* sv, Ctrl* ctrl, cudaStream_t s) {
   if (m.T) k_strain_face<<<nblk(m.T), TPB, 0, s>>>(m, x, p, flags, sv, ctrl);
@@ -1090,6 +1252,27 @@ void launch_check(Ctrl* ctrl, double tol, cudaStream_t s) { k_check<<<1, 1, 0, s
 void launch_assemble(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                      const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl, cudaStream_t s) {
   if (m.nnzb) k_assemble<<<nblk(m.nnzb), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, val, precond, ctrl);
+}
+void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                        const unsigned char* fixed, const double* g, double* Linv, float* Lf, float* bhat, unsigned char* chol_ok,
+                        const Ctrl* ctrl, cudaStream_t s) {
+  if (m.V) k_diag_factor<<<nblk(m.V), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, g, Linv, Lf, bhat, chol_ok, ctrl);
+}
+void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                            const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
+                            const Ctrl* ctrl, cudaStream_t s) {
+  if (m.nnzb) k_assemble_scaled<<<nblk(m.nnzb), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh, ctrl);
+}
+void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s) {
+  if (n) k_extra_key64<<<nblk(n), TPB, 0, s>>>(xent, xkeys, n, key, idx);
+}
+void launch_run_heads(const unsigned long long* key, int n, int* flags, cudaStream_t s) {
+  if (n) k_run_heads<<<nblk(n), TPB, 0, s>>>(key, n, flags);
+}
+void launch_extra_merge(const ContactDev* c, const ContactEntry* xent, const unsigned long long* key, const int* idx, const int* heads, int nu,
+                        int n, const unsigned char* fixed, const StepParams& p, const double* Linv, int* xrow, int* xcols, float* xval,
+                        float* xvalh, cudaStream_t s) {
+  if (nu) k_extra_merge<<<nblk(nu), TPB, 0, s>>>(c, xent, key, idx, heads, nu, n, fixed, p, Linv, xrow, xcols, xval, xvalh);
 }
 void launch_ls_wall(int V, const double* x, const float* d, WallDev w, Ctrl* ctrl, cudaStream_t s) {
   if (V) k_ls_wall<<<nblk(V), TPB, 0, s>>>(V, x, d, w, ctrl);

@@ -30,8 +30,6 @@ void launch_vertex_ranges(const int* sorted_keys, int n, int V, int* begin, int*
 void launch_contact_vertex(const MeshDev& m, const ContactDev* c, const ContactEntry* ents, const int* begin, const int* end,
                            const StepParams& p, const double* g_base, double* g_const, double* diag_const, cudaStream_t s);
 void launch_extra_flags(const ContactEntry* ents, const int* keys, int n, int* flags, cudaStream_t s);
-void launch_extra_values(const ContactDev* c, const ContactEntry* xent, const int* xkeys, const unsigned char* fixed, int* xcols, int nx,
-                         const StepParams& p, float* xval, cudaStream_t s);
 
 // Newton iteration
 void launch_ctrl_reset(Ctrl* ctrl, cudaStream_t s);
@@ -45,6 +43,18 @@ void launch_check(Ctrl* ctrl, double tol, cudaStream_t s);
 void launch_pin_heads(const int* pin_vertex, int num_pins, int* pin_head, cudaStream_t s);
 void launch_assemble(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                      const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl, cudaStream_t s);
+// scaled system (CORRECTED): L = chol(A_ii), A^ = L^-1 A L^-T (kernels.cu)
+void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                        const unsigned char* fixed, const double* g, double* Linv, float* Lf, float* bhat, unsigned char* chol_ok,
+                        const Ctrl* ctrl, cudaStream_t s);
+void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                            const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
+                            const Ctrl* ctrl, cudaStream_t s);
+void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s);
+void launch_run_heads(const unsigned long long* key, int n, int* flags, cudaStream_t s);
+void launch_extra_merge(const ContactDev* c, const ContactEntry* xent, const unsigned long long* key, const int* idx, const int* heads, int nu,
+                        int n, const unsigned char* fixed, const StepParams& p, const double* Linv, int* xrow, int* xcols, float* xval,
+                        float* xvalh, cudaStream_t s);
 void launch_ls_wall(int V, const double* x, const float* d, WallDev w, Ctrl* ctrl, cudaStream_t s);
 void launch_ls_contacts(const ContactDev* c, int nc, const double* x, const float* d, Ctrl* ctrl, cudaStream_t s);
 void launch_update(int V, double* x, const float* d, Ctrl* ctrl, cudaStream_t s);
@@ -91,6 +101,26 @@ struct PcgArgs {
   float tol; int max_iters;
 };
 int pcg_grid_size(int device);
+
+// CG on the block-scaled system (pcg.cu): identity (= block-Jacobi on A) or
+// the learned approximate inverse S of the scaled system.
+struct PcgScaledArgs {
+  int V;
+  const int* rowptr; const int* cols; const float* valh;                      // A^ on the static pattern
+  const int* xbegin; const int* xend; const int* xcols; const float* xvalh;  // A^ extra contact segment
+  const float* S;       // learned preconditioner blocks on the static pattern (learned solves only)
+  const double* Linv;   // 6V packed L^-1
+  const float* Lf;      // 6V packed L
+  const float* bhat;    // 3V  L^-1 b
+  float* d;             // 3V  output: L^-T x^
+  double* xh;           // 3V  scaled iterate x^ (FP64)
+  float *r, *r2, *z, *p0, *p1, *Ap;
+  double* partials;     // 3 * grid
+  Ctrl* ctrl;
+  float tol; int max_iters; int stall_window;
+};
+int pcg_scaled_grid_size(int device, bool learned);
+cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, int grid, cudaStream_t s);
 cudaError_t launch_pcg(const PcgArgs& a, int grid, cudaStream_t s);
 
 }  // namespace ando

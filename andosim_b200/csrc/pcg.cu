@@ -199,6 +199,224 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg(PcgArgs a) {
   }
 }
 
+// ------------------------------------------------------------ scaled PCG
+// CG on the block-scaled system A^ = L^-1 A L^-T (A_ii = L_i L_i^T), used by
+// the CORRECTED step. With the identity as preconditioner on A^ this is the
+// block-Jacobi PCG of the reference, iterate for iterate in exact arithmetic:
+// x = L^-T x^, r = L r^. The stopping test is the reference's, on the
+// unscaled residual: max_i |L_i r^_i| < tol * max |b|.
+//
+// LEARNED: z = S r with S a symmetric positive definite block matrix on the
+// static pattern (the learned approximate inverse of A^). Phase B then is a
+// second warp-per-row product; it gathers r - alpha Ap from the neighbours, so
+// the iteration still needs only two grid barriers (r ping-pongs between two
+// buffers because neighbours read the old values). r^T z <= 0 (S lost
+// definiteness) or no new best residual for `stall_window` iterations ends
+// the solve with PCG_PRECOND / PCG_STALL, and the caller redoes it with
+// block-Jacobi.
+
+// One warp computes y = (M v)_row over the static segment (and the extra
+// segment when given); lanes (comp = lane / 8, bi = lane % 8) cover 8 blocks x
+// 3 block rows per pass. vec(j, q) yields the gathered vector at column j.
+template <class Vec>
+__device__ inline void warp_row(int row, const int* rowptr, const int* cols, const float* val, const int* xbegin, const int* xend,
+                                const int* xcols, const float* xval, const Vec& vec, int lane, float& y0, float& y1, float& y2) {
+  const int comp = lane >> 3, bi = lane & 7;
+  float acc = 0.f;
+  int s0 = rowptr[row], s1 = rowptr[row + 1];
+  for (int k0 = s0; k0 < s1; k0 += 8) {
+    int k = k0 + bi;
+    if (comp < 3 && k < s1) {
+      int col = cols[k];
+      const float* h = val + 9 * (long long)k + 3 * comp;
+      float q0, q1, q2; vec(col, q0, q1, q2);
+      acc += h[0] * q0 + h[1] * q1 + h[2] * q2;
+    }
+  }
+  if (xbegin) {
+    int e0 = xbegin[row], e1 = xend[row];
+    for (int k0 = e0; k0 < e1; k0 += 8) {
+      int k = k0 + bi;
+      if (comp < 3 && k < e1) {
+        int col = xcols[k];
+        const float* h = xval + 9 * (long long)k + 3 * comp;
+        float q0, q1, q2; vec(col, q0, q1, q2);
+        acc += h[0] * q0 + h[1] * q1 + h[2] * q2;
+      }
+    }
+  }
+  acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+  y0 = __shfl_sync(0xffffffffu, acc, 0); y1 = __shfl_sync(0xffffffffu, acc, 8); y2 = __shfl_sync(0xffffffffu, acc, 16);
+}
+
+// |L_i r_i|_inf with L lower triangular (FP32, packed l00 l10 l11 l20 l21 l22).
+__device__ inline double unscaled_inf(const float* Lf, int i, float r0, float r1, float r2) {
+  const float* l = Lf + 6 * (long long)i;
+  double u0 = double(l[0]) * r0;
+  double u1 = double(l[1]) * r0 + double(l[2]) * r1;
+  double u2 = double(l[3]) * r0 + double(l[4]) * r1 + double(l[5]) * r2;
+  return fmax(fabs(u0), fmax(fabs(u1), fabs(u2)));
+}
+
+struct GatherP {  // p = z + beta p_old
+  const float* z; const float* pold; float beta; bool first;
+  __device__ void operator()(int j, float& q0, float& q1, float& q2) const { p_at(z, pold, beta, first, j, q0, q1, q2); }
+};
+struct GatherV {  // plain vector
+  const float* v;
+  __device__ void operator()(int j, float& q0, float& q1, float& q2) const { q0 = v[3 * j]; q1 = v[3 * j + 1]; q2 = v[3 * j + 2]; }
+};
+struct GatherR {  // r - alpha Ap
+  const float* r; const float* Ap; float alpha;
+  __device__ void operator()(int j, float& q0, float& q1, float& q2) const {
+    q0 = r[3 * j] - alpha * Ap[3 * j]; q1 = r[3 * j + 1] - alpha * Ap[3 * j + 1]; q2 = r[3 * j + 2] - alpha * Ap[3 * j + 2];
+  }
+};
+
+template <bool LEARNED>
+__global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
+  Ctrl* ctrl = a.ctrl;
+  if (ctrl->converged) return;
+  __shared__ double sh[PCG_WARPS + 1];
+  const int V = a.V;
+  const unsigned nb = gridDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31, gwarp = tid >> 5, nwarps = nthreads >> 5;
+  double* part_pap = a.partials;
+  double* part_rz = a.partials + nb;
+  double* part_rinf = a.partials + 2 * nb;
+  const double binf = __longlong_as_double((long long)ctrl->gnorm_bits);  // max |b| = max |g|
+  float* r = a.r;
+  float* rn = a.r2;
+  const float* zsrc = LEARNED ? a.z : a.r;
+
+  // init: x^ = 0, r = b^, z = S b^
+  double rz_loc = 0.0;
+  for (int i = tid; i < V; i += nthreads) {
+    float b0 = a.bhat[3 * i], b1 = a.bhat[3 * i + 1], b2 = a.bhat[3 * i + 2];
+    a.xh[3 * i] = 0.0; a.xh[3 * i + 1] = 0.0; a.xh[3 * i + 2] = 0.0;
+    r[3 * i] = b0; r[3 * i + 1] = b1; r[3 * i + 2] = b2;
+    if (!LEARNED) rz_loc += double(b0) * b0 + double(b1) * b1 + double(b2) * b2;
+  }
+  if (LEARNED) {
+    GatherV gb{a.bhat};
+    for (int row = gwarp; row < V; row += nwarps) {
+      float y0, y1, y2;
+      warp_row(row, a.rowptr, a.cols, a.S, nullptr, nullptr, nullptr, nullptr, gb, lane, y0, y1, y2);
+      if (lane == 0) {
+        a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
+        rz_loc += double(a.bhat[3 * row]) * y0 + double(a.bhat[3 * row + 1]) * y1 + double(a.bhat[3 * row + 2]) * y2;
+      }
+    }
+  }
+  rz_loc = block_sum(rz_loc, sh);
+  if (threadIdx.x == 0) part_rz[blockIdx.x] = rz_loc;
+  bool ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+  int status = PCG_MAXIT, iters = 0;
+  double rel = 0.0;
+  if (!ok) status = PCG_TIMEOUT;
+  double rz = ok ? grid_sum(part_rz, nb, sh) : 0.0;
+  if (ok) {
+    rel = binf < 1e-16 ? binf : 1.0;
+    if (rel < double(a.tol)) status = PCG_OK;
+    else if (LEARNED && !(rz > 0.0)) status = PCG_PRECOND;
+  }
+  float* pold = a.p0;
+  float* pnew = a.p1;
+  float beta = 0.f;
+  bool first = true;
+  double best = rel;
+  int since = 0;
+  for (int it = 0; ok && status == PCG_MAXIT && it < a.max_iters; ++it) {
+    // ---- phase A: p_new = z + beta p_old, Ap = A^ p_new, p^T Ap
+    double pap_loc = 0.0;
+    GatherP gp{zsrc, pold, beta, first};
+    for (int row = gwarp; row < V; row += nwarps) {
+      float y0, y1, y2;
+      warp_row(row, a.rowptr, a.cols, a.valh, a.xbegin, a.xend, a.xcols, a.xvalh, gp, lane, y0, y1, y2);
+      if (lane == 0) {
+        float q0, q1, q2; gp(row, q0, q1, q2);
+        pnew[3 * row] = q0; pnew[3 * row + 1] = q1; pnew[3 * row + 2] = q2;
+        a.Ap[3 * row] = y0; a.Ap[3 * row + 1] = y1; a.Ap[3 * row + 2] = y2;
+        pap_loc += double(q0) * y0 + double(q1) * y1 + double(q2) * y2;
+      }
+    }
+    pap_loc = block_sum(pap_loc, sh);
+    if (threadIdx.x == 0) part_pap[blockIdx.x] = pap_loc;
+    ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+    if (!ok) { status = PCG_TIMEOUT; break; }
+    double pap = grid_sum(part_pap, nb, sh);
+    iters = it + 1;
+    if (fabs(pap) < 1e-16) { status = PCG_NOT_SPD; break; }
+    float alpha = float(rz / pap);
+    // ---- phase B: x^ += alpha p, r -= alpha Ap, z = S r, r^T z, |L r|_inf
+    double rz_new_loc = 0.0, rinf_loc = 0.0;
+    if (!LEARNED) {
+      for (int i = tid; i < V; i += nthreads) {
+        float p0 = pnew[3 * i], p1 = pnew[3 * i + 1], p2 = pnew[3 * i + 2];
+        a.xh[3 * i] += double(alpha) * p0; a.xh[3 * i + 1] += double(alpha) * p1; a.xh[3 * i + 2] += double(alpha) * p2;
+        float r0 = r[3 * i] - alpha * a.Ap[3 * i], r1 = r[3 * i + 1] - alpha * a.Ap[3 * i + 1], r2 = r[3 * i + 2] - alpha * a.Ap[3 * i + 2];
+        r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
+        rz_new_loc += double(r0) * r0 + double(r1) * r1 + double(r2) * r2;
+        rinf_loc = fmax(rinf_loc, unscaled_inf(a.Lf, i, r0, r1, r2));
+      }
+    } else {
+      GatherR gr{r, a.Ap, alpha};
+      for (int row = gwarp; row < V; row += nwarps) {
+        float y0, y1, y2;
+        warp_row(row, a.rowptr, a.cols, a.S, nullptr, nullptr, nullptr, nullptr, gr, lane, y0, y1, y2);
+        if (lane == 0) {
+          float r0, r1, r2; gr(row, r0, r1, r2);
+          a.xh[3 * row] += double(alpha) * pnew[3 * row]; a.xh[3 * row + 1] += double(alpha) * pnew[3 * row + 1];
+          a.xh[3 * row + 2] += double(alpha) * pnew[3 * row + 2];
+          rn[3 * row] = r0; rn[3 * row + 1] = r1; rn[3 * row + 2] = r2;
+          a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
+          rz_new_loc += double(r0) * y0 + double(r1) * y1 + double(r2) * y2;
+          rinf_loc = fmax(rinf_loc, unscaled_inf(a.Lf, row, r0, r1, r2));
+        }
+      }
+    }
+    rz_new_loc = block_sum(rz_new_loc, sh);
+    rinf_loc = block_max(rinf_loc, sh);
+    if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz_new_loc; part_rinf[blockIdx.x] = rinf_loc; }
+    ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+    if (!ok) { status = PCG_TIMEOUT; break; }
+    double rz_new = grid_sum(part_rz, nb, sh);
+    double rinf = grid_max(part_rinf, nb, sh);
+    rel = binf < 1e-16 ? rinf : rinf / binf;
+    if (LEARNED) { float* t = r; r = rn; rn = t; }
+    if (rel < double(a.tol)) { status = PCG_OK; break; }
+    if (LEARNED) {
+      if (!(rz_new > 0.0)) { status = PCG_PRECOND; break; }
+      if (rel < best) { best = rel; since = 0; }
+      else if (++since >= a.stall_window) { status = PCG_STALL; break; }
+    }
+    beta = float(rz_new / rz);
+    rz = rz_new;
+    first = false;
+    float* t = pold; pold = pnew; pnew = t;
+  }
+  // d = L^-T x^ (every x^ write precedes the last grid barrier); x^ is FP64:
+  // rounding it to FP32 would cost up to cond(L_i) x 6e-8 of d_i at stiff vertices
+  if (ok) {
+    for (int i = tid; i < V; i += nthreads) {
+      const double* q = a.Linv + 6 * (long long)i;
+      double x0 = a.xh[3 * i], x1 = a.xh[3 * i + 1], x2 = a.xh[3 * i + 2];
+      a.d[3 * i] = float(q[0] * x0 + q[1] * x1 + q[3] * x2);
+      a.d[3 * i + 1] = float(q[2] * x1 + q[4] * x2);
+      a.d[3 * i + 2] = float(q[5] * x2);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctrl->pcg_iters = iters;
+    ctrl->pcg_status = status;
+    ctrl->pcg_converged = status == PCG_OK ? 1 : 0;
+    ctrl->pcg_rel = rel;
+  }
+}
+
 }  // namespace
 
 int pcg_grid_size(int device) {
@@ -209,6 +427,26 @@ int pcg_grid_size(int device) {
   int co = sms * per_sm;
   int want = 2 * sms;
   return co < want ? co : want;
+}
+
+int pcg_scaled_grid_size(int device, bool learned) {
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (learned) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_scaled<true>, PCG_TPB, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_scaled<false>, PCG_TPB, 0);
+  if (per_sm < 1) per_sm = 1;
+  int co = sms * per_sm;
+  int want = 2 * sms;
+  return co < want ? co : want;
+}
+
+cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, int grid, cudaStream_t s) {
+  int need = (a.V + PCG_TPB - 1) / PCG_TPB;
+  if (need < 1) need = 1;
+  if (grid > need) grid = need;
+  void* args[] = {(void*)&a};
+  if (learned) return cudaLaunchCooperativeKernel((void*)k_pcg_scaled<true>, dim3(grid), dim3(PCG_TPB), args, 0, s);
+  return cudaLaunchCooperativeKernel((void*)k_pcg_scaled<false>, dim3(grid), dim3(PCG_TPB), args, 0, s);
 }
 
 cudaError_t launch_pcg(const PcgArgs& a, int grid, cudaStream_t s) {

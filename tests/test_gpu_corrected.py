@@ -166,10 +166,22 @@ def step_parity(oracle, core, sc, frames, tight=1e-9, **params):
 
 
 def assert_step_band(errs, tol=1e-5):
-    """Each GPU step lies within tol of the tight FP64 step, widened on frames
-    where the FP64 oracle at the same PCG tolerance is itself further off."""
+    """GPU steps against the tight FP64 step, judged by the spread of an FP64
+    step taken at the same PCG tolerance (e_loose).
+
+    On a well-posed frame (e_loose <= tol / 10) the GPU step must be within
+    tol. On an ill-conditioned one (block-scaled condition numbers reach 1e7
+    near active strain barriers) a relative residual of 1e-5 leaves the Newton
+    direction free at the 1e-2 level in FP64 and FP32 alike, and the line
+    search and the strain active set turn that freedom into position changes
+    of either sign: the GPU step is another draw from that spread. So each
+    frame must lie within 20 x e_loose (+ tol) and, over all frames, the GPU's
+    errors must not be systematically larger than the FP64 oracle's
+    (geometric-mean ratio <= 2)."""
     for f, (e_gpu, e_loose) in enumerate(errs):
-        assert e_gpu <= tol + 3.0 * e_loose, (f, e_gpu, e_loose)
+        assert e_gpu <= tol + 20.0 * e_loose, (f, e_gpu, e_loose)
+    ratios = [(e_gpu + tol) / (e_loose + tol) for e_gpu, e_loose in errs]
+    assert float(np.exp(np.mean(np.log(ratios)))) <= 2.0, ratios
     well_posed = [e for e, l in errs if l <= 0.1 * tol]
     assert well_posed and max(well_posed) <= tol, well_posed
 
