@@ -151,6 +151,22 @@ def lib() -> C.CDLL:
     L.ando_profile_read.restype = I32; L.ando_profile_read.argtypes = [P, C.POINTER(Profile)]
     L.ando_ctx_stream.restype = I32; L.ando_ctx_stream.argtypes = [P, C.POINTER(C.c_void_p)]
     L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
+    pu8 = C.POINTER(C.c_ubyte)
+    L.ando_precond_num_params.restype = I32
+    L.ando_precond_init_weights.restype = I32; L.ando_precond_init_weights.argtypes = [C.c_uint64, pf, I32]
+    L.ando_ctx_set_precond_weights.restype = I32; L.ando_ctx_set_precond_weights.argtypes = [P, pf, I32]
+    L.ando_precond_eval.restype = I32; L.ando_precond_eval.argtypes = [P]
+    L.ando_last_precond.restype = I32; L.ando_last_precond.argtypes = [P, pf]
+    L.ando_last_scaled_system.restype = I32; L.ando_last_scaled_system.argtypes = [P, pf, pf, pf, pf, pd]
+    L.ando_trainer_create.restype = I32; L.ando_trainer_create.argtypes = [I32, pf, I32, C.POINTER(P)]
+    L.ando_trainer_destroy.restype = None; L.ando_trainer_destroy.argtypes = [P]
+    L.ando_trainer_add_system.restype = I32; L.ando_trainer_add_system.argtypes = [P, P, I32, D, I32]
+    L.ando_trainer_num_systems.restype = I32; L.ando_trainer_num_systems.argtypes = [P]
+    L.ando_trainer_probes.restype = I32; L.ando_trainer_probes.argtypes = [P, I32, pf, pd, pi]
+    L.ando_trainer_loss.restype = I32; L.ando_trainer_loss.argtypes = [P, I32, pd, pf]
+    L.ando_trainer_step.restype = I32; L.ando_trainer_step.argtypes = [P, C.c_float, pd]
+    L.ando_trainer_get_weights.restype = I32; L.ando_trainer_get_weights.argtypes = [P, pf, I32]
+    L.ando_trainer_set_weights.restype = I32; L.ando_trainer_set_weights.argtypes = [P, pf, I32]
     L.ando_pcg_solve_noalloc.restype = I32
     L.ando_pcg_solve_noalloc.argtypes = [I32, P, I32, P, P, P, P, P, P, C.c_int64, D, I32, pi, pi, pd]
     _lib = L
@@ -361,6 +377,36 @@ class Scene:
         _check(lib().ando_ctx_stream(self.ctx, C.byref(sp)), "ando_ctx_stream")
         return sp.value or 0
 
+    def set_precond_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().ando_ctx_set_precond_weights(self.ctx, _fptr(w), len(w)), "ando_ctx_set_precond_weights")
+
+    def precond_eval(self) -> np.ndarray:
+        """S of the current scaled system under the loaded weights, (nnzb, 3, 3)."""
+        _check(lib().ando_precond_eval(self.ctx), "ando_precond_eval")
+        return self.last_precond()
+
+    def last_precond(self) -> np.ndarray:
+        V = C.c_int32(); nnzb = C.c_int32()
+        _check(lib().ando_last_system(self.ctx, C.byref(V), C.byref(nnzb), None, None, None, None, None), "ando_last_system")
+        S = np.empty(9 * nnzb.value, dtype=np.float32)
+        _check(lib().ando_last_precond(self.ctx, _fptr(S)), "ando_last_precond")
+        return S.reshape(-1, 3, 3)
+
+    def last_scaled_system(self) -> dict:
+        """Scaled system of the last CORRECTED Newton iteration (see ando_last_scaled_system)."""
+        rowptr, cols, _, _, _ = self.last_system()
+        xr, xc, _ = self.last_contact_blocks()
+        valh = np.empty(9 * len(cols), dtype=np.float32)
+        xvalh = np.empty(max(9 * len(xr), 9), dtype=np.float32)
+        bhat = np.empty(3 * self.V, dtype=np.float32)
+        Lf = np.empty(6 * self.V, dtype=np.float32)
+        Linv = np.empty(6 * self.V)
+        _check(lib().ando_last_scaled_system(self.ctx, _fptr(valh), _fptr(xvalh), _fptr(bhat), _fptr(Lf), _dptr(Linv)),
+               "ando_last_scaled_system")
+        return dict(rowptr=rowptr, cols=cols, valh=valh.reshape(-1, 3, 3), xrow=xr, xcol=xc,
+                    xvalh=xvalh[:9 * len(xr)].reshape(-1, 3, 3), bhat=bhat, Lf=Lf.reshape(-1, 6), Linv=Linv.reshape(-1, 6))
+
     def contacts(self, rigids: Optional[List[Rigid]] = None) -> List[Contact]:
         nr = len(rigids) if rigids else 0
         ra = (Rigid * max(1, nr))(*(rigids or []))
@@ -400,3 +446,68 @@ def make_rigid(vertices, triangles, density: float, keep: list) -> Rigid:
     for q in range(3):
         r.position[q] = c[q]; r.linear_velocity[q] = 0.0; r.angular_velocity[q] = 0.0
     return r
+
+
+def precond_num_params() -> int:
+    return int(lib().ando_precond_num_params())
+
+
+def precond_init_weights(seed: int = 0) -> np.ndarray:
+    """Initial preconditioner weights (ando_precond_init_weights)."""
+    w = np.empty(precond_num_params(), dtype=np.float32)
+    _check(lib().ando_precond_init_weights(C.c_uint64(seed), _fptr(w), len(w)), "ando_precond_init_weights")
+    return w
+
+
+class Trainer:
+    """Device-side trainer of the learned preconditioner (ando_trainer_*)."""
+
+    def __init__(self, weights: np.ndarray, device: int = 0):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        self.t = C.c_void_p()
+        _check(lib().ando_trainer_create(device, _fptr(w), len(w), C.byref(self.t)), "ando_trainer_create")
+
+    def close(self):
+        if self.t:
+            lib().ando_trainer_destroy(self.t)
+            self.t = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_system(self, scene: "Scene", max_probes: int = 6, tol: float = 1e-6, max_iters: int = 2000):
+        _check(lib().ando_trainer_add_system(self.t, scene.ctx, max_probes, tol, max_iters), "ando_trainer_add_system")
+
+    def __len__(self) -> int:
+        return int(lib().ando_trainer_num_systems(self.t))
+
+    def probes(self, idx: int, V: int):
+        n = C.c_int32()
+        _check(lib().ando_trainer_probes(self.t, idx, None, None, C.byref(n)), "ando_trainer_probes")
+        pr = np.empty(3 * V * n.value, dtype=np.float32)
+        nr = np.empty(n.value)
+        _check(lib().ando_trainer_probes(self.t, idx, _fptr(pr), _dptr(nr), C.byref(n)), "ando_trainer_probes")
+        return pr.reshape(n.value, 3 * V), nr
+
+    def loss(self, idx: int, grad: bool = False):
+        L = C.c_double()
+        g = np.empty(precond_num_params(), dtype=np.float32) if grad else None
+        _check(lib().ando_trainer_loss(self.t, idx, C.byref(L), _fptr(g) if grad else None), "ando_trainer_loss")
+        return (L.value, g) if grad else L.value
+
+    def step(self, lr: float) -> float:
+        L = C.c_double()
+        _check(lib().ando_trainer_step(self.t, C.c_float(lr), C.byref(L)), "ando_trainer_step")
+        return L.value
+
+    def weights(self) -> np.ndarray:
+        w = np.empty(precond_num_params(), dtype=np.float32)
+        _check(lib().ando_trainer_get_weights(self.t, _fptr(w), len(w)), "ando_trainer_get_weights")
+        return w
+
+    def set_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().ando_trainer_set_weights(self.t, _fptr(w), len(w)), "ando_trainer_set_weights")

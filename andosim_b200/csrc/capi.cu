@@ -25,6 +25,7 @@
 #include "../../include/ando_gpu.h"
 #include "kernels.cuh"
 #include "lbvh.cuh"
+#include "learned.cuh"
 
 using namespace ando;
 
@@ -82,6 +83,15 @@ struct ando_ctx_s {
   DevBuf<float> Lf, bhat, valh, xvalh, r2;
   DevBuf<unsigned char> chol_ok;
   int pcg_scaled_grid = 1, pcg_learned_grid = 1;
+  double dt2inv = 0.0;             // of the last assembled system
+
+  // learned preconditioner: weights, activations, S on the static pattern
+  DevBuf<int> slot_T;
+  DevBuf<float> net_master, net_buf, lw_buf, Sval;
+  DevBuf<unsigned short> net_bf16;
+  NetDev net;
+  LearnedWork lw;
+  bool net_ready = false, S_ready = false;
 
   // contacts
   DevBuf<int> det_counts, det_offsets;
@@ -565,6 +575,7 @@ int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, i
 // scaled system A^ = L^-1 A L^-T with its right-hand side.
 void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
   MeshDev m = c->mesh_dev();
+  c->dt2inv = sp.dt2inv;
   launch_diag_factor(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->g.p, c->Linv.p, c->Lf.p, c->bhat.p,
                      c->chol_ok.p, c->ctrl.p, s);
   launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p, c->val.p,
@@ -580,7 +591,57 @@ PcgScaledArgs scaled_args(ando_ctx c, const ando_params& p) {
   a.S = nullptr; a.Linv = c->Linv.p; a.Lf = c->Lf.p; a.bhat = c->bhat.p; a.d = c->d.p;
   a.xh = c->xh.p; a.r = c->r.p; a.r2 = c->r2.p; a.z = c->z.p; a.p0 = c->p0.p; a.p1 = c->p1.p; a.Ap = c->Ap.p;
   a.partials = c->partials.p; a.ctrl = c->ctrl.p; a.tol = float(p.pcg_tol); a.max_iters = p.pcg_max_iters; a.stall_window = 50;
+  a.snap_r = nullptr; a.snap_x = nullptr; a.snap_max = 0;
   return a;
+}
+
+LsView ls_view(ando_ctx c) {
+  LsView v;
+  v.V = c->V; v.nnzb = c->nnzb; v.rowptr = c->rowptr.p; v.cols = c->cols.p; v.slot_row = c->slot_row.p; v.slot_T = c->slot_T.p;
+  v.valh = c->valh.p;
+  v.xbegin = c->nx ? c->xbegin.p : nullptr; v.xend = c->nx ? c->xend.p : nullptr; v.xcols = c->xcols.p; v.xvalh = c->xvalh.p;
+  v.Lf = c->Lf.p; v.mass = c->mass.p; v.fixed = c->fixed.p; v.dt2inv = c->dt2inv;
+  return v;
+}
+
+// Inference buffers sized for the mesh; weights must have been set.
+int ensure_learned(ando_ctx c) {
+  if (!c->net_ready) return fail(ANDO_ERR_STATE, "learned preconditioner: no weights (ando_ctx_set_precond_weights)");
+  size_t need = learned_work_floats(c->V, c->nnzb, false);
+  if (c->lw.V != c->V || c->lw.nnzb != c->nnzb || c->lw_buf.n < need || c->lw.training) {
+    CK(c->lw_buf.reserve(need));
+    learned_work_carve(c->lw, c->lw_buf.p, c->V, c->nnzb, false);
+  }
+  CK(c->Sval.reserve(9ull * c->nnzb));
+  return ANDO_OK;
+}
+
+// The scaled PCG of one Newton iteration: learned S when asked for (with
+// block-Jacobi redoing the solve when S loses definiteness, stalls or hits
+// the iteration cap), block-Jacobi otherwise.
+int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
+  cudaStream_t s = c->stream;
+  Phase ph(c, ANDO_PHASE_PCG);
+  PcgScaledArgs sa = scaled_args(c, p);
+  if (p.precond == ANDO_PRECOND_LEARNED) {
+    int rc = ensure_learned(c);
+    if (rc) return rc;
+    LsView v = ls_view(c);
+    learned_forward(v, c->net, c->lw, c->Sval.p, s);
+    c->S_ready = true;
+    sa.S = c->Sval.p;
+    CK(launch_pcg_scaled(sa, true, c->pcg_learned_grid, s));
+    ph.launched(5 + 3 * net::NL + 1);
+    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const Ctrl& h = *c->ctrl_host;
+    if (h.converged || h.pcg_status == PCG_OK || h.pcg_status == PCG_TIMEOUT) return ANDO_OK;
+    st.precond_fallbacks++;
+    sa.S = nullptr;
+  }
+  CK(launch_pcg_scaled(sa, false, c->pcg_scaled_grid, s));
+  ph.launched();
+  return ANDO_OK;
 }
 
 // inner_newton_step with the CORRECTED terms and line search.
@@ -600,12 +661,8 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
       enqueue_scaled_assembly(c, sp, s);
       ph.launched(c->nx ? 3 : 2);
     }
-    {
-      Phase ph(c, ANDO_PHASE_PCG);
-      PcgScaledArgs sa = scaled_args(c, p);
-      CK(launch_pcg_scaled(sa, false, c->pcg_scaled_grid, s));
-      ph.launched();
-    }
+    rc = scaled_solve(c, p, st);
+    if (rc) return rc;
     rc = corrected_line_search(c, nb);
     if (rc) return rc;
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
@@ -984,8 +1041,12 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     std::vector<int> pos(vfp.begin(), vfp.end() - 1);
     for (int f = 0; f < T; ++f) for (int a = 0; a < 3; ++a) vfl[pos[tris[3 * f + a]]++] = 3 * f + a;
   }
+  std::vector<int> slotT(nnzb);
+  for (int r = 0; r < V; ++r)
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) slotT[k] = slot_of(cols[k], r);
   cudaStream_t s = c->stream;
   c->V = V; c->T = T; c->nnzb = nnzb;
+  c->S_ready = false;
   c->mu = mat->youngs_modulus / (2.0 * (1.0 + mat->poisson_ratio));
   c->thickness = mat->thickness; c->density = mat->density;
   CK(c->tris.upload(tris, 3ull * T, s));
@@ -995,6 +1056,7 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->cols.upload(cols.data(), nnzb, s));
   CK(c->slot_row.upload(slot_row.data(), nnzb, s));
   CK(c->diag_slot.upload(diag_slot.data(), V, s));
+  CK(c->slot_T.upload(slotT.data(), nnzb, s));
   CK(c->face_slot.upload(face_slot.data(), 9ull * T, s));
   CK(c->slot_cptr.upload(cptr.data(), nnzb + 1, s));
   CK(c->slot_contrib.upload(contrib.data(), 9ull * T, s));
@@ -1100,7 +1162,11 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     return fail(ANDO_ERR_INVALID, "step arguments");
   const ando_params& p = *params;
   if (p.semantics != ANDO_SEMANTICS_REFERENCE && p.semantics != ANDO_SEMANTICS_CORRECTED) return fail(ANDO_ERR_INVALID, "unknown semantics");
-  if (p.precond != ANDO_PRECOND_BLOCK_JACOBI) return fail(ANDO_ERR_INVALID, "preconditioner not available");
+  if (p.precond != ANDO_PRECOND_BLOCK_JACOBI && p.precond != ANDO_PRECOND_LEARNED) return fail(ANDO_ERR_INVALID, "unknown preconditioner");
+  if (p.precond == ANDO_PRECOND_LEARNED && p.semantics != ANDO_SEMANTICS_CORRECTED)
+    return fail(ANDO_ERR_INVALID, "the learned preconditioner works on the scaled CORRECTED system");
+  if (p.precond == ANDO_PRECOND_LEARNED && !c->net_ready)
+    return fail(ANDO_ERR_STATE, "learned preconditioner: no weights (ando_ctx_set_precond_weights)");
   ando_step_stats st;
   std::memset(&st, 0, sizeof(st));
   cudaStream_t s = c->stream;
@@ -1339,6 +1405,331 @@ int32_t ando_last_gradient(ando_ctx c, double* g, int32_t V) {
   if (!c->mesh_ready || !g || V != c->V) return fail(ANDO_ERR_INVALID, "gradient arguments");
   CK(cudaMemcpyAsync(g, c->g.p, sizeof(double) * 3ull * V, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return ANDO_OK;
+}
+
+
+// ------------------------------------------------ learned preconditioner
+int32_t ando_precond_num_params(void) { return net::NPARAM; }
+
+int32_t ando_precond_init_weights(uint64_t seed, float* out, int32_t n) {
+  if (!out || n != net::NPARAM) return fail(ANDO_ERR_INVALID, "weight buffer must hold ando_precond_num_params() floats");
+  using namespace net;
+  uint64_t st = seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+  auto uni = [&]() {  // splitmix64 -> [-1, 1)
+    st += 0x9E3779B97F4A7C15ull;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return float(double(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0);
+  };
+  auto fill = [&](int off, int cnt, float scale) { for (int i = 0; i < cnt; ++i) out[off + i] = scale * uni(); };
+  std::fill(out, out + n, 0.f);
+  fill(W_IN, H * FN, std::sqrt(6.f / FN));
+  for (int l = 0; l < NL; ++l) {
+    int L = LAYER0 + l * L_SIZE;
+    fill(L + L_U, H * H, std::sqrt(6.f / H));
+    fill(L + L_E, H * FE, std::sqrt(6.f / FE));
+    fill(L + L_W, H * 2 * H, 0.5f * std::sqrt(6.f / (2 * H)));   // residual branch starts small
+  }
+  fill(DV, H, 0.01f);
+  fill(DE, 2 * DE_IN, 0.01f);
+  // start near the first-order Neumann form of an approximate inverse:
+  // S_ij = -0.25 A^_ij, delta = softplus(-1.26) = 0.25
+  out[DV0] = -1.2587f;
+  out[DE0] = 0.5f;
+  out[DE0 + 1] = -0.5f;
+  return ANDO_OK;
+}
+
+int32_t ando_ctx_set_precond_weights(ando_ctx c, const float* w, int32_t n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!w || n != net::NPARAM) return fail(ANDO_ERR_INVALID, "weights must hold ando_precond_num_params() floats");
+  CK(c->net_master.upload(w, n, c->stream));
+  CK(c->net_buf.reserve(net_dev_floats()));
+  CK(c->net_bf16.reserve(n));
+  net_dev_carve(c->net, c->net_buf.p);
+  launch_net_prepare(c->net_master.p, c->net, c->net_bf16.p, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  c->net_ready = true;
+  return ANDO_OK;
+}
+
+int32_t ando_precond_eval(ando_ctx c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready) return fail(ANDO_ERR_STATE, "mesh not uploaded");
+  rc = ensure_learned(c);
+  if (rc) return rc;
+  LsView v = ls_view(c);
+  learned_forward(v, c->net, c->lw, c->Sval.p, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  c->S_ready = true;
+  return ANDO_OK;
+}
+
+int32_t ando_last_precond(ando_ctx c, float* S) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!S) return fail(ANDO_ERR_INVALID, "null output");
+  if (!c->S_ready) return fail(ANDO_ERR_STATE, "no learned preconditioner evaluated yet");
+  CK(cudaMemcpyAsync(S, c->Sval.p, sizeof(float) * 9ull * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ANDO_OK;
+}
+
+int32_t ando_last_scaled_system(ando_ctx c, float* valh, float* xvalh, float* bhat, float* Lf, double* Linv) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready) return fail(ANDO_ERR_STATE, "mesh not uploaded");
+  cudaStream_t s = c->stream;
+  if (valh) CK(cudaMemcpyAsync(valh, c->valh.p, sizeof(float) * 9ull * c->nnzb, cudaMemcpyDeviceToHost, s));
+  if (xvalh && c->nx) CK(cudaMemcpyAsync(xvalh, c->xvalh.p, sizeof(float) * 9ull * c->nx, cudaMemcpyDeviceToHost, s));
+  if (bhat) CK(cudaMemcpyAsync(bhat, c->bhat.p, sizeof(float) * 3ull * c->V, cudaMemcpyDeviceToHost, s));
+  if (Lf) CK(cudaMemcpyAsync(Lf, c->Lf.p, sizeof(float) * 6ull * c->V, cudaMemcpyDeviceToHost, s));
+  if (Linv) CK(cudaMemcpyAsync(Linv, c->Linv.p, sizeof(double) * 6ull * c->V, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return ANDO_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ trainer
+struct ando_trainer_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf<float> master, m1, m2, grad, netbuf;
+  DevBuf<unsigned short> bf16;
+  NetDev net;
+  struct Sys {
+    int V = 0, nnzb = 0, nx = 0, P = 0;
+    double dt2inv = 0.0;
+    DevBuf<int> rowptr, cols, slot_row, slot_T, xbegin, xend, xcols;
+    DevBuf<float> valh, xvalh, Lf, probes;
+    DevBuf<double> mass, pnorm;
+    DevBuf<unsigned char> fixed;
+    LsView view() const {
+      LsView v;
+      v.V = V; v.nnzb = nnzb; v.rowptr = rowptr.p; v.cols = cols.p; v.slot_row = slot_row.p; v.slot_T = slot_T.p; v.valh = valh.p;
+      v.xbegin = nx ? xbegin.p : nullptr; v.xend = nx ? xend.p : nullptr; v.xcols = xcols.p; v.xvalh = xvalh.p;
+      v.Lf = Lf.p; v.mass = mass.p; v.fixed = fixed.p; v.dt2inv = dt2inv;
+      return v;
+    }
+  };
+  std::vector<Sys*> sys;
+  DevBuf<float> lw_buf, S, Y, Wv;
+  DevBuf<double> loss_parts, loss;
+  LearnedWork lw;
+  double* loss_host = nullptr;
+  int t = 0, next = 0;
+  ~ando_trainer_s() {
+    for (auto* p : sys) delete p;
+    if (loss_host) cudaFreeHost(loss_host);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+template <class T> cudaError_t dcopy(DevBuf<T>& dst, const T* src, size_t n, cudaStream_t s) {
+  cudaError_t e = dst.reserve(n ? n : 1);
+  if (e || !n) return e;
+  return cudaMemcpyAsync(dst.p, src, n * sizeof(T), cudaMemcpyDeviceToDevice, s);
+}
+int trainer_prepare(ando_trainer t) {
+  launch_net_prepare(t->master.p, t->net, t->bf16.p, t->stream);
+  CK(cudaGetLastError());
+  return ANDO_OK;
+}
+int trainer_loss(ando_trainer t, int idx, bool with_grad, double* loss) {
+  ando_trainer_s::Sys& S = *t->sys[idx];
+  size_t need = learned_work_floats(S.V, S.nnzb, true);
+  if (t->lw.V != S.V || t->lw.nnzb != S.nnzb || t->lw_buf.n < need) {
+    CK(t->lw_buf.reserve(need));
+    learned_work_carve(t->lw, t->lw_buf.p, S.V, S.nnzb, true);
+  }
+  CK(t->S.reserve(9ull * S.nnzb));
+  CK(t->Y.reserve(3ull * S.V * S.P)); CK(t->Wv.reserve(3ull * S.V * S.P));
+  CK(t->loss_parts.reserve(296ull * S.P)); CK(t->loss.reserve(1));
+  if (with_grad) CK(cudaMemsetAsync(t->grad.p, 0, sizeof(float) * net::NPARAM, t->stream));
+  learned_loss(S.view(), t->net, t->lw, t->S.p, S.probes.p, S.pnorm.p, S.P, t->Y.p, t->Wv.p, t->loss_parts.p, t->loss.p,
+               with_grad ? t->grad.p : nullptr, t->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(t->loss_host, t->loss.p, sizeof(double), cudaMemcpyDeviceToHost, t->stream));
+  CK(cudaStreamSynchronize(t->stream));
+  *loss = *t->loss_host;
+  return ANDO_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int32_t ando_trainer_create(int32_t device, const float* weights, int32_t n, ando_trainer* out) {
+  if (!out) return fail(ANDO_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  if (!weights || n != net::NPARAM) return fail(ANDO_ERR_INVALID, "weights must hold ando_precond_num_params() floats");
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) return fail(ANDO_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= nd) return fail(ANDO_ERR_INVALID, "device index out of range");
+  CK(cudaSetDevice(device));
+  ando_trainer t = new ando_trainer_s();
+  t->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+  if (!e) e = cudaMallocHost(&t->loss_host, sizeof(double));
+  if (!e) e = t->master.upload(weights, n, t->stream);
+  if (!e) e = t->m1.reserve(n);
+  if (!e) e = t->m2.reserve(n);
+  if (!e) e = t->grad.reserve(n);
+  if (!e) e = t->bf16.reserve(n);
+  if (!e) e = t->netbuf.reserve(net_dev_floats());
+  if (!e) e = cudaMemsetAsync(t->m1.p, 0, sizeof(float) * n, t->stream);
+  if (!e) e = cudaMemsetAsync(t->m2.p, 0, sizeof(float) * n, t->stream);
+  if (e) { delete t; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
+  net_dev_carve(t->net, t->netbuf.p);
+  int rc = trainer_prepare(t);
+  if (rc) { delete t; return rc; }
+  *out = t;
+  return ANDO_OK;
+}
+
+void ando_trainer_destroy(ando_trainer t) {
+  if (!t) return;
+  cudaSetDevice(t->device);
+  cudaStreamSynchronize(t->stream);
+  delete t;
+}
+
+int32_t ando_trainer_add_system(ando_trainer t, ando_ctx c, int32_t max_probes, double tol, int32_t max_iters) {
+  if (!t) return fail(ANDO_ERR_INVALID, "null trainer");
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (c->device != t->device) return fail(ANDO_ERR_INVALID, "trainer and context on different devices");
+  if (!c->mesh_ready || c->dt2inv <= 0.0) return fail(ANDO_ERR_STATE, "no scaled system evaluated (ando_eval_system, CORRECTED)");
+  if (max_probes < 1 || max_probes > 16 || max_iters < 1) return fail(ANDO_ERR_INVALID, "probe arguments");
+  cudaStream_t s = c->stream;
+  const int V = c->V;
+  // Block-Jacobi solve of the current scaled system to `tol`, keeping the
+  // residual and iterate after 2^k - 1 iterations: probe k is r_k with
+  // energy norm (x* - x_k)^T r_k.
+  DevBuf<float> snap_r;
+  DevBuf<double> snap_x;
+  CK(snap_r.reserve(3ull * V * max_probes));
+  CK(snap_x.reserve(3ull * V * max_probes));
+  ando_params p{};
+  p.pcg_tol = tol; p.pcg_max_iters = max_iters;
+  PcgScaledArgs sa = scaled_args(c, p);
+  sa.snap_r = snap_r.p; sa.snap_x = snap_x.p; sa.snap_max = max_probes;
+  CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (c->ctrl_host->converged) return fail(ANDO_ERR_STATE, "the evaluated Newton system had already converged (nothing was assembled)");
+  CK(launch_pcg_scaled(sa, false, c->pcg_scaled_grid, s));
+  CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (c->ctrl_host->pcg_status == PCG_TIMEOUT) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
+  int iters = c->ctrl_host->pcg_iters;
+  int taken = 0;
+  while (taken < max_probes && ((1 << taken) - 1) <= iters) ++taken;
+  std::vector<float> hr(3ull * V * taken);
+  std::vector<double> hx(3ull * V * taken), xs(3ull * V);
+  CK(cudaMemcpyAsync(hr.data(), snap_r.p, sizeof(float) * hr.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hx.data(), snap_x.p, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(xs.data(), c->xh.p, sizeof(double) * xs.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::vector<int> keep;
+  std::vector<double> norms;
+  double n0 = -1.0;
+  for (int k = 0; k < taken; ++k) {
+    double nk = 0.0;
+    const float* r = hr.data() + 3ull * V * k;
+    const double* x = hx.data() + 3ull * V * k;
+    for (size_t e = 0; e < 3ull * V; ++e) nk += (xs[e] - x[e]) * double(r[e]);
+    if (k == 0) n0 = nk;
+    if (nk > 1e-12 * std::max(n0, 0.0) && nk > 0.0) { keep.push_back(k); norms.push_back(nk); }
+  }
+  if (keep.empty()) return fail(ANDO_ERR_STATE, "system has no usable probe (zero right-hand side)");
+  auto* S = new ando_trainer_s::Sys();
+  S->V = V; S->nnzb = c->nnzb; S->nx = c->nx; S->P = int(keep.size()); S->dt2inv = c->dt2inv;
+  cudaError_t e = cudaSuccess;
+  cudaStream_t ts = s;   // copies on the context's stream, then synchronised
+  if (!e) e = dcopy(S->rowptr, c->rowptr.p, V + 1, ts);
+  if (!e) e = dcopy(S->cols, c->cols.p, c->nnzb, ts);
+  if (!e) e = dcopy(S->slot_row, c->slot_row.p, c->nnzb, ts);
+  if (!e) e = dcopy(S->slot_T, c->slot_T.p, c->nnzb, ts);
+  if (!e) e = dcopy(S->valh, c->valh.p, 9ull * c->nnzb, ts);
+  if (!e) e = dcopy(S->Lf, c->Lf.p, 6ull * V, ts);
+  if (!e) e = dcopy(S->mass, c->mass.p, V, ts);
+  if (!e) e = dcopy(S->fixed, c->fixed.p, V, ts);
+  if (!e && c->nx) {
+    e = dcopy(S->xbegin, c->xbegin.p, V, ts);
+    if (!e) e = dcopy(S->xend, c->xend.p, V, ts);
+    if (!e) e = dcopy(S->xcols, c->xcols.p, c->nx, ts);
+    if (!e) e = dcopy(S->xvalh, c->xvalh.p, 9ull * c->nx, ts);
+  }
+  if (!e) e = S->probes.reserve(3ull * V * S->P);
+  for (int q = 0; !e && q < S->P; ++q)
+    e = cudaMemcpyAsync(S->probes.p + 3ull * V * q, hr.data() + 3ull * V * keep[q], sizeof(float) * 3ull * V, cudaMemcpyHostToDevice, ts);
+  if (!e) e = S->pnorm.upload(norms.data(), norms.size(), ts);
+  if (!e) e = cudaStreamSynchronize(ts);
+  if (e) { delete S; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
+  t->sys.push_back(S);
+  return ANDO_OK;
+}
+
+int32_t ando_trainer_num_systems(ando_trainer t) { return t ? int32_t(t->sys.size()) : 0; }
+
+int32_t ando_trainer_probes(ando_trainer t, int32_t idx, float* probes, double* norms, int32_t* num) {
+  if (!t || !num || idx < 0 || idx >= int(t->sys.size())) return fail(ANDO_ERR_INVALID, "trainer system index");
+  const auto& S = *t->sys[idx];
+  *num = S.P;
+  CK(cudaSetDevice(t->device));
+  if (probes) CK(cudaMemcpy(probes, S.probes.p, sizeof(float) * 3ull * S.V * S.P, cudaMemcpyDeviceToHost));
+  if (norms) CK(cudaMemcpy(norms, S.pnorm.p, sizeof(double) * S.P, cudaMemcpyDeviceToHost));
+  return ANDO_OK;
+}
+
+int32_t ando_trainer_loss(ando_trainer t, int32_t idx, double* loss, float* grad) {
+  if (!t || !loss || idx < 0 || idx >= int(t->sys.size())) return fail(ANDO_ERR_INVALID, "trainer system index");
+  CK(cudaSetDevice(t->device));
+  int rc = trainer_loss(t, idx, grad != nullptr, loss);
+  if (rc) return rc;
+  if (grad) CK(cudaMemcpy(grad, t->grad.p, sizeof(float) * net::NPARAM, cudaMemcpyDeviceToHost));
+  return ANDO_OK;
+}
+
+int32_t ando_trainer_step(ando_trainer t, float lr, double* loss) {
+  if (!t || t->sys.empty()) return fail(ANDO_ERR_STATE, "trainer has no systems");
+  CK(cudaSetDevice(t->device));
+  int idx = t->next;
+  t->next = (t->next + 1) % int(t->sys.size());
+  double L = 0.0;
+  int rc = trainer_loss(t, idx, true, &L);
+  if (rc) return rc;
+  t->t += 1;
+  launch_adam(t->master.p, t->m1.p, t->m2.p, t->grad.p, net::NPARAM, lr, 0.9f, 0.999f, 1e-8f, t->t, t->stream);
+  rc = trainer_prepare(t);
+  if (rc) return rc;
+  if (loss) *loss = L;
+  return ANDO_OK;
+}
+
+int32_t ando_trainer_get_weights(ando_trainer t, float* w, int32_t n) {
+  if (!t || !w || n != net::NPARAM) return fail(ANDO_ERR_INVALID, "weights must hold ando_precond_num_params() floats");
+  CK(cudaSetDevice(t->device));
+  CK(cudaStreamSynchronize(t->stream));
+  CK(cudaMemcpy(w, t->master.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return ANDO_OK;
+}
+
+int32_t ando_trainer_set_weights(ando_trainer t, const float* w, int32_t n) {
+  if (!t || !w || n != net::NPARAM) return fail(ANDO_ERR_INVALID, "weights must hold ando_precond_num_params() floats");
+  CK(cudaSetDevice(t->device));
+  CK(cudaMemcpyAsync(t->master.p, w, sizeof(float) * n, cudaMemcpyHostToDevice, t->stream));
+  int rc = trainer_prepare(t);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(t->stream));
   return ANDO_OK;
 }
 

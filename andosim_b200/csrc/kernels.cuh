@@ -118,6 +118,8 @@ struct PcgScaledArgs {
   double* partials;     // 3 * grid
   Ctrl* ctrl;
   float tol; int max_iters; int stall_window;
+  // block-Jacobi solves only: snapshot k of (r^, x^) after 2^k - 1 iterations, k < snap_max
+  float* snap_r; double* snap_x; int snap_max;
 };
 int pcg_scaled_grid_size(int device, bool learned);
 cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, int grid, cudaStream_t s);

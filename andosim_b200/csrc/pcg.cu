@@ -299,6 +299,10 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
     a.xh[3 * i] = 0.0; a.xh[3 * i + 1] = 0.0; a.xh[3 * i + 2] = 0.0;
     r[3 * i] = b0; r[3 * i + 1] = b1; r[3 * i + 2] = b2;
     if (!LEARNED) rz_loc += double(b0) * b0 + double(b1) * b1 + double(b2) * b2;
+    if (!LEARNED && a.snap_r && a.snap_max > 0) {
+      a.snap_r[3 * i] = b0; a.snap_r[3 * i + 1] = b1; a.snap_r[3 * i + 2] = b2;
+      a.snap_x[3 * i] = 0.0; a.snap_x[3 * i + 1] = 0.0; a.snap_x[3 * i + 2] = 0.0;
+    }
   }
   if (LEARNED) {
     GatherV gb{a.bhat};
@@ -354,11 +358,20 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
     // ---- phase B: x^ += alpha p, r -= alpha Ap, z = S r, r^T z, |L r|_inf
     double rz_new_loc = 0.0, rinf_loc = 0.0;
     if (!LEARNED) {
+      // snapshot k of (r^, x^) after 2^k - 1 iterations (training probes)
+      const int done = it + 1;
+      const int snap = (a.snap_r && ((done & (done + 1)) == 0)) ? __ffs(done + 1) - 1 : -1;
+      float* sr = (snap >= 0 && snap < a.snap_max) ? a.snap_r + 3ll * V * snap : nullptr;
+      double* sx = sr ? a.snap_x + 3ll * V * snap : nullptr;
       for (int i = tid; i < V; i += nthreads) {
         float p0 = pnew[3 * i], p1 = pnew[3 * i + 1], p2 = pnew[3 * i + 2];
         a.xh[3 * i] += double(alpha) * p0; a.xh[3 * i + 1] += double(alpha) * p1; a.xh[3 * i + 2] += double(alpha) * p2;
         float r0 = r[3 * i] - alpha * a.Ap[3 * i], r1 = r[3 * i + 1] - alpha * a.Ap[3 * i + 1], r2 = r[3 * i + 2] - alpha * a.Ap[3 * i + 2];
         r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
+        if (sr) {
+          sr[3 * i] = r0; sr[3 * i + 1] = r1; sr[3 * i + 2] = r2;
+          sx[3 * i] = a.xh[3 * i]; sx[3 * i + 1] = a.xh[3 * i + 1]; sx[3 * i + 2] = a.xh[3 * i + 2];
+        }
         rz_new_loc += double(r0) * r0 + double(r1) * r1 + double(r2) * r2;
         rinf_loc = fmax(rinf_loc, unscaled_inf(a.Lf, i, r0, r1, r2));
       }
@@ -441,7 +454,10 @@ int pcg_scaled_grid_size(int device, bool learned) {
 }
 
 cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, int grid, cudaStream_t s) {
-  int need = (a.V + PCG_TPB - 1) / PCG_TPB;
+  // both phases of a learned iteration (and phase A of block Jacobi) are
+  // warp-per-row products: enough CTAs for about 4 rows per warp, up to the
+  // co-resident grid
+  int need = (a.V + 4 * PCG_WARPS - 1) / (4 * PCG_WARPS);
   if (need < 1) need = 1;
   if (grid > need) grid = need;
   void* args[] = {(void*)&a};

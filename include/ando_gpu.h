@@ -282,6 +282,61 @@ ANDO_API int32_t ando_pcg_solve_noalloc(int32_t device, void* stream, int32_t nu
                                         int64_t work_floats, double tol, int32_t max_iters, int32_t* iterations,
                                         int32_t* pcg_status, double* rel_residual);
 
+/* ---------------------------------------------------------------------------
+ * Learned preconditioner (no reference counterpart: the reference's only
+ * preconditioner is block Jacobi, pcg_solver.cpp:77-114).
+ *
+ * In CORRECTED semantics the PCG runs on the block-scaled system
+ * A^ = L^-1 A L^-T (A_ii = L_i L_i^T). With params.precond =
+ * ANDO_PRECOND_LEARNED a mesh-graph message-passing network (3 layers, 64
+ * wide, BF16 weights, FP32 accumulation) turns per-vertex and per-edge
+ * features of A^ into a symmetric positive definite block-sparse S ~ A^-1 on
+ * the mesh pattern:
+ *   S = sum_i delta_i E_ii + sum_{edges i<j} W_e W_e^T,  W_e = [a_e I ; b_e A^_ij^T],
+ * delta_i > 0. A solve whose S loses definiteness, stalls or reaches the
+ * iteration cap is redone with block Jacobi (ando_step_stats.precond_fallbacks).
+ * Weights are a flat float vector of ando_precond_num_params() entries. */
+ANDO_API int32_t ando_precond_num_params(void);
+/* Deterministic initial weights for `seed` (starts near S = 0.25 (2 I - A^)). */
+ANDO_API int32_t ando_precond_init_weights(uint64_t seed, float* out, int32_t n);
+/* Load weights into a context (rounded to BF16 for inference). */
+ANDO_API int32_t ando_ctx_set_precond_weights(ando_ctx ctx, const float* weights, int32_t n);
+/* Evaluate S for the context's current scaled system (after ando_eval_system
+ * or a CORRECTED step) without solving; read it with ando_last_precond. */
+ANDO_API int32_t ando_precond_eval(ando_ctx ctx);
+/* S of the last learned evaluation: 9 floats per static pattern slot. */
+ANDO_API int32_t ando_last_precond(ando_ctx ctx, float* S);
+/* The scaled system of the last CORRECTED Newton iteration: A^ on the static
+ * pattern (9 * nnzb), A^ of the contact blocks of ando_last_contact_blocks
+ * (9 * count), b^ = L^-1 b (3 V), L packed lower-triangular per vertex
+ * (6 V, FP32) and L^-1 (6 V, FP64). Any pointer may be NULL. */
+ANDO_API int32_t ando_last_scaled_system(ando_ctx ctx, float* valh, float* xvalh, float* bhat, float* Lf, double* Linv);
+
+/* Training of the preconditioner on the device (forward and backward
+ * kernels of this library, Adam). A trainer holds weights, optimiser state
+ * and a set of scaled Newton systems, each with probe vectors dumped by the
+ * solver itself: the residuals of a block-Jacobi solve after 2^k - 1
+ * iterations. The loss of a system is the mean over its probes r of the
+ * relative energy error of one preconditioned step, 1 + (y^T A^ y - 2 r^T y)
+ * / (r^T A^-1 r) with y = S r. */
+typedef struct ando_trainer_s* ando_trainer;
+ANDO_API int32_t ando_trainer_create(int32_t device, const float* weights, int32_t n, ando_trainer* out);
+ANDO_API void ando_trainer_destroy(ando_trainer t);
+/* Add the context's current scaled system (ando_eval_system in CORRECTED
+ * semantics), solving it with block Jacobi to `tol` (at most `max_iters`
+ * iterations) to record up to `max_probes` probes. */
+ANDO_API int32_t ando_trainer_add_system(ando_trainer t, ando_ctx ctx, int32_t max_probes, double tol, int32_t max_iters);
+ANDO_API int32_t ando_trainer_num_systems(ando_trainer t);
+/* Probes of system `idx` (3 V floats each) and their energy norms. */
+ANDO_API int32_t ando_trainer_probes(ando_trainer t, int32_t idx, float* probes, double* norms, int32_t* num);
+/* Loss of system `idx` at the current weights; with `grad` (num_params
+ * floats) also its gradient w.r.t. the FP32 master weights. */
+ANDO_API int32_t ando_trainer_loss(ando_trainer t, int32_t idx, double* loss, float* grad);
+/* One Adam step (beta 0.9 / 0.999) on the next system in turn. */
+ANDO_API int32_t ando_trainer_step(ando_trainer t, float lr, double* loss);
+ANDO_API int32_t ando_trainer_get_weights(ando_trainer t, float* weights, int32_t n);
+ANDO_API int32_t ando_trainer_set_weights(ando_trainer t, const float* weights, int32_t n);
+
 #ifdef __cplusplus
 }
 #endif
