@@ -47,7 +47,7 @@ class Params(C.Structure):
         ("friction_tangent_threshold", C.c_double), ("velocity_damping", C.c_double), ("contact_restitution", C.c_double),
         ("enable_strain_limiting", C.c_int32), ("strain_limit", C.c_double), ("strain_tau", C.c_double),
         ("strain_epsilon", C.c_double), ("strain_svd_epsilon", C.c_double), ("hessian_epsilon", C.c_double),
-        ("min_gap", C.c_double), ("semantics", C.c_int32), ("precond", C.c_int32),
+        ("min_gap", C.c_double), ("semantics", C.c_int32), ("precond", C.c_int32), ("precond_refresh", C.c_int32),
     ]
 
 
@@ -97,10 +97,13 @@ class Contact(C.Structure):
 
 class Profile(C.Structure):
     _fields_ = [("launches", C.c_int64), ("phase_launches", C.c_int64 * 7), ("phase_ms", C.c_double * 7),
-                ("pcg_iterations", C.c_int64), ("newton_iterations", C.c_int64)]
+                ("pcg_iterations", C.c_int64), ("newton_iterations", C.c_int64), ("pcg_learned_iterations", C.c_int64),
+                ("pcg_extra_block_iterations", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {"launches": self.launches, "pcg_iterations": self.pcg_iterations, "newton_iterations": self.newton_iterations,
+                "pcg_learned_iterations": self.pcg_learned_iterations,
+                "pcg_extra_block_iterations": self.pcg_extra_block_iterations,
                 "phase_ms": {p: self.phase_ms[i] for i, p in enumerate(PHASES)},
                 "phase_launches": {p: self.phase_launches[i] for i, p in enumerate(PHASES)}}
 
@@ -228,7 +231,7 @@ def lumped_masses(num_vertices: int, triangles: np.ndarray, area: np.ndarray, th
     return m
 
 
-def make_params(params: dict, semantics: str = "reference", precond: str = "block_jacobi") -> Params:
+def make_params(params: dict, semantics: str = "reference", precond: str = "block_jacobi", precond_refresh: int = 1) -> Params:
     """Params with the reference's SimParams defaults (types.h:60-100), overridden by `params`."""
     d = dict(dt=0.002, beta_max=0.25, min_newton_steps=2, max_newton_steps=8, friction_min_newton_steps=32,
              pcg_tol=1e-3, pcg_max_iters=1000, contact_gap_max=0.001, wall_gap=0.001, enable_ccd=1,
@@ -239,12 +242,13 @@ def make_params(params: dict, semantics: str = "reference", precond: str = "bloc
     d.update({k: v for k, v in params.items()})
     p = Params()
     for name, typ in Params._fields_:
-        if name in ("semantics", "precond"):
+        if name in ("semantics", "precond", "precond_refresh"):
             continue
         val = d[name]
         setattr(p, name, int(val) if typ is C.c_int32 else float(val))
     p.semantics = SEMANTICS[semantics]
     p.precond = PRECOND[precond]
+    p.precond_refresh = int(precond_refresh)
     return p
 
 

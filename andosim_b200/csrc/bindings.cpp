@@ -69,6 +69,7 @@ struct SimParams {
   // GPU-only knobs
   std::string semantics = "reference";
   std::string preconditioner = "block_jacobi";
+  int precond_refresh = 1;
 };
 
 struct Triangle { int32_t v[3] = {-1, -1, -1}; };
@@ -219,24 +220,37 @@ struct RigidBody {
 // and must be uploaded before the next GPU call.
 struct State {
   std::vector<V3> x, v, xp;
+  std::vector<V3> start;          // CORRECTED: where the next step starts (ando_state_set_start)
   std::vector<double> m;
   ando_ctx ctx = nullptr;
-  uint64_t topo = 0, verts = 0;
+  uint64_t topo = 0, verts = 0, weights = 0;
   bool device_newer = false, host_dirty = true, masses_dirty = true;
   ando_step_stats last{};
 
   State() = default;
-  State(const State& o) : x(o.x), v(o.v), xp(o.xp), m(o.m) {}
+  State(const State& o) : x(o.x), v(o.v), xp(o.xp), start(o.start), m(o.m) {}
   ~State() { if (ctx) ando_ctx_destroy(ctx); }
 
   size_t nv() const { return x.size(); }
   static int& device() { static int d = 0; return d; }
+  // Learned-preconditioner weights shared by every state (set_precond_weights);
+  // a state loads them into its context when it first steps with them.
+  static std::vector<float>& precond_weights() { static std::vector<float> w; return w; }
+  static uint64_t& precond_version() { static uint64_t v = 0; return v; }
+  void bind_weights() {
+    if (weights == precond_version() || precond_weights().empty()) return;
+    check(ando_ctx_set_precond_weights(ctx, precond_weights().data(), int32_t(precond_weights().size())), "preconditioner weights");
+    weights = precond_version();
+  }
 
   void sync_host() {
     if (!device_newer || !ctx) return;
     std::vector<double> hx(3 * nv()), hv(3 * nv());
     check(ando_state_download(ctx, hx.data(), hv.data(), int32_t(nv())), "state download");
     for (size_t i = 0; i < nv(); ++i) { x[i] = {hx[3 * i], hx[3 * i + 1], hx[3 * i + 2]}; v[i] = {hv[3 * i], hv[3 * i + 1], hv[3 * i + 2]}; }
+    check(ando_state_get_start(ctx, hx.data(), int32_t(nv())), "state start");
+    start.resize(nv());
+    for (size_t i = 0; i < nv(); ++i) start[i] = {hx[3 * i], hx[3 * i + 1], hx[3 * i + 2]};
     device_newer = false;
   }
   static std::vector<double> flat(const std::vector<V3>& a) {
@@ -266,6 +280,10 @@ struct State {
       std::vector<double> fx = flat(x), fv = flat(v), fp = flat(xp);
       check(ando_state_upload(ctx, fx.data(), fv.data(), fp.data(), m.data(), int32_t(nv())), "state upload");
       host_dirty = false; masses_dirty = false;
+      if (start.size() == nv()) {     // the upload made x the start; put the real one back
+        std::vector<double> fs = flat(start);
+        check(ando_state_set_start(ctx, fs.data(), int32_t(nv())), "state start");
+      }
     }
   }
 };
@@ -415,7 +433,7 @@ void mesh_initialize(Mesh& me, std::vector<V3> verts, std::vector<int32_t> tris,
 
 void state_initialize(State& s, const Mesh& me) {
   if (me.nv() == 0) throw std::invalid_argument("Mesh must be initialised before creating a state");
-  s.x = me.vertices; s.xp = me.vertices;
+  s.x = me.vertices; s.xp = me.vertices; s.start = me.vertices;
   s.v.assign(me.nv(), V3{});
   s.m.assign(me.nv(), 0.0);
   for (size_t f = 0; f < me.nt(); ++f) {
@@ -442,6 +460,7 @@ ando_params to_abi(const SimParams& p) {
   if (p.preconditioner == "block_jacobi") a.precond = ANDO_PRECOND_BLOCK_JACOBI;
   else if (p.preconditioner == "learned") a.precond = ANDO_PRECOND_LEARNED;
   else throw py::value_error("preconditioner must be 'block_jacobi' or 'learned'");
+  a.precond_refresh = p.precond_refresh;
   return a;
 }
 
@@ -479,6 +498,13 @@ PYBIND11_MODULE(ando_barrier_core, m) {
   m.attr("ABI_VERSION") = ando_abi_version();
   m.def("set_device", [](int d) { State::device() = d; }, "CUDA device for states created from now on (default 0)");
   m.def("get_device", []() { return State::device(); });
+  m.def("set_precond_weights", [](py::array_t<float, py::array::c_style | py::array::forcecast> w) {
+    if (w.ndim() != 1 || w.shape(0) != ando_precond_num_params())
+      throw py::value_error("weights must be a flat array of precond_num_params() floats");
+    State::precond_weights().assign(w.data(), w.data() + w.shape(0));
+    State::precond_version()++;
+  }, "Weights of the learned preconditioner (SimParams.preconditioner = 'learned') for every state");
+  m.def("precond_num_params", []() { return ando_precond_num_params(); });
 
   py::class_<Material>(m, "Material")
       .def(py::init<>())
@@ -517,7 +543,8 @@ PYBIND11_MODULE(ando_barrier_core, m) {
       .def_readwrite("strain_epsilon", &SimParams::strain_epsilon).def_readwrite("strain_svd_epsilon", &SimParams::strain_svd_epsilon)
       .def_readwrite("hessian_epsilon", &SimParams::hessian_epsilon).def_readwrite("min_gap", &SimParams::min_gap)
       // GPU-only knobs
-      .def_readwrite("semantics", &SimParams::semantics).def_readwrite("preconditioner", &SimParams::preconditioner);
+      .def_readwrite("semantics", &SimParams::semantics).def_readwrite("preconditioner", &SimParams::preconditioner)
+      .def_readwrite("precond_refresh", &SimParams::precond_refresh);
 
   py::class_<Triangle>(m, "Triangle")
       .def(py::init<>())
@@ -592,7 +619,7 @@ PYBIND11_MODULE(ando_barrier_core, m) {
       .def("set_positions64", [](State& s, py::object p) {
         auto v = to_v3(p, "positions");
         if (v.size() != s.nv()) throw py::value_error("positions must have one row per vertex");
-        s.sync_host(); s.x = v; s.host_dirty = true;
+        s.sync_host(); s.x = v; s.start = v; s.host_dirty = true;
       })
       .def("_stream_handle", [](State& s) -> uintptr_t {
         if (!s.ctx) return 0;
@@ -694,6 +721,7 @@ PYBIND11_MODULE(ando_barrier_core, m) {
       .def_static("step", [](Mesh& me, State& s, Constraints& c, const SimParams& p, py::object rigid_list) {
         ando_params ap = to_abi(p);
         s.bind(me);
+        if (ap.precond == ANDO_PRECOND_LEARNED) s.bind_weights();
         std::vector<ando_pin> pins;
         for (auto& q : c.pins) pins.push_back({q.vertex, q.active ? 1 : 0, {q.target.x, q.target.y, q.target.z}});
         std::vector<ando_wall> walls;

@@ -84,6 +84,7 @@ struct ando_ctx_s {
   DevBuf<unsigned char> chol_ok;
   int pcg_scaled_grid = 1, pcg_learned_grid = 1;
   double dt2inv = 0.0;             // of the last assembled system
+  double gap_max = 1e-3;           // contact activation distance of the current step
 
   // learned preconditioner: weights, activations, S on the static pattern
   DevBuf<int> slot_T;
@@ -92,6 +93,9 @@ struct ando_ctx_s {
   NetDev net;
   LearnedWork lw;
   bool net_ready = false, S_ready = false;
+  bool coeff_valid = false;        // lw.zv / lw.ab hold network outputs for this mesh
+  int coeff_age = 0;               // Newton iterations since the network last ran
+  long long coeff_mesh = -1;
 
   // contacts
   DevBuf<int> det_counts, det_offsets;
@@ -125,9 +129,11 @@ struct ando_ctx_s {
   long long mesh_generation = 0;
 
   // CORRECTED semantics
+  DevBuf<double> x_safe;           // where the last step ended (or the uploaded positions): start of the next CORRECTED step
+  bool safe_valid = false;
   DevBuf<unsigned char> fixed;
   DevBuf<double> g_el_x, x1, ext;
-  DevBuf<unsigned long long> toi, emax_cap;
+  DevBuf<unsigned long long> toi;
   double max_move = 1e300;   // 4 x mean rest edge length: largest displacement per Newton iteration
   DevBuf<int2> pairs_ee;
 
@@ -522,7 +528,7 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
 int corrected_line_search(ando_ctx c, int nb) {
   cudaStream_t s = c->stream;
   Phase ph(c, ANDO_PHASE_LINE_SEARCH);
-  launch_swept_end(c->V, c->x.p, c->d.p, c->fixed.p, 1.25, c->max_move, c->emax_cap.p, c->x1.p, c->ext.p, s);
+  launch_swept_end(c->V, c->x.p, c->d.p, c->fixed.p, 1.25, c->max_move, c->x1.p, c->ext.p, s);
   launch_toi_reset(c->toi.p, s);
   launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
   ph.launched(2 + (c->num_walls ? 1 : 0));
@@ -533,9 +539,9 @@ int corrected_line_search(ando_ctx c, int nb) {
   CK(c->bvh_edge.build(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->cub_tmp, s));
   CK(c->bvh_edge.query(c->x.p, c->x1.p, 1, c->edges.p, c->E, 0.f, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
-  if (nvt + nee) { launch_toi_pairs(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, c->ext.p, c->toi.p, s); ph.launched(); }
+  if (nvt + nee) { launch_toi_pairs(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, c->ext.p, 0.0, 1e-3 * c->gap_max, c->toi.p, s); ph.launched(); }
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
-  launch_update_toi(c->V, c->x.p, c->d.p, c->fixed.p, c->ctrl.p, c->toi.p, c->emax_cap.p, s);
+  launch_update_toi(c->V, c->x.p, c->ext.p, 1.25, c->fixed.p, c->ctrl.p, c->toi.p, s);
   ph.launched();
   CK(cudaGetLastError());
   return ANDO_OK;
@@ -627,15 +633,29 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
     int rc = ensure_learned(c);
     if (rc) return rc;
     LsView v = ls_view(c);
-    learned_forward(v, c->net, c->lw, c->Sval.p, s);
+    const int refresh = p.precond_refresh > 1 ? p.precond_refresh : 1;
+    if (!c->coeff_valid || c->coeff_mesh != c->mesh_generation || c->coeff_age >= refresh) {
+      learned_forward(v, c->net, c->lw, c->Sval.p, s);
+      c->coeff_valid = true; c->coeff_mesh = c->mesh_generation; c->coeff_age = 1;
+      ph.launched(5 + 3 * net::NL);
+    } else {
+      learned_build_S(v, c->lw, c->Sval.p, s);
+      c->coeff_age++;
+      ph.launched();
+    }
     c->S_ready = true;
     sa.S = c->Sval.p;
     CK(launch_pcg_scaled(sa, true, c->pcg_learned_grid, s));
-    ph.launched(5 + 3 * net::NL + 1);
+    ph.launched();
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     const Ctrl& h = *c->ctrl_host;
+    c->profile.pcg_learned_iterations += h.pcg_iters;
     if (h.converged || h.pcg_status == PCG_OK || h.pcg_status == PCG_TIMEOUT) return ANDO_OK;
+    // the learned attempt's iterations count as work done; the caller adds the final solve's
+    c->profile.pcg_iterations += h.pcg_iters;
+    c->profile.pcg_extra_block_iterations += (long long)h.pcg_iters * c->nx;
+    st.pcg_iters += h.pcg_iters;
     st.precond_fallbacks++;
     sa.S = nullptr;
   }
@@ -673,6 +693,7 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
     st.newton_iters++;
     st.pcg_iters += h.pcg_iters;
     c->profile.pcg_iterations += h.pcg_iters;
+    c->profile.pcg_extra_block_iterations += (long long)h.pcg_iters * c->nx;
     c->profile.newton_iterations += 1;
     st.pcg_max_per_newton = std::max(st.pcg_max_per_newton, h.pcg_iters);
     if (!h.pcg_converged) st.pcg_not_converged++;
@@ -684,15 +705,52 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
   return ANDO_OK;
 }
 
-// Kinematic pins of the CORRECTED step: pinned vertices sit on their targets.
-int apply_pins(ando_ctx c) {
+// CORRECTED: the step starts where the previous one ended (or at the
+// caller's uploaded positions). State.apply_gravity's position update is an
+// explicit, collision-unchecked move; the implicit predictor x_hat = x + dt v
+// already carries its velocity change.
+int restore_start(ando_ctx c) {
+  if (!c->safe_valid) return ANDO_OK;
+  CK(cudaMemcpyAsync(c->x.p, c->x_safe.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, c->stream));
+  return ANDO_OK;
+}
+
+int remember_safe(ando_ctx c) {
+  CK(cudaMemcpyAsync(c->x_safe.p, c->x.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, c->stream));
+  c->safe_valid = true;
+  return ANDO_OK;
+}
+
+// Kinematic pins of the CORRECTED step: pinned vertices move toward their
+// targets as far as the move's conservative time of impact allows (walls,
+// self contact, rigid triangles; a teleported pin would drag the cloth into
+// itself), then stay fixed for the step.
+int apply_pins(ando_ctx c, int nb) {
   cudaStream_t s = c->stream;
   CK(cudaMemsetAsync(c->fixed.p, 0, c->V, s));
-  if (c->num_pins) {
-    Phase ph(c, ANDO_PHASE_SETUP);
-    launch_pin_apply(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->fixed.p, s);
+  if (!c->num_pins) return ANDO_OK;
+  Phase ph(c, ANDO_PHASE_SETUP);
+  CK(cudaMemsetAsync(c->ext.p, 0, sizeof(double) * 3ull * c->V, s));
+  CK(cudaMemcpyAsync(c->x1.p, c->x.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, s));
+  launch_pin_ext(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->ext.p, c->x1.p, c->fixed.p, s);
+  launch_toi_reset(c->toi.p, s);
+  launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
+  ph.launched(2 + (c->num_walls ? 1 : 0));
+  int nvt = 0, nee = 0;
+  long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
+  CK(c->bvh_tri.build(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->cub_tmp, s));
+  CK(c->bvh_tri.query(c->x.p, c->x1.p, 0, nullptr, c->V, 0.f, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
+  CK(c->bvh_edge.build(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->cub_tmp, s));
+  CK(c->bvh_edge.query(c->x.p, c->x1.p, 1, c->edges.p, c->E, 0.f, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
+  ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
+  if (nvt + nee) {
+    launch_toi_pairs(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, c->ext.p, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, s);
     ph.launched();
   }
+  if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
+  launch_pin_move(c->pin_vertex.p, c->num_pins, c->ext.p, c->toi.p, c->x.p, s);
+  ph.launched();
+  CK(cudaGetLastError());
   return ANDO_OK;
 }
 
@@ -894,7 +952,14 @@ int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_ri
   }
   st.beta = beta;
   Phase ph(c, ANDO_PHASE_FINISH);
-  if (beta > 1e-6) {
+  if (corrected) {
+    // CORRECTED: v = (x - x_old) / dt. The reference divides by beta dt,
+    // which turns the error-reduction pass of a step whose line search held
+    // beta near zero into an arbitrarily large velocity.
+    double damp = p.velocity_damping > 0.0 ? 1.0 - std::min(std::max(p.velocity_damping, 0.0), 1.0) : 1.0;
+    launch_velocity(c->V, c->x.p, c->x_old.p, p.dt, damp, c->v.p, s);
+    ph.launched();
+  } else if (beta > 1e-6) {
     double damp = p.velocity_damping > 0.0 ? 1.0 - std::min(std::max(p.velocity_damping, 0.0), 1.0) : 1.0;
     launch_velocity(c->V, c->x.p, c->x_old.p, beta * p.dt, damp, c->v.p, s);
     ph.launched();
@@ -1076,7 +1141,6 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->Linv.reserve(6ull * V)); CK(c->Lf.reserve(6ull * V)); CK(c->bhat.reserve(3ull * V)); CK(c->chol_ok.reserve(V));
   CK(c->valh.reserve(9ull * nnzb)); CK(c->xh.reserve(3ull * V)); CK(c->r2.reserve(3ull * V));
   CK(c->sflags.reserve(std::max(T, 1))); CK(c->sv.reserve(2ull * std::max(T, 1)));
-  CK(c->emax_cap.reserve(2));
   {
     double sum = 0.0;
     for (size_t e = 0; e + 1 < edges.size(); e += 2) {
@@ -1085,11 +1149,12 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     }
     c->max_move = edges.empty() ? 1e300 : 4.0 * sum / double(edges.size() / 2);
   }
-  CK(c->fixed.reserve(V)); CK(c->g_el_x.reserve(3ull * V)); CK(c->x1.reserve(3ull * V)); CK(c->ext.reserve(3ull * V)); CK(c->toi.reserve(1));
+  CK(c->fixed.reserve(V)); CK(c->x_safe.reserve(3ull * V)); CK(c->g_el_x.reserve(3ull * V)); CK(c->x1.reserve(3ull * V)); CK(c->ext.reserve(3ull * V)); CK(c->toi.reserve(1));
   CK(cudaMemsetAsync(c->fixed.p, 0, V, s));
   CK(cudaMemsetAsync(c->sflags.p, 0, std::max(T, 1), s));
   CK(cudaMemsetAsync(c->d.p, 0, sizeof(float) * 3ull * V, s));
   c->el_semantics = -1;
+  c->safe_valid = false;
   c->mesh_generation++;
   c->mesh_ready = true;
   c->state_ready = false;
@@ -1118,12 +1183,37 @@ int32_t ando_state_upload(ando_ctx c, const double* x, const double* v, const do
   if (!c->mesh_ready) return fail(ANDO_ERR_STATE, "mesh not uploaded");
   if (V != c->V) return fail(ANDO_ERR_INVALID, "vertex count mismatch");
   if (!c->state_ready && (!x || !v || !xp || !mass)) return fail(ANDO_ERR_INVALID, "first state upload needs every array");
-  if (x) CK(cudaMemcpyAsync(c->x.p, x, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
+  if (x) {
+    CK(cudaMemcpyAsync(c->x.p, x, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->x_safe.p, x, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
+    c->safe_valid = true;
+  }
   if (v) CK(cudaMemcpyAsync(c->v.p, v, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
   if (xp) CK(cudaMemcpyAsync(c->x_prev.p, xp, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
   if (mass) CK(cudaMemcpyAsync(c->mass.p, mass, sizeof(double) * V, cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->state_ready = true;
+  return ANDO_OK;
+}
+
+int32_t ando_state_set_start(ando_ctx c, const double* x, int32_t V) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->state_ready) return fail(ANDO_ERR_STATE, "state not uploaded");
+  if (!x || V != c->V) return fail(ANDO_ERR_INVALID, "start positions");
+  CK(cudaMemcpyAsync(c->x_safe.p, x, sizeof(double) * 3ull * V, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->safe_valid = true;
+  return ANDO_OK;
+}
+
+int32_t ando_state_get_start(ando_ctx c, double* x, int32_t V) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->state_ready || !c->safe_valid) return fail(ANDO_ERR_STATE, "state not uploaded");
+  if (!x || V != c->V) return fail(ANDO_ERR_INVALID, "start positions");
+  CK(cudaMemcpyAsync(x, c->x_safe.p, sizeof(double) * 3ull * V, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return ANDO_OK;
 }
 
@@ -1174,6 +1264,11 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
   StepParams sp;
   rc = upload_constraints(c, p, pins, num_pins, walls, num_walls, rigids, num_rigids, sp);
   if (rc) return rc;
+  c->gap_max = p.contact_gap_max;
+  if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
+    rc = restore_start(c);
+    if (rc) return rc;
+  }
   {
     Phase ph(c, ANDO_PHASE_SETUP);
     launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
@@ -1196,6 +1291,8 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     }
     if (c->use_graphs && c->frame_exec) {
       CK(cudaGraphLaunch(c->frame_exec, s));
+      rc = remember_safe(c);
+      if (rc) return rc;
       CK(cudaEventRecord(c->ev1, s));
       CK(cudaEventSynchronize(c->ev1));
       const StepCtl& h = *c->sctl_host;
@@ -1216,7 +1313,7 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     }
   }
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
-    rc = apply_pins(c);
+    rc = apply_pins(c, num_rigids);
     if (rc) return rc;
   } else {
     rc = detect(c, num_rigids);
@@ -1226,6 +1323,8 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     if (rc) return rc;
   }
   rc = step_body(c, p, sp, num_rigids, num_walls, st);
+  if (rc) return rc;
+  rc = remember_safe(c);
   if (rc) return rc;
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev1, s));
@@ -1258,10 +1357,15 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   rc = upload_constraints(c, p, pins, num_pins, walls, num_walls, copy.data(), num_rigids, sp);
   if (rc) return rc;
   cudaStream_t s = c->stream;
+  c->gap_max = p.contact_gap_max;
+  if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
+    rc = restore_start(c);
+    if (rc) return rc;
+  }
   launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
   MeshDev m = c->mesh_dev();
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
-    rc = apply_pins(c);
+    rc = apply_pins(c, num_rigids);
     if (rc) return rc;
     rc = corrected_gradient(c, p, sp, num_rigids);
     if (rc) return rc;
@@ -1455,6 +1559,7 @@ int32_t ando_ctx_set_precond_weights(ando_ctx c, const float* w, int32_t n) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   c->net_ready = true;
+  c->coeff_valid = false;
   return ANDO_OK;
 }
 
@@ -1469,6 +1574,7 @@ int32_t ando_precond_eval(ando_ctx c) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   c->S_ready = true;
+  c->coeff_valid = true; c->coeff_mesh = c->mesh_generation; c->coeff_age = 1;
   return ANDO_OK;
 }
 

@@ -128,29 +128,43 @@ __global__ void k_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int
   out[k] = C;
 }
 
-// Largest extended displacement |1.25 d_i| over free vertices (max-reduction on IEEE bits).
-__global__ void k_ext_max(int V, const float* d, const unsigned char* fixed, double ext_scale, unsigned long long* emax) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double e = 0.0;
-  if (i < V && !(fixed && fixed[i])) {
-    double a = d[3 * i], b = d[3 * i + 1], c = d[3 * i + 2];
-    e = ext_scale * sqrt(a * a + b * b + c * c);
+// Kinematic pins: flag the vertex, and its wanted move (target - x) into ext
+// and x1 = target (several pins on one vertex: the last in list order wins).
+__global__ void k_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
+                          unsigned char* fixed) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= num_pins) return;
+  int v = pin_vertex[k];
+  if (k + 1 < num_pins && pin_vertex[k + 1] == v) return;
+  for (int q = 0; q < 3; ++q) { ext[3 * v + q] = pin_target[3 * k + q] - x[3 * v + q]; x1[3 * v + q] = pin_target[3 * k + q]; }
+  fixed[v] = 1;
+}
+// x += toi * ext on pinned vertices (toi: the move's conservative time of impact).
+__global__ void k_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= num_pins) return;
+  int v = pin_vertex[k];
+  if (k + 1 < num_pins && pin_vertex[k + 1] == v) return;
+  double t = fmin(1.0, __longlong_as_double((long long)*toi));
+  if (t >= 1.0) {   // exactly on the target
+    for (int q = 0; q < 3; ++q) x[3 * v + q] += ext[3 * v + q];
+    return;
   }
-  for (int o = 16; o; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
-  if ((threadIdx.x & 31) == 0 && e > 0.0) atomicMax(emax, (unsigned long long)__double_as_longlong(e));
+  for (int q = 0; q < 3; ++q) x[3 * v + q] += t * ext[3 * v + q];
 }
 
-// ext = cap * 1.25 d with cap = min(1, lmax / max|1.25 d|) (no vertex moves
-// more than lmax in one Newton iteration); x1 = x + ext. cap is stored in
-// emax_cap[1] for the position update.
+// ext = 1.25 d, clipped vertex by vertex to length lmax (no vertex moves
+// more than lmax in one Newton iteration; a single runaway entry of d no
+// longer scales the whole step down); x1 = x + ext.
 __global__ void k_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double ext_scale, double lmax,
-                            unsigned long long* emax_cap, double* x1, double* ext) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double emax = __longlong_as_double((long long)emax_cap[0]);
-  double cap = emax > lmax ? lmax / emax : 1.0;
-  if (i == 0) emax_cap[1] = (unsigned long long)__double_as_longlong(cap);
-  if (i >= 3 * V) return;
-  double e = fixed && fixed[i / 3] ? 0.0 : cap * (ext_scale * double(d[i]));
+                            double* x1, double* ext) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3ll * V) return;
+  long long v = i / 3;
+  double a = ext_scale * double(d[3 * v]), b = ext_scale * double(d[3 * v + 1]), c = ext_scale * double(d[3 * v + 2]);
+  double len = sqrt(a * a + b * b + c * c);
+  double cap = len > lmax ? lmax / len : 1.0;
+  double e = fixed && fixed[v] ? 0.0 : cap * (ext_scale * double(d[i]));
   ext[i] = e;
   x1[i] = x[i] + e;
 }
@@ -181,12 +195,41 @@ __global__ void k_toi_walls(int V, const double* x, const double* ext, const Wal
 
 // Conservative advancement: the distance of a pair cannot shrink faster than
 // l (sum of the largest displacements of either side) per unit time, so
-// stepping by (d - eta) / l never skips contact; stop at eta = d0 / 10.
-template <class F> __device__ inline double advance(F dist, double l) {
+// stepping by (d - eta) / l never skips contact; stop at eta = d0 / 10. A
+// pair that already touches (d0 = 0; only a kinematic pin snap can make one)
+// cannot be advanced conservatively and does not bound the step: with it in,
+// every later line search of the scene would return 0 and freeze the cloth.
+// With eta_min > 0 (the kinematic pin pass) the move may not bring a pair
+// closer than eta_min at all: pins that keep consuming 90% of a gap every
+// frame would squeeze it to nothing, and no later line search could separate
+// the pair.
+//
+// A pair closer than `near` at the start is where conservative advancement
+// breaks down: it cannot tell a pair moving apart from one closing in, so it
+// returns t ~ d0 / l and a pair squeezed to 1e-12 m would freeze every later
+// line search. Such a pair is sampled instead (geometric times 2^-40..2^-1,
+// then 0.5..1 in steps of 1/32): the step is allowed up to the last sample
+// before the distance first falls below half its starting value.
+template <class F> __device__ inline double advance(F dist, double l, double eta_min, double near) {
   if (!(l > 0.0)) return 1.0;
   double d0 = dist(0.0);
-  if (!(d0 > 0.0)) return 0.0;
-  double eta = 0.1 * d0, t = 0.0, d = d0;
+  if (!(d0 > 0.0)) return 1.0;
+  if (d0 <= eta_min) return 0.0;
+  if (d0 < near) {
+    double prev = 0.0;
+    for (int k = 40; k >= 1; --k) {
+      double ts = ldexp(1.0, -k);
+      if (!(dist(ts) >= 0.5 * d0)) return prev;
+      prev = ts;
+    }
+    for (int k = 17; k <= 32; ++k) {
+      double ts = double(k) / 32.0;
+      if (!(dist(ts) >= 0.5 * d0)) return prev;
+      prev = ts;
+    }
+    return 1.0;
+  }
+  double eta = fmax(0.1 * d0, eta_min), t = 0.0, d = d0;
   for (int it = 0; it < 200; ++it) {
     if (it) d = dist(t);
     if (d <= eta) return t;
@@ -197,7 +240,7 @@ template <class F> __device__ inline double advance(F dist, double l) {
 }
 
 __global__ void k_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges,
-                            const double* x, const double* ext, unsigned long long* toi) {
+                            const double* x, const double* ext, double eta_min, double near, unsigned long long* toi) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   double t = 1.0;
   if (k < nvt + nee) {
@@ -209,10 +252,12 @@ __global__ void k_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, co
     for (int q = 0; q < 4; ++q) { p[q] = ld3(x, id[q]); e[q] = ld3(ext, id[q]); L[q] = nrm(e[q]); }
     if (k < nvt) {
       double l = L[0] + fmax(L[1], fmax(L[2], L[3]));
-      t = advance([&](double s) { d3 n, wq; return pt_dist(p[0] + e[0] * s, p[1] + e[1] * s, p[2] + e[2] * s, p[3] + e[3] * s, n, wq); }, l);
+      t = advance([&](double s) { d3 n, wq; return pt_dist(p[0] + e[0] * s, p[1] + e[1] * s, p[2] + e[2] * s, p[3] + e[3] * s, n, wq); }, l,
+                  eta_min, near);
     } else {
       double l = fmax(L[0], L[1]) + fmax(L[2], L[3]);
-      t = advance([&](double s) { double a, b; d3 wp, wq; return ee_dist(p[0] + e[0] * s, p[1] + e[1] * s, p[2] + e[2] * s, p[3] + e[3] * s, a, b, wp, wq); }, l);
+      t = advance([&](double s) { double a, b; d3 wp, wq; return ee_dist(p[0] + e[0] * s, p[1] + e[1] * s, p[2] + e[2] * s, p[3] + e[3] * s, a, b, wp, wq); }, l,
+                  eta_min, near);
     }
   }
   t = warp_min(t);
@@ -238,7 +283,7 @@ __global__ void k_toi_rigid(int V, const double* x, const double* ext, const Rig
             if (!(lo <= th && hi >= tl)) overlap = false;
           }
           if (!overlap) continue;
-          t = fmin(t, advance([&](double s) { d3 n, wq; return pt_dist(p + e * s, a, bb, c, n, wq); }, l));
+          t = fmin(t, advance([&](double s) { d3 n, wq; return pt_dist(p + e * s, a, bb, c, n, wq); }, l, 0.0, 0.0));
         }
       }
     }
@@ -248,17 +293,15 @@ __global__ void k_toi_rigid(int V, const double* x, const double* ext, const Rig
 }
 
 // x += alpha d for free vertices, alpha = the time of impact bound (<= 1).
-__global__ void k_update_toi(int V, double* x, const float* d, const unsigned char* fixed, Ctrl* ctrl, const unsigned long long* toi,
-                             const unsigned long long* emax_cap) {
+// x += toi * ext / 1.25 (the clipped Newton direction times the time of impact).
+__global__ void k_update_toi(int V, double* x, const double* ext, double ext_scale, const unsigned char* fixed, Ctrl* ctrl,
+                             const unsigned long long* toi) {
   if (ctrl->converged) return;
-  double cap = __longlong_as_double((long long)emax_cap[1]);
-  double a = cap * fmin(1.0, __longlong_as_double((long long)*toi));
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double a = fmin(1.0, __longlong_as_double((long long)*toi));
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) ctrl->alpha = a;
-  if (a < 1e-8 || i >= V || (fixed && fixed[i])) return;
-  x[3 * i] += a * double(d[3 * i]);
-  x[3 * i + 1] += a * double(d[3 * i + 1]);
-  x[3 * i + 2] += a * double(d[3 * i + 2]);
+  if (a < 1e-8 || i >= 3ll * V || (fixed && fixed[i / 3])) return;
+  x[i] += a * (ext[i] / ext_scale);
 }
 
 __global__ void k_toi_reset(unsigned long long* toi) { *toi = (unsigned long long)__double_as_longlong(1.0); }
@@ -268,31 +311,35 @@ __global__ void k_toi_reset(unsigned long long* toi) { *toi = (unsigned long lon
 void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed, cudaStream_t s) {
   if (num_pins) k_pin_apply<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, fixed);
 }
+void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
+                    unsigned char* fixed, cudaStream_t s) {
+  if (num_pins) k_pin_ext<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, ext, x1, fixed);
+}
+void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x, cudaStream_t s) {
+  if (num_pins) k_pin_move<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, ext, toi, x);
+}
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s) {
   if (nvt + nee) k_pairs_to_contacts<<<nblk(nvt + nee), TPB, 0, s>>>(vt, nvt, ee, nee, tris, edges, x, gap_max, out);
 }
 void launch_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double scale, double lmax,
-                      unsigned long long* emax_cap, double* x1, double* ext, cudaStream_t s) {
-  if (!V) return;
-  cudaMemsetAsync(emax_cap, 0, sizeof(unsigned long long), s);
-  k_ext_max<<<nblk(V), TPB, 0, s>>>(V, d, fixed, scale, emax_cap);
-  k_swept_end<<<nblk(3ll * V), TPB, 0, s>>>(V, x, d, fixed, scale, lmax, emax_cap, x1, ext);
+                      double* x1, double* ext, cudaStream_t s) {
+  if (V) k_swept_end<<<nblk(3ll * V), TPB, 0, s>>>(V, x, d, fixed, scale, lmax, x1, ext);
 }
 void launch_toi_reset(unsigned long long* toi, cudaStream_t s) { k_toi_reset<<<1, 1, 0, s>>>(toi); }
 void launch_toi_walls(int V, const double* x, const double* ext, const WallDev* walls, int nw, unsigned long long* toi, cudaStream_t s) {
   if (V && nw) k_toi_walls<<<nblk(V), TPB, 0, s>>>(V, x, ext, walls, nw, toi);
 }
 void launch_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
-                      const double* ext, unsigned long long* toi, cudaStream_t s) {
-  if (nvt + nee) k_toi_pairs<<<nblk(nvt + nee), TPB, 0, s>>>(vt, nvt, ee, nee, tris, edges, x, ext, toi);
+                      const double* ext, double eta_min, double near, unsigned long long* toi, cudaStream_t s) {
+  if (nvt + nee) k_toi_pairs<<<nblk(nvt + nee), TPB, 0, s>>>(vt, nvt, ee, nee, tris, edges, x, ext, eta_min, near, toi);
 }
 void launch_toi_rigid(int V, const double* x, const double* ext, const RigidDev* bodies, int nb, unsigned long long* toi, cudaStream_t s) {
   if (V && nb) k_toi_rigid<<<nblk(V), TPB, 0, s>>>(V, x, ext, bodies, nb, toi);
 }
-void launch_update_toi(int V, double* x, const float* d, const unsigned char* fixed, Ctrl* ctrl, const unsigned long long* toi,
-                       const unsigned long long* emax_cap, cudaStream_t s) {
-  k_update_toi<<<nblk(V > 0 ? V : 1), TPB, 0, s>>>(V, x, d, fixed, ctrl, toi, emax_cap);
+void launch_update_toi(int V, double* x, const double* ext, double scale, const unsigned char* fixed, Ctrl* ctrl,
+                       const unsigned long long* toi, cudaStream_t s) {
+  k_update_toi<<<nblk(V > 0 ? 3ll * V : 1), TPB, 0, s>>>(V, x, ext, scale, fixed, ctrl, toi);
 }
 
 }  // namespace ando

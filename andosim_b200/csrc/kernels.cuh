@@ -76,17 +76,20 @@ void launch_velocity_ctl(int V, const double* x, const double* x_old, double dt,
 
 // CORRECTED semantics (corrected.cu)
 void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed, cudaStream_t s);
+void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
+                    unsigned char* fixed, cudaStream_t s);
+void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x, cudaStream_t s);
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s);
 void launch_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double scale, double lmax,
-                      unsigned long long* emax_cap, double* x1, double* ext, cudaStream_t s);
+                      double* x1, double* ext, cudaStream_t s);
 void launch_toi_reset(unsigned long long* toi, cudaStream_t s);
 void launch_toi_walls(int V, const double* x, const double* ext, const WallDev* walls, int nw, unsigned long long* toi, cudaStream_t s);
 void launch_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
-                      const double* ext, unsigned long long* toi, cudaStream_t s);
+                      const double* ext, double eta_min, double near, unsigned long long* toi, cudaStream_t s);
 void launch_toi_rigid(int V, const double* x, const double* ext, const RigidDev* bodies, int nb, unsigned long long* toi, cudaStream_t s);
-void launch_update_toi(int V, double* x, const float* d, const unsigned char* fixed, Ctrl* ctrl, const unsigned long long* toi,
-                       const unsigned long long* emax_cap, cudaStream_t s);
+void launch_update_toi(int V, double* x, const double* ext, double scale, const unsigned char* fixed, Ctrl* ctrl,
+                       const unsigned long long* toi, cudaStream_t s);
 
 // PCG (pcg.cu)
 struct PcgArgs {

@@ -565,6 +565,10 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
   k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S);
 }
 
+void learned_build_S(const LsView& s, const LearnedWork& w, float* S, cudaStream_t st) {
+  if (s.V) k_build_S<<<nblk(s.V), TPB, 0, st>>>(s, w.zv, w.ab, S);
+}
+
 void learned_loss(const LsView& s, const NetDev& n, LearnedWork& w, float* S, const float* probes, const double* pnorm, int P,
                   float* Y, float* Wv, double* loss_parts, double* loss_out, float* grad, cudaStream_t st) {
   const int V = s.V;

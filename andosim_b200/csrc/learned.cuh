@@ -84,6 +84,10 @@ void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cud
 // Inference: features, network, S (9 floats per static slot).
 void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, cudaStream_t st);
 
+// S from the coefficients of the last forward (w.zv, w.ab) and the current
+// A^: the network output reused while A^ changes; still SPD by construction.
+void learned_build_S(const LsView& s, const LearnedWork& w, float* S, cudaStream_t st);
+
 // Training loss of one system: P probe vectors r_p (3V each) with energy
 // norms n_p = r_p^T A^-1 r_p; loss = mean_p (1 + (y^T A y - 2 r^T y) / n_p),
 // y = S r_p (the relative A-norm error of one preconditioned Richardson step

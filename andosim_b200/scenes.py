@@ -145,13 +145,16 @@ def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
     """Two 2 m curtains (n x n each) 3 mm apart in y, top rows pinned and driven +-0.3 m along x at 0.5 Hz
     in opposite phase. The reference has no call to move a pin, so the pin set is rebuilt every frame.
     The drive amplitude ramps in with a smoothstep over the first 0.5 s: started at full amplitude the
-    pinned rows would jump two edge lengths (1.6 cm at n = 256) in the first frame."""
+    pinned rows would jump two edge lengths (1.6 cm at n = 256) in the first frame. Every vertex gets a
+    seeded +-0.1 mm jitter in all three axes: a curtain lying exactly in a plane has no out-of-plane
+    force until contact, so under the drive's in-plane compression it would fold within its own plane
+    (a vertex sliding onto a triangle of the same sheet at zero distance) instead of buckling."""
     rng = np.random.default_rng(seed)
     verts, tris, top = [], [], []
     for k in range(2):
         g = grid_plane(n, 2.0)
         v = np.stack([g[:, 0] - 1.0, np.full(n * n, 0.003 * k), g[:, 1] + 0.2], axis=1)
-        v[:, [0, 2]] += rng.uniform(-1e-4, 1e-4, size=(n * n, 2))
+        v += rng.uniform(-1e-4, 1e-4, size=(n * n, 3))
         verts.append(v)
         tris.append(grid_triangles(n, n, offset=k * n * n))
         top.extend(range(k * n * n + (n - 1) * n, (k + 1) * n * n))

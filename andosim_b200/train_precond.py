@@ -1,0 +1,98 @@
+"""Train the learned preconditioner on the two-curtain workload and evaluate it.
+
+    python -m andosim_b200.train_precond [--n 256] [--train-seeds 0-7] [--eval-seeds 8-11]
+        [--frames 300] [--every 10] [--steps 3000] [--out PATH] [--report PATH]
+
+Training data are the solver's own dumps: the first Newton system of every
+`every`-th frame of CORRECTED-semantics runs of scenes.c4 for the training
+seeds, each with probe residuals of a block-Jacobi solve. Evaluation steps the
+held-out seeds for `frames` frames with block Jacobi and with the trained
+network (device timing, PCG iterations per Newton step, fallbacks, and the
+final position difference between the two runs).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import abi, learned, scenes
+
+
+def seeds(spec: str):
+    out = []
+    for part in spec.split(","):
+        if "-" in part:
+            a, b = part.split("-")
+            out.extend(range(int(a), int(b) + 1))
+        elif part:
+            out.append(int(part))
+    return out
+
+
+def evaluate(sc, weights, frames: int, precond: str, refresh: int = 1, device: int = 0):
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=device)
+    if weights is not None:
+        S.set_precond_weights(weights)
+    p = abi.make_params(sc.params, semantics="corrected", precond=precond, precond_refresh=refresh)
+    it = nw = fb = 0
+    ms = 0.0
+    for f in range(frames):
+        S.apply_gravity(sc.gravity, p.dt)
+        st = S.step(p, sc.pins_at(f), sc.walls)
+        it += st["pcg_iters"]; nw += st["newton_iters"]; fb += st["precond_fallbacks"]; ms += st["device_ms"]
+    x, _ = S.download()
+    S.close()
+    return dict(pcg_iters=it, newton_iters=nw, pcg_per_newton=it / max(nw, 1), fallbacks=fb, device_ms=ms,
+                frames_per_s=frames / (ms * 1e-3) if ms > 0 else None), x
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--train-seeds", default="0-7")
+    ap.add_argument("--eval-seeds", default="8-11")
+    ap.add_argument("--frames", type=int, default=300)
+    ap.add_argument("--every", type=int, default=10)
+    ap.add_argument("--eval-frames", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--init-seed", type=int, default=0)
+    ap.add_argument("--refresh", type=int, default=1)
+    ap.add_argument("--out", default=str(learned.DEFAULT_WEIGHTS))
+    ap.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+
+    t0 = time.time()
+    trainer = abi.Trainer(abi.precond_init_weights(a.init_seed))
+    n_sys = learned.c4_training_set(trainer, seeds(a.train_seeds), a.n, range(0, a.frames, a.every))
+    t_collect = time.time() - t0
+    loss0 = learned.mean_loss(trainer)
+    t1 = time.time()
+    losses = learned.train(trainer, a.steps, lr=a.lr, log_every=max(a.steps // 10, 1))
+    t_train = time.time() - t1
+    loss1 = learned.mean_loss(trainer)
+    w = trainer.weights()
+    trainer.close()
+    out = learned.save_weights(w, a.out)
+    report = dict(n=a.n, train_seeds=seeds(a.train_seeds), systems=n_sys, collect_s=t_collect, train_steps=a.steps,
+                  train_s=t_train, loss_before=loss0, loss_after=loss1, weights=str(out), eval=[])
+    print(json.dumps({k: v for k, v in report.items() if k != "eval"}), flush=True)
+    for sd in seeds(a.eval_seeds):
+        sc = scenes.c4(seed=sd, n=a.n)
+        rj, xj = evaluate(sc, None, a.eval_frames, "block_jacobi")
+        rl, xl = evaluate(sc, w, a.eval_frames, "learned", a.refresh)
+        ext = float(np.ptp(sc.vertices, axis=0).max())
+        row = dict(seed=sd, jacobi=rj, learned=rl, pos_diff_rel=float(np.abs(xl - xj).max() / ext),
+                   iter_ratio=rl["pcg_per_newton"] / max(rj["pcg_per_newton"], 1e-30))
+        report["eval"].append(row)
+        print(json.dumps(row), flush=True)
+    if a.report:
+        Path(a.report).write_text(json.dumps(report, indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -3,9 +3,16 @@
 
 Workload: two 2 m x 2 m curtains of 256 x 256 vertices (131,072 vertices,
 260,100 triangles), 3 mm apart, top rows pinned and driven +-0.3 m along x at
-0.5 Hz in opposite phase, ground plane at z = 0 (synthetic, seeded), stepped
-with the reference's semantics and block-Jacobi PCG. One bench step = one
-frame: State.apply_gravity + Integrator.step, as the reference demos drive it.
+0.5 Hz in opposite phase, ground plane at z = 0 (synthetic, seeded). One bench
+step = one frame: State.apply_gravity + Integrator.step, as the reference
+demos drive it.
+
+Headline (`value`): frames/s of the CORRECTED step (the step the reference
+intends: elasticity on the current positions, kinematic pins, working self
+contact, time-of-impact line search) with the learned preconditioner, next to
+the same frames with block-Jacobi PCG (`jacobi`), with PCG iterations per
+Newton step for both. `reference_semantics` times the reference's own step
+(REFERENCE semantics, block Jacobi, whole frame as one CUDA graph).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -47,7 +54,9 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="curtain grid side")
     ap.add_argument("--cpu-frames", type=int, default=1, help="frames of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--corrected-steps", type=int, default=60, help="frames of the CORRECTED-semantics measurement (0: skip)")
+    ap.add_argument("--reference-steps", type=int, default=240, help="frames of the REFERENCE-semantics measurement (0: skip)")
+    ap.add_argument("--refresh", type=int, default=1, help="Newton iterations between evaluations of the preconditioner network")
+    ap.add_argument("--weights", default=None, help="learned preconditioner weights (.npy); default: the shipped C4 weights")
     return ap.parse_args()
 
 
@@ -132,95 +141,188 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- ours
-def algorithmic_bytes(V, T, nnzb, prof):
-    """Algorithmic bytes per phase over the timed region.
+def pcg_bytes(V, nnzb, prof):
+    """Algorithmic bytes of the scaled PCG over the profiled frames.
 
-    assembly  : 24 V + 72 nnzb per launch (x and g read once, the cached 36-B
-                constant block read and the 36-B value block written per slot)
-    PCG       : 40 nnzb + 160 V per iteration (block SpMV + fused vector updates)
-                plus 48 V per launch (x, r, z initialisation)
-    gradient  : 212 V per launch (x, x_hat, per-step constants and mass read,
-                g, rhs and the diagonal terms written)
-    strain    : 53 T + 24 V per launch (indices, rest data, positions, flags)
-    """
-    pl = prof["phase_launches"]
+    Per block-Jacobi iteration (CG on the scaled system, identity diagonal):
+      phase A  40 nnzb (scaled BSR values + column) + 40 per contact block
+               outside the mesh pattern, 12 V each for z, p_old (gathered
+               once), p_new and Ap
+      phase B  12 V p, 24 V x^ read+write (FP64), 12 V Ap, 24 V r read+write,
+               24 V L (FP32, residual norm)
+      = 40 nnzb + 40 n_extra + 144 V
+    A learned iteration adds the second product z = S r on the mesh pattern:
+      + 40 nnzb (S values + column) + 24 V (r2, z written) + 12 V (Ap gathered)
+    plus 48 V per launch (initialisation and d = L^-T x^)."""
+    it = prof["pcg_iterations"]
+    lit = prof["pcg_learned_iterations"]
+    return (40 * nnzb + 144 * V) * it + 40 * prof["pcg_extra_block_iterations"] + (40 * nnzb + 36 * V) * lit \
+        + 48 * V * prof["phase_launches"]["pcg"]
+
+
+class Timer:
+    """CUDA-event timing of frames on the library's stream, L2 flushed before each."""
+
+    def __init__(self, torch, stream, flush):
+        self.torch, self.stream, self.flush = torch, stream, flush
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+
+    def frame(self, fn):
+        with self.torch.cuda.stream(self.stream):
+            self.flush.zero_()          # evict L2 (256 MB > 126 MB) before every timed frame
+            self.a.record(self.stream)
+        r = fn()
+        self.b.record(self.stream)
+        self.b.synchronize()
+        return r, self.a.elapsed_time(self.b)
+
+
+def corrected_run(args, sc, local, flush, pg, precond, weights, profile=False, frames=None):
+    """`frames` CORRECTED frames after `warmup` untimed ones, device-resident
+    (the profiled pass: per-phase CUDA events)."""
+    import torch
+
+    from andosim_b200 import abi
+
+    frames = args.steps if frames is None else frames
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
+    if weights is not None:
+        S.set_precond_weights(weights)
+    params = abi.make_params(sc.params, semantics="corrected", precond=precond, precond_refresh=args.refresh)
+    tm = Timer(torch, torch.cuda.ExternalStream(S.stream(), device=torch.device("cuda", local)), flush)
+    for f in range(args.warmup):
+        S.apply_gravity(sc.gravity, params.dt)
+        S.step(params, sc.pins_at(f), sc.walls)
+    S.profile_enable(profile)
+    total_ms, stats = 0.0, []
+    for k in range(frames):
+        pins = abi.pin_array(sc.pins_at(args.warmup + k))
+
+        def one():
+            S.apply_gravity(sc.gravity, params.dt)
+            return S.step(params, pins, sc.walls)
+        st, ms = tm.frame(one)
+        stats.append(st)
+        total_ms += ms
+    prof = S.profile()
+    nnzb = int(len(S.last_system()[1]))
+    S.close()
+    newton = sum(s["newton_iters"] for s in stats)
+    pcg = sum(s["pcg_iters"] for s in stats)
+    return {"preconditioner": precond, "frames": frames, "ms_per_frame": round(total_ms / frames, 3),
+            "pcg_iters_per_newton": round(pcg / newton, 2) if newton else 0.0,
+            "phase_ms_per_frame": {k: round(v / frames, 4) for k, v in prof["phase_ms"].items()},
+            "pcg_us_per_iteration": round(prof["phase_ms"]["pcg"] * 1e3 / prof["pcg_iterations"], 2) if prof["pcg_iterations"] else None,
+            "_prof": prof, "_nnzb": nnzb}
+
+
+def paired_run(args, sc, local, flush, pg, weights):
+    """The learned-preconditioner trajectory, timed frame by frame; before each
+    learned frame a block-Jacobi frame is timed from the same state and then
+    undone, so both preconditioners solve exactly the same Newton systems of
+    the first iteration and the comparison does not depend on where two
+    contact-rich trajectories drift apart."""
+    import torch
+
+    from andosim_b200 import abi
+
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
+    S.set_precond_weights(weights)
+    pl = abi.make_params(sc.params, semantics="corrected", precond="learned", precond_refresh=args.refresh)
+    pj = abi.make_params(sc.params, semantics="corrected", precond="block_jacobi")
+    tm = Timer(torch, torch.cuda.ExternalStream(S.stream(), device=torch.device("cuda", local)), flush)
+    for f in range(args.warmup):
+        S.apply_gravity(sc.gravity, pl.dt)
+        S.step(pl, sc.pins_at(f), sc.walls)
+    torch.cuda.synchronize()
+    barrier(pg)
+    S.profile_enable(False)
+    ext = float(np.ptp(sc.vertices, axis=0).max())
+    res = {"learned": dict(ms=0.0, stats=[], launches=0), "block_jacobi": dict(ms=0.0, stats=[], launches=0)}
+    diffs = []
+    for k in range(args.steps):
+        pins = abi.pin_array(sc.pins_at(args.warmup + k))
+        x0, v0 = S.download()
+        outs = {}
+        for name, p in (("block_jacobi", pj), ("learned", pl)):
+            if name == "learned":
+                S.upload(x0, v0)
+            n0 = S.profile()["launches"]
+
+            def one():
+                S.apply_gravity(sc.gravity, p.dt)
+                return S.step(p, pins, sc.walls)
+            st, ms = tm.frame(one)
+            r = res[name]
+            r["ms"] += ms
+            r["stats"].append(st)
+            r["launches"] += S.profile()["launches"] - n0
+            outs[name] = S.download()[0]
+        diffs.append(float(np.abs(outs["learned"] - outs["block_jacobi"]).max() / ext))
+    S.close()
     out = {}
-    out["assemble"] = (24 * V + 72 * nnzb) * pl["assemble"]
-    out["pcg"] = (40 * nnzb + 160 * V) * prof["pcg_iterations"] + 48 * V * pl["pcg"]
-    # the gradient phase counts the gradient kernel and the 1-thread check kernel
-    out["gradient"] = 212 * V * (pl["gradient"] // 2 if pl["gradient"] else 0)
-    out["strain"] = (53 * T + 24 * V) * (pl["strain"] // 2 if pl["strain"] else 0)
+    for name, r in res.items():
+        ms = dist_max(r["ms"], pg)
+        stats = r["stats"]
+        newton = sum(s["newton_iters"] for s in stats)
+        pcg = sum(s["pcg_iters"] for s in stats)
+        out[name] = {"frames": args.steps, "total_ms": ms, "frames_per_s": round(args.steps / (ms * 1e-3), 2),
+                     "ms_per_frame": round(ms / args.steps, 3), "newton_iters_per_frame": round(newton / args.steps, 3),
+                     "pcg_iters_per_newton": round(pcg / newton, 2) if newton else 0.0,
+                     "newton_iters_per_s": round(newton / (ms * 1e-3), 1),
+                     "precond_fallbacks": sum(s["precond_fallbacks"] for s in stats),
+                     "contacts_max": max(s["contacts"] for s in stats) if stats else 0,
+                     "gpu_launches": int(r["launches"])}
+    out["learned"]["refresh"] = args.refresh
+    out["step_position_diff_rel_extent"] = {"max": max(diffs) if diffs else 0.0, "median": float(np.median(diffs)) if diffs else 0.0}
     return out
 
 
-def run_ours(args, rank, world, local, pg):
+def reference_semantics_run(args, sc, local, flush, pg):
+    """The reference's own step (REFERENCE semantics, block Jacobi): each frame one whole-frame CUDA graph."""
     import torch
 
-    from andosim_b200 import abi, scenes
-    from andosim_b200.build import build
+    from andosim_b200 import abi
 
-    if rank == 0:
-        build()
-    barrier(pg)
-    torch.cuda.set_device(local)
-    sc = scenes.c4(seed=rank, n=args.n)
-    V, T = sc.num_vertices, sc.num_triangles
     S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
     params = abi.make_params(sc.params)
-    stream = torch.cuda.ExternalStream(S.stream(), device=torch.device("cuda", local))
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-    clocks = ClockSampler(local)
-
-    frame = 0
-
-    def do_frame(f, pins=None):
+    tm = Timer(torch, torch.cuda.ExternalStream(S.stream(), device=torch.device("cuda", local)), flush)
+    for f in range(args.warmup):
         S.apply_gravity(sc.gravity, params.dt)
-        return S.step(params, sc.pins_at(f) if pins is None else pins, sc.walls)
-
-    ev_a = torch.cuda.Event(enable_timing=True)
-    ev_b = torch.cuda.Event(enable_timing=True)
-
-    def timed(n, first):
-        stats, ms = [], 0.0
-        for k in range(n):
-            pins = abi.pin_array(sc.pins_at(first + k))     # the scene's driven pin targets, built untimed
-            with torch.cuda.stream(stream):
-                flush.zero_()          # evict L2 (256 MB > 126 MB) before every timed frame
-                ev_a.record(stream)
-            stats.append(do_frame(first + k, pins))
-            ev_b.record(stream)
-            ev_b.synchronize()
-            ms += ev_a.elapsed_time(ev_b)
-        return stats, ms
-
-    for _ in range(args.warmup):
-        do_frame(frame)
-        frame += 1
-    torch.cuda.synchronize()
-    barrier(pg)
-    clocks.start()
-    # headline pass: profiler off, so each frame is one whole-frame CUDA graph launch
-    S.profile_enable(False)                 # also resets the launch counters
-    stats, total_ms = timed(args.steps, frame)
-    frame += args.steps
-    launches = int(S.profile()["launches"])
-    graph_frames = sum(int(s["graph_launched"]) for s in stats)
-    torch.cuda.synchronize()
-    total_ms = dist_max(total_ms, pg)
-    barrier(pg)
-    # phase breakdown: a separate pass with per-phase CUDA events (host-driven loop)
-    prof_frames = min(args.steps, 120)
-    S.profile_enable(True)
-    _, prof_total_ms = timed(prof_frames, frame)
-    frame += prof_frames
-    prof = S.profile()
+        S.step(params, sc.pins_at(f), sc.walls)
     S.profile_enable(False)
-    barrier(pg)
+    total_ms, stats = 0.0, []
+    for k in range(args.reference_steps):
+        pins = abi.pin_array(sc.pins_at(args.warmup + k))
 
-    # end to end through the Python API: host buffers, copies inside the timed region
+        def one():
+            S.apply_gravity(sc.gravity, params.dt)
+            return S.step(params, pins, sc.walls)
+        st, ms = tm.frame(one)
+        stats.append(st)
+        total_ms += ms
+    launches = int(S.profile()["launches"])
+    S.close()
+    total_ms = dist_max(total_ms, pg)
+    newton = sum(s["newton_iters"] for s in stats)
+    pcg = sum(s["pcg_iters"] for s in stats)
+    return {"semantics": "REFERENCE", "preconditioner": "block_jacobi", "frames": args.reference_steps,
+            "frames_per_s": round(args.reference_steps / (total_ms * 1e-3), 2),
+            "ms_per_frame": round(total_ms / args.reference_steps, 4),
+            "newton_iters_per_frame": round(newton / args.reference_steps, 3),
+            "pcg_iters_per_newton": round(pcg / newton, 3) if newton else 0.0,
+            "graph_frames": sum(int(s["graph_launched"]) for s in stats), "gpu_launches": launches}
+
+
+def e2e_run(args, sc, local, flush, pg, weights):
+    """Frames/s through the ando_barrier_core API (host arrays in, positions out every frame)."""
+    import torch
+
     from andosim_b200 import ando_barrier_core as abc
 
     abc.set_device(local)
+    abc.set_precond_weights(weights)
     m = abc.Mesh()
     m.initialize(sc.vertices, sc.triangles, abc.Material(**sc.material))
     st = abc.State()
@@ -228,6 +330,9 @@ def run_ours(args, rank, world, local, pg):
     p = abc.SimParams()
     for k, v in sc.params.items():
         setattr(p, k, v)
+    p.semantics = "corrected"
+    p.preconditioner = "learned"
+    p.precond_refresh = args.refresh
 
     def api_frame(f):
         c = abc.Constraints()
@@ -241,127 +346,85 @@ def run_ours(args, rank, world, local, pg):
 
     for f in range(args.warmup):
         api_frame(f)
-    e2e_stream = torch.cuda.ExternalStream(st._stream_handle(), device=torch.device("cuda", local))
+    tm = Timer(torch, torch.cuda.ExternalStream(st._stream_handle(), device=torch.device("cuda", local)), flush)
     e2e_ms = 0.0
     for f in range(args.steps):
-        with torch.cuda.stream(e2e_stream):
-            flush.zero_()
-            ev_a.record(e2e_stream)
-        pos = api_frame(args.warmup + f)
-        ev_b.record(e2e_stream)
-        ev_b.synchronize()
-        e2e_ms += ev_a.elapsed_time(ev_b)
+        _, ms = tm.frame(lambda: api_frame(args.warmup + f))
+        e2e_ms += ms
     e2e_ms = dist_max(e2e_ms, pg)
-    clock_info = clocks.stop()
     n_pins = len(sc.pins_at(0))
-    h2d = n_pins * (4 + 24) + len(sc.walls) * 48          # pins and walls uploaded each step
-    d2h = 2 * 24 * V                                      # positions and velocities (FP64) read back
+    return {"value": round(args.steps * int(os.environ.get("WORLD_SIZE", "1")) / (e2e_ms * 1e-3), 2), "unit": "frames/s",
+            "h2d_bytes_per_step": n_pins * (4 + 24) + len(sc.walls) * 48,     # pins and walls uploaded each step
+            "d2h_bytes_per_step": 2 * 24 * sc.num_vertices}                   # positions and velocities (FP64) read back
 
-    # roofline of the dominant phase
-    nnzb = 0
-    try:
-        rowptr, cols, vals, rhs, sol = S.last_system()
-        nnzb = int(len(cols))
-    except Exception:
-        pass
-    ab = algorithmic_bytes(V, T, nnzb, prof)
+
+def run_ours(args, rank, world, local, pg):
+    import torch
+
+    from andosim_b200 import learned, scenes
+    from andosim_b200.build import build
+
+    if rank == 0:
+        build()
+    barrier(pg)
+    torch.cuda.set_device(local)
+    sc = scenes.c4(seed=rank, n=args.n)
+    V, T = sc.num_vertices, sc.num_triangles
+    weights = learned.load_weights(Path(args.weights) if args.weights else None)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    clocks = ClockSampler(local)
+    clocks.start()
+    pair = paired_run(args, sc, local, flush, pg, weights)
+    clock_info = clocks.stop()
+    lrn, jac = pair["learned"], pair["block_jacobi"]
+    # phase breakdown and PCG roofline: a separate profiled pass (per-phase CUDA events)
+    prof_frames = min(args.steps, 60)
+    lp = corrected_run(args, sc, local, flush, pg, "learned", weights, profile=True, frames=prof_frames)
+    prof, nnzb = lp.pop("_prof"), lp.pop("_nnzb")
     peaks = json.loads(PEAKS_FILE.read_text()) if PEAKS_FILE.exists() else {}
     hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
-    phase_ms = prof["phase_ms"]
-    # dominant kernel phase among those with an algorithmic byte count
-    dom = max(ab, key=lambda k: phase_ms.get(k, 0.0))
-    dom_bytes = ab.get(dom)
+    pcg_ms = prof["phase_ms"]["pcg"]
+    launches = max(1, prof["phase_launches"]["pcg"])
+    pb = pcg_bytes(V, nnzb, prof)
     roof = None
-    if dom_bytes is not None and phase_ms[dom] > 0:
-        dom_launches = max(1, prof["phase_launches"][dom] // (2 if dom in ("gradient", "strain") else 1))
-        achieved = dom_bytes / (phase_ms[dom] * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": "measured" if peaks else "fallback",
-                "bytes_per_launch": dom_bytes // dom_launches, "launches": dom_launches,
-                "avg_launch_us": round(phase_ms[dom] * 1e3 / dom_launches, 2)}
-    newton = sum(s["newton_iters"] for s in stats)
-    pcg = sum(s["pcg_iters"] for s in stats)
-    fps = args.steps * world / (total_ms * 1e-3)
+    if pcg_ms > 0:
+        achieved = pb / (pcg_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_pcg_scaled (learned and block-Jacobi launches)", "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                "peak_source": "measured" if peaks else "fallback", "bytes_per_launch": int(pb // launches),
+                "launches": int(launches), "avg_launch_us": round(pcg_ms * 1e3 / launches, 2),
+                "pcg_iterations": int(prof["pcg_iterations"]), "share_of_frame": round(pcg_ms / max(sum(prof["phase_ms"].values()), 1e-9), 3)}
+    ms_l = lrn.pop("total_ms")
+    jac.pop("total_ms")
     out = {
-        "metric": METRIC, "value": round(fps, 2), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "metric": METRIC, "value": round(args.steps * world / (ms_l * 1e-3), 2), "unit": "frames/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_l / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 BSR/PCG vectors, f64 positions/gradient/dots",
         "data": "synthetic (seeded curtains, scenes.c4)",
-        "config": {"workload": WORKLOAD, "vertices": V, "triangles": T, "bsr_blocks": nnzb, "semantics": "REFERENCE",
-                   "preconditioner": "block_jacobi", "frames_timed_per_gpu": args.steps, "l2": "flushed before every timed frame",
-                   "parallelism": f"replicas x{world}"},
-        "newton_iters_per_frame": round(newton / args.steps, 3),
-        "pcg_iters_per_newton": round(pcg / newton, 3) if newton else 0.0,
-        "newton_iters_per_s": round(newton * world / (total_ms * 1e-3), 1),
-        "graph_frames": graph_frames,
-        "profiled_pass": {"frames": prof_frames, "ms_per_frame": round(prof_total_ms / prof_frames, 4),
-                          "phase_ms_per_frame": {k: round(v / prof_frames, 5) for k, v in phase_ms.items()}},
-        "gpu_launches": launches,
-        "e2e": {"value": round(args.steps * world / (e2e_ms * 1e-3), 2), "unit": "frames/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "config": {"workload": WORKLOAD, "vertices": V, "triangles": T, "bsr_blocks": nnzb, "semantics": "CORRECTED",
+                   "preconditioner": "learned", "precond_refresh": args.refresh, "frames_timed_per_gpu": args.steps,
+                   "l2": "flushed before every timed frame", "parallelism": f"replicas x{world}"},
+        "pcg_iters_per_newton": lrn["pcg_iters_per_newton"],
+        "newton_iters_per_frame": lrn["newton_iters_per_frame"],
+        "newton_iters_per_s": round(lrn["newton_iters_per_s"] * world, 1),
+        "learned": lrn, "jacobi": jac,
+        "learned_vs_jacobi": {"frames_per_s_ratio": round(lrn["frames_per_s"] / jac["frames_per_s"], 3),
+                              "pcg_iters_per_newton_ratio": round(lrn["pcg_iters_per_newton"] / max(jac["pcg_iters_per_newton"], 1e-9), 3),
+                              "paired": "each frame both preconditioners step from the same state",
+                              "step_position_diff_rel_extent": pair["step_position_diff_rel_extent"]},
+        "profiled_pass": lp,
+        "gpu_launches": lrn["gpu_launches"],
         "roofline": roof,
         "clocks": clock_info,
     }
-    S.close()
-    if args.corrected_steps > 0:
-        out["corrected"] = run_corrected(args, sc, local, flush, pg)
+    if args.reference_steps > 0:
+        out["reference_semantics"] = reference_semantics_run(args, sc, local, flush, pg)
+    out["e2e"] = e2e_run(args, sc, local, flush, pg, weights)
     return out, sc
 
 
-def run_corrected(args, sc, local, flush, pg, precond="block_jacobi"):
-    """The same workload in CORRECTED semantics (elasticity on the current
-    positions, kinematic pins, working self contact, time-of-impact line
-    search): a real PCG solve every Newton iteration."""
-    import torch
-
-    from andosim_b200 import abi
-
-    S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
-    params = abi.make_params(sc.params, semantics="corrected", precond=precond)
-    stream = torch.cuda.ExternalStream(S.stream(), device=torch.device("cuda", local))
-    ev_a = torch.cuda.Event(enable_timing=True)
-    ev_b = torch.cuda.Event(enable_timing=True)
-    for f in range(args.warmup):
-        S.apply_gravity(sc.gravity, params.dt)
-        S.step(params, sc.pins_at(f), sc.walls)
-    S.profile_enable(True)
-    total_ms, stats = 0.0, []
-    for k in range(args.corrected_steps):
-        f = args.warmup + k
-        pins = abi.pin_array(sc.pins_at(f))
-        with torch.cuda.stream(stream):
-            flush.zero_()
-            ev_a.record(stream)
-        S.apply_gravity(sc.gravity, params.dt)
-        stats.append(S.step(params, pins, sc.walls))
-        ev_b.record(stream)
-        ev_b.synchronize()
-        total_ms += ev_a.elapsed_time(ev_b)
-    prof = S.profile()
-    S.close()
-    total_ms = dist_max(total_ms, pg)
-    newton = sum(s["newton_iters"] for s in stats)
-    pcg = sum(s["pcg_iters"] for s in stats)
-    nnzb = 0
-    V = sc.num_vertices
-    pcg_ms = prof["phase_ms"]["pcg"]
-    pcg_iters = prof["pcg_iterations"]
-    return {
-        "semantics": "CORRECTED", "preconditioner": precond, "frames": args.corrected_steps,
-        "frames_per_s": round(args.corrected_steps / (total_ms * 1e-3), 2),
-        "ms_per_frame": round(total_ms / args.corrected_steps, 3),
-        "newton_iters_per_frame": round(newton / args.corrected_steps, 3),
-        "pcg_iters_per_newton": round(pcg / newton, 2) if newton else 0.0,
-        "newton_iters_per_s": round(newton / (total_ms * 1e-3), 1),
-        "pcg_us_per_iteration": round(pcg_ms * 1e3 / pcg_iters, 2) if pcg_iters else None,
-        "phase_ms_per_frame": {k: round(v / args.corrected_steps, 4) for k, v in prof["phase_ms"].items()},
-        "contacts_max": max(s["contacts"] for s in stats) if stats else 0,
-        "gpu_launches": int(prof["launches"]),
-    }
-
-
 # ----------------------------------------------------------- CPU baseline
-def oracle_frames(sc, frames, prec="f32", lookup="indexed"):
+def oracle_frames(sc, frames, prec="f32", lookup="indexed", semantics="reference"):
     """Time `frames` oracle steps of scene `sc` (single thread). Returns seconds per frame."""
     from oracle.build import load
 
@@ -382,16 +445,20 @@ def oracle_frames(sc, frames, prec="f32", lookup="indexed"):
             c.add_wall(n, o, g)
         s.apply_gravity(sc.gravity, p.dt)
         t0 = time.perf_counter()
-        O.Integrator.step(m, s, c, p, None, lookup)
+        if semantics == "reference":
+            O.Integrator.step(m, s, c, p, None, lookup)
+        else:
+            O.Integrator.step(m, s, c, p, None, lookup, "literal", "corrected")
         secs += time.perf_counter() - t0
     return secs / frames
 
 
 def cpu_baseline(sc, frames):
-    spf = oracle_frames(sc, frames)
+    """The oracle on one host core, on the headline's semantics (CORRECTED, block Jacobi)."""
+    spf = oracle_frames(sc, frames, semantics="corrected")
     return {"value": round(1.0 / spf, 4), "unit": "frames/s", "cores": 1, "kind": "port",
-            "sample": f"{frames} frame(s) of {WORKLOAD} ({sc.num_vertices} vertices) through the FP32 oracle "
-                      f"(C++ restatement of the reference, INDEXED block lookup, one thread)"}
+            "sample": f"{frames} frame(s) of {WORKLOAD} ({sc.num_vertices} vertices), CORRECTED semantics, through the "
+                      f"FP32 oracle (C++ restatement, block-Jacobi PCG, one thread)"}
 
 
 def run_reference(args, rank, world, pg):

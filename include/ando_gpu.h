@@ -61,7 +61,7 @@ typedef struct {
   double youngs_modulus, poisson_ratio, density, thickness, bending_stiffness;
 } ando_material;
 
-/* SimParams (types.h:60-100), every field, plus the two GPU-only knobs at the end. */
+/* SimParams (types.h:60-100), every field, plus the GPU-only knobs at the end. */
 typedef struct {
   double dt, beta_max;
   int32_t min_newton_steps, max_newton_steps, friction_min_newton_steps;
@@ -78,6 +78,10 @@ typedef struct {
   double hessian_epsilon, min_gap;
   int32_t semantics; /* ando_semantics */
   int32_t precond;   /* ando_precond */
+  /* Learned preconditioner: Newton iterations between evaluations of the
+   * network (<= 1: every iteration). In between, S is rebuilt from the
+   * current scaled system with the last coefficients (still SPD). */
+  int32_t precond_refresh;
 } ando_params;
 
 /* PinConstraint (constraints.h:12-17). */
@@ -147,6 +151,8 @@ typedef struct {
   double phase_ms[ANDO_PHASE_COUNT];       /* summed CUDA-event time of each phase (profiling on) */
   int64_t pcg_iterations;                  /* PCG iterations inside the profiled PCG launches */
   int64_t newton_iterations;               /* Newton iterations that assembled and solved */
+  int64_t pcg_learned_iterations;          /* of pcg_iterations: iterations with the learned preconditioner */
+  int64_t pcg_extra_block_iterations;      /* sum over PCG iterations of the contact blocks outside the mesh pattern */
 } ando_profile;
 
 /* Library identity. */
@@ -179,6 +185,15 @@ ANDO_API int32_t ando_mesh_set_vertices(ando_ctx ctx, const double* vertices, in
  * pointers may be NULL to keep the device copy). */
 ANDO_API int32_t ando_state_upload(ando_ctx ctx, const double* positions, const double* velocities,
                           const double* positions_prev, const double* masses, int32_t num_vertices);
+
+/* CORRECTED semantics: the positions the next step starts from. A step
+ * starts where the previous one ended, or at the positions of the last
+ * ando_state_upload; State.apply_gravity's position update is not a start
+ * (it is an explicit, collision-unchecked move whose velocity change the
+ * implicit predictor x_hat = x + dt v already carries). No reference
+ * counterpart: the reference starts from the moved positions. */
+ANDO_API int32_t ando_state_set_start(ando_ctx ctx, const double* positions, int32_t num_vertices);
+ANDO_API int32_t ando_state_get_start(ando_ctx ctx, double* positions, int32_t num_vertices);
 
 /* Download positions and/or velocities (State.get_positions/get_velocities,
  * bindings.cpp:248-267). Either pointer may be NULL. */

@@ -255,10 +255,13 @@ template <class R> struct Mesh {
 // state.cpp:6-32
 template <class R> struct State {
   std::vector<V3<R>> positions, velocities, positions_prev;
+  // CORRECTED semantics only: where the last step ended (or what the caller
+  // set), the start of the intersection-free move of the next step.
+  std::vector<V3<R>> positions_safe;
   std::vector<R> masses;
   void initialize(const Mesh<R>& mesh) {
     if (mesh.vertices.empty()) throw std::invalid_argument("Mesh must be initialised before creating a state");
-    positions = mesh.vertices; positions_prev = mesh.vertices;
+    positions = mesh.vertices; positions_prev = mesh.vertices; positions_safe = mesh.vertices;
     velocities.assign(mesh.vertices.size(), V3<R>());
     masses.assign(mesh.vertices.size(), R(0));
     for (size_t i = 0; i < mesh.triangles.size(); ++i) {
@@ -1536,11 +1539,35 @@ template <class R> void elastic_gradient_at(const Mesh<R>& mesh, const std::vect
 // Conservative time of impact of one pair along the motion x -> x + e: advance
 // by (d - eta) / l until the distance falls to eta = 0.1 d0 (l bounds how fast
 // the distance can shrink per unit time). Returns t in [0, 1].
-template <class R> R advance_toi(const std::function<R(R)>& dist, R l) {
+// A pair that already touches (d0 = 0; only a kinematic pin snap makes one)
+// cannot be advanced conservatively and does not bound the step.
+// With eta_min > 0 (the kinematic pin pass) the move may not bring a pair
+// closer than eta_min at all.
+// A pair closer than `near` at the start is sampled instead of advanced
+// (geometric times 2^-40..2^-1, then 0.5..1 in steps of 1/32): the step is
+// allowed up to the last sample before the distance first falls below half
+// its starting value (conservative advancement cannot tell such a pair moving
+// apart from one closing in).
+template <class R> R advance_toi(const std::function<R(R)>& dist, R l, R eta_min = R(0), R near = R(0)) {
   if (!(l > R(0))) return R(1);
   R d0 = dist(R(0));
-  if (!(d0 > R(0))) return R(0);
-  R eta = R(0.1) * d0, t = 0;
+  if (!(d0 > R(0))) return R(1);
+  if (d0 <= eta_min) return R(0);
+  if (d0 < near) {
+    R prev = 0;
+    for (int k = 40; k >= 1; --k) {
+      R ts = R(std::ldexp(1.0, -k));
+      if (!(dist(ts) >= R(0.5) * d0)) return prev;
+      prev = ts;
+    }
+    for (int k = 17; k <= 32; ++k) {
+      R ts = R(double(k) / 32.0);
+      if (!(dist(ts) >= R(0.5) * d0)) return prev;
+      prev = ts;
+    }
+    return R(1);
+  }
+  R eta = std::max(R(0.1) * d0, eta_min), t = 0;
   for (int it = 0; it < 200; ++it) {
     R d = it == 0 ? d0 : dist(t);
     if (d <= eta) return t;
@@ -1556,10 +1583,28 @@ template <class R> class CorrectedIntegrator {
     StepStats<R> local; StepStats<R>& S = stats ? *stats : local;
     S = StepStats<R>();
     const size_t n = st.positions.size(); const R dt = p.dt;
-    std::vector<V3<R>> x_old = st.positions, x_target(n);
     std::vector<char> fixed(n, 0);
-    for (const auto& pin : C.pins) if (pin.active) { st.positions[size_t(pin.vertex_idx)] = pin.target_position; fixed[size_t(pin.vertex_idx)] = 1; }
+    for (const auto& pin : C.pins) if (pin.active) fixed[size_t(pin.vertex_idx)] = 1;
+    // The step starts where the previous one ended (or at the caller's own
+    // positions): the position update of State::apply_gravity is an explicit,
+    // collision-unchecked move, and the implicit predictor below already
+    // carries its velocity (x_target = x_n + dt v with v = v_n + g dt).
+    if (st.positions_safe.size() == n) st.positions = st.positions_safe;
+    std::vector<V3<R>> x_old = st.positions, x_target(n);
     for (size_t i = 0; i < n; ++i) x_target[i] = x_old[i] + st.velocities[i] * dt;
+    // Kinematic pins move toward their targets only as far as their
+    // conservative time of impact allows (a teleported pin would drag the
+    // cloth into itself); the rest of the move waits for the next step.
+    {
+      std::vector<V3<R>> pm(n);
+      std::vector<char> none(n, 0);
+      bool any = false;
+      for (const auto& pin : C.pins) if (pin.active) { pm[size_t(pin.vertex_idx)] = pin.target_position - st.positions[size_t(pin.vertex_idx)]; any = true; }
+      if (any) {
+        R t = toi(mesh, st.positions, pm, none, C, rigids, R(0.5) * p.contact_gap_max, R(1e-3) * p.contact_gap_max);
+        for (size_t i = 0; i < n; ++i) if (fixed[i]) st.positions[i] = st.positions[i] + pm[i] * t;
+      }
+    }
     R beta = 0; int bi = 0;
     while (beta < p.beta_max && bi < 20) {
       R alpha = inner_newton(mesh, st, x_target, fixed, C, p, rigids, S);
@@ -1569,11 +1614,12 @@ template <class R> class CorrectedIntegrator {
     }
     if (beta > R(1e-6)) inner_newton(mesh, st, x_target, fixed, C, p, rigids, S);
     S.beta = beta;
-    if (beta > R(1e-6)) {
-      R bdt = beta * dt;
-      for (size_t i = 0; i < n; ++i) st.velocities[i] = (st.positions[i] - x_old[i]) / bdt;
-      if (p.velocity_damping > R(0)) { R sc = R(1) - std::clamp(p.velocity_damping, R(0), R(1)); for (auto& v : st.velocities) v = v * sc; }
-    }
+    // v = (x - x_old) / dt: dividing by beta dt (the reference) turns the
+    // error-reduction pass of a step whose line search held beta near zero
+    // into an arbitrarily large velocity
+    for (size_t i = 0; i < n; ++i) st.velocities[i] = (st.positions[i] - x_old[i]) / dt;
+    if (p.velocity_damping > R(0)) { R sc = R(1) - std::clamp(p.velocity_damping, R(0), R(1)); for (auto& v : st.velocities) v = v * sc; }
+    st.positions_safe = st.positions;
   }
 
   static Csr<R> base_elastic(const Mesh<R>& mesh) { std::vector<Triplet<R>> el; corrected_elastic_triplets(mesh, el); return Csr<R>::from_triplets(Index(3 * mesh.vertices.size()), el); }
@@ -1666,7 +1712,7 @@ template <class R> class CorrectedIntegrator {
 
   // Conservative time of impact along ext (line search of the CORRECTED step).
   static R toi(const Mesh<R>& mesh, const std::vector<V3<R>>& x, const std::vector<V3<R>>& ext, const std::vector<char>& fixed,
-               const Constraints<R>& C, const std::vector<RigidBody<R>>* rigids) {
+               const Constraints<R>& C, const std::vector<RigidBody<R>>* rigids, R eta_min = R(0), R near = R(0)) {
     const size_t n = x.size();
     R t = 1;
     for (const auto& w : C.walls) {
@@ -1691,7 +1737,7 @@ template <class R> class CorrectedIntegrator {
       R l = L(v) + std::max(L(a), std::max(L(b), L(c)));
       auto dist = [&](R s) { R d; V3<R> nm, wp, wq; narrow_pt(x[size_t(v)] + ext[size_t(v)] * s, x[size_t(a)] + ext[size_t(a)] * s,
                                                               x[size_t(b)] + ext[size_t(b)] * s, x[size_t(c)] + ext[size_t(c)] * s, d, nm, wp, wq); return d; };
-      t = std::min(t, advance_toi<R>(dist, l));
+      t = std::min(t, advance_toi<R>(dist, l, eta_min, near));
     }
     for (auto& pr : ee) {
       const Edge &e1 = mesh.edges[size_t(pr.first)], &e2 = mesh.edges[size_t(pr.second)];
@@ -1699,7 +1745,7 @@ template <class R> class CorrectedIntegrator {
       R l = std::max(L(a), L(b)) + std::max(L(c), L(d));
       auto dist = [&](R s) { R dd; V3<R> nm, wp, wq; narrow_ee(x[size_t(a)] + ext[size_t(a)] * s, x[size_t(b)] + ext[size_t(b)] * s,
                                                                x[size_t(c)] + ext[size_t(c)] * s, x[size_t(d)] + ext[size_t(d)] * s, dd, nm, wp, wq); return dd; };
-      t = std::min(t, advance_toi<R>(dist, l));
+      t = std::min(t, advance_toi<R>(dist, l, eta_min, near));
     }
     if (rigids) {
       for (const auto& body : *rigids) {
@@ -1746,18 +1792,19 @@ template <class R> class CorrectedIntegrator {
       auto pr = pcg_solve(H, ng, d, p.pcg_tol, p.pcg_max_iters);
       S.pcg_iters += pr.iters; S.pcg_per_newton.push_back(pr.iters);
       if (!pr.converged) S.pcg_not_converged++;
+      // extended direction 1.25 d, clipped vertex by vertex to length lmax:
+      // no vertex moves more than lmax in one Newton iteration, and a single
+      // runaway entry of d does not scale the whole step down
       std::vector<V3<R>> ext(n);
-      R emax = 0;
       for (size_t i = 0; i < n; ++i) {
         ext[i] = fixed[i] ? V3<R>() : V3<R>(d[3 * i], d[3 * i + 1], d[3 * i + 2]) * R(1.25);
-        emax = std::max(emax, ext[i].norm());
+        R len = ext[i].norm();
+        if (len > lmax) ext[i] = ext[i] * (lmax / len);
       }
-      R cap = emax > lmax ? lmax / emax : R(1);
-      if (cap < R(1)) for (auto& e : ext) e = e * cap;
-      R alpha = cap * toi(mesh, st.positions, ext, fixed, C, rigids);
+      R alpha = std::min(R(1), toi(mesh, st.positions, ext, fixed, C, rigids, R(0), R(1e-3) * p.contact_gap_max));
       S.alphas.push_back(alpha);
       if (alpha < R(1e-8)) return R(0);
-      for (size_t i = 0; i < n; ++i) if (!fixed[i]) st.positions[i] = st.positions[i] + V3<R>(d[3 * i], d[3 * i + 1], d[3 * i + 2]) * alpha;
+      for (size_t i = 0; i < n; ++i) if (!fixed[i]) st.positions[i] = st.positions[i] + ext[i] * (alpha / R(1.25));
       if (alpha > R(0.99)) return R(1);
     }
     return R(0.5);

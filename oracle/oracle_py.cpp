@@ -139,7 +139,7 @@ template <class R> void bind(py::module_& m) {
       .def("initialize", &StateT::initialize)
       .def("num_vertices", [](const StateT& s) { return s.positions.size(); })
       .def("get_positions", [](const StateT& s) { return from_v3(s.positions); })
-      .def("set_positions", [](StateT& s, Arr<R> p) { s.positions = to_v3<R>(p); })
+      .def("set_positions", [](StateT& s, Arr<R> p) { s.positions = to_v3<R>(p); s.positions_safe = s.positions; })
       .def("get_velocities", [](const StateT& s) { return from_v3(s.velocities); })
       .def("set_velocities", [](StateT& s, Arr<R> v) { auto vv = to_v3<R>(v); for (size_t i = 0; i < vv.size() && i < s.velocities.size(); ++i) s.velocities[i] = vv[i]; })
       .def("get_positions_prev", [](const StateT& s) { return from_v3(s.positions_prev); })
