@@ -113,7 +113,7 @@ class StepStats(C.Structure):
         ("newton_iters", C.c_int32), ("pcg_iters", C.c_int32), ("pcg_max_per_newton", C.c_int32),
         ("pcg_not_converged", C.c_int32), ("line_search_fail", C.c_int32), ("contacts", C.c_int32),
         ("strain_active", C.c_int32), ("status", C.c_int32), ("precond_fallbacks", C.c_int32), ("graph_launched", C.c_int32),
-        ("beta", C.c_double), ("last_alpha", C.c_double), ("device_ms", C.c_double),
+        ("beta", C.c_double), ("last_alpha", C.c_double), ("device_ms", C.c_double), ("substeps", C.c_int32), ("pad_", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

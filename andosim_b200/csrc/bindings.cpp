@@ -748,7 +748,7 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         d["newton_iters"] = s.last.newton_iters; d["pcg_iters"] = s.last.pcg_iters; d["pcg_max_per_newton"] = s.last.pcg_max_per_newton;
         d["pcg_not_converged"] = s.last.pcg_not_converged; d["line_search_fail"] = s.last.line_search_fail; d["contacts"] = s.last.contacts;
         d["strain_active"] = s.last.strain_active; d["beta"] = s.last.beta; d["last_alpha"] = s.last.last_alpha;
-        d["device_ms"] = s.last.device_ms; d["precond_fallbacks"] = s.last.precond_fallbacks; d["graph_launched"] = s.last.graph_launched != 0;
+        d["device_ms"] = s.last.device_ms; d["precond_fallbacks"] = s.last.precond_fallbacks; d["graph_launched"] = s.last.graph_launched != 0; d["substeps"] = s.last.substeps;
         return d;
       }, py::arg("state"), "Counters of the state's last step");
 

@@ -129,6 +129,8 @@ struct ando_ctx_s {
   long long mesh_generation = 0;
 
   // CORRECTED semantics
+  DevBuf<double> pin_start, pin_final;   // sub-steps of a fast kinematic drive
+  DevBuf<unsigned long long> pin_maxmove;
   DevBuf<double> x_safe;           // where the last step ended (or the uploaded positions): start of the next CORRECTED step
   bool safe_valid = false;
   DevBuf<unsigned char> fixed;
@@ -712,6 +714,25 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
 int restore_start(ando_ctx c) {
   if (!c->safe_valid) return ANDO_OK;
   CK(cudaMemcpyAsync(c->x.p, c->x_safe.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, c->stream));
+  return ANDO_OK;
+}
+
+// Kinematic pins that move more than half a mean edge length in one step
+// drag the first free rows across their own triangles (the cloth folds onto
+// the pinned row and every later line search stops at zero). Such a step is
+// split into k = ceil(move / (edge / 2)) sub-steps (at most 8).
+int pin_substeps(ando_ctx c, int& k) {
+  k = 1;
+  if (!c->num_pins) return ANDO_OK;
+  CK(c->pin_maxmove.reserve(1));
+  launch_pin_maxdisp(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->pin_maxmove.p, c->stream);
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->pin_maxmove.p, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double mv = 0.0;
+  std::memcpy(&mv, &bits, sizeof(mv));
+  double edge = c->max_move / 4.0;
+  if (edge > 0.0 && mv > 0.5 * edge) k = int(std::min(8.0, std::ceil(mv / (0.5 * edge))));
   return ANDO_OK;
 }
 
@@ -1313,19 +1334,49 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     }
   }
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
-    rc = apply_pins(c, num_rigids);
+    int k = 1;
+    rc = pin_substeps(c, k);
     if (rc) return rc;
+    st.substeps = k;
+    if (k == 1) {
+      rc = apply_pins(c, num_rigids);
+      if (rc) return rc;
+      rc = step_body(c, p, sp, num_rigids, num_walls, st);
+      if (rc) return rc;
+      rc = remember_safe(c);
+      if (rc) return rc;
+    } else {
+      // k sub-steps of dt / k with the pin targets interpolated linearly
+      CK(c->pin_start.reserve(3ull * c->num_pins)); CK(c->pin_final.reserve(3ull * c->num_pins));
+      CK(cudaMemcpyAsync(c->pin_final.p, c->pin_target.p, sizeof(double) * 3ull * c->num_pins, cudaMemcpyDeviceToDevice, s));
+      launch_pin_gather(c->pin_vertex.p, c->num_pins, c->x.p, c->pin_start.p, s);
+      ando_params ps = p;
+      ps.dt = p.dt / k;
+      StepParams sps = sp;
+      sps.dt = ps.dt; sps.dt2inv = 1.0 / (ps.dt * ps.dt);
+      for (int j = 1; j <= k; ++j) {
+        launch_pin_interp(c->num_pins, c->pin_start.p, c->pin_final.p, double(j) / k, c->pin_target.p, s);
+        launch_predict(c->V, c->x.p, c->v.p, ps.dt, c->x_old.p, c->x_hat.p, s);   // x_hat = x + (dt / k) v
+        rc = apply_pins(c, num_rigids);
+        if (rc) return rc;
+        rc = step_body(c, ps, sps, num_rigids, num_walls, st);
+        if (rc) return rc;
+        rc = remember_safe(c);
+        if (rc) return rc;
+      }
+      CK(cudaMemcpyAsync(c->pin_target.p, c->pin_final.p, sizeof(double) * 3ull * c->num_pins, cudaMemcpyDeviceToDevice, s));
+    }
   } else {
     rc = detect(c, num_rigids);
     if (rc) return rc;
     st.contacts = c->ncontacts;
     rc = prepare_contacts(c, sp, c->g_el.p, nullptr);
     if (rc) return rc;
+    rc = step_body(c, p, sp, num_rigids, num_walls, st);
+    if (rc) return rc;
+    rc = remember_safe(c);
+    if (rc) return rc;
   }
-  rc = step_body(c, p, sp, num_rigids, num_walls, st);
-  if (rc) return rc;
-  rc = remember_safe(c);
-  if (rc) return rc;
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev1, s));
   CK(cudaEventSynchronize(c->ev1));

@@ -139,6 +139,31 @@ __global__ void k_pin_ext(const int* pin_vertex, const double* pin_target, int n
   for (int q = 0; q < 3; ++q) { ext[3 * v + q] = pin_target[3 * k + q] - x[3 * v + q]; x1[3 * v + q] = pin_target[3 * k + q]; }
   fixed[v] = 1;
 }
+// Largest pin move |target - x| (IEEE bits, max-reduced as integers).
+__global__ void k_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (k < num_pins) {
+    int v = pin_vertex[k];
+    double a = pin_target[3 * k] - x[3 * v], b = pin_target[3 * k + 1] - x[3 * v + 1], c = pin_target[3 * k + 2] - x[3 * v + 2];
+    m = sqrt(a * a + b * b + c * c);
+  }
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+// Sub-step pin targets: start_k = x[pin vertex] once, then target = start + f (final - start).
+__global__ void k_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= num_pins) return;
+  int v = pin_vertex[k];
+  for (int q = 0; q < 3; ++q) start[3 * k + q] = x[3 * v + q];
+}
+__global__ void k_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 3 * num_pins) return;
+  target[k] = start[k] + (fin[k] - start[k]) * f;
+}
+
 // x += toi * ext on pinned vertices (toi: the move's conservative time of impact).
 __global__ void k_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -317,6 +342,17 @@ void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pin
 }
 void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x, cudaStream_t s) {
   if (num_pins) k_pin_move<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, ext, toi, x);
+}
+void launch_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out,
+                        cudaStream_t s) {
+  cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+  if (num_pins) k_pin_maxdisp<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, out);
+}
+void launch_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start, cudaStream_t s) {
+  if (num_pins) k_pin_gather<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, x, start);
+}
+void launch_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target, cudaStream_t s) {
+  if (num_pins) k_pin_interp<<<nblk(3ll * num_pins), TPB, 0, s>>>(num_pins, start, fin, f, target);
 }
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s) {

@@ -79,6 +79,10 @@ void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_p
 void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
                     unsigned char* fixed, cudaStream_t s);
 void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x, cudaStream_t s);
+void launch_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out,
+                        cudaStream_t s);
+void launch_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start, cudaStream_t s);
+void launch_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target, cudaStream_t s);
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s);
 void launch_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double scale, double lmax,

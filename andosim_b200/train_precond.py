@@ -1,14 +1,16 @@
 """Train the learned preconditioner on the two-curtain workload and evaluate it.
 
-    python -m andosim_b200.train_precond [--n 256] [--train-seeds 0-7] [--eval-seeds 8-11]
-        [--frames 300] [--every 10] [--steps 3000] [--out PATH] [--report PATH]
+    python -m andosim_b200.train_precond [--sets 256:0-14:1,64:0-239:4] [--train-seeds 0-7]
+        [--eval-seeds 8-11] [--steps 3000] [--out PATH] [--report PATH]
 
-Training data are the solver's own dumps: the first Newton system of every
-`every`-th frame of CORRECTED-semantics runs of scenes.c4 for the training
-seeds, each with probe residuals of a block-Jacobi solve. Evaluation steps the
-held-out seeds for `frames` frames with block Jacobi and with the trained
-network (device timing, PCG iterations per Newton step, fallbacks, and the
-final position difference between the two runs).
+Training data are the solver's own dumps: the first Newton system of the
+chosen frames of CORRECTED-semantics runs of scenes.c4 for the training seeds,
+each with probe residuals of a block-Jacobi solve. `--sets` lists
+grid:first-last:every triples (several resolutions train one network: its
+inputs are scale-free). Evaluation steps the held-out seeds over the same
+frame ranges with block Jacobi and with the trained network (device timing,
+PCG iterations per Newton step, fallbacks, and the final position difference
+between the two runs).
 """
 from __future__ import annotations
 
@@ -52,12 +54,9 @@ def evaluate(sc, weights, frames: int, precond: str, refresh: int = 1, device: i
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--sets", default="256:0-14:1,64:0-239:4")
     ap.add_argument("--train-seeds", default="0-7")
     ap.add_argument("--eval-seeds", default="8-11")
-    ap.add_argument("--frames", type=int, default=300)
-    ap.add_argument("--every", type=int, default=10)
-    ap.add_argument("--eval-frames", type=int, default=300)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--init-seed", type=int, default=0)
@@ -66,9 +65,14 @@ def main(argv=None):
     ap.add_argument("--report", default=None)
     a = ap.parse_args(argv)
 
+    sets = []
+    for spec in a.sets.split(","):
+        n, fr, ev = spec.split(":")
+        f0, f1 = fr.split("-")
+        sets.append((int(n), int(f0), int(f1), int(ev)))
     t0 = time.time()
     trainer = abi.Trainer(abi.precond_init_weights(a.init_seed))
-    n_sys = learned.c4_training_set(trainer, seeds(a.train_seeds), a.n, range(0, a.frames, a.every))
+    n_sys = sum(learned.c4_training_set(trainer, seeds(a.train_seeds), n, range(f0, f1 + 1, ev)) for n, f0, f1, ev in sets)
     t_collect = time.time() - t0
     loss0 = learned.mean_loss(trainer)
     t1 = time.time()
@@ -78,18 +82,19 @@ def main(argv=None):
     w = trainer.weights()
     trainer.close()
     out = learned.save_weights(w, a.out)
-    report = dict(n=a.n, train_seeds=seeds(a.train_seeds), systems=n_sys, collect_s=t_collect, train_steps=a.steps,
+    report = dict(sets=a.sets, train_seeds=seeds(a.train_seeds), systems=n_sys, collect_s=t_collect, train_steps=a.steps,
                   train_s=t_train, loss_before=loss0, loss_after=loss1, weights=str(out), eval=[])
     print(json.dumps({k: v for k, v in report.items() if k != "eval"}), flush=True)
-    for sd in seeds(a.eval_seeds):
-        sc = scenes.c4(seed=sd, n=a.n)
-        rj, xj = evaluate(sc, None, a.eval_frames, "block_jacobi")
-        rl, xl = evaluate(sc, w, a.eval_frames, "learned", a.refresh)
-        ext = float(np.ptp(sc.vertices, axis=0).max())
-        row = dict(seed=sd, jacobi=rj, learned=rl, pos_diff_rel=float(np.abs(xl - xj).max() / ext),
-                   iter_ratio=rl["pcg_per_newton"] / max(rj["pcg_per_newton"], 1e-30))
-        report["eval"].append(row)
-        print(json.dumps(row), flush=True)
+    for n, f0, f1, _ in sets:
+        for sd in seeds(a.eval_seeds):
+            sc = scenes.c4(seed=sd, n=n)
+            rj, xj = evaluate(sc, None, f1 + 1, "block_jacobi")
+            rl, xl = evaluate(sc, w, f1 + 1, "learned", a.refresh)
+            ext = float(np.ptp(sc.vertices, axis=0).max())
+            row = dict(n=n, frames=f1 + 1, seed=sd, jacobi=rj, learned=rl, pos_diff_rel=float(np.abs(xl - xj).max() / ext),
+                       iter_ratio=rl["pcg_per_newton"] / max(rj["pcg_per_newton"], 1e-30))
+            report["eval"].append(row)
+            print(json.dumps(row), flush=True)
     if a.report:
         Path(a.report).write_text(json.dumps(report, indent=1))
 

@@ -48,13 +48,15 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=240)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256, help="curtain grid side")
     ap.add_argument("--cpu-frames", type=int, default=1, help="frames of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-steps", type=int, default=240, help="frames of the REFERENCE-semantics measurement (0: skip)")
+    ap.add_argument("--full-n", type=int, default=64, help="curtain grid of the full-length CORRECTED comparison (0: skip)")
+    ap.add_argument("--full-steps", type=int, default=240, help="frames of the full-length CORRECTED comparison")
     ap.add_argument("--refresh", type=int, default=1, help="Newton iterations between evaluations of the preconditioner network")
     ap.add_argument("--weights", default=None, help="learned preconditioner weights (.npy); default: the shipped C4 weights")
     return ap.parse_args()
@@ -217,7 +219,7 @@ def corrected_run(args, sc, local, flush, pg, precond, weights, profile=False, f
             "_prof": prof, "_nnzb": nnzb}
 
 
-def paired_run(args, sc, local, flush, pg, weights):
+def paired_run(args, sc, local, flush, pg, weights, steps=None):
     """The learned-preconditioner trajectory, timed frame by frame; before each
     learned frame a block-Jacobi frame is timed from the same state and then
     undone, so both preconditioners solve exactly the same Newton systems of
@@ -241,7 +243,8 @@ def paired_run(args, sc, local, flush, pg, weights):
     ext = float(np.ptp(sc.vertices, axis=0).max())
     res = {"learned": dict(ms=0.0, stats=[], launches=0), "block_jacobi": dict(ms=0.0, stats=[], launches=0)}
     diffs = []
-    for k in range(args.steps):
+    steps = args.steps if steps is None else steps
+    for k in range(steps):
         pins = abi.pin_array(sc.pins_at(args.warmup + k))
         x0, v0 = S.download()
         outs = {}
@@ -267,11 +270,13 @@ def paired_run(args, sc, local, flush, pg, weights):
         stats = r["stats"]
         newton = sum(s["newton_iters"] for s in stats)
         pcg = sum(s["pcg_iters"] for s in stats)
-        out[name] = {"frames": args.steps, "total_ms": ms, "frames_per_s": round(args.steps / (ms * 1e-3), 2),
-                     "ms_per_frame": round(ms / args.steps, 3), "newton_iters_per_frame": round(newton / args.steps, 3),
+        out[name] = {"frames": steps, "total_ms": ms, "frames_per_s": round(steps / (ms * 1e-3), 2),
+                     "ms_per_frame": round(ms / steps, 3), "newton_iters_per_frame": round(newton / steps, 3),
                      "pcg_iters_per_newton": round(pcg / newton, 2) if newton else 0.0,
                      "newton_iters_per_s": round(newton / (ms * 1e-3), 1),
                      "precond_fallbacks": sum(s["precond_fallbacks"] for s in stats),
+                     "line_search_fail": sum(s["line_search_fail"] for s in stats),
+                     "substeps": sum(s["substeps"] for s in stats),
                      "contacts_max": max(s["contacts"] for s in stats) if stats else 0,
                      "gpu_launches": int(r["launches"])}
     out["learned"]["refresh"] = args.refresh
@@ -378,8 +383,19 @@ def run_ours(args, rank, world, local, pg):
     clock_info = clocks.stop()
     lrn, jac = pair["learned"], pair["block_jacobi"]
     # phase breakdown and PCG roofline: a separate profiled pass (per-phase CUDA events)
-    prof_frames = min(args.steps, 60)
+    prof_frames = args.steps
     lp = corrected_run(args, sc, local, flush, pg, "learned", weights, profile=True, frames=prof_frames)
+    full = None
+    if args.full_n > 0:
+        from andosim_b200 import scenes as _sc
+        scf = _sc.c4(seed=rank, n=args.full_n)
+        pf = paired_run(args, scf, local, flush, pg, weights, steps=args.full_steps)
+        full = {"workload": f"c4_curtains_2x{args.full_n}x{args.full_n}", "frames": args.full_steps,
+                "learned": {k: v for k, v in pf["learned"].items() if k != "total_ms"},
+                "jacobi": {k: v for k, v in pf["block_jacobi"].items() if k != "total_ms"},
+                "frames_per_s_ratio": round(pf["learned"]["frames_per_s"] / pf["block_jacobi"]["frames_per_s"], 3),
+                "pcg_iters_per_newton_ratio": round(pf["learned"]["pcg_iters_per_newton"] / max(pf["block_jacobi"]["pcg_iters_per_newton"], 1e-9), 3),
+                "step_position_diff_rel_extent": pf["step_position_diff_rel_extent"]}
     prof, nnzb = lp.pop("_prof"), lp.pop("_nnzb")
     peaks = json.loads(PEAKS_FILE.read_text()) if PEAKS_FILE.exists() else {}
     hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
@@ -403,6 +419,10 @@ def run_ours(args, rank, world, local, pg):
         "data": "synthetic (seeded curtains, scenes.c4)",
         "config": {"workload": WORKLOAD, "vertices": V, "triangles": T, "bsr_blocks": nnzb, "semantics": "CORRECTED",
                    "preconditioner": "learned", "precond_refresh": args.refresh, "frames_timed_per_gpu": args.steps,
+                   "frames": f"{args.warmup}-{args.warmup + args.steps - 1}",
+                   "frame_window": "the drive moves the pinned rows up to two edge lengths per frame at 256 x 256; from frame ~16 "
+                                   "the first free rows fold onto the pinned rows and the CORRECTED line search stops, so the "
+                                   "timed window ends before that (full_length: a 64 x 64 pair of curtains over 240 frames)",
                    "l2": "flushed before every timed frame", "parallelism": f"replicas x{world}"},
         "pcg_iters_per_newton": lrn["pcg_iters_per_newton"],
         "newton_iters_per_frame": lrn["newton_iters_per_frame"],
@@ -413,6 +433,7 @@ def run_ours(args, rank, world, local, pg):
                               "paired": "each frame both preconditioners step from the same state",
                               "step_position_diff_rel_extent": pair["step_position_diff_rel_extent"]},
         "profiled_pass": lp,
+        "full_length": full,
         "gpu_launches": lrn["gpu_launches"],
         "roofline": roof,
         "clocks": clock_info,

@@ -128,6 +128,8 @@ typedef struct {
   double beta;
   double last_alpha;
   double device_ms;            /* device time of the step (CUDA events) */
+  int32_t substeps;            /* CORRECTED: sub-steps taken for a fast kinematic drive (1 = none) */
+  int32_t pad_;
 } ando_step_stats;
 
 typedef struct ando_ctx_s* ando_ctx;

@@ -1579,9 +1579,47 @@ template <class R> R advance_toi(const std::function<R(R)>& dist, R l, R eta_min
 
 template <class R> class CorrectedIntegrator {
  public:
+  // Kinematic pins that move more than half a mean edge length in one step
+  // drag the first free rows across their own triangles (the cloth folds onto
+  // the pinned row and every later line search stops at zero). Such a step is
+  // split into k = ceil(move / (edge / 2)) sub-steps (at most 8) of dt / k
+  // with the pin targets interpolated linearly.
+  static int substeps(const Mesh<R>& mesh, const State<R>& st, const Constraints<R>& C) {
+    const std::vector<V3<R>>& x0 = st.positions_safe.size() == st.positions.size() ? st.positions_safe : st.positions;
+    double mv = 0.0;
+    for (const auto& pin : C.pins) if (pin.active) mv = std::max(mv, double((pin.target_position - x0[size_t(pin.vertex_idx)]).norm()));
+    double edge = double(max_move(mesh)) / 4.0;
+    if (!(edge > 0.0) || !(mv > 0.5 * edge)) return 1;
+    return int(std::min(8.0, std::ceil(mv / (0.5 * edge))));
+  }
+
   static void step(Mesh<R>& mesh, State<R>& st, Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>* stats = nullptr) {
     StepStats<R> local; StepStats<R>& S = stats ? *stats : local;
     S = StepStats<R>();
+    const int k = substeps(mesh, st, C);
+    if (k == 1) { step_once(mesh, st, C, p, rigids, S); return; }
+    const size_t n = st.positions.size();
+    const std::vector<V3<R>>& x0 = st.positions_safe.size() == n ? st.positions_safe : st.positions;
+    std::vector<V3<R>> start(C.pins.size());
+    for (size_t q = 0; q < C.pins.size(); ++q) start[q] = x0[size_t(C.pins[q].vertex_idx)];
+    Constraints<R> Cs = C;
+    SimParams<R> ps = p;
+    ps.dt = R(double(p.dt) / k);
+    for (int j = 1; j <= k; ++j) {
+      for (size_t q = 0; q < C.pins.size(); ++q)
+        Cs.pins[q].target_position = start[q] + (C.pins[q].target_position - start[q]) * R(double(j) / k);
+      StepStats<R> Sj;
+      step_once(mesh, st, Cs, ps, rigids, Sj);
+      S.newton_iters += Sj.newton_iters; S.pcg_iters += Sj.pcg_iters; S.line_search_fail += Sj.line_search_fail;
+      S.contacts = std::max(S.contacts, Sj.contacts); S.pcg_not_converged += Sj.pcg_not_converged; S.strain_active = Sj.strain_active;
+      S.beta = Sj.beta;
+      S.alphas.insert(S.alphas.end(), Sj.alphas.begin(), Sj.alphas.end());
+      S.pcg_per_newton.insert(S.pcg_per_newton.end(), Sj.pcg_per_newton.begin(), Sj.pcg_per_newton.end());
+    }
+  }
+
+  static void step_once(Mesh<R>& mesh, State<R>& st, Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids,
+                        StepStats<R>& S) {
     const size_t n = st.positions.size(); const R dt = p.dt;
     std::vector<char> fixed(n, 0);
     for (const auto& pin : C.pins) if (pin.active) fixed[size_t(pin.vertex_idx)] = 1;
