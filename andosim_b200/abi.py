@@ -29,7 +29,7 @@ EXPORTED = [
     "ando_broad_phase", "ando_pcg_solve_noalloc",
 ]
 
-PHASES = ["setup", "strain", "gradient", "assemble", "pcg", "line_search", "finish"]
+PHASES = ["setup", "strain", "gradient", "assemble", "pcg", "line_search", "finish", "precond"]
 
 
 class Material(C.Structure):
@@ -96,7 +96,7 @@ class Contact(C.Structure):
 
 
 class Profile(C.Structure):
-    _fields_ = [("launches", C.c_int64), ("phase_launches", C.c_int64 * 7), ("phase_ms", C.c_double * 7),
+    _fields_ = [("launches", C.c_int64), ("phase_launches", C.c_int64 * 8), ("phase_ms", C.c_double * 8),
                 ("pcg_iterations", C.c_int64), ("newton_iterations", C.c_int64), ("pcg_learned_iterations", C.c_int64),
                 ("pcg_extra_block_iterations", C.c_int64)]
 

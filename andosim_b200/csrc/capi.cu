@@ -86,6 +86,11 @@ struct ando_ctx_s {
   double dt2inv = 0.0;             // of the last assembled system
   double gap_max = 1e-3;           // contact activation distance of the current step
 
+  // SELL-32 copy of the static pattern for the scaled PCG (pcg.cu)
+  DevBuf<int> chunk_off, sell_col, sell_base;
+  DevBuf<float> valh_sell, S_sell;
+  int sell_blocks = 0;
+
   // learned preconditioner: weights, activations, S on the static pattern
   DevBuf<int> slot_T;
   DevBuf<float> net_master, net_buf, lw_buf, Sval;
@@ -139,7 +144,8 @@ struct ando_ctx_s {
   double max_move = 1e300;   // 4 x mean rest edge length: largest displacement per Newton iteration
   DevBuf<int2> pairs_ee;
 
-  // broad phase
+  // broad phase (the LBVHs are rebuilt once per step, refit in between)
+  long long bvh_epoch = 0;
   DevBuf<int> edges;
   int E = 0;
   Lbvh bvh_tri, bvh_edge;
@@ -481,9 +487,9 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
   {
     Phase ph(c, ANDO_PHASE_SETUP);
     long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-    CK(c->bvh_tri.build(c->x.p, nullptr, c->tris.p, 3, c->T, float(gap_max), c->cub_tmp, s));
+    CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
     CK(c->bvh_tri.query(c->x.p, nullptr, 0, nullptr, c->V, float(gap_max), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
-    CK(c->bvh_edge.build(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->cub_tmp, s));
+    CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
     CK(c->bvh_edge.query(c->x.p, nullptr, 1, c->edges.p, c->E, float(gap_max), c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
     ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   }
@@ -536,9 +542,9 @@ int corrected_line_search(ando_ctx c, int nb) {
   ph.launched(2 + (c->num_walls ? 1 : 0));
   int nvt = 0, nee = 0;
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-  CK(c->bvh_tri.build(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->cub_tmp, s));
+  CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
   CK(c->bvh_tri.query(c->x.p, c->x1.p, 0, nullptr, c->V, 0.f, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
-  CK(c->bvh_edge.build(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->cub_tmp, s));
+  CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
   CK(c->bvh_edge.query(c->x.p, c->x1.p, 1, c->edges.p, c->E, 0.f, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nvt + nee) { launch_toi_pairs(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, c->ext.p, 0.0, 1e-3 * c->gap_max, c->toi.p, s); ph.launched(); }
@@ -587,14 +593,14 @@ void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
   launch_diag_factor(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->g.p, c->Linv.p, c->Lf.p, c->bhat.p,
                      c->chol_ok.p, c->ctrl.p, s);
   launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p, c->val.p,
-                         c->valh.p, c->ctrl.p, s);
+                         c->valh.p, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s);
   if (c->nx) launch_extra_merge(c->contacts.p, c->xent.p, c->xk1.p, c->xi1.p, c->xheads.p, c->nx, c->nx_raw, c->fixed.p, sp, c->Linv.p,
                                 nullptr, nullptr, nullptr, c->xvalh.p, s);
 }
 
 PcgScaledArgs scaled_args(ando_ctx c, const ando_params& p) {
   PcgScaledArgs a;
-  a.V = c->V; a.rowptr = c->rowptr.p; a.cols = c->cols.p; a.valh = c->valh.p;
+  a.V = c->V; a.chunk_off = c->chunk_off.p; a.sell_col = c->sell_col.p; a.valh = c->valh_sell.p;
   a.xbegin = c->nx ? c->xbegin.p : nullptr; a.xend = c->nx ? c->xend.p : nullptr; a.xcols = c->xcols.p; a.xvalh = c->xvalh.p;
   a.S = nullptr; a.Linv = c->Linv.p; a.Lf = c->Lf.p; a.bhat = c->bhat.p; a.d = c->d.p;
   a.xh = c->xh.p; a.r = c->r.p; a.r2 = c->r2.p; a.z = c->z.p; a.p0 = c->p0.p; a.p1 = c->p1.p; a.Ap = c->Ap.p;
@@ -606,7 +612,7 @@ PcgScaledArgs scaled_args(ando_ctx c, const ando_params& p) {
 LsView ls_view(ando_ctx c) {
   LsView v;
   v.V = c->V; v.nnzb = c->nnzb; v.rowptr = c->rowptr.p; v.cols = c->cols.p; v.slot_row = c->slot_row.p; v.slot_T = c->slot_T.p;
-  v.valh = c->valh.p;
+  v.sell_base = c->sell_base.p; v.valh = c->valh.p;
   v.xbegin = c->nx ? c->xbegin.p : nullptr; v.xend = c->nx ? c->xend.p : nullptr; v.xcols = c->xcols.p; v.xvalh = c->xvalh.p;
   v.Lf = c->Lf.p; v.mass = c->mass.p; v.fixed = c->fixed.p; v.dt2inv = c->dt2inv;
   return v;
@@ -621,6 +627,7 @@ int ensure_learned(ando_ctx c) {
     learned_work_carve(c->lw, c->lw_buf.p, c->V, c->nnzb, false);
   }
   CK(c->Sval.reserve(9ull * c->nnzb));
+  CK(c->S_sell.reserve(9ull * c->sell_blocks));
   return ANDO_OK;
 }
 
@@ -629,24 +636,27 @@ int ensure_learned(ando_ctx c) {
 // the iteration cap), block-Jacobi otherwise.
 int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
   cudaStream_t s = c->stream;
-  Phase ph(c, ANDO_PHASE_PCG);
   PcgScaledArgs sa = scaled_args(c, p);
   if (p.precond == ANDO_PRECOND_LEARNED) {
     int rc = ensure_learned(c);
     if (rc) return rc;
     LsView v = ls_view(c);
     const int refresh = p.precond_refresh > 1 ? p.precond_refresh : 1;
+    Phase pn(c, ANDO_PHASE_PRECOND);
     if (!c->coeff_valid || c->coeff_mesh != c->mesh_generation || c->coeff_age >= refresh) {
-      learned_forward(v, c->net, c->lw, c->Sval.p, s);
+      learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, s);
       c->coeff_valid = true; c->coeff_mesh = c->mesh_generation; c->coeff_age = 1;
-      ph.launched(5 + 3 * net::NL);
+      pn.launched(5 + 3 * net::NL);
     } else {
-      learned_build_S(v, c->lw, c->Sval.p, s);
+      learned_build_S(v, c->lw, c->Sval.p, c->S_sell.p, s);
       c->coeff_age++;
-      ph.launched();
+      pn.launched();
     }
     c->S_ready = true;
-    sa.S = c->Sval.p;
+  }
+  Phase ph(c, ANDO_PHASE_PCG);
+  if (p.precond == ANDO_PRECOND_LEARNED) {
+    sa.S = c->S_sell.p;
     CK(launch_pcg_scaled(sa, true, c->pcg_learned_grid, s));
     ph.launched();
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
@@ -759,9 +769,9 @@ int apply_pins(ando_ctx c, int nb) {
   ph.launched(2 + (c->num_walls ? 1 : 0));
   int nvt = 0, nee = 0;
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-  CK(c->bvh_tri.build(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->cub_tmp, s));
+  CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
   CK(c->bvh_tri.query(c->x.p, c->x1.p, 0, nullptr, c->V, 0.f, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
-  CK(c->bvh_edge.build(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->cub_tmp, s));
+  CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
   CK(c->bvh_edge.query(c->x.p, c->x1.p, 1, c->edges.p, c->E, 0.f, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nvt + nee) {
@@ -1130,6 +1140,23 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   std::vector<int> slotT(nnzb);
   for (int r = 0; r < V; ++r)
     for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) slotT[k] = slot_of(cols[k], r);
+  // SELL-32: chunks of 32 rows padded to the chunk's longest row
+  const int nch = (V + 31) / 32;
+  std::vector<int> choff(nch + 1, 0);
+  for (int ch = 0; ch < nch; ++ch) {
+    int w = 0;
+    for (int r = 32 * ch; r < std::min(V, 32 * ch + 32); ++r) w = std::max(w, rowptr[r + 1] - rowptr[r]);
+    choff[ch + 1] = choff[ch] + 32 * w;
+  }
+  std::vector<int> scol(choff[nch], -1), sbase(nnzb);
+  for (int r = 0; r < V; ++r) {
+    int ch = r >> 5, l = r & 31;
+    for (int k = 0; k < rowptr[r + 1] - rowptr[r]; ++k) {
+      int slot = choff[ch] + 32 * k;
+      scol[slot + l] = cols[rowptr[r] + k];
+      sbase[rowptr[r] + k] = 9 * slot + l;
+    }
+  }
   cudaStream_t s = c->stream;
   c->V = V; c->T = T; c->nnzb = nnzb;
   c->S_ready = false;
@@ -1143,6 +1170,11 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->slot_row.upload(slot_row.data(), nnzb, s));
   CK(c->diag_slot.upload(diag_slot.data(), V, s));
   CK(c->slot_T.upload(slotT.data(), nnzb, s));
+  c->sell_blocks = choff[nch];
+  CK(c->chunk_off.upload(choff.data(), nch + 1, s));
+  CK(c->sell_col.upload(scol.data(), choff[nch], s));
+  CK(c->sell_base.upload(sbase.data(), nnzb, s));
+  CK(c->valh_sell.reserve(9ull * choff[nch]));
   CK(c->face_slot.upload(face_slot.data(), 9ull * T, s));
   CK(c->slot_cptr.upload(cptr.data(), nnzb + 1, s));
   CK(c->slot_contrib.upload(contrib.data(), 9ull * T, s));
@@ -1286,6 +1318,7 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
   rc = upload_constraints(c, p, pins, num_pins, walls, num_walls, rigids, num_rigids, sp);
   if (rc) return rc;
   c->gap_max = p.contact_gap_max;
+  c->bvh_epoch++;
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
     rc = restore_start(c);
     if (rc) return rc;
@@ -1409,6 +1442,7 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   if (rc) return rc;
   cudaStream_t s = c->stream;
   c->gap_max = p.contact_gap_max;
+  c->bvh_epoch++;
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
     rc = restore_start(c);
     if (rc) return rc;
@@ -1621,7 +1655,7 @@ int32_t ando_precond_eval(ando_ctx c) {
   rc = ensure_learned(c);
   if (rc) return rc;
   LsView v = ls_view(c);
-  learned_forward(v, c->net, c->lw, c->Sval.p, c->stream);
+  learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, c->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   c->S_ready = true;
@@ -1672,6 +1706,7 @@ struct ando_trainer_s {
     LsView view() const {
       LsView v;
       v.V = V; v.nnzb = nnzb; v.rowptr = rowptr.p; v.cols = cols.p; v.slot_row = slot_row.p; v.slot_T = slot_T.p; v.valh = valh.p;
+      v.sell_base = nullptr;
       v.xbegin = nx ? xbegin.p : nullptr; v.xend = nx ? xend.p : nullptr; v.xcols = xcols.p; v.xvalh = xvalh.p;
       v.Lf = Lf.p; v.mass = mass.p; v.fixed = fixed.p; v.dt2inv = dt2inv;
       return v;

@@ -814,27 +814,30 @@ __global__ void k_diag_factor(MeshDev m, const unsigned char* sflags, const Stra
 // factored rows are exactly I.
 __global__ void k_assemble_scaled(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                                   const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                                  const Ctrl* ctrl) {
+                                  const int* sell_base, float* valh_sell, const Ctrl* ctrl) {
   if (ctrl->converged) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= m.nnzb) return;
   int row = m.slot_row[s], col = m.cols[s];
-  float* vh = valh + 9 * (long long)s;
+  float R[9];
   if (fixed && (fixed[row] || fixed[col])) {
     float one = row == col ? 1.f : 0.f;
-    for (int k = 0; k < 9; ++k) { float v = (k % 4 == 0) ? one : 0.f; vh[k] = v; if (val) val[9 * (long long)s + k] = v; }
-    return;
+    for (int k = 0; k < 9; ++k) { R[k] = (k % 4 == 0) ? one : 0.f; if (val) val[9 * (long long)s + k] = R[k]; }
+  } else {
+    double H[9];
+    slot_block(m, s, row, col, sflags, sv, diag_extra, enable_strain, H);
+    if (val) for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = float(H[k]);
+    if (row == col && chol_ok[row]) {
+      for (int k = 0; k < 9; ++k) R[k] = (k % 4 == 0) ? 1.f : 0.f;
+    } else {
+      double Rd[9];
+      scale_block(ld_tri(Linv, row), H, ld_tri(Linv, col), Rd);
+      for (int k = 0; k < 9; ++k) R[k] = float(Rd[k]);
+    }
   }
-  double H[9];
-  slot_block(m, s, row, col, sflags, sv, diag_extra, enable_strain, H);
-  if (val) for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = float(H[k]);
-  if (row == col && chol_ok[row]) {
-    for (int k = 0; k < 9; ++k) vh[k] = (k % 4 == 0) ? 1.f : 0.f;
-    return;
-  }
-  double R[9];
-  scale_block(ld_tri(Linv, row), H, ld_tri(Linv, col), R);
-  for (int k = 0; k < 9; ++k) vh[k] = float(R[k]);
+  float* vh = valh + 9 * (long long)s;
+  float* vs = valh_sell + sell_base[s];
+  for (int k = 0; k < 9; ++k) { vh[k] = R[k]; vs[32 * k] = R[k]; }
 }
 
 // Contact blocks outside the static pattern. Entries of the same (row, col)
@@ -1260,8 +1263,9 @@ void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const Str
 }
 void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                             const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                            const Ctrl* ctrl, cudaStream_t s) {
-  if (m.nnzb) k_assemble_scaled<<<nblk(m.nnzb), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh, ctrl);
+                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s) {
+  if (m.nnzb) k_assemble_scaled<<<nblk(m.nnzb), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh,
+                                                             sell_base, valh_sell, ctrl);
 }
 void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s) {
   if (n) k_extra_key64<<<nblk(n), TPB, 0, s>>>(xent, xkeys, n, key, idx);

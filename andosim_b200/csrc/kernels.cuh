@@ -49,7 +49,7 @@ void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const Str
                         const Ctrl* ctrl, cudaStream_t s);
 void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                             const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                            const Ctrl* ctrl, cudaStream_t s);
+                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s);
 void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s);
 void launch_run_heads(const unsigned long long* key, int n, int* flags, cudaStream_t s);
 void launch_extra_merge(const ContactDev* c, const ContactEntry* xent, const unsigned long long* key, const int* idx, const int* heads, int nu,
@@ -113,9 +113,9 @@ int pcg_grid_size(int device);
 // the learned approximate inverse S of the scaled system.
 struct PcgScaledArgs {
   int V;
-  const int* rowptr; const int* cols; const float* valh;                      // A^ on the static pattern
+  const int* chunk_off; const int* sell_col; const float* valh;               // A^ on the static pattern (SELL-32, pcg.cu)
   const int* xbegin; const int* xend; const int* xcols; const float* xvalh;  // A^ extra contact segment
-  const float* S;       // learned preconditioner blocks on the static pattern (learned solves only)
+  const float* S;       // learned preconditioner blocks, SELL-32 like valh (learned solves only)
   const double* Linv;   // 6V packed L^-1
   const float* Lf;      // 6V packed L
   const float* bhat;    // 3V  L^-1 b

@@ -265,9 +265,10 @@ cudaError_t Lbvh::reserve_prims(int n) {
 }
 
 // Build the hierarchy over `n` primitives of `arity` vertex indices each.
-cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, int arity, int n_, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s) {
+cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, int arity_, int n_, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s) {
   n = n_;
   prims = prims_;
+  arity = arity_;
   cudaError_t e = reserve_prims(n);
   if (e) return e;
   if (n == 0) return cudaSuccess;
@@ -287,6 +288,27 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
   k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p);
   launches += n > 1 ? 6 : 5;
   return cudaGetLastError();
+}
+
+// Update the boxes of the last build for new positions (same primitives):
+// primitive boxes, then the bottom-up node boxes over the existing topology.
+// The candidate set of a query does not depend on the topology, only the
+// traversal cost does, so the Morton order of an earlier build stays valid.
+cudaError_t Lbvh::refit(const double* x, const double* x1, float pad, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  cudaError_t e;
+  k_prim_boxes<<<nblk(n), TPB, 0, s>>>(x, x1, prims, arity, n, pad, boxes.p);
+  if (n > 1 && (e = cudaMemsetAsync(arrive.p, 0, sizeof(int) * n, s))) return e;
+  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p);
+  launches += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t Lbvh::update(const double* x, const double* x1, const int* prims_, int arity_, int n_, float pad, long long epoch_,
+                         DevBuf<unsigned char>& tmp, cudaStream_t s) {
+  if (epoch_ == epoch && n_ == n && prims_ == prims && arity_ == arity && n > 0) return refit(x, x1, pad, s);
+  epoch = epoch_;
+  return build(x, x1, prims_, arity_, n_, pad, tmp, s);
 }
 
 // Query the hierarchy; returns the sorted (query, primitive) pairs in `out`

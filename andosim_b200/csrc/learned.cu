@@ -103,42 +103,60 @@ __global__ void k_node_feats(LsView s, const float* Ef, float* X) {
 // --------------------------------------------------------------- row GEMM
 // Y[r, :N] = act(X[r, :] M + bias) + R1[r, :N] + R2[r, :N], X = [X1 | X2]
 // (K = K1 + K2 <= 128), M row-major [K][N], N in {64, 128}; Q gets the
-// pre-activation. 32 rows per CTA, N/8 outputs per thread.
+// pre-activation. 64 rows per CTA (M is staged in shared memory once per 64
+// rows), each thread 4 rows x N/16 outputs held in registers (N is a template
+// parameter so the accumulators never spill to local memory).
+template <int N>
 __global__ void __launch_bounds__(TPB) k_gemm(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* M,
-                                              int N, const float* bias, const float* R1, int ldr1, const float* R2, int ldr2, float* Q,
+                                              const float* bias, const float* R1, int ldr1, const float* R2, int ldr2, float* Q,
                                               float* Y, int relu) {
+  constexpr int ROWS = 64, PER = N / 16;
   extern __shared__ float sm[];
   const int K = K1 + K2, XS = K + 1;
   float* Ms = sm;                // K x N
-  float* Xs = sm + K * N;        // 32 x XS
-  const int r0 = blockIdx.x * 32;
+  float* Xs = sm + K * N;        // ROWS x XS
+  const int r0 = blockIdx.x * ROWS;
   for (int i = threadIdx.x; i < K * N; i += TPB) Ms[i] = M[i];
-  for (int i = threadIdx.x; i < 32 * K; i += TPB) {
+  for (int i = threadIdx.x; i < ROWS * K; i += TPB) {
     int r = i / K, k = i % K, row = r0 + r;
     float v = 0.f;
     if (row < V) v = k < K1 ? X1[(long long)row * ld1 + k] : X2[(long long)row * ld2 + (k - K1)];
     Xs[r * XS + k] = v;
   }
   __syncthreads();
-  const int per = N / 8;
-  const int r = threadIdx.x / 8, c0 = (threadIdx.x % 8) * per;
-  float acc[16];
-  for (int j = 0; j < 16; ++j) acc[j] = 0.f;
+  // 16 row groups of 4 rows x 16 column groups of PER columns
+  const int r = (threadIdx.x / 16) * 4, c0 = (threadIdx.x % 16) * PER;
+  float acc[4][PER];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int j = 0; j < PER; ++j) acc[a][j] = 0.f;
   for (int k = 0; k < K; ++k) {
-    float xv = Xs[r * XS + k];
+    float xv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) xv[a] = Xs[(r + a) * XS + k];
     const float* mr = Ms + k * N + c0;
-    for (int j = 0; j < per; ++j) acc[j] += xv * mr[j];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      float m = mr[j];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) acc[a][j] += xv[a] * m;
+    }
   }
-  int row = r0 + r;
-  if (row >= V) return;
-  for (int j = 0; j < per; ++j) {
-    int c = c0 + j;
-    float q = acc[j] + (bias ? bias[c] : 0.f);
-    if (Q) Q[(long long)row * N + c] = q;
-    float y = relu ? fmaxf(q, 0.f) : q;
-    if (R1) y += R1[(long long)row * ldr1 + c];
-    if (R2) y += R2[(long long)row * ldr2 + c];
-    Y[(long long)row * N + c] = y;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    int row = r0 + r + a;
+    if (row >= V) continue;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      int c = c0 + j;
+      float q = acc[a][j] + (bias ? bias[c] : 0.f);
+      if (Q) Q[(long long)row * N + c] = q;
+      float y = relu ? fmaxf(q, 0.f) : q;
+      if (R1) y += R1[(long long)row * ldr1 + c];
+      if (R2) y += R2[(long long)row * ldr2 + c];
+      Y[(long long)row * N + c] = y;
+    }
   }
 }
 
@@ -296,7 +314,7 @@ __global__ void k_dec_fwd(LsView s, const float* h, const float* Ef, const float
 }
 
 // S on the static pattern (see learned.cuh); one thread per row.
-__global__ void k_build_S(LsView s, const float* zv, const float* ab, float* S) {
+__global__ void k_build_S(LsView s, const float* zv, const float* ab, float* S, float* S_sell) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.V) return;
   float D[9];
@@ -321,8 +339,12 @@ __global__ void k_build_S(LsView s, const float* zv, const float* ab, float* S) 
         for (int q = 0; q < 3; ++q) D[3 * r + q] += b2 * (A[3 * r] * A[3 * q] + A[3 * r + 1] * A[3 * q + 1] + A[3 * r + 2] * A[3 * q + 2]);
     }
     for (int q = 0; q < 9; ++q) S[9ll * k + q] = c * A[q];
+    if (S_sell) for (int q = 0; q < 9; ++q) S_sell[s.sell_base[k] + 32 * q] = c * A[q];
   }
-  if (kd >= 0) for (int q = 0; q < 9; ++q) S[9ll * kd + q] = D[q];
+  if (kd >= 0) {
+    for (int q = 0; q < 9; ++q) S[9ll * kd + q] = D[q];
+    if (S_sell) for (int q = 0; q < 9; ++q) S_sell[s.sell_base[kd] + 32 * q] = D[q];
+  }
 }
 
 // ------------------------------------------------------- training loss
@@ -501,12 +523,14 @@ void gemm(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 32 && !(attr & (1u << dev))) {
-    cudaFuncSetAttribute(k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_gemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_gemm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     attr |= 1u << dev;
   }
   int K = K1 + K2;
-  size_t smem = sizeof(float) * (size_t(K) * N + 32 * (K + 1));
-  k_gemm<<<nblk(V, 32), TPB, smem, s>>>(V, X1, ld1, K1, X2, ld2, K2, M, N, bias, R1, ldr1, R2, ldr2, Q, Y, relu);
+  size_t smem = sizeof(float) * (size_t(K) * N + 64 * (K + 1));
+  if (N == 64) k_gemm<64><<<nblk(V, 64), TPB, smem, s>>>(V, X1, ld1, K1, X2, ld2, K2, M, bias, R1, ldr1, R2, ldr2, Q, Y, relu);
+  else k_gemm<128><<<nblk(V, 64), TPB, smem, s>>>(V, X1, ld1, K1, X2, ld2, K2, M, bias, R1, ldr1, R2, ldr2, Q, Y, relu);
 }
 void reduce(const float* part, int off, int n, float* out, cudaStream_t s) {
   k_reduce_parts<<<nblk(n), TPB, 0, s>>>(part, GRID, off, n, out, 0);
@@ -546,7 +570,7 @@ void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cud
   k_net_transpose<<<nblk(WT_SIZE), TPB, 0, s>>>(n.wq, n.wt);
 }
 
-void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, cudaStream_t st) {
+void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st) {
   const int V = s.V;
   if (V == 0) return;
   const float* wq = n.wq;
@@ -562,17 +586,17 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
     gemm(V, w.h[l], H, H, w.m[l], H, H, T + WT_W, H, L + L_B, w.h[l], H, nullptr, 0, w.q[l], w.h[l + 1], 1, st);
   }
   k_dec_fwd<<<wgrid, TPB, 0, st>>>(s, w.h[NL], w.Ef, wq, w.zv, w.ab);
-  k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S);
+  k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S, S_sell);
 }
 
-void learned_build_S(const LsView& s, const LearnedWork& w, float* S, cudaStream_t st) {
-  if (s.V) k_build_S<<<nblk(s.V), TPB, 0, st>>>(s, w.zv, w.ab, S);
+void learned_build_S(const LsView& s, const LearnedWork& w, float* S, float* S_sell, cudaStream_t st) {
+  if (s.V) k_build_S<<<nblk(s.V), TPB, 0, st>>>(s, w.zv, w.ab, S, S_sell);
 }
 
 void learned_loss(const LsView& s, const NetDev& n, LearnedWork& w, float* S, const float* probes, const double* pnorm, int P,
                   float* Y, float* Wv, double* loss_parts, double* loss_out, float* grad, cudaStream_t st) {
   const int V = s.V;
-  learned_forward(s, n, w, S, st);
+  learned_forward(s, n, w, S, nullptr, st);
   const int wgrid = nblk(32ll * V);
   for (int p = 0; p < P; ++p) {
     k_spmv<<<wgrid, TPB, 0, st>>>(V, s.rowptr, s.cols, S, nullptr, nullptr, nullptr, nullptr, probes + 3ll * V * p, Y + 3ll * V * p);

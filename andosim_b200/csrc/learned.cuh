@@ -46,6 +46,7 @@ constexpr float DELTA_MIN = 1e-4f;       // delta_i = softplus(z_i) + DELTA_MIN
 struct LsView {
   int V, nnzb;
   const int* rowptr; const int* cols; const int* slot_row; const int* slot_T;
+  const int* sell_base;         // SELL-32 position of each static slot (writes of S in the PCG layout); may be null
   const float* valh;
   const int* xbegin; const int* xend; const int* xcols; const float* xvalh;  // null when no extra blocks
   const float* Lf;              // 6V packed Cholesky factor of the unscaled diagonal blocks
@@ -81,12 +82,13 @@ void net_dev_carve(NetDev& n, float* base);
 // Round master weights to BF16 into n.wq (and bf16 storage) and build n.wt.
 void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cudaStream_t s);
 
-// Inference: features, network, S (9 floats per static slot).
-void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, cudaStream_t st);
+// Inference: features, network, S (9 floats per static slot; with S_sell also
+// in the SELL-32 layout of the PCG).
+void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st);
 
 // S from the coefficients of the last forward (w.zv, w.ab) and the current
 // A^: the network output reused while A^ changes; still SPD by construction.
-void learned_build_S(const LsView& s, const LearnedWork& w, float* S, cudaStream_t st);
+void learned_build_S(const LsView& s, const LearnedWork& w, float* S, float* S_sell, cudaStream_t st);
 
 // Training loss of one system: P probe vectors r_p (3V each) with energy
 // norms n_p = r_p^T A^-1 r_p; loss = mean_p (1 + (y^T A y - 2 r^T y) / n_p),

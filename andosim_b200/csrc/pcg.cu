@@ -208,47 +208,46 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg(PcgArgs a) {
 //
 // LEARNED: z = S r with S a symmetric positive definite block matrix on the
 // static pattern (the learned approximate inverse of A^). Phase B then is a
-// second warp-per-row product; it gathers r - alpha Ap from the neighbours, so
+// second row product; it gathers r - alpha Ap from the neighbours, so
 // the iteration still needs only two grid barriers (r ping-pongs between two
 // buffers because neighbours read the old values). r^T z <= 0 (S lost
 // definiteness) or no new best residual for `stall_window` iterations ends
 // the solve with PCG_PRECOND / PCG_STALL, and the caller redoes it with
 // block-Jacobi.
 
-// One warp computes y = (M v)_row over the static segment (and the extra
-// segment when given); lanes (comp = lane / 8, bi = lane % 8) cover 8 blocks x
-// 3 block rows per pass. vec(j, q) yields the gathered vector at column j.
+// Sliced-ELL layout of the static pattern (SELL-32): rows in chunks of 32,
+// chunk c holding W_c = (chunk_off[c+1] - chunk_off[c]) / 32 block slots per
+// row; slot k of row lane l sits at block index chunk_off[c] + 32 k + l, its
+// column in sell_col (-1 pads a short row) and its 9 values at
+// 9 (chunk_off[c] + 32 k) + 32 q + l, q = 0..8. One thread per block row: a
+// warp's 32 rows read every value and column load as one coalesced 128-byte
+// line, and 32 rows' gathers are in flight at once.
 template <class Vec>
-__device__ inline void warp_row(int row, const int* rowptr, const int* cols, const float* val, const int* xbegin, const int* xend,
-                                const int* xcols, const float* xval, const Vec& vec, int lane, float& y0, float& y1, float& y2) {
-  const int comp = lane >> 3, bi = lane & 7;
-  float acc = 0.f;
-  int s0 = rowptr[row], s1 = rowptr[row + 1];
-  for (int k0 = s0; k0 < s1; k0 += 8) {
-    int k = k0 + bi;
-    if (comp < 3 && k < s1) {
-      int col = cols[k];
-      const float* h = val + 9 * (long long)k + 3 * comp;
-      float q0, q1, q2; vec(col, q0, q1, q2);
-      acc += h[0] * q0 + h[1] * q1 + h[2] * q2;
-    }
+__device__ inline void sell_row(int row, const int* chunk_off, const int* sell_col, const float* val, const int* xbegin, const int* xend,
+                                const int* xcols, const float* xval, const Vec& vec, float& y0, float& y1, float& y2) {
+  const int c = row >> 5, l = row & 31;
+  const int b0 = chunk_off[c], w = (chunk_off[c + 1] - b0) >> 5;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  for (int k = 0; k < w; ++k) {
+    const int slot = b0 + 32 * k;
+    const int col = sell_col[slot + l];
+    if (col < 0) continue;
+    const float* h = val + 9ll * slot + l;
+    float q0, q1, q2; vec(col, q0, q1, q2);
+    a0 += h[0] * q0 + h[32] * q1 + h[64] * q2;
+    a1 += h[96] * q0 + h[128] * q1 + h[160] * q2;
+    a2 += h[192] * q0 + h[224] * q1 + h[256] * q2;
   }
   if (xbegin) {
-    int e0 = xbegin[row], e1 = xend[row];
-    for (int k0 = e0; k0 < e1; k0 += 8) {
-      int k = k0 + bi;
-      if (comp < 3 && k < e1) {
-        int col = xcols[k];
-        const float* h = xval + 9 * (long long)k + 3 * comp;
-        float q0, q1, q2; vec(col, q0, q1, q2);
-        acc += h[0] * q0 + h[1] * q1 + h[2] * q2;
-      }
+    for (int e = xbegin[row]; e < xend[row]; ++e) {
+      const float* h = xval + 9ll * e;
+      float q0, q1, q2; vec(xcols[e], q0, q1, q2);
+      a0 += h[0] * q0 + h[1] * q1 + h[2] * q2;
+      a1 += h[3] * q0 + h[4] * q1 + h[5] * q2;
+      a2 += h[6] * q0 + h[7] * q1 + h[8] * q2;
     }
   }
-  acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-  acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-  acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-  y0 = __shfl_sync(0xffffffffu, acc, 0); y1 = __shfl_sync(0xffffffffu, acc, 8); y2 = __shfl_sync(0xffffffffu, acc, 16);
+  y0 = a0; y1 = a1; y2 = a2;
 }
 
 // |L_i r_i|_inf with L lower triangular (FP32, packed l00 l10 l11 l20 l21 l22).
@@ -283,7 +282,6 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
   const int V = a.V;
   const unsigned nb = gridDim.x;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
-  const int lane = threadIdx.x & 31, gwarp = tid >> 5, nwarps = nthreads >> 5;
   double* part_pap = a.partials;
   double* part_rz = a.partials + nb;
   double* part_rinf = a.partials + 2 * nb;
@@ -306,13 +304,11 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
   }
   if (LEARNED) {
     GatherV gb{a.bhat};
-    for (int row = gwarp; row < V; row += nwarps) {
+    for (int row = tid; row < V; row += nthreads) {
       float y0, y1, y2;
-      warp_row(row, a.rowptr, a.cols, a.S, nullptr, nullptr, nullptr, nullptr, gb, lane, y0, y1, y2);
-      if (lane == 0) {
-        a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
-        rz_loc += double(a.bhat[3 * row]) * y0 + double(a.bhat[3 * row + 1]) * y1 + double(a.bhat[3 * row + 2]) * y2;
-      }
+      sell_row(row, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, gb, y0, y1, y2);
+      a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
+      rz_loc += double(a.bhat[3 * row]) * y0 + double(a.bhat[3 * row + 1]) * y1 + double(a.bhat[3 * row + 2]) * y2;
     }
   }
   rz_loc = block_sum(rz_loc, sh);
@@ -337,15 +333,13 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
     // ---- phase A: p_new = z + beta p_old, Ap = A^ p_new, p^T Ap
     double pap_loc = 0.0;
     GatherP gp{zsrc, pold, beta, first};
-    for (int row = gwarp; row < V; row += nwarps) {
+    for (int row = tid; row < V; row += nthreads) {
       float y0, y1, y2;
-      warp_row(row, a.rowptr, a.cols, a.valh, a.xbegin, a.xend, a.xcols, a.xvalh, gp, lane, y0, y1, y2);
-      if (lane == 0) {
-        float q0, q1, q2; gp(row, q0, q1, q2);
-        pnew[3 * row] = q0; pnew[3 * row + 1] = q1; pnew[3 * row + 2] = q2;
-        a.Ap[3 * row] = y0; a.Ap[3 * row + 1] = y1; a.Ap[3 * row + 2] = y2;
-        pap_loc += double(q0) * y0 + double(q1) * y1 + double(q2) * y2;
-      }
+      sell_row(row, a.chunk_off, a.sell_col, a.valh, a.xbegin, a.xend, a.xcols, a.xvalh, gp, y0, y1, y2);
+      float q0, q1, q2; gp(row, q0, q1, q2);
+      pnew[3 * row] = q0; pnew[3 * row + 1] = q1; pnew[3 * row + 2] = q2;
+      a.Ap[3 * row] = y0; a.Ap[3 * row + 1] = y1; a.Ap[3 * row + 2] = y2;
+      pap_loc += double(q0) * y0 + double(q1) * y1 + double(q2) * y2;
     }
     pap_loc = block_sum(pap_loc, sh);
     if (threadIdx.x == 0) part_pap[blockIdx.x] = pap_loc;
@@ -377,18 +371,16 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
       }
     } else {
       GatherR gr{r, a.Ap, alpha};
-      for (int row = gwarp; row < V; row += nwarps) {
+      for (int row = tid; row < V; row += nthreads) {
         float y0, y1, y2;
-        warp_row(row, a.rowptr, a.cols, a.S, nullptr, nullptr, nullptr, nullptr, gr, lane, y0, y1, y2);
-        if (lane == 0) {
-          float r0, r1, r2; gr(row, r0, r1, r2);
-          a.xh[3 * row] += double(alpha) * pnew[3 * row]; a.xh[3 * row + 1] += double(alpha) * pnew[3 * row + 1];
-          a.xh[3 * row + 2] += double(alpha) * pnew[3 * row + 2];
-          rn[3 * row] = r0; rn[3 * row + 1] = r1; rn[3 * row + 2] = r2;
-          a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
-          rz_new_loc += double(r0) * y0 + double(r1) * y1 + double(r2) * y2;
-          rinf_loc = fmax(rinf_loc, unscaled_inf(a.Lf, row, r0, r1, r2));
-        }
+        sell_row(row, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, gr, y0, y1, y2);
+        float r0, r1, r2; gr(row, r0, r1, r2);
+        a.xh[3 * row] += double(alpha) * pnew[3 * row]; a.xh[3 * row + 1] += double(alpha) * pnew[3 * row + 1];
+        a.xh[3 * row + 2] += double(alpha) * pnew[3 * row + 2];
+        rn[3 * row] = r0; rn[3 * row + 1] = r1; rn[3 * row + 2] = r2;
+        a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
+        rz_new_loc += double(r0) * y0 + double(r1) * y1 + double(r2) * y2;
+        rinf_loc = fmax(rinf_loc, unscaled_inf(a.Lf, row, r0, r1, r2));
       }
     }
     rz_new_loc = block_sum(rz_new_loc, sh);
@@ -454,10 +446,8 @@ int pcg_scaled_grid_size(int device, bool learned) {
 }
 
 cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, int grid, cudaStream_t s) {
-  // both phases of a learned iteration (and phase A of block Jacobi) are
-  // warp-per-row products: enough CTAs for about 4 rows per warp, up to the
-  // co-resident grid
-  int need = (a.V + 4 * PCG_WARPS - 1) / (4 * PCG_WARPS);
+  // one thread per block row, up to the co-resident grid
+  int need = (a.V + PCG_TPB - 1) / PCG_TPB;
   if (need < 1) need = 1;
   if (grid > need) grid = need;
   void* args[] = {(void*)&a};

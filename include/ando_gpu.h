@@ -144,7 +144,8 @@ typedef enum {
   ANDO_PHASE_PCG = 4,          /* persistent PCG solve */
   ANDO_PHASE_LINE_SEARCH = 5,  /* feasibility masks and position update */
   ANDO_PHASE_FINISH = 6,       /* velocity update, restitution, rigid coupling, gravity */
-  ANDO_PHASE_COUNT = 7
+  ANDO_PHASE_PRECOND = 7,      /* learned preconditioner: features, network, S */
+  ANDO_PHASE_COUNT = 8
 } ando_phase;
 
 typedef struct {
