@@ -203,39 +203,57 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, in
       if (pad > 0.f) for (int k = 0; k < 3; ++k) { qb.lo[k] -= pad; qb.hi[k] += pad; }
     }
   }
-  // Depth-first with an explicit stack. With unique 64-bit keys the hierarchy
-  // is at most 64 levels deep, so 96 slots never overflow; an overflow would
-  // be reported through count[1] instead of dropping candidates silently.
+  // Depth-first traversal that tests both children of a node before
+  // descending (Karras 2012): an overlapping leaf child is reported at once,
+  // an overlapping internal child is entered, and the second of two
+  // overlapping internal children goes on the stack. With unique 64-bit keys
+  // the hierarchy is at most 64 levels deep, so 96 slots never overflow; an
+  // overflow would be reported through count[1] instead of dropping
+  // candidates silently.
   constexpr int STACK = 96;
   int stack[STACK];
   int sp = 0;
   const int leaf0 = n - 1;          // with one primitive the root (node 0) is its leaf
-  if (active && n > 0) stack[sp++] = 0;
-  while (__any_sync(0xffffffffu, sp > 0)) {
-    bool hit = false;
-    int prim = -1;
-    if (sp > 0) {
-      int node = stack[--sp];
-      bool is_leaf = node >= leaf0;
-      const Box& nb = nodes[node];
-      if (overlap(qb, nb)) {
-        if (is_leaf) {
-          prim = order[node - leaf0];
-          if (kind == 0) {
-            hit = prims[3 * prim] != q && prims[3 * prim + 1] != q && prims[3 * prim + 2] != q;
-          } else {
-            int pa = prims[2 * prim], pc = prims[2 * prim + 1];
-            hit = q < prim && pa != qa && pa != qc && pc != qa && pc != qc;
-          }
-        } else if (sp <= STACK - 2) {
-          stack[sp++] = left[node];
-          stack[sp++] = right[node];
-        } else {
-          atomicAdd(count + 1, 1);
+  int node = -1;
+  bool single = false;              // n == 1: test the root leaf once
+  if (active && n > 0) {
+    if (n == 1) single = true;
+    else if (overlap(qb, nodes[0])) node = 0;
+  }
+  auto accept = [&](int leaf) {
+    int prim = order[leaf - leaf0];
+    bool hit;
+    if (kind == 0) hit = prims[3 * prim] != q && prims[3 * prim + 1] != q && prims[3 * prim + 2] != q;
+    else {
+      int pa = prims[2 * prim], pc = prims[2 * prim + 1];
+      hit = q < prim && pa != qa && pa != qc && pc != qa && pc != qc;
+    }
+    return hit ? prim : -1;
+  };
+  if (__any_sync(0xffffffffu, single)) {
+    int prim = single && overlap(qb, nodes[0]) ? accept(0) : -1;
+    emit(prim >= 0, q, prim, out, count, cap);
+  }
+  while (__any_sync(0xffffffffu, node >= 0)) {
+    int hl = -1, hr = -1;
+    if (node >= 0) {
+      int l = left[node], r = right[node];
+      bool ol = overlap(qb, nodes[l]), orr = overlap(qb, nodes[r]);
+      bool ll = l >= leaf0, lr = r >= leaf0;
+      if (ol && ll) hl = accept(l);
+      if (orr && lr) hr = accept(r);
+      bool tl = ol && !ll, tr = orr && !lr;
+      if (!tl && !tr) node = sp > 0 ? stack[--sp] : -1;
+      else {
+        node = tl ? l : r;
+        if (tl && tr) {
+          if (sp < STACK) stack[sp++] = r;
+          else atomicAdd(count + 1, 1);
         }
       }
     }
-    emit(hit, q, prim, out, count, cap);
+    emit(hl >= 0, q, hl, out, count, cap);
+    emit(hr >= 0, q, hr, out, count, cap);
   }
 }
 

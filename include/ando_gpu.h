@@ -41,8 +41,11 @@ typedef enum {
 
 /* Step semantics. REFERENCE reproduces the reference step exactly, including
  * its documented quirks (elastic gradient on the rest mesh, repelling pins,
- * literal BVH broad phase, frozen contact gaps, sampled CCD). CORRECTED is
- * reserved for the physically corrected variant. */
+ * literal BVH broad phase, frozen contact gaps, sampled CCD). CORRECTED runs
+ * the step the reference intends: elastic gradient at the current positions,
+ * attracting pins, contact gaps re-evaluated per Newton iteration, conservative
+ * time of impact, the block-scaled PCG, each step restarting from the last
+ * step's end (ando_state_set_start) with v = (x - x_start) / dt. */
 typedef enum { ANDO_SEMANTICS_REFERENCE = 0, ANDO_SEMANTICS_CORRECTED = 1 } ando_semantics;
 
 /* Preconditioner of the PCG inner solve. */
