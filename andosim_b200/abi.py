@@ -153,6 +153,8 @@ def lib() -> C.CDLL:
     L.ando_profile_enable.restype = I32; L.ando_profile_enable.argtypes = [P, I32]
     L.ando_profile_read.restype = I32; L.ando_profile_read.argtypes = [P, C.POINTER(Profile)]
     L.ando_ctx_stream.restype = I32; L.ando_ctx_stream.argtypes = [P, C.POINTER(C.c_void_p)]
+    L.ando_ctx_select_pcg_shape.restype = I32; L.ando_ctx_select_pcg_shape.argtypes = [P, I32, I32]
+    L.ando_ctx_pcg_shape.restype = I32; L.ando_ctx_pcg_shape.argtypes = [P, I32, pi, pi, pd]
     L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
     pu8 = C.POINTER(C.c_ubyte)
     L.ando_precond_num_params.restype = I32
@@ -380,6 +382,15 @@ class Scene:
         sp = C.c_void_p()
         _check(lib().ando_ctx_stream(self.ctx, C.byref(sp)), "ando_ctx_stream")
         return sp.value or 0
+
+    def select_pcg_shape(self, learned: bool, index: int = -1):
+        """Fix scaled-PCG launch candidate `index` (-1: autotune on the next first solve)."""
+        _check(lib().ando_ctx_select_pcg_shape(self.ctx, 1 if learned else 0, index), "ando_ctx_select_pcg_shape")
+
+    def pcg_shape(self, learned: bool) -> dict:
+        n = C.c_int32(); sh = (C.c_int32 * 3)(); t = C.c_double()
+        _check(lib().ando_ctx_pcg_shape(self.ctx, 1 if learned else 0, C.byref(n), sh, C.byref(t)), "ando_ctx_pcg_shape")
+        return dict(candidates=n.value, tpb=sh[0], grid=sh[1], unroll=sh[2], tune_ms=t.value)
 
     def set_precond_weights(self, w: np.ndarray):
         w = np.ascontiguousarray(w, dtype=np.float32)

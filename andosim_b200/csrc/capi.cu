@@ -82,7 +82,12 @@ struct ando_ctx_s {
   DevBuf<double> Linv, xh;
   DevBuf<float> Lf, bhat, valh, xvalh, r2;
   DevBuf<unsigned char> chol_ok;
-  int pcg_scaled_grid = 1, pcg_learned_grid = 1;
+  DevBuf<double> spart;            // per-slice partials of the scaled PCG
+  double tune_ms = 0.0;            // device time spent timing launch shapes
+  // launch shape of the scaled PCG per preconditioner kind (0 Jacobi, 1 learned):
+  // autotuned on the first solve of a mesh (choice < 0) or a fixed candidate
+  PcgShape shape[2];
+  int shape_V[2] = {-1, -1}, shape_choice[2] = {-1, -1};
   double dt2inv = 0.0;             // of the last assembled system
   double gap_max = 1e-3;           // contact activation distance of the current step
 
@@ -104,7 +109,7 @@ struct ando_ctx_s {
 
   // contacts
   DevBuf<int> det_counts, det_offsets;
-  DevBuf<ContactDev> contacts, contacts_all;
+  DevBuf<ContactDev> contacts;
   int ncontacts = 0, n_pe = 0;
   int* ctrl_host_count = nullptr;  // pinned int for small device -> host counts
   DevBuf<int> ekeys, ekeys_sorted, ebegin, eend, xflags, xkeys, xcols, xbegin, xend, nsel;
@@ -217,9 +222,6 @@ struct ando_ctx_s {
 };
 
 namespace {
-struct ActiveContact {
-  __device__ bool operator()(const ContactDev& c) const { return c.type >= 0; }
-};
 
 // Times the launches issued while it is alive (one phase) and counts them.
 struct Phase {
@@ -488,9 +490,11 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
     Phase ph(c, ANDO_PHASE_SETUP);
     long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
     CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
-    CK(c->bvh_tri.query(c->x.p, nullptr, 0, nullptr, c->V, float(gap_max), c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
+    CK(c->bvh_tri.query_contacts(c->x.p, 0, nullptr, c->V, float(gap_max), gap_max, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount,
+                                 c->cub_tmp, &nvt, s));
     CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
-    CK(c->bvh_edge.query(c->x.p, nullptr, 1, c->edges.p, c->E, float(gap_max), c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
+    CK(c->bvh_edge.query_contacts(c->x.p, 1, c->edges.p, c->E, float(gap_max), gap_max, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1,
+                                  c->pcount, c->cub_tmp, &nee, s));
     ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   }
   int nr = 0;
@@ -500,24 +504,15 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
     if (rc) return rc;
     nr = c->ncontacts;
   }
-  // Candidate pairs become contacts; only those inside the activation
-  // distance carry a barrier term, so the rest are dropped here (stable
-  // compaction keeps the candidates' sorted order).
-  int na = 0;
+  // The queries ran the narrow phase at their leaves and kept only pairs
+  // inside the activation distance, sorted by (query, primitive): every one
+  // becomes a contact, vertex-triangle first.
+  const int na = nvt + nee;
   CK(c->contacts.reserve(size_t(nvt) + nee + nr + 1));
   if (nvt + nee) {
     Phase ph(c, ANDO_PHASE_SETUP);
-    CK(c->contacts_all.reserve(size_t(nvt) + nee));
-    CK(c->nsel.reserve(1));
-    launch_pairs_to_contacts(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, gap_max, c->contacts_all.p, s);
-    size_t bytes = 0;
-    CK(cub::DeviceSelect::If(nullptr, bytes, c->contacts_all.p, c->contacts.p, c->nsel.p, nvt + nee, ActiveContact(), s));
-    CK(c->cub_reserve(bytes));
-    CK(cub::DeviceSelect::If(c->cub_tmp.p, bytes, c->contacts_all.p, c->contacts.p, c->nsel.p, nvt + nee, ActiveContact(), s));
-    CK(cudaMemcpyAsync(c->ctrl_host_count, c->nsel.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    na = *c->ctrl_host_count;
-    ph.launched(2);
+    launch_pairs_to_contacts(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, gap_max, c->contacts.p, s);
+    ph.launched();
   }
   if (nb > 0 && nr) {
     MeshDev m = c->mesh_dev();
@@ -540,14 +535,12 @@ int corrected_line_search(ando_ctx c, int nb) {
   launch_toi_reset(c->toi.p, s);
   launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
   ph.launched(2 + (c->num_walls ? 1 : 0));
-  int nvt = 0, nee = 0;
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
   CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query(c->x.p, c->x1.p, 0, nullptr, c->V, 0.f, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.0, 1e-3 * c->gap_max, c->toi.p, s));
   CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query(c->x.p, c->x1.p, 1, c->edges.p, c->E, 0.f, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.0, 1e-3 * c->gap_max, c->toi.p, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
-  if (nvt + nee) { launch_toi_pairs(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, c->ext.p, 0.0, 1e-3 * c->gap_max, c->toi.p, s); ph.launched(); }
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
   launch_update_toi(c->V, c->x.p, c->ext.p, 1.25, c->fixed.p, c->ctrl.p, c->toi.p, s);
   ph.launched();
@@ -604,7 +597,7 @@ PcgScaledArgs scaled_args(ando_ctx c, const ando_params& p) {
   a.xbegin = c->nx ? c->xbegin.p : nullptr; a.xend = c->nx ? c->xend.p : nullptr; a.xcols = c->xcols.p; a.xvalh = c->xvalh.p;
   a.S = nullptr; a.Linv = c->Linv.p; a.Lf = c->Lf.p; a.bhat = c->bhat.p; a.d = c->d.p;
   a.xh = c->xh.p; a.r = c->r.p; a.r2 = c->r2.p; a.z = c->z.p; a.p0 = c->p0.p; a.p1 = c->p1.p; a.Ap = c->Ap.p;
-  a.partials = c->partials.p; a.ctrl = c->ctrl.p; a.tol = float(p.pcg_tol); a.max_iters = p.pcg_max_iters; a.stall_window = 50;
+  a.partials = c->spart.p; a.ctrl = c->ctrl.p; a.tol = float(p.pcg_tol); a.max_iters = p.pcg_max_iters; a.stall_window = 50;
   a.snap_r = nullptr; a.snap_x = nullptr; a.snap_max = 0;
   return a;
 }
@@ -629,6 +622,47 @@ int ensure_learned(ando_ctx c) {
   CK(c->Sval.reserve(9ull * c->nnzb));
   CK(c->S_sell.reserve(9ull * c->sell_blocks));
   return ANDO_OK;
+}
+
+// Launch shape of the scaled PCG for the current mesh. On the first solve
+// of a mesh (autotune on) every candidate runs the solve at hand once more,
+// timed with CUDA events after one untimed round, and the fastest is kept.
+// The solve is a pure function of its inputs and every shape gives the same
+// bits, so the solves run for timing leave exactly the state one solve leaves.
+const PcgShape& pcg_shape(ando_ctx c, bool learned, const PcgScaledArgs& sa) {
+  const int k = learned ? 1 : 0;
+  if (c->shape_V[k] == c->V) return c->shape[k];
+  PcgShape cand[16];
+  int n = pcg_scaled_shapes(c->device, c->V, learned, cand, 16);
+  c->shape[k] = n > 0 ? cand[0] : PcgShape{32, 1, 1};
+  c->shape_V[k] = c->V;
+  if (c->shape_choice[k] >= 0) {
+    if (c->shape_choice[k] < n) c->shape[k] = cand[c->shape_choice[k]];
+    return c->shape[k];
+  }
+  if (n < 2) return c->shape[k];
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return c->shape[k];
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return c->shape[k]; }
+  float best = 1e30f;
+  for (int rep = 0; rep < 2; ++rep) {
+    for (int i = 0; i < n; ++i) {
+      if (rep == 0 && i > 0) break;  // one untimed solve warms the caches
+      cudaEventRecord(e0, c->stream);
+      cudaError_t e = launch_pcg_scaled(sa, learned, cand[i], c->stream);
+      cudaEventRecord(e1, c->stream);
+      float ms = 0.f;
+      if (e != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      c->tune_ms += ms;
+      if (rep == 1 && ms < best) { best = ms; c->shape[k] = cand[i]; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return c->shape[k];
 }
 
 // The scaled PCG of one Newton iteration: learned S when asked for (with
@@ -657,7 +691,7 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
   Phase ph(c, ANDO_PHASE_PCG);
   if (p.precond == ANDO_PRECOND_LEARNED) {
     sa.S = c->S_sell.p;
-    CK(launch_pcg_scaled(sa, true, c->pcg_learned_grid, s));
+    CK(launch_pcg_scaled(sa, true, pcg_shape(c, true, sa), s));
     ph.launched();
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -671,7 +705,7 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
     st.precond_fallbacks++;
     sa.S = nullptr;
   }
-  CK(launch_pcg_scaled(sa, false, c->pcg_scaled_grid, s));
+  CK(launch_pcg_scaled(sa, false, pcg_shape(c, false, sa), s));
   ph.launched();
   return ANDO_OK;
 }
@@ -767,17 +801,12 @@ int apply_pins(ando_ctx c, int nb) {
   launch_toi_reset(c->toi.p, s);
   launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
   ph.launched(2 + (c->num_walls ? 1 : 0));
-  int nvt = 0, nee = 0;
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
   CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query(c->x.p, c->x1.p, 0, nullptr, c->V, 0.f, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nvt, s));
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, s));
   CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query(c->x.p, c->x1.p, 1, c->edges.p, c->E, 0.f, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1, c->pcount, c->cub_tmp, &nee, s));
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
-  if (nvt + nee) {
-    launch_toi_pairs(c->pairs.p, nvt, c->pairs_ee.p, nee, c->tris.p, c->edges.p, c->x.p, c->ext.p, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, s);
-    ph.launched();
-  }
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
   launch_pin_move(c->pin_vertex.p, c->num_pins, c->ext.p, c->toi.p, c->x.p, s);
   ph.launched();
@@ -1061,9 +1090,7 @@ int32_t ando_ctx_create(int32_t device, ando_ctx* out) {
   if (e == cudaSuccess) e = cudaMemset(c->ctrl.p, 0, sizeof(Ctrl));
   if (e != cudaSuccess) { delete c; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
   c->pcg_grid = pcg_grid_size(device);
-  c->pcg_scaled_grid = pcg_scaled_grid_size(device, false);
-  c->pcg_learned_grid = pcg_scaled_grid_size(device, true);
-  e = c->partials.reserve(3ull * std::max(std::max(c->pcg_grid, c->pcg_scaled_grid), std::max(c->pcg_learned_grid, 1)));
+  e = c->partials.reserve(3ull * std::max(c->pcg_grid, 1));
   if (e != cudaSuccess) { delete c; return fail(ANDO_ERR_CUDA, cudaGetErrorString(e)); }
   *out = c;
   return ANDO_OK;
@@ -1159,6 +1186,8 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   }
   cudaStream_t s = c->stream;
   c->V = V; c->T = T; c->nnzb = nnzb;
+  c->shape_V[0] = c->shape_V[1] = -1;
+  CK(c->spart.reserve(pcg_scaled_partials(V)));
   c->S_ready = false;
   c->mu = mat->youngs_modulus / (2.0 * (1.0 + mat->poisson_ratio));
   c->thickness = mat->thickness; c->density = mat->density;
@@ -1582,6 +1611,33 @@ int32_t ando_profile_read(ando_ctx c, ando_profile* out) {
   return ANDO_OK;
 }
 
+int32_t ando_ctx_select_pcg_shape(ando_ctx c, int32_t learned, int32_t index) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (learned < 0 || learned > 1 || index < -1) return fail(ANDO_ERR_INVALID, "shape arguments");
+  c->shape_choice[learned] = index;
+  c->shape_V[learned] = -1;
+  return ANDO_OK;
+}
+
+int32_t ando_ctx_pcg_shape(ando_ctx c, int32_t learned, int32_t* count, int32_t* shape, double* tune_ms) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (learned < 0 || learned > 1) return fail(ANDO_ERR_INVALID, "shape arguments");
+  if (count) {
+    PcgShape cand[16];
+    *count = c->mesh_ready ? pcg_scaled_shapes(c->device, c->V, learned != 0, cand, 16) : 0;
+  }
+  if (shape) {
+    const bool set = c->mesh_ready && c->shape_V[learned] == c->V;
+    shape[0] = set ? c->shape[learned].tpb : 0;
+    shape[1] = set ? c->shape[learned].grid : 0;
+    shape[2] = set ? c->shape[learned].unroll : 0;
+  }
+  if (tune_ms) *tune_ms = c->tune_ms;
+  return ANDO_OK;
+}
+
 int32_t ando_ctx_stream(ando_ctx c, void** stream) {
   if (!c || !stream) return fail(ANDO_ERR_INVALID, "null argument");
   *stream = (void*)c->stream;
@@ -1817,7 +1873,7 @@ int32_t ando_trainer_add_system(ando_trainer t, ando_ctx c, int32_t max_probes, 
   CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (c->ctrl_host->converged) return fail(ANDO_ERR_STATE, "the evaluated Newton system had already converged (nothing was assembled)");
-  CK(launch_pcg_scaled(sa, false, c->pcg_scaled_grid, s));
+  CK(launch_pcg_scaled(sa, false, pcg_shape(c, false, sa), s));
   CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (c->ctrl_host->pcg_status == PCG_TIMEOUT) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");

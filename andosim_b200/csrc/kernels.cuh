@@ -89,8 +89,6 @@ void launch_swept_end(int V, const double* x, const float* d, const unsigned cha
                       double* x1, double* ext, cudaStream_t s);
 void launch_toi_reset(unsigned long long* toi, cudaStream_t s);
 void launch_toi_walls(int V, const double* x, const double* ext, const WallDev* walls, int nw, unsigned long long* toi, cudaStream_t s);
-void launch_toi_pairs(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
-                      const double* ext, double eta_min, double near, unsigned long long* toi, cudaStream_t s);
 void launch_toi_rigid(int V, const double* x, const double* ext, const RigidDev* bodies, int nb, unsigned long long* toi, cudaStream_t s);
 void launch_update_toi(int V, double* x, const double* ext, double scale, const unsigned char* fixed, Ctrl* ctrl,
                        const unsigned long long* toi, cudaStream_t s);
@@ -122,14 +120,18 @@ struct PcgScaledArgs {
   float* d;             // 3V  output: L^-T x^
   double* xh;           // 3V  scaled iterate x^ (FP64)
   float *r, *r2, *z, *p0, *p1, *Ap;
-  double* partials;     // 3 * grid
+  double* partials;     // pcg_scaled_partials(V): three per-slice arrays
   Ctrl* ctrl;
   float tol; int max_iters; int stall_window;
   // block-Jacobi solves only: snapshot k of (r^, x^) after 2^k - 1 iterations, k < snap_max
   float* snap_r; double* snap_x; int snap_max;
 };
-int pcg_scaled_grid_size(int device, bool learned);
-cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, int grid, cudaStream_t s);
+// Launch shape of the scaled PCG (threads per CTA, CTAs, column slots loaded
+// ahead per thread). A tuning knob only: every shape gives the same bits.
+struct PcgShape { int tpb = 0, grid = 0, unroll = 1; };
+size_t pcg_scaled_partials(int V);
+int pcg_scaled_shapes(int device, int V, bool learned, PcgShape* out, int max);
+cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, const PcgShape& sh, cudaStream_t s);
 cudaError_t launch_pcg(const PcgArgs& a, int grid, cudaStream_t s);
 
 }  // namespace ando

@@ -20,6 +20,7 @@
 #include <cub/device/device_reduce.cuh>
 
 #include "lbvh.cuh"
+#include "narrow.cuh"
 
 namespace ando {
 
@@ -103,7 +104,7 @@ __device__ inline int delta(const unsigned long long* k, int n, int i, int j) {
 // Karras 2012: internal node i covers a key range found from the common
 // prefix lengths of its neighbours. Nodes [0, n-1) are internal, leaves are
 // encoded as n-1 + sorted position.
-__global__ void k_karras(const unsigned long long* keys, int n, int* left, int* right, int* parent) {
+__global__ void k_karras(const unsigned long long* keys, int n, int* left, int* right, int* parent, LbvhInner* inner) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -126,18 +127,27 @@ __global__ void k_karras(const unsigned long long* keys, int n, int* left, int* 
   int lc = (lo == gamma) ? (n - 1 + gamma) : gamma;
   int rc = (hi == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
   left[i] = lc; right[i] = rc;
+  inner[i].lc = lc; inner[i].rc = rc;
   parent[lc] = i; parent[rc] = i;
+}
+
+// Copy a finished node box into its parent's packed record.
+__device__ inline void to_parent(LbvhInner* inner, const int* left, int p, int child, const Box& b) {
+  float* dst = left[p] == child ? inner[p].lbox : inner[p].rbox;
+  for (int k = 0; k < 3; ++k) { dst[k] = b.lo[k]; dst[3 + k] = b.hi[k]; }
 }
 
 // Bottom-up refit: the second child to arrive at a node computes its box.
 __global__ void k_refit(const Box* boxes, const int* order, int n, const int* left, const int* right, const int* parent,
-                        Box* nodes, int* arrive) {
+                        Box* nodes, int* arrive, LbvhInner* inner) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int leaf = n - 1 + i;
-  nodes[leaf] = boxes[order[i]];
+  const Box lb = boxes[order[i]];
+  nodes[leaf] = lb;
   if (n == 1) return;
   int p = parent[leaf];
+  to_parent(inner, left, p, leaf, lb);
   while (p >= 0) {
     __threadfence();
     if (atomicAdd(&arrive[p], 1) == 0) return;  // first arrival: the sibling finishes this node
@@ -150,7 +160,9 @@ __global__ void k_refit(const Box* boxes, const int* order, int n, const int* le
     Box u;
     for (int k = 0; k < 3; ++k) { u.lo[k] = fminf(a.lo[k], b.lo[k]); u.hi[k] = fmaxf(a.hi[k], b.hi[k]); }
     nodes[p] = u;
+    const int c = p;
     p = p == 0 ? -1 : parent[p];
+    if (p >= 0) to_parent(inner, left, p, c, u);
   }
 }
 
@@ -173,11 +185,26 @@ __device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, in
   }
 }
 
+// What a query does at an accepted leaf: report the candidate pair
+// (Q_PAIRS); report it only when its FP64 distance at x is below nw.gap
+// (Q_CONTACTS); or fold its conservative time of impact along nw.ext into a
+// per-thread minimum that is min-reduced into *nw.toi (Q_TOI, nothing is
+// written per pair).
+enum QueryMode { Q_PAIRS = 0, Q_CONTACTS = 1, Q_TOI = 2 };
+struct QueryNarrow {
+  double gap = 0.0;
+  const double* ext = nullptr;
+  double eta_min = 0.0, near = 0.0;
+  unsigned long long* toi = nullptr;
+};
+
 // One thread per query. kind 0: query = vertex (point box +-1e-4 inflated by
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
 // prims = edges, keep e1 < e2 without shared vertex.
+template <int MODE>
 __global__ void k_query(const double* x, const double* x1, const int* qprims, int kind, int nq, float pad, const int* prims, int n,
-                        const int* order, const int* left, const int* right, const Box* nodes, int2* out, int* count, int cap) {
+                        const int* order, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap,
+                        QueryNarrow nw) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = q < nq;
   Box qb;
@@ -220,25 +247,40 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, in
     if (n == 1) single = true;
     else if (overlap(qb, nodes[0])) node = 0;
   }
+  double tmin = 1.0;
   auto accept = [&](int leaf) {
     int prim = order[leaf - leaf0];
     bool hit;
-    if (kind == 0) hit = prims[3 * prim] != q && prims[3 * prim + 1] != q && prims[3 * prim + 2] != q;
-    else {
+    int id[4];
+    if (kind == 0) {
+      id[0] = q; id[1] = prims[3 * prim]; id[2] = prims[3 * prim + 1]; id[3] = prims[3 * prim + 2];
+      hit = id[1] != q && id[2] != q && id[3] != q;
+    } else {
       int pa = prims[2 * prim], pc = prims[2 * prim + 1];
+      id[0] = qa; id[1] = qc; id[2] = pa; id[3] = pc;
       hit = q < prim && pa != qa && pa != qc && pc != qa && pc != qc;
+    }
+    if (MODE == Q_CONTACTS && hit) hit = pair_gap(kind, id, x) < nw.gap;
+    if (MODE == Q_TOI && hit) {
+      tmin = fmin(tmin, pair_toi(kind, id, x, nw.ext, nw.eta_min, nw.near));
+      hit = false;
     }
     return hit ? prim : -1;
   };
   if (__any_sync(0xffffffffu, single)) {
     int prim = single && overlap(qb, nodes[0]) ? accept(0) : -1;
-    emit(prim >= 0, q, prim, out, count, cap);
+    if (MODE != Q_TOI) emit(prim >= 0, q, prim, out, count, cap);
   }
   while (__any_sync(0xffffffffu, node >= 0)) {
     int hl = -1, hr = -1;
     if (node >= 0) {
-      int l = left[node], r = right[node];
-      bool ol = overlap(qb, nodes[l]), orr = overlap(qb, nodes[r]);
+      const float4* rec = reinterpret_cast<const float4*>(inner + node);
+      const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
+      Box bl, br;
+      bl.lo[0] = r0.x; bl.lo[1] = r0.y; bl.lo[2] = r0.z; bl.hi[0] = r0.w; bl.hi[1] = r1.x; bl.hi[2] = r1.y;
+      br.lo[0] = r1.z; br.lo[1] = r1.w; br.lo[2] = r2.x; br.hi[0] = r2.y; br.hi[1] = r2.z; br.hi[2] = r2.w;
+      const int l = __float_as_int(r3.x), r = __float_as_int(r3.y);
+      bool ol = overlap(qb, bl), orr = overlap(qb, br);
       bool ll = l >= leaf0, lr = r >= leaf0;
       if (ol && ll) hl = accept(l);
       if (orr && lr) hr = accept(r);
@@ -248,12 +290,18 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, in
         node = tl ? l : r;
         if (tl && tr) {
           if (sp < STACK) stack[sp++] = r;
-          else atomicAdd(count + 1, 1);
+          else if (count) atomicAdd(count + 1, 1);
         }
       }
     }
-    emit(hl >= 0, q, hl, out, count, cap);
-    emit(hr >= 0, q, hr, out, count, cap);
+    if (MODE != Q_TOI) {
+      emit(hl >= 0, q, hl, out, count, cap);
+      emit(hr >= 0, q, hr, out, count, cap);
+    }
+  }
+  if (MODE == Q_TOI) {
+    double t = warp_min(tmin);
+    if ((threadIdx.x & 31) == 0 && t < 1.0) atomic_min_pos(nw.toi, t);
   }
 }
 
@@ -277,6 +325,7 @@ cudaError_t Lbvh::reserve_prims(int n) {
   if ((e = right.reserve(N))) return e;
   if ((e = parent.reserve(2 * N))) return e;
   if ((e = nodes.reserve(2 * N))) return e;
+  if ((e = inner.reserve(N))) return e;
   if ((e = arrive.reserve(N))) return e;
   if ((e = bounds.reserve(6))) return e;
   return cudaSuccess;
@@ -300,10 +349,10 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
   if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, keys.p, keys_sorted.p, idx.p, order.p, n, 0, 64, s))) return e;
   if (n > 1) {
     if ((e = cudaMemsetAsync(parent.p, 0xff, sizeof(int) * (2 * n - 1), s))) return e;
-    k_karras<<<nblk(n - 1), TPB, 0, s>>>(keys_sorted.p, n, left.p, right.p, parent.p);
+    k_karras<<<nblk(n - 1), TPB, 0, s>>>(keys_sorted.p, n, left.p, right.p, parent.p, inner.p);
     if ((e = cudaMemsetAsync(arrive.p, 0, sizeof(int) * n, s))) return e;
   }
-  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p);
+  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p, inner.p);
   launches += n > 1 ? 6 : 5;
   return cudaGetLastError();
 }
@@ -317,7 +366,7 @@ cudaError_t Lbvh::refit(const double* x, const double* x1, float pad, cudaStream
   cudaError_t e;
   k_prim_boxes<<<nblk(n), TPB, 0, s>>>(x, x1, prims, arity, n, pad, boxes.p);
   if (n > 1 && (e = cudaMemsetAsync(arrive.p, 0, sizeof(int) * n, s))) return e;
-  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p);
+  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p, inner.p);
   launches += 2;
   return cudaGetLastError();
 }
@@ -329,21 +378,26 @@ cudaError_t Lbvh::update(const double* x, const double* x1, const int* prims_, i
   return build(x, x1, prims_, arity_, n_, pad, tmp, s);
 }
 
-// Query the hierarchy; returns the sorted (query, primitive) pairs in `out`
-// (capacity grown as needed) and their number in *npairs.
-cudaError_t Lbvh::query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
-                        DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
-                        DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
+namespace {
+// Sorted pairs of a Q_PAIRS or Q_CONTACTS query (capacity grown as needed).
+cudaError_t run_query(Lbvh& B, int mode, const QueryNarrow& nw, const double* x, const double* x1, int kind, const int* qprims, int nq,
+                      float pad, DevBuf<int2>& out, DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0,
+                      DevBuf<unsigned long long>& k1, DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
   cudaError_t e;
   *npairs = 0;
-  if (n == 0 || nq == 0) return cudaSuccess;
+  if (B.n == 0 || nq == 0) return cudaSuccess;
   if ((e = counter.reserve(2))) return e;
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   for (int attempt = 0; attempt < 2; ++attempt) {
     int cap = int(scratch.n);
     if ((e = cudaMemsetAsync(counter.p, 0, 2 * sizeof(int), s))) return e;
-    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, pad, prims, n, order.p, left.p, right.p, nodes.p, scratch.p, counter.p, cap);
-    launches += 1;
+    if (mode == Q_CONTACTS)
+      k_query<Q_CONTACTS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
+                                                   scratch.p, counter.p, cap, nw);
+    else
+      k_query<Q_PAIRS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
+                                                scratch.p, counter.p, cap, nw);
+    B.launches += 1;
     int cnt2[2] = {0, 0};
     if ((e = cudaMemcpyAsync(cnt2, counter.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
@@ -359,11 +413,38 @@ cudaError_t Lbvh::query(const double* x, const double* x1, int kind, const int* 
   if ((e = k1.reserve(m))) return e;
   if ((e = out.reserve(m))) return e;
   k_pair_keys<<<nblk(m), TPB, 0, s>>>(scratch.p, m, k0.p);
-  launches += 1;
+  B.launches += 1;
   size_t bytes = 0;
   if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
   if ((e = tmp.reserve(bytes))) return e;
   if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
+  return cudaGetLastError();
+}
+}  // namespace
+
+// Query the hierarchy; returns the sorted (query, primitive) pairs in `out`
+// (capacity grown as needed) and their number in *npairs.
+cudaError_t Lbvh::query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
+                        DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
+                        DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
+  return run_query(*this, Q_PAIRS, QueryNarrow{}, x, x1, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
+}
+
+cudaError_t Lbvh::query_contacts(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& out,
+                                 DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
+                                 DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
+  QueryNarrow nw;
+  nw.gap = gap;
+  return run_query(*this, Q_CONTACTS, nw, x, nullptr, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
+}
+
+cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, double eta_min,
+                            double near, unsigned long long* toi, cudaStream_t s) {
+  if (n == 0 || nq == 0) return cudaSuccess;
+  QueryNarrow nw;
+  nw.ext = ext; nw.eta_min = eta_min; nw.near = near; nw.toi = toi;
+  k_query<Q_TOI><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, 0.f, prims, n, order.p, inner.p, nodes.p, nullptr, nullptr, 0, nw);
+  launches += 1;
   return cudaGetLastError();
 }
 

@@ -9,6 +9,9 @@
 namespace ando {
 
 struct LbvhBox { float lo[3], hi[3]; };
+// Internal node as the traversal reads it: both children's boxes and indices
+// in one 64-byte record (one dependent load per level instead of two).
+struct alignas(16) LbvhInner { float lbox[6], rbox[6]; int lc, rc, pad_[2]; };
 
 struct Lbvh {
   int n = 0;                    // primitives
@@ -16,6 +19,7 @@ struct Lbvh {
   long long epoch = -1;         // caller's epoch of the last full build (update)
   const int* prims = nullptr;   // arity * n vertex indices (device)
   DevBuf<LbvhBox> boxes, nodes; // primitive boxes; node boxes (internal [0,n-1), leaves [n-1, 2n-1))
+  DevBuf<LbvhInner> inner;      // n-1 internal nodes, child boxes packed (written by the refit)
   DevBuf<unsigned long long> keys, keys_sorted;
   DevBuf<int> idx, order, left, right, parent, arrive, bounds;
   long long launches = 0;
@@ -29,9 +33,21 @@ struct Lbvh {
   cudaError_t update(const double* x, const double* x1, const int* prims, int arity, int n, float pad, long long epoch,
                      DevBuf<unsigned char>& tmp, cudaStream_t s);
   // kind 0: vertices against triangles; kind 1: edges against edges.
+  // Sorted candidate pairs (boxes overlap) in `out`, their number in *npairs.
   cudaError_t query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out, DevBuf<int2>& scratch,
                     DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1, DevBuf<int>& counter,
                     DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
+  // The candidates (boxes at x inflated by pad) whose FP64 distance at x is
+  // below `gap`, sorted: the narrow phase runs at the leaves, so only
+  // contacts are written and sorted.
+  cudaError_t query_contacts(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& out,
+                             DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
+                             DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
+  // min over the swept-box candidates (x -> x1 = x + ext, no pad) of the
+  // pair's conservative time of impact, min-reduced into *toi (IEEE bits of a
+  // non-negative double) on the device: no pair list, no host round trip.
+  cudaError_t query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, double eta_min,
+                        double near, unsigned long long* toi, cudaStream_t s);
 };
 
 }  // namespace ando

@@ -221,34 +221,7 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg(PcgArgs a) {
 // column in sell_col (-1 pads a short row) and its 9 values at
 // 9 (chunk_off[c] + 32 k) + 32 q + l, q = 0..8. One thread per block row: a
 // warp's 32 rows read every value and column load as one coalesced 128-byte
-// line, and 32 rows' gathers are in flight at once.
-template <class Vec>
-__device__ inline void sell_row(int row, const int* chunk_off, const int* sell_col, const float* val, const int* xbegin, const int* xend,
-                                const int* xcols, const float* xval, const Vec& vec, float& y0, float& y1, float& y2) {
-  const int c = row >> 5, l = row & 31;
-  const int b0 = chunk_off[c], w = (chunk_off[c + 1] - b0) >> 5;
-  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-  for (int k = 0; k < w; ++k) {
-    const int slot = b0 + 32 * k;
-    const int col = sell_col[slot + l];
-    if (col < 0) continue;
-    const float* h = val + 9ll * slot + l;
-    float q0, q1, q2; vec(col, q0, q1, q2);
-    a0 += h[0] * q0 + h[32] * q1 + h[64] * q2;
-    a1 += h[96] * q0 + h[128] * q1 + h[160] * q2;
-    a2 += h[192] * q0 + h[224] * q1 + h[256] * q2;
-  }
-  if (xbegin) {
-    for (int e = xbegin[row]; e < xend[row]; ++e) {
-      const float* h = xval + 9ll * e;
-      float q0, q1, q2; vec(xcols[e], q0, q1, q2);
-      a0 += h[0] * q0 + h[1] * q1 + h[2] * q2;
-      a1 += h[3] * q0 + h[4] * q1 + h[5] * q2;
-      a2 += h[6] * q0 + h[7] * q1 + h[8] * q2;
-    }
-  }
-  y0 = a0; y1 = a1; y2 = a2;
-}
+// line, and 32 rows' gathers are in flight at once (sell_row_u below).
 
 // |L_i r_i|_inf with L lower triangular (FP32, packed l00 l10 l11 l20 l21 l22).
 __device__ inline double unscaled_inf(const float* Lf, int i, float r0, float r1, float r2) {
@@ -274,50 +247,150 @@ struct GatherR {  // r - alpha Ap
   }
 };
 
-template <bool LEARNED>
-__global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
+// Fixed-order reductions over per-slice partials. Each warp owns whole
+// 32-row slices and writes one partial per slice (a xor butterfly, whose
+// result is the same in every lane); after the grid barrier every CTA adds
+// the partials in one order that does not depend on the launch shape:
+// s_t = sum_k part[t + 1024 k] for t < 1024, then butterflies over 32 groups
+// of 32. So the tuned launch shape never changes a result bit.
+__device__ inline double warp_sum(double v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ inline double warp_max(double v) {
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+constexpr int RED_T = 1024;
+struct RedSmem { double s[RED_T + 32]; double m[RED_T + 32]; };
+
+// sum of part[0, n) and (with MAX) max of pm[0, n), identical in every CTA
+template <bool MAX>
+__device__ inline void fixed_reduce(const double* part, const double* pm, int n, RedSmem& sh, double& sum, double& mx) {
+  for (int t = threadIdx.x; t < RED_T; t += blockDim.x) {
+    double s = 0.0, m = 0.0;
+    for (int k = t; k < n; k += RED_T) {
+      s += part[k];
+      if (MAX) m = fmax(m, pm[k]);
+    }
+    sh.s[t] = s;
+    if (MAX) sh.m[t] = m;
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int g = w; g < 32; g += nw) {
+    double v = warp_sum(sh.s[32 * g + l]);
+    if (l == 0) sh.s[RED_T + g] = v;
+    if (MAX) {
+      double u = warp_max(sh.m[32 * g + l]);
+      if (l == 0) sh.m[RED_T + g] = u;
+    }
+  }
+  __syncthreads();
+  sum = warp_sum(sh.s[RED_T + l]);
+  mx = MAX ? warp_max(sh.m[RED_T + l]) : 0.0;
+  __syncthreads();  // sh is reused by the next reduction
+}
+
+// a += H q for one 3x3 block (row-major, entries h(e) = h[e * stride]), with
+// the FMA order written out so that every product variant rounds alike.
+template <int STRIDE>
+__device__ inline void block_fma(const float* h, float q0, float q1, float q2, float& a0, float& a1, float& a2) {
+  a0 = __fmaf_rn(h[2 * STRIDE], q2, __fmaf_rn(h[1 * STRIDE], q1, __fmaf_rn(h[0], q0, a0)));
+  a1 = __fmaf_rn(h[5 * STRIDE], q2, __fmaf_rn(h[4 * STRIDE], q1, __fmaf_rn(h[3 * STRIDE], q0, a1)));
+  a2 = __fmaf_rn(h[8 * STRIDE], q2, __fmaf_rn(h[7 * STRIDE], q1, __fmaf_rn(h[6 * STRIDE], q0, a2)));
+}
+
+// One row of the SELL-32 product. U > 1 loads the column indices of U slots
+// ahead of their gathers (more loads in flight per thread, more registers);
+// the sum runs over k = 0, 1, ... with the same FMAs for every U.
+template <int U, class Vec>
+__device__ inline void sell_row_u(int row, const int* chunk_off, const int* sell_col, const float* val, const int* xbegin, const int* xend,
+                                  const int* xcols, const float* xval, const Vec& vec, float& y0, float& y1, float& y2) {
+  const int c = row >> 5, l = row & 31;
+  const int b0 = chunk_off[c], w = (chunk_off[c + 1] - b0) >> 5;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  if (U == 1) {
+    for (int k = 0; k < w; ++k) {
+      const int slot = b0 + 32 * k;
+      const int col = sell_col[slot + l];
+      if (col < 0) continue;
+      float q0, q1, q2; vec(col, q0, q1, q2);
+      block_fma<32>(val + 9ll * slot + l, q0, q1, q2, a0, a1, a2);
+    }
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < w; k += U) {
+      int col[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) col[u] = k + u < w ? sell_col[b0 + 32 * (k + u) + l] : -1;
+      float q[U][3];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (col[u] >= 0) vec(col[u], q[u][0], q[u][1], q[u][2]);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (col[u] >= 0) block_fma<32>(val + 9ll * (b0 + 32 * (k + u)) + l, q[u][0], q[u][1], q[u][2], a0, a1, a2);
+    }
+  }
+  if (xbegin) {
+    for (int e = xbegin[row]; e < xend[row]; ++e) {
+      float q0, q1, q2; vec(xcols[e], q0, q1, q2);
+      block_fma<1>(xval + 9ll * e, q0, q1, q2, a0, a1, a2);
+    }
+  }
+  y0 = a0; y1 = a1; y2 = a2;
+}
+
+constexpr int SCALED_MAX_TPB = 1024;
+
+template <bool LEARNED, int U>
+__global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) {
   Ctrl* ctrl = a.ctrl;
   if (ctrl->converged) return;
-  __shared__ double sh[PCG_WARPS + 1];
-  const int V = a.V;
+  __shared__ RedSmem sh;
+  const int V = a.V, ns = (V + 31) >> 5;
   const unsigned nb = gridDim.x;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, W = (gridDim.x * blockDim.x) >> 5;
   double* part_pap = a.partials;
-  double* part_rz = a.partials + nb;
-  double* part_rinf = a.partials + 2 * nb;
+  double* part_rz = a.partials + ns;
+  double* part_rinf = a.partials + 2 * ns;
   const double binf = __longlong_as_double((long long)ctrl->gnorm_bits);  // max |b| = max |g|
   float* r = a.r;
   float* rn = a.r2;
   const float* zsrc = LEARNED ? a.z : a.r;
+  double dummy;
 
   // init: x^ = 0, r = b^, z = S b^
-  double rz_loc = 0.0;
-  for (int i = tid; i < V; i += nthreads) {
-    float b0 = a.bhat[3 * i], b1 = a.bhat[3 * i + 1], b2 = a.bhat[3 * i + 2];
-    a.xh[3 * i] = 0.0; a.xh[3 * i + 1] = 0.0; a.xh[3 * i + 2] = 0.0;
-    r[3 * i] = b0; r[3 * i + 1] = b1; r[3 * i + 2] = b2;
-    if (!LEARNED) rz_loc += double(b0) * b0 + double(b1) * b1 + double(b2) * b2;
-    if (!LEARNED && a.snap_r && a.snap_max > 0) {
-      a.snap_r[3 * i] = b0; a.snap_r[3 * i + 1] = b1; a.snap_r[3 * i + 2] = b2;
-      a.snap_x[3 * i] = 0.0; a.snap_x[3 * i + 1] = 0.0; a.snap_x[3 * i + 2] = 0.0;
+  for (int sl = gw; sl < ns; sl += W) {
+    const int i = 32 * sl + lane;
+    double rz_loc = 0.0;
+    if (i < V) {
+      float b0 = a.bhat[3 * i], b1 = a.bhat[3 * i + 1], b2 = a.bhat[3 * i + 2];
+      a.xh[3 * i] = 0.0; a.xh[3 * i + 1] = 0.0; a.xh[3 * i + 2] = 0.0;
+      r[3 * i] = b0; r[3 * i + 1] = b1; r[3 * i + 2] = b2;
+      if (LEARNED) {
+        float y0, y1, y2;
+        sell_row_u<U>(i, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, GatherV{a.bhat}, y0, y1, y2);
+        a.z[3 * i] = y0; a.z[3 * i + 1] = y1; a.z[3 * i + 2] = y2;
+        rz_loc = double(b0) * y0 + double(b1) * y1 + double(b2) * y2;
+      } else {
+        rz_loc = double(b0) * b0 + double(b1) * b1 + double(b2) * b2;
+        if (a.snap_r && a.snap_max > 0) {
+          a.snap_r[3 * i] = b0; a.snap_r[3 * i + 1] = b1; a.snap_r[3 * i + 2] = b2;
+          a.snap_x[3 * i] = 0.0; a.snap_x[3 * i + 1] = 0.0; a.snap_x[3 * i + 2] = 0.0;
+        }
+      }
     }
+    rz_loc = warp_sum(rz_loc);
+    if (lane == 0) part_rz[sl] = rz_loc;
   }
-  if (LEARNED) {
-    GatherV gb{a.bhat};
-    for (int row = tid; row < V; row += nthreads) {
-      float y0, y1, y2;
-      sell_row(row, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, gb, y0, y1, y2);
-      a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
-      rz_loc += double(a.bhat[3 * row]) * y0 + double(a.bhat[3 * row + 1]) * y1 + double(a.bhat[3 * row + 2]) * y2;
-    }
-  }
-  rz_loc = block_sum(rz_loc, sh);
-  if (threadIdx.x == 0) part_rz[blockIdx.x] = rz_loc;
   bool ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
   int status = PCG_MAXIT, iters = 0;
-  double rel = 0.0;
+  double rel = 0.0, rz = 0.0;
   if (!ok) status = PCG_TIMEOUT;
-  double rz = ok ? grid_sum(part_rz, nb, sh) : 0.0;
+  else fixed_reduce<false>(part_rz, nullptr, ns, sh, rz, dummy);
   if (ok) {
     rel = binf < 1e-16 ? binf : 1.0;
     if (rel < double(a.tol)) status = PCG_OK;
@@ -331,65 +404,79 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
   int since = 0;
   for (int it = 0; ok && status == PCG_MAXIT && it < a.max_iters; ++it) {
     // ---- phase A: p_new = z + beta p_old, Ap = A^ p_new, p^T Ap
-    double pap_loc = 0.0;
     GatherP gp{zsrc, pold, beta, first};
-    for (int row = tid; row < V; row += nthreads) {
-      float y0, y1, y2;
-      sell_row(row, a.chunk_off, a.sell_col, a.valh, a.xbegin, a.xend, a.xcols, a.xvalh, gp, y0, y1, y2);
-      float q0, q1, q2; gp(row, q0, q1, q2);
-      pnew[3 * row] = q0; pnew[3 * row + 1] = q1; pnew[3 * row + 2] = q2;
-      a.Ap[3 * row] = y0; a.Ap[3 * row + 1] = y1; a.Ap[3 * row + 2] = y2;
-      pap_loc += double(q0) * y0 + double(q1) * y1 + double(q2) * y2;
+    for (int sl = gw; sl < ns; sl += W) {
+      const int row = 32 * sl + lane;
+      double pap_loc = 0.0;
+      if (row < V) {
+        float y0, y1, y2;
+        sell_row_u<U>(row, a.chunk_off, a.sell_col, a.valh, a.xbegin, a.xend, a.xcols, a.xvalh, gp, y0, y1, y2);
+        float q0, q1, q2; gp(row, q0, q1, q2);
+        pnew[3 * row] = q0; pnew[3 * row + 1] = q1; pnew[3 * row + 2] = q2;
+        a.Ap[3 * row] = y0; a.Ap[3 * row + 1] = y1; a.Ap[3 * row + 2] = y2;
+        pap_loc = double(q0) * y0 + double(q1) * y1 + double(q2) * y2;
+      }
+      pap_loc = warp_sum(pap_loc);
+      if (lane == 0) part_pap[sl] = pap_loc;
     }
-    pap_loc = block_sum(pap_loc, sh);
-    if (threadIdx.x == 0) part_pap[blockIdx.x] = pap_loc;
     ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
     if (!ok) { status = PCG_TIMEOUT; break; }
-    double pap = grid_sum(part_pap, nb, sh);
+    double pap;
+    fixed_reduce<false>(part_pap, nullptr, ns, sh, pap, dummy);
     iters = it + 1;
     if (fabs(pap) < 1e-16) { status = PCG_NOT_SPD; break; }
     float alpha = float(rz / pap);
     // ---- phase B: x^ += alpha p, r -= alpha Ap, z = S r, r^T z, |L r|_inf
-    double rz_new_loc = 0.0, rinf_loc = 0.0;
     if (!LEARNED) {
       // snapshot k of (r^, x^) after 2^k - 1 iterations (training probes)
       const int done = it + 1;
       const int snap = (a.snap_r && ((done & (done + 1)) == 0)) ? __ffs(done + 1) - 1 : -1;
       float* sr = (snap >= 0 && snap < a.snap_max) ? a.snap_r + 3ll * V * snap : nullptr;
       double* sx = sr ? a.snap_x + 3ll * V * snap : nullptr;
-      for (int i = tid; i < V; i += nthreads) {
-        float p0 = pnew[3 * i], p1 = pnew[3 * i + 1], p2 = pnew[3 * i + 2];
-        a.xh[3 * i] += double(alpha) * p0; a.xh[3 * i + 1] += double(alpha) * p1; a.xh[3 * i + 2] += double(alpha) * p2;
-        float r0 = r[3 * i] - alpha * a.Ap[3 * i], r1 = r[3 * i + 1] - alpha * a.Ap[3 * i + 1], r2 = r[3 * i + 2] - alpha * a.Ap[3 * i + 2];
-        r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
-        if (sr) {
-          sr[3 * i] = r0; sr[3 * i + 1] = r1; sr[3 * i + 2] = r2;
-          sx[3 * i] = a.xh[3 * i]; sx[3 * i + 1] = a.xh[3 * i + 1]; sx[3 * i + 2] = a.xh[3 * i + 2];
+      for (int sl = gw; sl < ns; sl += W) {
+        const int i = 32 * sl + lane;
+        double rz_new_loc = 0.0, rinf_loc = 0.0;
+        if (i < V) {
+          float p0 = pnew[3 * i], p1 = pnew[3 * i + 1], p2 = pnew[3 * i + 2];
+          a.xh[3 * i] += double(alpha) * p0; a.xh[3 * i + 1] += double(alpha) * p1; a.xh[3 * i + 2] += double(alpha) * p2;
+          float r0 = r[3 * i] - alpha * a.Ap[3 * i], r1 = r[3 * i + 1] - alpha * a.Ap[3 * i + 1], r2 = r[3 * i + 2] - alpha * a.Ap[3 * i + 2];
+          r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
+          if (sr) {
+            sr[3 * i] = r0; sr[3 * i + 1] = r1; sr[3 * i + 2] = r2;
+            sx[3 * i] = a.xh[3 * i]; sx[3 * i + 1] = a.xh[3 * i + 1]; sx[3 * i + 2] = a.xh[3 * i + 2];
+          }
+          rz_new_loc = double(r0) * r0 + double(r1) * r1 + double(r2) * r2;
+          rinf_loc = unscaled_inf(a.Lf, i, r0, r1, r2);
         }
-        rz_new_loc += double(r0) * r0 + double(r1) * r1 + double(r2) * r2;
-        rinf_loc = fmax(rinf_loc, unscaled_inf(a.Lf, i, r0, r1, r2));
+        rz_new_loc = warp_sum(rz_new_loc);
+        rinf_loc = warp_max(rinf_loc);
+        if (lane == 0) { part_rz[sl] = rz_new_loc; part_rinf[sl] = rinf_loc; }
       }
     } else {
       GatherR gr{r, a.Ap, alpha};
-      for (int row = tid; row < V; row += nthreads) {
-        float y0, y1, y2;
-        sell_row(row, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, gr, y0, y1, y2);
-        float r0, r1, r2; gr(row, r0, r1, r2);
-        a.xh[3 * row] += double(alpha) * pnew[3 * row]; a.xh[3 * row + 1] += double(alpha) * pnew[3 * row + 1];
-        a.xh[3 * row + 2] += double(alpha) * pnew[3 * row + 2];
-        rn[3 * row] = r0; rn[3 * row + 1] = r1; rn[3 * row + 2] = r2;
-        a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
-        rz_new_loc += double(r0) * y0 + double(r1) * y1 + double(r2) * y2;
-        rinf_loc = fmax(rinf_loc, unscaled_inf(a.Lf, row, r0, r1, r2));
+      for (int sl = gw; sl < ns; sl += W) {
+        const int row = 32 * sl + lane;
+        double rz_new_loc = 0.0, rinf_loc = 0.0;
+        if (row < V) {
+          float y0, y1, y2;
+          sell_row_u<U>(row, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, gr, y0, y1, y2);
+          float r0, r1, r2; gr(row, r0, r1, r2);
+          a.xh[3 * row] += double(alpha) * pnew[3 * row]; a.xh[3 * row + 1] += double(alpha) * pnew[3 * row + 1];
+          a.xh[3 * row + 2] += double(alpha) * pnew[3 * row + 2];
+          rn[3 * row] = r0; rn[3 * row + 1] = r1; rn[3 * row + 2] = r2;
+          a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
+          rz_new_loc = double(r0) * y0 + double(r1) * y1 + double(r2) * y2;
+          rinf_loc = unscaled_inf(a.Lf, row, r0, r1, r2);
+        }
+        rz_new_loc = warp_sum(rz_new_loc);
+        rinf_loc = warp_max(rinf_loc);
+        if (lane == 0) { part_rz[sl] = rz_new_loc; part_rinf[sl] = rinf_loc; }
       }
     }
-    rz_new_loc = block_sum(rz_new_loc, sh);
-    rinf_loc = block_max(rinf_loc, sh);
-    if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz_new_loc; part_rinf[blockIdx.x] = rinf_loc; }
     ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
     if (!ok) { status = PCG_TIMEOUT; break; }
-    double rz_new = grid_sum(part_rz, nb, sh);
-    double rinf = grid_max(part_rinf, nb, sh);
+    double rz_new, rinf;
+    fixed_reduce<true>(part_rz, part_rinf, ns, sh, rz_new, rinf);
     rel = binf < 1e-16 ? rinf : rinf / binf;
     if (LEARNED) { float* t = r; r = rn; rn = t; }
     if (rel < double(a.tol)) { status = PCG_OK; break; }
@@ -406,7 +493,9 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
   // d = L^-T x^ (every x^ write precedes the last grid barrier); x^ is FP64:
   // rounding it to FP32 would cost up to cond(L_i) x 6e-8 of d_i at stiff vertices
   if (ok) {
-    for (int i = tid; i < V; i += nthreads) {
+    for (int sl = gw; sl < ns; sl += W) {
+      const int i = 32 * sl + lane;
+      if (i >= V) continue;
       const double* q = a.Linv + 6 * (long long)i;
       double x0 = a.xh[3 * i], x1 = a.xh[3 * i + 1], x2 = a.xh[3 * i + 2];
       a.d[3 * i] = float(q[0] * x0 + q[1] * x1 + q[3] * x2);
@@ -422,6 +511,12 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_scaled(PcgScaledArgs a) {
   }
 }
 
+using ScaledKernel = void (*)(PcgScaledArgs);
+ScaledKernel scaled_kernel(bool learned, int unroll) {
+  if (learned) return unroll >= 2 ? k_pcg_scaled<true, 2> : k_pcg_scaled<true, 1>;
+  return unroll >= 2 ? k_pcg_scaled<false, 2> : k_pcg_scaled<false, 1>;
+}
+
 }  // namespace
 
 int pcg_grid_size(int device) {
@@ -434,25 +529,56 @@ int pcg_grid_size(int device) {
   return co < want ? co : want;
 }
 
-int pcg_scaled_grid_size(int device, bool learned) {
-  int sms = 0, per_sm = 0;
+size_t pcg_scaled_partials(int V) { return 3ull * (size_t)((V + 31) / 32 + 1); }
+
+// Candidate launch shapes of the scaled PCG for V rows on `device`; shape 0
+// is the default. Every shape gives the same result bits.
+//  - balanced: the 32-row slices spread evenly over the SMs (one or two
+//    CTAs per SM, each warp one slice per pass);
+//  - fixed CTA sizes of 256 and 512 threads up to the co-resident grid;
+// each with one and two column slots loaded ahead per thread.
+int pcg_scaled_shapes(int device, int V, bool learned, PcgShape* out, int max) {
+  int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  if (learned) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_scaled<true>, PCG_TPB, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_scaled<false>, PCG_TPB, 0);
-  if (per_sm < 1) per_sm = 1;
-  int co = sms * per_sm;
-  int want = 2 * sms;
-  return co < want ? co : want;
+  if (sms < 1) sms = 1;
+  const int ns = (V + 31) / 32 > 0 ? (V + 31) / 32 : 1;
+  int n = 0;
+  auto occ = [&](int unroll, int tpb) {
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, scaled_kernel(learned, unroll), tpb, 0);
+    return per;
+  };
+  for (int unroll = 1; unroll <= 2; ++unroll) {
+    const int wps = (ns + sms - 1) / sms;  // warps needed per SM for one pass
+    int k = (wps + 31) / 32;               // CTAs per SM
+    int tpb = 32 * ((wps + k - 1) / k);
+    while (k > 1 && occ(unroll, tpb) < k) {
+      --k;
+      tpb = 32 * ((wps + k - 1) / k);
+      if (tpb > SCALED_MAX_TPB) { tpb = SCALED_MAX_TPB; break; }
+    }
+    if (tpb > SCALED_MAX_TPB) tpb = SCALED_MAX_TPB;
+    int per = occ(unroll, tpb);
+    if (per >= 1 && n < max) {
+      int grid = (ns + tpb / 32 - 1) / (tpb / 32);
+      if (grid > sms * per) grid = sms * per;
+      out[n++] = PcgShape{tpb, grid, unroll};
+    }
+    for (int t : {256, 512}) {
+      int p = occ(unroll, t);
+      if (p < 1 || n >= max) continue;
+      int grid = (ns + t / 32 - 1) / (t / 32);
+      if (grid > sms * p) grid = sms * p;
+      out[n++] = PcgShape{t, grid, unroll};
+    }
+  }
+  return n;
 }
 
-cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, int grid, cudaStream_t s) {
-  // one thread per block row, up to the co-resident grid
-  int need = (a.V + PCG_TPB - 1) / PCG_TPB;
-  if (need < 1) need = 1;
-  if (grid > need) grid = need;
+cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, const PcgShape& sh, cudaStream_t s) {
+  if (sh.tpb < 32 || sh.tpb > SCALED_MAX_TPB || (sh.tpb & 31) || sh.grid < 1) return cudaErrorInvalidConfiguration;
   void* args[] = {(void*)&a};
-  if (learned) return cudaLaunchCooperativeKernel((void*)k_pcg_scaled<true>, dim3(grid), dim3(PCG_TPB), args, 0, s);
-  return cudaLaunchCooperativeKernel((void*)k_pcg_scaled<false>, dim3(grid), dim3(PCG_TPB), args, 0, s);
+  return cudaLaunchCooperativeKernel((void*)scaled_kernel(learned, sh.unroll), dim3(sh.grid), dim3(sh.tpb), args, 0, s);
 }
 
 cudaError_t launch_pcg(const PcgArgs& a, int grid, cudaStream_t s) {

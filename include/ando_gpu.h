@@ -264,6 +264,18 @@ ANDO_API int32_t ando_broad_phase(ando_ctx ctx, int32_t kind, double pad, int32_
 ANDO_API int32_t ando_profile_enable(ando_ctx ctx, int32_t enable);
 ANDO_API int32_t ando_profile_read(ando_ctx ctx, ando_profile* out);
 
+/* Launch shape of the scaled PCG (CORRECTED semantics) for the current mesh,
+ * per preconditioner (learned = 0: block Jacobi, 1: learned). The candidates
+ * (threads per CTA, CTAs, column slots loaded ahead) all give the same result
+ * bits. By default (index -1) the first solve of a mesh times every candidate
+ * and keeps the fastest; index >= 0 fixes candidate `index`. No reference
+ * counterpart (the reference solves on the CPU). */
+ANDO_API int32_t ando_ctx_select_pcg_shape(ando_ctx ctx, int32_t learned, int32_t index);
+/* Number of candidates for the current mesh and the shape in use
+ * (shape[0..2] = threads per CTA, CTAs, slots ahead; zeros before the first
+ * solve of the mesh). `tune_ms` (may be null): device time spent timing. */
+ANDO_API int32_t ando_ctx_pcg_shape(ando_ctx ctx, int32_t learned, int32_t* count, int32_t* shape, double* tune_ms);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
  * callers that time or order work around the library's. */
 ANDO_API int32_t ando_ctx_stream(ando_ctx ctx, void** stream);
