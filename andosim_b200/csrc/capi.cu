@@ -152,6 +152,7 @@ struct ando_ctx_s {
   // broad phase (the LBVHs are rebuilt once per step, refit in between)
   long long bvh_epoch = 0;
   DevBuf<int> edges;
+  DevBuf<int> vorder, eorder;      // vertices / edges in Morton order of their rest positions (query order)
   int E = 0;
   Lbvh bvh_tri, bvh_edge;
   DevBuf<int2> pairs, pair_scratch;
@@ -241,6 +242,39 @@ struct Phase {
 }  // namespace
 
 namespace {
+
+// Indices of n points sorted by the 63-bit Morton code of their position in
+// the points' bounding box (ties by index).
+std::vector<int> morton_order(const double* p, int n) {
+  std::vector<int> idx(n > 0 ? n : 0);
+  if (n <= 0) return idx;
+  double lo[3] = {p[0], p[1], p[2]}, hi[3] = {p[0], p[1], p[2]};
+  for (int i = 1; i < n; ++i)
+    for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], p[3ull * i + k]); hi[k] = std::max(hi[k], p[3ull * i + k]); }
+  auto spread = [](uint64_t v) {  // 21 bits -> every third bit
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+  };
+  std::vector<std::pair<uint64_t, int>> key(n);
+  for (int i = 0; i < n; ++i) {
+    uint64_t code = 0;
+    for (int k = 0; k < 3; ++k) {
+      double ext = hi[k] - lo[k];
+      double u = ext > 0.0 ? (p[3ull * i + k] - lo[k]) / ext : 0.0;
+      uint64_t q = uint64_t(std::min(std::max(u, 0.0), 1.0) * 2097151.0);
+      code |= spread(q) << k;
+    }
+    key[i] = {code, i};
+  }
+  std::sort(key.begin(), key.end());
+  for (int i = 0; i < n; ++i) idx[i] = key[i].second;
+  return idx;
+}
 
 int check_ctx(ando_ctx c) {
   if (!c) return fail(ANDO_ERR_INVALID, "null context");
@@ -1212,6 +1246,18 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->mesh_x.upload(vertices, 3ull * V, s));
   c->E = int(edges.size() / 2);
   CK(c->edges.upload(edges.data(), edges.size(), s));
+  {
+    // LBVH query order: vertices and edge midpoints sorted by the Morton code
+    // of their rest positions, so a warp's queries are spatial neighbours
+    std::vector<double> mid(3ull * c->E);
+    for (int e = 0; e < c->E; ++e)
+      for (int k = 0; k < 3; ++k) mid[3ull * e + k] = 0.5 * (vertices[3ull * edges[2 * e] + k] + vertices[3ull * edges[2 * e + 1] + k]);
+    std::vector<int> vo = morton_order(vertices, V), eo = morton_order(mid.data(), c->E);
+    CK(c->vorder.upload(vo.data(), V, s));
+    CK(c->eorder.upload(eo.data(), c->E, s));
+    c->bvh_tri.qorder = c->vorder.p;
+    c->bvh_edge.qorder = c->eorder.p;
+  }
   CK(c->el_a.reserve(nnzb)); CK(c->el_b.reserve(nnzb)); CK(c->g_el.reserve(3ull * V));
   // per-vertex / per-slot work buffers
   CK(c->x.reserve(3ull * V)); CK(c->v.reserve(3ull * V)); CK(c->x_prev.reserve(3ull * V)); CK(c->mass.reserve(V));

@@ -202,11 +202,12 @@ struct QueryNarrow {
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
 // prims = edges, keep e1 < e2 without shared vertex.
 template <int MODE>
-__global__ void k_query(const double* x, const double* x1, const int* qprims, int kind, int nq, float pad, const int* prims, int n,
-                        const int* order, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap,
+__global__ void k_query(const double* x, const double* x1, const int* qprims, const int* qorder, int kind, int nq, float pad, const int* prims,
+                        int n, const int* order, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap,
                         QueryNarrow nw) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  bool active = q < nq;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = t < nq;
+  const int q = active && qorder ? qorder[t] : t;
   Box qb;
   int qa = -1, qc = -1;
   if (active) {
@@ -392,10 +393,10 @@ cudaError_t run_query(Lbvh& B, int mode, const QueryNarrow& nw, const double* x,
     int cap = int(scratch.n);
     if ((e = cudaMemsetAsync(counter.p, 0, 2 * sizeof(int), s))) return e;
     if (mode == Q_CONTACTS)
-      k_query<Q_CONTACTS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
+      k_query<Q_CONTACTS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
                                                    scratch.p, counter.p, cap, nw);
     else
-      k_query<Q_PAIRS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
+      k_query<Q_PAIRS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
                                                 scratch.p, counter.p, cap, nw);
     B.launches += 1;
     int cnt2[2] = {0, 0};
@@ -443,7 +444,7 @@ cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext
   if (n == 0 || nq == 0) return cudaSuccess;
   QueryNarrow nw;
   nw.ext = ext; nw.eta_min = eta_min; nw.near = near; nw.toi = toi;
-  k_query<Q_TOI><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, kind, nq, 0.f, prims, n, order.p, inner.p, nodes.p, nullptr, nullptr, 0, nw);
+  k_query<Q_TOI><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, prims, n, order.p, inner.p, nodes.p, nullptr, nullptr, 0, nw);
   launches += 1;
   return cudaGetLastError();
 }

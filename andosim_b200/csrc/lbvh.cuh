@@ -18,6 +18,10 @@ struct Lbvh {
   int arity = 0;
   long long epoch = -1;         // caller's epoch of the last full build (update)
   const int* prims = nullptr;   // arity * n vertex indices (device)
+  // Order in which query threads take their queries (a permutation of the
+  // nq queries, device; null: identity). A spatially coherent order keeps the
+  // 32 traversals of a warp on similar paths; results do not depend on it.
+  const int* qorder = nullptr;
   DevBuf<LbvhBox> boxes, nodes; // primitive boxes; node boxes (internal [0,n-1), leaves [n-1, 2n-1))
   DevBuf<LbvhInner> inner;      // n-1 internal nodes, child boxes packed (written by the refit)
   DevBuf<unsigned long long> keys, keys_sorted;
