@@ -712,7 +712,7 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
     const int refresh = p.precond_refresh > 1 ? p.precond_refresh : 1;
     Phase pn(c, ANDO_PHASE_PRECOND);
     if (!c->coeff_valid || c->coeff_mesh != c->mesh_generation || c->coeff_age >= refresh) {
-      learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, s);
+      learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, s, &c->ctrl.p->tc_err);
       c->coeff_valid = true; c->coeff_mesh = c->mesh_generation; c->coeff_age = 1;
       pn.launched(5 + 3 * net::NL);
     } else {
@@ -730,6 +730,7 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     const Ctrl& h = *c->ctrl_host;
+    if (h.tc_err) return fail(ANDO_ERR_TIMEOUT, "learned preconditioner: a tensor-core layer's wait timed out");
     c->profile.pcg_learned_iterations += h.pcg_iters;
     if (h.converged || h.pcg_status == PCG_OK || h.pcg_status == PCG_TIMEOUT) return ANDO_OK;
     // the learned attempt's iterations count as work done; the caller adds the final solve's
@@ -1757,9 +1758,11 @@ int32_t ando_precond_eval(ando_ctx c) {
   rc = ensure_learned(c);
   if (rc) return rc;
   LsView v = ls_view(c);
-  learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, c->stream);
+  learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, c->stream, &c->ctrl.p->tc_err);
   CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (c->ctrl_host->tc_err) return fail(ANDO_ERR_TIMEOUT, "learned preconditioner: a tensor-core layer's wait timed out");
   c->S_ready = true;
   c->coeff_valid = true; c->coeff_mesh = c->mesh_generation; c->coeff_age = 1;
   return ANDO_OK;

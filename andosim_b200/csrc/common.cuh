@@ -112,7 +112,7 @@ struct Ctrl {
   double alpha;
   int strain_active;
   unsigned int bar_count, bar_gen; int bar_err;
-  int pad;
+  int tc_err;                     // a tensor-core GEMM's bounded wait gave up (sticky)
 };
 
 // PCG_PRECOND: the learned preconditioner lost positive definiteness

@@ -542,13 +542,13 @@ size_t learned_work_floats(int V, int nnzb, bool training) {
   size_t VH = size_t(V) * H;
   size_t n = size_t(V) * FN + size_t(nnzb) * FE + VH * (NL + 1) + 3 * VH * NL + VH + V + 2ull * nnzb;
   if (training) n += 7 * VH + V + 2ull * nnzb + size_t(GRID) * PART;
-  return n;
+  return n + 4 * 64;  // every buffer starts on a 16-byte boundary (vector loads and stores)
 }
 
 void learned_work_carve(LearnedWork& w, float* base, int V, int nnzb, bool training) {
   size_t VH = size_t(V) * H;
   float* p = base;
-  auto take = [&](size_t n) { float* r = p; p += n; return r; };
+  auto take = [&](size_t n) { float* r = p; p += (n + 3) & ~size_t(3); return r; };
   w.V = V; w.nnzb = nnzb; w.training = training; w.base = base;
   w.X = take(size_t(V) * FN); w.Ef = take(size_t(nnzb) * FE);
   for (int l = 0; l <= NL; ++l) w.h[l] = take(VH);
@@ -570,7 +570,7 @@ void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cud
   k_net_transpose<<<nblk(WT_SIZE), TPB, 0, s>>>(n.wq, n.wt);
 }
 
-void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st) {
+void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st, int* err) {
   const int V = s.V;
   if (V == 0) return;
   const float* wq = n.wq;
@@ -580,10 +580,10 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
   const int wgrid = nblk(32ll * V);
   for (int l = 0; l < NL; ++l) {
     const float* L = wq + LAYER0 + l * L_SIZE;
-    const float* T = n.wt + WT_LAYER0 + l * WT_LSIZE;
-    gemm(V, w.h[l], H, H, nullptr, 0, 0, T + WT_U, H, nullptr, nullptr, 0, nullptr, 0, nullptr, w.u[l], 0, st);
+    // u = U h and h' = relu(W [h ; m] + b) + h on the tensor cores
+    launch_gemm_tc(V, w.h[l], H, H, nullptr, 0, 0, L + L_U, nullptr, nullptr, 0, nullptr, w.u[l], 0, err, st);
     k_msg_fwd<<<wgrid, TPB, 0, st>>>(s, w.u[l], w.Ef, L + L_E, L + L_C, w.m[l]);
-    gemm(V, w.h[l], H, H, w.m[l], H, H, T + WT_W, H, L + L_B, w.h[l], H, nullptr, 0, w.q[l], w.h[l + 1], 1, st);
+    launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, L + L_B, w.h[l], H, w.q[l], w.h[l + 1], 1, err, st);
   }
   k_dec_fwd<<<wgrid, TPB, 0, st>>>(s, w.h[NL], w.Ef, wq, w.zv, w.ab);
   k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S, S_sell);

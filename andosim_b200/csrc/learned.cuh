@@ -83,8 +83,17 @@ void net_dev_carve(NetDev& n, float* base);
 void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cudaStream_t s);
 
 // Inference: features, network, S (9 floats per static slot; with S_sell also
-// in the SELL-32 layout of the PCG).
-void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st);
+// in the SELL-32 layout of the PCG). The hidden dense layers run on the
+// tensor cores (tc_gemm.cu); `err` (may be null) is set when one of their
+// bounded waits gives up.
+void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st, int* err = nullptr);
+
+// Tensor-core dense layer (tc_gemm.cu): Y = act(X W^T + bias) + R1 with
+// X = [X1 | X2] (K = K1 + K2 in 16..128, a multiple of 16), W row-major
+// [64][K] BF16-representable, 64 outputs.
+bool gemm_tc_supported(int K1, int K2, int N, int ldr1);
+cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W, const float* bias,
+                           const float* R1, int ldr1, float* Q, float* Y, int relu, int* err, cudaStream_t s);
 
 // S from the coefficients of the last forward (w.zv, w.ab) and the current
 // A^: the network output reused while A^ changes; still SPD by construction.

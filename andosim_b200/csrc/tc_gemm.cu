@@ -1,0 +1,241 @@
+// tc_gemm.cu -- dense layers of the learned preconditioner's forward pass on
+// the 5th-generation tensor cores: tcgen05.mma (kind::f16, BF16 x BF16 with
+// an FP32 accumulator in tensor memory), operands staged in shared memory in
+// the K-major no-swizzle core-matrix layout, one elected thread issuing the
+// MMAs, completion through tcgen05.commit on an mbarrier, epilogue read back
+// with tcgen05.ld.
+//
+// The weights are BF16 values already (the network's master weights are
+// rounded to BF16). The FP32 activations are split exactly into three BF16
+// terms x = hi + mid + lo (8 + 8 + 8 mantissa bits); every BF16 x BF16
+// product is exact in FP32, so the layer keeps FP32-level accuracy with the
+// BF16 weights, and three MMAs per K step cost nothing on a layer that is
+// bound by reading its FP32 inputs.
+#include <cuda_bf16.h>
+
+#include "learned.cuh"
+
+namespace ando {
+
+namespace {
+
+__device__ int g_tc_err;  // timeout flag of launches given no flag of their own
+
+constexpr int TC_M = 128;        // rows per CTA (one tensor-memory lane per row)
+constexpr int TC_N = 64;         // outputs per row (the network width)
+constexpr int TC_THREADS = 128;  // four warps: warp w reads tensor-memory lanes 32w..32w+31
+constexpr int TC_SPLITS = 3;
+
+__device__ inline uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Byte offset of element (r, k) in a K-major tile with K columns and no
+// swizzle: 8 x 16-byte core matrices, consecutive along K (128 bytes apart),
+// 8-row groups K * 16 bytes apart.
+__device__ inline int core_off(int r, int k, int K) { return (r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2; }
+
+// Shared-memory matrix descriptor (sm_100): start address, leading byte
+// offset (between core matrices along K), stride byte offset (between 8-row
+// groups), descriptor version 1, no swizzle.
+__device__ inline uint64_t smem_desc(uint32_t addr, int K) {
+  uint64_t d = uint64_t((addr >> 4) & 0x3fff);
+  d |= uint64_t((128 >> 4) & 0x3fff) << 16;
+  d |= uint64_t(((K * 16) >> 4) & 0x3fff) << 32;
+  d |= uint64_t(1) << 46;
+  return d;
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and
+// B BF16 (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4
+// at bit 24.
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(TC_N >> 3) << 17) | (uint32_t(TC_M >> 4) << 24);
+
+__device__ inline void mma_f16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, int acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ inline bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for phase 0 of the barrier (about a second at most).
+__device__ inline bool mbar_wait_bounded(uint32_t bar) {
+  for (long long it = 0; it < (1ll << 22); ++it) {
+    if (mbar_try_wait(bar, 0)) return true;
+    if (it > 32) __nanosleep(128);
+  }
+  return false;
+}
+
+__device__ inline void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
+        "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ inline uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return uint32_t(__bfloat16_as_ushort(a)) | (uint32_t(__bfloat16_as_ushort(b)) << 16);
+}
+
+// Y[r, :64] = act(X[r, :] W^T + bias) + R1[r, :64], X = [X1 | X2] (K = K1 + K2,
+// a multiple of 16, at most 128; K1 a multiple of 8), W row-major [64][K]
+// (BF16-representable); Q (may be null) gets the pre-activation.
+__global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __restrict__ X1, int ld1, int K1, const float* __restrict__ X2,
+                                                        int ld2, int K2, const float* __restrict__ W, const float* __restrict__ bias,
+                                                        const float* __restrict__ R1, int ldr1, float* __restrict__ Q, float* __restrict__ Y,
+                                                        int relu, int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int K = K1 + K2;
+  const int tile = TC_M * K * 2;  // bytes of one BF16 split of the row tile
+  unsigned char* A = sm;
+  unsigned char* B = sm + TC_SPLITS * tile;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(B + TC_N * K * 2);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int r0 = blockIdx.x * TC_M;
+  const uint32_t bar_a = smem_u32(bar);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)), "r"(TC_N));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_a), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  // B: W (64 x K), exact in BF16
+  for (int i = tid; i < TC_N * K; i += TC_THREADS) {
+    const int n = i / K, k = i - n * K;
+    *reinterpret_cast<__nv_bfloat16*>(B + core_off(n, k, K)) = __float2bfloat16_rn(W[i]);
+  }
+  // A: one row per thread, 8 columns (one 16-byte chunk per split) at a time
+  {
+    const int row = r0 + tid;
+    for (int k = 0; k < K; k += 8) {
+      float v[8];
+      if (row < V) {
+        const float* src = k < K1 ? X1 + (long long)row * ld1 + k : X2 + (long long)row * ld2 + (k - K1);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[e] = src[e];
+      } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[e] = 0.f;
+      }
+      uint32_t w[TC_SPLITS][4];
+#pragma unroll
+      for (int e = 0; e < 8; e += 2) {
+        __nv_bfloat16 h0 = __float2bfloat16_rn(v[e]), h1 = __float2bfloat16_rn(v[e + 1]);
+        float s0 = v[e] - __bfloat162float(h0), s1 = v[e + 1] - __bfloat162float(h1);
+        __nv_bfloat16 m0 = __float2bfloat16_rn(s0), m1 = __float2bfloat16_rn(s1);
+        __nv_bfloat16 l0 = __float2bfloat16_rn(s0 - __bfloat162float(m0)), l1 = __float2bfloat16_rn(s1 - __bfloat162float(m1));
+        w[0][e / 2] = pack2(h0, h1); w[1][e / 2] = pack2(m0, m1); w[2][e / 2] = pack2(l0, l1);
+      }
+      const int off = core_off(tid, k, K);
+#pragma unroll
+      for (int sp = 0; sp < TC_SPLITS; ++sp)
+        *reinterpret_cast<uint4*>(A + sp * tile + off) = make_uint4(w[sp][0], w[sp][1], w[sp][2], w[sp][3]);
+    }
+  }
+  // generic-proxy shared stores -> visible to the tensor core (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  if (tid == 0) {
+    int first = 1;
+    for (int sp = 0; sp < TC_SPLITS; ++sp)
+      for (int kk = 0; kk < K / 16; ++kk) {
+        const uint64_t ad = smem_desc(smem_u32(A + sp * tile + kk * 256), K);
+        const uint64_t bd = smem_desc(smem_u32(B + kk * 256), K);
+        mma_f16(tmem, ad, bd, TC_IDESC, first ? 0 : 1);
+        first = 0;
+      }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_a) : "memory");
+  }
+  const bool done = mbar_wait_bounded(bar_a);
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (done) {
+    float acc[TC_N];
+    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
+#pragma unroll
+    for (int c = 0; c < TC_N; c += 16) tmem_ld16(taddr + c, acc + c);
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    const int row = r0 + tid;  // tensor-memory lane 32 warp + lane = tile row tid
+    if (row < V) {
+      float4* yr = reinterpret_cast<float4*>(Y + (long long)row * TC_N);
+      float4* qr = Q ? reinterpret_cast<float4*>(Q + (long long)row * TC_N) : nullptr;
+      const float4* rr = R1 ? reinterpret_cast<const float4*>(R1 + (long long)row * ldr1) : nullptr;
+#pragma unroll
+      for (int c4 = 0; c4 < TC_N / 4; ++c4) {
+        float q[4], y[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          q[e] = acc[4 * c4 + e] + (bias ? bias[4 * c4 + e] : 0.f);
+          y[e] = relu ? fmaxf(q[e], 0.f) : q[e];
+        }
+        if (qr) qr[c4] = make_float4(q[0], q[1], q[2], q[3]);
+        if (rr) {
+          const float4 t = rr[c4];
+          y[0] += t.x; y[1] += t.y; y[2] += t.z; y[3] += t.w;
+        }
+        yr[c4] = make_float4(y[0], y[1], y[2], y[3]);
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(err ? err : &g_tc_err, 1);
+    mbar_wait_bounded(bar_a);  // give the MMAs in flight a second bound before the accumulator is freed
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_N));
+  }
+}
+
+}  // namespace
+
+size_t gemm_tc_smem(int K) { return size_t(TC_SPLITS) * TC_M * K * 2 + size_t(TC_N) * K * 2 + 16; }
+
+bool gemm_tc_supported(int K1, int K2, int N, int ldr1) {
+  const int K = K1 + K2;
+  return N == TC_N && K >= 16 && K <= 128 && K % 16 == 0 && K1 % 8 == 0 && (ldr1 % 4) == 0;
+}
+
+cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W, const float* bias,
+                           const float* R1, int ldr1, float* Q, float* Y, int relu, int* err, cudaStream_t s) {
+  if (V <= 0) return cudaSuccess;
+  if (!gemm_tc_supported(K1, K2, TC_N, R1 ? ldr1 : 0)) return cudaErrorInvalidValue;
+  auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+  if (!a16(Y) || (Q && !a16(Q)) || (R1 && !a16(R1))) return cudaErrorInvalidValue;  // float4 epilogue
+  static unsigned attr = 0;  // one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 32 && !(attr & (1u << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gemm_tc_smem(128)));
+    if (e != cudaSuccess) return e;
+    attr |= 1u << dev;
+  }
+  const int K = K1 + K2;
+  k_gemm_tc<<<(V + TC_M - 1) / TC_M, TC_THREADS, gemm_tc_smem(K), s>>>(V, X1, ld1, K1, X2, ld2, K2, W, bias, R1, ldr1, Q, Y, relu, err);
+  return cudaGetLastError();
+}
+
+}  // namespace ando
