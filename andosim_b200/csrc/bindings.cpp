@@ -215,16 +215,18 @@ struct RigidBody {
   }
 };
 
-// Simulation state with a device mirror. `device_newer`: the device copy of
-// positions/velocities is authoritative; `host_dirty`: the host copy changed
-// and must be uploaded before the next GPU call.
+// Simulation state with a device mirror. `dev_x` / `dev_v` / `start_stale`:
+// the device copy of the positions / velocities / step start is newer and is
+// downloaded only when the host reads that array; `host_dirty`: the host copy
+// changed and must be uploaded before the next GPU call.
 struct State {
   std::vector<V3> x, v, xp;
   std::vector<V3> start;          // CORRECTED: where the next step starts (ando_state_set_start)
   std::vector<double> m;
   ando_ctx ctx = nullptr;
   uint64_t topo = 0, verts = 0, weights = 0;
-  bool device_newer = false, host_dirty = true, masses_dirty = true;
+  bool dev_x = false, dev_v = false, start_stale = false, host_dirty = true, masses_dirty = true;
+  std::vector<double> stage;      // download staging (reused)
   ando_step_stats last{};
 
   State() = default;
@@ -243,16 +245,33 @@ struct State {
     weights = precond_version();
   }
 
-  void sync_host() {
-    if (!device_newer || !ctx) return;
-    std::vector<double> hx(3 * nv()), hv(3 * nv());
-    check(ando_state_download(ctx, hx.data(), hv.data(), int32_t(nv())), "state download");
-    for (size_t i = 0; i < nv(); ++i) { x[i] = {hx[3 * i], hx[3 * i + 1], hx[3 * i + 2]}; v[i] = {hv[3 * i], hv[3 * i + 1], hv[3 * i + 2]}; }
-    check(ando_state_get_start(ctx, hx.data(), int32_t(nv())), "state start");
-    start.resize(nv());
-    for (size_t i = 0; i < nv(); ++i) start[i] = {hx[3 * i], hx[3 * i + 1], hx[3 * i + 2]};
-    device_newer = false;
+  void mark_device_newer() { dev_x = dev_v = start_stale = true; }
+  void unpack(std::vector<V3>& dst) {
+    dst.resize(nv());
+    for (size_t i = 0; i < nv(); ++i) dst[i] = {stage[3 * i], stage[3 * i + 1], stage[3 * i + 2]};
   }
+  void sync_x() {
+    if (!dev_x || !ctx) return;
+    stage.resize(3 * nv());
+    check(ando_state_download(ctx, stage.data(), nullptr, int32_t(nv())), "state download");
+    unpack(x);
+    dev_x = false;
+  }
+  void sync_v() {
+    if (!dev_v || !ctx) return;
+    stage.resize(3 * nv());
+    check(ando_state_download(ctx, nullptr, stage.data(), int32_t(nv())), "state download");
+    unpack(v);
+    dev_v = false;
+  }
+  void sync_start() {
+    if (!start_stale || !ctx) return;
+    stage.resize(3 * nv());
+    check(ando_state_get_start(ctx, stage.data(), int32_t(nv())), "state start");
+    unpack(start);
+    start_stale = false;
+  }
+  void sync_host() { sync_x(); sync_v(); sync_start(); }
   static std::vector<double> flat(const std::vector<V3>& a) {
     std::vector<double> o(3 * a.size());
     for (size_t i = 0; i < a.size(); ++i) { o[3 * i] = a[i].x; o[3 * i + 1] = a[i].y; o[3 * i + 2] = a[i].z; }
@@ -440,7 +459,7 @@ void state_initialize(State& s, const Mesh& me) {
     double fm = me.areas[f] * me.material.thickness * me.material.density;
     for (int a = 0; a < 3; ++a) s.m[me.tris[3 * f + a]] += fm / 3.0;
   }
-  s.device_newer = false; s.host_dirty = true; s.masses_dirty = true;
+  s.dev_x = s.dev_v = s.start_stale = false; s.host_dirty = true; s.masses_dirty = true;
 }
 
 ando_params to_abi(const SimParams& p) {
@@ -584,8 +603,8 @@ PYBIND11_MODULE(ando_barrier_core, m) {
       .def(py::init<>())
       .def("initialize", &state_initialize)
       .def("num_vertices", &State::nv)
-      .def("get_positions", [](State& s) { s.sync_host(); return v3_array(s.x); })
-      .def("get_velocities", [](State& s) { s.sync_host(); return v3_array(s.v); })
+      .def("get_positions", [](State& s) { s.sync_x(); return v3_array(s.x); })
+      .def("get_velocities", [](State& s) { s.sync_v(); return v3_array(s.v); })
       .def("set_velocities", [](State& s, py::object vel) {
         auto v = to_v3(vel, "velocities");
         s.sync_host();
@@ -604,7 +623,7 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         double gv[3] = {ga.at(0), ga.at(1), ga.at(2)};
         if (s.ctx && !s.host_dirty) {
           check(ando_apply_gravity(s.ctx, gv, dt), "apply_gravity");
-          s.device_newer = true;
+          s.mark_device_newer();
         } else {
           for (size_t i = 0; i < s.nv(); ++i) {
             s.v[i] = add(s.v[i], mul(V3{gv[0], gv[1], gv[2]}, dt));
@@ -614,8 +633,8 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         }
       }, "Apply gravity acceleration to all vertices")
       // FP64 accessors (the device keeps positions and velocities in FP64)
-      .def("get_positions64", [](State& s) { s.sync_host(); return v3_array64(s.x); })
-      .def("get_velocities64", [](State& s) { s.sync_host(); return v3_array64(s.v); })
+      .def("get_positions64", [](State& s) { s.sync_x(); return v3_array64(s.x); })
+      .def("get_velocities64", [](State& s) { s.sync_v(); return v3_array64(s.v); })
       .def("set_positions64", [](State& s, py::object p) {
         auto v = to_v3(p, "positions");
         if (v.size() != s.nv()) throw py::value_error("positions must have one row per vertex");
@@ -736,7 +755,7 @@ PYBIND11_MODULE(ando_barrier_core, m) {
                          ab.data(), int32_t(ab.size()), &s.last);
         }
         check(rc, "Integrator.step");
-        s.device_newer = true;
+        s.mark_device_newer();
         for (size_t i = 0; i < h.size(); ++i) h[i]->from_abi(ab[i]);
       }, py::arg("mesh"), py::arg("state"), py::arg("constraints"), py::arg("params"), py::arg("rigid_bodies") = py::none(),
          "Take one simulation step using Newton integrator with beta accumulation")

@@ -565,15 +565,18 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
 int corrected_line_search(ando_ctx c, int nb) {
   cudaStream_t s = c->stream;
   Phase ph(c, ANDO_PHASE_LINE_SEARCH);
+  CK(cudaMemsetAsync(&c->ctrl.p->toi_overflow, 0, sizeof(int), s));
   launch_swept_end(c->V, c->x.p, c->d.p, c->fixed.p, 1.25, c->max_move, c->x1.p, c->ext.p, s);
   launch_toi_reset(c->toi.p, s);
   launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
   ph.launched(2 + (c->num_walls ? 1 : 0));
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
   CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.0, 1e-3 * c->gap_max, c->toi.p, s));
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.0, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch, c->pcount,
+                          &c->ctrl.p->toi_overflow, s));
   CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.0, 1e-3 * c->gap_max, c->toi.p, s));
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.0, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch, c->pcount,
+                           &c->ctrl.p->toi_overflow, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
   launch_update_toi(c->V, c->x.p, c->ext.p, 1.25, c->fixed.p, c->ctrl.p, c->toi.p, s);
@@ -745,6 +748,8 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
   return ANDO_OK;
 }
 
+int grow_toi_candidates(ando_ctx c, int need);
+
 // inner_newton_step with the CORRECTED terms and line search.
 int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& sp, int nb, ando_step_stats& st, double& ret) {
   cudaStream_t s = c->stream;
@@ -769,6 +774,16 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     c->collect();
+    for (int attempt = 0; c->ctrl_host->toi_overflow; ++attempt) {
+      if (attempt == 4) return fail(ANDO_ERR_CAPACITY, "time-of-impact candidates kept overflowing");
+      rc = grow_toi_candidates(c, c->ctrl_host->toi_overflow);
+      if (rc) return rc;
+      rc = corrected_line_search(c, nb);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      c->collect();
+    }
     const Ctrl& h = *c->ctrl_host;
     if (h.pcg_status == PCG_TIMEOUT || h.bar_err) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
     st.newton_iters++;
@@ -825,11 +840,12 @@ int remember_safe(ando_ctx c) {
 // targets as far as the move's conservative time of impact allows (walls,
 // self contact, rigid triangles; a teleported pin would drag the cloth into
 // itself), then stay fixed for the step.
-int apply_pins(ando_ctx c, int nb) {
+int apply_pins_once(ando_ctx c, int nb) {
   cudaStream_t s = c->stream;
   CK(cudaMemsetAsync(c->fixed.p, 0, c->V, s));
   if (!c->num_pins) return ANDO_OK;
   Phase ph(c, ANDO_PHASE_SETUP);
+  CK(cudaMemsetAsync(&c->ctrl.p->toi_overflow, 0, sizeof(int), s));
   CK(cudaMemsetAsync(c->ext.p, 0, sizeof(double) * 3ull * c->V, s));
   CK(cudaMemcpyAsync(c->x1.p, c->x.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, s));
   launch_pin_ext(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->ext.p, c->x1.p, c->fixed.p, s);
@@ -838,15 +854,48 @@ int apply_pins(ando_ctx c, int nb) {
   ph.launched(2 + (c->num_walls ? 1 : 0));
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
   CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, s));
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch,
+                          c->pcount, &c->ctrl.p->toi_overflow, s));
   CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, s));
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch,
+                           c->pcount, &c->ctrl.p->toi_overflow, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
-  launch_pin_move(c->pin_vertex.p, c->num_pins, c->ext.p, c->toi.p, c->x.p, s);
+  launch_pin_move(c->pin_vertex.p, c->num_pins, c->ext.p, c->toi.p, c->ctrl.p, c->x.p, s);
   ph.launched();
   CK(cudaGetLastError());
   return ANDO_OK;
+}
+
+// A time-of-impact candidate list that overflowed its buffer left the
+// state untouched (the move kernels check the flag): grow the buffer and run
+// the pass again.
+int grow_toi_candidates(ando_ctx c, int need) {
+  const size_t n = std::max<size_t>(2 * size_t(need), 2 * c->pair_scratch.n);
+  if (need < 0 || n > (size_t(1) << 26)) return fail(ANDO_ERR_CAPACITY, "more than 64M time-of-impact candidate pairs");
+  CK(c->pair_scratch.reserve(n));
+  return ANDO_OK;
+}
+
+int toi_overflow_need(ando_ctx c, int& need) {
+  need = 0;
+  CK(cudaMemcpyAsync(&need, &c->ctrl.p->toi_overflow, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ANDO_OK;
+}
+
+int apply_pins(ando_ctx c, int nb) {
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    int rc = apply_pins_once(c, nb);
+    if (rc) return rc;
+    if (!c->num_pins) return ANDO_OK;
+    int need = 0;
+    rc = toi_overflow_need(c, need);
+    if (rc || !need) return rc;
+    rc = grow_toi_candidates(c, need);
+    if (rc) return rc;
+  }
+  return fail(ANDO_ERR_CAPACITY, "time-of-impact candidates kept overflowing");
 }
 
 // One Newton iteration of the REFERENCE step as a fixed launch sequence
@@ -1258,6 +1307,10 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     CK(c->eorder.upload(eo.data(), c->E, s));
     c->bvh_tri.qorder = c->vorder.p;
     c->bvh_edge.qorder = c->eorder.p;
+    // candidate pairs: about two per vertex and four per edge on a flat
+    // sheet; start at twice that so growth (a reallocation and a redone
+    // pass) is rare
+    CK(c->pair_scratch.reserve(4ull * V + 8ull * c->E + 1024));
   }
   CK(c->el_a.reserve(nnzb)); CK(c->el_b.reserve(nnzb)); CK(c->g_el.reserve(3ull * V));
   // per-vertex / per-slot work buffers

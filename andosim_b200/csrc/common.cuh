@@ -113,6 +113,8 @@ struct Ctrl {
   int strain_active;
   unsigned int bar_count, bar_gen; int bar_err;
   int tc_err;                     // a tensor-core GEMM's bounded wait gave up (sticky)
+  int toi_overflow;               // > 0: a time-of-impact candidate list needed this many slots; the move was not applied
+  int pad_;
 };
 
 // PCG_PRECOND: the learned preconditioner lost positive definiteness

@@ -114,9 +114,9 @@ __global__ void k_pin_interp(int num_pins, const double* start, const double* fi
 }
 
 // x += toi * ext on pinned vertices (toi: the move's conservative time of impact).
-__global__ void k_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x) {
+__global__ void k_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, const Ctrl* ctrl, double* x) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= num_pins) return;
+  if (k >= num_pins || ctrl->toi_overflow) return;  // incomplete time of impact: the caller redoes the pass
   int v = pin_vertex[k];
   if (k + 1 < num_pins && pin_vertex[k + 1] == v) return;
   double t = fmin(1.0, __longlong_as_double((long long)*toi));
@@ -194,7 +194,7 @@ __global__ void k_toi_rigid(int V, const double* x, const double* ext, const Rig
 // x += toi * ext / 1.25 (the clipped Newton direction times the time of impact).
 __global__ void k_update_toi(int V, double* x, const double* ext, double ext_scale, const unsigned char* fixed, Ctrl* ctrl,
                              const unsigned long long* toi) {
-  if (ctrl->converged) return;
+  if (ctrl->converged || ctrl->toi_overflow) return;  // overflow: incomplete time of impact, the caller redoes the pass
   double a = fmin(1.0, __longlong_as_double((long long)*toi));
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) ctrl->alpha = a;
@@ -213,8 +213,9 @@ void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pin
                     unsigned char* fixed, cudaStream_t s) {
   if (num_pins) k_pin_ext<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, ext, x1, fixed);
 }
-void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x, cudaStream_t s) {
-  if (num_pins) k_pin_move<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, ext, toi, x);
+void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, const Ctrl* ctrl, double* x,
+                     cudaStream_t s) {
+  if (num_pins) k_pin_move<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, ext, toi, ctrl, x);
 }
 void launch_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out,
                         cudaStream_t s) {

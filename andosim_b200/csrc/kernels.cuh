@@ -78,7 +78,8 @@ void launch_velocity_ctl(int V, const double* x, const double* x_old, double dt,
 void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed, cudaStream_t s);
 void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
                     unsigned char* fixed, cudaStream_t s);
-void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, double* x, cudaStream_t s);
+void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, const Ctrl* ctrl, double* x,
+                     cudaStream_t s);
 void launch_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out,
                         cudaStream_t s);
 void launch_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start, cudaStream_t s);

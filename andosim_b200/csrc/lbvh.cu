@@ -149,9 +149,12 @@ __global__ void k_refit(const Box* boxes, const int* order, int n, const int* le
   int p = parent[leaf];
   to_parent(inner, left, p, leaf, lb);
   while (p >= 0) {
-    __threadfence();
-    if (atomicAdd(&arrive[p], 1) == 0) return;  // first arrival: the sibling finishes this node
-    __threadfence();
+    // first arrival: the sibling finishes this node. The acquire-release
+    // atomic publishes this thread's box writes to the sibling and makes the
+    // sibling's visible to it (no full fences).
+    int prior;
+    asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(prior) : "l"(arrive + p) : "memory");
+    if (prior == 0) return;
     // the sibling's box was written by another thread: read it past L1
     Box a, b;
     const float* pa = reinterpret_cast<const float*>(nodes + left[p]);
@@ -185,26 +188,11 @@ __device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, in
   }
 }
 
-// What a query does at an accepted leaf: report the candidate pair
-// (Q_PAIRS); report it only when its FP64 distance at x is below nw.gap
-// (Q_CONTACTS); or fold its conservative time of impact along nw.ext into a
-// per-thread minimum that is min-reduced into *nw.toi (Q_TOI, nothing is
-// written per pair).
-enum QueryMode { Q_PAIRS = 0, Q_CONTACTS = 1, Q_TOI = 2 };
-struct QueryNarrow {
-  double gap = 0.0;
-  const double* ext = nullptr;
-  double eta_min = 0.0, near = 0.0;
-  unsigned long long* toi = nullptr;
-};
-
 // One thread per query. kind 0: query = vertex (point box +-1e-4 inflated by
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
 // prims = edges, keep e1 < e2 without shared vertex.
-template <int MODE>
 __global__ void k_query(const double* x, const double* x1, const int* qprims, const int* qorder, int kind, int nq, float pad, const int* prims,
-                        int n, const int* order, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap,
-                        QueryNarrow nw) {
+                        int n, const int* order, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < nq;
   const int q = active && qorder ? qorder[t] : t;
@@ -248,29 +236,19 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
     if (n == 1) single = true;
     else if (overlap(qb, nodes[0])) node = 0;
   }
-  double tmin = 1.0;
   auto accept = [&](int leaf) {
     int prim = order[leaf - leaf0];
     bool hit;
-    int id[4];
-    if (kind == 0) {
-      id[0] = q; id[1] = prims[3 * prim]; id[2] = prims[3 * prim + 1]; id[3] = prims[3 * prim + 2];
-      hit = id[1] != q && id[2] != q && id[3] != q;
-    } else {
+    if (kind == 0) hit = prims[3 * prim] != q && prims[3 * prim + 1] != q && prims[3 * prim + 2] != q;
+    else {
       int pa = prims[2 * prim], pc = prims[2 * prim + 1];
-      id[0] = qa; id[1] = qc; id[2] = pa; id[3] = pc;
       hit = q < prim && pa != qa && pa != qc && pc != qa && pc != qc;
-    }
-    if (MODE == Q_CONTACTS && hit) hit = pair_gap(kind, id, x) < nw.gap;
-    if (MODE == Q_TOI && hit) {
-      tmin = fmin(tmin, pair_toi(kind, id, x, nw.ext, nw.eta_min, nw.near));
-      hit = false;
     }
     return hit ? prim : -1;
   };
   if (__any_sync(0xffffffffu, single)) {
     int prim = single && overlap(qb, nodes[0]) ? accept(0) : -1;
-    if (MODE != Q_TOI) emit(prim >= 0, q, prim, out, count, cap);
+    emit(prim >= 0, q, prim, out, count, cap);
   }
   while (__any_sync(0xffffffffu, node >= 0)) {
     int hl = -1, hr = -1;
@@ -291,19 +269,61 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
         node = tl ? l : r;
         if (tl && tr) {
           if (sp < STACK) stack[sp++] = r;
-          else if (count) atomicAdd(count + 1, 1);
+          else atomicAdd(count + 1, 1);
         }
       }
     }
-    if (MODE != Q_TOI) {
-      emit(hl >= 0, q, hl, out, count, cap);
-      emit(hr >= 0, q, hr, out, count, cap);
+    emit(hl >= 0, q, hl, out, count, cap);
+    emit(hr >= 0, q, hr, out, count, cap);
+  }
+}
+
+// The four vertices of candidate pair (q, prim): kind 0 vertex q against
+// triangle prim; kind 1 edge q against edge prim.
+__device__ inline void pair_ids(int kind, int2 pr, const int* prims, const int* qprims, int id[4]) {
+  if (kind == 0) { id[0] = pr.x; id[1] = prims[3 * pr.y]; id[2] = prims[3 * pr.y + 1]; id[3] = prims[3 * pr.y + 2]; }
+  else { id[0] = qprims[2 * pr.x]; id[1] = qprims[2 * pr.x + 1]; id[2] = prims[2 * pr.y]; id[3] = prims[2 * pr.y + 1]; }
+}
+
+// Narrow phase over the candidate list of the last traversal. The count
+// stays on the device (count[0]); a list that overflowed its capacity sets
+// *overflow instead of being used, so the caller grows it and runs again.
+constexpr int NARROW_GRID = 148 * 8;
+
+// candidates whose FP64 distance at x is below gap -> surv (count[2])
+__global__ void k_pairs_gap(const int2* cand, const int* count, int cap, int kind, const int* prims, const int* qprims, const double* x,
+                            double gap, int2* surv, int* scount) {
+  const int n = min(count[0], cap);
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    bool keep = false;
+    int2 pr = make_int2(0, 0);
+    if (i < n) {
+      pr = cand[i];
+      int id[4];
+      pair_ids(kind, pr, prims, qprims, id);
+      keep = pair_gap(kind, id, x) < gap;
     }
+    emit(keep, pr.x, pr.y, surv, scount, cap);
   }
-  if (MODE == Q_TOI) {
-    double t = warp_min(tmin);
-    if ((threadIdx.x & 31) == 0 && t < 1.0) atomic_min_pos(nw.toi, t);
+}
+
+// min over the candidates of the conservative time of impact along ext
+__global__ void k_pairs_toi(const int2* cand, const int* count, int cap, int kind, const int* prims, const int* qprims, const double* x,
+                            const double* ext, double eta_min, double near, unsigned long long* toi, int* overflow) {
+  if (count[0] > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(overflow, count[0]);  // the capacity that is needed
+    return;
   }
+  const int n = count[0];
+  double t = 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int id[4];
+    pair_ids(kind, cand[i], prims, qprims, id);
+    t = fmin(t, pair_toi(kind, id, x, ext, eta_min, near));
+  }
+  t = warp_min(t);
+  if ((threadIdx.x & 31) == 0 && t < 1.0) atomic_min_pos(toi, t);
 }
 
 __global__ void k_pair_keys(const int2* pairs, int n, unsigned long long* keys) {
@@ -380,32 +400,36 @@ cudaError_t Lbvh::update(const double* x, const double* x1, const int* prims_, i
 }
 
 namespace {
-// Sorted pairs of a Q_PAIRS or Q_CONTACTS query (capacity grown as needed).
-cudaError_t run_query(Lbvh& B, int mode, const QueryNarrow& nw, const double* x, const double* x1, int kind, const int* qprims, int nq,
-                      float pad, DevBuf<int2>& out, DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0,
-                      DevBuf<unsigned long long>& k1, DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
+// Sorted pairs of a query: every box candidate, or (gap >= 0) those whose
+// FP64 distance at x is below gap. Capacity grows as needed.
+cudaError_t run_query(Lbvh& B, double gap, const double* x, const double* x1, int kind, const int* qprims, int nq, float pad,
+                      DevBuf<int2>& out, DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
+                      DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
   cudaError_t e;
   *npairs = 0;
   if (B.n == 0 || nq == 0) return cudaSuccess;
-  if ((e = counter.reserve(2))) return e;
+  const bool narrow = gap >= 0.0;
+  if ((e = counter.reserve(3))) return e;
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
+  DevBuf<int2>& src = narrow ? B.surv : scratch;
   for (int attempt = 0; attempt < 2; ++attempt) {
     int cap = int(scratch.n);
-    if ((e = cudaMemsetAsync(counter.p, 0, 2 * sizeof(int), s))) return e;
-    if (mode == Q_CONTACTS)
-      k_query<Q_CONTACTS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
-                                                   scratch.p, counter.p, cap, nw);
-    else
-      k_query<Q_PAIRS><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p,
-                                                scratch.p, counter.p, cap, nw);
+    if (narrow && (e = B.surv.reserve(scratch.n))) return e;
+    if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
+    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p, scratch.p,
+                                     counter.p, cap);
     B.launches += 1;
-    int cnt2[2] = {0, 0};
-    if ((e = cudaMemcpyAsync(cnt2, counter.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
+    if (narrow) {
+      k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, B.prims, qprims, x, gap, B.surv.p, counter.p + 2);
+      B.launches += 1;
+    }
+    int cnt3[3] = {0, 0, 0};
+    if ((e = cudaMemcpyAsync(cnt3, counter.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
-    if (cnt2[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
-    int cnt = cnt2[0];
+    if (cnt3[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
+    int cnt = cnt3[0];
     if (cnt < 0 || cnt > (1 << 26)) return cudaErrorMemoryAllocation;  // > 64M candidate pairs: refuse instead of exhausting memory
-    if (cnt <= cap) { *npairs = cnt; break; }
+    if (cnt <= cap) { *npairs = narrow ? cnt3[2] : cnt; break; }
     if ((e = scratch.reserve(size_t(cnt) + size_t(cnt) / 4))) return e;
   }
   int m = *npairs;
@@ -413,12 +437,12 @@ cudaError_t run_query(Lbvh& B, int mode, const QueryNarrow& nw, const double* x,
   if ((e = k0.reserve(m))) return e;
   if ((e = k1.reserve(m))) return e;
   if ((e = out.reserve(m))) return e;
-  k_pair_keys<<<nblk(m), TPB, 0, s>>>(scratch.p, m, k0.p);
+  k_pair_keys<<<nblk(m), TPB, 0, s>>>(src.p, m, k0.p);
   B.launches += 1;
   size_t bytes = 0;
-  if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
+  if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.p, k1.p, src.p, out.p, m, 0, 64, s))) return e;
   if ((e = tmp.reserve(bytes))) return e;
-  if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
+  if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, k0.p, k1.p, src.p, out.p, m, 0, 64, s))) return e;
   return cudaGetLastError();
 }
 }  // namespace
@@ -428,24 +452,27 @@ cudaError_t run_query(Lbvh& B, int mode, const QueryNarrow& nw, const double* x,
 cudaError_t Lbvh::query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
                         DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
                         DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
-  return run_query(*this, Q_PAIRS, QueryNarrow{}, x, x1, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
+  return run_query(*this, -1.0, x, x1, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
 }
 
 cudaError_t Lbvh::query_contacts(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& out,
                                  DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
                                  DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
-  QueryNarrow nw;
-  nw.gap = gap;
-  return run_query(*this, Q_CONTACTS, nw, x, nullptr, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
+  return run_query(*this, gap < 0.0 ? 0.0 : gap, x, nullptr, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
 }
 
 cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, double eta_min,
-                            double near, unsigned long long* toi, cudaStream_t s) {
+                            double near, unsigned long long* toi, DevBuf<int2>& scratch, DevBuf<int>& counter, int* overflow,
+                            cudaStream_t s) {
   if (n == 0 || nq == 0) return cudaSuccess;
-  QueryNarrow nw;
-  nw.ext = ext; nw.eta_min = eta_min; nw.near = near; nw.toi = toi;
-  k_query<Q_TOI><<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, prims, n, order.p, inner.p, nodes.p, nullptr, nullptr, 0, nw);
-  launches += 1;
+  cudaError_t e;
+  if ((e = counter.reserve(3))) return e;
+  if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
+  const int cap = int(scratch.n);
+  if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, prims, n, order.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_pairs_toi<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, ext, eta_min, near, toi, overflow);
+  launches += 2;
   return cudaGetLastError();
 }
 

@@ -26,6 +26,7 @@ struct Lbvh {
   DevBuf<LbvhInner> inner;      // n-1 internal nodes, child boxes packed (written by the refit)
   DevBuf<unsigned long long> keys, keys_sorted;
   DevBuf<int> idx, order, left, right, parent, arrive, bounds;
+  DevBuf<int2> surv;            // candidates kept by the narrow phase of query_contacts
   long long launches = 0;
 
   cudaError_t reserve_prims(int n);
@@ -42,16 +43,20 @@ struct Lbvh {
                     DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1, DevBuf<int>& counter,
                     DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
   // The candidates (boxes at x inflated by pad) whose FP64 distance at x is
-  // below `gap`, sorted: the narrow phase runs at the leaves, so only
-  // contacts are written and sorted.
+  // below `gap`, sorted: a flat narrow-phase pass keeps the contacts before
+  // the sort, so only contacts are sorted.
   cudaError_t query_contacts(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& out,
                              DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
                              DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
   // min over the swept-box candidates (x -> x1 = x + ext, no pad) of the
   // pair's conservative time of impact, min-reduced into *toi (IEEE bits of a
-  // non-negative double) on the device: no pair list, no host round trip.
+  // non-negative double) on the device, with no host round trip: the
+  // candidate count stays on the device. When the candidates overflow
+  // `scratch`, *overflow is raised to the count needed and *toi is not
+  // lowered; the caller grows `scratch` and runs the pass again.
   cudaError_t query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, double eta_min,
-                        double near, unsigned long long* toi, cudaStream_t s);
+                        double near, unsigned long long* toi, DevBuf<int2>& scratch, DevBuf<int>& counter, int* overflow,
+                        cudaStream_t s);
 };
 
 }  // namespace ando

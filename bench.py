@@ -360,7 +360,7 @@ def e2e_run(args, sc, local, flush, pg, weights):
     n_pins = len(sc.pins_at(0))
     return {"value": round(args.steps * int(os.environ.get("WORLD_SIZE", "1")) / (e2e_ms * 1e-3), 2), "unit": "frames/s",
             "h2d_bytes_per_step": n_pins * (4 + 24) + len(sc.walls) * 48,     # pins and walls uploaded each step
-            "d2h_bytes_per_step": 2 * 24 * sc.num_vertices}                   # positions and velocities (FP64) read back
+            "d2h_bytes_per_step": 24 * sc.num_vertices}                       # positions (FP64) read back
 
 
 def run_ours(args, rank, world, local, pg):
