@@ -23,7 +23,8 @@ __device__ int g_tc_err;  // timeout flag of launches given no flag of their own
 
 constexpr int TC_M = 128;        // rows per CTA (one tensor-memory lane per row)
 constexpr int TC_N = 64;         // outputs per row (the network width)
-constexpr int TC_THREADS = 128;  // four warps: warp w reads tensor-memory lanes 32w..32w+31
+constexpr int TC_THREADS = 256;  // eight warps: warp w reads tensor-memory lanes 32 (w % 4).. and columns 32 (w / 4)..
+constexpr int TC_COLS_PER_WARP = TC_N / (TC_THREADS / 128);
 constexpr int TC_SPLITS = 3;
 
 __device__ inline uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
@@ -94,8 +95,9 @@ __device__ inline uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
 }
 
 // Y[r, :64] = act(X[r, :] W^T + bias) + R1[r, :64], X = [X1 | X2] (K = K1 + K2,
-// a multiple of 16, at most 128; K1 a multiple of 8), W row-major [64][K]
-// (BF16-representable); Q (may be null) gets the pre-activation.
+// a multiple of 16, at most 128; K1 a multiple of 8; rows 16-byte aligned),
+// W row-major [64][K] (BF16-representable); Q (may be null) gets the
+// pre-activation.
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __restrict__ X1, int ld1, int K1, const float* __restrict__ X2,
                                                         int ld2, int K2, const float* __restrict__ W, const float* __restrict__ bias,
                                                         const float* __restrict__ R1, int ldr1, float* __restrict__ Q, float* __restrict__ Y,
@@ -124,32 +126,29 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
     const int n = i / K, k = i - n * K;
     *reinterpret_cast<__nv_bfloat16*>(B + core_off(n, k, K)) = __float2bfloat16_rn(W[i]);
   }
-  // A: one row per thread, 8 columns (one 16-byte chunk per split) at a time
+  // A: coalesced 16-byte loads (consecutive threads take consecutive
+  // 4-column groups of a row), each split into three BF16 4-vectors
   {
-    const int row = r0 + tid;
-    for (int k = 0; k < K; k += 8) {
-      float v[8];
-      if (row < V) {
-        const float* src = k < K1 ? X1 + (long long)row * ld1 + k : X2 + (long long)row * ld2 + (k - K1);
+    const int K4 = K >> 2, n4 = TC_M * K4;
+#pragma unroll 4
+    for (int c = tid; c < n4; c += TC_THREADS) {
+      const int r = c / K4, k = (c - r * K4) << 2, row = r0 + r;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (row < V) v = k < K1 ? *reinterpret_cast<const float4*>(X1 + (long long)row * ld1 + k)
+                              : *reinterpret_cast<const float4*>(X2 + (long long)row * ld2 + (k - K1));
+      const float f[4] = {v.x, v.y, v.z, v.w};
+      uint32_t w[TC_SPLITS][2];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) v[e] = src[e];
-      } else {
-#pragma unroll
-        for (int e = 0; e < 8; ++e) v[e] = 0.f;
-      }
-      uint32_t w[TC_SPLITS][4];
-#pragma unroll
-      for (int e = 0; e < 8; e += 2) {
-        __nv_bfloat16 h0 = __float2bfloat16_rn(v[e]), h1 = __float2bfloat16_rn(v[e + 1]);
-        float s0 = v[e] - __bfloat162float(h0), s1 = v[e + 1] - __bfloat162float(h1);
+      for (int e = 0; e < 4; e += 2) {
+        __nv_bfloat16 h0 = __float2bfloat16_rn(f[e]), h1 = __float2bfloat16_rn(f[e + 1]);
+        float s0 = f[e] - __bfloat162float(h0), s1 = f[e + 1] - __bfloat162float(h1);
         __nv_bfloat16 m0 = __float2bfloat16_rn(s0), m1 = __float2bfloat16_rn(s1);
         __nv_bfloat16 l0 = __float2bfloat16_rn(s0 - __bfloat162float(m0)), l1 = __float2bfloat16_rn(s1 - __bfloat162float(m1));
         w[0][e / 2] = pack2(h0, h1); w[1][e / 2] = pack2(m0, m1); w[2][e / 2] = pack2(l0, l1);
       }
-      const int off = core_off(tid, k, K);
+      const int off = core_off(r, k, K);  // k % 4 == 0: 8-byte aligned inside a 16-byte core-matrix row
 #pragma unroll
-      for (int sp = 0; sp < TC_SPLITS; ++sp)
-        *reinterpret_cast<uint4*>(A + sp * tile + off) = make_uint4(w[sp][0], w[sp][1], w[sp][2], w[sp][3]);
+      for (int sp = 0; sp < TC_SPLITS; ++sp) *reinterpret_cast<uint2*>(A + sp * tile + off) = make_uint2(w[sp][0], w[sp][1]);
     }
   }
   // generic-proxy shared stores -> visible to the tensor core (async proxy)
@@ -172,22 +171,24 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
   const bool done = mbar_wait_bounded(bar_a);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (done) {
-    float acc[TC_N];
-    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16);
+    // warp w: tensor-memory lanes (rows) 32 (w % 4) + lane, columns c0 .. c0 + 31
+    const int quarter = warp & 3, c0 = (warp >> 2) * TC_COLS_PER_WARP;
+    float acc[TC_COLS_PER_WARP];
+    const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(c0);
 #pragma unroll
-    for (int c = 0; c < TC_N; c += 16) tmem_ld16(taddr + c, acc + c);
+    for (int c = 0; c < TC_COLS_PER_WARP; c += 16) tmem_ld16(taddr + c, acc + c);
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    const int row = r0 + tid;  // tensor-memory lane 32 warp + lane = tile row tid
+    const int row = r0 + quarter * 32 + (tid & 31);
     if (row < V) {
-      float4* yr = reinterpret_cast<float4*>(Y + (long long)row * TC_N);
-      float4* qr = Q ? reinterpret_cast<float4*>(Q + (long long)row * TC_N) : nullptr;
-      const float4* rr = R1 ? reinterpret_cast<const float4*>(R1 + (long long)row * ldr1) : nullptr;
+      float4* yr = reinterpret_cast<float4*>(Y + (long long)row * TC_N + c0);
+      float4* qr = Q ? reinterpret_cast<float4*>(Q + (long long)row * TC_N + c0) : nullptr;
+      const float4* rr = R1 ? reinterpret_cast<const float4*>(R1 + (long long)row * ldr1 + c0) : nullptr;
 #pragma unroll
-      for (int c4 = 0; c4 < TC_N / 4; ++c4) {
+      for (int c4 = 0; c4 < TC_COLS_PER_WARP / 4; ++c4) {
         float q[4], y[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-          q[e] = acc[4 * c4 + e] + (bias ? bias[4 * c4 + e] : 0.f);
+          q[e] = acc[4 * c4 + e] + (bias ? bias[c0 + 4 * c4 + e] : 0.f);
           y[e] = relu ? fmaxf(q[e], 0.f) : q[e];
         }
         if (qr) qr[c4] = make_float4(q[0], q[1], q[2], q[3]);
@@ -218,6 +219,7 @@ bool gemm_tc_supported(int K1, int K2, int N, int ldr1) {
   const int K = K1 + K2;
   return N == TC_N && K >= 16 && K <= 128 && K % 16 == 0 && K1 % 8 == 0 && (ldr1 % 4) == 0;
 }
+static_assert(TC_THREADS % 128 == 0 && TC_COLS_PER_WARP % 16 == 0, "epilogue: whole tensor-memory lane quarters, 16-column loads");
 
 cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W, const float* bias,
                            const float* R1, int ldr1, float* Q, float* Y, int relu, int* err, cudaStream_t s) {
@@ -225,6 +227,7 @@ cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float*
   if (!gemm_tc_supported(K1, K2, TC_N, R1 ? ldr1 : 0)) return cudaErrorInvalidValue;
   auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
   if (!a16(Y) || (Q && !a16(Q)) || (R1 && !a16(R1))) return cudaErrorInvalidValue;  // float4 epilogue
+  if (!a16(X1) || (ld1 & 3) || (K2 && (!a16(X2) || (ld2 & 3)))) return cudaErrorInvalidValue;  // float4 staging
   static unsigned attr = 0;  // one bit per device
   int dev = 0;
   cudaGetDevice(&dev);
