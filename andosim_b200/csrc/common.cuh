@@ -115,6 +115,7 @@ struct Ctrl {
   int tc_err;                     // a tensor-core GEMM's bounded wait gave up (sticky)
   int toi_overflow;               // > 0: a time-of-impact candidate list needed this many slots; the move was not applied
   int pad_;
+  unsigned long long bar_arrivals;  // grid_sync_ar: arrivals since the launcher zeroed it
 };
 
 // PCG_PRECOND: the learned preconditioner lost positive definiteness
@@ -162,6 +163,32 @@ __device__ inline bool grid_sync(unsigned int* count, unsigned int* gen, int* er
   __syncthreads();
   volatile int* verr = err;
   return *verr == 0;
+}
+
+// Bounded grid barrier with acquire/release atomics: every CTA adds one
+// arrival to a 64-bit counter that the launcher zeroed (release: the CTA's
+// writes, ordered before the arrival by __syncthreads, are published) and
+// polls with acquire loads until all nblocks CTAs have arrived `epoch` times.
+// About half the cost of grid_sync's full fences. Same error contract.
+__device__ inline bool grid_sync_ar(unsigned long long* arrivals, unsigned int nblocks, unsigned int& epoch, int* err) {
+  __syncthreads();
+  ++epoch;
+  if (threadIdx.x == 0) {
+    const unsigned long long target = (unsigned long long)epoch * nblocks;
+    unsigned long long prior;
+    asm volatile("atom.add.release.gpu.u64 %0, [%1], 1;" : "=l"(prior) : "l"(arrivals) : "memory");
+    long long polls = 0;
+    while (true) {
+      unsigned long long v;
+      asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(arrivals) : "memory");
+      if (v >= target) break;
+      if (*(volatile int*)err) break;
+      if (++polls > (1ll << 24)) { atomicExch(err, 1); break; }
+      if (polls > 1024) __nanosleep(32);
+    }
+  }
+  __syncthreads();
+  return *(volatile int*)err == 0;
 }
 
 }  // namespace ando

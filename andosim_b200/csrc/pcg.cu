@@ -270,8 +270,8 @@ __device__ inline void fixed_reduce(const double* part, const double* pm, int n,
   for (int t = threadIdx.x; t < RED_T; t += blockDim.x) {
     double s = 0.0, m = 0.0;
     for (int k = t; k < n; k += RED_T) {
-      s += part[k];
-      if (MAX) m = fmax(m, pm[k]);
+      s += __ldcg(part + k);  // written by other CTAs before the barrier: read from L2
+      if (MAX) m = fmax(m, __ldcg(pm + k));
     }
     sh.s[t] = s;
     if (MAX) sh.m[t] = m;
@@ -361,6 +361,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
   float* rn = a.r2;
   const float* zsrc = LEARNED ? a.z : a.r;
   double dummy;
+  unsigned int epoch = 0;  // grid barriers passed (the launcher zeroes the arrival counter)
 
   // init: x^ = 0, r = b^, z = S b^
   for (int sl = gw; sl < ns; sl += W) {
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
     rz_loc = warp_sum(rz_loc);
     if (lane == 0) part_rz[sl] = rz_loc;
   }
-  bool ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+  bool ok = grid_sync_ar(&ctrl->bar_arrivals, nb, epoch, &ctrl->bar_err);
   int status = PCG_MAXIT, iters = 0;
   double rel = 0.0, rz = 0.0;
   if (!ok) status = PCG_TIMEOUT;
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
       pap_loc = warp_sum(pap_loc);
       if (lane == 0) part_pap[sl] = pap_loc;
     }
-    ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+    ok = grid_sync_ar(&ctrl->bar_arrivals, nb, epoch, &ctrl->bar_err);
     if (!ok) { status = PCG_TIMEOUT; break; }
     double pap;
     fixed_reduce<false>(part_pap, nullptr, ns, sh, pap, dummy);
@@ -473,7 +474,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
         if (lane == 0) { part_rz[sl] = rz_new_loc; part_rinf[sl] = rinf_loc; }
       }
     }
-    ok = grid_sync(&ctrl->bar_count, &ctrl->bar_gen, &ctrl->bar_err, nb);
+    ok = grid_sync_ar(&ctrl->bar_arrivals, nb, epoch, &ctrl->bar_err);
     if (!ok) { status = PCG_TIMEOUT; break; }
     double rz_new, rinf;
     fixed_reduce<true>(part_rz, part_rinf, ns, sh, rz_new, rinf);
@@ -577,6 +578,8 @@ int pcg_scaled_shapes(int device, int V, bool learned, PcgShape* out, int max) {
 
 cudaError_t launch_pcg_scaled(const PcgScaledArgs& a, bool learned, const PcgShape& sh, cudaStream_t s) {
   if (sh.tpb < 32 || sh.tpb > SCALED_MAX_TPB || (sh.tpb & 31) || sh.grid < 1) return cudaErrorInvalidConfiguration;
+  cudaError_t e = cudaMemsetAsync(&a.ctrl->bar_arrivals, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
   void* args[] = {(void*)&a};
   return cudaLaunchCooperativeKernel((void*)scaled_kernel(learned, sh.unroll), dim3(sh.grid), dim3(sh.tpb), args, 0, s);
 }
