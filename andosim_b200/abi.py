@@ -154,6 +154,7 @@ def lib() -> C.CDLL:
     L.ando_profile_read.restype = I32; L.ando_profile_read.argtypes = [P, C.POINTER(Profile)]
     L.ando_ctx_stream.restype = I32; L.ando_ctx_stream.argtypes = [P, C.POINTER(C.c_void_p)]
     L.ando_ctx_select_pcg_shape.restype = I32; L.ando_ctx_select_pcg_shape.argtypes = [P, I32, I32]
+    L.ando_ctx_set_pair_capacity.restype = I32; L.ando_ctx_set_pair_capacity.argtypes = [P, I32]
     L.ando_ctx_pcg_shape.restype = I32; L.ando_ctx_pcg_shape.argtypes = [P, I32, pi, pi, pd]
     L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
     pu8 = C.POINTER(C.c_ubyte)
@@ -382,6 +383,10 @@ class Scene:
         sp = C.c_void_p()
         _check(lib().ando_ctx_stream(self.ctx, C.byref(sp)), "ando_ctx_stream")
         return sp.value or 0
+
+    def set_pair_capacity(self, pairs: int):
+        """Start the broad-phase candidate buffers at `pairs` (they grow on demand)."""
+        _check(lib().ando_ctx_set_pair_capacity(self.ctx, pairs), "ando_ctx_set_pair_capacity")
 
     def select_pcg_shape(self, learned: bool, index: int = -1):
         """Fix scaled-PCG launch candidate `index` (-1: autotune on the next first solve)."""

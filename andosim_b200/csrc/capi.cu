@@ -156,6 +156,7 @@ struct ando_ctx_s {
   int E = 0;
   Lbvh bvh_tri, bvh_edge;
   DevBuf<int2> pairs, pair_scratch;
+  DevBuf<int2> toi_scratch;        // candidates of the time-of-impact passes (grown on overflow)
   DevBuf<unsigned long long> pk0, pk1;
   DevBuf<int> pcount;
 
@@ -572,10 +573,10 @@ int corrected_line_search(ando_ctx c, int nb) {
   ph.launched(2 + (c->num_walls ? 1 : 0));
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
   CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.0, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch, c->pcount,
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.0, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch, c->pcount,
                           &c->ctrl.p->toi_overflow, s));
   CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.0, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch, c->pcount,
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.0, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch, c->pcount,
                            &c->ctrl.p->toi_overflow, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
@@ -854,10 +855,10 @@ int apply_pins_once(ando_ctx c, int nb) {
   ph.launched(2 + (c->num_walls ? 1 : 0));
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
   CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch,
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch,
                           c->pcount, &c->ctrl.p->toi_overflow, s));
   CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->pair_scratch,
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch,
                            c->pcount, &c->ctrl.p->toi_overflow, s));
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
@@ -871,9 +872,9 @@ int apply_pins_once(ando_ctx c, int nb) {
 // state untouched (the move kernels check the flag): grow the buffer and run
 // the pass again.
 int grow_toi_candidates(ando_ctx c, int need) {
-  const size_t n = std::max<size_t>(2 * size_t(need), 2 * c->pair_scratch.n);
+  const size_t n = std::max<size_t>(2 * size_t(need), 2 * c->toi_scratch.n);
   if (need < 0 || n > (size_t(1) << 26)) return fail(ANDO_ERR_CAPACITY, "more than 64M time-of-impact candidate pairs");
-  CK(c->pair_scratch.reserve(n));
+  CK(c->toi_scratch.reserve(n));
   return ANDO_OK;
 }
 
@@ -1310,7 +1311,8 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     // candidate pairs: about two per vertex and four per edge on a flat
     // sheet; start at twice that so growth (a reallocation and a redone
     // pass) is rare
-    CK(c->pair_scratch.reserve(4ull * V + 8ull * c->E + 1024));
+    CK(c->pair_scratch.resize_exact(4ull * V + 8ull * c->E + 1024));
+    CK(c->toi_scratch.resize_exact(4ull * V + 8ull * c->E + 1024));
   }
   CK(c->el_a.reserve(nnzb)); CK(c->el_b.reserve(nnzb)); CK(c->g_el.reserve(3ull * V));
   // per-vertex / per-slot work buffers
@@ -1735,6 +1737,16 @@ int32_t ando_ctx_pcg_shape(ando_ctx c, int32_t learned, int32_t* count, int32_t*
     shape[2] = set ? c->shape[learned].unroll : 0;
   }
   if (tune_ms) *tune_ms = c->tune_ms;
+  return ANDO_OK;
+}
+
+int32_t ando_ctx_set_pair_capacity(ando_ctx c, int32_t pairs) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (pairs < 1) return fail(ANDO_ERR_INVALID, "pair capacity must be positive");
+  CK(cudaStreamSynchronize(c->stream));
+  CK(c->pair_scratch.resize_exact(size_t(pairs)));
+  CK(c->toi_scratch.resize_exact(size_t(pairs)));
   return ANDO_OK;
 }
 

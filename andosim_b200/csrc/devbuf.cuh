@@ -25,6 +25,13 @@ template <class T> struct DevBuf {
     if (e == cudaSuccess) n = c;
     return e;
   }
+  // exactly `count` elements (at least one), contents dropped
+  cudaError_t resize_exact(size_t count) {
+    if (p) { cudaFree(p); p = nullptr; n = 0; }
+    cudaError_t e = cudaMalloc(&p, (count ? count : 1) * sizeof(T));
+    if (e == cudaSuccess) n = count ? count : 1;
+    return e;
+  }
   cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
     cudaError_t e = reserve(count);
     if (e != cudaSuccess || count == 0) return e;

@@ -276,6 +276,14 @@ ANDO_API int32_t ando_ctx_select_pcg_shape(ando_ctx ctx, int32_t learned, int32_
  * solve of the mesh). `tune_ms` (may be null): device time spent timing. */
 ANDO_API int32_t ando_ctx_pcg_shape(ando_ctx ctx, int32_t learned, int32_t* count, int32_t* shape, double* tune_ms);
 
+/* Capacity, in candidate pairs, of the context's broad-phase candidate
+ * buffers (contact and time-of-impact passes). They grow on demand (a larger
+ * buffer and the pass redone, with the same result), so this only sets where
+ * they start: a caller short of device memory can start small. A mesh upload
+ * resets them to their default size (about 4 per vertex + 8 per edge). No
+ * reference counterpart. */
+ANDO_API int32_t ando_ctx_set_pair_capacity(ando_ctx ctx, int32_t pairs);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
  * callers that time or order work around the library's. */
 ANDO_API int32_t ando_ctx_stream(ando_ctx ctx, void** stream);
