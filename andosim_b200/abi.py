@@ -143,6 +143,7 @@ def lib() -> C.CDLL:
     L.ando_apply_gravity.restype = I32; L.ando_apply_gravity.argtypes = [P, pd, D]
     L.ando_step.restype = I32
     L.ando_step.argtypes = [P, C.POINTER(Params), C.POINTER(Pin), I32, C.POINTER(Wall), I32, C.POINTER(Rigid), I32, C.POINTER(StepStats)]
+    L.ando_step_batch.restype = I32; L.ando_step_batch.argtypes = [C.POINTER(BatchItem), I32, I32]
     L.ando_eval_system.restype = I32
     L.ando_eval_system.argtypes = [P, C.POINTER(Params), C.POINTER(Pin), I32, C.POINTER(Wall), I32, C.POINTER(Rigid), I32]
     L.ando_compute_contacts.restype = I32
@@ -477,6 +478,34 @@ def precond_init_weights(seed: int = 0) -> np.ndarray:
     w = np.empty(precond_num_params(), dtype=np.float32)
     _check(lib().ando_precond_init_weights(C.c_uint64(seed), _fptr(w), len(w)), "ando_precond_init_weights")
     return w
+
+
+class BatchItem(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("params", C.POINTER(Params)), ("pins", C.POINTER(Pin)), ("num_pins", C.c_int32),
+                ("walls", C.POINTER(Wall)), ("num_walls", C.c_int32), ("rigids", C.POINTER(Rigid)), ("num_rigids", C.c_int32),
+                ("stats", C.POINTER(StepStats)), ("status", C.c_int32)]
+
+
+def step_batch(scenes: Sequence["Scene"], params: Sequence[Params], pins: Sequence, walls: Sequence, threads: int = 0) -> List[dict]:
+    """One ando_step_batch call: scene i steps with params[i], pins[i] ([(vertex, target)]) and walls[i]
+    ([(normal, offset, gap)]); the scenes run concurrently. Returns each scene's step statistics."""
+    n = len(scenes)
+    items = (BatchItem * n)()
+    keep = []
+    stats = [StepStats() for _ in range(n)]
+    for k, S in enumerate(scenes):
+        pa, wa = Scene._constraints(pins[k], list(walls[k]))
+        keep += [pa, wa]
+        items[k].ctx = S.ctx
+        items[k].params = C.pointer(params[k])
+        items[k].pins = pa.ctypes.data_as(C.POINTER(Pin))
+        items[k].num_pins = len(pa)
+        items[k].walls = C.cast(wa, C.POINTER(Wall))
+        items[k].num_walls = len(walls[k])
+        items[k].num_rigids = 0
+        items[k].stats = C.pointer(stats[k])
+    _check(lib().ando_step_batch(items, n, threads), "ando_step_batch")
+    return [st.as_dict() for st in stats]
 
 
 class Trainer:

@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1710,6 +1712,42 @@ int32_t ando_profile_read(ando_ctx c, ando_profile* out) {
   CK(cudaStreamSynchronize(c->stream));
   c->collect();
   *out = c->profile;
+  return ANDO_OK;
+}
+
+int32_t ando_step_batch(ando_batch_item* items, int32_t count, int32_t threads) {
+  if (count < 0 || (count && !items)) return fail(ANDO_ERR_INVALID, "batch arguments");
+  if (count == 0) return ANDO_OK;
+  {
+    std::vector<ando_ctx> seen;
+    for (int i = 0; i < count; ++i) {
+      if (!items[i].ctx) return fail(ANDO_ERR_INVALID, "batch item without a context");
+      seen.push_back(items[i].ctx);
+    }
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) return fail(ANDO_ERR_INVALID, "a context appears twice in the batch");
+  }
+  int nt = threads > 0 ? threads : count;
+  nt = std::max(1, std::min({nt, count, 16}));
+  std::atomic<int> next{0};
+  std::vector<std::string> msgs(count);  // the error text is per host thread: keep each item's
+  auto work = [&]() {
+    for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1)) {
+      ando_batch_item& it = items[i];
+      it.status = ando_step(it.ctx, it.params, it.pins, it.num_pins, it.walls, it.num_walls, it.rigids, it.num_rigids, it.stats);
+      if (it.status != ANDO_OK) msgs[i] = ando_last_error();
+    }
+  };
+  if (nt == 1) work();
+  else {
+    std::vector<std::thread> pool;
+    pool.reserve(nt - 1);
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+  }
+  for (int i = 0; i < count; ++i)
+    if (items[i].status != ANDO_OK) return fail(items[i].status, "batch item " + std::to_string(i) + ": " + msgs[i]);
   return ANDO_OK;
 }
 

@@ -4,6 +4,8 @@
 // Every reduction is in a fixed order: per-CTA partials over a fixed grid,
 // summed CTA by CTA; scatters to vertices are gathers through the pattern's
 // transpose slots. Forward and backward are therefore bitwise reproducible.
+#include <atomic>
+
 #include <cuda_bf16.h>
 
 #include "learned.cuh"
@@ -519,13 +521,13 @@ __global__ void k_adam(float* w, float* m1, float* m2, const float* g, int n, fl
 
 void gemm(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* M, int N, const float* bias,
           const float* R1, int ldr1, const float* R2, int ldr2, float* Q, float* Y, int relu, cudaStream_t s) {
-  static unsigned attr = 0;  // one bit per device
+  static std::atomic<unsigned> attr{0};  // one bit per device (steps of several contexts may run on host threads)
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 32 && !(attr & (1u << dev))) {
+  if (dev < 32 && !(attr.load() & (1u << dev))) {
     cudaFuncSetAttribute(k_gemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_gemm<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    attr |= 1u << dev;
+    attr.fetch_or(1u << dev);
   }
   int K = K1 + K2;
   size_t smem = sizeof(float) * (size_t(K) * N + 64 * (K + 1));

@@ -11,6 +11,8 @@
 // product is exact in FP32, so the layer keeps FP32-level accuracy with the
 // BF16 weights, and three MMAs per K step cost nothing on a layer that is
 // bound by reading its FP32 inputs.
+#include <atomic>
+
 #include <cuda_bf16.h>
 
 #include "learned.cuh"
@@ -228,13 +230,13 @@ cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float*
   auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
   if (!a16(Y) || (Q && !a16(Q)) || (R1 && !a16(R1))) return cudaErrorInvalidValue;  // float4 epilogue
   if (!a16(X1) || (ld1 & 3) || (K2 && (!a16(X2) || (ld2 & 3)))) return cudaErrorInvalidValue;  // float4 staging
-  static unsigned attr = 0;  // one bit per device
+  static std::atomic<unsigned> attr{0};  // one bit per device (steps of several contexts may run on host threads)
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 32 && !(attr & (1u << dev))) {
+  if (dev < 32 && !(attr.load() & (1u << dev))) {
     cudaError_t e = cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gemm_tc_smem(128)));
     if (e != cudaSuccess) return e;
-    attr |= 1u << dev;
+    attr.fetch_or(1u << dev);
   }
   const int K = K1 + K2;
   k_gemm_tc<<<(V + TC_M - 1) / TC_M, TC_THREADS, gemm_tc_smem(K), s>>>(V, X1, ld1, K1, X2, ld2, K2, W, bias, R1, ldr1, Q, Y, relu, err);

@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--full-steps", type=int, default=240, help="frames of the full-length CORRECTED comparison")
     ap.add_argument("--refresh", type=int, default=1, help="Newton iterations between evaluations of the preconditioner network")
     ap.add_argument("--weights", default=None, help="learned preconditioner weights (.npy); default: the shipped C4 weights")
+    ap.add_argument("--c3-frames", type=int, default=5, help="timed frames of the batched 64-scene comparison (0: skip)")
     return ap.parse_args()
 
 
@@ -363,6 +364,57 @@ def e2e_run(args, sc, local, flush, pg, weights):
             "d2h_bytes_per_step": 24 * sc.num_vertices}                       # positions (FP64) read back
 
 
+def c3_run(args, local, seed=0):
+    """The batched workload: 64 uneven cloths (16..128 per side, 1-4 corner pins,
+    log-uniform E), CORRECTED step with block Jacobi. Scene by scene (one host
+    thread, one scene at a time) against ando_step_batch (the scenes' contexts
+    stepping concurrently on their own streams). Each call returns when its
+    scenes' steps are done; the wall time of whole frames is measured with the
+    device idle on both sides. Both sets start from the same state and must end
+    with the same bits."""
+    import torch
+
+    from andosim_b200 import abi, scenes
+
+    scs = scenes.c3(seed=seed, scenes=64)
+    params = [abi.make_params(sc.params, semantics="corrected") for sc in scs]
+    sets = {m: [abi.Scene(sc.vertices, sc.triangles, sc.material, device=local) for sc in scs] for m in ("sequential", "batched")}
+    times = {m: 0.0 for m in sets}
+    newton = {m: 0 for m in sets}
+    warm = 2
+    for f in range(warm + args.c3_frames):
+        for mode, S in sets.items():
+            for s_, sc, p in zip(S, scs, params):
+                s_.apply_gravity(sc.gravity, p.dt)
+            torch.cuda.synchronize(local)
+            t0 = time.perf_counter()
+            if mode == "sequential":
+                st = [s_.step(p, sc.pins_at(f), sc.walls) for s_, sc, p in zip(S, scs, params)]
+            else:
+                st = abi.step_batch(S, params, [sc.pins_at(f) for sc in scs], [sc.walls for sc in scs], threads=16)
+            torch.cuda.synchronize(local)
+            if f >= warm:
+                times[mode] += time.perf_counter() - t0
+                newton[mode] += sum(x["newton_iters"] for x in st)
+    same = True
+    for a, b in zip(sets["sequential"], sets["batched"]):
+        xa, va = a.download()
+        xb, vb = b.download()
+        same = same and bool(np.array_equal(xa, xb) and np.array_equal(va, vb))
+    for S in sets.values():
+        for s_ in S:
+            s_.close()
+    nf = max(args.c3_frames, 1)
+    out = {"workload": "c3_64_scenes_16_to_128", "vertices": int(sum(sc.num_vertices for sc in scs)), "frames": args.c3_frames,
+           "semantics": "CORRECTED", "preconditioner": "block_jacobi", "timing": "host wall clock around whole batch frames, device idle before and after",
+           "identical_results": same}
+    for mode in sets:
+        out[mode] = {"scene_frames_per_s": round(64 * nf / max(times[mode], 1e-9), 1), "ms_per_batch_frame": round(1e3 * times[mode] / nf, 3),
+                     "newton_iters_per_frame": round(newton[mode] / (64 * nf), 3)}
+    out["speedup"] = round(times["sequential"] / max(times["batched"], 1e-9), 3)
+    return out
+
+
 def run_ours(args, rank, world, local, pg):
     import torch
 
@@ -441,6 +493,8 @@ def run_ours(args, rank, world, local, pg):
     if args.reference_steps > 0:
         out["reference_semantics"] = reference_semantics_run(args, sc, local, flush, pg)
     out["e2e"] = e2e_run(args, sc, local, flush, pg, weights)
+    if args.c3_frames > 0:
+        out["c3_batched"] = c3_run(args, local, seed=rank)
     return out, sc
 
 

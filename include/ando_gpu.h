@@ -264,6 +264,25 @@ ANDO_API int32_t ando_broad_phase(ando_ctx ctx, int32_t kind, double pad, int32_
 ANDO_API int32_t ando_profile_enable(ando_ctx ctx, int32_t enable);
 ANDO_API int32_t ando_profile_read(ando_ctx ctx, ando_profile* out);
 
+/* Many scenes in one call: item i runs ando_step(ctx, params, pins, walls,
+ * rigids, stats) and stores its status. The contexts (all distinct) step
+ * concurrently from up to `threads` host threads (0: one per item, at most
+ * 16), each on its own CUDA stream, so small scenes share the GPU. Every
+ * scene's result is the one its own ando_step call gives. Returns ANDO_OK
+ * when every item did, else the first failing item's status. Replaces the
+ * caller's loop over scenes (the reference steps one scene per call,
+ * integrator.h:33-35). */
+typedef struct {
+  ando_ctx ctx;
+  const ando_params* params;
+  const ando_pin* pins; int32_t num_pins;
+  const ando_wall* walls; int32_t num_walls;
+  ando_rigid* rigids; int32_t num_rigids;
+  ando_step_stats* stats;                 /* may be null */
+  int32_t status;                         /* out */
+} ando_batch_item;
+ANDO_API int32_t ando_step_batch(ando_batch_item* items, int32_t count, int32_t threads);
+
 /* Launch shape of the scaled PCG (CORRECTED semantics) for the current mesh,
  * per preconditioner (learned = 0: block Jacobi, 1: learned). The candidates
  * (threads per CTA, CTAs, column slots loaded ahead) all give the same result
