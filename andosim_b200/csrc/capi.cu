@@ -157,10 +157,11 @@ struct ando_ctx_s {
   DevBuf<int> vorder, eorder;      // vertices / edges in Morton order of their rest positions (query order)
   int E = 0;
   Lbvh bvh_tri, bvh_edge;
-  DevBuf<int2> pairs, pair_scratch;
+  DevBuf<int2> pairs, pair_scratch, pair_scratch_ee;
   DevBuf<int2> toi_scratch;        // candidates of the time-of-impact passes (grown on overflow)
   DevBuf<unsigned long long> pk0, pk1;
-  DevBuf<int> pcount;
+  DevBuf<int> pcount, pcount_ee;
+  int* counts_host = nullptr;      // pinned: both contact queries' counters, read in one round trip
 
   // rigid bodies
   DevBuf<RigidDev> bodies_dev;
@@ -179,6 +180,7 @@ struct ando_ctx_s {
     for (auto* b : body_tris) delete b;
     if (ctrl_host) cudaFreeHost(ctrl_host);
     if (ctrl_host_count) cudaFreeHost(ctrl_host_count);
+    if (counts_host) cudaFreeHost(counts_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -526,12 +528,30 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
   {
     Phase ph(c, ANDO_PHASE_SETUP);
     long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
+    // both queries launched back to back, both counters read in one round trip
     CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
-    CK(c->bvh_tri.query_contacts(c->x.p, 0, nullptr, c->V, float(gap_max), gap_max, c->pairs, c->pair_scratch, c->pk0, c->pk1, c->pcount,
-                                 c->cub_tmp, &nvt, s));
+    CK(c->bvh_tri.contacts_launch(c->x.p, 0, nullptr, c->V, float(gap_max), gap_max, c->pair_scratch, c->pcount, s));
     CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
-    CK(c->bvh_edge.query_contacts(c->x.p, 1, c->edges.p, c->E, float(gap_max), gap_max, c->pairs_ee, c->pair_scratch, c->pk0, c->pk1,
-                                  c->pcount, c->cub_tmp, &nee, s));
+    CK(c->bvh_edge.contacts_launch(c->x.p, 1, c->edges.p, c->E, float(gap_max), gap_max, c->pair_scratch_ee, c->pcount_ee, s));
+    int* h = c->counts_host;
+    CK(cudaMemcpyAsync(h, c->pcount.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h + 3, c->pcount_ee.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int kind = 0; kind < 2; ++kind) {
+      Lbvh& B = kind == 0 ? c->bvh_tri : c->bvh_edge;
+      DevBuf<int2>& scr = kind == 0 ? c->pair_scratch : c->pair_scratch_ee;
+      DevBuf<int>& cnt = kind == 0 ? c->pcount : c->pcount_ee;
+      int* hk = h + 3 * kind;
+      for (int attempt = 0; hk[0] > int(scr.n); ++attempt) {  // candidates overflowed: grow, launch again
+        if (attempt == 2 || hk[0] > (1 << 26)) return fail(ANDO_ERR_CAPACITY, "contact candidates overflowed");
+        CK(scr.reserve(size_t(hk[0]) + size_t(hk[0]) / 4));
+        CK(B.contacts_launch(c->x.p, kind, kind ? c->edges.p : nullptr, kind ? c->E : c->V, float(gap_max), gap_max, scr, cnt, s));
+        CK(cudaMemcpyAsync(hk, cnt.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+      }
+    }
+    CK(c->bvh_tri.contacts_finish(h, c->pairs, c->pk0, c->pk1, c->cub_tmp, &nvt, s));
+    CK(c->bvh_edge.contacts_finish(h + 3, c->pairs_ee, c->pk0, c->pk1, c->cub_tmp, &nee, s));
     ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   }
   int nr = 0;
@@ -1170,6 +1190,7 @@ int32_t ando_ctx_create(int32_t device, ando_ctx* out) {
   if (e == cudaSuccess) e = cudaMallocHost(&c->ctrl_host, sizeof(Ctrl));
   if (e == cudaSuccess) e = cudaMallocHost(&c->sctl_host, sizeof(StepCtl));
   if (e == cudaSuccess) e = cudaMallocHost(&c->ctrl_host_count, sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->counts_host, 8 * sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap2, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap3, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = c->sctl.reserve(1);
@@ -1314,6 +1335,7 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     // sheet; start at twice that so growth (a reallocation and a redone
     // pass) is rare
     CK(c->pair_scratch.resize_exact(4ull * V + 8ull * c->E + 1024));
+    CK(c->pair_scratch_ee.resize_exact(4ull * V + 8ull * c->E + 1024));
     CK(c->toi_scratch.resize_exact(4ull * V + 8ull * c->E + 1024));
   }
   CK(c->el_a.reserve(nnzb)); CK(c->el_b.reserve(nnzb)); CK(c->g_el.reserve(3ull * V));
@@ -1784,6 +1806,7 @@ int32_t ando_ctx_set_pair_capacity(ando_ctx c, int32_t pairs) {
   if (pairs < 1) return fail(ANDO_ERR_INVALID, "pair capacity must be positive");
   CK(cudaStreamSynchronize(c->stream));
   CK(c->pair_scratch.resize_exact(size_t(pairs)));
+  CK(c->pair_scratch_ee.resize_exact(size_t(pairs)));
   CK(c->toi_scratch.resize_exact(size_t(pairs)));
   return ANDO_OK;
 }

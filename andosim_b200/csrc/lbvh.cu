@@ -461,6 +461,42 @@ cudaError_t Lbvh::query_contacts(const double* x, int kind, const int* qprims, i
   return run_query(*this, gap < 0.0 ? 0.0 : gap, x, nullptr, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
 }
 
+cudaError_t Lbvh::contacts_launch(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& scratch,
+                                  DevBuf<int>& counter, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = counter.reserve(3))) return e;
+  if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
+  if (n == 0 || nq == 0) return cudaSuccess;
+  if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
+  if ((e = surv.reserve(scratch.n))) return e;
+  const int cap = int(scratch.n);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, nullptr, qprims, qorder, kind, nq, pad, prims, n, order.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, gap, surv.p, counter.p + 2);
+  launches += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t Lbvh::contacts_finish(const int count[3], DevBuf<int2>& out, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
+                                  DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
+  cudaError_t e;
+  *npairs = 0;
+  if (count[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
+  const int m = count[2];
+  if (m < 0 || m > int(surv.n)) return cudaErrorInvalidValue;
+  if (m == 0) return cudaSuccess;
+  if ((e = k0.reserve(m))) return e;
+  if ((e = k1.reserve(m))) return e;
+  if ((e = out.reserve(m))) return e;
+  k_pair_keys<<<nblk(m), TPB, 0, s>>>(surv.p, m, k0.p);
+  launches += 1;
+  size_t bytes = 0;
+  if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.p, k1.p, surv.p, out.p, m, 0, 64, s))) return e;
+  if ((e = tmp.reserve(bytes))) return e;
+  if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, k0.p, k1.p, surv.p, out.p, m, 0, 64, s))) return e;
+  *npairs = m;
+  return cudaGetLastError();
+}
+
 cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, double eta_min,
                             double near, unsigned long long* toi, DevBuf<int2>& scratch, DevBuf<int>& counter, int* overflow,
                             cudaStream_t s) {

@@ -48,6 +48,16 @@ struct Lbvh {
   cudaError_t query_contacts(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& out,
                              DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
                              DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
+  // query_contacts in two halves, so that several queries share one host
+  // round trip: the launch (traversal and narrow phase; counter[0] = box
+  // candidates, counter[1] = stack overflows, counter[2] = contacts) and,
+  // once the caller has read the counter, the sort of the contacts into
+  // `out`. A launch whose candidates overflowed `scratch` (counter[0] >
+  // scratch.n at launch) must be grown and launched again before finishing.
+  cudaError_t contacts_launch(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& scratch,
+                              DevBuf<int>& counter, cudaStream_t s);
+  cudaError_t contacts_finish(const int count[3], DevBuf<int2>& out, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
+                              DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
   // min over the swept-box candidates (x -> x1 = x + ext, no pad) of the
   // pair's conservative time of impact, min-reduced into *toi (IEEE bits of a
   // non-negative double) on the device, with no host round trip: the
