@@ -155,6 +155,8 @@ def lib() -> C.CDLL:
     L.ando_profile_read.restype = I32; L.ando_profile_read.argtypes = [P, C.POINTER(Profile)]
     L.ando_ctx_stream.restype = I32; L.ando_ctx_stream.argtypes = [P, C.POINTER(C.c_void_p)]
     L.ando_ctx_select_pcg_shape.restype = I32; L.ando_ctx_select_pcg_shape.argtypes = [P, I32, I32]
+    L.ando_ctx_select_assembly_tpb.restype = I32; L.ando_ctx_select_assembly_tpb.argtypes = [P, I32]
+    L.ando_ctx_assembly_tpb.restype = I32; L.ando_ctx_assembly_tpb.argtypes = [P, pi, pi]
     L.ando_ctx_set_pair_capacity.restype = I32; L.ando_ctx_set_pair_capacity.argtypes = [P, I32]
     L.ando_ctx_pcg_shape.restype = I32; L.ando_ctx_pcg_shape.argtypes = [P, I32, pi, pi, pd]
     L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
@@ -388,6 +390,15 @@ class Scene:
     def set_pair_capacity(self, pairs: int):
         """Start the broad-phase candidate buffers at `pairs` (they grow on demand)."""
         _check(lib().ando_ctx_set_pair_capacity(self.ctx, pairs), "ando_ctx_set_pair_capacity")
+
+    def select_assembly_tpb(self, index: int = -1):
+        """Fix scaled-assembly block-size candidate `index` (-1: autotune on the next first assembly)."""
+        _check(lib().ando_ctx_select_assembly_tpb(self.ctx, index), "ando_ctx_select_assembly_tpb")
+
+    def assembly_tpb(self) -> dict:
+        n = C.c_int32(); t = C.c_int32()
+        _check(lib().ando_ctx_assembly_tpb(self.ctx, C.byref(n), C.byref(t)), "ando_ctx_assembly_tpb")
+        return dict(candidates=n.value, tpb=t.value)
 
     def select_pcg_shape(self, learned: bool, index: int = -1):
         """Fix scaled-PCG launch candidate `index` (-1: autotune on the next first solve)."""

@@ -90,6 +90,7 @@ struct ando_ctx_s {
   // autotuned on the first solve of a mesh (choice < 0) or a fixed candidate
   PcgShape shape[2];
   int shape_V[2] = {-1, -1}, shape_choice[2] = {-1, -1};
+  int asm_tpb = 256, asm_V = -1, asm_choice = -1;  // scaled assembly block size (tuned like the PCG shape)
   double dt2inv = 0.0;             // of the last assembled system
   double gap_max = 1e-3;           // contact activation distance of the current step
 
@@ -640,13 +641,45 @@ int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, i
 // Assembly of the CORRECTED Newton system: the unscaled BSR values (kept for
 // ando_last_system), the block Cholesky factors of the diagonal and the
 // scaled system A^ = L^-1 A L^-T with its right-hand side.
-void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
+// Threads per block of the scaled assembly (k_diag_factor, k_assemble_scaled):
+// on the first assembly of a mesh every candidate runs once more, timed with
+// CUDA events, and the fastest is kept (one thread per vertex / slot and no
+// shared sums, so every block size gives the same bits).
+constexpr int ASM_TPB[3] = {128, 256, 512};
+
+void enqueue_scaled_assembly_tpb(ando_ctx c, const StepParams& sp, cudaStream_t s, int tpb) {
   MeshDev m = c->mesh_dev();
   c->dt2inv = sp.dt2inv;
   launch_diag_factor(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->g.p, c->Linv.p, c->Lf.p, c->bhat.p,
-                     c->chol_ok.p, c->ctrl.p, s);
+                     c->chol_ok.p, c->ctrl.p, s, tpb);
   launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p, c->val.p,
-                         c->valh.p, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s);
+                         c->valh.p, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s, tpb);
+}
+
+void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
+  if (c->asm_V != c->V) {
+    c->asm_V = c->V;
+    c->asm_tpb = c->asm_choice >= 0 ? ASM_TPB[c->asm_choice] : 256;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->asm_choice < 0 && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+      float best = 1e30f;
+      enqueue_scaled_assembly_tpb(c, sp, s, 256);  // warm-up
+      for (int tpb : ASM_TPB) {
+        cudaEventRecord(e0, s);
+        enqueue_scaled_assembly_tpb(c, sp, s, tpb);
+        cudaEventRecord(e1, s);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+          c->tune_ms += ms;
+          if (ms < best) { best = ms; c->asm_tpb = tpb; }
+        }
+        cudaGetLastError();
+      }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+  enqueue_scaled_assembly_tpb(c, sp, s, c->asm_tpb);
   if (c->nx) launch_extra_merge(c->contacts.p, c->xent.p, c->xk1.p, c->xi1.p, c->xheads.p, c->nx, c->nx_raw, c->fixed.p, sp, c->Linv.p,
                                 nullptr, nullptr, nullptr, c->xvalh.p, s);
 }
@@ -1295,6 +1328,7 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   cudaStream_t s = c->stream;
   c->V = V; c->T = T; c->nnzb = nnzb;
   c->shape_V[0] = c->shape_V[1] = -1;
+  c->asm_V = -1;
   CK(c->spart.reserve(pcg_scaled_partials(V)));
   c->S_ready = false;
   c->mu = mat->youngs_modulus / (2.0 * (1.0 + mat->poisson_ratio));
@@ -1808,6 +1842,23 @@ int32_t ando_ctx_set_pair_capacity(ando_ctx c, int32_t pairs) {
   CK(c->pair_scratch.resize_exact(size_t(pairs)));
   CK(c->pair_scratch_ee.resize_exact(size_t(pairs)));
   CK(c->toi_scratch.resize_exact(size_t(pairs)));
+  return ANDO_OK;
+}
+
+int32_t ando_ctx_select_assembly_tpb(ando_ctx c, int32_t index) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (index < -1 || index >= 3) return fail(ANDO_ERR_INVALID, "assembly candidate index");
+  c->asm_choice = index;
+  c->asm_V = -1;
+  return ANDO_OK;
+}
+
+int32_t ando_ctx_assembly_tpb(ando_ctx c, int32_t* count, int32_t* tpb) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (count) *count = 3;
+  if (tpb) *tpb = c->mesh_ready && c->asm_V == c->V ? c->asm_tpb : 0;
   return ANDO_OK;
 }
 

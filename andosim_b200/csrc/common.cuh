@@ -175,8 +175,7 @@ __device__ inline bool grid_sync_ar(unsigned long long* arrivals, unsigned int n
   ++epoch;
   if (threadIdx.x == 0) {
     const unsigned long long target = (unsigned long long)epoch * nblocks;
-    unsigned long long prior;
-    asm volatile("atom.add.release.gpu.u64 %0, [%1], 1;" : "=l"(prior) : "l"(arrivals) : "memory");
+    asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(arrivals) : "memory");
     long long polls = 0;
     while (true) {
       unsigned long long v;

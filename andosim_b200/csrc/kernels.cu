@@ -1258,14 +1258,14 @@ void launch_assemble(const MeshDev& m, const unsigned char* sflags, const Strain
 }
 void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                         const unsigned char* fixed, const double* g, double* Linv, float* Lf, float* bhat, unsigned char* chol_ok,
-                        const Ctrl* ctrl, cudaStream_t s) {
-  if (m.V) k_diag_factor<<<nblk(m.V), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, g, Linv, Lf, bhat, chol_ok, ctrl);
+                        const Ctrl* ctrl, cudaStream_t s, int tpb) {
+  if (m.V) k_diag_factor<<<nblk(m.V, tpb), tpb, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, g, Linv, Lf, bhat, chol_ok, ctrl);
 }
 void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                             const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s) {
-  if (m.nnzb) k_assemble_scaled<<<nblk(m.nnzb), TPB, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh,
-                                                             sell_base, valh_sell, ctrl);
+                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s, int tpb) {
+  if (m.nnzb) k_assemble_scaled<<<nblk(m.nnzb, tpb), tpb, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh,
+                                                                  sell_base, valh_sell, ctrl);
 }
 void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s) {
   if (n) k_extra_key64<<<nblk(n), TPB, 0, s>>>(xent, xkeys, n, key, idx);

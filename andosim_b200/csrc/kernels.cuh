@@ -44,12 +44,14 @@ void launch_pin_heads(const int* pin_vertex, int num_pins, int* pin_head, cudaSt
 void launch_assemble(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                      const unsigned char* fixed, float* val, float* precond, const Ctrl* ctrl, cudaStream_t s);
 // scaled system (CORRECTED): L = chol(A_ii), A^ = L^-1 A L^-T (kernels.cu)
+// tpb: threads per block (a tuning knob; one thread per vertex / slot, so the
+// results do not depend on it)
 void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                         const unsigned char* fixed, const double* g, double* Linv, float* Lf, float* bhat, unsigned char* chol_ok,
-                        const Ctrl* ctrl, cudaStream_t s);
+                        const Ctrl* ctrl, cudaStream_t s, int tpb = 256);
 void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                             const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s);
+                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s, int tpb = 256);
 void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s);
 void launch_run_heads(const unsigned long long* key, int n, int* flags, cudaStream_t s);
 void launch_extra_merge(const ContactDev* c, const ContactEntry* xent, const unsigned long long* key, const int* idx, const int* heads, int nu,

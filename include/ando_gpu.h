@@ -303,6 +303,15 @@ ANDO_API int32_t ando_ctx_pcg_shape(ando_ctx ctx, int32_t learned, int32_t* coun
  * reference counterpart. */
 ANDO_API int32_t ando_ctx_set_pair_capacity(ando_ctx ctx, int32_t pairs);
 
+/* Threads per block of the CORRECTED block-scaled assembly (candidates 128,
+ * 256, 512; one thread per vertex or block slot, so every candidate gives the
+ * same bits). Index -1 (default): the first assembly of a mesh times every
+ * candidate and keeps the fastest; 0..2 fixes one. ando_ctx_assembly_tpb
+ * returns the number of candidates and the block size in use (0 before the
+ * first assembly of the mesh). No reference counterpart. */
+ANDO_API int32_t ando_ctx_select_assembly_tpb(ando_ctx ctx, int32_t index);
+ANDO_API int32_t ando_ctx_assembly_tpb(ando_ctx ctx, int32_t* count, int32_t* tpb);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
  * callers that time or order work around the library's. */
 ANDO_API int32_t ando_ctx_stream(ando_ctx ctx, void** stream);
