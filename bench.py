@@ -64,7 +64,11 @@ def parse():
 
 
 # ---------------------------------------------------------------- distributed
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend=None):
+    """One process per GPU (RANK / WORLD_SIZE / LOCAL_RANK from torchrun). The
+    ranks run independent replicas (seeded by rank); the only collectives are
+    the barriers around timed regions and the max over ranks of each time.
+    NCCL on GPUs; gloo when given (the CPU tests of this logic)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -74,19 +78,23 @@ def dist_setup(n_gpus):
         import torch.distributed as dist
         from datetime import timedelta
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        backend = backend or "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
         pg = True
     return rank, world, local, pg
 
 
 def dist_max(x, pg):
+    """Max of x over the ranks (the job's time is its slowest rank's)."""
     if not pg:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
