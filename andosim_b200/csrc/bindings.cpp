@@ -22,6 +22,7 @@
 #include <stdexcept>
 #include <string>
 #include <unordered_set>
+#include <cstring>
 #include <vector>
 
 #include "../../include/ando_gpu.h"
@@ -39,6 +40,7 @@ void check(int32_t rc, const char* what) {
 }
 
 struct V3 { double x = 0, y = 0, z = 0; };
+static_assert(sizeof(V3) == 3 * sizeof(double), "V3 must be three packed doubles (bulk copies of state arrays)");
 inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 inline V3 mul(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
@@ -248,7 +250,7 @@ struct State {
   void mark_device_newer() { dev_x = dev_v = start_stale = true; }
   void unpack(std::vector<V3>& dst) {
     dst.resize(nv());
-    for (size_t i = 0; i < nv(); ++i) dst[i] = {stage[3 * i], stage[3 * i + 1], stage[3 * i + 2]};
+    std::memcpy(static_cast<void*>(dst.data()), stage.data(), sizeof(double) * 3 * nv());  // V3 is three packed doubles
   }
   void sync_x() {
     if (!dev_x || !ctx) return;

@@ -163,6 +163,8 @@ struct ando_ctx_s {
   DevBuf<unsigned long long> pk0, pk1;
   DevBuf<int> pcount, pcount_ee;
   int* counts_host = nullptr;      // pinned: both contact queries' counters, read in one round trip
+  void* stage_host = nullptr;      // pinned staging of state downloads
+  size_t stage_bytes = 0;
 
   // rigid bodies
   DevBuf<RigidDev> bodies_dev;
@@ -182,6 +184,7 @@ struct ando_ctx_s {
     if (ctrl_host) cudaFreeHost(ctrl_host);
     if (ctrl_host_count) cudaFreeHost(ctrl_host_count);
     if (counts_host) cudaFreeHost(counts_host);
+    if (stage_host) cudaFreeHost(stage_host);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1464,9 +1467,23 @@ int32_t ando_state_download(ando_ctx c, double* x, double* v, int32_t V) {
   if (rc) return rc;
   if (!c->state_ready) return fail(ANDO_ERR_STATE, "state not uploaded");
   if (V != c->V) return fail(ANDO_ERR_INVALID, "vertex count mismatch");
-  if (x) CK(cudaMemcpyAsync(x, c->x.p, sizeof(double) * 3ull * V, cudaMemcpyDeviceToHost, c->stream));
-  if (v) CK(cudaMemcpyAsync(v, c->v.p, sizeof(double) * 3ull * V, cudaMemcpyDeviceToHost, c->stream));
+  // through the context's page-locked staging buffer: a device -> pageable
+  // copy runs several times slower than device -> pinned + a host copy
+  const size_t bytes = sizeof(double) * 3ull * V;
+  const size_t need = (x ? bytes : 0) + (v ? bytes : 0);
+  if (need > c->stage_bytes) {
+    if (c->stage_host) cudaFreeHost(c->stage_host);
+    c->stage_host = nullptr;
+    c->stage_bytes = 0;
+    CK(cudaMallocHost(&c->stage_host, need));
+    c->stage_bytes = need;
+  }
+  unsigned char* st = static_cast<unsigned char*>(c->stage_host);
+  if (x) CK(cudaMemcpyAsync(st, c->x.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (v) CK(cudaMemcpyAsync(st + (x ? bytes : 0), c->v.p, bytes, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (x) std::memcpy(x, st, bytes);
+  if (v) std::memcpy(v, st + (x ? bytes : 0), bytes);
   return ANDO_OK;
 }
 
