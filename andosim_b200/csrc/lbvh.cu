@@ -128,7 +128,13 @@ __global__ void k_karras(const unsigned long long* keys, int n, int* left, int* 
   int rc = (hi == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
   left[i] = lc; right[i] = rc;
   inner[i].lc = lc; inner[i].rc = rc;
+  inner[i].lmax = gamma; inner[i].rmax = hi;  // leaf ranges [lo, gamma] and [gamma + 1, hi]
   parent[lc] = i; parent[rc] = i;
+}
+
+__global__ void k_rank(const int* order, int n, int* rank) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) rank[order[p]] = p;
 }
 
 // Copy a finished node box into its parent's packed record.
@@ -192,7 +198,8 @@ __device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, in
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
 // prims = edges, keep e1 < e2 without shared vertex.
 __global__ void k_query(const double* x, const double* x1, const int* qprims, const int* qorder, int kind, int nq, float pad, const int* prims,
-                        int n, const int* order, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap) {
+                        int n, const int* order, const int* rank, const LbvhInner* inner, const Box* nodes, int2* out, int* count,
+                        int cap) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < nq;
   const int q = active && qorder ? qorder[t] : t;
@@ -226,10 +233,17 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
   // the hierarchy is at most 64 levels deep, so 96 slots never overflow; an
   // overflow would be reported through count[1] instead of dropping
   // candidates silently.
+  //
+  // The edge-edge query is a self query: each pair is found from the edge
+  // that comes first in the tree's sorted leaf order (subtrees whose leaves
+  // all come before the query's own position are skipped) and reported with
+  // the lower edge index first, which is the set the q < prim rule of a full
+  // query gives.
   constexpr int STACK = 96;
   int stack[STACK];
   int sp = 0;
   const int leaf0 = n - 1;          // with one primitive the root (node 0) is its leaf
+  const int qpos = active && kind == 1 ? rank[q] : -1;
   int node = -1;
   bool single = false;              // n == 1: test the root leaf once
   if (active && n > 0) {
@@ -242,13 +256,18 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
     if (kind == 0) hit = prims[3 * prim] != q && prims[3 * prim + 1] != q && prims[3 * prim + 2] != q;
     else {
       int pa = prims[2 * prim], pc = prims[2 * prim + 1];
-      hit = q < prim && pa != qa && pa != qc && pc != qa && pc != qc;
+      hit = leaf - leaf0 > qpos && pa != qa && pa != qc && pc != qa && pc != qc;
     }
     return hit ? prim : -1;
   };
+  auto emit_pair = [&](int prim) {  // (lower, higher) edge index for the self query
+    const bool hit = prim >= 0;
+    const int a = kind == 1 && hit ? min(q, prim) : q, b = kind == 1 && hit ? max(q, prim) : prim;
+    emit(hit, a, b, out, count, cap);
+  };
   if (__any_sync(0xffffffffu, single)) {
     int prim = single && overlap(qb, nodes[0]) ? accept(0) : -1;
-    emit(prim >= 0, q, prim, out, count, cap);
+    emit_pair(prim);
   }
   while (__any_sync(0xffffffffu, node >= 0)) {
     int hl = -1, hr = -1;
@@ -259,7 +278,8 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
       bl.lo[0] = r0.x; bl.lo[1] = r0.y; bl.lo[2] = r0.z; bl.hi[0] = r0.w; bl.hi[1] = r1.x; bl.hi[2] = r1.y;
       br.lo[0] = r1.z; br.lo[1] = r1.w; br.lo[2] = r2.x; br.hi[0] = r2.y; br.hi[1] = r2.z; br.hi[2] = r2.w;
       const int l = __float_as_int(r3.x), r = __float_as_int(r3.y);
-      bool ol = overlap(qb, bl), orr = overlap(qb, br);
+      // self query: a subtree whose last leaf is at or before the query's position holds no new pair
+      bool ol = __float_as_int(r3.z) > qpos && overlap(qb, bl), orr = __float_as_int(r3.w) > qpos && overlap(qb, br);
       bool ll = l >= leaf0, lr = r >= leaf0;
       if (ol && ll) hl = accept(l);
       if (orr && lr) hr = accept(r);
@@ -273,8 +293,8 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
         }
       }
     }
-    emit(hl >= 0, q, hl, out, count, cap);
-    emit(hr >= 0, q, hr, out, count, cap);
+    emit_pair(hl);
+    emit_pair(hr);
   }
 }
 
@@ -347,6 +367,7 @@ cudaError_t Lbvh::reserve_prims(int n) {
   if ((e = parent.reserve(2 * N))) return e;
   if ((e = nodes.reserve(2 * N))) return e;
   if ((e = inner.reserve(N))) return e;
+  if ((e = rank.reserve(N))) return e;
   if ((e = arrive.reserve(N))) return e;
   if ((e = bounds.reserve(6))) return e;
   return cudaSuccess;
@@ -368,13 +389,14 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
   if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, keys_sorted.p, idx.p, order.p, n, 0, 64, s))) return e;
   if ((e = tmp.reserve(bytes))) return e;
   if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, keys.p, keys_sorted.p, idx.p, order.p, n, 0, 64, s))) return e;
+  k_rank<<<nblk(n), TPB, 0, s>>>(order.p, n, rank.p);
   if (n > 1) {
     if ((e = cudaMemsetAsync(parent.p, 0xff, sizeof(int) * (2 * n - 1), s))) return e;
     k_karras<<<nblk(n - 1), TPB, 0, s>>>(keys_sorted.p, n, left.p, right.p, parent.p, inner.p);
     if ((e = cudaMemsetAsync(arrive.p, 0, sizeof(int) * n, s))) return e;
   }
   k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p, inner.p);
-  launches += n > 1 ? 6 : 5;
+  launches += n > 1 ? 7 : 6;
   return cudaGetLastError();
 }
 
@@ -416,7 +438,7 @@ cudaError_t run_query(Lbvh& B, double gap, const double* x, const double* x1, in
     int cap = int(scratch.n);
     if (narrow && (e = B.surv.reserve(scratch.n))) return e;
     if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.inner.p, B.nodes.p, scratch.p,
+    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.rank.p, B.inner.p, B.nodes.p, scratch.p,
                                      counter.p, cap);
     B.launches += 1;
     if (narrow) {
@@ -470,7 +492,7 @@ cudaError_t Lbvh::contacts_launch(const double* x, int kind, const int* qprims, 
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   if ((e = surv.reserve(scratch.n))) return e;
   const int cap = int(scratch.n);
-  k_query<<<nblk(nq), TPB, 0, s>>>(x, nullptr, qprims, qorder, kind, nq, pad, prims, n, order.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, nullptr, qprims, qorder, kind, nq, pad, prims, n, order.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
   k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, gap, surv.p, counter.p + 2);
   launches += 2;
   return cudaGetLastError();
@@ -506,7 +528,7 @@ cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   const int cap = int(scratch.n);
   if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, prims, n, order.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, prims, n, order.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
   k_pairs_toi<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, ext, eta_min, near, toi, overflow);
   launches += 2;
   return cudaGetLastError();

@@ -10,8 +10,9 @@ namespace ando {
 
 struct LbvhBox { float lo[3], hi[3]; };
 // Internal node as the traversal reads it: both children's boxes and indices
-// in one 64-byte record (one dependent load per level instead of two).
-struct alignas(16) LbvhInner { float lbox[6], rbox[6]; int lc, rc, pad_[2]; };
+// in one 64-byte record (one dependent load per level instead of two), and
+// the last sorted leaf position under each child (prunes the self-query).
+struct alignas(16) LbvhInner { float lbox[6], rbox[6]; int lc, rc, lmax, rmax; };
 
 struct Lbvh {
   int n = 0;                    // primitives
@@ -26,6 +27,7 @@ struct Lbvh {
   DevBuf<LbvhInner> inner;      // n-1 internal nodes, child boxes packed (written by the refit)
   DevBuf<unsigned long long> keys, keys_sorted;
   DevBuf<int> idx, order, left, right, parent, arrive, bounds;
+  DevBuf<int> rank;             // sorted leaf position of each primitive (inverse of order)
   DevBuf<int2> surv;            // candidates kept by the narrow phase of query_contacts
   long long launches = 0;
 
