@@ -134,6 +134,10 @@ struct ando_ctx_s {
 
   // whole-frame CUDA graph (REFERENCE semantics without contact detection)
   cudaStream_t cap2 = nullptr, cap3 = nullptr;
+  // the edge-edge broad phase runs on `side` beside the vertex-triangle one
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  DevBuf<unsigned char> cub_tmp_side;
   DevBuf<StepCtl> sctl;
   StepCtl* sctl_host = nullptr;
   cudaGraphExec_t frame_exec = nullptr;
@@ -159,7 +163,7 @@ struct ando_ctx_s {
   int E = 0;
   Lbvh bvh_tri, bvh_edge;
   DevBuf<int2> pairs, pair_scratch, pair_scratch_ee;
-  DevBuf<int2> toi_scratch;        // candidates of the time-of-impact passes (grown on overflow)
+  DevBuf<int2> toi_scratch, toi_scratch_ee;  // candidates of the time-of-impact passes (grown on overflow)
   DevBuf<unsigned long long> pk0, pk1;
   DevBuf<int> pcount, pcount_ee;
   int* counts_host = nullptr;      // pinned: both contact queries' counters, read in one round trip
@@ -178,6 +182,9 @@ struct ando_ctx_s {
     if (sctl_host) cudaFreeHost(sctl_host);
     if (cap2) cudaStreamDestroy(cap2);
     if (cap3) cudaStreamDestroy(cap3);
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     for (auto* b : body_local) delete b;
     for (auto* b : body_world) delete b;
     for (auto* b : body_tris) delete b;
@@ -524,6 +531,32 @@ int inner_newton(ando_ctx c, const ando_params& p, const StepParams& sp, ando_st
   return ANDO_OK;
 }
 
+// Fork the context's side stream off the main one / join it back.
+cudaError_t fork_side(ando_ctx c) {
+  cudaError_t e = cudaEventRecord(c->ev_fork, c->stream);
+  return e == cudaSuccess ? cudaStreamWaitEvent(c->side, c->ev_fork, 0) : e;
+}
+cudaError_t join_side(ando_ctx c) {
+  cudaError_t e = cudaEventRecord(c->ev_join, c->side);
+  return e == cudaSuccess ? cudaStreamWaitEvent(c->stream, c->ev_join, 0) : e;
+}
+
+// Self-contact time of impact of the move x -> x1 (= x + ext), min-reduced
+// into toi: swept-box traversals of both trees, vertex-triangle on the main
+// stream and edge-edge on the side stream.
+int swept_toi(ando_ctx c, double eta_min, double near) {
+  cudaStream_t s = c->stream;
+  CK(fork_side(c));
+  CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, eta_min, near, c->toi.p, c->toi_scratch, c->pcount,
+                          &c->ctrl.p->toi_overflow, s));
+  CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp_side, c->side));
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, eta_min, near, c->toi.p, c->toi_scratch_ee, c->pcount_ee,
+                           &c->ctrl.p->toi_overflow, c->side));
+  CK(join_side(c));
+  return ANDO_OK;
+}
+
 // CORRECTED contact set at the current positions: LBVH vertex-triangle and
 // edge-edge candidates within the activation distance, then rigid contacts.
 int detect_corrected(ando_ctx c, int nb, double gap_max) {
@@ -533,10 +566,13 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
     Phase ph(c, ANDO_PHASE_SETUP);
     long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
     // both queries launched back to back, both counters read in one round trip
+    // the two queries on two streams (each is latency-bound), joined before the counts are read
+    CK(fork_side(c));
     CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
     CK(c->bvh_tri.contacts_launch(c->x.p, 0, nullptr, c->V, float(gap_max), gap_max, c->pair_scratch, c->pcount, s));
-    CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
-    CK(c->bvh_edge.contacts_launch(c->x.p, 1, c->edges.p, c->E, float(gap_max), gap_max, c->pair_scratch_ee, c->pcount_ee, s));
+    CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->bvh_epoch, c->cub_tmp_side, c->side));
+    CK(c->bvh_edge.contacts_launch(c->x.p, 1, c->edges.p, c->E, float(gap_max), gap_max, c->pair_scratch_ee, c->pcount_ee, c->side));
+    CK(join_side(c));
     int* h = c->counts_host;
     CK(cudaMemcpyAsync(h, c->pcount.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(h + 3, c->pcount_ee.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -598,12 +634,8 @@ int corrected_line_search(ando_ctx c, int nb) {
   launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
   ph.launched(2 + (c->num_walls ? 1 : 0));
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-  CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.0, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch, c->pcount,
-                          &c->ctrl.p->toi_overflow, s));
-  CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.0, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch, c->pcount,
-                           &c->ctrl.p->toi_overflow, s));
+  int rc = swept_toi(c, 0.0, 1e-3 * c->gap_max);
+  if (rc) return rc;
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
   launch_update_toi(c->V, c->x.p, c->ext.p, 1.25, c->fixed.p, c->ctrl.p, c->toi.p, s);
@@ -912,12 +944,8 @@ int apply_pins_once(ando_ctx c, int nb) {
   launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
   ph.launched(2 + (c->num_walls ? 1 : 0));
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-  CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch,
-                          c->pcount, &c->ctrl.p->toi_overflow, s));
-  CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, 0.5 * c->gap_max, 1e-3 * c->gap_max, c->toi.p, c->toi_scratch,
-                           c->pcount, &c->ctrl.p->toi_overflow, s));
+  int rc = swept_toi(c, 0.5 * c->gap_max, 1e-3 * c->gap_max);
+  if (rc) return rc;
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
   launch_pin_move(c->pin_vertex.p, c->num_pins, c->ext.p, c->toi.p, c->ctrl.p, c->x.p, s);
@@ -930,9 +958,10 @@ int apply_pins_once(ando_ctx c, int nb) {
 // state untouched (the move kernels check the flag): grow the buffer and run
 // the pass again.
 int grow_toi_candidates(ando_ctx c, int need) {
-  const size_t n = std::max<size_t>(2 * size_t(need), 2 * c->toi_scratch.n);
+  const size_t n = std::max<size_t>(2 * size_t(need), 2 * std::min(c->toi_scratch.n, c->toi_scratch_ee.n));
   if (need < 0 || n > (size_t(1) << 26)) return fail(ANDO_ERR_CAPACITY, "more than 64M time-of-impact candidate pairs");
   CK(c->toi_scratch.reserve(n));
+  CK(c->toi_scratch_ee.reserve(n));
   return ANDO_OK;
 }
 
@@ -1229,6 +1258,9 @@ int32_t ando_ctx_create(int32_t device, ando_ctx* out) {
   if (e == cudaSuccess) e = cudaMallocHost(&c->counts_host, 8 * sizeof(int));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap2, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap3, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
   if (e == cudaSuccess) e = c->sctl.reserve(1);
   if (e == cudaSuccess) e = c->ctrl.reserve(1);
   if (e == cudaSuccess) e = cudaMemset(c->ctrl.p, 0, sizeof(Ctrl));
@@ -1374,6 +1406,7 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     CK(c->pair_scratch.resize_exact(4ull * V + 8ull * c->E + 1024));
     CK(c->pair_scratch_ee.resize_exact(4ull * V + 8ull * c->E + 1024));
     CK(c->toi_scratch.resize_exact(4ull * V + 8ull * c->E + 1024));
+    CK(c->toi_scratch_ee.resize_exact(4ull * V + 8ull * c->E + 1024));
   }
   CK(c->el_a.reserve(nnzb)); CK(c->el_b.reserve(nnzb)); CK(c->g_el.reserve(3ull * V));
   // per-vertex / per-slot work buffers
@@ -1859,6 +1892,7 @@ int32_t ando_ctx_set_pair_capacity(ando_ctx c, int32_t pairs) {
   CK(c->pair_scratch.resize_exact(size_t(pairs)));
   CK(c->pair_scratch_ee.resize_exact(size_t(pairs)));
   CK(c->toi_scratch.resize_exact(size_t(pairs)));
+  CK(c->toi_scratch_ee.resize_exact(size_t(pairs)));
   return ANDO_OK;
 }
 
