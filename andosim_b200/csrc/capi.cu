@@ -648,21 +648,23 @@ int corrected_line_search(ando_ctx c, int nb) {
 int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, int nb) {
   MeshDev m = c->mesh_dev();
   cudaStream_t s = c->stream;
-  int rc = detect_corrected(c, nb, p.contact_gap_max);
-  if (rc) return rc;
+  // the contact-free terms first: they depend on x only and overlap the
+  // broad phase's edge-edge half, which runs on the side stream
   {
     Phase ph(c, ANDO_PHASE_GRADIENT);
     launch_ctrl_reset(c->ctrl.p, s);
     launch_elastic_gradient(m, c->x.p, c->mu, c->thickness, c->g_el_x.p, s);
     ph.launched(2);
   }
-  rc = prepare_contacts(c, sp, c->g_el_x.p, c->fixed.p);
-  if (rc) return rc;
   if (sp.enable_strain) {
     Phase ph(c, ANDO_PHASE_STRAIN);
     launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, s);
     ph.launched();
   }
+  int rc = detect_corrected(c, nb, p.contact_gap_max);
+  if (rc) return rc;
+  rc = prepare_contacts(c, sp, c->g_el_x.p, c->fixed.p);
+  if (rc) return rc;
   Phase ph(c, ANDO_PHASE_GRADIENT);
   launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
                   c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
