@@ -96,7 +96,8 @@ struct ando_ctx_s {
 
   // SELL-32 copy of the static pattern for the scaled PCG (pcg.cu)
   DevBuf<int> chunk_off, sell_col, sell_base;
-  DevBuf<float> valh_sell, S_sell;
+  DevBuf<float> valh_sell, S_coef, S_diag;   // S_coef / S_diag: the learned S in the PCG's form
+  bool Sval_stale = false;                   // slot-major S not written by the steps since
   int sell_blocks = 0;
 
   // learned preconditioner: weights, activations, S on the static pattern
@@ -725,7 +726,7 @@ PcgScaledArgs scaled_args(ando_ctx c, const ando_params& p) {
   PcgScaledArgs a;
   a.V = c->V; a.chunk_off = c->chunk_off.p; a.sell_col = c->sell_col.p; a.valh = c->valh_sell.p;
   a.xbegin = c->nx ? c->xbegin.p : nullptr; a.xend = c->nx ? c->xend.p : nullptr; a.xcols = c->xcols.p; a.xvalh = c->xvalh.p;
-  a.S = nullptr; a.Linv = c->Linv.p; a.Lf = c->Lf.p; a.bhat = c->bhat.p; a.d = c->d.p;
+  a.coef = nullptr; a.Sdiag = nullptr; a.Linv = c->Linv.p; a.Lf = c->Lf.p; a.bhat = c->bhat.p; a.d = c->d.p;
   a.xh = c->xh.p; a.r = c->r.p; a.r2 = c->r2.p; a.z = c->z.p; a.p0 = c->p0.p; a.p1 = c->p1.p; a.Ap = c->Ap.p;
   a.partials = c->spart.p; a.ctrl = c->ctrl.p; a.tol = float(p.pcg_tol); a.max_iters = p.pcg_max_iters; a.stall_window = 50;
   a.snap_r = nullptr; a.snap_x = nullptr; a.snap_max = 0;
@@ -750,7 +751,8 @@ int ensure_learned(ando_ctx c) {
     learned_work_carve(c->lw, c->lw_buf.p, c->V, c->nnzb, false);
   }
   CK(c->Sval.reserve(9ull * c->nnzb));
-  CK(c->S_sell.reserve(9ull * c->sell_blocks));
+  CK(c->S_coef.reserve(c->sell_blocks));
+  CK(c->S_diag.reserve(9ull * c->V));
   return ANDO_OK;
 }
 
@@ -808,19 +810,20 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
     const int refresh = p.precond_refresh > 1 ? p.precond_refresh : 1;
     Phase pn(c, ANDO_PHASE_PRECOND);
     if (!c->coeff_valid || c->coeff_mesh != c->mesh_generation || c->coeff_age >= refresh) {
-      learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, s, &c->ctrl.p->tc_err);
+      learned_forward(v, c->net, c->lw, nullptr, SPcg{c->S_coef.p, c->S_diag.p}, s, &c->ctrl.p->tc_err);
       c->coeff_valid = true; c->coeff_mesh = c->mesh_generation; c->coeff_age = 1;
       pn.launched(5 + 3 * net::NL);
     } else {
-      learned_build_S(v, c->lw, c->Sval.p, c->S_sell.p, s);
+      learned_build_S(v, c->lw, nullptr, SPcg{c->S_coef.p, c->S_diag.p}, s);
       c->coeff_age++;
       pn.launched();
     }
     c->S_ready = true;
+    c->Sval_stale = true;
   }
   Phase ph(c, ANDO_PHASE_PCG);
   if (p.precond == ANDO_PRECOND_LEARNED) {
-    sa.S = c->S_sell.p;
+    sa.coef = c->S_coef.p; sa.Sdiag = c->S_diag.p;
     CK(launch_pcg_scaled(sa, true, pcg_shape(c, true, sa), s));
     ph.launched();
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
@@ -834,7 +837,7 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
     c->profile.pcg_extra_block_iterations += (long long)h.pcg_iters * c->nx;
     st.pcg_iters += h.pcg_iters;
     st.precond_fallbacks++;
-    sa.S = nullptr;
+    sa.coef = nullptr; sa.Sdiag = nullptr;
   }
   CK(launch_pcg_scaled(sa, false, pcg_shape(c, false, sa), s));
   ph.launched();
@@ -1988,12 +1991,13 @@ int32_t ando_precond_eval(ando_ctx c) {
   rc = ensure_learned(c);
   if (rc) return rc;
   LsView v = ls_view(c);
-  learned_forward(v, c->net, c->lw, c->Sval.p, c->S_sell.p, c->stream, &c->ctrl.p->tc_err);
+  learned_forward(v, c->net, c->lw, c->Sval.p, SPcg{c->S_coef.p, c->S_diag.p}, c->stream, &c->ctrl.p->tc_err);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (c->ctrl_host->tc_err) return fail(ANDO_ERR_TIMEOUT, "learned preconditioner: a tensor-core layer's wait timed out");
   c->S_ready = true;
+  c->Sval_stale = false;
   c->coeff_valid = true; c->coeff_mesh = c->mesh_generation; c->coeff_age = 1;
   return ANDO_OK;
 }
@@ -2003,6 +2007,11 @@ int32_t ando_last_precond(ando_ctx c, float* S) {
   if (rc) return rc;
   if (!S) return fail(ANDO_ERR_INVALID, "null output");
   if (!c->S_ready) return fail(ANDO_ERR_STATE, "no learned preconditioner evaluated yet");
+  if (c->Sval_stale) {  // the steps keep S in the PCG's form only: rebuild the slot-major copy
+    learned_build_S(ls_view(c), c->lw, c->Sval.p, SPcg{}, c->stream);
+    CK(cudaGetLastError());
+    c->Sval_stale = false;
+  }
   CK(cudaMemcpyAsync(S, c->Sval.p, sizeof(float) * 9ull * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return ANDO_OK;

@@ -116,7 +116,9 @@ struct PcgScaledArgs {
   int V;
   const int* chunk_off; const int* sell_col; const float* valh;               // A^ on the static pattern (SELL-32, pcg.cu)
   const int* xbegin; const int* xend; const int* xcols; const float* xvalh;  // A^ extra contact segment
-  const float* S;       // learned preconditioner blocks, SELL-32 like valh (learned solves only)
+  // learned solves only: S_ij = coef * A^_ij off the diagonal (coef per SELL
+  // slot, at the positions of sell_col) and S_ii = Sdiag (9 per vertex)
+  const float* coef; const float* Sdiag;
   const double* Linv;   // 6V packed L^-1
   const float* Lf;      // 6V packed L
   const float* bhat;    // 3V  L^-1 b

@@ -316,7 +316,7 @@ __global__ void k_dec_fwd(LsView s, const float* h, const float* Ef, const float
 }
 
 // S on the static pattern (see learned.cuh); one thread per row.
-__global__ void k_build_S(LsView s, const float* zv, const float* ab, float* S, float* S_sell) {
+__global__ void k_build_S(LsView s, const float* zv, const float* ab, float* S, SPcg pcg) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.V) return;
   float D[9];
@@ -340,13 +340,14 @@ __global__ void k_build_S(LsView s, const float* zv, const float* ab, float* S, 
       for (int r = 0; r < 3; ++r)
         for (int q = 0; q < 3; ++q) D[3 * r + q] += b2 * (A[3 * r] * A[3 * q] + A[3 * r + 1] * A[3 * q + 1] + A[3 * r + 2] * A[3 * q + 2]);
     }
-    for (int q = 0; q < 9; ++q) S[9ll * k + q] = c * A[q];
-    if (S_sell) for (int q = 0; q < 9; ++q) S_sell[s.sell_base[k] + 32 * q] = c * A[q];
+    if (S) for (int q = 0; q < 9; ++q) S[9ll * k + q] = c * A[q];
+    if (pcg.coef) {
+      const int l = i & 31;
+      pcg.coef[(s.sell_base[k] - l) / 9 + l] = c;  // sell_base = 9 (chunk slot) + lane
+    }
   }
-  if (kd >= 0) {
-    for (int q = 0; q < 9; ++q) S[9ll * kd + q] = D[q];
-    if (S_sell) for (int q = 0; q < 9; ++q) S_sell[s.sell_base[kd] + 32 * q] = D[q];
-  }
+  if (kd >= 0 && S) for (int q = 0; q < 9; ++q) S[9ll * kd + q] = D[q];
+  if (pcg.diag) for (int q = 0; q < 9; ++q) pcg.diag[9ll * i + q] = D[q];
 }
 
 // ------------------------------------------------------- training loss
@@ -572,7 +573,7 @@ void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cud
   k_net_transpose<<<nblk(WT_SIZE), TPB, 0, s>>>(n.wq, n.wt);
 }
 
-void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st, int* err) {
+void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, SPcg pcg, cudaStream_t st, int* err) {
   const int V = s.V;
   if (V == 0) return;
   const float* wq = n.wq;
@@ -588,17 +589,17 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
     launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, L + L_B, w.h[l], H, w.q[l], w.h[l + 1], 1, err, st);
   }
   k_dec_fwd<<<wgrid, TPB, 0, st>>>(s, w.h[NL], w.Ef, wq, w.zv, w.ab);
-  k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S, S_sell);
+  k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S, pcg);
 }
 
-void learned_build_S(const LsView& s, const LearnedWork& w, float* S, float* S_sell, cudaStream_t st) {
-  if (s.V) k_build_S<<<nblk(s.V), TPB, 0, st>>>(s, w.zv, w.ab, S, S_sell);
+void learned_build_S(const LsView& s, const LearnedWork& w, float* S, SPcg pcg, cudaStream_t st) {
+  if (s.V) k_build_S<<<nblk(s.V), TPB, 0, st>>>(s, w.zv, w.ab, S, pcg);
 }
 
 void learned_loss(const LsView& s, const NetDev& n, LearnedWork& w, float* S, const float* probes, const double* pnorm, int P,
                   float* Y, float* Wv, double* loss_parts, double* loss_out, float* grad, cudaStream_t st) {
   const int V = s.V;
-  learned_forward(s, n, w, S, nullptr, st);
+  learned_forward(s, n, w, S, SPcg{}, st);
   const int wgrid = nblk(32ll * V);
   for (int p = 0; p < P; ++p) {
     k_spmv<<<wgrid, TPB, 0, st>>>(V, s.rowptr, s.cols, S, nullptr, nullptr, nullptr, nullptr, probes + 3ll * V * p, Y + 3ll * V * p);

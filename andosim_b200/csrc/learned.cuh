@@ -82,11 +82,16 @@ void net_dev_carve(NetDev& n, float* base);
 // Round master weights to BF16 into n.wq (and bf16 storage) and build n.wt.
 void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cudaStream_t s);
 
-// Inference: features, network, S (9 floats per static slot; with S_sell also
-// in the SELL-32 layout of the PCG). The hidden dense layers run on the
-// tensor cores (tc_gemm.cu); `err` (may be null) is set when one of their
-// bounded waits gives up.
-void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, float* S_sell, cudaStream_t st, int* err = nullptr);
+// S in the form the PCG applies it: off the diagonal S_ij = coef * A^_ij, so
+// one coefficient per SELL-32 slot (at slot position chunk_off + 32 k + lane,
+// like sell_col) and the 3x3 diagonal blocks (9 per vertex, row-major).
+struct SPcg { float* coef = nullptr; float* diag = nullptr; };
+
+// Inference: features, network, S (9 floats per static slot when S is not
+// null; the PCG form when pcg.coef is not null). The hidden dense layers run
+// on the tensor cores (tc_gemm.cu); `err` (may be null) is set when one of
+// their bounded waits gives up.
+void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, SPcg pcg, cudaStream_t st, int* err = nullptr);
 
 // Tensor-core dense layer (tc_gemm.cu): Y = act(X W^T + bias) + R1 with
 // X = [X1 | X2] (K = K1 + K2 in 16..128, a multiple of 16), W row-major
@@ -97,7 +102,7 @@ cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float*
 
 // S from the coefficients of the last forward (w.zv, w.ab) and the current
 // A^: the network output reused while A^ changes; still SPD by construction.
-void learned_build_S(const LsView& s, const LearnedWork& w, float* S, float* S_sell, cudaStream_t st);
+void learned_build_S(const LsView& s, const LearnedWork& w, float* S, SPcg pcg, cudaStream_t st);
 
 // Training loss of one system: P probe vectors r_p (3V each) with energy
 // norms n_p = r_p^T A^-1 r_p; loss = mean_p (1 + (y^T A y - 2 r^T y) / n_p),

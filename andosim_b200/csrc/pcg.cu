@@ -207,8 +207,10 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg(PcgArgs a) {
 // unscaled residual: max_i |L_i r^_i| < tol * max |b|.
 //
 // LEARNED: z = S r with S a symmetric positive definite block matrix on the
-// static pattern (the learned approximate inverse of A^). Phase B then is a
-// second row product; it gathers r - alpha Ap from the neighbours, so
+// static pattern (the learned approximate inverse of A^), applied as
+// S_ij = coef_ij A^_ij off the diagonal plus its diagonal blocks. Phase B then
+// is a second row product over A^'s values; it gathers r - alpha Ap from the
+// neighbours, so
 // the iteration still needs only two grid barriers (r ping-pongs between two
 // buffers because neighbours read the old values). r^T z <= 0 (S lost
 // definiteness) or no new best residual for `stall_window` iterations ends
@@ -342,6 +344,51 @@ __device__ inline void sell_row_u(int row, const int* chunk_off, const int* sell
   y0 = a0; y1 = a1; y2 = a2;
 }
 
+// One row of z = S g with S_ij = coef_ij A^_ij off the diagonal and S_ii =
+// Sdiag_i: the SELL-32 product over A^'s static slots (the values phase A
+// has just read) with each gathered g_j scaled by its slot's coefficient,
+// the row's own slot skipped, then the diagonal block. The same FMA order
+// for every U.
+template <int U, class Vec>
+__device__ inline void sell_row_S(int row, const int* chunk_off, const int* sell_col, const float* val, const float* coef, const float* Sdiag,
+                                  const Vec& vec, float& y0, float& y1, float& y2) {
+  const int c = row >> 5, l = row & 31;
+  const int b0 = chunk_off[c], w = (chunk_off[c + 1] - b0) >> 5;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  if (U == 1) {
+    for (int k = 0; k < w; ++k) {
+      const int slot = b0 + 32 * k;
+      const int col = sell_col[slot + l];
+      if (col < 0 || col == row) continue;
+      const float cf = coef[slot + l];
+      float q0, q1, q2; vec(col, q0, q1, q2);
+      block_fma<32>(val + 9ll * slot + l, cf * q0, cf * q1, cf * q2, a0, a1, a2);
+    }
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < w; k += U) {
+      int col[U];
+      float cf[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        col[u] = k + u < w ? sell_col[b0 + 32 * (k + u) + l] : -1;
+        if (col[u] == row) col[u] = -1;
+        cf[u] = col[u] >= 0 ? coef[b0 + 32 * (k + u) + l] : 0.f;
+      }
+      float q[U][3];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (col[u] >= 0) vec(col[u], q[u][0], q[u][1], q[u][2]);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (col[u] >= 0) block_fma<32>(val + 9ll * (b0 + 32 * (k + u)) + l, cf[u] * q[u][0], cf[u] * q[u][1], cf[u] * q[u][2], a0, a1, a2);
+    }
+  }
+  float g0, g1, g2; vec(row, g0, g1, g2);
+  block_fma<1>(Sdiag + 9ll * row, g0, g1, g2, a0, a1, a2);
+  y0 = a0; y1 = a1; y2 = a2;
+}
+
 constexpr int SCALED_MAX_TPB = 1024;
 
 template <bool LEARNED, int U>
@@ -373,7 +420,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
       r[3 * i] = b0; r[3 * i + 1] = b1; r[3 * i + 2] = b2;
       if (LEARNED) {
         float y0, y1, y2;
-        sell_row_u<U>(i, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, GatherV{a.bhat}, y0, y1, y2);
+        sell_row_S<U>(i, a.chunk_off, a.sell_col, a.valh, a.coef, a.Sdiag, GatherV{a.bhat}, y0, y1, y2);
         a.z[3 * i] = y0; a.z[3 * i + 1] = y1; a.z[3 * i + 2] = y2;
         rz_loc = double(b0) * y0 + double(b1) * y1 + double(b2) * y2;
       } else {
@@ -460,7 +507,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
         double rz_new_loc = 0.0, rinf_loc = 0.0;
         if (row < V) {
           float y0, y1, y2;
-          sell_row_u<U>(row, a.chunk_off, a.sell_col, a.S, nullptr, nullptr, nullptr, nullptr, gr, y0, y1, y2);
+          sell_row_S<U>(row, a.chunk_off, a.sell_col, a.valh, a.coef, a.Sdiag, gr, y0, y1, y2);
           float r0, r1, r2; gr(row, r0, r1, r2);
           a.xh[3 * row] += double(alpha) * pnew[3 * row]; a.xh[3 * row + 1] += double(alpha) * pnew[3 * row + 1];
           a.xh[3 * row + 2] += double(alpha) * pnew[3 * row + 2];
