@@ -162,12 +162,14 @@ def pcg_bytes(V, nnzb, prof):
       phase B  12 V p, 24 V x^ read+write (FP64), 12 V Ap, 24 V r read+write,
                24 V L (FP32, residual norm)
       = 40 nnzb + 40 n_extra + 144 V
-    A learned iteration adds the second product z = S r on the mesh pattern:
-      + 40 nnzb (S values + column) + 24 V (r2, z written) + 12 V (Ap gathered)
+    A learned iteration adds the second product z = S r on the mesh pattern,
+    applied as S_ij = coef_ij A^_ij plus S's diagonal blocks:
+      + 44 nnzb (A^ values, column, coefficient) + 36 V (diagonal blocks)
+      + 24 V (r2, z written) + 12 V (Ap gathered)
     plus 48 V per launch (initialisation and d = L^-T x^)."""
     it = prof["pcg_iterations"]
     lit = prof["pcg_learned_iterations"]
-    return (40 * nnzb + 144 * V) * it + 40 * prof["pcg_extra_block_iterations"] + (40 * nnzb + 36 * V) * lit \
+    return (40 * nnzb + 144 * V) * it + 40 * prof["pcg_extra_block_iterations"] + (44 * nnzb + 72 * V) * lit \
         + 48 * V * prof["phase_launches"]["pcg"]
 
 
