@@ -422,36 +422,28 @@ cudaError_t Lbvh::update(const double* x, const double* x1, const int* prims_, i
 }
 
 namespace {
-// Sorted pairs of a query: every box candidate, or (gap >= 0) those whose
-// FP64 distance at x is below gap. Capacity grows as needed.
-cudaError_t run_query(Lbvh& B, double gap, const double* x, const double* x1, int kind, const int* qprims, int nq, float pad,
-                      DevBuf<int2>& out, DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
-                      DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
+// Sorted box-candidate pairs of a query (capacity grown as needed).
+cudaError_t run_query(Lbvh& B, const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
+                      DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1, DevBuf<int>& counter,
+                      DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
   cudaError_t e;
   *npairs = 0;
   if (B.n == 0 || nq == 0) return cudaSuccess;
-  const bool narrow = gap >= 0.0;
   if ((e = counter.reserve(3))) return e;
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
-  DevBuf<int2>& src = narrow ? B.surv : scratch;
   for (int attempt = 0; attempt < 2; ++attempt) {
     int cap = int(scratch.n);
-    if (narrow && (e = B.surv.reserve(scratch.n))) return e;
     if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.rank.p, B.inner.p, B.nodes.p, scratch.p,
-                                     counter.p, cap);
+    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.rank.p, B.inner.p, B.nodes.p,
+                                     scratch.p, counter.p, cap);
     B.launches += 1;
-    if (narrow) {
-      k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, B.prims, qprims, x, gap, B.surv.p, counter.p + 2);
-      B.launches += 1;
-    }
-    int cnt3[3] = {0, 0, 0};
-    if ((e = cudaMemcpyAsync(cnt3, counter.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
+    int cnt2[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(cnt2, counter.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
-    if (cnt3[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
-    int cnt = cnt3[0];
+    if (cnt2[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
+    int cnt = cnt2[0];
     if (cnt < 0 || cnt > (1 << 26)) return cudaErrorMemoryAllocation;  // > 64M candidate pairs: refuse instead of exhausting memory
-    if (cnt <= cap) { *npairs = narrow ? cnt3[2] : cnt; break; }
+    if (cnt <= cap) { *npairs = cnt; break; }
     if ((e = scratch.reserve(size_t(cnt) + size_t(cnt) / 4))) return e;
   }
   int m = *npairs;
@@ -459,12 +451,12 @@ cudaError_t run_query(Lbvh& B, double gap, const double* x, const double* x1, in
   if ((e = k0.reserve(m))) return e;
   if ((e = k1.reserve(m))) return e;
   if ((e = out.reserve(m))) return e;
-  k_pair_keys<<<nblk(m), TPB, 0, s>>>(src.p, m, k0.p);
+  k_pair_keys<<<nblk(m), TPB, 0, s>>>(scratch.p, m, k0.p);
   B.launches += 1;
   size_t bytes = 0;
-  if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.p, k1.p, src.p, out.p, m, 0, 64, s))) return e;
+  if ((e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
   if ((e = tmp.reserve(bytes))) return e;
-  if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, k0.p, k1.p, src.p, out.p, m, 0, 64, s))) return e;
+  if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, k0.p, k1.p, scratch.p, out.p, m, 0, 64, s))) return e;
   return cudaGetLastError();
 }
 }  // namespace
@@ -474,13 +466,7 @@ cudaError_t run_query(Lbvh& B, double gap, const double* x, const double* x1, in
 cudaError_t Lbvh::query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out,
                         DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
                         DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
-  return run_query(*this, -1.0, x, x1, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
-}
-
-cudaError_t Lbvh::query_contacts(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& out,
-                                 DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
-                                 DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s) {
-  return run_query(*this, gap < 0.0 ? 0.0 : gap, x, nullptr, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
+  return run_query(*this, x, x1, kind, qprims, nq, pad, out, scratch, k0, k1, counter, tmp, npairs, s);
 }
 
 cudaError_t Lbvh::contacts_launch(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& scratch,

@@ -28,7 +28,7 @@ struct Lbvh {
   DevBuf<unsigned long long> keys, keys_sorted;
   DevBuf<int> idx, order, left, right, parent, arrive, bounds;
   DevBuf<int> rank;             // sorted leaf position of each primitive (inverse of order)
-  DevBuf<int2> surv;            // candidates kept by the narrow phase of query_contacts
+  DevBuf<int2> surv;            // candidates kept by the narrow phase of contacts_launch
   long long launches = 0;
 
   cudaError_t reserve_prims(int n);
@@ -45,13 +45,8 @@ struct Lbvh {
                     DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1, DevBuf<int>& counter,
                     DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
   // The candidates (boxes at x inflated by pad) whose FP64 distance at x is
-  // below `gap`, sorted: a flat narrow-phase pass keeps the contacts before
-  // the sort, so only contacts are sorted.
-  cudaError_t query_contacts(const double* x, int kind, const int* qprims, int nq, float pad, double gap, DevBuf<int2>& out,
-                             DevBuf<int2>& scratch, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
-                             DevBuf<int>& counter, DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
-  // query_contacts in two halves, so that several queries share one host
-  // round trip: the launch (traversal and narrow phase; counter[0] = box
+  // below `gap`, sorted, in two halves so that several queries share one
+  // host round trip: the launch (traversal and narrow phase; counter[0] = box
   // candidates, counter[1] = stack overflows, counter[2] = contacts) and,
   // once the caller has read the counter, the sort of the contacts into
   // `out`. A launch whose candidates overflowed `scratch` (counter[0] >
