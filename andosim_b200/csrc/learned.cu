@@ -579,14 +579,15 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
   const float* wq = n.wq;
   k_edge_feats<<<nblk(s.nnzb), TPB, 0, st>>>(s.nnzb, s.valh, w.Ef);
   k_node_feats<<<nblk(V), TPB, 0, st>>>(s, w.Ef, w.X);
-  gemm(V, w.X, FN, FN, nullptr, 0, 0, n.wt + WT_IN, H, wq + B_IN, nullptr, 0, nullptr, 0, w.q0, w.h[0], 1, st);
+  // pre-activations (Q) are kept for the training backward only
+  gemm(V, w.X, FN, FN, nullptr, 0, 0, n.wt + WT_IN, H, wq + B_IN, nullptr, 0, nullptr, 0, w.training ? w.q0 : nullptr, w.h[0], 1, st);
   const int wgrid = nblk(32ll * V);
   for (int l = 0; l < NL; ++l) {
     const float* L = wq + LAYER0 + l * L_SIZE;
     // u = U h and h' = relu(W [h ; m] + b) + h on the tensor cores
     launch_gemm_tc(V, w.h[l], H, H, nullptr, 0, 0, L + L_U, nullptr, nullptr, 0, nullptr, w.u[l], 0, err, st);
     k_msg_fwd<<<wgrid, TPB, 0, st>>>(s, w.u[l], w.Ef, L + L_E, L + L_C, w.m[l]);
-    launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, L + L_B, w.h[l], H, w.q[l], w.h[l + 1], 1, err, st);
+    launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, L + L_B, w.h[l], H, w.training ? w.q[l] : nullptr, w.h[l + 1], 1, err, st);
   }
   k_dec_fwd<<<wgrid, TPB, 0, st>>>(s, w.h[NL], w.Ef, wq, w.zv, w.ab);
   k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S, pcg);
