@@ -5,8 +5,9 @@
 
 Runs the frames under torch.profiler (CUPTI kernel and CUDA runtime activity,
 warm caches, no serialisation), writes the Chrome trace and prints a summary:
-the span of the traced frames, the time some kernel was running, the idle
-gaps between kernels, the runtime calls and the per-kernel totals.
+the span of the traced frames, the time some kernel was running (kernels on
+two streams overlap, so their summed durations can exceed it), the idle gaps
+between kernels, the runtime calls and the per-kernel totals.
 """
 from __future__ import annotations
 
@@ -40,7 +41,8 @@ def summarise(trace: dict) -> dict:
             api[e["name"]][0] += 1
             api[e["name"]][1] += e["dur"]
     top = sorted(per.items(), key=lambda kv: -kv[1][1])
-    return {"span_us": round(end - t0, 1), "kernel_busy_us": round(busy, 1), "idle_us": round(idle, 1),
+    return {"span_us": round(end - t0, 1), "gpu_busy_us": round(end - t0 - idle, 1), "kernel_sum_us": round(busy, 1),
+            "idle_us": round(idle, 1),
             "kernels": [{"name": k, "launches": v[0], "total_us": round(v[1], 1), "avg_us": round(v[1] / v[0], 1)} for k, v in top],
             "runtime_calls": {k: {"calls": v[0], "total_us": round(v[1], 1)} for k, v in sorted(api.items(), key=lambda kv: -kv[1][1])}}
 
