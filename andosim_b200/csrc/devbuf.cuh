@@ -1,7 +1,7 @@
 // devbuf.cuh -- owning device buffer that only grows (host-side helper).
-// A buffer that has to grow takes at least 1.5x its old capacity, so sizes
-// that creep up step by step (contacts, pairs) reallocate rarely: cudaFree
-// synchronises the whole device.
+// A buffer that has to grow takes at least 1.5x its old capacity and never
+// less than 64 KiB, so sizes that creep up step by step from zero (contacts,
+// pairs) reallocate rarely: cudaFree synchronises the whole device.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -19,7 +19,8 @@ template <class T> struct DevBuf {
   ~DevBuf() { if (p) cudaFree(p); }
   cudaError_t reserve(size_t count) {
     if (count <= n && p) return cudaSuccess;
-    size_t c = count ? count : 1;
+    constexpr size_t floor_elems = (size_t(64) << 10) / sizeof(T) > 0 ? (size_t(64) << 10) / sizeof(T) : 1;
+    size_t c = count > floor_elems ? count : floor_elems;
     if (p) { c = c > n + n / 2 ? c : n + n / 2; cudaFree(p); p = nullptr; n = 0; }
     cudaError_t e = cudaMalloc(&p, c * sizeof(T));
     if (e == cudaSuccess) n = c;

@@ -12,12 +12,15 @@
 //
 // Pipeline: primitive boxes -> scene bounds -> 30-bit Morton codes of box
 // centres (index appended, so keys are unique) -> radix sort -> Karras
-// hierarchy (one thread per internal node) -> bottom-up refit with arrival
-// counters -> one thread per query with an explicit stack; hits are compacted
+// hierarchy (one thread per internal node) -> bottom-up refit in shared
+// memory (cut subtrees, then the nodes above the cut) -> one thread per query with an explicit stack; hits are compacted
 // with a warp ballot (one atomic per warp) and the pair list is then sorted so
 // its order does not depend on scheduling.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
 
 #include "lbvh.cuh"
 #include "narrow.cuh"
@@ -39,15 +42,19 @@ __device__ inline void grow(Box& b, float3 q) {
 }
 
 // Box of primitive i at positions x, or swept over x -> x1 when x1 is given.
-__global__ void k_prim_boxes(const double* x, const double* x1, const int* prims, int arity, int n, float pad, Box* boxes) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ inline Box prim_box(const double* x, const double* x1, const int* prims, int arity, int i, float pad) {
   float3 p = xf(x, prims[arity * i]);
   Box b; b.lo[0] = b.hi[0] = p.x; b.lo[1] = b.hi[1] = p.y; b.lo[2] = b.hi[2] = p.z;
   for (int k = 1; k < arity; ++k) grow(b, xf(x, prims[arity * i + k]));
   if (x1) for (int k = 0; k < arity; ++k) grow(b, xf(x1, prims[arity * i + k]));
   if (pad > 0.f) for (int k = 0; k < 3; ++k) { b.lo[k] -= pad; b.hi[k] += pad; }
-  boxes[i] = b;
+  return b;
+}
+
+__global__ void k_prim_boxes(const double* x, const double* x1, const int* prims, int arity, int n, float pad, Box* boxes) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  boxes[i] = prim_box(x, x1, prims, arity, i, pad);
 }
 
 // Scene bounds as min/max over box centres (block reduction + float atomics
@@ -104,7 +111,10 @@ __device__ inline int delta(const unsigned long long* k, int n, int i, int j) {
 // Karras 2012: internal node i covers a key range found from the common
 // prefix lengths of its neighbours. Nodes [0, n-1) are internal, leaves are
 // encoded as n-1 + sorted position.
-__global__ void k_karras(const unsigned long long* keys, int n, int* left, int* right, int* parent, LbvhInner* inner) {
+// topo[i] = {first leaf, last leaf of the left child, last leaf, parent} in
+// sorted leaf positions (parent -1 at the root); the parent component is
+// written by the parent's thread.
+__global__ void k_karras(const unsigned long long* keys, int n, int* parent, LbvhInner* inner, int4* topo) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n - 1) return;
   int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -126,10 +136,14 @@ __global__ void k_karras(const unsigned long long* keys, int n, int* left, int* 
   int lo = min(i, j), hi = max(i, j);
   int lc = (lo == gamma) ? (n - 1 + gamma) : gamma;
   int rc = (hi == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
-  left[i] = lc; right[i] = rc;
   inner[i].lc = lc; inner[i].rc = rc;
   inner[i].lmax = gamma; inner[i].rmax = hi;  // leaf ranges [lo, gamma] and [gamma + 1, hi]
   parent[lc] = i; parent[rc] = i;
+  int* tw = reinterpret_cast<int*>(topo);
+  tw[4 * i] = lo; tw[4 * i + 1] = gamma; tw[4 * i + 2] = hi;
+  if (i == 0) tw[3] = -1;
+  if (lc < n - 1) tw[4 * lc + 3] = i;
+  if (rc < n - 1) tw[4 * rc + 3] = i;
 }
 
 __global__ void k_rank(const int* order, int n, int* rank) {
@@ -137,41 +151,179 @@ __global__ void k_rank(const int* order, int n, int* rank) {
   if (p < n) rank[order[p]] = p;
 }
 
-// Copy a finished node box into its parent's packed record.
-__device__ inline void to_parent(LbvhInner* inner, const int* left, int p, int child, const Box& b) {
-  float* dst = left[p] == child ? inner[p].lbox : inner[p].rbox;
-  for (int k = 0; k < 3; ++k) { dst[k] = b.lo[k]; dst[3 + k] = b.hi[k]; }
+__device__ inline Box ld_box_volatile(const Box* b) {
+  const volatile float* v = reinterpret_cast<const volatile float*>(b);
+  Box r;
+  for (int k = 0; k < 3; ++k) { r.lo[k] = v[k]; r.hi[k] = v[3 + k]; }
+  return r;
 }
 
-// Bottom-up refit: the second child to arrive at a node computes its box.
-__global__ void k_refit(const Box* boxes, const int* order, int n, const int* left, const int* right, const int* parent,
-                        Box* nodes, int* arrive, LbvhInner* inner) {
+__device__ inline Box ld_box_cg(const Box* b) {
+  const float* v = reinterpret_cast<const float*>(b);
+  Box r;
+  for (int k = 0; k < 3; ++k) { r.lo[k] = __ldcg(v + k); r.hi[k] = __ldcg(v + 3 + k); }
+  return r;
+}
+
+__device__ inline Box unite(const Box& a, const Box& b) {
+  Box u;
+  for (int k = 0; k < 3; ++k) { u.lo[k] = fminf(a.lo[k], b.lo[k]); u.hi[k] = fmaxf(a.hi[k], b.hi[k]); }
+  return u;
+}
+
+// Tiled bottom-up refit in two launches over a cut of the hierarchy made at
+// build time. Below the cut: every subtree of at most RF_CUT leaves whose
+// parent has more ("cut subtree"). Above it: the top nodes (more than RF_CUT
+// leaves), numbered compactly.
+//
+// k_refit_cut: one CTA per cut subtree (grid-stride over the cut list). With
+// Karras numbering a node covering leaves [lo, hi] has its index in [lo, hi],
+// so every node of a subtree over [c0, c1] has a shared-memory slot (index -
+// c0): the subtree's topology is staged once and each node is finished in
+// shared memory by the second of its children to arrive (block-scope arrival
+// counters). The leaf boxes are computed from the positions here.
+//
+// k_refit_top: one CTA finishes the top nodes the same way in shared memory,
+// reading the cut subtrees' boxes from nodes[].
+//
+// When the top has more nodes than one CTA holds, k_refit_cut carries on
+// through the top nodes itself with global arrival counters (acquire/release
+// atomics; the second arrival zeroes the counter for the next refit) and
+// k_refit_top does nothing. Min/max are exact, so every box has the same bits
+// in any arrival order.
+constexpr int RF_TPB = 512, RF_CUT = 1024;
+struct RefitSmem { Box leaf[RF_CUT]; Box node[RF_CUT]; int4 topo[RF_CUT]; int arr[RF_CUT]; };
+constexpr int TOP_TPB = 1024, TOP_MAX = 4096;
+// top node: {node index, parent's top number (-1 at the root), left, right};
+// a child is its top number (>= 0) or -(1 + its nodes[] index) below the cut
+struct TopSmem { int4 rec[TOP_MAX]; Box box[TOP_MAX]; int arr[TOP_MAX]; };
+
+__device__ inline bool is_top(const int4& t) { return t.z - t.x + 1 > RF_CUT; }
+
+// Build time: 1 for the top nodes (exclusive-scanned into their numbers).
+__global__ void k_top_flags(const int4* topo, int n, int* flag) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int leaf = n - 1 + i;
-  const Box lb = boxes[order[i]];
-  nodes[leaf] = lb;
-  if (n == 1) return;
-  int p = parent[leaf];
-  to_parent(inner, left, p, leaf, lb);
-  while (p >= 0) {
-    // first arrival: the sibling finishes this node. The acquire-release
-    // atomic publishes this thread's box writes to the sibling and makes the
-    // sibling's visible to it (no full fences).
-    int prior;
-    asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(prior) : "l"(arrive + p) : "memory");
-    if (prior == 0) return;
-    // the sibling's box was written by another thread: read it past L1
-    Box a, b;
-    const float* pa = reinterpret_cast<const float*>(nodes + left[p]);
-    const float* pb = reinterpret_cast<const float*>(nodes + right[p]);
-    for (int k = 0; k < 3; ++k) { a.lo[k] = __ldcg(pa + k); a.hi[k] = __ldcg(pa + 3 + k); b.lo[k] = __ldcg(pb + k); b.hi[k] = __ldcg(pb + 3 + k); }
-    Box u;
-    for (int k = 0; k < 3; ++k) { u.lo[k] = fminf(a.lo[k], b.lo[k]); u.hi[k] = fmaxf(a.hi[k], b.hi[k]); }
-    nodes[p] = u;
-    const int c = p;
-    p = p == 0 ? -1 : parent[p];
-    if (p >= 0) to_parent(inner, left, p, c, u);
+  if (i < n - 1) flag[i] = is_top(topo[i]) ? 1 : 0;
+}
+
+// Build time: the top records and the cut list (entries 2k, 2k+1: the
+// below-cut children of top node k as leaf ranges, {-1, -1} for a top child).
+__global__ void k_top_records(const int4* topo, const LbvhInner* inner, const int* topnum, int n, int4* rec, int2* cuts) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int4 t = topo[i];
+  if (!is_top(t)) return;
+  const int k = topnum[i];
+  const int lc = inner[i].lc, rc = inner[i].rc;
+  const bool ltop = lc < n - 1 && is_top(topo[lc]), rtop = rc < n - 1 && is_top(topo[rc]);
+  rec[k] = make_int4(i, t.w >= 0 ? topnum[t.w] : -1, ltop ? topnum[lc] : -(1 + lc), rtop ? topnum[rc] : -(1 + rc));
+  cuts[2 * k] = ltop ? make_int2(-1, -1) : make_int2(t.x, t.y);
+  cuts[2 * k + 1] = rtop ? make_int2(-1, -1) : make_int2(t.y + 1, t.z);
+}
+
+// Build time: meta = {top nodes, cut entries}; with no top node the whole
+// hierarchy is one cut subtree.
+__global__ void k_top_count(const int* flag, const int* topnum, int n, int* meta, int2* cuts) {
+  const int m = n > 1 ? topnum[n - 2] + flag[n - 2] : 0;
+  meta[0] = m;
+  meta[1] = m > 0 ? 2 * m : 1;
+  if (m == 0) cuts[0] = make_int2(0, n - 1);
+}
+
+__global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const double* x1, const int* prims, int arity, float pad,
+                                                      const int* order, int n, const int* parent, const int4* topo, const int2* cuts,
+                                                      const int* meta, Box* nodes, int* arrive, LbvhInner* inner) {
+  extern __shared__ __align__(16) unsigned char rf_raw[];
+  RefitSmem& S = *reinterpret_cast<RefitSmem*>(rf_raw);
+  const int ncut = meta[1];
+  const bool top_global = meta[0] > TOP_MAX;
+  for (int cb = blockIdx.x; cb < ncut; cb += gridDim.x) {
+    const int2 cut = cuts[cb];
+    if (cut.x < 0) continue;  // uniform over the CTA
+    const int c0 = cut.x, c1 = cut.y;
+    __syncthreads();  // the previous subtree's shared memory is no longer read
+    for (int t = threadIdx.x; t <= c1 - c0; t += RF_TPB) {
+      S.arr[t] = 0;
+      const int q = c0 + t;
+      if (q < n - 1) S.topo[t] = topo[q];
+      const Box b = prim_box(x, x1, prims, arity, order[q], pad);
+      S.leaf[t] = b;
+      nodes[n - 1 + q] = b;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t <= c1 - c0; t += RF_TPB) {
+      const int i = c0 + t;
+      Box box = S.leaf[t];
+      int chi = i;  // last leaf under the current node
+      int p = n > 1 ? parent[n - 1 + i] : -1;
+      int4 tp = p < 0 ? make_int4(0, 0, 0, -1) : (p <= c1 && p >= c0 ? S.topo[p - c0] : __ldg(topo + p));
+      while (p >= 0) {
+        const int plo = tp.x, pl = tp.y, phi = tp.z, pp = tp.w;
+        const bool inside = plo >= c0 && phi <= c1;
+        const bool from_left = chi == pl;
+        float* dst = from_left ? inner[p].lbox : inner[p].rbox;
+        for (int k = 0; k < 3; ++k) { dst[k] = box.lo[k]; dst[3 + k] = box.hi[k]; }
+        if (!inside && !top_global) break;  // a top node: k_refit_top finishes it
+        // topology of the next parent (read-only here), fetched before the arrival
+        const int4 tnext = pp < 0 ? make_int4(0, 0, 0, -1) : (pp <= c1 && pp >= c0 ? S.topo[pp - c0] : __ldg(topo + pp));
+        // the sibling covers [sl, sh]: a leaf when sl == sh, else internal node sidx
+        const int sl = from_left ? pl + 1 : plo, sh = from_left ? phi : pl, sidx = from_left ? pl + 1 : pl;
+        if (inside) {
+          __threadfence_block();
+          if (atomicAdd(&S.arr[p - c0], 1) == 0) break;
+          __threadfence_block();
+          box = unite(box, sl == sh ? ld_box_volatile(&S.leaf[sl - c0]) : ld_box_volatile(&S.node[sidx - c0]));
+          S.node[p - c0] = box;
+        } else {
+          // this thread wrote nodes[] of its current node before the release
+          int prior;
+          asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(prior) : "l"(arrive + p) : "memory");
+          if (prior == 0) break;
+          arrive[p] = 0;
+          box = unite(box, ld_box_cg(nodes + (sl == sh ? n - 1 + sl : sidx)));
+        }
+        nodes[p] = box;
+        chi = phi;
+        p = pp;
+        tp = tnext;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, const int4* rec, Box* nodes, LbvhInner* inner) {
+  extern __shared__ __align__(16) unsigned char rt_raw[];
+  TopSmem& S = *reinterpret_cast<TopSmem*>(rt_raw);
+  const int m = meta[0];
+  if (m <= 0 || m > TOP_MAX) return;
+  for (int k = threadIdx.x; k < m; k += TOP_TPB) {
+    const int4 r = rec[k];
+    S.rec[k] = r;
+    S.arr[k] = (r.z < 0) + (r.w < 0);  // below-cut children have arrived already
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < m; k += TOP_TPB) {
+    int4 r = S.rec[k];
+    if (r.z >= 0 || r.w >= 0) continue;  // starts only where both children are below the cut
+    int cur = k;
+    Box box = unite(ld_box_cg(nodes + (-r.z - 1)), ld_box_cg(nodes + (-r.w - 1)));
+    while (true) {
+      S.box[cur] = box;
+      nodes[r.x] = box;
+      const int pc = r.y;
+      if (pc < 0) break;
+      const int4 pr = S.rec[pc];
+      const bool from_left = pr.z == cur;
+      float* dst = from_left ? inner[pr.x].lbox : inner[pr.x].rbox;
+      for (int q = 0; q < 3; ++q) { dst[q] = box.lo[q]; dst[3 + q] = box.hi[q]; }
+      __threadfence_block();
+      if (atomicAdd(&S.arr[pc], 1) == 0) break;
+      __threadfence_block();
+      const int sib = from_left ? pr.w : pr.z;
+      box = unite(box, sib >= 0 ? ld_box_volatile(&S.box[sib]) : ld_box_cg(nodes + (-sib - 1)));
+      cur = pc;
+      r = pr;
+    }
   }
 }
 
@@ -362,13 +514,17 @@ cudaError_t Lbvh::reserve_prims(int n) {
   if ((e = keys_sorted.reserve(N))) return e;
   if ((e = idx.reserve(N))) return e;
   if ((e = order.reserve(N))) return e;
-  if ((e = left.reserve(N))) return e;
-  if ((e = right.reserve(N))) return e;
   if ((e = parent.reserve(2 * N))) return e;
   if ((e = nodes.reserve(2 * N))) return e;
   if ((e = inner.reserve(N))) return e;
   if ((e = rank.reserve(N))) return e;
   if ((e = arrive.reserve(N))) return e;
+  if ((e = topo.reserve(N))) return e;
+  if ((e = topflag.reserve(N))) return e;
+  if ((e = topnum.reserve(N))) return e;
+  if ((e = toprec.reserve(N))) return e;
+  if ((e = cuts.reserve(2 * N))) return e;
+  if ((e = meta.reserve(2))) return e;
   if ((e = bounds.reserve(6))) return e;
   return cudaSuccess;
 }
@@ -392,11 +548,19 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
   k_rank<<<nblk(n), TPB, 0, s>>>(order.p, n, rank.p);
   if (n > 1) {
     if ((e = cudaMemsetAsync(parent.p, 0xff, sizeof(int) * (2 * n - 1), s))) return e;
-    k_karras<<<nblk(n - 1), TPB, 0, s>>>(keys_sorted.p, n, left.p, right.p, parent.p, inner.p);
+    k_karras<<<nblk(n - 1), TPB, 0, s>>>(keys_sorted.p, n, parent.p, inner.p, topo.p);
     if ((e = cudaMemsetAsync(arrive.p, 0, sizeof(int) * n, s))) return e;
+    k_top_flags<<<nblk(n - 1), TPB, 0, s>>>(topo.p, n, topflag.p);
+    size_t sb = 0;
+    if ((e = cub::DeviceScan::ExclusiveSum(nullptr, sb, topflag.p, topnum.p, n - 1, s))) return e;
+    if ((e = tmp.reserve(sb))) return e;
+    if ((e = cub::DeviceScan::ExclusiveSum(tmp.p, sb, topflag.p, topnum.p, n - 1, s))) return e;
+    k_top_records<<<nblk(n - 1), TPB, 0, s>>>(topo.p, inner.p, topnum.p, n, toprec.p, cuts.p);
+    launches += 2;
   }
-  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p, inner.p);
-  launches += n > 1 ? 7 : 6;
+  k_top_count<<<1, 1, 0, s>>>(topflag.p, topnum.p, n, meta.p, cuts.p);
+  if ((e = launch_refit(x, x1, pad, s))) return e;
+  launches += (n > 1 ? 8 : 7) + (n > RF_CUT ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -406,11 +570,29 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
 // traversal cost does, so the Morton order of an earlier build stays valid.
 cudaError_t Lbvh::refit(const double* x, const double* x1, float pad, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  cudaError_t e;
-  k_prim_boxes<<<nblk(n), TPB, 0, s>>>(x, x1, prims, arity, n, pad, boxes.p);
-  if (n > 1 && (e = cudaMemsetAsync(arrive.p, 0, sizeof(int) * n, s))) return e;
-  k_refit<<<nblk(n), TPB, 0, s>>>(boxes.p, order.p, n, left.p, right.p, parent.p, nodes.p, arrive.p, inner.p);
-  launches += 2;
+  cudaError_t e = launch_refit(x, x1, pad, s);
+  launches += n > RF_CUT ? 2 : 1;
+  return e;
+}
+
+// The global arrival counters are zero between refits: the build zeroes them
+// and every refit leaves them zero (each node's second arrival resets it).
+cudaError_t Lbvh::launch_refit(const double* x, const double* x1, float pad, cudaStream_t s) {
+  static_assert(sizeof(RefitSmem) <= 227 * 1024 && sizeof(TopSmem) <= 227 * 1024, "refit tile exceeds shared memory");
+  cudaError_t e = cudaFuncSetAttribute(k_refit_cut, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(RefitSmem)));
+  if (!e) e = cudaFuncSetAttribute(k_refit_top, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TopSmem)));
+  if (e) return e;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+  }
+  // grid-stride over the cut list (its length stays on the device): about
+  // three subtrees per SM resident at once
+  const int grid = std::max(1, std::min(3 * sms, 2 * ((n + 255) / 256)));
+  k_refit_cut<<<grid, RF_TPB, sizeof(RefitSmem), s>>>(x, x1, prims, arity, pad, order.p, n, parent.p, topo.p, cuts.p, meta.p, nodes.p,
+                                                      arrive.p, inner.p);
+  if (n > RF_CUT) k_refit_top<<<1, TOP_TPB, sizeof(TopSmem), s>>>(meta.p, toprec.p, nodes.p, inner.p);
   return cudaGetLastError();
 }
 

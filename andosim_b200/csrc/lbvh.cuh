@@ -26,8 +26,14 @@ struct Lbvh {
   DevBuf<LbvhBox> boxes, nodes; // primitive boxes; node boxes (internal [0,n-1), leaves [n-1, 2n-1))
   DevBuf<LbvhInner> inner;      // n-1 internal nodes, child boxes packed (written by the refit)
   DevBuf<unsigned long long> keys, keys_sorted;
-  DevBuf<int> idx, order, left, right, parent, arrive, bounds;
+  DevBuf<int> idx, order, parent, arrive, bounds;
   DevBuf<int> rank;             // sorted leaf position of each primitive (inverse of order)
+  DevBuf<int4> topo;            // per internal node: first leaf, split, last leaf, parent
+  // refit schedule made at build time: nodes above the cut (flags, numbers,
+  // records), the cut subtrees as leaf ranges, meta = {top nodes, cut entries}
+  DevBuf<int> topflag, topnum, meta;
+  DevBuf<int4> toprec;
+  DevBuf<int2> cuts;
   DevBuf<int2> surv;            // candidates kept by the narrow phase of contacts_launch
   long long launches = 0;
 
@@ -36,6 +42,7 @@ struct Lbvh {
   cudaError_t build(const double* x, const double* x1, const int* prims, int arity, int n, float pad, DevBuf<unsigned char>& tmp, cudaStream_t s);
   // new boxes over the last build's topology (same primitives)
   cudaError_t refit(const double* x, const double* x1, float pad, cudaStream_t s);
+  cudaError_t launch_refit(const double* x, const double* x1, float pad, cudaStream_t s);
   // full build once per caller epoch, refit otherwise
   cudaError_t update(const double* x, const double* x1, const int* prims, int arity, int n, float pad, long long epoch,
                      DevBuf<unsigned char>& tmp, cudaStream_t s);

@@ -565,12 +565,23 @@ void learned_work_carve(LearnedWork& w, float* base, int V, int nnzb, bool train
   }
 }
 
-size_t net_dev_floats() { return size_t(NPARAM) + WT_SIZE; }
-void net_dev_carve(NetDev& n, float* base) { n.wq = base; n.wt = base + NPARAM; }
+// B images of the hidden layers: per layer U (64 x 64) then W (64 x 128)
+constexpr int BIMG_U = 0, BIMG_W = H * H, BIMG_LSIZE = BIMG_W + H * 2 * H;
+constexpr size_t BIMG_OFF = (size_t(NPARAM) + WT_SIZE + 3) / 4 * 4;  // floats; 16-byte aligned
+size_t net_dev_floats() { return BIMG_OFF + size_t(NL) * BIMG_LSIZE / 2; }
+void net_dev_carve(NetDev& n, float* base) {
+  n.wq = base; n.wt = base + NPARAM;
+  n.bimg = reinterpret_cast<unsigned short*>(base + BIMG_OFF);
+}
 
 void launch_net_prepare(const float* master, NetDev n, unsigned short* bf16, cudaStream_t s) {
   k_net_round<<<nblk(NPARAM), TPB, 0, s>>>(master, n.wq, bf16, NPARAM);
   k_net_transpose<<<nblk(WT_SIZE), TPB, 0, s>>>(n.wq, n.wt);
+  for (int l = 0; l < NL; ++l) {
+    const float* L = n.wq + LAYER0 + l * L_SIZE;
+    launch_gemm_tc_image(L + L_U, H, n.bimg + l * BIMG_LSIZE + BIMG_U, s);
+    launch_gemm_tc_image(L + L_W, 2 * H, n.bimg + l * BIMG_LSIZE + BIMG_W, s);
+  }
 }
 
 void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S, SPcg pcg, cudaStream_t st, int* err) {
@@ -585,9 +596,11 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
   for (int l = 0; l < NL; ++l) {
     const float* L = wq + LAYER0 + l * L_SIZE;
     // u = U h and h' = relu(W [h ; m] + b) + h on the tensor cores
-    launch_gemm_tc(V, w.h[l], H, H, nullptr, 0, 0, L + L_U, nullptr, nullptr, 0, nullptr, w.u[l], 0, err, st);
+    const unsigned short* bi = n.bimg ? n.bimg + l * BIMG_LSIZE : nullptr;
+    launch_gemm_tc(V, w.h[l], H, H, nullptr, 0, 0, L + L_U, bi ? bi + BIMG_U : nullptr, nullptr, nullptr, 0, nullptr, w.u[l], 0, err, st);
     k_msg_fwd<<<wgrid, TPB, 0, st>>>(s, w.u[l], w.Ef, L + L_E, L + L_C, w.m[l]);
-    launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, L + L_B, w.h[l], H, w.training ? w.q[l] : nullptr, w.h[l + 1], 1, err, st);
+    launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, bi ? bi + BIMG_W : nullptr, L + L_B, w.h[l], H, w.training ? w.q[l] : nullptr,
+                   w.h[l + 1], 1, err, st);
   }
   k_dec_fwd<<<wgrid, TPB, 0, st>>>(s, w.h[NL], w.Ef, wq, w.zv, w.ab);
   k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S, pcg);

@@ -76,6 +76,7 @@ void learned_work_carve(LearnedWork& w, float* base, int V, int nnzb, bool train
 struct NetDev {
   float* wq = nullptr;       // NPARAM, BF16-representable values
   float* wt = nullptr;       // transposed copies of the dense matrices (forward layout)
+  unsigned short* bimg = nullptr;  // hidden layers' U and W as tensor-core B operand images (launch_gemm_tc_image)
 };
 size_t net_dev_floats();
 void net_dev_carve(NetDev& n, float* base);
@@ -96,9 +97,13 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
 // Tensor-core dense layer (tc_gemm.cu): Y = act(X W^T + bias) + R1 with
 // X = [X1 | X2] (K = K1 + K2 in 16..128, a multiple of 16), W row-major
 // [64][K] BF16-representable, 64 outputs.
+// Bimg (may be null): W's B operand image from launch_gemm_tc_image (64 K
+// BF16 values, 16-byte aligned), copied instead of converting W per CTA.
 bool gemm_tc_supported(int K1, int K2, int N, int ldr1);
-cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W, const float* bias,
-                           const float* R1, int ldr1, float* Q, float* Y, int relu, int* err, cudaStream_t s);
+cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W,
+                           const unsigned short* Bimg, const float* bias, const float* R1, int ldr1, float* Q, float* Y, int relu, int* err,
+                           cudaStream_t s);
+cudaError_t launch_gemm_tc_image(const float* W, int K, unsigned short* img, cudaStream_t s);
 
 // S from the coefficients of the last forward (w.zv, w.ab) and the current
 // A^: the network output reused while A^ changes; still SPD by construction.

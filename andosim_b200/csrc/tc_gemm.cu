@@ -96,14 +96,27 @@ __device__ inline uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
   return uint32_t(__bfloat16_as_ushort(a)) | (uint32_t(__bfloat16_as_ushort(b)) << 16);
 }
 
+// B image: W (64 x K, row-major, BF16-representable) as BF16 in the shared
+// memory layout of the MMA's B operand, 128 K bytes.
+__global__ void k_gemm_tc_image(const float* __restrict__ W, int K, unsigned short* __restrict__ img) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= TC_N * K) return;
+  const int n = i / K, k = i - n * K;
+  img[core_off(n, k, K) >> 1] = __bfloat16_as_ushort(__float2bfloat16_rn(W[i]));
+}
+
+constexpr int TC_AV = TC_M * 128 / 4 / TC_THREADS;  // float4 loads per thread of the A tile at K = 128
+
 // Y[r, :64] = act(X[r, :] W^T + bias) + R1[r, :64], X = [X1 | X2] (K = K1 + K2,
 // a multiple of 16, at most 128; K1 a multiple of 8; rows 16-byte aligned),
-// W row-major [64][K] (BF16-representable); Q (may be null) gets the
-// pre-activation.
+// W row-major [64][K] (BF16-representable), or its B image Bimg when not
+// null; Q (may be null) gets the pre-activation. res_a: R1 is X1 itself (the
+// first 64 columns), taken from the A tile in shared memory, whose three
+// BF16 terms sum back to the FP32 value exactly.
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __restrict__ X1, int ld1, int K1, const float* __restrict__ X2,
-                                                        int ld2, int K2, const float* __restrict__ W, const float* __restrict__ bias,
-                                                        const float* __restrict__ R1, int ldr1, float* __restrict__ Q, float* __restrict__ Y,
-                                                        int relu, int* err) {
+                                                        int ld2, int K2, const float* __restrict__ W, const uint4* __restrict__ Bimg,
+                                                        const float* __restrict__ bias, const float* __restrict__ R1, int ldr1, int res_a,
+                                                        float* __restrict__ Q, float* __restrict__ Y, int relu, int* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int K = K1 + K2;
   const int tile = TC_M * K * 2;  // bytes of one BF16 split of the row tile
@@ -123,22 +136,50 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_a), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  // B: W (64 x K), exact in BF16
-  for (int i = tid; i < TC_N * K; i += TC_THREADS) {
-    const int n = i / K, k = i - n * K;
-    *reinterpret_cast<__nv_bfloat16*>(B + core_off(n, k, K)) = __float2bfloat16_rn(W[i]);
+  // B: the image (16-byte copies), or W converted here (exact in BF16)
+  constexpr int TC_BV = TC_N * 128 * 2 / 16 / TC_THREADS;
+  uint4 bv[TC_BV];
+  const int nb16 = TC_N * K * 2 / 16;
+  if (Bimg) {
+#pragma unroll
+    for (int j = 0; j < TC_BV; ++j) {
+      const int i = tid + j * TC_THREADS;
+      if (i < nb16) bv[j] = Bimg[i];
+    }
+  } else {
+    for (int i = tid; i < TC_N * K; i += TC_THREADS) {
+      const int n = i / K, k = i - n * K;
+      *reinterpret_cast<__nv_bfloat16*>(B + core_off(n, k, K)) = __float2bfloat16_rn(W[i]);
+    }
   }
   // A: coalesced 16-byte loads (consecutive threads take consecutive
-  // 4-column groups of a row), each split into three BF16 4-vectors
+  // 4-column groups of a row), all issued before the first is used, then
+  // each split into three BF16 4-vectors
   {
     const int K4 = K >> 2, n4 = TC_M * K4;
-#pragma unroll 4
-    for (int c = tid; c < n4; c += TC_THREADS) {
+    float4 av[TC_AV];
+#pragma unroll
+    for (int j = 0; j < TC_AV; ++j) {
+      const int c = tid + j * TC_THREADS;
       const int r = c / K4, k = (c - r * K4) << 2, row = r0 + r;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (row < V) v = k < K1 ? *reinterpret_cast<const float4*>(X1 + (long long)row * ld1 + k)
-                              : *reinterpret_cast<const float4*>(X2 + (long long)row * ld2 + (k - K1));
-      const float f[4] = {v.x, v.y, v.z, v.w};
+      av[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (c < n4 && row < V)
+        av[j] = k < K1 ? *reinterpret_cast<const float4*>(X1 + (long long)row * ld1 + k)
+                       : *reinterpret_cast<const float4*>(X2 + (long long)row * ld2 + (k - K1));
+    }
+    if (Bimg) {
+#pragma unroll
+      for (int j = 0; j < TC_BV; ++j) {
+        const int i = tid + j * TC_THREADS;
+        if (i < nb16) reinterpret_cast<uint4*>(B)[i] = bv[j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TC_AV; ++j) {
+      const int c = tid + j * TC_THREADS;
+      if (c >= n4) break;
+      const int r = c / K4, k = (c - r * K4) << 2;
+      const float f[4] = {av[j].x, av[j].y, av[j].z, av[j].w};
       uint32_t w[TC_SPLITS][2];
 #pragma unroll
       for (int e = 0; e < 4; e += 2) {
@@ -184,7 +225,26 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
     if (row < V) {
       float4* yr = reinterpret_cast<float4*>(Y + (long long)row * TC_N + c0);
       float4* qr = Q ? reinterpret_cast<float4*>(Q + (long long)row * TC_N + c0) : nullptr;
-      const float4* rr = R1 ? reinterpret_cast<const float4*>(R1 + (long long)row * ldr1 + c0) : nullptr;
+      const float4* rr = R1 && !res_a ? reinterpret_cast<const float4*>(R1 + (long long)row * ldr1 + c0) : nullptr;
+      float res[TC_COLS_PER_WARP];
+      if (res_a) {
+        const int r = quarter * 32 + (tid & 31);
+#pragma unroll
+        for (int c8 = 0; c8 < TC_COLS_PER_WARP; c8 += 8) {
+          const int off = core_off(r, c0 + c8, K);
+          const uint4 h = *reinterpret_cast<const uint4*>(A + off), m = *reinterpret_cast<const uint4*>(A + tile + off),
+                      l = *reinterpret_cast<const uint4*>(A + 2 * tile + off);
+          const uint32_t hw[4] = {h.x, h.y, h.z, h.w}, mw[4] = {m.x, m.y, m.z, m.w}, lw[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int sh = (e & 1) * 16;
+            const float fh = __uint_as_float(((hw[e >> 1] >> sh) & 0xffffu) << 16);
+            const float fm = __uint_as_float(((mw[e >> 1] >> sh) & 0xffffu) << 16);
+            const float fl = __uint_as_float(((lw[e >> 1] >> sh) & 0xffffu) << 16);
+            res[c8 + e] = (fh + fm) + fl;
+          }
+        }
+      }
 #pragma unroll
       for (int c4 = 0; c4 < TC_COLS_PER_WARP / 4; ++c4) {
         float q[4], y[4];
@@ -197,6 +257,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
         if (rr) {
           const float4 t = rr[c4];
           y[0] += t.x; y[1] += t.y; y[2] += t.z; y[3] += t.w;
+        } else if (res_a) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) y[e] += res[4 * c4 + e];
         }
         yr[c4] = make_float4(y[0], y[1], y[2], y[3]);
       }
@@ -223,13 +286,22 @@ bool gemm_tc_supported(int K1, int K2, int N, int ldr1) {
 }
 static_assert(TC_THREADS % 128 == 0 && TC_COLS_PER_WARP % 16 == 0, "epilogue: whole tensor-memory lane quarters, 16-column loads");
 
-cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W, const float* bias,
-                           const float* R1, int ldr1, float* Q, float* Y, int relu, int* err, cudaStream_t s) {
+cudaError_t launch_gemm_tc_image(const float* W, int K, unsigned short* img, cudaStream_t s) {
+  if (K < 16 || K > 128 || K % 16) return cudaErrorInvalidValue;
+  k_gemm_tc_image<<<(TC_N * K + 255) / 256, 256, 0, s>>>(W, K, img);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W,
+                           const unsigned short* Bimg, const float* bias, const float* R1, int ldr1, float* Q, float* Y, int relu, int* err,
+                           cudaStream_t s) {
   if (V <= 0) return cudaSuccess;
   if (!gemm_tc_supported(K1, K2, TC_N, R1 ? ldr1 : 0)) return cudaErrorInvalidValue;
   auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
   if (!a16(Y) || (Q && !a16(Q)) || (R1 && !a16(R1))) return cudaErrorInvalidValue;  // float4 epilogue
   if (!a16(X1) || (ld1 & 3) || (K2 && (!a16(X2) || (ld2 & 3)))) return cudaErrorInvalidValue;  // float4 staging
+  if (Bimg && !a16(Bimg)) return cudaErrorInvalidValue;
+  const int res_a = R1 && R1 == X1 && ldr1 == ld1 && K1 >= TC_N;
   static std::atomic<unsigned> attr{0};  // one bit per device (steps of several contexts may run on host threads)
   int dev = 0;
   cudaGetDevice(&dev);
@@ -239,7 +311,8 @@ cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float*
     attr.fetch_or(1u << dev);
   }
   const int K = K1 + K2;
-  k_gemm_tc<<<(V + TC_M - 1) / TC_M, TC_THREADS, gemm_tc_smem(K), s>>>(V, X1, ld1, K1, X2, ld2, K2, W, bias, R1, ldr1, Q, Y, relu, err);
+  k_gemm_tc<<<(V + TC_M - 1) / TC_M, TC_THREADS, gemm_tc_smem(K), s>>>(V, X1, ld1, K1, X2, ld2, K2, W, reinterpret_cast<const uint4*>(Bimg),
+                                                                      bias, R1, ldr1, res_a, Q, Y, relu, err);
   return cudaGetLastError();
 }
 
