@@ -103,6 +103,7 @@ struct ando_ctx_s {
   // learned preconditioner: weights, activations, S on the static pattern
   DevBuf<int> slot_T;
   DevBuf<float> net_master, net_buf, lw_buf, Sval;
+  std::vector<float> net_host;    // the BF16-rounded weights (net.wq) on the host
   DevBuf<unsigned short> net_bf16;
   NetDev net;
   LearnedWork lw;
@@ -1978,7 +1979,10 @@ int32_t ando_ctx_set_precond_weights(ando_ctx c, const float* w, int32_t n) {
   net_dev_carve(c->net, c->net_buf.p);
   launch_net_prepare(c->net_master.p, c->net, c->net_bf16.p, c->stream);
   CK(cudaGetLastError());
+  c->net_host.resize(net::NPARAM);
+  CK(cudaMemcpyAsync(c->net_host.data(), c->net.wq, sizeof(float) * net::NPARAM, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  c->net.host_wq = c->net_host.data();
   c->net_ready = true;
   c->coeff_valid = false;
   return ANDO_OK;

@@ -61,13 +61,17 @@ __global__ void k_net_transpose(const float* wq, float* wt) {
 
 // ------------------------------------------------------------------ features
 // Edge features of every static slot: the 9 entries of A^_k and its Frobenius norm.
+// Rows of FES floats (16-byte aligned, the last two zero).
 __global__ void k_edge_feats(int nnzb, const float* valh, float* Ef) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nnzb) return;
   const float* a = valh + 9ll * k;
+  float e[FES];
   float s = 0.f;
-  for (int q = 0; q < 9; ++q) { Ef[(long long)k * FE + q] = a[q]; s += a[q] * a[q]; }
-  Ef[(long long)k * FE + 9] = sqrtf(s);
+  for (int q = 0; q < 9; ++q) { e[q] = a[q]; s += a[q] * a[q]; }
+  e[9] = sqrtf(s); e[10] = 0.f; e[11] = 0.f;
+  float4* o = reinterpret_cast<float4*>(Ef + (long long)k * FES);
+  for (int q = 0; q < FES / 4; ++q) o[q] = make_float4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
 }
 // Node features: 1, log(1 + contact blocks), static and contact coupling
 // (sums of |A^_ij|_F), stiffness of the diagonal block relative to the mass
@@ -80,7 +84,7 @@ __global__ void k_node_feats(LsView s, const float* Ef, float* X) {
   int deg = 0, ncont = 0;
   for (int k = s.rowptr[i]; k < s.rowptr[i + 1]; ++k) {
     if (s.cols[k] == i) continue;
-    float nf = Ef[(long long)k * FE + 9];
+    float nf = Ef[(long long)k * FES + 9];
     stat += nf; mx = fmaxf(mx, nf); ++deg;
   }
   if (s.xbegin) {
@@ -215,8 +219,18 @@ __global__ void k_relu_mask(long long n, const float* dh, const float* q, float*
 
 // ------------------------------------------------------------ messages
 // m_i = (1 / deg_i) sum_{j in N(i)} relu(u_j + E e_ij + c); one warp per row,
-// lane l owns channels 2l and 2l+1.
-__global__ void k_msg_fwd(LsView s, const float* u, const float* Ef, const float* Ew, const float* cb, float* m) {
+// lane l owns channels 2l and 2l+1. A row of at most MSG_SLOTS slots loads
+// its columns with one coalesced load and then every neighbour's u at once;
+// each slot's features reach all lanes as three broadcast 16-byte loads.
+// Longer rows walk their slots one by one. Both paths add the same terms in
+// the same order.
+constexpr int MSG_SLOTS = 8;
+__device__ inline void msg_term(float4 q0, float4 q1, float4 q2, const float* e0, const float* e1, float& t0, float& t1) {
+  const float ef[FE] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
+#pragma unroll
+  for (int f = 0; f < FE; ++f) { t0 += e0[f] * ef[f]; t1 += e1[f] * ef[f]; }
+}
+__global__ void __launch_bounds__(TPB) k_msg_fwd(LsView s, const float* u, const float* Ef, const float* Ew, const float* cb, float* m) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   const int c0 = 2 * lane, c1 = c0 + 1;
@@ -226,19 +240,84 @@ __global__ void k_msg_fwd(LsView s, const float* u, const float* Ef, const float
   for (int i = gw; i < s.V; i += nw) {
     float a0 = 0.f, a1 = 0.f;
     int deg = 0;
-    for (int k = s.rowptr[i]; k < s.rowptr[i + 1]; ++k) {
-      int j = s.cols[k];
-      if (j == i) continue;
-      const float* e = Ef + (long long)k * FE;
-      float t0 = u[(long long)j * H + c0] + b0, t1 = u[(long long)j * H + c1] + b1;
-      for (int f = 0; f < FE; ++f) { float ef = e[f]; t0 += e0[f] * ef; t1 += e1[f] * ef; }
-      a0 += fmaxf(t0, 0.f); a1 += fmaxf(t1, 0.f);
-      ++deg;
+    const int kb = s.rowptr[i], ns = s.rowptr[i + 1] - kb;
+    if (ns <= MSG_SLOTS) {
+      const int jl = lane < ns ? s.cols[kb + lane] : -1;
+      float2 uv[MSG_SLOTS];
+#pragma unroll
+      for (int sl = 0; sl < MSG_SLOTS; ++sl) {
+        const int j = __shfl_sync(0xffffffffu, jl, sl);
+        uv[sl] = sl < ns && j != i ? *reinterpret_cast<const float2*>(u + (long long)j * H + c0) : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int sl = 0; sl < MSG_SLOTS; ++sl) {
+        const int j = __shfl_sync(0xffffffffu, jl, sl);
+        if (sl < ns && j != i) {  // uniform over the warp
+          const float4* e4 = reinterpret_cast<const float4*>(Ef + (long long)(kb + sl) * FES);
+          float t0 = uv[sl].x + b0, t1 = uv[sl].y + b1;
+          msg_term(e4[0], e4[1], e4[2], e0, e1, t0, t1);
+          a0 += fmaxf(t0, 0.f); a1 += fmaxf(t1, 0.f);
+          ++deg;
+        }
+      }
+    } else {
+      for (int k = kb; k < kb + ns; ++k) {
+        int j = s.cols[k];
+        if (j == i) continue;
+        const float4* e4 = reinterpret_cast<const float4*>(Ef + (long long)k * FES);
+        float t0 = u[(long long)j * H + c0] + b0, t1 = u[(long long)j * H + c1] + b1;
+        msg_term(e4[0], e4[1], e4[2], e0, e1, t0, t1);
+        a0 += fmaxf(t0, 0.f); a1 += fmaxf(t1, 0.f);
+        ++deg;
+      }
     }
     float inv = deg ? 1.f / float(deg) : 0.f;
     m[(long long)i * H + c0] = a0 * inv;
     m[(long long)i * H + c1] = a1 * inv;
   }
+}
+
+// The same messages with one thread per row (inference): the thread reads its
+// neighbours' whole u rows and its slots' own features, and the edge weights
+// and bias arrive by value as kernel parameters (constant-bank operands of
+// the FMAs), so no value is replicated across lanes. Same terms, same order.
+struct MsgWeights { float E[H * FE]; float c[H]; };
+constexpr int MSG_ROWS_TPB = 128;
+__global__ void __launch_bounds__(MSG_ROWS_TPB) k_msg_rows(LsView s, const float* __restrict__ u, const float* __restrict__ Ef,
+                                                           const MsgWeights P, float* __restrict__ m) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.V) return;
+  float acc[H];
+#pragma unroll
+  for (int c = 0; c < H; ++c) acc[c] = 0.f;
+  int deg = 0;
+  const int ke = s.rowptr[i + 1];
+  for (int k = s.rowptr[i]; k < ke; ++k) {
+    const int j = s.cols[k];
+    if (j == i) continue;
+    const float4* e4 = reinterpret_cast<const float4*>(Ef + (long long)k * FES);
+    const float4 q0 = e4[0], q1 = e4[1], q2 = e4[2];
+    const float ef[FE] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
+    const float4* u4 = reinterpret_cast<const float4*>(u + (long long)j * H);
+#pragma unroll
+    for (int c4 = 0; c4 < H / 4; ++c4) {
+      const float4 uv = u4[c4];
+      const float ux[4] = {uv.x, uv.y, uv.z, uv.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int c = 4 * c4 + e;
+        float t = ux[e] + P.c[c];
+#pragma unroll
+        for (int f = 0; f < FE; ++f) t += P.E[c * FE + f] * ef[f];
+        acc[c] += fmaxf(t, 0.f);
+      }
+    }
+    ++deg;
+  }
+  const float inv = deg ? 1.f / float(deg) : 0.f;
+  float4* mo = reinterpret_cast<float4*>(m + (long long)i * H);
+#pragma unroll
+  for (int c4 = 0; c4 < H / 4; ++c4) mo[c4] = make_float4(acc[4 * c4] * inv, acc[4 * c4 + 1] * inv, acc[4 * c4 + 2] * inv, acc[4 * c4 + 3] * inv);
 }
 
 // Backward of k_msg_fwd. Row j gathers over its slots (j, i) the messages it
@@ -263,7 +342,7 @@ __global__ void __launch_bounds__(TPB) k_msg_bwd(LsView s, const float* u, const
       int kT = s.slot_T[k];
       int deg = s.rowptr[i + 1] - s.rowptr[i] - 1;
       if (deg <= 0) continue;
-      const float* e = Ef + (long long)kT * FE;
+      const float* e = Ef + (long long)kT * FES;
       float t0 = uj0 + b0, t1 = uj1 + b1;
       for (int f = 0; f < FE; ++f) { float ef = e[f]; t0 += e0[f] * ef; t1 += e1[f] * ef; }
       float inv = 1.f / float(deg);
@@ -308,7 +387,7 @@ __global__ void k_dec_fwd(LsView s, const float* h, const float* Ef, const float
       float hj0 = h[(long long)j * H + c0], hj1 = h[(long long)j * H + c1];
       float a = pa + De0[H + c0] * hj0 + De0[H + c1] * hj1;
       float b = pb + De1[H + c0] * hj0 + De1[H + c1] * hj1;
-      if (lane < FE) { float ef = Ef[(long long)k * FE + lane]; a += De0[2 * H + lane] * ef; b += De1[2 * H + lane] * ef; }
+      if (lane < FE) { float ef = Ef[(long long)k * FES + lane]; a += De0[2 * H + lane] * ef; b += De1[2 * H + lane] * ef; }
       a = warp_sum(a); b = warp_sum(b);
       if (lane == 0) { ab[2ll * k] = a + w[DE0]; ab[2ll * k + 1] = b + w[DE0 + 1]; }
     }
@@ -480,7 +559,7 @@ __global__ void __launch_bounds__(TPB) k_dec_bwd(LsView s, const float* h, const
         float hj0 = h[(long long)j * H + c0], hj1 = h[(long long)j * H + c1];
         gA[0] += da * hr0; gA[1] += da * hr1; gA[2] += da * hj0; gA[3] += da * hj1;
         gB[0] += db * hr0; gB[1] += db * hr1; gB[2] += db * hj0; gB[3] += db * hj1;
-        if (lane < FE) { float ef = Ef[(long long)k * FE + lane]; gAe += da * ef; gBe += db * ef; }
+        if (lane < FE) { float ef = Ef[(long long)k * FES + lane]; gAe += da * ef; gBe += db * ef; }
         if (lane == 0) { gde0 += da; gde1 += db; }
       } else {
         long long kT = s.slot_T[k];
@@ -543,7 +622,7 @@ void reduce(const float* part, int off, int n, float* out, cudaStream_t s) {
 
 size_t learned_work_floats(int V, int nnzb, bool training) {
   size_t VH = size_t(V) * H;
-  size_t n = size_t(V) * FN + size_t(nnzb) * FE + VH * (NL + 1) + 3 * VH * NL + VH + V + 2ull * nnzb;
+  size_t n = size_t(V) * FN + size_t(nnzb) * FES + VH * (NL + 1) + 3 * VH * NL + VH + V + 2ull * nnzb;
   if (training) n += 7 * VH + V + 2ull * nnzb + size_t(GRID) * PART;
   return n + 4 * 64;  // every buffer starts on a 16-byte boundary (vector loads and stores)
 }
@@ -553,7 +632,7 @@ void learned_work_carve(LearnedWork& w, float* base, int V, int nnzb, bool train
   float* p = base;
   auto take = [&](size_t n) { float* r = p; p += (n + 3) & ~size_t(3); return r; };
   w.V = V; w.nnzb = nnzb; w.training = training; w.base = base;
-  w.X = take(size_t(V) * FN); w.Ef = take(size_t(nnzb) * FE);
+  w.X = take(size_t(V) * FN); w.Ef = take(size_t(nnzb) * FES);
   for (int l = 0; l <= NL; ++l) w.h[l] = take(VH);
   for (int l = 0; l < NL; ++l) { w.u[l] = take(VH); w.m[l] = take(VH); w.q[l] = take(VH); }
   w.q0 = take(VH); w.zv = take(V); w.ab = take(2ull * nnzb);
@@ -598,7 +677,15 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
     // u = U h and h' = relu(W [h ; m] + b) + h on the tensor cores
     const unsigned short* bi = n.bimg ? n.bimg + l * BIMG_LSIZE : nullptr;
     launch_gemm_tc(V, w.h[l], H, H, nullptr, 0, 0, L + L_U, bi ? bi + BIMG_U : nullptr, nullptr, nullptr, 0, nullptr, w.u[l], 0, err, st);
-    k_msg_fwd<<<wgrid, TPB, 0, st>>>(s, w.u[l], w.Ef, L + L_E, L + L_C, w.m[l]);
+    if (n.host_wq && !w.training) {
+      MsgWeights P;
+      const float* Lh = n.host_wq + LAYER0 + l * L_SIZE;
+      for (int q = 0; q < H * FE; ++q) P.E[q] = Lh[L_E + q];
+      for (int q = 0; q < H; ++q) P.c[q] = Lh[L_C + q];
+      k_msg_rows<<<nblk(V, MSG_ROWS_TPB), MSG_ROWS_TPB, 0, st>>>(s, w.u[l], w.Ef, P, w.m[l]);
+    } else {
+      k_msg_fwd<<<wgrid, TPB, 0, st>>>(s, w.u[l], w.Ef, L + L_E, L + L_C, w.m[l]);
+    }
     launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, bi ? bi + BIMG_W : nullptr, L + L_B, w.h[l], H, w.training ? w.q[l] : nullptr,
                    w.h[l + 1], 1, err, st);
   }

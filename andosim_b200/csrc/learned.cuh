@@ -21,6 +21,7 @@ namespace ando {
 namespace net {
 constexpr int FN = 8;              // node features
 constexpr int FE = 10;             // edge features (the 9 entries of A^_ij and its Frobenius norm)
+constexpr int FES = 12;            // row stride of the edge features in memory (16-byte rows)
 constexpr int H = 64;              // width
 constexpr int NL = 3;              // message-passing layers
 constexpr int DE_IN = 2 * H + FE;  // edge decoder input [h_i ; h_j ; e_ij]
@@ -60,7 +61,7 @@ struct LearnedWork {
   int V = 0, nnzb = 0;
   bool training = false;
   float* base = nullptr;
-  float *X, *Ef;                        // V x FN, nnzb x FE
+  float *X, *Ef;                        // V x FN, nnzb x FES
   float *h[net::NL + 1], *u[net::NL], *m[net::NL], *q[net::NL], *q0;
   float *zv, *ab;                       // V, 2 nnzb
   // backward
@@ -77,6 +78,7 @@ struct NetDev {
   float* wq = nullptr;       // NPARAM, BF16-representable values
   float* wt = nullptr;       // transposed copies of the dense matrices (forward layout)
   unsigned short* bimg = nullptr;  // hidden layers' U and W as tensor-core B operand images (launch_gemm_tc_image)
+  const float* host_wq = nullptr;  // host copy of wq (may be null): lets inference pass small weight blocks by value
 };
 size_t net_dev_floats();
 void net_dev_carve(NetDev& n, float* base);
