@@ -151,6 +151,16 @@ __global__ void k_rank(const int* order, int n, int* rank) {
   if (p < n) rank[order[p]] = p;
 }
 
+// Per sorted leaf position: {primitive, its vertices (-1 past the arity)},
+// so a query's leaf test is one 16-byte load.
+__global__ void k_leafv(const int* order, const int* prims, int arity, int n, int4* leafv) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int prim = order[p];
+  const int* v = prims + (long long)arity * prim;
+  leafv[p] = make_int4(prim, v[0], arity > 1 ? v[1] : -1, arity > 2 ? v[2] : -1);
+}
+
 __device__ inline Box ld_box_volatile(const Box* b) {
   const volatile float* v = reinterpret_cast<const volatile float*>(b);
   Box r;
@@ -349,9 +359,8 @@ __device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, in
 // One thread per query. kind 0: query = vertex (point box +-1e-4 inflated by
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
 // prims = edges, keep e1 < e2 without shared vertex.
-__global__ void k_query(const double* x, const double* x1, const int* qprims, const int* qorder, int kind, int nq, float pad, const int* prims,
-                        int n, const int* order, const int* rank, const LbvhInner* inner, const Box* nodes, int2* out, int* count,
-                        int cap) {
+__global__ void k_query(const double* x, const double* x1, const int* qprims, const int* qorder, int kind, int nq, float pad, int n,
+                        const int4* leafv, const int* rank, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < nq;
   const int q = active && qorder ? qorder[t] : t;
@@ -403,14 +412,11 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
     else if (overlap(qb, nodes[0])) node = 0;
   }
   auto accept = [&](int leaf) {
-    int prim = order[leaf - leaf0];
+    const int4 lv = leafv[leaf - leaf0];
     bool hit;
-    if (kind == 0) hit = prims[3 * prim] != q && prims[3 * prim + 1] != q && prims[3 * prim + 2] != q;
-    else {
-      int pa = prims[2 * prim], pc = prims[2 * prim + 1];
-      hit = leaf - leaf0 > qpos && pa != qa && pa != qc && pc != qa && pc != qc;
-    }
-    return hit ? prim : -1;
+    if (kind == 0) hit = lv.y != q && lv.z != q && lv.w != q;
+    else hit = leaf - leaf0 > qpos && lv.y != qa && lv.y != qc && lv.z != qa && lv.z != qc;
+    return hit ? lv.x : -1;
   };
   auto emit_pair = [&](int prim) {  // (lower, higher) edge index for the self query
     const bool hit = prim >= 0;
@@ -520,6 +526,7 @@ cudaError_t Lbvh::reserve_prims(int n) {
   if ((e = rank.reserve(N))) return e;
   if ((e = arrive.reserve(N))) return e;
   if ((e = topo.reserve(N))) return e;
+  if ((e = leafv.reserve(N))) return e;
   if ((e = topflag.reserve(N))) return e;
   if ((e = topnum.reserve(N))) return e;
   if ((e = toprec.reserve(N))) return e;
@@ -546,6 +553,7 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
   if ((e = tmp.reserve(bytes))) return e;
   if ((e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, keys.p, keys_sorted.p, idx.p, order.p, n, 0, 64, s))) return e;
   k_rank<<<nblk(n), TPB, 0, s>>>(order.p, n, rank.p);
+  k_leafv<<<nblk(n), TPB, 0, s>>>(order.p, prims, arity, n, leafv.p);
   if (n > 1) {
     if ((e = cudaMemsetAsync(parent.p, 0xff, sizeof(int) * (2 * n - 1), s))) return e;
     k_karras<<<nblk(n - 1), TPB, 0, s>>>(keys_sorted.p, n, parent.p, inner.p, topo.p);
@@ -560,7 +568,7 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
   }
   k_top_count<<<1, 1, 0, s>>>(topflag.p, topnum.p, n, meta.p, cuts.p);
   if ((e = launch_refit(x, x1, pad, s))) return e;
-  launches += (n > 1 ? 8 : 7) + (n > RF_CUT ? 1 : 0);
+  launches += (n > 1 ? 9 : 8) + (n > RF_CUT ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -616,7 +624,7 @@ cudaError_t run_query(Lbvh& B, const double* x, const double* x1, int kind, cons
   for (int attempt = 0; attempt < 2; ++attempt) {
     int cap = int(scratch.n);
     if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.prims, B.n, B.order.p, B.rank.p, B.inner.p, B.nodes.p,
+    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.n, B.leafv.p, B.rank.p, B.inner.p, B.nodes.p,
                                      scratch.p, counter.p, cap);
     B.launches += 1;
     int cnt2[2] = {0, 0};
@@ -660,7 +668,7 @@ cudaError_t Lbvh::contacts_launch(const double* x, int kind, const int* qprims, 
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   if ((e = surv.reserve(scratch.n))) return e;
   const int cap = int(scratch.n);
-  k_query<<<nblk(nq), TPB, 0, s>>>(x, nullptr, qprims, qorder, kind, nq, pad, prims, n, order.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, nullptr, qprims, qorder, kind, nq, pad, n, leafv.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
   k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, gap, surv.p, counter.p + 2);
   launches += 2;
   return cudaGetLastError();
@@ -696,7 +704,7 @@ cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   const int cap = int(scratch.n);
   if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, prims, n, order.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, n, leafv.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
   k_pairs_toi<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, ext, eta_min, near, toi, overflow);
   launches += 2;
   return cudaGetLastError();

@@ -29,6 +29,7 @@ struct Lbvh {
   DevBuf<int> idx, order, parent, arrive, bounds;
   DevBuf<int> rank;             // sorted leaf position of each primitive (inverse of order)
   DevBuf<int4> topo;            // per internal node: first leaf, split, last leaf, parent
+  DevBuf<int4> leafv;           // per sorted leaf: primitive and its vertices (-1 past the arity)
   // refit schedule made at build time: nodes above the cut (flags, numbers,
   // records), the cut subtrees as leaf ranges, meta = {top nodes, cut entries}
   DevBuf<int> topflag, topnum, meta;

@@ -277,10 +277,11 @@ __global__ void __launch_bounds__(TPB) k_msg_fwd(LsView s, const float* u, const
   }
 }
 
-// The same messages with one thread per row (inference): the thread reads its
-// neighbours' whole u rows and its slots' own features, and the edge weights
-// and bias arrive by value as kernel parameters (constant-bank operands of
-// the FMAs), so no value is replicated across lanes. Same terms, same order.
+// The same messages at inference with one thread per row: the thread reads
+// its slots' own features and its neighbours' whole u rows, and the edge
+// weights and bias arrive by value as kernel parameters (constant-bank
+// operands of the FMAs), so no value is replicated across lanes. Same terms,
+// same order as k_msg_fwd.
 struct MsgWeights { float E[H * FE]; float c[H]; };
 constexpr int MSG_ROWS_TPB = 128;
 __global__ void __launch_bounds__(MSG_ROWS_TPB) k_msg_rows(LsView s, const float* __restrict__ u, const float* __restrict__ Ef,
