@@ -240,6 +240,21 @@ __global__ void k_top_count(const int* flag, const int* topnum, int n, int* meta
   if (m == 0) cuts[0] = make_int2(0, n - 1);
 }
 
+__device__ inline void store_children(LbvhInner* rec, const Box& l, const Box& r) {
+  float4* d = reinterpret_cast<float4*>(rec);  // lbox[6], rbox[6]: the record's first 48 bytes
+  d[0] = make_float4(l.lo[0], l.lo[1], l.lo[2], l.hi[0]);
+  d[1] = make_float4(l.hi[1], l.hi[2], r.lo[0], r.lo[1]);
+  d[2] = make_float4(r.lo[2], r.hi[0], r.hi[1], r.hi[2]);
+}
+
+__device__ inline void store_side(LbvhInner* rec, bool left, const Box& b) {
+  float* dst = left ? rec->lbox : rec->rbox;
+  for (int k = 0; k < 3; ++k) { dst[k] = b.lo[k]; dst[3 + k] = b.hi[k]; }
+}
+
+// The climbs below touch shared memory only (their block-scope fences then
+// have no global store to wait for); each kernel writes its boxes to global
+// memory in one pass after the climb.
 __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const double* x1, const int* prims, int arity, float pad,
                                                       const int* order, int n, const int* parent, const int4* topo, const int2* cuts,
                                                       const int* meta, Box* nodes, int* arrive, LbvhInner* inner) {
@@ -256,46 +271,75 @@ __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const dou
       S.arr[t] = 0;
       const int q = c0 + t;
       if (q < n - 1) S.topo[t] = topo[q];
-      const Box b = prim_box(x, x1, prims, arity, order[q], pad);
-      S.leaf[t] = b;
-      nodes[n - 1 + q] = b;
+      S.leaf[t] = prim_box(x, x1, prims, arity, order[q], pad);
     }
     __syncthreads();
+    const int4 outside = make_int4(-1, 0, 0, -1);  // fails the inside test
     for (int t = threadIdx.x; t <= c1 - c0; t += RF_TPB) {
       const int i = c0 + t;
       Box box = S.leaf[t];
       int chi = i;  // last leaf under the current node
       int p = n > 1 ? parent[n - 1 + i] : -1;
-      int4 tp = p < 0 ? make_int4(0, 0, 0, -1) : (p <= c1 && p >= c0 ? S.topo[p - c0] : __ldg(topo + p));
-      while (p >= 0) {
+      int4 tp = p >= c0 && p <= c1 ? S.topo[p - c0] : outside;
+      while (p >= 0 && tp.x >= c0 && tp.z <= c1) {  // p's leaves all in this subtree
         const int plo = tp.x, pl = tp.y, phi = tp.z, pp = tp.w;
-        const bool inside = plo >= c0 && phi <= c1;
         const bool from_left = chi == pl;
-        float* dst = from_left ? inner[p].lbox : inner[p].rbox;
-        for (int k = 0; k < 3; ++k) { dst[k] = box.lo[k]; dst[3 + k] = box.hi[k]; }
-        if (!inside && !top_global) break;  // a top node: k_refit_top finishes it
-        // topology of the next parent (read-only here), fetched before the arrival
-        const int4 tnext = pp < 0 ? make_int4(0, 0, 0, -1) : (pp <= c1 && pp >= c0 ? S.topo[pp - c0] : __ldg(topo + pp));
         // the sibling covers [sl, sh]: a leaf when sl == sh, else internal node sidx
         const int sl = from_left ? pl + 1 : plo, sh = from_left ? phi : pl, sidx = from_left ? pl + 1 : pl;
-        if (inside) {
-          __threadfence_block();
-          if (atomicAdd(&S.arr[p - c0], 1) == 0) break;
-          __threadfence_block();
-          box = unite(box, sl == sh ? ld_box_volatile(&S.leaf[sl - c0]) : ld_box_volatile(&S.node[sidx - c0]));
-          S.node[p - c0] = box;
-        } else {
-          // this thread wrote nodes[] of its current node before the release
+        __threadfence_block();
+        if (atomicAdd(&S.arr[p - c0], 1) == 0) break;
+        __threadfence_block();
+        box = unite(box, sl == sh ? ld_box_volatile(&S.leaf[sl - c0]) : ld_box_volatile(&S.node[sidx - c0]));
+        S.node[p - c0] = box;
+        chi = phi;
+        p = pp;
+        tp = p >= c0 && p <= c1 ? S.topo[p - c0] : outside;
+      }
+    }
+    __syncthreads();
+    // write-out: leaf boxes, and the boxes and child boxes of the subtree's internal nodes
+    for (int t = threadIdx.x; t <= c1 - c0; t += RF_TPB) {
+      const int q = c0 + t;
+      nodes[n - 1 + q] = S.leaf[t];
+      if (q < n - 1) {
+        const int4 tq = S.topo[t];
+        if (tq.x >= c0 && tq.z <= c1) {
+          const Box& bl = tq.x == tq.y ? S.leaf[tq.x - c0] : S.node[tq.y - c0];
+          const Box& br = tq.y + 1 == tq.z ? S.leaf[tq.z - c0] : S.node[tq.y + 1 - c0];
+          store_children(inner + q, bl, br);
+          nodes[q] = S.node[t];
+        }
+      }
+    }
+    // the subtree's root (index c0 or c1, or the leaf) goes into its parent's
+    // record; carrying on through the top nodes needs every thread's nodes[]
+    // published first
+    if (top_global) {
+      __threadfence();
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      int root = -1;  // internal root index, -1: a single leaf
+      if (c1 > c0) root = (S.topo[0].x == c0 && S.topo[0].z == c1) ? c0 : c1;
+      Box box = root < 0 ? S.leaf[0] : S.node[root - c0];
+      int p = root < 0 ? (n > 1 ? parent[n - 1 + c0] : -1) : S.topo[root - c0].w;
+      int chi = c1;
+      if (p >= 0) {
+        while (p >= 0) {
+          const int4 tp = __ldg(topo + p);
+          const bool from_left = chi == tp.y;
+          store_side(inner + p, from_left, box);
+          if (!top_global) break;  // k_refit_top finishes the top nodes
           int prior;
           asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(prior) : "l"(arrive + p) : "memory");
           if (prior == 0) break;
           arrive[p] = 0;
+          const int sl = from_left ? tp.y + 1 : tp.x, sh = from_left ? tp.z : tp.y, sidx = from_left ? tp.y + 1 : tp.y;
           box = unite(box, ld_box_cg(nodes + (sl == sh ? n - 1 + sl : sidx)));
+          nodes[p] = box;
+          chi = tp.z;
+          p = tp.w;
         }
-        nodes[p] = box;
-        chi = phi;
-        p = pp;
-        tp = tnext;
       }
     }
   }
@@ -319,13 +363,10 @@ __global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, const in
     Box box = unite(ld_box_cg(nodes + (-r.z - 1)), ld_box_cg(nodes + (-r.w - 1)));
     while (true) {
       S.box[cur] = box;
-      nodes[r.x] = box;
       const int pc = r.y;
       if (pc < 0) break;
       const int4 pr = S.rec[pc];
       const bool from_left = pr.z == cur;
-      float* dst = from_left ? inner[pr.x].lbox : inner[pr.x].rbox;
-      for (int q = 0; q < 3; ++q) { dst[q] = box.lo[q]; dst[3 + q] = box.hi[q]; }
       __threadfence_block();
       if (atomicAdd(&S.arr[pc], 1) == 0) break;
       __threadfence_block();
@@ -334,6 +375,14 @@ __global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, const in
       cur = pc;
       r = pr;
     }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < m; k += TOP_TPB) {
+    const int4 r = S.rec[k];
+    nodes[r.x] = S.box[k];
+    const Box bl = r.z >= 0 ? S.box[r.z] : ld_box_cg(nodes + (-r.z - 1));
+    const Box br = r.w >= 0 ? S.box[r.w] : ld_box_cg(nodes + (-r.w - 1));
+    store_children(inner + r.x, bl, br);
   }
 }
 
