@@ -158,6 +158,7 @@ def lib() -> C.CDLL:
     L.ando_ctx_select_assembly_tpb.restype = I32; L.ando_ctx_select_assembly_tpb.argtypes = [P, I32]
     L.ando_ctx_assembly_tpb.restype = I32; L.ando_ctx_assembly_tpb.argtypes = [P, pi, pi]
     L.ando_ctx_set_pair_capacity.restype = I32; L.ando_ctx_set_pair_capacity.argtypes = [P, I32]
+    L.ando_ctx_set_refit_top_capacity.restype = I32; L.ando_ctx_set_refit_top_capacity.argtypes = [P, I32]
     L.ando_ctx_pcg_shape.restype = I32; L.ando_ctx_pcg_shape.argtypes = [P, I32, pi, pi, pd]
     L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
     pu8 = C.POINTER(C.c_ubyte)
@@ -390,6 +391,10 @@ class Scene:
     def set_pair_capacity(self, pairs: int):
         """Start the broad-phase candidate buffers at `pairs` (they grow on demand)."""
         _check(lib().ando_ctx_set_pair_capacity(self.ctx, pairs), "ando_ctx_set_pair_capacity")
+
+    def set_refit_top_capacity(self, nodes: int):
+        """Top nodes the one-CTA refit finishes in shared memory (-1: 4096); more go through global counters."""
+        _check(lib().ando_ctx_set_refit_top_capacity(self.ctx, nodes), "ando_ctx_set_refit_top_capacity")
 
     def select_assembly_tpb(self, index: int = -1):
         """Fix scaled-assembly block-size candidate `index` (-1: autotune on the next first assembly)."""

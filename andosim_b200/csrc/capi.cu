@@ -1902,6 +1902,17 @@ int32_t ando_ctx_set_pair_capacity(ando_ctx c, int32_t pairs) {
   return ANDO_OK;
 }
 
+int32_t ando_ctx_set_refit_top_capacity(ando_ctx c, int32_t nodes) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nodes < -1 || nodes > 4096) return fail(ANDO_ERR_INVALID, "refit top capacity must be in [-1, 4096]");
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->side) CK(cudaStreamSynchronize(c->side));
+  c->bvh_tri.top_cap = nodes;
+  c->bvh_edge.top_cap = nodes;
+  return ANDO_OK;
+}
+
 int32_t ando_ctx_select_assembly_tpb(ando_ctx c, int32_t index) {
   int rc = check_ctx(c);
   if (rc) return rc;

@@ -196,7 +196,8 @@ __device__ inline Box unite(const Box& a, const Box& b) {
 // k_refit_top: one CTA finishes the top nodes the same way in shared memory,
 // reading the cut subtrees' boxes from nodes[].
 //
-// When the top has more nodes than one CTA holds, k_refit_cut carries on
+// When the top has more nodes than one CTA holds (or than the caller's
+// capacity, Lbvh::top_cap), k_refit_cut carries on
 // through the top nodes itself with global arrival counters (acquire/release
 // atomics; the second arrival zeroes the counter for the next refit) and
 // k_refit_top does nothing. Min/max are exact, so every box has the same bits
@@ -257,11 +258,11 @@ __device__ inline void store_side(LbvhInner* rec, bool left, const Box& b) {
 // memory in one pass after the climb.
 __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const double* x1, const int* prims, int arity, float pad,
                                                       const int* order, int n, const int* parent, const int4* topo, const int2* cuts,
-                                                      const int* meta, Box* nodes, int* arrive, LbvhInner* inner) {
+                                                      const int* meta, int top_cap, Box* nodes, int* arrive, LbvhInner* inner) {
   extern __shared__ __align__(16) unsigned char rf_raw[];
   RefitSmem& S = *reinterpret_cast<RefitSmem*>(rf_raw);
   const int ncut = meta[1];
-  const bool top_global = meta[0] > TOP_MAX;
+  const bool top_global = meta[0] > top_cap;
   for (int cb = blockIdx.x; cb < ncut; cb += gridDim.x) {
     const int2 cut = cuts[cb];
     if (cut.x < 0) continue;  // uniform over the CTA
@@ -345,11 +346,11 @@ __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const dou
   }
 }
 
-__global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, const int4* rec, Box* nodes, LbvhInner* inner) {
+__global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, int top_cap, const int4* rec, Box* nodes, LbvhInner* inner) {
   extern __shared__ __align__(16) unsigned char rt_raw[];
   TopSmem& S = *reinterpret_cast<TopSmem*>(rt_raw);
   const int m = meta[0];
-  if (m <= 0 || m > TOP_MAX) return;
+  if (m <= 0 || m > top_cap) return;
   for (int k = threadIdx.x; k < m; k += TOP_TPB) {
     const int4 r = rec[k];
     S.rec[k] = r;
@@ -647,9 +648,10 @@ cudaError_t Lbvh::launch_refit(const double* x, const double* x1, float pad, cud
   // grid-stride over the cut list (its length stays on the device): about
   // three subtrees per SM resident at once
   const int grid = std::max(1, std::min(3 * sms, 2 * ((n + 255) / 256)));
-  k_refit_cut<<<grid, RF_TPB, sizeof(RefitSmem), s>>>(x, x1, prims, arity, pad, order.p, n, parent.p, topo.p, cuts.p, meta.p, nodes.p,
-                                                      arrive.p, inner.p);
-  if (n > RF_CUT) k_refit_top<<<1, TOP_TPB, sizeof(TopSmem), s>>>(meta.p, toprec.p, nodes.p, inner.p);
+  const int cap = top_cap < 0 || top_cap > TOP_MAX ? TOP_MAX : top_cap;
+  k_refit_cut<<<grid, RF_TPB, sizeof(RefitSmem), s>>>(x, x1, prims, arity, pad, order.p, n, parent.p, topo.p, cuts.p, meta.p, cap,
+                                                      nodes.p, arrive.p, inner.p);
+  if (n > RF_CUT) k_refit_top<<<1, TOP_TPB, sizeof(TopSmem), s>>>(meta.p, cap, toprec.p, nodes.p, inner.p);
   return cudaGetLastError();
 }
 

@@ -37,6 +37,9 @@ struct Lbvh {
   DevBuf<int2> cuts;
   DevBuf<int2> surv;            // candidates kept by the narrow phase of contacts_launch
   long long launches = 0;
+  // top nodes the one-CTA refit finishes in shared memory (at most 4096;
+  // negative: 4096); above that the cut kernel climbs on with global counters
+  int top_cap = -1;
 
   cudaError_t reserve_prims(int n);
   // x1 (may be null): boxes swept from positions x to x1

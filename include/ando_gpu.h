@@ -303,6 +303,13 @@ ANDO_API int32_t ando_ctx_pcg_shape(ando_ctx ctx, int32_t learned, int32_t* coun
  * reference counterpart. */
 ANDO_API int32_t ando_ctx_set_pair_capacity(ando_ctx ctx, int32_t pairs);
 
+/* Nodes above the refit's cut (more than 1,024 leaves) that one CTA finishes
+ * in shared memory, 0..4096 (-1: 4096, the default). A hierarchy with more
+ * top nodes is refit through global acquire/release arrival counters instead;
+ * both give the same boxes. Lowering it exercises that path on small meshes.
+ * No reference counterpart. */
+ANDO_API int32_t ando_ctx_set_refit_top_capacity(ando_ctx ctx, int32_t nodes);
+
 /* Threads per block of the CORRECTED block-scaled assembly (candidates 128,
  * 256, 512; one thread per vertex or block slot, so every candidate gives the
  * same bits). Index -1 (default): the first assembly of a mesh times every

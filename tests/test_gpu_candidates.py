@@ -13,8 +13,10 @@ from andosim_b200 import scenes
 pytestmark = pytest.mark.gpu
 
 
-def run(abi, sc, capacity, frames=4):
+def run(abi, sc, capacity, frames=4, top_cap=None):
     S = abi.Scene(sc.vertices, sc.triangles, sc.material)
+    if top_cap is not None:
+        S.set_refit_top_capacity(top_cap)
     p = abi.make_params(sc.params, semantics="corrected")
     stats = []
     for f in range(frames):
@@ -41,4 +43,27 @@ def test_pair_capacity_must_be_positive(abi):
     S = abi.Scene(sc.vertices, sc.triangles, sc.material)
     with pytest.raises(abi.AbiError):
         S.set_pair_capacity(0)
+    S.close()
+
+
+def test_global_counter_refit_gives_the_same_trajectory(abi):
+    """A top capacity of 0 sends every node above the refit's cut through the
+    global acquire/release arrival counters instead of the one-CTA shared
+    memory climb; the boxes, hence the trajectory, are the same bits."""
+    sc = scenes.c4(n=48)  # 8,836 triangles and 13,442 edges: nodes above the 1,024-leaf cut
+    x0, v0, s0 = run(abi, sc, None)
+    x1, v1, s1 = run(abi, sc, None, top_cap=0)
+    x2, v2, s2 = run(abi, sc, None, top_cap=3)
+    assert [st["pcg_iters"] for st in s1] == [st["pcg_iters"] for st in s0]
+    assert np.array_equal(x1, x0) and np.array_equal(v1, v0)
+    assert np.array_equal(x2, x0) and np.array_equal(v2, v0)
+
+
+def test_refit_top_capacity_is_checked(abi):
+    sc = scenes.c4(n=16)
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material)
+    for bad in (-2, 4097):
+        with pytest.raises(abi.AbiError):
+            S.set_refit_top_capacity(bad)
+    S.set_refit_top_capacity(-1)
     S.close()
