@@ -96,6 +96,7 @@ struct ando_ctx_s {
 
   // SELL-32 copy of the static pattern for the scaled PCG (pcg.cu)
   DevBuf<int> chunk_off, sell_col, sell_base;
+  int sell_wmax = 0;              // column slots of the widest SELL-32 slice
   DevBuf<float> valh_sell, S_coef, S_diag;   // S_coef / S_diag: the learned S in the PCG's form
   bool Sval_stale = false;                   // slot-major S not written by the steps since
   int sell_blocks = 0;
@@ -692,7 +693,7 @@ void enqueue_scaled_assembly_tpb(ando_ctx c, const StepParams& sp, cudaStream_t 
   launch_diag_factor(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->g.p, c->Linv.p, c->Lf.p, c->bhat.p,
                      c->chol_ok.p, c->ctrl.p, s, tpb);
   launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p, c->val.p,
-                         c->valh.p, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s, tpb);
+                         c->valh.p, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s, tpb, c->chunk_off.p, c->sell_wmax);
 }
 
 void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
@@ -1383,6 +1384,8 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->diag_slot.upload(diag_slot.data(), V, s));
   CK(c->slot_T.upload(slotT.data(), nnzb, s));
   c->sell_blocks = choff[nch];
+  c->sell_wmax = 0;
+  for (int ch = 0; ch < nch; ++ch) c->sell_wmax = std::max(c->sell_wmax, (choff[ch + 1] - choff[ch]) / 32);
   CK(c->chunk_off.upload(choff.data(), nch + 1, s));
   CK(c->sell_col.upload(scol.data(), choff[nch], s));
   CK(c->sell_base.upload(sbase.data(), nnzb, s));

@@ -6,6 +6,8 @@
 // precomputed sorted lists, never accumulated with floating-point atomics.
 #include <cfloat>
 
+#include <atomic>
+
 #include "kernels.cuh"
 
 namespace ando {
@@ -778,7 +780,7 @@ __global__ void k_diag_factor(MeshDev m, const unsigned char* sflags, const Stra
   if (fixed && fixed[i]) {
     for (int k = 0; k < 9; ++k) H[k] = (k % 4 == 0) ? 1.0 : 0.0;
   } else {
-    slot_block(m, m.diag_slot[i], i, i, sflags, sv, diag_extra, enable_strain, H);
+    slot_block(m, m.diag_slot[i], i, i, sflags, sv, diag_extra, enable_strain && ctrl->strain_active > 0, H);
   }
   Tri3 L;
   bool ok = chol3(H, L);
@@ -812,21 +814,21 @@ __global__ void k_diag_factor(MeshDev m, const unsigned char* sflags, const Stra
 // Per slot: the unscaled block (val, FP32; optional) and the scaled block
 // valh = L_row^-1 H L_col^-T (FP32, computed in FP64). Diagonal slots of
 // factored rows are exactly I.
-__global__ void k_assemble_scaled(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
-                                  const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                                  const int* sell_base, float* valh_sell, const Ctrl* ctrl) {
-  if (ctrl->converged) return;
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= m.nnzb) return;
+// One scaled slot: R = the scaled block (FP32), H = the unscaled block. The
+// scaled kernels pass enable_strain only when the strain pass of this Newton
+// iteration counted an active face (ctrl->strain_active): with none, every
+// face's flag is zero and the contribution walk adds nothing.
+__device__ inline void scaled_slot(const MeshDev& m, int s, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra,
+                                   int enable_strain, const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok,
+                                   float R[9], float Hf[9]) {
   int row = m.slot_row[s], col = m.cols[s];
-  float R[9];
   if (fixed && (fixed[row] || fixed[col])) {
     float one = row == col ? 1.f : 0.f;
-    for (int k = 0; k < 9; ++k) { R[k] = (k % 4 == 0) ? one : 0.f; if (val) val[9 * (long long)s + k] = R[k]; }
+    for (int k = 0; k < 9; ++k) { R[k] = (k % 4 == 0) ? one : 0.f; Hf[k] = R[k]; }
   } else {
     double H[9];
     slot_block(m, s, row, col, sflags, sv, diag_extra, enable_strain, H);
-    if (val) for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = float(H[k]);
+    for (int k = 0; k < 9; ++k) Hf[k] = float(H[k]);
     if (row == col && chol_ok[row]) {
       for (int k = 0; k < 9; ++k) R[k] = (k % 4 == 0) ? 1.f : 0.f;
     } else {
@@ -835,9 +837,60 @@ __global__ void k_assemble_scaled(MeshDev m, const unsigned char* sflags, const 
       for (int k = 0; k < 9; ++k) R[k] = float(Rd[k]);
     }
   }
+}
+
+__global__ void k_assemble_scaled(MeshDev m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
+                                  const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
+                                  const int* sell_base, float* valh_sell, const Ctrl* ctrl) {
+  if (ctrl->converged) return;
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= m.nnzb) return;
+  float R[9], Hf[9];
+  scaled_slot(m, s, sflags, sv, diag_extra, enable_strain && ctrl->strain_active > 0, fixed, Linv, chol_ok, R, Hf);
+  if (val) for (int k = 0; k < 9; ++k) val[9 * (long long)s + k] = Hf[k];
   float* vh = valh + 9 * (long long)s;
   float* vs = valh_sell + sell_base[s];
   for (int k = 0; k < 9; ++k) { vh[k] = R[k]; vs[32 * k] = R[k]; }
+}
+
+// The same values, one CTA per 32-row SELL slice: the slice's CSR slots
+// (contiguous) and its SELL region (contiguous, 9 x 32 floats per column
+// slot) are staged in shared memory and written with coalesced stores; the
+// SELL padding gets zeros. wmax = the widest slice (column slots).
+__global__ void __launch_bounds__(ASM_SLICE_TPB) k_assemble_scaled_slice(MeshDev m, const unsigned char* sflags, const StrainSV* sv,
+                                                                         const double* diag_extra, int enable_strain,
+                                                                         const unsigned char* fixed, const double* Linv,
+                                                                         const unsigned char* chol_ok, float* val, float* valh,
+                                                                         const int* sell_base, const int* chunk_off, int wmax,
+                                                                         float* valh_sell, const Ctrl* ctrl) {
+  if (ctrl->converged) return;
+  extern __shared__ float asm_sm[];
+  const int ch = blockIdx.x;
+  const int r0 = 32 * ch, r1 = min(m.V, r0 + 32);
+  const int k0 = m.rowptr[r0], nk = m.rowptr[r1] - k0;
+  const int sell0 = 9 * chunk_off[ch], nsell = 9 * (chunk_off[ch + 1] - chunk_off[ch]);
+  float* cs = asm_sm;                   // 9 nk: scaled blocks, CSR order
+  float* cv = cs + 9 * 32 * wmax;       // 9 nk: unscaled blocks, CSR order
+  float* ss = cv + 9 * 32 * wmax;       // nsell: SELL order
+  for (int q = threadIdx.x; q < nsell; q += ASM_SLICE_TPB) ss[q] = 0.f;
+  const int strain_on = enable_strain && ctrl->strain_active > 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < nk; t += ASM_SLICE_TPB) {
+    const int s = k0 + t;
+    float R[9], Hf[9];
+    scaled_slot(m, s, sflags, sv, diag_extra, strain_on, fixed, Linv, chol_ok, R, Hf);
+    const int sp = sell_base[s] - sell0;
+    for (int k = 0; k < 9; ++k) { cs[9 * t + k] = R[k]; cv[9 * t + k] = Hf[k]; ss[sp + 32 * k] = R[k]; }
+  }
+  __syncthreads();
+  float* vh = valh + 9ll * k0;
+  float* vv = val ? val + 9ll * k0 : nullptr;
+  for (int q = threadIdx.x; q < 9 * nk; q += ASM_SLICE_TPB) {
+    vh[q] = cs[q];
+    if (vv) vv[q] = cv[q];
+  }
+  float* vs = valh_sell + sell0;
+  for (int q = threadIdx.x; q < nsell; q += ASM_SLICE_TPB) vs[q] = ss[q];
 }
 
 // Contact blocks outside the static pattern. Entries of the same (row, col)
@@ -1263,9 +1316,26 @@ void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const Str
 }
 void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                             const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s, int tpb) {
-  if (m.nnzb) k_assemble_scaled<<<nblk(m.nnzb, tpb), tpb, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh,
-                                                                  sell_base, valh_sell, ctrl);
+                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s, int tpb, const int* chunk_off,
+                            int wmax) {
+  if (!m.nnzb) return;
+  if (chunk_off && wmax > 0 && wmax <= ASM_SLICE_WMAX) {
+    static std::atomic<unsigned> attr{0};  // one bit per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(attr.load() & (1u << dev))) {
+      if (cudaFuncSetAttribute(k_assemble_scaled_slice, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_slice_smem(ASM_SLICE_WMAX))) ==
+          cudaSuccess)
+        attr.fetch_or(1u << dev);
+    }
+    if (dev < 32 && (attr.load() & (1u << dev))) {
+      k_assemble_scaled_slice<<<(m.V + 31) / 32, ASM_SLICE_TPB, asm_slice_smem(wmax), s>>>(
+          m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh, sell_base, chunk_off, wmax, valh_sell, ctrl);
+      return;
+    }
+  }
+  k_assemble_scaled<<<nblk(m.nnzb, tpb), tpb, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh, sell_base,
+                                                      valh_sell, ctrl);
 }
 void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s) {
   if (n) k_extra_key64<<<nblk(n), TPB, 0, s>>>(xent, xkeys, n, key, idx);
