@@ -228,7 +228,6 @@ struct State {
   ando_ctx ctx = nullptr;
   uint64_t topo = 0, verts = 0, weights = 0;
   bool dev_x = false, dev_v = false, start_stale = false, host_dirty = true, masses_dirty = true;
-  std::vector<double> stage;      // download staging (reused)
   ando_step_stats last{};
 
   State() = default;
@@ -248,29 +247,24 @@ struct State {
   }
 
   void mark_device_newer() { dev_x = dev_v = start_stale = true; }
-  void unpack(std::vector<V3>& dst) {
-    dst.resize(nv());
-    std::memcpy(static_cast<void*>(dst.data()), stage.data(), sizeof(double) * 3 * nv());  // V3 is three packed doubles
-  }
+  // V3 is three packed doubles, so the host arrays are downloaded into directly.
+  static double* raw(std::vector<V3>& a) { return reinterpret_cast<double*>(a.data()); }
   void sync_x() {
     if (!dev_x || !ctx) return;
-    stage.resize(3 * nv());
-    check(ando_state_download(ctx, stage.data(), nullptr, int32_t(nv())), "state download");
-    unpack(x);
+    x.resize(nv());
+    check(ando_state_download(ctx, raw(x), nullptr, int32_t(nv())), "state download");
     dev_x = false;
   }
   void sync_v() {
     if (!dev_v || !ctx) return;
-    stage.resize(3 * nv());
-    check(ando_state_download(ctx, nullptr, stage.data(), int32_t(nv())), "state download");
-    unpack(v);
+    v.resize(nv());
+    check(ando_state_download(ctx, nullptr, raw(v), int32_t(nv())), "state download");
     dev_v = false;
   }
   void sync_start() {
     if (!start_stale || !ctx) return;
-    stage.resize(3 * nv());
-    check(ando_state_get_start(ctx, stage.data(), int32_t(nv())), "state start");
-    unpack(start);
+    start.resize(nv());
+    check(ando_state_get_start(ctx, raw(start), int32_t(nv())), "state start");
     start_stale = false;
   }
   void sync_host() { sync_x(); sync_v(); sync_start(); }

@@ -163,17 +163,17 @@ def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
     half = n * n
     dt = 1.0 / 60.0
 
+    top_idx = np.asarray(top)
+    base_rows = v[top_idx].copy()
+    sgn_rows = np.where(top_idx < half, 1.0, -1.0)
+
     def schedule(frame: int):
         t = (frame + 1) * dt
         r = min(1.0, t / 0.5)
         ramp = r * r * (3.0 - 2.0 * r)
-        out = []
-        for i in top:
-            sgn = 1.0 if i < half else -1.0
-            tgt = base[i].copy()
-            tgt[0] += sgn * 0.3 * ramp * math.sin(2 * math.pi * 0.5 * t)
-            out.append((i, tgt))
-        return out
+        tgt = base_rows.copy()
+        tgt[:, 0] += sgn_rows * 0.3 * ramp * math.sin(2 * math.pi * 0.5 * t)
+        return list(zip(top, tgt))
 
     mat = dict(youngs_modulus=2e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
     return Scene(f"c4_2x{n}x{n}", v, np.concatenate(tris), mat, cloth_params(),
