@@ -677,7 +677,10 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
     const float* L = wq + LAYER0 + l * L_SIZE;
     // u = U h and h' = relu(W [h ; m] + b) + h on the tensor cores
     const unsigned short* bi = n.bimg ? n.bimg + l * BIMG_LSIZE : nullptr;
-    launch_gemm_tc(V, w.h[l], H, H, nullptr, 0, 0, L + L_U, bi ? bi + BIMG_U : nullptr, nullptr, nullptr, 0, nullptr, w.u[l], 0, err, st);
+    // u = U h: its own launch for the first layer, fused into the previous
+    // layer's update launch (same bits) for the others when the images exist
+    if (l == 0 || !bi)
+      launch_gemm_tc(V, w.h[l], H, H, nullptr, 0, 0, L + L_U, bi ? bi + BIMG_U : nullptr, nullptr, nullptr, 0, nullptr, w.u[l], 0, err, st);
     if (n.host_wq && !w.training) {
       MsgWeights P;
       const float* Lh = n.host_wq + LAYER0 + l * L_SIZE;
@@ -687,8 +690,9 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
     } else {
       k_msg_fwd<<<wgrid, TPB, 0, st>>>(s, w.u[l], w.Ef, L + L_E, L + L_C, w.m[l]);
     }
+    const unsigned short* bnext = bi && l + 1 < NL ? n.bimg + (l + 1) * BIMG_LSIZE + BIMG_U : nullptr;
     launch_gemm_tc(V, w.h[l], H, H, w.m[l], H, H, L + L_W, bi ? bi + BIMG_W : nullptr, L + L_B, w.h[l], H, w.training ? w.q[l] : nullptr,
-                   w.h[l + 1], 1, err, st);
+                   w.h[l + 1], 1, err, st, bnext, bnext ? w.u[l + 1] : nullptr);
   }
   k_dec_fwd<<<wgrid, TPB, 0, st>>>(s, w.h[NL], w.Ef, wq, w.zv, w.ab);
   k_build_S<<<nblk(V), TPB, 0, st>>>(s, w.zv, w.ab, S, pcg);

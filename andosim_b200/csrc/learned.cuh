@@ -102,9 +102,11 @@ void learned_forward(const LsView& s, const NetDev& n, LearnedWork& w, float* S,
 // Bimg (may be null): W's B operand image from launch_gemm_tc_image (64 K
 // BF16 values, 16-byte aligned), copied instead of converting W per CTA.
 bool gemm_tc_supported(int K1, int K2, int N, int ldr1);
+// Bimg2 (may be null): the B image of a 64 x 64 matrix U; the launch then
+// also writes Y2 = Y U^T (the next layer's U product, fused).
 cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W,
                            const unsigned short* Bimg, const float* bias, const float* R1, int ldr1, float* Q, float* Y, int relu, int* err,
-                           cudaStream_t s);
+                           cudaStream_t s, const unsigned short* Bimg2 = nullptr, float* Y2 = nullptr);
 cudaError_t launch_gemm_tc_image(const float* W, int K, unsigned short* img, cudaStream_t s);
 
 // S from the coefficients of the last forward (w.zv, w.ab) and the current

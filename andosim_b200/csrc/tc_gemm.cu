@@ -72,13 +72,30 @@ __device__ inline bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for phase 0 of the barrier (about a second at most).
-__device__ inline bool mbar_wait_bounded(uint32_t bar) {
+// Bounded wait for the barrier's phase of the given parity (about a second
+// at most).
+__device__ inline bool mbar_wait_bounded(uint32_t bar, uint32_t parity = 0) {
   for (long long it = 0; it < (1ll << 22); ++it) {
-    if (mbar_try_wait(bar, 0)) return true;
+    if (mbar_try_wait(bar, parity)) return true;
     if (it > 32) __nanosleep(128);
   }
   return false;
+}
+
+__device__ inline uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
+  return uint32_t(__bfloat16_as_ushort(a)) | (uint32_t(__bfloat16_as_ushort(b)) << 16);
+}
+
+// Split four FP32 values exactly into three BF16 4-vectors (hi, mid, lo).
+__device__ inline void split3(const float f[4], uint32_t w[3][2]) {
+#pragma unroll
+  for (int e = 0; e < 4; e += 2) {
+    __nv_bfloat16 h0 = __float2bfloat16_rn(f[e]), h1 = __float2bfloat16_rn(f[e + 1]);
+    float s0 = f[e] - __bfloat162float(h0), s1 = f[e + 1] - __bfloat162float(h1);
+    __nv_bfloat16 m0 = __float2bfloat16_rn(s0), m1 = __float2bfloat16_rn(s1);
+    __nv_bfloat16 l0 = __float2bfloat16_rn(s0 - __bfloat162float(m0)), l1 = __float2bfloat16_rn(s1 - __bfloat162float(m1));
+    w[0][e / 2] = pack2(h0, h1); w[1][e / 2] = pack2(m0, m1); w[2][e / 2] = pack2(l0, l1);
+  }
 }
 
 __device__ inline void tmem_ld16(uint32_t taddr, float* v) {
@@ -92,9 +109,6 @@ __device__ inline void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ inline uint32_t pack2(__nv_bfloat16 a, __nv_bfloat16 b) {
-  return uint32_t(__bfloat16_as_ushort(a)) | (uint32_t(__bfloat16_as_ushort(b)) << 16);
-}
 
 // B image: W (64 x K, row-major, BF16-representable) as BF16 in the shared
 // memory layout of the MMA's B operand, 128 K bytes.
@@ -116,7 +130,8 @@ constexpr int TC_AV = TC_M * 128 / 4 / TC_THREADS;  // float4 loads per thread o
 __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __restrict__ X1, int ld1, int K1, const float* __restrict__ X2,
                                                         int ld2, int K2, const float* __restrict__ W, const uint4* __restrict__ Bimg,
                                                         const float* __restrict__ bias, const float* __restrict__ R1, int ldr1, int res_a,
-                                                        float* __restrict__ Q, float* __restrict__ Y, int relu, int* err) {
+                                                        float* __restrict__ Q, float* __restrict__ Y, int relu, int* err,
+                                                        const uint4* __restrict__ Bimg2, float* __restrict__ Y2) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int K = K1 + K2;
   const int tile = TC_M * K * 2;  // bytes of one BF16 split of the row tile
@@ -181,14 +196,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
       const int r = c / K4, k = (c - r * K4) << 2;
       const float f[4] = {av[j].x, av[j].y, av[j].z, av[j].w};
       uint32_t w[TC_SPLITS][2];
-#pragma unroll
-      for (int e = 0; e < 4; e += 2) {
-        __nv_bfloat16 h0 = __float2bfloat16_rn(f[e]), h1 = __float2bfloat16_rn(f[e + 1]);
-        float s0 = f[e] - __bfloat162float(h0), s1 = f[e + 1] - __bfloat162float(h1);
-        __nv_bfloat16 m0 = __float2bfloat16_rn(s0), m1 = __float2bfloat16_rn(s1);
-        __nv_bfloat16 l0 = __float2bfloat16_rn(s0 - __bfloat162float(m0)), l1 = __float2bfloat16_rn(s1 - __bfloat162float(m1));
-        w[0][e / 2] = pack2(h0, h1); w[1][e / 2] = pack2(m0, m1); w[2][e / 2] = pack2(l0, l1);
-      }
+      split3(f, w);
       const int off = core_off(r, k, K);  // k % 4 == 0: 8-byte aligned inside a 16-byte core-matrix row
 #pragma unroll
       for (int sp = 0; sp < TC_SPLITS; ++sp) *reinterpret_cast<uint2*>(A + sp * tile + off) = make_uint2(w[sp][0], w[sp][1]);
@@ -213,6 +221,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
   }
   const bool done = mbar_wait_bounded(bar_a);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  float hv[TC_COLS_PER_WARP];  // this thread's outputs, the input of the fused second product
+#pragma unroll
+  for (int c = 0; c < TC_COLS_PER_WARP; ++c) hv[c] = 0.f;
   if (done) {
     // warp w: tensor-memory lanes (rows) 32 (w % 4) + lane, columns c0 .. c0 + 31
     const int quarter = warp & 3, c0 = (warp >> 2) * TC_COLS_PER_WARP;
@@ -262,11 +273,69 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(int V, const float* __re
           for (int e = 0; e < 4; ++e) y[e] += res[4 * c4 + e];
         }
         yr[c4] = make_float4(y[0], y[1], y[2], y[3]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) hv[4 * c4 + e] = y[e];
       }
     }
   } else if (tid == 0) {
     atomicExch(err ? err : &g_tc_err, 1);
     mbar_wait_bounded(bar_a);  // give the MMAs in flight a second bound before the accumulator is freed
+  }
+  // Fused second product Y2 = Y U^T (U: 64 x 64, its B image Bimg2): Y's tile
+  // goes back into shared memory as three BF16 terms (K = 64 layout) and one
+  // more set of MMAs reuses the accumulator columns, whose loads have all
+  // completed. The result is the bits a separate launch on Y gives.
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  if (Bimg2 && __syncthreads_and(done)) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    constexpr int K2 = TC_N, tile2 = TC_M * K2 * 2;
+    for (int i = tid; i < TC_N * K2 * 2 / 16; i += TC_THREADS) reinterpret_cast<uint4*>(B)[i] = Bimg2[i];
+    {
+      const int quarter = warp & 3, c0 = (warp >> 2) * TC_COLS_PER_WARP, r = quarter * 32 + (tid & 31);
+#pragma unroll
+      for (int c4 = 0; c4 < TC_COLS_PER_WARP / 4; ++c4) {
+        const float f[4] = {hv[4 * c4], hv[4 * c4 + 1], hv[4 * c4 + 2], hv[4 * c4 + 3]};
+        uint32_t w[TC_SPLITS][2];
+        split3(f, w);
+        const int off = core_off(r, c0 + 4 * c4, K2);
+#pragma unroll
+        for (int sp = 0; sp < TC_SPLITS; ++sp) *reinterpret_cast<uint2*>(A + sp * tile2 + off) = make_uint2(w[sp][0], w[sp][1]);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (tid == 0) {
+      int first = 1;
+      for (int sp = 0; sp < TC_SPLITS; ++sp)
+        for (int kk = 0; kk < K2 / 16; ++kk) {
+          const uint64_t ad = smem_desc(smem_u32(A + sp * tile2 + kk * 256), K2);
+          const uint64_t bd = smem_desc(smem_u32(B + kk * 256), K2);
+          mma_f16(tmem, ad, bd, TC_IDESC, first ? 0 : 1);
+          first = 0;
+        }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_a) : "memory");
+    }
+    const bool done2 = mbar_wait_bounded(bar_a, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (done2) {
+      const int quarter = warp & 3, c0 = (warp >> 2) * TC_COLS_PER_WARP;
+      float acc[TC_COLS_PER_WARP];
+      const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(c0);
+#pragma unroll
+      for (int c = 0; c < TC_COLS_PER_WARP; c += 16) tmem_ld16(taddr + c, acc + c);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      const int row = r0 + quarter * 32 + (tid & 31);
+      if (row < V) {
+        float4* ur = reinterpret_cast<float4*>(Y2 + (long long)row * TC_N + c0);
+#pragma unroll
+        for (int c4 = 0; c4 < TC_COLS_PER_WARP / 4; ++c4) ur[c4] = make_float4(acc[4 * c4], acc[4 * c4 + 1], acc[4 * c4 + 2], acc[4 * c4 + 3]);
+      }
+    } else if (tid == 0) {
+      atomicExch(err ? err : &g_tc_err, 1);
+      mbar_wait_bounded(bar_a, 1);
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
@@ -294,13 +363,14 @@ cudaError_t launch_gemm_tc_image(const float* W, int K, unsigned short* img, cud
 
 cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float* X2, int ld2, int K2, const float* W,
                            const unsigned short* Bimg, const float* bias, const float* R1, int ldr1, float* Q, float* Y, int relu, int* err,
-                           cudaStream_t s) {
+                           cudaStream_t s, const unsigned short* Bimg2, float* Y2) {
   if (V <= 0) return cudaSuccess;
   if (!gemm_tc_supported(K1, K2, TC_N, R1 ? ldr1 : 0)) return cudaErrorInvalidValue;
   auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
   if (!a16(Y) || (Q && !a16(Q)) || (R1 && !a16(R1))) return cudaErrorInvalidValue;  // float4 epilogue
   if (!a16(X1) || (ld1 & 3) || (K2 && (!a16(X2) || (ld2 & 3)))) return cudaErrorInvalidValue;  // float4 staging
   if (Bimg && !a16(Bimg)) return cudaErrorInvalidValue;
+  if (Bimg2 && (!a16(Bimg2) || !Y2 || !a16(Y2))) return cudaErrorInvalidValue;
   const int res_a = R1 && R1 == X1 && ldr1 == ld1 && K1 >= TC_N;
   static std::atomic<unsigned> attr{0};  // one bit per device (steps of several contexts may run on host threads)
   int dev = 0;
@@ -312,7 +382,8 @@ cudaError_t launch_gemm_tc(int V, const float* X1, int ld1, int K1, const float*
   }
   const int K = K1 + K2;
   k_gemm_tc<<<(V + TC_M - 1) / TC_M, TC_THREADS, gemm_tc_smem(K), s>>>(V, X1, ld1, K1, X2, ld2, K2, W, reinterpret_cast<const uint4*>(Bimg),
-                                                                      bias, R1, ldr1, res_a, Q, Y, relu, err);
+                                                                      bias, R1, ldr1, res_a, Q, Y, relu, err,
+                                                                      reinterpret_cast<const uint4*>(Bimg2), Y2);
   return cudaGetLastError();
 }
 
