@@ -189,19 +189,21 @@ __device__ inline Box unite(const Box& a, const Box& b) {
 // k_refit_cut: one CTA per cut subtree (grid-stride over the cut list). With
 // Karras numbering a node covering leaves [lo, hi] has its index in [lo, hi],
 // so every node of a subtree over [c0, c1] has a shared-memory slot (index -
-// c0): the subtree's topology is staged once and each node is finished in
-// shared memory by the second of its children to arrive (block-scope arrival
-// counters). The leaf boxes are computed from the positions here.
+// c0): the subtree's topology is staged once, each node is finished in shared
+// memory by the second of its children to arrive (block-scope arrival
+// counters), and the subtree's node boxes and child records are written in
+// one pass afterwards; thread 0 puts the subtree's root box into its parent's
+// record. The leaf boxes are computed from the positions here.
 //
 // k_refit_top: one CTA finishes the top nodes the same way in shared memory,
-// reading the cut subtrees' boxes from nodes[].
+// reading the cut subtrees' boxes from nodes[], and writes them in one pass.
 //
 // When the top has more nodes than one CTA holds (or than the caller's
-// capacity, Lbvh::top_cap), k_refit_cut carries on
-// through the top nodes itself with global arrival counters (acquire/release
-// atomics; the second arrival zeroes the counter for the next refit) and
-// k_refit_top does nothing. Min/max are exact, so every box has the same bits
-// in any arrival order.
+// capacity, Lbvh::top_cap), thread 0 of each cut subtree carries on through
+// the top nodes with global arrival counters (acquire/release atomics; the
+// second arrival zeroes the counter for the next refit) and k_refit_top does
+// nothing. Min/max are exact, so every box has the same bits in any arrival
+// order.
 constexpr int RF_TPB = 512, RF_CUT = 1024;
 struct RefitSmem { Box leaf[RF_CUT]; Box node[RF_CUT]; int4 topo[RF_CUT]; int arr[RF_CUT]; };
 constexpr int TOP_TPB = 1024, TOP_MAX = 4096;
