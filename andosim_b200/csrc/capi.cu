@@ -90,6 +90,7 @@ struct ando_ctx_s {
   // autotuned on the first solve of a mesh (choice < 0) or a fixed candidate
   PcgShape shape[2];
   int shape_V[2] = {-1, -1}, shape_choice[2] = {-1, -1};
+  PcgShape shape_untuned;          // block-Jacobi fallback launch before its shape has been tuned
   int asm_tpb = 256, asm_V = -1, asm_choice = -1;  // scaled assembly block size (tuned like the PCG shape)
   double dt2inv = 0.0;             // of the last assembled system
   double gap_max = 1e-3;           // contact activation distance of the current step
@@ -799,9 +800,25 @@ const PcgShape& pcg_shape(ando_ctx c, bool learned, const PcgScaledArgs& sa) {
   return c->shape[k];
 }
 
-// The scaled PCG of one Newton iteration: learned S when asked for (with
-// block-Jacobi redoing the solve when S loses definiteness, stalls or hits
-// the iteration cap), block-Jacobi otherwise.
+// Shape of a launch that must not run the autotuner (its timing solves would
+// overwrite the solution of the solve before it): the tuned shape when there
+// is one, else the caller's choice or the first candidate.
+const PcgShape& pcg_shape_no_tuning(ando_ctx c, bool learned) {
+  const int k = learned ? 1 : 0;
+  if (c->shape_V[k] == c->V) return c->shape[k];
+  PcgShape cand[16];
+  const int n = pcg_scaled_shapes(c->device, c->V, learned, cand, 16);
+  const int pick = c->shape_choice[k] >= 0 && c->shape_choice[k] < n ? c->shape_choice[k] : 0;
+  c->shape_untuned = n > 0 ? cand[pick] : PcgShape{32, 1, 1};
+  return c->shape_untuned;
+}
+
+// The scaled PCG of one Newton iteration: learned S when asked for, with a
+// block-Jacobi launch behind it that redoes the solve on the device when S
+// lost definiteness, stalled or hit the iteration cap (and returns at once
+// otherwise), so no host round trip sits between the solve and the line
+// search; block-Jacobi alone otherwise. The learned attempt's iterations and
+// whether the fallback ran are read with the line search's control block.
 int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
   cudaStream_t s = c->stream;
   PcgScaledArgs sa = scaled_args(c, p);
@@ -828,21 +845,29 @@ int scaled_solve(ando_ctx c, const ando_params& p, ando_step_stats& st) {
     sa.coef = c->S_coef.p; sa.Sdiag = c->S_diag.p;
     CK(launch_pcg_scaled(sa, true, pcg_shape(c, true, sa), s));
     ph.launched();
-    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    const Ctrl& h = *c->ctrl_host;
-    if (h.tc_err) return fail(ANDO_ERR_TIMEOUT, "learned preconditioner: a tensor-core layer's wait timed out");
-    c->profile.pcg_learned_iterations += h.pcg_iters;
-    if (h.converged || h.pcg_status == PCG_OK || h.pcg_status == PCG_TIMEOUT) return ANDO_OK;
-    // the learned attempt's iterations count as work done; the caller adds the final solve's
-    c->profile.pcg_iterations += h.pcg_iters;
-    c->profile.pcg_extra_block_iterations += (long long)h.pcg_iters * c->nx;
-    st.pcg_iters += h.pcg_iters;
-    st.precond_fallbacks++;
-    sa.coef = nullptr; sa.Sdiag = nullptr;
+    sa.coef = nullptr; sa.Sdiag = nullptr; sa.fallback = 1;
+    CK(launch_pcg_scaled(sa, false, pcg_shape_no_tuning(c, false), s));
+    ph.launched();
+    return ANDO_OK;
   }
   CK(launch_pcg_scaled(sa, false, pcg_shape(c, false, sa), s));
   ph.launched();
+  return ANDO_OK;
+}
+
+// Statistics of the learned attempt (scaled_solve), from the control block
+// read after the line search; the caller adds the final solve's iterations.
+int learned_solve_stats(ando_ctx c, const ando_params& p, const Ctrl& h, ando_step_stats& st) {
+  if (p.precond != ANDO_PRECOND_LEARNED) return ANDO_OK;
+  if (h.tc_err) return fail(ANDO_ERR_TIMEOUT, "learned preconditioner: a tensor-core layer's wait timed out");
+  c->profile.pcg_learned_iterations += h.learned_iters;
+  if (h.fallback_ran) {
+    // the learned attempt's iterations count as work done
+    c->profile.pcg_iterations += h.learned_iters;
+    c->profile.pcg_extra_block_iterations += (long long)h.learned_iters * c->nx;
+    st.pcg_iters += h.learned_iters;
+    st.precond_fallbacks++;
+  }
   return ANDO_OK;
 }
 
@@ -884,6 +909,8 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
     }
     const Ctrl& h = *c->ctrl_host;
     if (h.pcg_status == PCG_TIMEOUT || h.bar_err) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
+    rc = learned_solve_stats(c, p, h, st);
+    if (rc) return rc;
     st.newton_iters++;
     st.pcg_iters += h.pcg_iters;
     c->profile.pcg_iterations += h.pcg_iters;

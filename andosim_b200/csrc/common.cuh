@@ -114,6 +114,8 @@ struct Ctrl {
   unsigned int bar_count, bar_gen; int bar_err;
   int tc_err;                     // a tensor-core GEMM's bounded wait gave up (sticky)
   int toi_overflow;               // > 0: a time-of-impact candidate list needed this many slots; the move was not applied
+  int learned_iters;              // iterations of this Newton iteration's learned solve
+  int fallback_ran;               // block-Jacobi redid this Newton iteration's learned solve
   int pad_;
   unsigned long long bar_arrivals;  // grid_sync_ar: arrivals since the launcher zeroed it
 };

@@ -407,6 +407,7 @@ __global__ void k_ctrl_reset(Ctrl* c) {
   c->gnorm_bits = 0ull; c->ls_mask = (1u << 20) - 1u; c->converged = 0;
   c->pcg_iters = 0; c->pcg_converged = 0; c->pcg_status = PCG_SKIPPED; c->pcg_rel = 0.0;
   c->alpha = 0.0; c->strain_active = 0; c->bar_count = 0; c->bar_err = 0;
+  c->learned_iters = 0; c->fallback_ran = 0;
 }
 
 // Thin SVD of the 3x2 deformation gradient through the eigenpairs of F^T F

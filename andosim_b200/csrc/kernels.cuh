@@ -138,6 +138,9 @@ struct PcgScaledArgs {
   float tol; int max_iters; int stall_window;
   // block-Jacobi solves only: snapshot k of (r^, x^) after 2^k - 1 iterations, k < snap_max
   float* snap_r; double* snap_x; int snap_max;
+  // block-Jacobi only: 1 = the fallback of the learned solve just before it
+  // on the stream; returns at once when that solve ended PCG_OK (or timed out)
+  int fallback = 0;
 };
 // Launch shape of the scaled PCG (threads per CTA, CTAs, column slots loaded
 // ahead per thread). A tuning knob only: every shape gives the same bits.

@@ -395,6 +395,13 @@ template <bool LEARNED, int U>
 __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) {
   Ctrl* ctrl = a.ctrl;
   if (ctrl->converged) return;
+  if (!LEARNED && a.fallback) {
+    // every CTA reads the learned solve's status before the first grid
+    // barrier; it is rewritten only after one
+    const int st = ctrl->pcg_status;
+    if (st == PCG_OK || st == PCG_TIMEOUT) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->fallback_ran = 1;
+  }
   __shared__ RedSmem sh;
   const int V = a.V, ns = (V + 31) >> 5;
   const unsigned nb = gridDim.x;
@@ -552,6 +559,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (LEARNED) ctrl->learned_iters = iters;
     ctrl->pcg_iters = iters;
     ctrl->pcg_status = status;
     ctrl->pcg_converged = status == PCG_OK ? 1 : 0;
