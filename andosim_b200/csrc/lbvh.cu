@@ -642,11 +642,17 @@ cudaError_t Lbvh::launch_refit(const double* x, const double* x1, float pad, cud
   cudaError_t e = cudaFuncSetAttribute(k_refit_cut, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(RefitSmem)));
   if (!e) e = cudaFuncSetAttribute(k_refit_top, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(TopSmem)));
   if (e) return e;
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
-  }
+  // SMs of the device (contexts of a batch step on host threads: the
+  // function-local static is initialised once, thread-safely; 148 if the
+  // query fails)
+  static const int sms = [] {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+      cudaGetLastError();
+      return 148;
+    }
+    return n;
+  }();
   // grid-stride over the cut list (its length stays on the device): about
   // three subtrees per SM resident at once
   const int grid = std::max(1, std::min(3 * sms, 2 * ((n + 255) / 256)));
