@@ -21,6 +21,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <unordered_set>
 #include <cstring>
 #include <vector>
@@ -391,6 +392,33 @@ std::vector<double> elastic_gradient(const Mesh& me) {
   return g;
 }
 
+// Elasticity::compute_hessian (elasticity.cpp:63-91, face_hessian at :135-181):
+// per face the 3 x 3 blocks c_ab diag(1, 1, 0) of K = k Dm^-T Dm^-1, each made
+// SPD by clamping its eigenvalues at 1e-8 (stiffness.cpp:236-254; the blocks
+// are diagonal, so the clamp gives diag(max(c, 1e-8), max(c, 1e-8), 1e-8)).
+// 81 (row, col, value) triplets per face, in the reference's order.
+std::vector<std::tuple<int, int, float>> elastic_hessian_triplets(const Mesh& me) {
+  double mu = double(me.material.youngs_modulus) / (2.0 * (1.0 + double(me.material.poisson_ratio)));
+  std::vector<std::tuple<int, int, float>> out;
+  out.reserve(81 * me.nt());
+  for (size_t f = 0; f < me.nt(); ++f) {
+    const double* D = &me.dm_inv[4 * f];
+    double k = me.areas[f] * me.material.thickness * mu;
+    // K = k Dm^-T Dm^-1 (2 x 2, symmetric)
+    double K00 = k * (D[0] * D[0] + D[2] * D[2]), K01 = k * (D[0] * D[1] + D[2] * D[3]), K11 = k * (D[1] * D[1] + D[3] * D[3]);
+    const double c[3][3] = {{K00 + K11 + 2.0 * K01, -K00, -K11}, {-K00, K00, -K01}, {-K11, -K01, K11}};
+    const int ids[3] = {me.tris[3 * f], me.tris[3 * f + 1], me.tris[3 * f + 2]};
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double d = std::max(c[a][b], 1e-8);
+        const double blk[3] = {d, d, 1e-8};
+        for (int r = 0; r < 3; ++r)
+          for (int q = 0; q < 3; ++q) out.emplace_back(3 * ids[a] + r, 3 * ids[b] + q, float(r == q ? blk[r] : 0.0));
+      }
+  }
+  return out;
+}
+
 // ------------------------------------------------------------ conversions
 std::vector<V3> to_v3(py::object o, const char* what) {
   auto a = Arr<double>::ensure(o);
@@ -716,7 +744,14 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         auto g = elastic_gradient(me);
         auto o = out.mutable_unchecked<1>();
         for (py::ssize_t i = 0; i < o.shape(0); ++i) o(i) = size_t(i) < g.size() ? float(g[size_t(i)]) : 0.0f;
-      }, "Compute elastic gradient (forces)");
+      }, "Compute elastic gradient (forces)")
+      // The reference binds its C++ signature (mesh, state, std::vector<Triplet>&); here the
+      // (row, col, value) triplets are appended to the list given (a new one if omitted) and returned.
+      .def_static("compute_hessian", [](const Mesh& me, const State&, py::object triplets) {
+        py::list out = triplets.is_none() ? py::list() : triplets.cast<py::list>();
+        for (const auto& t : elastic_hessian_triplets(me)) out.append(py::make_tuple(std::get<0>(t), std::get<1>(t), std::get<2>(t)));
+        return out;
+      }, py::arg("mesh"), py::arg("state"), py::arg("triplets") = py::none(), "Compute elastic Hessian (explicit assembly)");
 
   // barrier.cpp:29-65
   m.def("barrier_energy", [](Real g, Real gm, Real k) -> Real {

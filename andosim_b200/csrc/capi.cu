@@ -150,8 +150,6 @@ struct ando_ctx_s {
   long long mesh_generation = 0;
 
   // CORRECTED semantics
-  DevBuf<double> pin_start, pin_final;   // sub-steps of a fast kinematic drive
-  DevBuf<unsigned long long> pin_maxmove;
   DevBuf<double> x_safe;           // where the last step ended (or the uploaded positions): start of the next CORRECTED step
   bool safe_valid = false;
   DevBuf<unsigned char> fixed;
@@ -657,7 +655,7 @@ int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, i
   {
     Phase ph(c, ANDO_PHASE_GRADIENT);
     launch_ctrl_reset(c->ctrl.p, s);
-    launch_elastic_gradient(m, c->x.p, c->mu, c->thickness, c->g_el_x.p, s);
+    launch_arap_gradient(m, c->x.p, c->mu, c->thickness, c->g_el_x.p, s);
     ph.launched(2);
   }
   if (sp.enable_strain) {
@@ -936,55 +934,9 @@ int restore_start(ando_ctx c) {
   return ANDO_OK;
 }
 
-// Kinematic pins that move more than half a mean edge length in one step
-// drag the first free rows across their own triangles (the cloth folds onto
-// the pinned row and every later line search stops at zero). Such a step is
-// split into k = ceil(move / (edge / 2)) sub-steps (at most 8).
-int pin_substeps(ando_ctx c, int& k) {
-  k = 1;
-  if (!c->num_pins) return ANDO_OK;
-  CK(c->pin_maxmove.reserve(1));
-  launch_pin_maxdisp(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->pin_maxmove.p, c->stream);
-  unsigned long long bits = 0;
-  CK(cudaMemcpyAsync(&bits, c->pin_maxmove.p, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  double mv = 0.0;
-  std::memcpy(&mv, &bits, sizeof(mv));
-  double edge = c->max_move / 4.0;
-  if (edge > 0.0 && mv > 0.5 * edge) k = int(std::min(8.0, std::ceil(mv / (0.5 * edge))));
-  return ANDO_OK;
-}
-
 int remember_safe(ando_ctx c) {
   CK(cudaMemcpyAsync(c->x_safe.p, c->x.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, c->stream));
   c->safe_valid = true;
-  return ANDO_OK;
-}
-
-// Kinematic pins of the CORRECTED step: pinned vertices move toward their
-// targets as far as the move's conservative time of impact allows (walls,
-// self contact, rigid triangles; a teleported pin would drag the cloth into
-// itself), then stay fixed for the step.
-int apply_pins_once(ando_ctx c, int nb) {
-  cudaStream_t s = c->stream;
-  CK(cudaMemsetAsync(c->fixed.p, 0, c->V, s));
-  if (!c->num_pins) return ANDO_OK;
-  Phase ph(c, ANDO_PHASE_SETUP);
-  CK(cudaMemsetAsync(&c->ctrl.p->toi_overflow, 0, sizeof(int), s));
-  CK(cudaMemsetAsync(c->ext.p, 0, sizeof(double) * 3ull * c->V, s));
-  CK(cudaMemcpyAsync(c->x1.p, c->x.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, s));
-  launch_pin_ext(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->ext.p, c->x1.p, c->fixed.p, s);
-  launch_toi_reset(c->toi.p, s);
-  launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
-  ph.launched(2 + (c->num_walls ? 1 : 0));
-  long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-  int rc = swept_toi(c, 0.5 * c->gap_max, 1e-3 * c->gap_max);
-  if (rc) return rc;
-  ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
-  if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
-  launch_pin_move(c->pin_vertex.p, c->num_pins, c->ext.p, c->toi.p, c->ctrl.p, c->x.p, s);
-  ph.launched();
-  CK(cudaGetLastError());
   return ANDO_OK;
 }
 
@@ -997,27 +949,6 @@ int grow_toi_candidates(ando_ctx c, int need) {
   CK(c->toi_scratch.reserve(n));
   CK(c->toi_scratch_ee.reserve(n));
   return ANDO_OK;
-}
-
-int toi_overflow_need(ando_ctx c, int& need) {
-  need = 0;
-  CK(cudaMemcpyAsync(&need, &c->ctrl.p->toi_overflow, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  return ANDO_OK;
-}
-
-int apply_pins(ando_ctx c, int nb) {
-  for (int attempt = 0; attempt < 4; ++attempt) {
-    int rc = apply_pins_once(c, nb);
-    if (rc) return rc;
-    if (!c->num_pins) return ANDO_OK;
-    int need = 0;
-    rc = toi_overflow_need(c, need);
-    if (rc || !need) return rc;
-    rc = grow_toi_candidates(c, need);
-    if (rc) return rc;
-  }
-  return fail(ANDO_ERR_CAPACITY, "time-of-impact candidates kept overflowing");
 }
 
 // One Newton iteration of the REFERENCE step as a fixed launch sequence
@@ -1642,38 +1573,12 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     }
   }
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
-    int k = 1;
-    rc = pin_substeps(c, k);
+    // pins are springs of the implicit solve: no kinematic pre-move, no sub-steps
+    st.substeps = 1;
+    rc = step_body(c, p, sp, num_rigids, num_walls, st);
     if (rc) return rc;
-    st.substeps = k;
-    if (k == 1) {
-      rc = apply_pins(c, num_rigids);
-      if (rc) return rc;
-      rc = step_body(c, p, sp, num_rigids, num_walls, st);
-      if (rc) return rc;
-      rc = remember_safe(c);
-      if (rc) return rc;
-    } else {
-      // k sub-steps of dt / k with the pin targets interpolated linearly
-      CK(c->pin_start.reserve(3ull * c->num_pins)); CK(c->pin_final.reserve(3ull * c->num_pins));
-      CK(cudaMemcpyAsync(c->pin_final.p, c->pin_target.p, sizeof(double) * 3ull * c->num_pins, cudaMemcpyDeviceToDevice, s));
-      launch_pin_gather(c->pin_vertex.p, c->num_pins, c->x.p, c->pin_start.p, s);
-      ando_params ps = p;
-      ps.dt = p.dt / k;
-      StepParams sps = sp;
-      sps.dt = ps.dt; sps.dt2inv = 1.0 / (ps.dt * ps.dt);
-      for (int j = 1; j <= k; ++j) {
-        launch_pin_interp(c->num_pins, c->pin_start.p, c->pin_final.p, double(j) / k, c->pin_target.p, s);
-        launch_predict(c->V, c->x.p, c->v.p, ps.dt, c->x_old.p, c->x_hat.p, s);   // x_hat = x + (dt / k) v
-        rc = apply_pins(c, num_rigids);
-        if (rc) return rc;
-        rc = step_body(c, ps, sps, num_rigids, num_walls, st);
-        if (rc) return rc;
-        rc = remember_safe(c);
-        if (rc) return rc;
-      }
-      CK(cudaMemcpyAsync(c->pin_target.p, c->pin_final.p, sizeof(double) * 3ull * c->num_pins, cudaMemcpyDeviceToDevice, s));
-    }
+    rc = remember_safe(c);
+    if (rc) return rc;
   } else {
     rc = detect(c, num_rigids);
     if (rc) return rc;
@@ -1725,8 +1630,6 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
   MeshDev m = c->mesh_dev();
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
-    rc = apply_pins(c, num_rigids);
-    if (rc) return rc;
     rc = corrected_gradient(c, p, sp, num_rigids);
     if (rc) return rc;
     enqueue_scaled_assembly(c, sp, s);

@@ -50,6 +50,11 @@ __host__ __device__ inline double bar_hess(double g, double gm, double k) {
 __host__ __device__ inline bool in_domain(double g, double gm) { return gm > 0.0 && g <= gm; }
 __host__ __device__ inline d3 normalize_or_default(d3 n, double eps) { return sqn(n) > eps * eps ? normalized(n) : mk(0.0, 1.0, 0.0); }
 
+// CORRECTED pin stiffness: kappa = PIN_SCALE (m / dt^2 + a) with a the
+// vertex's elastic diagonal coefficient; a pinned vertex then follows its
+// target within about 1 % of the elastic load on it.
+constexpr double PIN_SCALE = 100.0;
+
 // -------------------------------------------------------------- parameters
 struct WallDev { double n[3]; double offset, gap; int active; };
 

@@ -3,11 +3,12 @@
 // The CORRECTED step keeps the reference's algorithm (beta accumulation,
 // Newton with a block-Jacobi PCG inner solve, cubic barriers with
 // elasticity-inclusive dynamic stiffness) and fixes what the reference gets
-// wrong: elasticity is evaluated on the current positions, pins are
-// kinematic, self contact comes from a working broad phase with vertex-
-// triangle and edge-edge barriers refreshed every Newton iteration, and the
-// line search bounds the step by a conservative time of impact (FP64) instead
-// of 10 temporal samples.
+// wrong: elasticity is evaluated on the current positions, pins attract
+// (springs of the implicit solve, in k_gradient), contact and wall stiffness
+// take the current gap, self contact comes from a working broad phase with
+// vertex-triangle and edge-edge barriers refreshed every Newton iteration, and
+// the line search bounds the step by a conservative time of impact (FP64)
+// instead of 10 temporal samples.
 #include <cfloat>
 
 #include "kernels.cuh"
@@ -28,17 +29,6 @@ __device__ inline d3 bary(d3 p, d3 a, d3 b, d3 c) {
   v = fmin(fmax(v, 0.0), 1.0); w = fmin(fmax(w, 0.0), 1.0);
   if (v + w > 1.0) { double sm = v + w; if (sm > DBL_EPSILON) { v /= sm; w /= sm; } }
   return mk(1.0 - v - w, v, w);
-}
-
-__global__ void k_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= num_pins) return;
-  // several pins on one vertex: the last one in list order wins (pins arrive
-  // stably sorted by vertex)
-  int v = pin_vertex[k];
-  if (k + 1 < num_pins && pin_vertex[k + 1] == v) return;
-  x[3 * v] = pin_target[3 * k]; x[3 * v + 1] = pin_target[3 * k + 1]; x[3 * v + 2] = pin_target[3 * k + 2];
-  fixed[v] = 1;
 }
 
 // Candidate pairs -> contacts at the current positions. Every candidate gets a
@@ -75,56 +65,6 @@ __global__ void k_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int
   }
   if (!(C.gap < gap_max)) C.type = -1 - C.type;  // outside the activation distance: inactive
   out[k] = C;
-}
-
-// Kinematic pins: flag the vertex, and its wanted move (target - x) into ext
-// and x1 = target (several pins on one vertex: the last in list order wins).
-__global__ void k_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
-                          unsigned char* fixed) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= num_pins) return;
-  int v = pin_vertex[k];
-  if (k + 1 < num_pins && pin_vertex[k + 1] == v) return;
-  for (int q = 0; q < 3; ++q) { ext[3 * v + q] = pin_target[3 * k + q] - x[3 * v + q]; x1[3 * v + q] = pin_target[3 * k + q]; }
-  fixed[v] = 1;
-}
-// Largest pin move |target - x| (IEEE bits, max-reduced as integers).
-__global__ void k_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  double m = 0.0;
-  if (k < num_pins) {
-    int v = pin_vertex[k];
-    double a = pin_target[3 * k] - x[3 * v], b = pin_target[3 * k + 1] - x[3 * v + 1], c = pin_target[3 * k + 2] - x[3 * v + 2];
-    m = sqrt(a * a + b * b + c * c);
-  }
-  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
-}
-// Sub-step pin targets: start_k = x[pin vertex] once, then target = start + f (final - start).
-__global__ void k_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= num_pins) return;
-  int v = pin_vertex[k];
-  for (int q = 0; q < 3; ++q) start[3 * k + q] = x[3 * v + q];
-}
-__global__ void k_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= 3 * num_pins) return;
-  target[k] = start[k] + (fin[k] - start[k]) * f;
-}
-
-// x += toi * ext on pinned vertices (toi: the move's conservative time of impact).
-__global__ void k_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, const Ctrl* ctrl, double* x) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= num_pins || ctrl->toi_overflow) return;  // incomplete time of impact: the caller redoes the pass
-  int v = pin_vertex[k];
-  if (k + 1 < num_pins && pin_vertex[k + 1] == v) return;
-  double t = fmin(1.0, __longlong_as_double((long long)*toi));
-  if (t >= 1.0) {   // exactly on the target
-    for (int q = 0; q < 3; ++q) x[3 * v + q] += ext[3 * v + q];
-    return;
-  }
-  for (int q = 0; q < 3; ++q) x[3 * v + q] += t * ext[3 * v + q];
 }
 
 // ext = 1.25 d, clipped vertex by vertex to length lmax (no vertex moves
@@ -206,28 +146,6 @@ __global__ void k_toi_reset(unsigned long long* toi) { *toi = (unsigned long lon
 
 }  // namespace
 
-void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed, cudaStream_t s) {
-  if (num_pins) k_pin_apply<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, fixed);
-}
-void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
-                    unsigned char* fixed, cudaStream_t s) {
-  if (num_pins) k_pin_ext<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, ext, x1, fixed);
-}
-void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, const Ctrl* ctrl, double* x,
-                     cudaStream_t s) {
-  if (num_pins) k_pin_move<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, ext, toi, ctrl, x);
-}
-void launch_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out,
-                        cudaStream_t s) {
-  cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
-  if (num_pins) k_pin_maxdisp<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, out);
-}
-void launch_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start, cudaStream_t s) {
-  if (num_pins) k_pin_gather<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, x, start);
-}
-void launch_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target, cudaStream_t s) {
-  if (num_pins) k_pin_interp<<<nblk(3ll * num_pins), TPB, 0, s>>>(num_pins, start, fin, f, target);
-}
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s) {
   if (nvt + nee) k_pairs_to_contacts<<<nblk(nvt + nee), TPB, 0, s>>>(vt, nvt, ee, nee, tris, edges, x, gap_max, out);

@@ -279,6 +279,8 @@ __global__ void k_detect_write(MeshDev m, const double* x, const RigidDev* bodie
 // constant elastic Hessian: sum_i m_i w_i^2 / dt^2 + max(0, Wn^T H_el Wn), the
 // submatrix taken over the contact's valid vertices (each vertex at its last
 // list position, as extract_submatrix maps it).
+// `dt` divides the inertial part sum(m w^2): the time step in REFERENCE
+// semantics, the current gap in CORRECTED semantics.
 __device__ inline double contact_kbar(const MeshDev& m, const ContactDev& C, double dt) {
   if (dt <= 0.0) return 0.0;
   d3 n = mk(C.n[0], C.n[1], C.n[2]);
@@ -321,7 +323,11 @@ __global__ void k_contact_prep(MeshDev m, ContactDev* cs, int nc, StepParams p) 
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   ContactDev& C = cs[c];
-  C.kbar = contact_kbar(m, C, p.dt);
+  // CORRECTED: the inertial part of the stiffness is sum(m w^2) / g^2 at the
+  // current gap instead of / dt^2 (the form of the reference's pin and strain
+  // stiffness), so the finite cubic barrier's force grows without bound as the
+  // pair closes instead of saturating at 1.5 k g_max
+  C.kbar = contact_kbar(m, C, p.semantics == 1 ? fmax(fmax(C.gap, p.min_gap), 1e-12) : p.dt);
   d3 nn = normalize_or_default(mk(C.n[0], C.n[1], C.n[2]), p.normal_eps);
   C.nn[0] = nn.x; C.nn[1] = nn.y; C.nn[2] = nn.z;
   bool barrier_type = (C.type == 0 || C.type == 3 || (p.semantics == 1 && C.type == 1));
@@ -440,6 +446,33 @@ __device__ inline Svd32 svd32(d3 c0, d3 c1) {
 }
 
 
+// CORRECTED elasticity: the as-rigid-as-possible membrane energy
+// k |F - R|^2 per face (F = [x1 - x0, x2 - x0] Dm^-1, R = U V^T from its thin
+// SVD, k = area * thickness * mu). The reference's force formula
+// (elasticity.cpp:18-61) drops the rotation of its edge-aligned frame and is
+// not the gradient of its own energy away from rest; this one is exact, and
+// the constant Hessian 2k (G G^T) (x) I3 of k_elastic_slots is its Hessian at
+// fixed R. Gathered per vertex over its incident faces in face order.
+__global__ void k_arap_gradient(MeshDev m, const double* X, double mu, double thickness, double* g) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.V) return;
+  d3 acc = mk(0, 0, 0);
+  for (int k = m.vf_ptr[i]; k < m.vf_ptr[i + 1]; ++k) {
+    int f = m.vf[k] / 3, a = m.vf[k] % 3;
+    int v0 = m.tris[3 * f], v1 = m.tris[3 * f + 1], v2 = m.tris[3 * f + 2];
+    d3 e1 = ld3(X, v1) - ld3(X, v0), e2 = ld3(X, v2) - ld3(X, v0);
+    double da = m.dm_inv[4 * f], db = m.dm_inv[4 * f + 1], dc = m.dm_inv[4 * f + 2], dd = m.dm_inv[4 * f + 3];
+    d3 F0 = e1 * da + e2 * dc, F1 = e1 * db + e2 * dd;
+    Svd32 s = svd32(F0, F1);
+    d3 R0 = s.U0 * s.V00 + s.U1 * s.V01, R1 = s.U0 * s.V10 + s.U1 * s.V11;
+    double tk = 2.0 * m.rest_area[f] * thickness * mu;
+    d3 P0 = (F0 - R0) * tk, P1 = (F1 - R1) * tk;
+    double G0 = a == 0 ? -(da + dc) : (a == 1 ? da : dc), G1 = a == 0 ? -(db + dd) : (a == 1 ? db : dd);
+    acc = acc + P0 * G0 + P1 * G1;
+  }
+  st3(g, i, acc);
+}
+
 __device__ inline int warp_sum_i(int v) { for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o); return v; }
 __device__ inline unsigned warp_and(unsigned v) { for (int o = 16; o; o >>= 1) v &= __shfl_xor_sync(0xffffffffu, v, o); return v; }
 __device__ inline double warp_max_d(double v) { for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
@@ -554,8 +587,17 @@ __global__ void __launch_bounds__(256, 3) k_gradient(MeshDev m, const double* x,
     int ds = m.diag_slot[i];
     double A = mdiag + m.el_a[ds], B = mdiag + m.el_b[ds];
     double D0 = fmax(A, 1e-8), D2 = fmax(B, 1e-8);  // enforce_spd of the diagonal H_total block
-    // pins (sorted by vertex; pin_head[i] = first pin of vertex i or -1);
-    // CORRECTED pins are kinematic and carry no barrier
+    // CORRECTED pins attract: kappa / 2 |x - target|^2 per pin with
+    // kappa = 100 (m / dt^2 + a), a the vertex's elastic diagonal coefficient
+    if (num_pins > 0 && p.semantics == 1) {
+      int lo = pin_head[i];
+      double kp = PIN_SCALE * (mdiag + m.el_a[ds]);
+      for (int k = lo; k >= 0 && k < num_pins && pin_vertex[k] == i; ++k) {
+        gi = gi + (xi - mk(pin_target[3 * k], pin_target[3 * k + 1], pin_target[3 * k + 2])) * kp;
+        H[0] += kp; H[4] += kp; H[8] += kp;
+      }
+    }
+    // pins (sorted by vertex; pin_head[i] = first pin of vertex i or -1)
     if (num_pins > 0 && p.semantics == 0) {
       int lo = pin_head[i];
       for (int k = lo; k >= 0 && k < num_pins && pin_vertex[k] == i; ++k) {
@@ -585,11 +627,12 @@ __global__ void __launch_bounds__(256, 3) k_gradient(MeshDev m, const double* x,
       if (!W.active) continue;
       d3 wn = mk(W.n[0], W.n[1], W.n[2]);
       d3 n = normalize_or_default(wn, p.normal_eps);
-      double gh = fmax(fmax(p.wall_gap, p.min_gap), 1e-12);
+      double gap = dot(n, xi) - W.offset;
+      // REFERENCE: m / wall_gap^2; CORRECTED: m / g^2 at the current gap (as for contacts)
+      double gh = fmax(fmax(p.semantics == 1 ? gap : p.wall_gap, p.min_gap), 1e-12);
       double wnn = nrm(wn);
       d3 ns = wnn > 1e-9 ? wn / wnn : mk(0, 1, 0);
       double kbar = mi / (gh * gh) + fmax(0.0, ns.x * (D0 * ns.x) + ns.y * (D0 * ns.y) + ns.z * (D2 * ns.z));
-      double gap = dot(n, xi) - W.offset;
       if (!in_domain(gap, p.contact_gap_max)) continue;
       double dV = bar_grad(gap, p.contact_gap_max, kbar), d2V = bar_hess(gap, p.contact_gap_max, kbar);
       gi = gi + n * dV;
@@ -1254,6 +1297,9 @@ void launch_elastic_slots(const MeshDev& m, double mu, double thickness, int sem
 }
 void launch_elastic_gradient(const MeshDev& m, const double* X, double mu, double thickness, double* g, cudaStream_t s) {
   if (m.V) k_elastic_gradient<<<nblk(m.V), TPB, 0, s>>>(m, X, mu, thickness, g);
+}
+void launch_arap_gradient(const MeshDev& m, const double* X, double mu, double thickness, double* g, cudaStream_t s) {
+  if (m.V) k_arap_gradient<<<nblk(m.V), TPB, 0, s>>>(m, X, mu, thickness, g);
 }
 void launch_predict(int V, const double* x, const double* v, double dt, double* x_old, double* x_hat, cudaStream_t s) {
   if (V) k_predict<<<nblk(3ll * V), TPB, 0, s>>>(V, x, v, dt, x_old, x_hat);

@@ -16,6 +16,7 @@ struct RigidDev {
 // setup
 void launch_elastic_slots(const MeshDev& m, double mu, double thickness, int semantics, double* el_a, double* el_b, cudaStream_t s);
 void launch_elastic_gradient(const MeshDev& m, const double* mesh_vertices, double mu, double thickness, double* g_el, cudaStream_t s);
+void launch_arap_gradient(const MeshDev& m, const double* X, double mu, double thickness, double* g, cudaStream_t s);
 
 // per step
 void launch_predict(int V, const double* x, const double* v, double dt, double* x_old, double* x_hat, cudaStream_t s);
@@ -85,15 +86,6 @@ void launch_outer_ctl(StepCtl* c, double beta_max, cudaGraphConditionalHandle ou
 void launch_velocity_ctl(int V, const double* x, const double* x_old, double dt, double damp_scale, double* v, const StepCtl* c, cudaStream_t s);
 
 // CORRECTED semantics (corrected.cu)
-void launch_pin_apply(const int* pin_vertex, const double* pin_target, int num_pins, double* x, unsigned char* fixed, cudaStream_t s);
-void launch_pin_ext(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, double* ext, double* x1,
-                    unsigned char* fixed, cudaStream_t s);
-void launch_pin_move(const int* pin_vertex, int num_pins, const double* ext, const unsigned long long* toi, const Ctrl* ctrl, double* x,
-                     cudaStream_t s);
-void launch_pin_maxdisp(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, unsigned long long* out,
-                        cudaStream_t s);
-void launch_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start, cudaStream_t s);
-void launch_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target, cudaStream_t s);
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s);
 void launch_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double scale, double lmax,

@@ -112,11 +112,17 @@ template <class F> __device__ inline double advance(F dist, double l, double eta
 }
 
 // Time of impact of pair (kind 0: vertex id[0] against triangle id[1..3];
-// kind 1: edge id[0..1] against edge id[2..3]) moving x -> x + ext.
+// kind 1: edge id[0..1] against edge id[2..3]) moving x -> x + ext. The
+// distance only depends on the relative motion of the four vertices, so the
+// bound l on its rate of change is taken from the displacements minus their
+// mean (additive CCD): two layers sliding together bound nothing, where the
+// absolute displacements would cap the step at about 200 d0 / l.
 __device__ inline double pair_toi(int kind, const int id[4], const double* x, const double* ext, double eta_min, double near) {
   d3 p[4], e[4];
   double L[4];
-  for (int q = 0; q < 4; ++q) { p[q] = ld3(x, id[q]); e[q] = ld3(ext, id[q]); L[q] = nrm(e[q]); }
+  for (int q = 0; q < 4; ++q) { p[q] = ld3(x, id[q]); e[q] = ld3(ext, id[q]); }
+  const d3 mean = (e[0] + e[1] + e[2] + e[3]) * 0.25;
+  for (int q = 0; q < 4; ++q) L[q] = nrm(e[q] - mean);
   if (kind == 0) {
     double l = L[0] + fmax(L[1], fmax(L[2], L[3]));
     return advance([&](double s) { d3 n, wq; return pt_dist(p[0] + e[0] * s, p[1] + e[1] * s, p[2] + e[2] * s, p[3] + e[3] * s, n, wq); }, l,

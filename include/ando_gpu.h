@@ -339,8 +339,8 @@ ANDO_API int32_t ando_last_gradient(ando_ctx ctx, double* gradient, int32_t num_
  *
  * Device pointers: rowptr (num_rows+1), cols (sorted per row), vals (9 floats
  * per block, row-major), rhs (3*num_rows), x (3*num_rows, overwritten) and
- * work (>= 24*num_rows floats, any contents; larger sizes are rejected with
- * ANDO_ERR_CAPACITY, as are num_rows > ANDO_NOALLOC_MAX_ROWS). `stream` is a
+ * work (>= 24*num_rows floats, any contents; smaller work buffers are rejected
+ * with ANDO_ERR_CAPACITY, as are num_rows > ANDO_NOALLOC_MAX_ROWS). `stream` is a
  * cudaStream_t of `device` (NULL = legacy default stream). Reduction partials
  * and grid-barrier words live in a 16 KiB static device array per device
  * (partials for up to 640 CTAs; the grid is capped there); the call zeroes its
@@ -350,9 +350,12 @@ ANDO_API int32_t ando_last_gradient(ando_ctx ctx, double* gradient, int32_t num_
  * kernel's grid size (which may load the module): make it before any stream
  * capture. Calls on one device share the scratch, so overlapping calls (other
  * streams or threads without ordering) race; serialise them. With all three
- * outputs NULL the call is asynchronous on `stream`; otherwise it synchronises
- * `stream` and reports iterations, the PCG status (0 converged, 1 max
- * iterations, 2 not SPD, 3 barrier timeout) and the final relative residual. */
+ * outputs NULL the call is asynchronous on `stream` and reports launch errors
+ * only: a grid-barrier timeout, a not-SPD stop or reaching max_iters is not
+ * reported, and the next call clears the status words. A caller that needs the
+ * PCG status passes at least one output; the call then synchronises `stream`
+ * and reports iterations, the PCG status (0 converged, 1 max iterations, 2 not
+ * SPD, 3 barrier timeout) and the final relative residual. */
 ANDO_API int32_t ando_pcg_solve_noalloc(int32_t device, void* stream, int32_t num_rows, const int32_t* rowptr,
                                         const int32_t* cols, const float* vals, const float* rhs, float* x, float* work,
                                         int64_t work_floats, double tol, int32_t max_iters, int32_t* iterations,

@@ -530,6 +530,32 @@ template <class R> R wall_stiffness(R mass, R wall_gap, const V3<R>& normal, con
   return ki + std::max(R(0), n.dot(H * n));
 }
 
+// CORRECTED dynamic stiffness. The cubic barrier (k / 2 g_max)(g_max - g)^3
+// (barrier.cpp:29-65) is finite at g = 0, so its force saturates at
+// 1.5 k g_max: with the reference's contact stiffness sum(m w^2) / dt^2 +
+// elastic (stiffness.cpp:53-116) a pair pressed harder than that closes to
+// zero distance, where no time-of-impact line search can move it again. The
+// reference's own pin (stiffness.cpp:118-144) and strain-limit
+// (strain_limiting.cpp:113-193) stiffnesses take the inertial part as
+// mass / g^2 at the current gap, which makes the force grow without bound as
+// the gap closes; CORRECTED uses that form for contacts and walls as well.
+// The elastic part is the reference's.
+template <class R> R corrected_gap_scale(R gap, R min_gap) { return std::max(std::max(gap, min_gap), R(1e-12)); }
+template <class R> R corrected_contact_stiffness(const ContactPair<R>& c, const std::vector<R>& masses, const Csr<R>& H_el, R min_gap) {
+  // contact_stiffness divides sum(m w^2) by its `dt` argument squared
+  return contact_stiffness(c, masses, corrected_gap_scale(c.gap, min_gap), H_el, Lookup::INDEXED);
+}
+template <class R> R corrected_wall_stiffness(R mass, R gap, const V3<R>& normal, const M3<R>& Hb, R min_gap) {
+  return wall_stiffness(mass, corrected_gap_scale(gap, min_gap), normal, Hb, min_gap);
+}
+// CORRECTED pins attract: E = kappa / 2 |x - target|^2 inside the implicit
+// solve, with kappa = 100 (m / dt^2 + a) where a is the vertex's elastic
+// diagonal coefficient, so a pinned vertex follows its target within about
+// 1 % of the elastic load on it while contacts can still push it aside
+// (the reference's pins repel: barrier.cpp:161-215).
+constexpr double kPinScale = 100.0;
+template <class R> R corrected_pin_stiffness(R mass, R dt, R el_diag) { return R(kPinScale * (double(mass) / (double(dt) * double(dt)) + double(el_diag))); }
+
 // ------------------------------------------------------------------ barrier
 // barrier.cpp:29-65
 template <class R> R barrier_energy(R g, R gm, R k) {
@@ -1531,9 +1557,57 @@ template <class R> void corrected_elastic_triplets(const Mesh<R>& mesh, std::vec
     for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) for (int k = 0; k < 3; ++k) out.push_back({t.v[a] * 3 + k, t.v[b] * 3 + k, c[a][b]});
   }
 }
+// CORRECTED elasticity. The reference's membrane energy k |F - I|^2 is taken
+// in a frame aligned with edge e1, and its force formula (elasticity.cpp:18-61)
+// drops the rotation of that frame, so away from the rest shape it is not the
+// gradient of that energy (central differences differ by tens of percent on a
+// sheared face). CORRECTED uses the as-rigid-as-possible membrane energy
+// E = k |F - R|^2 = k ((s0 - 1)^2 + (s1 - 1)^2), F = [x1 - x0, x2 - x0] Dm^-1
+// (3 x 2), R = U V^T from its thin SVD, k = area * thickness * mu. Its
+// gradient 2k (F - R) G^T (G = [[-1,-1],[1,0],[0,1]] Dm^-1) is exact, and
+// 2k (G G^T) (x) I3 (corrected_elastic_triplets) is its Hessian at fixed R.
+// Returns the face energy; adds the face's gradient to grad[0..2].
+template <class R> double arap_face(const Mesh<R>& mesh, const std::vector<V3<R>>& X, size_t f, double grad[3][3]) {
+  const auto& t = mesh.triangles[f];
+  const double mu = double(mesh.material.youngs_modulus) / (2.0 * (1.0 + double(mesh.material.poisson_ratio)));
+  const double k = double(mesh.rest_areas[f]) * double(mesh.material.thickness) * mu;
+  const M2<R>& D = mesh.Dm_inv[f];
+  const double da = D.a, db = D.b, dc = D.c, dd = D.d;
+  double e1[3], e2[3], F0[3], F1[3];
+  for (int q = 0; q < 3; ++q) {
+    e1[q] = double(X[size_t(t.v[1])][q]) - double(X[size_t(t.v[0])][q]);
+    e2[q] = double(X[size_t(t.v[2])][q]) - double(X[size_t(t.v[0])][q]);
+    F0[q] = e1[q] * da + e2[q] * dc; F1[q] = e1[q] * db + e2[q] * dd;
+  }
+  V3<double> Fc[2] = {V3<double>(F0[0], F0[1], F0[2]), V3<double>(F1[0], F1[1], F1[2])};
+  Svd32<double> sv; svd32(Fc, sv);
+  // R = U V^T: column c is U0 V[c][0] + U1 V[c][1]
+  V3<double> Rc[2] = {sv.U[0] * sv.V[0][0] + sv.U[1] * sv.V[0][1], sv.U[0] * sv.V[1][0] + sv.U[1] * sv.V[1][1]};
+  double P0[3], P1[3], E = 0.0;
+  for (int q = 0; q < 3; ++q) {
+    double a = F0[q] - Rc[0][q], b = F1[q] - Rc[1][q];
+    E += a * a + b * b;
+    P0[q] = 2.0 * k * a; P1[q] = 2.0 * k * b;
+  }
+  const double G[3][2] = {{-(da + dc), -(db + dd)}, {da, db}, {dc, dd}};
+  for (int a = 0; a < 3; ++a) for (int q = 0; q < 3; ++q) grad[a][q] += P0[q] * G[a][0] + P1[q] * G[a][1];
+  return k * E;
+}
 template <class R> void elastic_gradient_at(const Mesh<R>& mesh, const std::vector<V3<R>>& X, std::vector<R>& g) {
-  Mesh<R> tmp; tmp.vertices = X; tmp.triangles = mesh.triangles; tmp.Dm_inv = mesh.Dm_inv; tmp.rest_areas = mesh.rest_areas; tmp.material = mesh.material;
-  elastic_gradient(tmp, g);
+  std::vector<double> acc(3 * X.size(), 0.0);
+  for (size_t f = 0; f < mesh.triangles.size(); ++f) {
+    double gr[3][3] = {};
+    arap_face(mesh, X, f, gr);
+    const auto& t = mesh.triangles[f];
+    for (int a = 0; a < 3; ++a) for (int q = 0; q < 3; ++q) acc[3 * size_t(t.v[a]) + size_t(q)] += gr[a][q];
+  }
+  g.assign(acc.size(), R(0));
+  for (size_t i = 0; i < acc.size(); ++i) g[i] = R(acc[i]);
+}
+template <class R> double elastic_energy_at(const Mesh<R>& mesh, const std::vector<V3<R>>& X) {
+  double e = 0.0;
+  for (size_t f = 0; f < mesh.triangles.size(); ++f) { double gr[3][3] = {}; e += arap_face(mesh, X, f, gr); }
+  return e;
 }
 
 // Conservative time of impact of one pair along the motion x -> x + e: advance
@@ -1577,52 +1651,102 @@ template <class R> R advance_toi(const std::function<R(R)>& dist, R l, R eta_min
   return t;
 }
 
+// Discrete intersection check of one configuration (test infrastructure; the
+// reference's CollisionValidator only reads a contact list,
+// collision_validator.cpp:133-180, and cannot see a crossing that no contact
+// reports). Counts (mesh edge, triangle) pairs that share no vertex and where
+// the edge's segment passes through the triangle, over a uniform grid of cell
+// `cell`. Segment-triangle test in FP64: the segment's end points lie strictly
+// on opposite sides of the triangle's plane and the crossing point lies inside
+// the triangle (barycentric coordinates in [0, 1]).
+template <class R> long long count_edge_triangle_crossings(const Mesh<R>& m, const std::vector<V3<R>>& x, double cell) {
+  if (m.triangles.empty() || m.edges.empty() || !(cell > 0.0)) return 0;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (const auto& p : x) for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], double(p[k])); hi[k] = std::max(hi[k], double(p[k])); }
+  long long dims[3];
+  for (int k = 0; k < 3; ++k) dims[k] = std::max<long long>(1, std::min<long long>(1 << 10, (long long)((hi[k] - lo[k]) / cell) + 1));
+  auto key = [&](long long i, long long j, long long k) { return (i * dims[1] + j) * dims[2] + k; };
+  auto cidx = [&](double v, int k) { return std::min<long long>(dims[k] - 1, std::max<long long>(0, (long long)((v - lo[k]) / cell))); };
+  std::unordered_map<long long, std::vector<int>> grid;
+  for (size_t t = 0; t < m.triangles.size(); ++t) {
+    long long a[3], b[3];
+    for (int k = 0; k < 3; ++k) {
+      double mn = 1e300, mx = -1e300;
+      for (int q = 0; q < 3; ++q) { double v = double(x[size_t(m.triangles[t].v[q])][k]); mn = std::min(mn, v); mx = std::max(mx, v); }
+      a[k] = cidx(mn, k); b[k] = cidx(mx, k);
+    }
+    for (long long i = a[0]; i <= b[0]; ++i) for (long long j = a[1]; j <= b[1]; ++j) for (long long k = a[2]; k <= b[2]; ++k) grid[key(i, j, k)].push_back(int(t));
+  }
+  long long crossings = 0;
+  std::vector<int> seen;
+  for (const auto& e : m.edges) {
+    const V3<R>& P = x[size_t(e.v[0])];
+    const V3<R>& Q = x[size_t(e.v[1])];
+    long long a[3], b[3];
+    for (int k = 0; k < 3; ++k) { a[k] = cidx(std::min(double(P[k]), double(Q[k])), k); b[k] = cidx(std::max(double(P[k]), double(Q[k])), k); }
+    seen.clear();
+    for (long long i = a[0]; i <= b[0]; ++i) for (long long j = a[1]; j <= b[1]; ++j) for (long long k = a[2]; k <= b[2]; ++k) {
+      auto it = grid.find(key(i, j, k));
+      if (it != grid.end()) seen.insert(seen.end(), it->second.begin(), it->second.end());
+    }
+    std::sort(seen.begin(), seen.end());
+    seen.erase(std::unique(seen.begin(), seen.end()), seen.end());
+    for (int t : seen) {
+      const auto& tri = m.triangles[size_t(t)];
+      bool shares = false;
+      for (int q = 0; q < 3; ++q) if (tri.v[q] == e.v[0] || tri.v[q] == e.v[1]) shares = true;
+      if (shares) continue;
+      double A[3], B[3], C[3], p0[3], p1[3];
+      for (int k = 0; k < 3; ++k) {
+        A[k] = x[size_t(tri.v[0])][k]; B[k] = x[size_t(tri.v[1])][k]; C[k] = x[size_t(tri.v[2])][k];
+        p0[k] = P[k]; p1[k] = Q[k];
+      }
+      double u[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]}, w[3] = {C[0] - A[0], C[1] - A[1], C[2] - A[2]};
+      double nrm[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+      double s0 = nrm[0] * (p0[0] - A[0]) + nrm[1] * (p0[1] - A[1]) + nrm[2] * (p0[2] - A[2]);
+      double s1 = nrm[0] * (p1[0] - A[0]) + nrm[1] * (p1[1] - A[1]) + nrm[2] * (p1[2] - A[2]);
+      if (!((s0 > 0 && s1 < 0) || (s0 < 0 && s1 > 0))) continue;
+      double tt = s0 / (s0 - s1), X[3];
+      for (int k = 0; k < 3; ++k) X[k] = p0[k] + tt * (p1[k] - p0[k]) - A[k];
+      double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2], uw = u[0] * w[0] + u[1] * w[1] + u[2] * w[2], ww = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+      double xu = X[0] * u[0] + X[1] * u[1] + X[2] * u[2], xw = X[0] * w[0] + X[1] * w[1] + X[2] * w[2];
+      double den = uu * ww - uw * uw;
+      if (!(std::fabs(den) > 0.0)) continue;
+      double bv = (ww * xu - uw * xw) / den, bw = (uu * xw - uw * xu) / den;
+      if (bv >= 0.0 && bw >= 0.0 && bv + bw <= 1.0) ++crossings;
+    }
+  }
+  return crossings;
+}
+
+// Diagnostics of the CORRECTED Newton loop (test infrastructure): when
+// enabled, every Newton iteration appends the pair that bounded its time of
+// impact and the gradient norm it started from.
+struct NewtonTrace {
+  bool enabled = false;
+  struct Row { int kind = -1; int ids[4] = {-1, -1, -1, -1}; double d0 = 0, l = 0, t = 1, gnorm = 0; int below_half = 0; };
+  std::vector<Row> rows;
+  Row cur;
+  static NewtonTrace& get() { static NewtonTrace t; return t; }
+};
+
 template <class R> class CorrectedIntegrator {
  public:
-  // Kinematic pins that move more than half a mean edge length in one step
-  // drag the first free rows across their own triangles (the cloth folds onto
-  // the pinned row and every later line search stops at zero). Such a step is
-  // split into k = ceil(move / (edge / 2)) sub-steps (at most 8) of dt / k
-  // with the pin targets interpolated linearly.
-  static int substeps(const Mesh<R>& mesh, const State<R>& st, const Constraints<R>& C) {
-    const std::vector<V3<R>>& x0 = st.positions_safe.size() == st.positions.size() ? st.positions_safe : st.positions;
-    double mv = 0.0;
-    for (const auto& pin : C.pins) if (pin.active) mv = std::max(mv, double((pin.target_position - x0[size_t(pin.vertex_idx)]).norm()));
-    double edge = double(max_move(mesh)) / 4.0;
-    if (!(edge > 0.0) || !(mv > 0.5 * edge)) return 1;
-    return int(std::min(8.0, std::ceil(mv / (0.5 * edge))));
-  }
-
+  // One step per call, as the reference steps (integrator.cpp:70-150). Pins
+  // are energy terms of the implicit solve (corrected_pin_stiffness), so a
+  // fast drive needs no kinematic pre-move and no sub-steps: the Newton solve
+  // moves the pinned rows and the cloth they pull together, and the time of
+  // impact bounds both.
   static void step(Mesh<R>& mesh, State<R>& st, Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>* stats = nullptr) {
     StepStats<R> local; StepStats<R>& S = stats ? *stats : local;
     S = StepStats<R>();
-    const int k = substeps(mesh, st, C);
-    if (k == 1) { step_once(mesh, st, C, p, rigids, S); return; }
-    const size_t n = st.positions.size();
-    const std::vector<V3<R>>& x0 = st.positions_safe.size() == n ? st.positions_safe : st.positions;
-    std::vector<V3<R>> start(C.pins.size());
-    for (size_t q = 0; q < C.pins.size(); ++q) start[q] = x0[size_t(C.pins[q].vertex_idx)];
-    Constraints<R> Cs = C;
-    SimParams<R> ps = p;
-    ps.dt = R(double(p.dt) / k);
-    for (int j = 1; j <= k; ++j) {
-      for (size_t q = 0; q < C.pins.size(); ++q)
-        Cs.pins[q].target_position = start[q] + (C.pins[q].target_position - start[q]) * R(double(j) / k);
-      StepStats<R> Sj;
-      step_once(mesh, st, Cs, ps, rigids, Sj);
-      S.newton_iters += Sj.newton_iters; S.pcg_iters += Sj.pcg_iters; S.line_search_fail += Sj.line_search_fail;
-      S.contacts = std::max(S.contacts, Sj.contacts); S.pcg_not_converged += Sj.pcg_not_converged; S.strain_active = Sj.strain_active;
-      S.beta = Sj.beta;
-      S.alphas.insert(S.alphas.end(), Sj.alphas.begin(), Sj.alphas.end());
-      S.pcg_per_newton.insert(S.pcg_per_newton.end(), Sj.pcg_per_newton.begin(), Sj.pcg_per_newton.end());
-    }
+    step_once(mesh, st, C, p, rigids, S);
   }
 
   static void step_once(Mesh<R>& mesh, State<R>& st, Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids,
                         StepStats<R>& S) {
     const size_t n = st.positions.size(); const R dt = p.dt;
-    std::vector<char> fixed(n, 0);
-    for (const auto& pin : C.pins) if (pin.active) fixed[size_t(pin.vertex_idx)] = 1;
+    std::vector<char> fixed(n, 0);  // no kinematic vertices: pins are springs of the solve
     // The step starts where the previous one ended (or at the caller's own
     // positions): the position update of State::apply_gravity is an explicit,
     // collision-unchecked move, and the implicit predictor below already
@@ -1630,19 +1754,6 @@ template <class R> class CorrectedIntegrator {
     if (st.positions_safe.size() == n) st.positions = st.positions_safe;
     std::vector<V3<R>> x_old = st.positions, x_target(n);
     for (size_t i = 0; i < n; ++i) x_target[i] = x_old[i] + st.velocities[i] * dt;
-    // Kinematic pins move toward their targets only as far as their
-    // conservative time of impact allows (a teleported pin would drag the
-    // cloth into itself); the rest of the move waits for the next step.
-    {
-      std::vector<V3<R>> pm(n);
-      std::vector<char> none(n, 0);
-      bool any = false;
-      for (const auto& pin : C.pins) if (pin.active) { pm[size_t(pin.vertex_idx)] = pin.target_position - st.positions[size_t(pin.vertex_idx)]; any = true; }
-      if (any) {
-        R t = toi(mesh, st.positions, pm, none, C, rigids, R(0.5) * p.contact_gap_max, R(1e-3) * p.contact_gap_max);
-        for (size_t i = 0; i < n; ++i) if (fixed[i]) st.positions[i] = st.positions[i] + pm[i] * t;
-      }
-    }
     R beta = 0; int bi = 0;
     while (beta < p.beta_max && bi < 20) {
       R alpha = inner_newton(mesh, st, x_target, fixed, C, p, rigids, S);
@@ -1672,7 +1783,7 @@ template <class R> class CorrectedIntegrator {
     if (p.enable_strain_limiting) { strain_rebuild(mesh, st, p, H_el, C, Lookup::INDEXED); strain_gradient(mesh, st, C, p, g); }
     else C.strain_limits.clear();
     for (const auto& c : contacts) {
-      R kb = contact_stiffness(c, st.masses, dt, H_el, Lookup::INDEXED);
+      R kb = corrected_contact_stiffness(c, st.masses, H_el, p.min_gap);
       if (!in_domain(c.gap, p.contact_gap_max)) continue;
       V3<R> nrm = normalize_or_default(c.normal, p.contact_normal_epsilon);
       R dV = barrier_gradient(c.gap, p.contact_gap_max, kb);
@@ -1692,12 +1803,18 @@ template <class R> class CorrectedIntegrator {
         M3<R> Hb = extract_hessian_block(H_el, Index(vi), Lookup::INDEXED);
         R md = st.masses[vi] / (dt * dt);
         Hb(0, 0) += md; Hb(1, 1) += md; Hb(2, 2) += md;
-        R kb = wall_stiffness(st.masses[vi], p.wall_gap, w.normal, Hb, p.min_gap);
         R gap = nrm.dot(st.positions[vi]) - w.offset;
+        R kb = corrected_wall_stiffness(st.masses[vi], gap, w.normal, Hb, p.min_gap);
         if (!in_domain(gap, p.contact_gap_max)) continue;
         R dV = barrier_gradient(gap, p.contact_gap_max, kb);
         for (int k = 0; k < 3; ++k) g[vi * 3 + size_t(k)] += dV * nrm[k];
       }
+    }
+    for (const auto& pin : C.pins) {
+      if (!pin.active || pin.vertex_idx < 0 || size_t(pin.vertex_idx) >= n) continue;
+      size_t vi = size_t(pin.vertex_idx);
+      R kp = corrected_pin_stiffness(st.masses[vi], dt, extract_hessian_block(H_el, Index(vi), Lookup::INDEXED)(0, 0));
+      for (int k = 0; k < 3; ++k) g[3 * vi + size_t(k)] += kp * (st.positions[vi][k] - pin.target_position[k]);
     }
     for (size_t i = 0; i < n; ++i) if (fixed[i]) for (int k = 0; k < 3; ++k) g[3 * i + size_t(k)] = R(0);
   }
@@ -1711,7 +1828,7 @@ template <class R> class CorrectedIntegrator {
     corrected_elastic_triplets(mesh, tr);
     if (p.enable_strain_limiting) strain_hessian(mesh, st, C, p, tr);
     for (const auto& c : contacts) {
-      R kb = contact_stiffness(c, st.masses, dt, H_el, Lookup::INDEXED);
+      R kb = corrected_contact_stiffness(c, st.masses, H_el, p.min_gap);
       if (!in_domain(c.gap, p.contact_gap_max)) continue;
       V3<R> nrm = normalize_or_default(c.normal, p.contact_normal_epsilon);
       R d2V = barrier_hessian(c.gap, p.contact_gap_max, kb);
@@ -1734,18 +1851,77 @@ template <class R> class CorrectedIntegrator {
         M3<R> Hb = extract_hessian_block(H_el, vi, Lookup::INDEXED);
         R md = st.masses[size_t(vi)] / (dt * dt);
         Hb(0, 0) += md; Hb(1, 1) += md; Hb(2, 2) += md;
-        R kb = wall_stiffness(st.masses[size_t(vi)], p.wall_gap, w.normal, Hb, p.min_gap);
         R gap = nrm.dot(st.positions[size_t(vi)]) - w.offset;
+        R kb = corrected_wall_stiffness(st.masses[size_t(vi)], gap, w.normal, Hb, p.min_gap);
         if (!in_domain(gap, p.contact_gap_max)) continue;
         R d2V = barrier_hessian(gap, p.contact_gap_max, kb);
         for (int r = 0; r < 3; ++r) for (int q = 0; q < 3; ++q) { R v = d2V * nrm[r] * nrm[q]; if (std::fabs(v) >= p.barrier_tolerance) tr.push_back({vi * 3 + r, vi * 3 + q, v}); }
       }
+    }
+    for (const auto& pin : C.pins) {
+      if (!pin.active || pin.vertex_idx < 0 || pin.vertex_idx >= n) continue;
+      R kp = corrected_pin_stiffness(st.masses[size_t(pin.vertex_idx)], dt, extract_hessian_block(H_el, pin.vertex_idx, Lookup::INDEXED)(0, 0));
+      for (int k = 0; k < 3; ++k) tr.push_back({3 * pin.vertex_idx + k, 3 * pin.vertex_idx + k, kp});
     }
     // kinematic pins: drop every entry touching a fixed vertex, unit diagonal
     std::vector<Triplet<R>> kept; kept.reserve(tr.size());
     for (auto& t : tr) if (!fixed[size_t(t.row / 3)] && !fixed[size_t(t.col / 3)]) kept.push_back(t);
     for (Index i = 0; i < n; ++i) if (fixed[size_t(i)]) for (int k = 0; k < 3; ++k) kept.push_back({3 * i + k, 3 * i + k, R(1)});
     return Csr<R>::from_triplets(3 * n, kept);
+  }
+
+  // Incremental potential of the CORRECTED Newton system at positions X, with
+  // everything `gradient` evaluates at the state's positions frozen there: the
+  // contact pairs and their stiffness, the strain-limit constraints and their
+  // stiffness, the wall stiffness. Test infrastructure: its central
+  // differences at X = st.positions check `gradient` term by term.
+  static double energy(const Mesh<R>& mesh, const State<R>& st, const std::vector<V3<R>>& X, const std::vector<V3<R>>& x_target,
+                       const std::vector<ContactPair<R>>& contacts, Constraints<R>& C, const SimParams<R>& p, const Csr<R>& H_el) {
+    const size_t n = st.positions.size(); const double dt = double(p.dt);
+    double E = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      double mf = double(st.masses[i]) / (dt * dt);
+      for (int k = 0; k < 3; ++k) { double d = double(X[i][k]) - double(x_target[i][k]); E += 0.5 * mf * d * d; }
+    }
+    E += elastic_energy_at(mesh, X);
+    if (p.enable_strain_limiting) {
+      strain_rebuild(mesh, st, p, H_el, C, Lookup::INDEXED);
+      R tau = to_fraction(p.strain_tau);
+      R eps = p.strain_epsilon > R(0) ? to_fraction(p.strain_epsilon) : tau;
+      State<R> sx = st; sx.positions = X;
+      for (const auto& sc : C.strain_limits) {
+        V3<R> F[2]; strain_F(sx, mesh, size_t(sc.face_idx), F);
+        Svd32<R> sv; if (!svd32(F, sv)) continue;
+        R gap = (R(1) + tau + eps) - sv.sigma[std::clamp(sc.singular_index, 0, 1)];
+        E += double(barrier_energy(gap, eps, sc.stiffness));
+      }
+    }
+    for (const auto& c : contacts) {
+      if (c.type != ContactType::POINT_TRIANGLE && c.type != ContactType::EDGE_EDGE) continue;
+      R kb = corrected_contact_stiffness(c, st.masses, H_el, p.min_gap);
+      R d; V3<R> nm, wp, wq;
+      if (c.type == ContactType::POINT_TRIANGLE) narrow_pt(X[size_t(c.idx0)], X[size_t(c.idx1)], X[size_t(c.idx2)], X[size_t(c.idx3)], d, nm, wp, wq);
+      else narrow_ee(X[size_t(c.idx0)], X[size_t(c.idx1)], X[size_t(c.idx2)], X[size_t(c.idx3)], d, nm, wp, wq);
+      E += double(barrier_energy(d, p.contact_gap_max, kb));
+    }
+    for (const auto& w : C.walls) {
+      if (!w.active) continue;
+      V3<R> nrm = normalize_or_default(w.normal, p.contact_normal_epsilon);
+      for (size_t vi = 0; vi < n; ++vi) {
+        M3<R> Hb = extract_hessian_block(H_el, Index(vi), Lookup::INDEXED);
+        R md = st.masses[vi] / (p.dt * p.dt);
+        Hb(0, 0) += md; Hb(1, 1) += md; Hb(2, 2) += md;
+        R kb = corrected_wall_stiffness(st.masses[vi], nrm.dot(st.positions[vi]) - w.offset, w.normal, Hb, p.min_gap);
+        E += double(barrier_energy(nrm.dot(X[vi]) - w.offset, p.contact_gap_max, kb));
+      }
+    }
+    for (const auto& pin : C.pins) {
+      if (!pin.active || pin.vertex_idx < 0 || size_t(pin.vertex_idx) >= n) continue;
+      size_t vi = size_t(pin.vertex_idx);
+      double kp = double(corrected_pin_stiffness(st.masses[vi], p.dt, extract_hessian_block(H_el, Index(vi), Lookup::INDEXED)(0, 0)));
+      for (int k = 0; k < 3; ++k) { double d = double(X[vi][k]) - double(pin.target_position[k]); E += 0.5 * kp * d * d; }
+    }
+    return E;
   }
 
   // Conservative time of impact along ext (line search of the CORRECTED step).
@@ -1769,21 +1945,38 @@ template <class R> class CorrectedIntegrator {
     std::vector<std::pair<int, int>> vt, ee;
     candidates(mesh, x, &x1, R(0), vt, ee);
     auto L = [&](int i) { return ext[size_t(i)].norm(); };
+    // additive CCD: the distance depends on the relative motion only, so the
+    // rate bound comes from the displacements minus the pair's mean
+    auto Lrel = [&](int i, const V3<R>& mean) { return (ext[size_t(i)] - mean).norm(); };
     for (auto& pr : vt) {
       const auto& tri = mesh.triangles[size_t(pr.second)];
       int v = pr.first, a = tri.v[0], b = tri.v[1], c = tri.v[2];
-      R l = L(v) + std::max(L(a), std::max(L(b), L(c)));
+      V3<R> mean = (ext[size_t(v)] + ext[size_t(a)] + ext[size_t(b)] + ext[size_t(c)]) * R(0.25);
+      R l = Lrel(v, mean) + std::max(Lrel(a, mean), std::max(Lrel(b, mean), Lrel(c, mean)));
       auto dist = [&](R s) { R d; V3<R> nm, wp, wq; narrow_pt(x[size_t(v)] + ext[size_t(v)] * s, x[size_t(a)] + ext[size_t(a)] * s,
                                                               x[size_t(b)] + ext[size_t(b)] * s, x[size_t(c)] + ext[size_t(c)] * s, d, nm, wp, wq); return d; };
-      t = std::min(t, advance_toi<R>(dist, l, eta_min, near));
+      R tp = advance_toi<R>(dist, l, eta_min, near);
+      auto& tr = NewtonTrace::get();
+      if (tr.enabled) {
+        if (tp < R(0.5)) tr.cur.below_half++;
+        if (tp < t) { tr.cur.kind = 0; tr.cur.ids[0] = v; tr.cur.ids[1] = a; tr.cur.ids[2] = b; tr.cur.ids[3] = c; tr.cur.d0 = double(dist(R(0))); tr.cur.l = double(l); tr.cur.t = double(tp); }
+      }
+      t = std::min(t, tp);
     }
     for (auto& pr : ee) {
       const Edge &e1 = mesh.edges[size_t(pr.first)], &e2 = mesh.edges[size_t(pr.second)];
       int a = e1.v[0], b = e1.v[1], c = e2.v[0], d = e2.v[1];
-      R l = std::max(L(a), L(b)) + std::max(L(c), L(d));
+      V3<R> mean = (ext[size_t(a)] + ext[size_t(b)] + ext[size_t(c)] + ext[size_t(d)]) * R(0.25);
+      R l = std::max(Lrel(a, mean), Lrel(b, mean)) + std::max(Lrel(c, mean), Lrel(d, mean));
       auto dist = [&](R s) { R dd; V3<R> nm, wp, wq; narrow_ee(x[size_t(a)] + ext[size_t(a)] * s, x[size_t(b)] + ext[size_t(b)] * s,
                                                                x[size_t(c)] + ext[size_t(c)] * s, x[size_t(d)] + ext[size_t(d)] * s, dd, nm, wp, wq); return dd; };
-      t = std::min(t, advance_toi<R>(dist, l, eta_min, near));
+      R tp = advance_toi<R>(dist, l, eta_min, near);
+      auto& tr = NewtonTrace::get();
+      if (tr.enabled) {
+        if (tp < R(0.5)) tr.cur.below_half++;
+        if (tp < t) { tr.cur.kind = 1; tr.cur.ids[0] = a; tr.cur.ids[1] = b; tr.cur.ids[2] = c; tr.cur.ids[3] = d; tr.cur.d0 = double(dist(R(0))); tr.cur.l = double(l); tr.cur.t = double(tp); }
+      }
+      t = std::min(t, tp);
     }
     if (rigids) {
       for (const auto& body : *rigids) {
@@ -1824,6 +2017,7 @@ template <class R> class CorrectedIntegrator {
       R gn = 0; for (R e : g) gn = std::max(gn, std::fabs(e));
       if (gn < p.pcg_tol) return R(1);
       S.newton_iters++;
+      if (NewtonTrace::get().enabled) { NewtonTrace::get().cur = NewtonTrace::Row(); NewtonTrace::get().cur.gnorm = double(gn); }
       Csr<R> H = assemble(mesh, st, fixed, contacts, C, p, H_el);
       std::vector<R> d(3 * n, R(0)), ng(3 * n);
       for (size_t i = 0; i < 3 * n; ++i) ng[i] = -g[i];
@@ -1840,6 +2034,7 @@ template <class R> class CorrectedIntegrator {
         if (len > lmax) ext[i] = ext[i] * (lmax / len);
       }
       R alpha = std::min(R(1), toi(mesh, st.positions, ext, fixed, C, rigids, R(0), R(1e-3) * p.contact_gap_max));
+      if (NewtonTrace::get().enabled) NewtonTrace::get().rows.push_back(NewtonTrace::get().cur);
       S.alphas.push_back(alpha);
       if (alpha < R(1e-8)) return R(0);
       for (size_t i = 0; i < n; ++i) if (!fixed[i]) st.positions[i] = st.positions[i] + ext[i] * (alpha / R(1.25));

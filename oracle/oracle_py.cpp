@@ -222,6 +222,12 @@ template <class R> void bind(py::module_& m) {
         d["contacts"] = contacts;
         return d;
       })
+      // frozen-stiffness CORRECTED incremental potential at positions X (contacts, strain limits and walls from the state)
+      .def_static("corrected_energy", [](const MeshT& me, StateT& s, Arr<R> X, Arr<R> x_target, ConT& c, const ParT& p) {
+        auto contacts = detect_corrected(me, s.positions, (const std::vector<RB>*)nullptr, p.contact_gap_max);
+        Csr<R> H_el = CorrectedIntegrator<R>::base_elastic(me);
+        return CorrectedIntegrator<R>::energy(me, s, to_v3<R>(X), to_v3<R>(x_target), contacts, c, p, H_el);
+      })
       .def_static("corrected_toi", [](const MeshT& me, Arr<R> x, Arr<R> ext, py::object fixed_mask, const ConT& c) {
         auto fm = py::array_t<int8_t, py::array::c_style | py::array::forcecast>::ensure(fixed_mask);
         std::vector<char> fixed(fm.data(), fm.data() + fm.size());
@@ -247,11 +253,29 @@ template <class R> void bind(py::module_& m) {
         py::dict d; d["H_total"] = csr_dict(Ht); d["H_elastic"] = csr_dict(He); return d;
       });
 
+  m.def("edge_triangle_crossings", [](const MeshT& me, Arr<R> x, double cell) { return count_edge_triangle_crossings(me, to_v3<R>(x), cell); },
+        py::arg("mesh"), py::arg("positions"), py::arg("cell") = 0.01,
+        "Number of (edge, triangle) pairs sharing no vertex whose segment passes through the triangle");
+  m.def("newton_trace", [](bool enable) {
+    auto& tr = NewtonTrace::get();
+    py::list out;
+    for (const auto& r : tr.rows) {
+      py::dict d; d["kind"] = r.kind; d["ids"] = py::make_tuple(r.ids[0], r.ids[1], r.ids[2], r.ids[3]);
+      d["d0"] = r.d0; d["l"] = r.l; d["t"] = r.t; d["gnorm"] = r.gnorm; d["below_half"] = r.below_half;
+      out.append(d);
+    }
+    tr.rows.clear(); tr.enabled = enable;
+    return out;
+  }, "Enable or disable the CORRECTED Newton trace; returns and clears the rows recorded so far");
   m.def("barrier_energy", &barrier_energy<R>);
   m.def("barrier_gradient", &barrier_gradient<R>);
   m.def("barrier_hessian", &barrier_hessian<R>);
   m.def("elastic_gradient", [](const MeshT& me) { std::vector<R> g; elastic_gradient(me, g); return py::array_t<R>(py::ssize_t(g.size()), g.data()); });
   m.def("elastic_energy", [](const MeshT& me) { return elastic_energy(me); });
+  // CORRECTED (as-rigid-as-possible) membrane energy and its gradient at positions X
+  m.def("arap_energy", [](const MeshT& me, Arr<R> X) { return elastic_energy_at(me, to_v3<R>(X)); });
+  m.def("arap_gradient", [](const MeshT& me, Arr<R> X) {
+    std::vector<R> g; elastic_gradient_at(me, to_v3<R>(X), g); return py::array_t<R>(py::ssize_t(g.size()), g.data()); });
   m.def("pin_stiffness", [](R mass, R dt, py::object off, py::object H, R min_gap) {
     auto h = Arr<R>::ensure(H); M3<R> Hm; for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Hm(i, j) = h.at(i, j);
     return pin_stiffness(mass, dt, vec3<R>(off), Hm, min_gap); });

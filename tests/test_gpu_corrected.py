@@ -2,9 +2,10 @@
 
 CORRECTED keeps the reference's algorithm and fixes its defects: elasticity on
 the current positions with the consistent constant Hessian 2k (G G^T) (x) I3,
-kinematic pins, self contact from a working broad phase with vertex-triangle
-and edge-edge barriers refreshed every Newton iteration, and a conservative
-time-of-impact line search. Tolerances as in the REFERENCE parity tests.
+attracting pins (stiff springs of the implicit solve), contact and wall
+stiffness from the current gap, self contact from a working broad phase with
+vertex-triangle and edge-edge barriers refreshed every Newton iteration, and a
+conservative time-of-impact line search. Tolerances as in the REFERENCE parity tests.
 """
 from __future__ import annotations
 
@@ -18,26 +19,14 @@ from test_gpu_parity import bsr_to_dense, csr_to_dense, extent, max_rel_error, s
 pytestmark = pytest.mark.gpu
 
 
-def pinned_mask(sc, frame=0):
-    m = np.zeros(sc.num_vertices, dtype=np.int8)
-    for i, _ in sc.pins_at(frame):
-        m[i] = 1
-    return m
-
-
-def snapped(sc, x, frame=0):
-    y = x.copy()
-    for i, t in sc.pins_at(frame):
-        y[i] = t
-    return y
+def free_mask(sc):
+    """CORRECTED has no kinematic vertices: pins are springs of the solve."""
+    return np.zeros(sc.num_vertices, dtype=np.int8)
 
 
 def corrected_parity(oracle, abi, sc, x, v, params=None, expect_contacts=None):
-    # pinned vertices start on their targets: the step's collision-limited pin
-    # move is then a no-op and the oracle's snapped system is the one to match
-    x = snapped(sc, x)
     p = dict(sc.params, **(params or {}))
-    # GPU: eval_system snaps pinned vertices and evaluates the first Newton system
+    # GPU: eval_system evaluates the first Newton system at the uploaded state
     S = abi.Scene(sc.vertices, sc.triangles, sc.material)
     S.upload(x, v, sc.vertices, None)
     S.eval_system(abi.make_params(p, semantics="corrected"), sc.pins_at(0), sc.walls)
@@ -47,15 +36,14 @@ def corrected_parity(oracle, abi, sc, x, v, params=None, expect_contacts=None):
     for r, c, blk in zip(*S.last_contact_blocks()):
         H_g[3 * r:3 * r + 3, 3 * c:3 * c + 3] += blk
     S.close()
-    # oracle at the same (snapped) state
+    # oracle at the same state
     O = oracle.f64
     m, s, op = oracle_scene(O, sc)
     for k, val in p.items():
         setattr(op, k, val)
-    xs = snapped(sc, x)
-    s.set_positions(xs)
+    s.set_positions(x)
     s.set_velocities(v)
-    res = O.Integrator.corrected_system(m, s, x + op.dt * v, pinned_mask(sc), oracle_constraints(O, sc), op)
+    res = O.Integrator.corrected_system(m, s, x + op.dt * v, free_mask(sc), oracle_constraints(O, sc), op)
     g_o = np.asarray(res["gradient"])
     H_o = csr_to_dense(res["hessian"])
     if expect_contacts is not None:
@@ -211,7 +199,9 @@ def test_corrected_step_parity_hanging_cloth(oracle, core):
     assert all(s["newton_iters"] > 0 for s in stats)
     x = gs.get_positions64()
     for i, t in sc.pins:
-        assert np.abs(x[i] - t).max() < 1e-12       # kinematic pins sit on their targets
+        # pins are stiff springs: each corner carries half the cloth's weight
+        # (about 1 N) at a stiffness of about 2e4 N/m
+        assert np.abs(x[i] - t).max() < 2e-4
 
 
 def test_corrected_free_run_hanging_cloth(oracle, core):

@@ -20,11 +20,9 @@ def contact_scene(n=16):
     return sc
 
 
-def pinned_mask(sc, f=0):
-    m = np.zeros(sc.num_vertices)
-    for i, _ in sc.pins_at(f):
-        m[i] = 1
-    return m
+def kinematic_mask(sc):
+    """CORRECTED has no kinematic vertices (pins are springs of the solve)."""
+    return np.zeros(sc.num_vertices)
 
 
 def evaluated(abi, sc):
@@ -33,7 +31,7 @@ def evaluated(abi, sc):
     S.apply_gravity(sc.gravity, p.dt)
     S.eval_system(p, sc.pins_at(0), sc.walls)
     d = S.last_scaled_system()
-    s = lo.System(d["rowptr"], d["cols"], d["valh"].astype(np.float64), d["Lf"], S.masses, pinned_mask(sc), 1.0 / p.dt ** 2,
+    s = lo.System(d["rowptr"], d["cols"], d["valh"].astype(np.float64), d["Lf"], S.masses, kinematic_mask(sc), 1.0 / p.dt ** 2,
                   d["xrow"], d["xcol"], d["xvalh"].astype(np.float64))
     return S, s
 

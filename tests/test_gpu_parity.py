@@ -223,9 +223,17 @@ def test_pcg_direction_matches_oracle_solve(oracle, abi):
     S.close()
     H = bsr_to_dense(rowptr, cols, vals, len(rowptr) - 1)
     b = rhs.astype(np.float64)
-    r = b - H @ sol.astype(np.float64)
+    x = sol.astype(np.float64)
+    r = b - H @ x
     assert np.abs(r).max() / np.abs(b).max() < 5e-5
     assert st["pcg_iters"] >= 1
+    # the FP64 oracle's block-Jacobi PCG (pcg_solver.cpp:8-146) on the same system, same tolerance
+    rp, cc, vv = dense_to_csr(H)
+    xo, conv, iters, _ = oracle.f64.pcg_solve_csr(H.shape[0], rp, cc, vv, b, 1e-5, 1000)
+    xo = np.asarray(xo)
+    assert conv
+    assert abs(iters - st["pcg_iters"]) <= 2
+    assert np.abs(x - xo).max() <= 1e-4 * np.abs(xo).max()
 
 
 # ---------------------------------------------------------- whole steps

@@ -192,13 +192,6 @@ def test_stale_contact_stiffness_expectation_is_zero(oracle, prec):
     assert k == pytest.approx(expect, rel=1e-5)
 
 
-def _fd_check(O, sc, scale, rel=1e-5):
-    """Central-difference check of the oracle's Newton gradient, FP64."""
-    from conftest import oracle_constraints, oracle_scene
-    m, s, p = oracle_scene(O, sc)
-    return m, s, p
-
-
 # Elasticity::face_hessian (elasticity.cpp:135-181) blocks are c*diag(1,1,0) and
 # enforce_spd clamps them to diag(max(c,1e-8), max(c,1e-8), 1e-8) exactly.
 @pytest.mark.parametrize("prec", PRECISIONS)

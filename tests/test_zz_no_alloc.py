@@ -35,12 +35,15 @@ def last_newton_system(abi, tol):
     return p, rowptr, cols, vals, rhs, sol
 
 
-def solve_noalloc(abi, dev, p, V, work_floats=None):
+def solve_noalloc(abi, dev, p, V, work_floats=None, bufs=None):
     import torch
 
     rowptr, cols, vals, rhs = dev
-    x = torch.zeros(3 * V, dtype=torch.float32, device="cuda:0")
-    work = torch.full((24 * V,), float("nan"), dtype=torch.float32, device="cuda:0")   # contents must not matter
+    if bufs is None:
+        bufs = (torch.empty(3 * V, dtype=torch.float32, device="cuda:0"), torch.empty(24 * V, dtype=torch.float32, device="cuda:0"))
+    x, work = bufs
+    x.zero_()
+    work.fill_(float("nan"))                        # contents must not matter
     it, status, rel = C.c_int32(-1), C.c_int32(-1), C.c_double(-1.0)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     rc = abi.lib().ando_pcg_solve_noalloc(
@@ -65,9 +68,15 @@ def test_noalloc_pcg_matches_step_solve(abi):
     assert scale > 0
     A = bsr_to_dense(rowptr, cols, np.asarray(vals, dtype=np.float64).reshape(-1, 3, 3), V)
     b = np.asarray(rhs, dtype=np.float64).ravel()
+    # caller-owned output and work buffers, allocated once up front
+    bufs = (torch.empty(3 * V, dtype=torch.float32, device="cuda:0"), torch.empty(24 * V, dtype=torch.float32, device="cuda:0"))
+    rc, *_ = solve_noalloc(abi, dev, p, V, bufs=bufs)   # warm-up: the first call on a device may load the module
+    assert rc == abi.ANDO_OK, abi.lib().ando_last_error().decode()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(0)[0]
     results = []
     for _ in range(2):
-        rc, x, iters, status, rel = solve_noalloc(abi, dev, p, V)
+        rc, x, iters, status, rel = solve_noalloc(abi, dev, p, V, bufs=bufs)
         assert rc == abi.ANDO_OK, abi.lib().ando_last_error().decode()
         assert status == 0 and 0 < iters <= p.pcg_max_iters and rel < p.pcg_tol
         # same iteration as the step's solve: same answer within 1e-5 of its size
@@ -76,6 +85,9 @@ def test_noalloc_pcg_matches_step_solve(abi):
         assert np.abs(b - A @ x).max() <= 10 * p.pcg_tol * np.abs(b).max()
         results.append(x)
     np.testing.assert_array_equal(results[0], results[1])
+    # the calls took no device memory: a cudaMalloc (or a cudaFree) would move the free byte count
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free_before
 
 
 def test_noalloc_pcg_rejects_small_work_buffer(abi):
