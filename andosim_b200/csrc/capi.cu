@@ -153,6 +153,8 @@ struct ando_ctx_s {
   DevBuf<double> x_safe;           // where the last step ended (or the uploaded positions): start of the next CORRECTED step
   bool safe_valid = false;
   DevBuf<unsigned char> fixed;
+  DevBuf<double> pin_start, pin_final;   // sub-step pin targets
+  DevBuf<unsigned long long> drive_extent;
   DevBuf<double> g_el_x, x1, ext;
   DevBuf<unsigned long long> toi;
   double max_move = 1e300;   // 4 x mean rest edge length: largest displacement per Newton iteration
@@ -934,6 +936,27 @@ int restore_start(ando_ctx c) {
   return ANDO_OK;
 }
 
+// Sub-steps of a CORRECTED step. Its conservative time of impact bounds every
+// Newton move, so a step whose pins or free vertices travel several edge
+// lengths (the C4 drive moves two per frame at 256 x 256, with the two
+// curtains 3 mm apart) advances by small fractions over many iterations.
+// Such a step is split into k = ceil(extent / (edge / 2)) sub-steps of dt / k
+// (at most 8), extent = max(largest pin move, dt max |v|), with the pin
+// targets interpolated linearly.
+int step_substeps(ando_ctx c, double dt, int& k) {
+  k = 1;
+  CK(c->drive_extent.reserve(1));
+  launch_drive_extent(c->pin_vertex.p, c->pin_target.p, c->num_pins, c->x.p, c->v.p, c->V, dt, c->drive_extent.p, c->stream);
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->drive_extent.p, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double mv = 0.0;
+  std::memcpy(&mv, &bits, sizeof(mv));
+  double edge = c->max_move / 4.0;
+  if (edge > 0.0 && mv > 0.5 * edge) k = int(std::min(8.0, std::ceil(mv / (0.5 * edge))));
+  return ANDO_OK;
+}
+
 int remember_safe(ando_ctx c) {
   CK(cudaMemcpyAsync(c->x_safe.p, c->x.p, sizeof(double) * 3ull * c->V, cudaMemcpyDeviceToDevice, c->stream));
   c->safe_valid = true;
@@ -1573,12 +1596,35 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
     }
   }
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
-    // pins are springs of the implicit solve: no kinematic pre-move, no sub-steps
-    st.substeps = 1;
-    rc = step_body(c, p, sp, num_rigids, num_walls, st);
+    int k = 1;
+    rc = step_substeps(c, p.dt, k);
     if (rc) return rc;
-    rc = remember_safe(c);
-    if (rc) return rc;
+    st.substeps = k;
+    if (k == 1) {
+      rc = step_body(c, p, sp, num_rigids, num_walls, st);
+      if (rc) return rc;
+      rc = remember_safe(c);
+      if (rc) return rc;
+    } else {
+      // k sub-steps of dt / k with the pin targets interpolated linearly from
+      // where the pinned vertices start
+      CK(c->pin_start.reserve(3ull * c->num_pins)); CK(c->pin_final.reserve(3ull * c->num_pins));
+      CK(cudaMemcpyAsync(c->pin_final.p, c->pin_target.p, sizeof(double) * 3ull * c->num_pins, cudaMemcpyDeviceToDevice, s));
+      launch_pin_gather(c->pin_vertex.p, c->num_pins, c->x.p, c->pin_start.p, s);
+      ando_params ps = p;
+      ps.dt = p.dt / k;
+      StepParams sps = sp;
+      sps.dt = ps.dt; sps.dt2inv = 1.0 / (ps.dt * ps.dt);
+      for (int j = 1; j <= k; ++j) {
+        launch_pin_interp(c->num_pins, c->pin_start.p, c->pin_final.p, double(j) / k, c->pin_target.p, s);
+        launch_predict(c->V, c->x.p, c->v.p, ps.dt, c->x_old.p, c->x_hat.p, s);   // x_hat = x + (dt / k) v
+        rc = step_body(c, ps, sps, num_rigids, num_walls, st);
+        if (rc) return rc;
+        rc = remember_safe(c);
+        if (rc) return rc;
+      }
+      CK(cudaMemcpyAsync(c->pin_target.p, c->pin_final.p, sizeof(double) * 3ull * c->num_pins, cudaMemcpyDeviceToDevice, s));
+    }
   } else {
     rc = detect(c, num_rigids);
     if (rc) return rc;

@@ -31,6 +31,35 @@ __device__ inline d3 bary(d3 p, d3 a, d3 b, d3 c) {
   return mk(1.0 - v - w, v, w);
 }
 
+// Extent of one step's motion, for its sub-step count: the largest pin move
+// |target - x| and the largest free motion dt |v| (IEEE bits of non-negative
+// doubles, max-reduced as integers).
+__global__ void k_drive_extent(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, const double* v, int V,
+                               double dt, unsigned long long* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (k < num_pins) {
+    int i = pin_vertex[k];
+    double a = pin_target[3 * k] - x[3 * i], b = pin_target[3 * k + 1] - x[3 * i + 1], c = pin_target[3 * k + 2] - x[3 * i + 2];
+    m = sqrt(a * a + b * b + c * c);
+  }
+  if (k < V) m = fmax(m, dt * sqrt(v[3 * k] * v[3 * k] + v[3 * k + 1] * v[3 * k + 1] + v[3 * k + 2] * v[3 * k + 2]));
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+// Sub-step pin targets: start_k = x[pin vertex] once, then target = start + f (final - start).
+__global__ void k_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= num_pins) return;
+  int v = pin_vertex[k];
+  for (int q = 0; q < 3; ++q) start[3 * k + q] = x[3 * v + q];
+}
+__global__ void k_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 3 * num_pins) return;
+  target[k] = start[k] + (fin[k] - start[k]) * f;
+}
+
 // Candidate pairs -> contacts at the current positions. Every candidate gets a
 // slot; the ones outside the activation distance are marked inactive
 // (type < 0) and contribute nothing.
@@ -146,6 +175,18 @@ __global__ void k_toi_reset(unsigned long long* toi) { *toi = (unsigned long lon
 
 }  // namespace
 
+void launch_drive_extent(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, const double* v, int V, double dt,
+                         unsigned long long* out, cudaStream_t s) {
+  cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+  int n = num_pins > V ? num_pins : V;
+  if (n) k_drive_extent<<<nblk(n), TPB, 0, s>>>(pin_vertex, pin_target, num_pins, x, v, V, dt, out);
+}
+void launch_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start, cudaStream_t s) {
+  if (num_pins) k_pin_gather<<<nblk(num_pins), TPB, 0, s>>>(pin_vertex, num_pins, x, start);
+}
+void launch_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target, cudaStream_t s) {
+  if (num_pins) k_pin_interp<<<nblk(3ll * num_pins), TPB, 0, s>>>(num_pins, start, fin, f, target);
+}
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s) {
   if (nvt + nee) k_pairs_to_contacts<<<nblk(nvt + nee), TPB, 0, s>>>(vt, nvt, ee, nee, tris, edges, x, gap_max, out);

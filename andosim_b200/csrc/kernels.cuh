@@ -86,6 +86,10 @@ void launch_outer_ctl(StepCtl* c, double beta_max, cudaGraphConditionalHandle ou
 void launch_velocity_ctl(int V, const double* x, const double* x_old, double dt, double damp_scale, double* v, const StepCtl* c, cudaStream_t s);
 
 // CORRECTED semantics (corrected.cu)
+void launch_drive_extent(const int* pin_vertex, const double* pin_target, int num_pins, const double* x, const double* v, int V, double dt,
+                         unsigned long long* out, cudaStream_t s);
+void launch_pin_gather(const int* pin_vertex, int num_pins, const double* x, double* start, cudaStream_t s);
+void launch_pin_interp(int num_pins, const double* start, const double* fin, double f, double* target, cudaStream_t s);
 void launch_pairs_to_contacts(const int2* vt, int nvt, const int2* ee, int nee, const int* tris, const int* edges, const double* x,
                               double gap_max, ContactDev* out, cudaStream_t s);
 void launch_swept_end(int V, const double* x, const float* d, const unsigned char* fixed, double scale, double lmax,

@@ -1078,19 +1078,77 @@ template <class R> R line_search(const std::vector<V3<R>>& x, const std::vector<
 template <class R> struct PcgResult { bool converged = false; int iters = 0; R rel_res = 0; };
 
 // PCGSolver::solve (pcg_solver.cpp:8-146): block-Jacobi, x0 as given, relative L-inf stop.
-template <class R> PcgResult<R> pcg_solve(const Csr<R>& A, const std::vector<R>& b, std::vector<R>& x, R tol, int max_iters) {
+// Inverse of the lower Cholesky factor of a symmetric 3x3 block, in FP64, with
+// the shifted retries of the GPU's diagonal factorisation (tr * 1e-12, 1e-8,
+// 1e-4 added to the diagonal; last resort: sqrt|diagonal|). Row-major 3x3.
+inline void chol_inverse3(const double H[9], double Linv[9]) {
+  auto chol = [](const double A[9], double L[9]) {
+    for (int k = 0; k < 9; ++k) L[k] = 0.0;
+    double d0 = A[0]; if (!(d0 > 0.0)) return false;
+    L[0] = std::sqrt(d0); L[3] = A[3] / L[0]; L[6] = A[6] / L[0];
+    double d1 = A[4] - L[3] * L[3]; if (!(d1 > 0.0)) return false;
+    L[4] = std::sqrt(d1); L[7] = (A[7] - L[6] * L[3]) / L[4];
+    double d2 = A[8] - L[6] * L[6] - L[7] * L[7]; if (!(d2 > 0.0)) return false;
+    L[8] = std::sqrt(d2); return true;
+  };
+  double L[9];
+  bool ok = chol(H, L);
+  if (!ok) {
+    double tr = std::fabs(H[0]) + std::fabs(H[4]) + std::fabs(H[8]) + 1e-300;
+    const double shift[3] = {1e-12, 1e-8, 1e-4};
+    for (int t = 0; t < 3 && !ok; ++t) {
+      double Hs[9]; for (int k = 0; k < 9; ++k) Hs[k] = H[k];
+      Hs[0] += tr * shift[t]; Hs[4] += tr * shift[t]; Hs[8] += tr * shift[t];
+      ok = chol(Hs, L);
+    }
+    if (!ok) {
+      for (int k = 0; k < 9; ++k) L[k] = 0.0;
+      L[0] = std::sqrt(std::max(std::fabs(H[0]), 1e-300)); L[4] = std::sqrt(std::max(std::fabs(H[4]), 1e-300)); L[8] = std::sqrt(std::max(std::fabs(H[8]), 1e-300));
+    }
+  }
+  for (int k = 0; k < 9; ++k) Linv[k] = 0.0;
+  Linv[0] = 1.0 / L[0]; Linv[4] = 1.0 / L[4]; Linv[8] = 1.0 / L[8];
+  Linv[3] = -L[3] * Linv[0] / L[4];
+  Linv[7] = -L[7] * Linv[4] / L[8];
+  Linv[6] = -(L[6] * Linv[0] + L[7] * Linv[3]) / L[8];
+}
+
+// PCGSolver::solve (pcg_solver.cpp:8-146): block-Jacobi PCG from x0, stop on
+// the relative L-inf residual. With scaled_stop (the CORRECTED step) the test
+// is taken on the block-scaled residual max_i |L_i^-1 r_i| < tol *
+// max_i |L_i^-1 b_i| (A_ii = L_i L_i^T), which a few rows with forces orders of
+// magnitude above the rest cannot dominate; the iteration is unchanged.
+template <class R> PcgResult<R> pcg_solve(const Csr<R>& A, const std::vector<R>& b, std::vector<R>& x, R tol, int max_iters,
+                                          bool scaled_stop = false) {
   PcgResult<R> res;
   const int n = int(b.size()), nv = n / 3;
   std::vector<M3<R>> P(static_cast<size_t>(nv));
+  std::vector<double> Li(scaled_stop ? size_t(9) * size_t(nv) : 0);
   for (int i = 0; i < nv; ++i) {
     M3<R> blk;
     for (int lr = 0; lr < 3; ++lr) { Index r = 3 * i + lr;
       for (Index k = A.rowptr[r]; k < A.rowptr[r + 1]; ++k) { Index c = A.cols[k]; if (c >= 3 * i && c < 3 * i + 3) blk(lr, c - 3 * i) = A.vals[k]; } }
     R det = blk.determinant();
     P[size_t(i)] = std::fabs(det) > R(1e-16) ? blk.inverse() : M3<R>::identity();
+    if (scaled_stop) {
+      double H[9]; for (int q = 0; q < 9; ++q) H[q] = double(blk(q / 3, q % 3));
+      chol_inverse3(H, &Li[size_t(9) * size_t(i)]);
+    }
   }
-  auto linf = [](const std::vector<R>& v) { R m = 0; for (R e : v) m = std::max(m, std::fabs(e)); return m; };
-  auto rel = [&](const std::vector<R>& r) { R ri = linf(r), bi = linf(b); return bi < R(1e-16) ? ri : ri / bi; };
+  auto linf = [&](const std::vector<R>& v) {
+    double m = 0;
+    if (!scaled_stop) { for (R e : v) m = std::max(m, double(std::fabs(e))); return R(m); }
+    for (int i = 0; i < nv; ++i) {
+      const double* q = &Li[size_t(9) * size_t(i)];
+      for (int r = 0; r < 3; ++r) {
+        double u = q[3 * r] * double(v[size_t(3 * i)]) + q[3 * r + 1] * double(v[size_t(3 * i + 1)]) + q[3 * r + 2] * double(v[size_t(3 * i + 2)]);
+        m = std::max(m, std::fabs(u));
+      }
+    }
+    return R(m);
+  };
+  const R binf = linf(b);
+  auto rel = [&](const std::vector<R>& r) { R ri = linf(r); return binf < R(1e-16) ? ri : ri / binf; };
   auto dot = [](const std::vector<R>& a, const std::vector<R>& c) { R s = 0; for (size_t k = 0; k < a.size(); ++k) s += a[k] * c[k]; return s; };
   auto apply = [&](const std::vector<R>& r, std::vector<R>& z) {
     for (int i = 0; i < nv; ++i) { V3<R> rb(r[size_t(3 * i)], r[size_t(3 * i + 1)], r[size_t(3 * i + 2)]); V3<R> zb = P[size_t(i)] * rb;
@@ -1121,7 +1179,7 @@ template <class R> PcgResult<R> pcg_solve(const Csr<R>& A, const std::vector<R>&
 
 // -------------------------------------------------------------- integrator
 template <class R> struct StepStats {
-  int newton_iters = 0, pcg_iters = 0, line_search_fail = 0, contacts = 0, pcg_not_converged = 0, strain_active = 0;
+  int newton_iters = 0, pcg_iters = 0, line_search_fail = 0, contacts = 0, pcg_not_converged = 0, strain_active = 0, substeps = 1;
   R beta = 0; std::vector<R> alphas; std::vector<int> pcg_per_newton;
 };
 
@@ -1732,15 +1790,47 @@ struct NewtonTrace {
 
 template <class R> class CorrectedIntegrator {
  public:
-  // One step per call, as the reference steps (integrator.cpp:70-150). Pins
-  // are energy terms of the implicit solve (corrected_pin_stiffness), so a
-  // fast drive needs no kinematic pre-move and no sub-steps: the Newton solve
-  // moves the pinned rows and the cloth they pull together, and the time of
-  // impact bounds both.
+  // Pins are energy terms of the implicit solve (corrected_pin_stiffness): no
+  // kinematic pre-move. The conservative time of impact bounds every Newton
+  // move, so a step whose pins or free vertices travel several edge lengths
+  // advances by small fractions over many iterations; such a step is split
+  // into k = ceil(extent / (edge / 2)) sub-steps of dt / k (at most 8),
+  // extent = max(largest pin move, dt max |v|), with the pin targets
+  // interpolated linearly from where the pinned vertices start.
+  static int substeps(const Mesh<R>& mesh, const State<R>& st, const Constraints<R>& C, R dt) {
+    const std::vector<V3<R>>& x0 = st.positions_safe.size() == st.positions.size() ? st.positions_safe : st.positions;
+    double mv = 0.0;
+    for (const auto& pin : C.pins) if (pin.active) mv = std::max(mv, double((pin.target_position - x0[size_t(pin.vertex_idx)]).norm()));
+    for (const auto& v : st.velocities) mv = std::max(mv, double(dt) * double(v.norm()));
+    double edge = double(max_move(mesh)) / 4.0;
+    if (!(edge > 0.0) || !(mv > 0.5 * edge)) return 1;
+    return int(std::min(8.0, std::ceil(mv / (0.5 * edge))));
+  }
+
   static void step(Mesh<R>& mesh, State<R>& st, Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>* stats = nullptr) {
     StepStats<R> local; StepStats<R>& S = stats ? *stats : local;
     S = StepStats<R>();
-    step_once(mesh, st, C, p, rigids, S);
+    const int k = substeps(mesh, st, C, p.dt);
+    S.substeps = k;
+    if (k == 1) { step_once(mesh, st, C, p, rigids, S); return; }
+    const size_t n = st.positions.size();
+    const std::vector<V3<R>>& x0 = st.positions_safe.size() == n ? st.positions_safe : st.positions;
+    std::vector<V3<R>> start(C.pins.size());
+    for (size_t q = 0; q < C.pins.size(); ++q) start[q] = x0[size_t(C.pins[q].vertex_idx)];
+    Constraints<R> Cs = C;
+    SimParams<R> ps = p;
+    ps.dt = R(double(p.dt) / k);
+    for (int j = 1; j <= k; ++j) {
+      for (size_t q = 0; q < C.pins.size(); ++q)
+        Cs.pins[q].target_position = start[q] + (C.pins[q].target_position - start[q]) * R(double(j) / k);
+      StepStats<R> Sj;
+      step_once(mesh, st, Cs, ps, rigids, Sj);
+      S.newton_iters += Sj.newton_iters; S.pcg_iters += Sj.pcg_iters; S.line_search_fail += Sj.line_search_fail;
+      S.contacts = std::max(S.contacts, Sj.contacts); S.pcg_not_converged += Sj.pcg_not_converged; S.strain_active = Sj.strain_active;
+      S.beta = Sj.beta;
+      S.alphas.insert(S.alphas.end(), Sj.alphas.begin(), Sj.alphas.end());
+      S.pcg_per_newton.insert(S.pcg_per_newton.end(), Sj.pcg_per_newton.begin(), Sj.pcg_per_newton.end());
+    }
   }
 
   static void step_once(Mesh<R>& mesh, State<R>& st, Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids,
@@ -2021,7 +2111,7 @@ template <class R> class CorrectedIntegrator {
       Csr<R> H = assemble(mesh, st, fixed, contacts, C, p, H_el);
       std::vector<R> d(3 * n, R(0)), ng(3 * n);
       for (size_t i = 0; i < 3 * n; ++i) ng[i] = -g[i];
-      auto pr = pcg_solve(H, ng, d, p.pcg_tol, p.pcg_max_iters);
+      auto pr = pcg_solve(H, ng, d, p.pcg_tol, p.pcg_max_iters, true);
       S.pcg_iters += pr.iters; S.pcg_per_newton.push_back(pr.iters);
       if (!pr.converged) S.pcg_not_converged++;
       // extended direction 1.25 d, clipped vertex by vertex to length lmax:

@@ -186,7 +186,7 @@ template <class R> void bind(py::module_& m) {
   auto stats_dict = [](const StepStats<R>& S, double seconds) {
     py::dict d;
     d["newton_iters"] = S.newton_iters; d["pcg_iters"] = S.pcg_iters; d["line_search_fail"] = S.line_search_fail;
-    d["contacts"] = S.contacts; d["pcg_not_converged"] = S.pcg_not_converged; d["beta"] = S.beta;
+    d["contacts"] = S.contacts; d["pcg_not_converged"] = S.pcg_not_converged; d["beta"] = S.beta; d["substeps"] = S.substeps;
     d["alphas"] = S.alphas; d["pcg_per_newton"] = S.pcg_per_newton; d["seconds"] = seconds;
     return d;
   };

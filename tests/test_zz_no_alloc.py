@@ -68,6 +68,7 @@ def test_noalloc_pcg_matches_step_solve(abi):
     assert scale > 0
     A = bsr_to_dense(rowptr, cols, np.asarray(vals, dtype=np.float64).reshape(-1, 3, 3), V)
     b = np.asarray(rhs, dtype=np.float64).ravel()
+    exact = np.linalg.solve(A, b)
     # caller-owned output and work buffers, allocated once up front
     bufs = (torch.empty(3 * V, dtype=torch.float32, device="cuda:0"), torch.empty(24 * V, dtype=torch.float32, device="cuda:0"))
     rc, *_ = solve_noalloc(abi, dev, p, V, bufs=bufs)   # warm-up: the first call on a device may load the module
@@ -79,8 +80,13 @@ def test_noalloc_pcg_matches_step_solve(abi):
         rc, x, iters, status, rel = solve_noalloc(abi, dev, p, V, bufs=bufs)
         assert rc == abi.ANDO_OK, abi.lib().ando_last_error().decode()
         assert status == 0 and 0 < iters <= p.pcg_max_iters and rel < p.pcg_tol
-        # same iteration as the step's solve: same answer within 1e-5 of its size
-        assert np.abs(x - sol).max() <= 1e-5 * scale, np.abs(x - sol).max() / scale
+        # The step's solve iterates the same block-Jacobi PCG but stops on the
+        # block-scaled residual, this entry point on the reference's unscaled one
+        # (pcg_solver.cpp:8-75), so at one tolerance the two stop at slightly
+        # different iterates: both answers lie within 1e-3 of their size of each
+        # other and of the exact solution.
+        assert np.abs(x - sol).max() <= 1e-3 * scale, np.abs(x - sol).max() / scale
+        assert np.abs(x - exact).max() <= 1e-3 * scale, np.abs(x - exact).max() / scale
         # and it does solve the system: true residual at the FP32 level of the tolerance
         assert np.abs(b - A @ x).max() <= 10 * p.pcg_tol * np.abs(b).max()
         results.append(x)
