@@ -24,7 +24,8 @@ PRECOND = {"block_jacobi": 0, "learned": 1}
 EXPORTED = [
     "ando_abi_version", "ando_status_string", "ando_last_error", "ando_ctx_create", "ando_ctx_destroy",
     "ando_mesh_upload", "ando_mesh_set_vertices", "ando_state_upload", "ando_state_download",
-    "ando_apply_gravity", "ando_step", "ando_compute_contacts", "ando_last_system", "ando_eval_system",
+    "ando_apply_gravity", "ando_step", "ando_compute_contacts", "ando_compute_contacts_corrected", "ando_last_system",
+    "ando_eval_system",
     "ando_last_gradient", "ando_last_contact_blocks", "ando_profile_enable", "ando_profile_read", "ando_ctx_stream",
     "ando_broad_phase", "ando_pcg_solve_noalloc",
 ]
@@ -148,6 +149,8 @@ def lib() -> C.CDLL:
     L.ando_eval_system.argtypes = [P, C.POINTER(Params), C.POINTER(Pin), I32, C.POINTER(Wall), I32, C.POINTER(Rigid), I32]
     L.ando_compute_contacts.restype = I32
     L.ando_compute_contacts.argtypes = [P, C.POINTER(Rigid), I32, C.POINTER(Contact), I32, pi]
+    L.ando_compute_contacts_corrected.restype = I32
+    L.ando_compute_contacts_corrected.argtypes = [P, C.c_double, C.POINTER(Rigid), I32, C.POINTER(Contact), I32, pi]
     L.ando_last_system.restype = I32; L.ando_last_system.argtypes = [P, pi, pi, pi, pi, pf, pf, pf]
     L.ando_last_gradient.restype = I32; L.ando_last_gradient.argtypes = [P, pd, I32]
     L.ando_last_contact_blocks.restype = I32; L.ando_last_contact_blocks.argtypes = [P, pi, pi, pi, pf]
@@ -444,18 +447,26 @@ class Scene:
         return dict(rowptr=rowptr, cols=cols, valh=valh.reshape(-1, 3, 3), xrow=xr, xcol=xc,
                     xvalh=xvalh[:9 * len(xr)].reshape(-1, 3, 3), bhat=bhat, Lf=Lf.reshape(-1, 6), Linv=Linv.reshape(-1, 6))
 
-    def contacts(self, rigids: Optional[List[Rigid]] = None) -> List[Contact]:
+    def contacts(self, rigids: Optional[List[Rigid]] = None, semantics: str = "reference", gap_max: float = 1e-3) -> List[Contact]:
+        """Contacts at the current state: the reference's query, or (semantics="corrected") the
+        self and rigid contacts within gap_max that the CORRECTED step uses."""
         nr = len(rigids) if rigids else 0
         ra = (Rigid * max(1, nr))(*(rigids or []))
+        if semantics == "corrected":
+            name = "ando_compute_contacts_corrected"
+            query = lambda b, cap, n: lib().ando_compute_contacts_corrected(self.ctx, float(gap_max), ra, nr, b, cap, n)
+        else:
+            name = "ando_compute_contacts"
+            query = lambda b, cap, n: lib().ando_compute_contacts(self.ctx, ra, nr, b, cap, n)
         n = C.c_int32()
         buf = (Contact * 1)()
-        rc = lib().ando_compute_contacts(self.ctx, ra, nr, buf, 0, C.byref(n))
+        rc = query(buf, 0, C.byref(n))
         if rc not in (ANDO_OK, ANDO_ERR_CAPACITY):
-            _check(rc, "ando_compute_contacts")
+            _check(rc, name)
         if n.value == 0:
             return []
         buf = (Contact * n.value)()
-        _check(lib().ando_compute_contacts(self.ctx, ra, nr, buf, n.value, C.byref(n)), "ando_compute_contacts")
+        _check(query(buf, n.value, C.byref(n)), name)
         return list(buf)
 
 

@@ -514,17 +514,23 @@ std::vector<RigidBody*> rigid_handles(py::object lst) {
   return h;
 }
 
-std::vector<Contact> compute_contacts(const Mesh& me, State& s, py::object rigid_list) {
+std::vector<Contact> compute_contacts(const Mesh& me, State& s, py::object rigid_list, const std::string& semantics, double gap_max) {
+  if (semantics != "reference" && semantics != "corrected") throw py::value_error("semantics must be 'reference' or 'corrected'");
   s.bind(me);
   std::vector<RigidBody*> h = rigid_handles(rigid_list);
   std::vector<ando_rigid> ab;
   for (auto* b : h) ab.push_back(b->to_abi());
+  const bool corrected = semantics == "corrected";
+  auto query = [&](ando_contact* out, int32_t cap, int32_t* n) {
+    return corrected ? ando_compute_contacts_corrected(s.ctx, gap_max, ab.data(), int32_t(ab.size()), out, cap, n)
+                     : ando_compute_contacts(s.ctx, ab.data(), int32_t(ab.size()), out, cap, n);
+  };
   int32_t n = 0;
   std::vector<ando_contact> buf(256);
-  int32_t rc = ando_compute_contacts(s.ctx, ab.data(), int32_t(ab.size()), buf.data(), int32_t(buf.size()), &n);
+  int32_t rc = query(buf.data(), int32_t(buf.size()), &n);
   if (rc == ANDO_ERR_CAPACITY) {
     buf.resize(size_t(n));
-    rc = ando_compute_contacts(s.ctx, ab.data(), int32_t(ab.size()), buf.data(), n, &n);
+    rc = query(buf.data(), n, &n);
   }
   check(rc, "compute_contacts");
   std::vector<Contact> out(static_cast<size_t>(n));
@@ -790,9 +796,12 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         for (size_t i = 0; i < h.size(); ++i) h[i]->from_abi(ab[i]);
       }, py::arg("mesh"), py::arg("state"), py::arg("constraints"), py::arg("params"), py::arg("rigid_bodies") = py::none(),
          "Take one simulation step using Newton integrator with beta accumulation")
-      .def_static("compute_contacts", [](const Mesh& me, State& s, py::object rigid_list) { return compute_contacts(me, s, rigid_list); },
-                  py::arg("mesh"), py::arg("state"), py::arg("rigid_bodies") = py::none(),
-                  "Detect all collision contacts for the current mesh/state")
+      // semantics="corrected" (not in the reference's binding) returns the self and rigid contacts
+      // within gap_max that the CORRECTED step uses
+      .def_static("compute_contacts", [](const Mesh& me, State& s, py::object rigid_list, const std::string& semantics, double gap_max) {
+        return compute_contacts(me, s, rigid_list, semantics, gap_max); },
+                  py::arg("mesh"), py::arg("state"), py::arg("rigid_bodies") = py::none(), py::arg("semantics") = "reference",
+                  py::arg("gap_max") = 1e-3, "Detect all collision contacts for the current mesh/state")
       .def_static("last_step_stats", [](const State& s) {
         py::dict d;
         d["newton_iters"] = s.last.newton_iters; d["pcg_iters"] = s.last.pcg_iters; d["pcg_max_per_newton"] = s.last.pcg_max_per_newton;

@@ -1707,6 +1707,10 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   return ANDO_OK;
 }
 
+namespace {
+int contacts_out(ando_ctx c, ando_contact* out, int32_t capacity, int32_t* num_out);
+}
+
 int32_t ando_compute_contacts(ando_ctx c, const ando_rigid* rigids, int32_t num_rigids, ando_contact* out, int32_t capacity, int32_t* num_out) {
   int rc = check_ctx(c);
   if (rc) return rc;
@@ -1718,6 +1722,28 @@ int32_t ando_compute_contacts(ando_ctx c, const ando_rigid* rigids, int32_t num_
   if (rc) return rc;
   rc = detect(c, num_rigids);
   if (rc) return rc;
+  return contacts_out(c, out, capacity, num_out);
+}
+
+int32_t ando_compute_contacts_corrected(ando_ctx c, double gap_max, const ando_rigid* rigids, int32_t num_rigids, ando_contact* out,
+                                        int32_t capacity, int32_t* num_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  if (!num_out || capacity < 0 || (capacity && !out) || num_rigids < 0 || (num_rigids && !rigids) || !(gap_max > 0.0))
+    return fail(ANDO_ERR_INVALID, "contact arguments");
+  std::vector<ando_rigid> copy(rigids, rigids + num_rigids);
+  rc = upload_rigids(c, copy.data(), num_rigids);
+  if (rc) return rc;
+  c->gap_max = gap_max;
+  c->bvh_epoch++;
+  rc = detect_corrected(c, num_rigids, gap_max);
+  if (rc) return rc;
+  return contacts_out(c, out, capacity, num_out);
+}
+
+namespace {
+int contacts_out(ando_ctx c, ando_contact* out, int32_t capacity, int32_t* num_out) {
   *num_out = c->ncontacts;
   if (c->ncontacts == 0) return ANDO_OK;
   std::vector<ContactDev> h(c->ncontacts);
@@ -1735,6 +1761,7 @@ int32_t ando_compute_contacts(ando_ctx c, const ando_rigid* rigids, int32_t num_
   }
   return c->ncontacts > capacity ? fail(ANDO_ERR_CAPACITY, "contact buffer too small") : ANDO_OK;
 }
+}  // namespace
 
 int32_t ando_last_system(ando_ctx c, int32_t* V, int32_t* nnzb, int32_t* rowptr, int32_t* cols, float* vals, float* rhs, float* sol) {
   int rc = check_ctx(c);

@@ -148,9 +148,11 @@ def c3(seed: int = 0, scenes: int = 64, frames: int = 60) -> List[Scene]:
     return out
 
 
-def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
+def c4(seed: int = 0, n: int = 256, frames: int = 300, size: float = 2.0, spacing: float = 0.003) -> Scene:
     """Two 2 m curtains (n x n each) 3 mm apart in y, top rows pinned and driven +-0.3 m along x at 0.5 Hz
-    in opposite phase. The reference has no call to move a pin, so the pin set is rebuilt every frame.
+    in opposite phase. `size` (default 2 m) shrinks the curtains: n = 48 with size = 0.375 keeps the edge
+    length (7.8 mm) and the drive of the 256 x 256 configuration on a smaller cloth; `spacing` (default
+    3 mm) sets the distance between the curtains. The reference has no call to move a pin, so the pin set is rebuilt every frame.
     The drive amplitude ramps in with a smoothstep over the first 0.5 s: started at full amplitude the
     pinned rows would jump two edge lengths (1.6 cm at n = 256) in the first frame. Every vertex gets a
     seeded +-0.1 mm jitter in all three axes: a curtain lying exactly in a plane has no out-of-plane
@@ -159,8 +161,8 @@ def c4(seed: int = 0, n: int = 256, frames: int = 300) -> Scene:
     rng = np.random.default_rng(seed)
     verts, tris, top = [], [], []
     for k in range(2):
-        g = grid_plane(n, 2.0)
-        v = np.stack([g[:, 0] - 1.0, np.full(n * n, 0.003 * k), g[:, 1] + 0.2], axis=1)
+        g = grid_plane(n, size)
+        v = np.stack([g[:, 0] - size / 2, np.full(n * n, spacing * k), g[:, 1] + 0.2], axis=1)
         v += rng.uniform(-1e-4, 1e-4, size=(n * n, 3))
         verts.append(v)
         tris.append(grid_triangles(n, n, offset=k * n * n))

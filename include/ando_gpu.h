@@ -131,7 +131,7 @@ typedef struct {
   double beta;
   double last_alpha;
   double device_ms;            /* device time of the step (CUDA events) */
-  int32_t substeps;            /* CORRECTED: sub-steps taken for a fast kinematic drive (1 = none) */
+  int32_t substeps;            /* CORRECTED: sub-steps taken for a fast drive or fast motion (1 = none) */
   int32_t pad_;
 } ando_step_stats;
 
@@ -223,6 +223,17 @@ ANDO_API int32_t ando_step(ando_ctx ctx, const ando_params* params,
  * the total exceeds `capacity`. */
 ANDO_API int32_t ando_compute_contacts(ando_ctx ctx, const ando_rigid* rigids, int32_t num_rigids,
                               ando_contact* out, int32_t capacity, int32_t* num_out);
+
+/* The contact set the CORRECTED step uses at the current positions: every
+ * vertex-triangle and edge-edge pair of the mesh closer than gap_max (LBVH
+ * broad phase, FP64 narrow phase, unsigned distances), then vertices against
+ * rigid triangles. Integrator.compute_contacts(..., semantics="corrected")
+ * and CollisionValidator read it; the reference's own query
+ * (integrator.cpp:238-244) finds no self contact (its BVH drops every leaf of
+ * 2-4 primitives, collision.cpp:65-159). Same output conventions as
+ * ando_compute_contacts. */
+ANDO_API int32_t ando_compute_contacts_corrected(ando_ctx ctx, double gap_max, const ando_rigid* rigids, int32_t num_rigids,
+                                                 ando_contact* out, int32_t capacity, int32_t* num_out);
 
 /* Block-sparse (3x3 BSR) system of the most recent Newton iteration, for
  * inspection and for the preconditioner-training dump. Pass NULL pointers to

@@ -216,3 +216,14 @@ def test_corrected_step_parity_sheets_in_contact(oracle, core):
     errs, stats, gs = step_parity(oracle, core, sc, 12, pcg_tol=1e-5)
     assert_step_band(errs)
     assert max(s["contacts"] for s in stats) > 0
+
+
+def test_corrected_c4_reduced_free_run_matches_fp64(oracle, core):
+    """The curtain workload shrunk to 2 x 32 x 32 over 0.5 m (one edge length of drive per frame, so the
+    step sub-steps; pins are springs of the solve, tolerance 1e-4 as configured): 60 frames of the GPU
+    step stay within 1e-4 of the extent of an all-FP64 oracle run."""
+    sc = scenes.c4(n=32, size=0.5, frames=60)
+    to, tg, sg = free_run(oracle, core, sc, 60)
+    assert max_rel_error(to, tg, extent(sc)) <= 1e-4
+    assert sum(s["substeps"] for s in sg) > 60
+    assert all(s["line_search_fail"] == 0 for s in sg)

@@ -149,3 +149,36 @@ def test_learned_needs_weights_and_corrected_semantics(abi):
     with pytest.raises(abi.AbiError, match="CORRECTED"):
         S.step(abi.make_params(sc.params, semantics="reference", precond="learned"), sc.pins, sc.walls)
     S.close()
+
+
+def test_learned_and_block_jacobi_steps_agree_on_the_curtains(abi):
+    """The curtain workload (64 x 64, the shipped weights, pcg_tol 1e-4 as configured): from the same
+    state, a step with the learned preconditioner and one with block Jacobi land within 1e-4 of the
+    extent of each other on every one of 20 paired frames. Both solves stop on the same block-scaled
+    residual test and both Newton loops on the same gradient test."""
+    from andosim_b200 import learned as learned_mod
+
+    sc = scenes.c4(n=64)
+    ext = float(np.ptp(sc.vertices, axis=0).max())
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material)
+    S.set_precond_weights(learned_mod.load_weights(None))
+    pl = abi.make_params(sc.params, semantics="corrected", precond="learned")
+    pj = abi.make_params(sc.params, semantics="corrected", precond="block_jacobi")
+    for f in range(5):
+        S.apply_gravity(sc.gravity, pl.dt)
+        S.step(pl, sc.pins_at(f), sc.walls)
+    diffs = []
+    for f in range(5, 25):
+        x0, v0 = S.download()
+        S.apply_gravity(sc.gravity, pj.dt)
+        sj = S.step(pj, sc.pins_at(f), sc.walls)
+        xj = S.download()[0]
+        S.upload(x0, v0)
+        S.apply_gravity(sc.gravity, pl.dt)
+        sl = S.step(pl, sc.pins_at(f), sc.walls)
+        xl = S.download()[0]
+        assert sj["line_search_fail"] == 0 and sl["line_search_fail"] == 0
+        assert sj["beta"] > 0.99 and sl["beta"] > 0.99            # both Newton loops converged
+        diffs.append(float(np.abs(xl - xj).max()) / ext)
+    S.close()
+    assert max(diffs) <= 1e-4, diffs
