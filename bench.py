@@ -52,14 +52,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256, help="curtain grid side")
-    ap.add_argument("--cpu-frames", type=int, default=1, help="frames of the CPU baseline sample")
+    ap.add_argument("--reference-budget", type=float, default=150.0,
+                    help="seconds of timed frames the CPU reference arm may spend (it times the frames that fit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-steps", type=int, default=240, help="frames of the REFERENCE-semantics measurement (0: skip)")
     ap.add_argument("--full-n", type=int, default=64, help="curtain grid of the full-length CORRECTED comparison (0: skip)")
     ap.add_argument("--full-steps", type=int, default=240, help="frames of the full-length CORRECTED comparison")
     ap.add_argument("--refresh", type=int, default=1, help="Newton iterations between evaluations of the preconditioner network")
     ap.add_argument("--weights", default=None, help="learned preconditioner weights (.npy); default: the shipped C4 weights")
-    ap.add_argument("--c3-frames", type=int, default=5, help="timed frames of the batched 64-scene comparison (0: skip)")
+    ap.add_argument("--c3-frames", type=int, default=60, help="timed frames of the batched 64-scene comparison (0: skip)")
+    ap.add_argument("--c2-frames", type=int, default=200, help="frames of the four-sheet stack (0: skip)")
     ap.add_argument("--seeds", type=int, default=3, help="seeds of the curtain workload in the paired learned/Jacobi window")
     return ap.parse_args()
 
@@ -172,6 +174,19 @@ def pcg_bytes(V, nnzb, prof):
     lit = prof["pcg_learned_iterations"]
     return (40 * nnzb + 144 * V) * it + 40 * prof["pcg_extra_block_iterations"] + (44 * nnzb + 72 * V) * lit \
         + 48 * V * prof["phase_launches"]["pcg"]
+
+
+def assembly_bytes(V, nnzb):
+    """Algorithmic bytes of one CORRECTED assembly (k_diag_factor + the scaled assembly): the diagonal
+    terms in (FP64 9 per vertex, 72 V), the factors out (FP64 L^-1 and FP32 L, 72 V) and per block slot
+    the elastic constants in (FP64 pair, 16), the unscaled block out (FP32, 36) and the scaled block out
+    (FP32, 36): 144 V + 88 nnzb."""
+    return 144 * V + 88 * nnzb
+
+
+# DRAM bytes per launch from one ncu capture of the kernel (None: not captured for this build)
+PCG_TRAFFIC = None
+ASSEMBLY_TRAFFIC = None
 
 
 class Timer:
@@ -339,47 +354,52 @@ def reference_semantics_run(args, sc, local, flush, pg):
             "graph_frames": sum(int(s["graph_launched"]) for s in stats), "gpu_launches": launches}
 
 
-def e2e_run(args, sc, local, flush, pg, weights):
-    """Frames/s through the ando_barrier_core API (host arrays in, positions out every frame)."""
+def e2e_run(args, scs, local, flush, pg, weights):
+    """Frames/s through the ando_barrier_core API (host arrays in, positions out every frame), over the
+    same seeds and frames as the device-resident number: frames 0..W-1 untimed, W..W+K-1 timed."""
     import torch
 
     from andosim_b200 import ando_barrier_core as abc
 
     abc.set_device(local)
     abc.set_precond_weights(weights)
-    m = abc.Mesh()
-    m.initialize(sc.vertices, sc.triangles, abc.Material(**sc.material))
-    st = abc.State()
-    st.initialize(m)
-    p = abc.SimParams()
-    for k, v in sc.params.items():
-        setattr(p, k, v)
-    p.semantics = "corrected"
-    p.preconditioner = "learned"
-    p.precond_refresh = args.refresh
+    e2e_ms, frames = 0.0, 0
+    for sc in scs:
+        m = abc.Mesh()
+        m.initialize(sc.vertices, sc.triangles, abc.Material(**sc.material))
+        st = abc.State()
+        st.initialize(m)
+        p = abc.SimParams()
+        for k, v in sc.params.items():
+            setattr(p, k, v)
+        p.semantics = "corrected"
+        p.preconditioner = "learned"
+        p.precond_refresh = args.refresh
 
-    def api_frame(f):
-        c = abc.Constraints()
-        for i, t in sc.pins_at(f):
-            c.add_pin(int(i), t)
-        for n, o, g in sc.walls:
-            c.add_wall(n, o, g)
-        st.apply_gravity(sc.gravity, p.dt)
-        abc.Integrator.step(m, st, c, p)
-        return st.get_positions()
+        def api_frame(f):
+            c = abc.Constraints()
+            for i, t in sc.pins_at(f):
+                c.add_pin(int(i), t)
+            for n, o, g in sc.walls:
+                c.add_wall(n, o, g)
+            st.apply_gravity(sc.gravity, p.dt)
+            abc.Integrator.step(m, st, c, p)
+            return st.get_positions()
 
-    for f in range(args.warmup):
-        api_frame(f)
-    tm = Timer(torch, torch.cuda.ExternalStream(st._stream_handle(), device=torch.device("cuda", local)), flush)
-    e2e_ms = 0.0
-    for f in range(args.steps):
-        _, ms = tm.frame(lambda: api_frame(args.warmup + f))
-        e2e_ms += ms
+        for f in range(args.warmup):
+            api_frame(f)
+        tm = Timer(torch, torch.cuda.ExternalStream(st._stream_handle(), device=torch.device("cuda", local)), flush)
+        for f in range(args.steps):
+            _, ms = tm.frame(lambda: api_frame(args.warmup + f))
+            e2e_ms += ms
+            frames += 1
+        del st, m
     e2e_ms = dist_max(e2e_ms, pg)
+    sc = scs[0]
     n_pins = len(sc.pins_at(0))
-    return {"value": round(args.steps * int(os.environ.get("WORLD_SIZE", "1")) / (e2e_ms * 1e-3), 2), "unit": "frames/s",
-            "h2d_bytes_per_step": n_pins * (4 + 24) + len(sc.walls) * 48,     # pins and walls uploaded each step
-            "d2h_bytes_per_step": 24 * sc.num_vertices}                       # positions (FP64) read back
+    return {"value": round(frames * int(os.environ.get("WORLD_SIZE", "1")) / (e2e_ms * 1e-3), 2), "unit": "frames/s",
+            "frames": frames, "h2d_bytes_per_step": n_pins * (4 + 24) + len(sc.walls) * 48,   # pins and walls uploaded each step
+            "d2h_bytes_per_step": 24 * sc.num_vertices}                                      # positions (FP64) read back
 
 
 def c3_run(args, local, seed=0):
@@ -433,6 +453,48 @@ def c3_run(args, local, seed=0):
     return out
 
 
+def c2_run(args, local, pg, seed=0):
+    """The four-sheet stack (4 x 96 x 96, 200 frames: drop, land, stack), CORRECTED with block Jacobi,
+    device-resident; contacts judged every 20 frames by the module's CollisionValidator on the CORRECTED
+    contact set, and the lowest vertex height."""
+    import torch
+
+    from andosim_b200 import abi, ando_barrier_core as abc, scenes
+
+    sc = scenes.c2(seed=seed, frames=args.c2_frames)
+    abc.set_device(local)
+    m = abc.Mesh()
+    m.initialize(sc.vertices, sc.triangles, abc.Material(**sc.material))
+    st = abc.State()
+    st.initialize(m)
+    p = abc.SimParams()
+    for k, v in sc.params.items():
+        setattr(p, k, v)
+    p.semantics = "corrected"
+    ms, newton, pcg, contacts, penetrations, zmin, fails = 0.0, 0, 0, 0, 0, 1e9, 0
+    c = abc.Constraints()
+    for n, o, g in sc.walls:
+        c.add_wall(n, o, g)
+    for f in range(args.c2_frames):
+        st.apply_gravity(sc.gravity, p.dt)
+        abc.Integrator.step(m, st, c, p)
+        s_ = abc.Integrator.last_step_stats(st)
+        ms += s_["device_ms"]; newton += s_["newton_iters"]; pcg += s_["pcg_iters"]; fails += s_["line_search_fail"]
+        if f % 20 == 19 or f == args.c2_frames - 1:
+            cs = abc.Integrator.compute_contacts(m, st, None, "corrected", float(p.contact_gap_max))
+            contacts = max(contacts, len(cs))
+            met = abc.CollisionValidator.compute_metrics(m, st, cs, float(p.contact_gap_max), True)
+            penetrations += int(met.num_penetrations)
+            zmin = min(zmin, float(st.get_positions64()[:, 2].min()))
+    ms = dist_max(ms, pg)
+    return {"workload": "c2_stack_4x96x96", "vertices": sc.num_vertices, "frames": args.c2_frames, "semantics": "CORRECTED",
+            "preconditioner": "block_jacobi", "frames_per_s": round(args.c2_frames / (ms * 1e-3), 2),
+            "newton_iters_per_frame": round(newton / args.c2_frames, 2), "pcg_iters_per_newton": round(pcg / max(newton, 1), 2),
+            "line_search_fail": fails, "contacts_max": contacts, "validator_penetrations": penetrations, "z_min": zmin,
+            "timing": "CUDA events of each step (device_ms), positions stay on the device",
+            "waves": "2 mm (the configured 2 cm waves on sheets 5 mm apart start the stack self-intersecting)"}
+
+
 def run_ours(args, rank, world, local, pg):
     import torch
 
@@ -443,7 +505,8 @@ def run_ours(args, rank, world, local, pg):
         build()
     barrier(pg)
     torch.cuda.set_device(local)
-    sc = scenes.c4(seed=rank, n=args.n)
+    scs = [scenes.c4(seed=rank + world * k, n=args.n) for k in range(max(args.seeds, 1))]
+    sc = scs[0]
     V, T = sc.num_vertices, sc.num_triangles
     weights = learned.load_weights(Path(args.weights) if args.weights else None)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
@@ -452,8 +515,7 @@ def run_ours(args, rank, world, local, pg):
     # the paired window over several seeds of the workload: one trajectory's
     # iteration counts depend on which hard Newton systems its frames contain
     res, diffs, nframes = None, [], 0
-    for k in range(max(args.seeds, 1)):
-        sck = sc if k == 0 else scenes.c4(seed=rank + world * k, n=args.n)
+    for sck in scs:
         r, d, n = paired_run(args, sck, local, flush, pg, weights, raw=True)
         if res is None:
             res = r
@@ -467,13 +529,11 @@ def run_ours(args, rank, world, local, pg):
     pair = summarize_pair(args, res, diffs, nframes, pg)
     clock_info = clocks.stop()
     lrn, jac = pair["learned"], pair["block_jacobi"]
-    # phase breakdown and PCG roofline: a separate profiled pass (per-phase CUDA events)
-    prof_frames = args.steps
-    lp = corrected_run(args, sc, local, flush, pg, "learned", weights, profile=True, frames=prof_frames)
+    # phase breakdown and rooflines: a separate profiled pass (per-phase CUDA events)
+    lp = corrected_run(args, sc, local, flush, pg, "learned", weights, profile=True, frames=args.steps)
     full = None
     if args.full_n > 0:
-        from andosim_b200 import scenes as _sc
-        scf = _sc.c4(seed=rank, n=args.full_n)
+        scf = scenes.c4(seed=rank, n=args.full_n)
         pf = paired_run(args, scf, local, flush, pg, weights, steps=args.full_steps)
         full = {"workload": f"c4_curtains_2x{args.full_n}x{args.full_n}", "frames": args.full_steps,
                 "learned": {k: v for k, v in pf["learned"].items() if k != "total_ms"},
@@ -484,6 +544,7 @@ def run_ours(args, rank, world, local, pg):
     prof, nnzb = lp.pop("_prof"), lp.pop("_nnzb")
     peaks = json.loads(PEAKS_FILE.read_text()) if PEAKS_FILE.exists() else {}
     hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    source = "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback"
     pcg_ms = prof["phase_ms"]["pcg"]
     launches = max(1, prof["phase_launches"]["pcg"])
     pb = pcg_bytes(V, nnzb, prof)
@@ -491,10 +552,20 @@ def run_ours(args, rank, world, local, pg):
     if pcg_ms > 0:
         achieved = pb / (pcg_ms * 1e-3) / 1e9
         roof = {"bound": "hbm", "kernel": "k_pcg_scaled (learned and block-Jacobi launches)", "achieved": round(achieved, 1),
-                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
-                "peak_source": "measured" if peaks else "fallback", "bytes_per_launch": int(pb // launches),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": PCG_TRAFFIC,
+                "peak_source": source, "bytes_per_launch": int(pb // launches),
                 "launches": int(launches), "avg_launch_us": round(pcg_ms * 1e3 / launches, 2),
                 "pcg_iterations": int(prof["pcg_iterations"]), "share_of_frame": round(pcg_ms / max(sum(prof["phase_ms"].values()), 1e-9), 3)}
+    asm_ms = prof["phase_ms"]["assemble"]
+    asm_n = max(1, prof["newton_iterations"])
+    roof_asm = None
+    if asm_ms > 0:
+        ab = assembly_bytes(V, nnzb) * asm_n
+        achieved = ab / (asm_ms * 1e-3) / 1e9
+        roof_asm = {"bound": "hbm", "kernel": "k_diag_factor + k_assemble_scaled_slice (+ k_extra_merge)", "achieved": round(achieved, 1),
+                    "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": ASSEMBLY_TRAFFIC, "peak_source": source,
+                    "bytes_per_newton_iteration": int(assembly_bytes(V, nnzb)), "newton_iterations": int(asm_n),
+                    "avg_us_per_newton_iteration": round(asm_ms * 1e3 / asm_n, 2)}
     ms_l = lrn.pop("total_ms")
     jac.pop("total_ms")
     out = {
@@ -503,12 +574,9 @@ def run_ours(args, rank, world, local, pg):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 BSR/PCG vectors, f64 positions/gradient/dots",
         "data": "synthetic (seeded curtains, scenes.c4)",
         "config": {"workload": WORKLOAD, "vertices": V, "triangles": T, "bsr_blocks": nnzb, "semantics": "CORRECTED",
-                   "preconditioner": "learned", "precond_refresh": args.refresh, "frames_timed_per_gpu": nframes,
-                   "frames": f"{args.warmup}-{args.warmup + args.steps - 1} of seeds "
-                             + ",".join(str(rank + world * k) for k in range(max(args.seeds, 1))),
-                   "frame_window": "the drive moves the pinned rows up to two edge lengths per frame at 256 x 256; from frame ~16 "
-                                   "the first free rows fold onto the pinned rows and the CORRECTED line search stops, so the "
-                                   "timed window ends before that (full_length: a 64 x 64 pair of curtains over 240 frames)",
+                   "preconditioner": "learned", "precond_refresh": args.refresh, "pcg_tol": sc.params["pcg_tol"],
+                   "frames_timed_per_gpu": nframes,
+                   "frames": f"{args.warmup}-{args.warmup + args.steps - 1} of seeds " + ",".join(str(rank + world * k) for k in range(len(scs))),
                    "l2": "flushed before every timed frame", "parallelism": f"replicas x{world}"},
         "pcg_iters_per_newton": lrn["pcg_iters_per_newton"],
         "newton_iters_per_frame": lrn["newton_iters_per_frame"],
@@ -522,72 +590,126 @@ def run_ours(args, rank, world, local, pg):
         "full_length": full,
         "gpu_launches": lrn["gpu_launches"],
         "roofline": roof,
+        "roofline_assembly": roof_asm,
         "clocks": clock_info,
     }
     if args.reference_steps > 0:
         out["reference_semantics"] = reference_semantics_run(args, sc, local, flush, pg)
-    out["e2e"] = e2e_run(args, sc, local, flush, pg, weights)
+    out["e2e"] = e2e_run(args, scs, local, flush, pg, weights)
     if args.c3_frames > 0:
         out["c3_batched"] = c3_run(args, local, seed=rank)
-    return out, sc
+    if args.c2_frames > 0:
+        out["c2_stack"] = c2_run(args, local, pg, seed=rank)
+    return out, sc, weights
 
 
 # ----------------------------------------------------------- CPU baseline
-def oracle_frames(sc, frames, prec="f32", lookup="indexed", semantics="reference"):
-    """Time `frames` oracle steps of scene `sc` (single thread). Returns seconds per frame."""
-    from oracle.build import load
-
-    O = getattr(load(), prec)
+def oracle_state(O, sc, x, v):
+    """Oracle objects for scene `sc` at positions x and velocities v (FP64 arrays)."""
     m = O.Mesh()
     m.initialize(sc.vertices, sc.triangles, O.Material(**sc.material))
     s = O.State()
     s.initialize(m)
+    s.set_positions(x)
+    s.set_velocities(v)
     p = O.SimParams()
-    for k, v in sc.params.items():
-        setattr(p, k, v)
-    secs = 0.0
-    for f in range(frames):
-        c = O.Constraints()
-        for i, t in sc.pins_at(f):
-            c.add_pin(int(i), t)
-        for n, o, g in sc.walls:
-            c.add_wall(n, o, g)
-        s.apply_gravity(sc.gravity, p.dt)
-        t0 = time.perf_counter()
-        if semantics == "reference":
-            O.Integrator.step(m, s, c, p, None, lookup)
-        else:
-            O.Integrator.step(m, s, c, p, None, lookup, "literal", "corrected")
-        secs += time.perf_counter() - t0
-    return secs / frames
+    for k, val in sc.params.items():
+        setattr(p, k, val)
+    return m, s, p
 
 
-def cpu_baseline(sc, frames):
-    """The oracle on one host core, on the headline's semantics (CORRECTED, block Jacobi)."""
-    spf = oracle_frames(sc, frames, semantics="corrected")
-    return {"value": round(1.0 / spf, 4), "unit": "frames/s", "cores": 1, "kind": "port",
-            "sample": f"{frames} frame(s) of {WORKLOAD} ({sc.num_vertices} vertices), CORRECTED semantics, through the "
-                      f"FP32 oracle (C++ restatement, block-Jacobi PCG, one thread)"}
+def oracle_step(O, sc, m, s, p, frame):
+    c = O.Constraints()
+    for i, t in sc.pins_at(frame):
+        c.add_pin(int(i), t)
+    for n, o, g in sc.walls:
+        c.add_wall(n, o, g)
+    s.apply_gravity(sc.gravity, p.dt)
+    t0 = time.perf_counter()
+    st = O.Integrator.step(m, s, c, p, None, "indexed", "literal", "corrected")
+    return time.perf_counter() - t0, st
+
+
+def cpu_baseline(args, sc, local, weights):
+    """CPU baseline and per-frame FP64 error, from the GPU's own state at the first timed frame.
+
+    The GPU runs frames 0..W-1 (learned), then steps frame W from that state with each preconditioner;
+    the oracle steps the same frame from the same state in FP32 (timed: the reference's default
+    Real = float build, CORRECTED semantics, block-Jacobi PCG) and in FP64 (the all-FP64 reference
+    run the position error is quoted against)."""
+    from andosim_b200 import abi
+    from oracle.build import load
+
+    ora = load()
+    S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
+    S.set_precond_weights(weights)
+    pl = abi.make_params(sc.params, semantics="corrected", precond="learned", precond_refresh=args.refresh)
+    pj = abi.make_params(sc.params, semantics="corrected", precond="block_jacobi")
+    W = args.warmup
+    for f in range(W):
+        S.apply_gravity(sc.gravity, pl.dt)
+        S.step(pl, sc.pins_at(f), sc.walls)
+    x0, v0 = S.download()
+    gpu = {}
+    for name, p in (("learned", pl), ("block_jacobi", pj)):
+        S.upload(x0, v0)
+        S.apply_gravity(sc.gravity, p.dt)
+        S.step(p, sc.pins_at(W), sc.walls)
+        gpu[name] = S.download()[0]
+    S.close()
+    m, s, p = oracle_state(ora.f64, sc, x0, v0)
+    sec64, _ = oracle_step(ora.f64, sc, m, s, p, W)
+    x64 = np.asarray(s.get_positions(), dtype=np.float64)
+    m, s, p = oracle_state(ora.f32, sc, x0, v0)
+    sec32, st32 = oracle_step(ora.f32, sc, m, s, p, W)
+    ext = float(np.ptp(sc.vertices, axis=0).max())
+    threads = int(os.environ.get("ANDO_ORACLE_THREADS", "0")) or (os.cpu_count() or 1)
+    base = {"value": round(1.0 / sec32, 4), "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"frame {W} of seed 0 of {WORKLOAD} ({sc.num_vertices} vertices; the first timed frame), stepped by the "
+                      f"FP32 oracle (C++ restatement of the reference, CORRECTED semantics, block-Jacobi PCG) from the GPU's "
+                      f"own state at that frame; sparse products, PCG vector updates, broad-phase queries and "
+                      f"time-of-impact pairs on {threads} threads, the rest on one",
+            "newton_iters": int(st32["newton_iters"]), "substeps": int(st32["substeps"])}
+    err = {"frame": W, "seed": 0, "unit": "max |x_gpu - x_fp64| / extent, one step from the same state",
+           "learned": float(np.abs(gpu["learned"] - x64).max() / ext),
+           "block_jacobi": float(np.abs(gpu["block_jacobi"] - x64).max() / ext), "fp64_oracle_seconds": round(sec64, 2)}
+    return base, err
 
 
 def run_reference(args, rank, world, pg):
-    """The reference's CPU path (oracle port; the reference itself does not build here) on the same workload."""
+    """The reference's CPU path on the same workload and semantics: the oracle (a C++ restatement of the
+    reference; the reference itself does not build here) stepping the curtain workload in CORRECTED
+    semantics with block-Jacobi PCG, seed 0, frames 0..W-1 untimed and frames W.. timed until K frames
+    or the time budget (--reference-budget) is reached; `steps` is the number of frames actually timed.
+    Rank 0 only; the other ranks do no work."""
     if rank != 0:
         return None
     from andosim_b200 import scenes
+    from oracle.build import load
 
+    O = load().f32
     sc = scenes.c4(seed=0, n=args.n)
-    spf = oracle_frames(sc, max(1, min(args.steps, 3)))
-    base = {"value": round(1.0 / spf, 4), "unit": "frames/s", "cores": 1, "kind": "port",
-            "sample": f"{max(1, min(args.steps, 3))} frame(s) of {WORKLOAD} through the FP32 oracle "
-                      "(C++ restatement of the reference, INDEXED block lookup, one thread; the reference "
-                      "is single-threaded)"}
-    return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "frames/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(spf * 1e3, 2), "higher_is_better": True,
+    m, s, p = oracle_state(O, sc, sc.vertices, np.zeros_like(sc.vertices))
+    for f in range(args.warmup):
+        oracle_step(O, sc, m, s, p, f)
+    secs, frames, newton = 0.0, 0, 0
+    while frames < args.steps and (frames == 0 or secs < args.reference_budget):
+        dt, st = oracle_step(O, sc, m, s, p, args.warmup + frames)
+        secs += dt
+        frames += 1
+        newton += st["newton_iters"]
+    threads = int(os.environ.get("ANDO_ORACLE_THREADS", "0")) or (os.cpu_count() or 1)
+    value = round(frames / secs, 4)
+    sample = (f"frames {args.warmup}-{args.warmup + frames - 1} of seed 0 of {WORKLOAD} ({frames} of the {args.steps} asked "
+              f"for fit the {args.reference_budget:.0f} s budget), FP32 oracle, CORRECTED semantics, block-Jacobi PCG; "
+              f"sparse products, PCG updates, queries and time-of-impact pairs on {threads} threads")
+    base = {"value": value, "unit": "frames/s", "cores": threads, "kind": "port", "sample": sample}
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+            "steps": frames, "warmup": args.warmup, "ms_per_step": round(secs * 1e3 / frames, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded curtains, scenes.c4)",
-            "config": {"workload": WORKLOAD, "vertices": sc.num_vertices, "semantics": "REFERENCE"},
-            "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "frames/s", "h2d_bytes_per_step": 0,
-                                          "d2h_bytes_per_step": 0}}
+            "config": {"workload": WORKLOAD, "vertices": sc.num_vertices, "semantics": "CORRECTED", "preconditioner": "block_jacobi",
+                       "frames": f"{args.warmup}-{args.warmup + frames - 1} of seed 0", "newton_iters_per_frame": round(newton / frames, 2)},
+            "cpu_baseline": base, "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
@@ -597,9 +719,9 @@ def main():
         if args.impl == "reference":
             out = run_reference(args, rank, world, pg)
         else:
-            out, sc = run_ours(args, rank, world, local, pg)
+            out, sc, weights = run_ours(args, rank, world, local, pg)
             if rank == 0 and world == 1 and not args.no_cpu_baseline:
-                out["cpu_baseline"] = cpu_baseline(sc, args.cpu_frames)
+                out["cpu_baseline"], out["fp64_step_error"] = cpu_baseline(args, sc, local, weights)
         if rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:

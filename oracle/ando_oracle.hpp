@@ -49,8 +49,35 @@
 #include <unordered_set>
 #include <utility>
 #include <vector>
+#include <cstdlib>
+#include <thread>
 
 namespace ando_oracle {
+
+// Loop over [0, n) on the host's cores (ANDO_ORACLE_THREADS, default all),
+// in static chunks: used only where every index computes and writes its own
+// results, so the outcome is the same bits as one thread's.
+inline int oracle_threads() {
+  static const int t = [] {
+    const char* e = std::getenv("ANDO_ORACLE_THREADS");
+    int v = e ? std::atoi(e) : int(std::thread::hardware_concurrency());
+    return v > 0 ? v : 1;
+  }();
+  return t;
+}
+template <class F> void parallel_for(long long n, F&& f) {
+  const int T = oracle_threads();
+  if (T <= 1 || n < 4096) { for (long long i = 0; i < n; ++i) f(i); return; }
+  const long long chunk = (n + T - 1) / T;
+  std::vector<std::thread> th;
+  for (int k = 0; k < T; ++k) {
+    const long long lo = k * chunk, hi = std::min(n, lo + chunk);
+    if (lo >= hi) break;
+    th.emplace_back([lo, hi, &f] { for (long long i = lo; i < hi; ++i) f(i); });
+  }
+  for (auto& t : th) t.join();
+}
+
 
 enum class Lookup { LITERAL, INDEXED };
 enum class BroadPhase { LITERAL, INTENDED };
@@ -423,7 +450,8 @@ template <class R> struct Csr {
   }
   void multiply(const std::vector<R>& x, std::vector<R>& y) const {
     y.assign(n, R(0));
-    for (Index r = 0; r < n; ++r) { R s = 0; for (Index k = rowptr[r]; k < rowptr[r + 1]; ++k) s += vals[k] * x[cols[k]]; y[r] = s; }
+    // rows on the host's cores; each row sums in the same order
+    parallel_for(n, [&](long long r) { R s = 0; for (Index k = rowptr[r]; k < rowptr[r + 1]; ++k) s += vals[k] * x[cols[k]]; y[size_t(r)] = s; });
   }
   size_t nnz() const { return vals.size(); }
 };
@@ -1151,8 +1179,8 @@ template <class R> PcgResult<R> pcg_solve(const Csr<R>& A, const std::vector<R>&
   auto rel = [&](const std::vector<R>& r) { R ri = linf(r); return binf < R(1e-16) ? ri : ri / binf; };
   auto dot = [](const std::vector<R>& a, const std::vector<R>& c) { R s = 0; for (size_t k = 0; k < a.size(); ++k) s += a[k] * c[k]; return s; };
   auto apply = [&](const std::vector<R>& r, std::vector<R>& z) {
-    for (int i = 0; i < nv; ++i) { V3<R> rb(r[size_t(3 * i)], r[size_t(3 * i + 1)], r[size_t(3 * i + 2)]); V3<R> zb = P[size_t(i)] * rb;
-      z[size_t(3 * i)] = zb.x; z[size_t(3 * i + 1)] = zb.y; z[size_t(3 * i + 2)] = zb.z; }
+    parallel_for(nv, [&](long long i) { V3<R> rb(r[size_t(3 * i)], r[size_t(3 * i + 1)], r[size_t(3 * i + 2)]); V3<R> zb = P[size_t(i)] * rb;
+      z[size_t(3 * i)] = zb.x; z[size_t(3 * i + 1)] = zb.y; z[size_t(3 * i + 2)] = zb.z; });
   };
   std::vector<R> Ax; A.multiply(x, Ax);
   std::vector<R> r(static_cast<size_t>(n)); for (int i = 0; i < n; ++i) r[size_t(i)] = b[size_t(i)] - Ax[size_t(i)];
@@ -1167,12 +1195,12 @@ template <class R> PcgResult<R> pcg_solve(const Csr<R>& A, const std::vector<R>&
     res.iters = it + 1;
     if (std::fabs(pAp) < R(1e-16)) { res.converged = false; return res; }
     R al = rz / pAp;
-    for (int i = 0; i < n; ++i) { x[size_t(i)] += al * p[size_t(i)]; r[size_t(i)] -= al * Ap[size_t(i)]; }
+    parallel_for(n, [&](long long i) { x[size_t(i)] += al * p[size_t(i)]; r[size_t(i)] -= al * Ap[size_t(i)]; });
     res.rel_res = rel(r);
     if (res.rel_res < tol) { res.converged = true; return res; }
     apply(r, z);
     R rzn = dot(r, z); R be = rzn / rz; rz = rzn;
-    for (int i = 0; i < n; ++i) p[size_t(i)] = z[size_t(i)] + be * p[size_t(i)];
+    parallel_for(n, [&](long long i) { p[size_t(i)] = z[size_t(i)] + be * p[size_t(i)]; });
   }
   return res;
 }
@@ -1539,24 +1567,30 @@ template <class R> void candidates(const Mesh<R>& m, const std::vector<V3<R>>& x
   for (auto& b : tb) inflate(b, pad);
   for (auto& b : eb) inflate(b, pad);
   QBVH<R> tq, eq; tq.init(tb); eq.init(eb);
-  for (size_t v = 0; v < x0.size(); ++v) {
-    AABB<R> pbx = point_box(x0[v]);
-    if (x1) pbx.expand(point_box((*x1)[v]));
+  // queries on the host's cores into per-query lists, concatenated in query
+  // order: the same pairs in the same order as one thread finds them
+  const long long nv = (long long)x0.size(), ne = (long long)eb.size();
+  std::vector<std::vector<int>> vt_of(static_cast<size_t>(nv)), ee_of(static_cast<size_t>(ne));
+  parallel_for(nv, [&](long long v) {
+    AABB<R> pbx = point_box(x0[size_t(v)]);
+    if (x1) pbx.expand(point_box((*x1)[size_t(v)]));
     inflate(pbx, pad);
     tq.query(pbx, tb, [&](int t) {
       const auto& tri = m.triangles[size_t(t)];
       if (tri.v[0] == int(v) || tri.v[1] == int(v) || tri.v[2] == int(v)) return;
-      vt.push_back({int(v), t});
+      vt_of[size_t(v)].push_back(t);
     });
-  }
-  for (size_t a = 0; a < eb.size(); ++a) {
-    eq.query(eb[a], eb, [&](int b) {
+  });
+  parallel_for(ne, [&](long long a) {
+    eq.query(eb[size_t(a)], eb, [&](int b) {
       if (int(a) >= b) return;
-      const Edge &e1 = m.edges[a], &e2 = m.edges[size_t(b)];
+      const Edge &e1 = m.edges[size_t(a)], &e2 = m.edges[size_t(b)];
       if (e1.v[0] == e2.v[0] || e1.v[0] == e2.v[1] || e1.v[1] == e2.v[0] || e1.v[1] == e2.v[1]) return;
-      ee.push_back({int(a), b});
+      ee_of[size_t(a)].push_back(b);
     });
-  }
+  });
+  for (long long v = 0; v < nv; ++v) for (int t : vt_of[size_t(v)]) vt.push_back({int(v), t});
+  for (long long a = 0; a < ne; ++a) for (int b : ee_of[size_t(a)]) ee.push_back({int(a), b});
   std::sort(vt.begin(), vt.end()); std::sort(ee.begin(), ee.end());
 }
 
@@ -1849,14 +1883,15 @@ template <class R> class CorrectedIntegrator {
     // always solved: with the gradient test alone, a scene whose forces all lie
     // below pcg_tol (a light cloth starting to fall) would never move.
     bool solve_first = true;
+    const Csr<R> H_el = base_elastic(mesh);  // constant: built once per step
     while (beta < p.beta_max && bi < 20) {
-      R alpha = inner_newton(mesh, st, x_target, fixed, C, p, rigids, S, solve_first);
+      R alpha = inner_newton(mesh, st, x_target, fixed, C, p, rigids, S, solve_first, H_el);
       solve_first = false;
       beta = R(double(beta) + (1.0 - double(beta)) * double(alpha));
       ++bi;
       if (alpha < R(1e-6)) { S.line_search_fail++; break; }
     }
-    if (beta > R(1e-6)) inner_newton(mesh, st, x_target, fixed, C, p, rigids, S, false);
+    if (beta > R(1e-6)) inner_newton(mesh, st, x_target, fixed, C, p, rigids, S, false, H_el);
     S.beta = beta;
     // v = (x - x_old) / dt: dividing by beta dt (the reference) turns the
     // error-reduction pass of a step whose line search held beta near zero
@@ -2043,35 +2078,55 @@ template <class R> class CorrectedIntegrator {
     // additive CCD: the distance depends on the relative motion only, so the
     // rate bound comes from the displacements minus the pair's mean
     auto Lrel = [&](int i, const V3<R>& mean) { return (ext[size_t(i)] - mean).norm(); };
-    for (auto& pr : vt) {
+    // pairs on the host's cores, each pair's time of impact computed as one
+    // thread computes it; the minimum (and the trace) taken in pair order
+    auto pt_pair = [&](size_t k, R* d0_out) {
+      const auto& pr = vt[k];
       const auto& tri = mesh.triangles[size_t(pr.second)];
       int v = pr.first, a = tri.v[0], b = tri.v[1], c = tri.v[2];
       V3<R> mean = (ext[size_t(v)] + ext[size_t(a)] + ext[size_t(b)] + ext[size_t(c)]) * R(0.25);
       R l = Lrel(v, mean) + std::max(Lrel(a, mean), std::max(Lrel(b, mean), Lrel(c, mean)));
       auto dist = [&](R s) { R d; V3<R> nm, wp, wq; narrow_pt(x[size_t(v)] + ext[size_t(v)] * s, x[size_t(a)] + ext[size_t(a)] * s,
                                                               x[size_t(b)] + ext[size_t(b)] * s, x[size_t(c)] + ext[size_t(c)] * s, d, nm, wp, wq); return d; };
-      R tp = advance_toi<R>(dist, l, eta_min, near);
-      auto& tr = NewtonTrace::get();
-      if (tr.enabled) {
-        if (tp < R(0.5)) tr.cur.below_half++;
-        if (tp < t) { tr.cur.kind = 0; tr.cur.ids[0] = v; tr.cur.ids[1] = a; tr.cur.ids[2] = b; tr.cur.ids[3] = c; tr.cur.d0 = double(dist(R(0))); tr.cur.l = double(l); tr.cur.t = double(tp); }
-      }
-      t = std::min(t, tp);
-    }
-    for (auto& pr : ee) {
+      if (d0_out) *d0_out = dist(R(0));
+      return std::make_pair(advance_toi<R>(dist, l, eta_min, near), l);
+    };
+    auto ee_pair = [&](size_t k, R* d0_out) {
+      const auto& pr = ee[k];
       const Edge &e1 = mesh.edges[size_t(pr.first)], &e2 = mesh.edges[size_t(pr.second)];
       int a = e1.v[0], b = e1.v[1], c = e2.v[0], d = e2.v[1];
       V3<R> mean = (ext[size_t(a)] + ext[size_t(b)] + ext[size_t(c)] + ext[size_t(d)]) * R(0.25);
       R l = std::max(Lrel(a, mean), Lrel(b, mean)) + std::max(Lrel(c, mean), Lrel(d, mean));
       auto dist = [&](R s) { R dd; V3<R> nm, wp, wq; narrow_ee(x[size_t(a)] + ext[size_t(a)] * s, x[size_t(b)] + ext[size_t(b)] * s,
                                                                x[size_t(c)] + ext[size_t(c)] * s, x[size_t(d)] + ext[size_t(d)] * s, dd, nm, wp, wq); return dd; };
-      R tp = advance_toi<R>(dist, l, eta_min, near);
-      auto& tr = NewtonTrace::get();
-      if (tr.enabled) {
-        if (tp < R(0.5)) tr.cur.below_half++;
-        if (tp < t) { tr.cur.kind = 1; tr.cur.ids[0] = a; tr.cur.ids[1] = b; tr.cur.ids[2] = c; tr.cur.ids[3] = d; tr.cur.d0 = double(dist(R(0))); tr.cur.l = double(l); tr.cur.t = double(tp); }
+      if (d0_out) *d0_out = dist(R(0));
+      return std::make_pair(advance_toi<R>(dist, l, eta_min, near), l);
+    };
+    std::vector<R> tvt(vt.size()), tee(ee.size());
+    parallel_for((long long)vt.size(), [&](long long k) { tvt[size_t(k)] = pt_pair(size_t(k), nullptr).first; });
+    parallel_for((long long)ee.size(), [&](long long k) { tee[size_t(k)] = ee_pair(size_t(k), nullptr).first; });
+    auto& trace = NewtonTrace::get();
+    for (int kind = 0; kind < 2; ++kind) {
+      const std::vector<R>& tv = kind == 0 ? tvt : tee;
+      for (size_t k = 0; k < tv.size(); ++k) {
+        R tp = tv[k];
+        if (trace.enabled) {
+          if (tp < R(0.5)) trace.cur.below_half++;
+          if (tp < t) {
+            R d0 = 0;
+            auto res = kind == 0 ? pt_pair(k, &d0) : ee_pair(k, &d0);
+            trace.cur.kind = kind; trace.cur.d0 = double(d0); trace.cur.l = double(res.second); trace.cur.t = double(tp);
+            if (kind == 0) {
+              const auto& tri = mesh.triangles[size_t(vt[k].second)];
+              trace.cur.ids[0] = vt[k].first; trace.cur.ids[1] = tri.v[0]; trace.cur.ids[2] = tri.v[1]; trace.cur.ids[3] = tri.v[2];
+            } else {
+              const Edge &e1 = mesh.edges[size_t(ee[k].first)], &e2 = mesh.edges[size_t(ee[k].second)];
+              trace.cur.ids[0] = e1.v[0]; trace.cur.ids[1] = e1.v[1]; trace.cur.ids[2] = e2.v[0]; trace.cur.ids[3] = e2.v[1];
+            }
+          }
+        }
+        t = std::min(t, tp);
       }
-      t = std::min(t, tp);
     }
     if (rigids) {
       for (const auto& body : *rigids) {
@@ -2100,9 +2155,9 @@ template <class R> class CorrectedIntegrator {
   }
 
   static R inner_newton(const Mesh<R>& mesh, State<R>& st, const std::vector<V3<R>>& x_target, const std::vector<char>& fixed,
-                        Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>& S, bool solve_first) {
+                        Constraints<R>& C, const SimParams<R>& p, std::vector<RigidBody<R>>* rigids, StepStats<R>& S, bool solve_first,
+                        const Csr<R>& H_el) {
     const size_t n = st.positions.size();
-    Csr<R> H_el = base_elastic(mesh);
     const R lmax = max_move(mesh);
     for (int it = 0; it < p.max_newton_steps; ++it) {
       auto contacts = detect_corrected(mesh, st.positions, rigids, p.contact_gap_max);

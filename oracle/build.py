@@ -28,7 +28,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     import pybind11
 
     cmd = [
-        os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+        os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden", "-pthread",
         f"-I{pybind11.get_include()}", f"-I{sysconfig.get_paths()['include']}", f"-I{HERE}",
         str(HERE / "oracle_py.cpp"), "-o", str(out) + ".tmp",
     ]
