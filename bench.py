@@ -184,9 +184,11 @@ def assembly_bytes(V, nnzb):
     return 144 * V + 88 * nnzb
 
 
-# DRAM bytes per launch from one ncu capture of the kernel (None: not captured for this build)
-PCG_TRAFFIC = None
-ASSEMBLY_TRAFFIC = None
+# DRAM bytes (read + write) per launch of the kernel on this workload, from one ncu capture (the summaries
+# under profiles/ give the command): the PCG's matrix and vectors come from DRAM once per launch and from L2
+# for every later iteration; the assembly's figure is k_assemble_scaled_slice alone.
+PCG_TRAFFIC = 45_572_352
+ASSEMBLY_TRAFFIC = 82_325_760
 
 
 class Timer:
