@@ -27,7 +27,7 @@ EXPORTED = [
     "ando_apply_gravity", "ando_step", "ando_compute_contacts", "ando_compute_contacts_corrected", "ando_last_system",
     "ando_eval_system",
     "ando_last_gradient", "ando_last_contact_blocks", "ando_profile_enable", "ando_profile_read", "ando_ctx_stream",
-    "ando_broad_phase", "ando_pcg_solve_noalloc",
+    "ando_broad_phase", "ando_pcg_solve_noalloc", "ando_ctx_keep_system",
 ]
 
 PHASES = ["setup", "strain", "gradient", "assemble", "pcg", "line_search", "finish", "precond"]
@@ -161,6 +161,7 @@ def lib() -> C.CDLL:
     L.ando_ctx_select_assembly_tpb.restype = I32; L.ando_ctx_select_assembly_tpb.argtypes = [P, I32]
     L.ando_ctx_assembly_tpb.restype = I32; L.ando_ctx_assembly_tpb.argtypes = [P, pi, pi]
     L.ando_ctx_set_pair_capacity.restype = I32; L.ando_ctx_set_pair_capacity.argtypes = [P, I32]
+    L.ando_ctx_keep_system.restype = I32; L.ando_ctx_keep_system.argtypes = [P, I32]
     L.ando_ctx_set_refit_top_capacity.restype = I32; L.ando_ctx_set_refit_top_capacity.argtypes = [P, I32]
     L.ando_ctx_pcg_shape.restype = I32; L.ando_ctx_pcg_shape.argtypes = [P, I32, pi, pi, pd]
     L.ando_broad_phase.restype = I32; L.ando_broad_phase.argtypes = [P, I32, D, pi, I32, pi]
@@ -344,6 +345,16 @@ class Scene:
         g = np.empty(3 * self.V)
         _check(lib().ando_last_gradient(self.ctx, _dptr(g), self.V), "ando_last_gradient")
         return g
+
+    def keep_system(self, keep: bool = True):
+        """CORRECTED steps also keep the unscaled system for last_system (off by default)."""
+        _check(lib().ando_ctx_keep_system(self.ctx, int(bool(keep))), "ando_ctx_keep_system")
+
+    def system_size(self) -> Tuple[int, int]:
+        """(block rows, static block slots) of the mesh's system."""
+        V = C.c_int32(); nnzb = C.c_int32()
+        _check(lib().ando_last_system(self.ctx, C.byref(V), C.byref(nnzb), None, None, None, None, None), "ando_last_system")
+        return V.value, nnzb.value
 
     def last_system(self):
         V = C.c_int32(); nnzb = C.c_int32()

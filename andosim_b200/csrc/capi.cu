@@ -96,7 +96,11 @@ struct ando_ctx_s {
   double gap_max = 1e-3;           // contact activation distance of the current step
 
   // SELL-32 copy of the static pattern for the scaled PCG (pcg.cu)
-  DevBuf<int> chunk_off, sell_col, sell_base;
+  DevBuf<int> chunk_off, sell_col, sell_base, sell_slot;   // sell_slot: SELL position -> CSR slot (-1 padding)
+  DevBuf<double> el_sell;          // CORRECTED elastic coefficient per SELL position
+  bool keep_system = false;        // CORRECTED: also write the unscaled blocks (ando_last_system)
+  bool write_val = false, write_valh = false;   // this assembly writes the CSR-ordered copies
+  bool val_valid = false;          // val holds the last assembled system's unscaled blocks
   int sell_wmax = 0;              // column slots of the widest SELL-32 slice
   DevBuf<float> valh_sell, S_coef, S_diag;   // S_coef / S_diag: the learned S in the PCG's form
   bool Sval_stale = false;                   // slot-major S not written by the steps since
@@ -695,8 +699,9 @@ void enqueue_scaled_assembly_tpb(ando_ctx c, const StepParams& sp, cudaStream_t 
   c->dt2inv = sp.dt2inv;
   launch_diag_factor(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->g.p, c->Linv.p, c->Lf.p, c->bhat.p,
                      c->chol_ok.p, c->ctrl.p, s, tpb);
-  launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p, c->val.p,
-                         c->valh.p, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s, tpb, c->chunk_off.p, c->sell_wmax);
+  launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p,
+                         c->write_val ? c->val.p : nullptr, c->write_valh ? c->valh.p : nullptr, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s,
+                         tpb, c->sell_slot.p, c->el_sell.p, c->sell_col.p, c->sell_blocks);
 }
 
 void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
@@ -890,6 +895,8 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
     if (c->ctrl_host->converged) { ret = 1.0; return ANDO_OK; }
     {
       Phase ph(c, ANDO_PHASE_ASSEMBLE);
+      c->write_val = c->keep_system;                       // unscaled copy only for ando_last_system
+      c->write_valh = p.precond == ANDO_PRECOND_LEARNED;   // CSR-ordered scaled copy: the network's features
       enqueue_scaled_assembly(c, sp, s);
       ph.launched(c->nx ? 3 : 2);
     }
@@ -1110,7 +1117,8 @@ int upload_constraints(ando_ctx c, const ando_params& p, const ando_pin* pins, i
   if (c->el_semantics != p.semantics) {
     Phase ph(c, ANDO_PHASE_SETUP);
     launch_elastic_slots(c->mesh_dev(), c->mu, c->thickness, p.semantics, c->el_a.p, c->el_b.p, s);
-    ph.launched();
+    launch_el_sell(c->sell_slot.p, c->el_b.p, c->sell_blocks, c->el_sell.p, s);
+    ph.launched(2);
     c->el_semantics = p.semantics;
   }
   std::vector<int> order;
@@ -1347,12 +1355,14 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     choff[ch + 1] = choff[ch] + 32 * w;
   }
   std::vector<int> scol(choff[nch], -1), sbase(nnzb);
+  std::vector<int> sslot(scol.size(), -1);
   for (int r = 0; r < V; ++r) {
     int ch = r >> 5, l = r & 31;
     for (int k = 0; k < rowptr[r + 1] - rowptr[r]; ++k) {
       int slot = choff[ch] + 32 * k;
       scol[slot + l] = cols[rowptr[r] + k];
       sbase[rowptr[r] + k] = 9 * slot + l;
+      sslot[slot + l] = rowptr[r] + k;
     }
   }
   cudaStream_t s = c->stream;
@@ -1377,6 +1387,8 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->chunk_off.upload(choff.data(), nch + 1, s));
   CK(c->sell_col.upload(scol.data(), choff[nch], s));
   CK(c->sell_base.upload(sbase.data(), nnzb, s));
+  CK(c->sell_slot.upload(sslot.data(), choff[nch], s));
+  CK(c->el_sell.reserve(choff[nch]));
   CK(c->valh_sell.reserve(9ull * choff[nch]));
   CK(c->face_slot.upload(face_slot.data(), 9ull * T, s));
   CK(c->slot_cptr.upload(cptr.data(), nnzb + 1, s));
@@ -1555,6 +1567,7 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
   if (rc) return rc;
   c->gap_max = p.contact_gap_max;
   c->bvh_epoch++;
+  c->val_valid = p.semantics == ANDO_SEMANTICS_REFERENCE || c->keep_system;
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
     rc = restore_start(c);
     if (rc) return rc;
@@ -1676,6 +1689,7 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   cudaStream_t s = c->stream;
   c->gap_max = p.contact_gap_max;
   c->bvh_epoch++;
+  c->val_valid = true;   // both semantics assemble the unscaled values here
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
     rc = restore_start(c);
     if (rc) return rc;
@@ -1687,7 +1701,9 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
     rc = corrected_gradient(c, p, sp, num_rigids);
     c->solve_first = false;
     if (rc) return rc;
+    c->write_val = c->write_valh = true;   // the system is read back (tests, training data)
     enqueue_scaled_assembly(c, sp, s);
+    c->val_valid = true;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
     return ANDO_OK;
@@ -1772,6 +1788,8 @@ int32_t ando_last_system(ando_ctx c, int32_t* V, int32_t* nnzb, int32_t* rowptr,
   cudaStream_t s = c->stream;
   if (rowptr) CK(cudaMemcpyAsync(rowptr, c->rowptr.p, sizeof(int) * (c->V + 1), cudaMemcpyDeviceToHost, s));
   if (cols) CK(cudaMemcpyAsync(cols, c->cols.p, sizeof(int) * c->nnzb, cudaMemcpyDeviceToHost, s));
+  if (vals && !c->val_valid)
+    return fail(ANDO_ERR_STATE, "the last CORRECTED step kept no unscaled system: call ando_ctx_keep_system(ctx, 1) before stepping");
   if (vals) CK(cudaMemcpyAsync(vals, c->val.p, sizeof(float) * 9ull * c->nnzb, cudaMemcpyDeviceToHost, s));
   if (rhs) CK(cudaMemcpyAsync(rhs, c->b.p, sizeof(float) * 3ull * c->V, cudaMemcpyDeviceToHost, s));
   if (sol) CK(cudaMemcpyAsync(sol, c->d.p, sizeof(float) * 3ull * c->V, cudaMemcpyDeviceToHost, s));
@@ -1942,6 +1960,13 @@ int32_t ando_ctx_assembly_tpb(ando_ctx c, int32_t* count, int32_t* tpb) {
   if (rc) return rc;
   if (count) *count = 3;
   if (tpb) *tpb = c->mesh_ready && c->asm_V == c->V ? c->asm_tpb : 0;
+  return ANDO_OK;
+}
+
+int32_t ando_ctx_keep_system(ando_ctx c, int32_t keep) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  c->keep_system = keep != 0;
   return ANDO_OK;
 }
 

@@ -330,6 +330,14 @@ ANDO_API int32_t ando_ctx_set_refit_top_capacity(ando_ctx ctx, int32_t nodes);
 ANDO_API int32_t ando_ctx_select_assembly_tpb(ando_ctx ctx, int32_t index);
 ANDO_API int32_t ando_ctx_assembly_tpb(ando_ctx ctx, int32_t* count, int32_t* tpb);
 
+/* CORRECTED steps assemble the block-scaled system the PCG solves and, by
+ * default, not the unscaled block values: ando_last_system then has no values
+ * to return for a CORRECTED step and fails with ANDO_ERR_STATE. keep != 0 makes
+ * every CORRECTED Newton iteration also write them (36 bytes per block), so
+ * ando_last_system returns the last system solved. ando_eval_system always
+ * writes them. No reference counterpart. */
+ANDO_API int32_t ando_ctx_keep_system(ando_ctx ctx, int32_t keep);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
  * callers that time or order work around the library's. */
 ANDO_API int32_t ando_ctx_stream(ando_ctx ctx, void** stream);

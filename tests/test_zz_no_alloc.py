@@ -24,6 +24,7 @@ def last_newton_system(abi, tol):
     sc = scenes.c1(n=16)
     p = abi.make_params(dict(sc.params, pcg_tol=tol), semantics="corrected")
     S = abi.Scene(sc.vertices, sc.triangles, sc.material)
+    S.keep_system()                    # the step also keeps the unscaled system it solves
     S.upload(sc.vertices, np.zeros_like(sc.vertices), sc.vertices, None)
     S.apply_gravity(sc.gravity, p.dt)
     st = S.step(p, sc.pins, sc.walls)
