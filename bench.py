@@ -3,16 +3,21 @@
 
 Workload: two 2 m x 2 m curtains of 256 x 256 vertices (131,072 vertices,
 260,100 triangles), 3 mm apart, top rows pinned and driven +-0.3 m along x at
-0.5 Hz in opposite phase, ground plane at z = 0 (synthetic, seeded). One bench
-step = one frame: State.apply_gravity + Integrator.step, as the reference
-demos drive it.
+0.5 Hz in opposite phase, ground plane at z = 0, Newton/PCG tolerance 1e-4
+(synthetic, seeded). One bench step = one frame: State.apply_gravity +
+Integrator.step, as the reference demos drive it.
 
 Headline (`value`): frames/s of the CORRECTED step (the step the reference
-intends: elasticity on the current positions, kinematic pins, working self
-contact, time-of-impact line search) with the learned preconditioner, next to
-the same frames with block-Jacobi PCG (`jacobi`), with PCG iterations per
-Newton step for both. `reference_semantics` times the reference's own step
-(REFERENCE semantics, block Jacobi, whole frame as one CUDA graph).
+intends: as-rigid-as-possible membrane forces on the current positions, pins
+as springs of the implicit solve, contact stiffness from the current gap,
+working self contact, conservative time-of-impact line search, sub-steps for
+fast drives) with the learned preconditioner, next to the same frames with
+block-Jacobi PCG (`jacobi`, each frame stepped from the same state), with PCG
+iterations per Newton step for both. `reference_semantics` times the
+reference's own step (REFERENCE semantics, block Jacobi, whole frame as one
+CUDA graph); `cpu_baseline` and `fp64_step_error` step the oracle from the
+GPU's state at the first timed frame; `--impl reference` runs the oracle on
+the same workload, semantics and frames.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
