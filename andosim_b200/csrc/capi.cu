@@ -96,8 +96,7 @@ struct ando_ctx_s {
   double gap_max = 1e-3;           // contact activation distance of the current step
 
   // SELL-32 copy of the static pattern for the scaled PCG (pcg.cu)
-  DevBuf<int> chunk_off, sell_col, sell_base, sell_slot;   // sell_slot: SELL position -> CSR slot (-1 padding)
-  DevBuf<double> el_sell;          // CORRECTED elastic coefficient per SELL position
+  DevBuf<int> chunk_off, sell_col, sell_base;
   bool keep_system = false;        // CORRECTED: also write the unscaled blocks (ando_last_system)
   bool write_val = false, write_valh = false;   // this assembly writes the CSR-ordered copies
   bool val_valid = false;          // val holds the last assembled system's unscaled blocks
@@ -701,7 +700,7 @@ void enqueue_scaled_assembly_tpb(ando_ctx c, const StepParams& sp, cudaStream_t 
                      c->chol_ok.p, c->ctrl.p, s, tpb);
   launch_assemble_scaled(m, c->sflags.p, c->sv.p, c->diag_extra.p, sp.enable_strain, c->fixed.p, c->Linv.p, c->chol_ok.p,
                          c->write_val ? c->val.p : nullptr, c->write_valh ? c->valh.p : nullptr, c->sell_base.p, c->valh_sell.p, c->ctrl.p, s,
-                         tpb, c->sell_slot.p, c->el_sell.p, c->sell_col.p, c->sell_blocks);
+                         tpb, c->chunk_off.p, c->sell_wmax);
 }
 
 void enqueue_scaled_assembly(ando_ctx c, const StepParams& sp, cudaStream_t s) {
@@ -1117,8 +1116,7 @@ int upload_constraints(ando_ctx c, const ando_params& p, const ando_pin* pins, i
   if (c->el_semantics != p.semantics) {
     Phase ph(c, ANDO_PHASE_SETUP);
     launch_elastic_slots(c->mesh_dev(), c->mu, c->thickness, p.semantics, c->el_a.p, c->el_b.p, s);
-    launch_el_sell(c->sell_slot.p, c->el_b.p, c->sell_blocks, c->el_sell.p, s);
-    ph.launched(2);
+    ph.launched();
     c->el_semantics = p.semantics;
   }
   std::vector<int> order;
@@ -1355,14 +1353,12 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     choff[ch + 1] = choff[ch] + 32 * w;
   }
   std::vector<int> scol(choff[nch], -1), sbase(nnzb);
-  std::vector<int> sslot(scol.size(), -1);
   for (int r = 0; r < V; ++r) {
     int ch = r >> 5, l = r & 31;
     for (int k = 0; k < rowptr[r + 1] - rowptr[r]; ++k) {
       int slot = choff[ch] + 32 * k;
       scol[slot + l] = cols[rowptr[r] + k];
       sbase[rowptr[r] + k] = 9 * slot + l;
-      sslot[slot + l] = rowptr[r] + k;
     }
   }
   cudaStream_t s = c->stream;
@@ -1387,8 +1383,6 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->chunk_off.upload(choff.data(), nch + 1, s));
   CK(c->sell_col.upload(scol.data(), choff[nch], s));
   CK(c->sell_base.upload(sbase.data(), nnzb, s));
-  CK(c->sell_slot.upload(sslot.data(), choff[nch], s));
-  CK(c->el_sell.reserve(choff[nch]));
   CK(c->valh_sell.reserve(9ull * choff[nch]));
   CK(c->face_slot.upload(face_slot.data(), 9ull * T, s));
   CK(c->slot_cptr.upload(cptr.data(), nnzb + 1, s));

@@ -897,74 +897,51 @@ __global__ void k_assemble_scaled(MeshDev m, const unsigned char* sflags, const 
   for (int k = 0; k < 9; ++k) vs[32 * k] = R[k];
 }
 
-// The same values straight into the SELL-32 copy the PCG reads: one warp per
-// column slot of a slice (32 consecutive SELL positions, one row each), so
-// every one of the block's nine value stores is one coalesced 128-byte line.
-// The elastic constant comes in SELL order (el_sell, the FP64 value of the
-// slot's constant block), the row's factor from the lane's row and the
-// column's factor by gather. The CSR-ordered copies are written only when a
-// caller needs them: the scaled one for the learned preconditioner's
-// features, the unscaled one for ando_last_system.
-__global__ void k_assemble_sell(MeshDev m, const int* sell_slot, const double* el_sell, const int* sell_col, int npos,
-                                const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
-                                const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                                float* valh_sell, const Ctrl* ctrl) {
+// The same values, one CTA per 32-row SELL slice: the slice's SELL region
+// (contiguous, 9 x 32 floats per column slot) and, when asked for, its CSR
+// slots' scaled and unscaled blocks (contiguous) are staged in shared memory
+// and written with coalesced stores; the SELL padding gets zeros. wmax = the
+// widest slice (column slots). The CSR-ordered copies are written only when
+// a caller reads them (valh: the learned preconditioner's features; val:
+// ando_last_system), and only their staging space is requested.
+__global__ void __launch_bounds__(ASM_SLICE_TPB) k_assemble_scaled_slice(MeshDev m, const unsigned char* sflags, const StrainSV* sv,
+                                                                         const double* diag_extra, int enable_strain,
+                                                                         const unsigned char* fixed, const double* Linv,
+                                                                         const unsigned char* chol_ok, float* val, float* valh,
+                                                                         const int* sell_base, const int* chunk_off, int wmax,
+                                                                         float* valh_sell, const Ctrl* ctrl) {
   if (ctrl->converged) return;
-  const long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (pos >= npos) return;
-  const int s = sell_slot[pos];
-  if (s < 0) return;  // padding: the PCG skips it (its column is -1)
-  const int row = m.slot_row[s], col = sell_col[pos];
-  float R[9], Hf[9];
-  if (fixed && (fixed[row] || fixed[col])) {
-    float one = row == col ? 1.f : 0.f;
-    for (int k = 0; k < 9; ++k) { R[k] = (k % 4 == 0) ? one : 0.f; Hf[k] = R[k]; }
-  } else {
-    double H[9];
-    for (int k = 0; k < 9; ++k) H[k] = 0.0;
-    const double el = el_sell[pos];
-    H[0] = H[4] = H[8] = el;
-    if (enable_strain) {
-      for (int k = m.slot_cptr[s]; k < m.slot_cptr[s + 1]; ++k) {
-        int e = m.slot_contrib[k];
-        int f = e / 9, a = (e % 9) / 3, bb = e % 3;
-        unsigned char fl = sflags[f];
-        if (!fl) continue;
-        for (int q = 0; q < 2; ++q) {
-          if (!(fl & (1u << q))) continue;
-          const StrainSV& S = sv[2 * f + q];
-          if (fabs(S.d2V) < 1e-12) continue;
-          double blk[9], mx = 0.0;
-          for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c) { blk[3 * r + c] = S.d2V * (S.J[3 * a + r] * S.J[3 * bb + c]); mx = fmax(mx, fabs(blk[3 * r + c])); }
-          if (mx < 1e-12) continue;
-          for (int k2 = 0; k2 < 9; ++k2) if (fabs(blk[k2]) >= 1e-12) H[k2] += blk[k2];
-        }
-      }
-    }
-    if (row == col) for (int k = 0; k < 9; ++k) H[k] += diag_extra[9 * row + k];
-    for (int k = 0; k < 9; ++k) Hf[k] = float(H[k]);
-    if (row == col && chol_ok[row]) {
-      for (int k = 0; k < 9; ++k) R[k] = (k % 4 == 0) ? 1.f : 0.f;
-    } else {
-      double Rd[9];
-      scale_block(ld_tri(Linv, row), H, ld_tri(Linv, col), Rd);
-      for (int k = 0; k < 9; ++k) R[k] = float(Rd[k]);
-    }
+  extern __shared__ float asm_sm[];
+  const int ch = blockIdx.x;
+  const int r0 = 32 * ch, r1 = min(m.V, r0 + 32);
+  const int k0 = m.rowptr[r0], nk = m.rowptr[r1] - k0;
+  const int sell0 = 9 * chunk_off[ch], nsell = 9 * (chunk_off[ch + 1] - chunk_off[ch]);
+  float* ss = asm_sm;                               // nsell: SELL order
+  float* cs = valh ? ss + 9 * 32 * wmax : nullptr;  // 9 nk: scaled blocks, CSR order
+  float* cv = val ? ss + 9 * 32 * wmax * (valh ? 2 : 1) : nullptr;  // 9 nk: unscaled blocks, CSR order
+  for (int q = threadIdx.x; q < nsell; q += ASM_SLICE_TPB) ss[q] = 0.f;
+  const int strain_on = enable_strain && ctrl->strain_active > 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < nk; t += ASM_SLICE_TPB) {
+    const int s = k0 + t;
+    float R[9], Hf[9];
+    scaled_slot(m, s, sflags, sv, diag_extra, strain_on, fixed, Linv, chol_ok, R, Hf);
+    const int sp = sell_base[s] - sell0;
+    for (int k = 0; k < 9; ++k) ss[sp + 32 * k] = R[k];
+    if (cs) for (int k = 0; k < 9; ++k) cs[9 * t + k] = R[k];
+    if (cv) for (int k = 0; k < 9; ++k) cv[9 * t + k] = Hf[k];
   }
-  float* vs = valh_sell + 9 * (pos - (pos & 31)) + (pos & 31);
-  for (int k = 0; k < 9; ++k) vs[32 * k] = R[k];
-  if (valh) for (int k = 0; k < 9; ++k) valh[9ll * s + k] = R[k];
-  if (val) for (int k = 0; k < 9; ++k) val[9ll * s + k] = Hf[k];
-}
-
-// el_sell[pos] = the constant elastic coefficient of the slot at SELL position
-// pos (CORRECTED blocks are c I3, so el_a = el_b); padding keeps 0.
-__global__ void k_el_sell(const int* sell_slot, const double* el_b, int npos, double* el_sell) {
-  const long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (pos >= npos) return;
-  const int s = sell_slot[pos];
-  el_sell[pos] = s < 0 ? 0.0 : el_b[s];
+  __syncthreads();
+  if (cs) {
+    float* vh = valh + 9ll * k0;
+    for (int q = threadIdx.x; q < 9 * nk; q += ASM_SLICE_TPB) vh[q] = cs[q];
+  }
+  if (cv) {
+    float* vv = val + 9ll * k0;
+    for (int q = threadIdx.x; q < 9 * nk; q += ASM_SLICE_TPB) vv[q] = cv[q];
+  }
+  float* vs = valh_sell + sell0;
+  for (int q = threadIdx.x; q < nsell; q += ASM_SLICE_TPB) vs[q] = ss[q];
 }
 
 // Contact blocks outside the static pattern. Entries of the same (row, col)
@@ -1393,19 +1370,27 @@ void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const Str
 }
 void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                             const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
-                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s, int tpb, const int* sell_slot,
-                            const double* el_sell, const int* sell_col, int npos) {
+                            const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s, int tpb, const int* chunk_off,
+                            int wmax) {
   if (!m.nnzb) return;
-  if (sell_slot && el_sell && sell_col && npos > 0) {
-    k_assemble_sell<<<nblk(npos, tpb), tpb, 0, s>>>(m, sell_slot, el_sell, sell_col, npos, sflags, sv, diag_extra, enable_strain, fixed, Linv,
-                                                   chol_ok, val, valh, valh_sell, ctrl);
-    return;
+  if (chunk_off && wmax > 0 && wmax <= ASM_SLICE_WMAX) {
+    static std::atomic<unsigned> attr{0};  // one bit per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(attr.load() & (1u << dev))) {
+      if (cudaFuncSetAttribute(k_assemble_scaled_slice, cudaFuncAttributeMaxDynamicSharedMemorySize, int(asm_slice_smem(ASM_SLICE_WMAX, 3))) ==
+          cudaSuccess)
+        attr.fetch_or(1u << dev);
+    }
+    if (dev < 32 && (attr.load() & (1u << dev))) {
+      const int copies = 1 + (valh ? 1 : 0) + (val ? 1 : 0);
+      k_assemble_scaled_slice<<<(m.V + 31) / 32, ASM_SLICE_TPB, asm_slice_smem(wmax, copies), s>>>(
+          m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh, sell_base, chunk_off, wmax, valh_sell, ctrl);
+      return;
+    }
   }
   k_assemble_scaled<<<nblk(m.nnzb, tpb), tpb, 0, s>>>(m, sflags, sv, diag_extra, enable_strain, fixed, Linv, chol_ok, val, valh, sell_base,
                                                       valh_sell, ctrl);
-}
-void launch_el_sell(const int* sell_slot, const double* el_b, int npos, double* el_sell, cudaStream_t s) {
-  if (npos) k_el_sell<<<nblk(npos), TPB, 0, s>>>(sell_slot, el_b, npos, el_sell);
 }
 void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s) {
   if (n) k_extra_key64<<<nblk(n), TPB, 0, s>>>(xent, xkeys, n, key, idx);

@@ -50,17 +50,18 @@ void launch_assemble(const MeshDev& m, const unsigned char* sflags, const Strain
 void launch_diag_factor(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                         const unsigned char* fixed, const double* g, double* Linv, float* Lf, float* bhat, unsigned char* chol_ok,
                         const Ctrl* ctrl, cudaStream_t s, int tpb = 256);
-// With the SELL-32 position -> slot map (sell_slot, -1 for padding), the
-// constant elastic coefficients in SELL order (el_sell) and the SELL columns,
-// one thread per SELL position writes the scaled block straight into
-// valh_sell (coalesced); otherwise one thread per slot. val (unscaled) and
-// valh (scaled, CSR order) are written only when non-null. Both forms write
-// the same values; tpb only sizes the blocks.
+// With the SELL-32 slice offsets (chunk_off) and the widest slice's column
+// slots (wmax <= ASM_SLICE_WMAX), one CTA per slice stages the slice in
+// shared memory and writes with coalesced stores (tpb then sizes nothing);
+// otherwise one thread per slot with tpb threads per block. Both write the
+// same values: always the SELL copy, val (unscaled) and valh (scaled, CSR
+// order) only when non-null.
+constexpr int ASM_SLICE_TPB = 128, ASM_SLICE_WMAX = 32;
+inline size_t asm_slice_smem(int wmax, int copies) { return size_t(copies) * 9 * 32 * wmax * sizeof(float); }
 void launch_assemble_scaled(const MeshDev& m, const unsigned char* sflags, const StrainSV* sv, const double* diag_extra, int enable_strain,
                             const unsigned char* fixed, const double* Linv, const unsigned char* chol_ok, float* val, float* valh,
                             const int* sell_base, float* valh_sell, const Ctrl* ctrl, cudaStream_t s, int tpb = 256,
-                            const int* sell_slot = nullptr, const double* el_sell = nullptr, const int* sell_col = nullptr, int npos = 0);
-void launch_el_sell(const int* sell_slot, const double* el_b, int npos, double* el_sell, cudaStream_t s);
+                            const int* chunk_off = nullptr, int wmax = 0);
 void launch_extra_key64(const ContactEntry* xent, const int* xkeys, int n, unsigned long long* key, int* idx, cudaStream_t s);
 void launch_run_heads(const unsigned long long* key, int n, int* flags, cudaStream_t s);
 void launch_extra_merge(const ContactDev* c, const ContactEntry* xent, const unsigned long long* key, const int* idx, const int* heads, int nu,

@@ -63,7 +63,9 @@ def parse():
     ap.add_argument("--reference-steps", type=int, default=240, help="frames of the REFERENCE-semantics measurement (0: skip)")
     ap.add_argument("--full-n", type=int, default=64, help="curtain grid of the full-length CORRECTED comparison (0: skip)")
     ap.add_argument("--full-steps", type=int, default=240, help="frames of the full-length CORRECTED comparison")
-    ap.add_argument("--refresh", type=int, default=1, help="Newton iterations between evaluations of the preconditioner network")
+    ap.add_argument("--refresh", type=int, default=2,
+                    help="Newton iterations between evaluations of the preconditioner network (2: one evaluation per sub-step, "
+                         "whose second Newton iteration reuses the first one's coefficients)")
     ap.add_argument("--weights", default=None, help="learned preconditioner weights (.npy); default: the shipped C4 weights")
     ap.add_argument("--c3-frames", type=int, default=60, help="timed frames of the batched 64-scene comparison (0: skip)")
     ap.add_argument("--c2-frames", type=int, default=200, help="frames of the four-sheet stack (0: skip)")
@@ -182,15 +184,15 @@ def pcg_bytes(V, nnzb, prof):
 
 
 def assembly_bytes(V, nnzb, learned=True):
-    """Algorithmic bytes of one CORRECTED assembly, k_diag_factor + k_assemble_sell.
+    """Algorithmic bytes of one CORRECTED assembly, k_diag_factor + k_assemble_scaled_slice.
       k_diag_factor, per vertex: the FP64 diagonal terms (72) and gradient (24) in; L^-1 (FP64, 48),
         L (FP32, 24), b^ (12) and the factor flag (1) out                                   = 181 V
-      k_assemble_sell, per block slot: its slot, column, row (4 each) and FP64 elastic constant (8) in,
-        the scaled FP32 block out in SELL order (36)                                        = 56 nnzb
+      k_assemble_scaled_slice, per block slot: the FP64 elastic pair (16), its row, column and SELL
+        position (12) in, the scaled FP32 block out in SELL order (36)                      = 64 nnzb
         per vertex: the row's and the column's L^-1 (48 each, each read once) and the diagonal terms
         (72) again                                                                          = 168 V
       learned preconditioner: the scaled block again in CSR order for the network's features = 36 nnzb"""
-    return 349 * V + (92 if learned else 56) * nnzb
+    return 349 * V + (100 if learned else 64) * nnzb
 
 
 # DRAM bytes (read + write) per launch of the kernel on this workload, from one ncu capture (the summaries
@@ -573,7 +575,7 @@ def run_ours(args, rank, world, local, pg):
     if asm_ms > 0:
         ab = assembly_bytes(V, nnzb) * asm_n
         achieved = ab / (asm_ms * 1e-3) / 1e9
-        roof_asm = {"bound": "hbm", "kernel": "k_diag_factor + k_assemble_sell (+ k_extra_merge)", "achieved": round(achieved, 1),
+        roof_asm = {"bound": "hbm", "kernel": "k_diag_factor + k_assemble_scaled_slice (+ k_extra_merge)", "achieved": round(achieved, 1),
                     "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": ASSEMBLY_TRAFFIC, "peak_source": source,
                     "bytes_per_newton_iteration": int(assembly_bytes(V, nnzb)), "newton_iterations": int(asm_n),
                     "avg_us_per_newton_iteration": round(asm_ms * 1e3 / asm_n, 2)}
