@@ -63,9 +63,9 @@ def parse():
     ap.add_argument("--reference-steps", type=int, default=240, help="frames of the REFERENCE-semantics measurement (0: skip)")
     ap.add_argument("--full-n", type=int, default=64, help="curtain grid of the full-length CORRECTED comparison (0: skip)")
     ap.add_argument("--full-steps", type=int, default=240, help="frames of the full-length CORRECTED comparison")
-    ap.add_argument("--refresh", type=int, default=2,
-                    help="Newton iterations between evaluations of the preconditioner network (2: one evaluation per sub-step, "
-                         "whose second Newton iteration reuses the first one's coefficients)")
+    ap.add_argument("--refresh", type=int, default=8,
+                    help="Newton iterations between evaluations of the preconditioner network (8: about once per frame; in "
+                         "between, S is rebuilt from each Newton system with the last coefficients)")
     ap.add_argument("--weights", default=None, help="learned preconditioner weights (.npy); default: the shipped C4 weights")
     ap.add_argument("--c3-frames", type=int, default=60, help="timed frames of the batched 64-scene comparison (0: skip)")
     ap.add_argument("--c2-frames", type=int, default=200, help="frames of the four-sheet stack (0: skip)")
