@@ -570,16 +570,24 @@ int swept_toi(ando_ctx c, double eta_min, double near) {
 int detect_corrected(ando_ctx c, int nb, double gap_max) {
   cudaStream_t s = c->stream;
   int nvt = 0, nee = 0;
+  // Query and hierarchy boxes are both inflated by `pad`, so two primitives
+  // are candidates when their boxes come closer than 2 pad. Half the
+  // activation distance is enough for every pair closer than it (a box gap
+  // never exceeds the distance of what it bounds); the 6.25 % and 1e-6 m on
+  // top cover the rounding of the FP32 boxes for coordinates up to about
+  // 64 m. The narrow phase keeps the pairs whose FP64 distance is below
+  // gap_max, so the contact set does not depend on the pad.
+  const float pad = float(0.5 * gap_max * 1.0625 + 1e-6);
   {
     Phase ph(c, ANDO_PHASE_SETUP);
     long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
     // both queries launched back to back, both counters read in one round trip
     // the two queries on two streams (each is latency-bound), joined before the counts are read
     CK(fork_side(c));
-    CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, float(gap_max), c->bvh_epoch, c->cub_tmp, s));
-    CK(c->bvh_tri.contacts_launch(c->x.p, 0, nullptr, c->V, float(gap_max), gap_max, c->pair_scratch, c->pcount, s));
-    CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, float(gap_max), c->bvh_epoch, c->cub_tmp_side, c->side));
-    CK(c->bvh_edge.contacts_launch(c->x.p, 1, c->edges.p, c->E, float(gap_max), gap_max, c->pair_scratch_ee, c->pcount_ee, c->side));
+    CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, pad, c->bvh_epoch, c->cub_tmp, s));
+    CK(c->bvh_tri.contacts_launch(c->x.p, 0, nullptr, c->V, pad, gap_max, c->pair_scratch, c->pcount, s));
+    CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, pad, c->bvh_epoch, c->cub_tmp_side, c->side));
+    CK(c->bvh_edge.contacts_launch(c->x.p, 1, c->edges.p, c->E, pad, gap_max, c->pair_scratch_ee, c->pcount_ee, c->side));
     CK(join_side(c));
     int* h = c->counts_host;
     CK(cudaMemcpyAsync(h, c->pcount.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -593,7 +601,7 @@ int detect_corrected(ando_ctx c, int nb, double gap_max) {
       for (int attempt = 0; hk[0] > int(scr.n); ++attempt) {  // candidates overflowed: grow, launch again
         if (attempt == 2 || hk[0] > (1 << 26)) return fail(ANDO_ERR_CAPACITY, "contact candidates overflowed");
         CK(scr.reserve(size_t(hk[0]) + size_t(hk[0]) / 4));
-        CK(B.contacts_launch(c->x.p, kind, kind ? c->edges.p : nullptr, kind ? c->E : c->V, float(gap_max), gap_max, scr, cnt, s));
+        CK(B.contacts_launch(c->x.p, kind, kind ? c->edges.p : nullptr, kind ? c->E : c->V, pad, gap_max, scr, cnt, s));
         CK(cudaMemcpyAsync(hk, cnt.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
       }

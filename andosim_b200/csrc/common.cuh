@@ -176,25 +176,33 @@ __device__ inline bool grid_sync(unsigned int* count, unsigned int* gen, int* er
 // arrival to a 64-bit counter that the launcher zeroed (release: the CTA's
 // writes, ordered before the arrival by __syncthreads, are published) and
 // polls with acquire loads until all nblocks CTAs have arrived `epoch` times.
-// About half the cost of grid_sync's full fences. Same error contract.
+// About half the cost of grid_sync's full fences. The polling thread hands
+// its verdict to the CTA through shared memory, so the other threads leave
+// the barrier without another L2 round trip. A CTA that passed a barrier
+// while another CTA was giving up on it meets the error flag in the poll of
+// the next barrier (every wait stays bounded), and the host reads the flag
+// after the launch.
 __device__ inline bool grid_sync_ar(unsigned long long* arrivals, unsigned int nblocks, unsigned int& epoch, int* err) {
-  __syncthreads();
+  __shared__ int passed;
+  __syncthreads();  // also orders the previous call's reads of `passed` before this call's write
   ++epoch;
   if (threadIdx.x == 0) {
     const unsigned long long target = (unsigned long long)epoch * nblocks;
     asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(arrivals) : "memory");
     long long polls = 0;
+    int ok = 1;
     while (true) {
       unsigned long long v;
       asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(arrivals) : "memory");
       if (v >= target) break;
-      if (*(volatile int*)err) break;
-      if (++polls > (1ll << 24)) { atomicExch(err, 1); break; }
+      if (*(volatile int*)err) { ok = 0; break; }
+      if (++polls > (1ll << 24)) { atomicExch(err, 1); ok = 0; break; }
       if (polls > 1024) __nanosleep(32);
     }
+    passed = ok;
   }
   __syncthreads();
-  return *(volatile int*)err == 0;
+  return passed != 0;
 }
 
 }  // namespace ando

@@ -21,6 +21,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <climits>
 
 #include "lbvh.cuh"
 #include "narrow.cuh"
@@ -161,6 +162,17 @@ __global__ void k_leafv(const int* order, const int* prims, int arity, int n, in
   leafv[p] = make_int4(prim, v[0], arity > 1 ? v[1] : -1, arity > 2 ? v[2] : -1);
 }
 
+// Build time: 1 for the internal nodes at even depth, the nodes of the
+// four-wide hierarchy (the root is node 0 at depth 0). Karras depth is at most
+// about 64 with unique 64-bit keys; the climb is bounded at 256 regardless.
+__global__ void k_wide_flags(const int4* topo, int n, int* wflag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int d = 0, p = topo[i].w;
+  while (p >= 0 && d < 256) { ++d; p = topo[p].w; }
+  wflag[i] = (d & 1) == 0;
+}
+
 __device__ inline Box ld_box_volatile(const Box* b) {
   const volatile float* v = reinterpret_cast<const volatile float*>(b);
   Box r;
@@ -243,16 +255,13 @@ __global__ void k_top_count(const int* flag, const int* topnum, int n, int* meta
   if (m == 0) cuts[0] = make_int2(0, n - 1);
 }
 
-__device__ inline void store_children(LbvhInner* rec, const Box& l, const Box& r) {
-  float4* d = reinterpret_cast<float4*>(rec);  // lbox[6], rbox[6]: the record's first 48 bytes
-  d[0] = make_float4(l.lo[0], l.lo[1], l.lo[2], l.hi[0]);
-  d[1] = make_float4(l.hi[1], l.hi[2], r.lo[0], r.lo[1]);
-  d[2] = make_float4(r.lo[2], r.hi[0], r.hi[1], r.hi[2]);
-}
-
-__device__ inline void store_side(LbvhInner* rec, bool left, const Box& b) {
-  float* dst = left ? rec->lbox : rec->rbox;
-  for (int k = 0; k < 3; ++k) { dst[k] = b.lo[k]; dst[3 + k] = b.hi[k]; }
+// A node's final box into its four-wide slot (ws = 4 * node + slot; the
+// slot's six floats start on an 8-byte boundary).
+__device__ inline void store_slot(LbvhWide* wide, int ws, const Box& b) {
+  float2* d = reinterpret_cast<float2*>(&wide[ws >> 2].box[ws & 3][0]);
+  d[0] = make_float2(b.lo[0], b.lo[1]);
+  d[1] = make_float2(b.lo[2], b.hi[0]);
+  d[2] = make_float2(b.hi[1], b.hi[2]);
 }
 
 // The climbs below touch shared memory only (their block-scope fences then
@@ -260,7 +269,7 @@ __device__ inline void store_side(LbvhInner* rec, bool left, const Box& b) {
 // memory in one pass after the climb.
 __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const double* x1, const int* prims, int arity, float pad,
                                                       const int* order, int n, const int* parent, const int4* topo, const int2* cuts,
-                                                      const int* meta, int top_cap, Box* nodes, int* arrive, LbvhInner* inner) {
+                                                      const int* meta, int top_cap, Box* nodes, int* arrive, const int* wslot, LbvhWide* wide) {
   extern __shared__ __align__(16) unsigned char rf_raw[];
   RefitSmem& S = *reinterpret_cast<RefitSmem*>(rf_raw);
   const int ncut = meta[1];
@@ -300,28 +309,30 @@ __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const dou
       }
     }
     __syncthreads();
-    // write-out: leaf boxes, and the boxes and child boxes of the subtree's internal nodes
+    // write-out: the boxes of the subtree's leaves and internal nodes, each
+    // also into its four-wide slot
     for (int t = threadIdx.x; t <= c1 - c0; t += RF_TPB) {
       const int q = c0 + t;
       nodes[n - 1 + q] = S.leaf[t];
+      const int wl = wslot[n - 1 + q];
+      if (wl >= 0) store_slot(wide, wl, S.leaf[t]);
       if (q < n - 1) {
         const int4 tq = S.topo[t];
         if (tq.x >= c0 && tq.z <= c1) {
-          const Box& bl = tq.x == tq.y ? S.leaf[tq.x - c0] : S.node[tq.y - c0];
-          const Box& br = tq.y + 1 == tq.z ? S.leaf[tq.z - c0] : S.node[tq.y + 1 - c0];
-          store_children(inner + q, bl, br);
           nodes[q] = S.node[t];
+          const int wn = wslot[q];
+          if (wn >= 0) store_slot(wide, wn, S.node[t]);
         }
       }
     }
-    // the subtree's root (index c0 or c1, or the leaf) goes into its parent's
-    // record; carrying on through the top nodes needs every thread's nodes[]
-    // published first
+    // with more top nodes than k_refit_top holds, thread 0 carries on from
+    // the subtree's root (index c0 or c1, or the leaf) through the top nodes;
+    // that needs every thread's nodes[] published first
     if (top_global) {
       __threadfence();
       __syncthreads();
     }
-    if (threadIdx.x == 0) {
+    if (top_global && threadIdx.x == 0) {
       int root = -1;  // internal root index, -1: a single leaf
       if (c1 > c0) root = (S.topo[0].x == c0 && S.topo[0].z == c1) ? c0 : c1;
       Box box = root < 0 ? S.leaf[0] : S.node[root - c0];
@@ -331,8 +342,6 @@ __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const dou
         while (p >= 0) {
           const int4 tp = __ldg(topo + p);
           const bool from_left = chi == tp.y;
-          store_side(inner + p, from_left, box);
-          if (!top_global) break;  // k_refit_top finishes the top nodes
           int prior;
           asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(prior) : "l"(arrive + p) : "memory");
           if (prior == 0) break;
@@ -340,6 +349,8 @@ __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const dou
           const int sl = from_left ? tp.y + 1 : tp.x, sh = from_left ? tp.z : tp.y, sidx = from_left ? tp.y + 1 : tp.y;
           box = unite(box, ld_box_cg(nodes + (sl == sh ? n - 1 + sl : sidx)));
           nodes[p] = box;
+          const int wp = wslot[p];
+          if (wp >= 0) store_slot(wide, wp, box);
           chi = tp.z;
           p = tp.w;
         }
@@ -348,7 +359,7 @@ __global__ void __launch_bounds__(RF_TPB) k_refit_cut(const double* x, const dou
   }
 }
 
-__global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, int top_cap, const int4* rec, Box* nodes, LbvhInner* inner) {
+__global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, int top_cap, const int4* rec, Box* nodes, const int* wslot, LbvhWide* wide) {
   extern __shared__ __align__(16) unsigned char rt_raw[];
   TopSmem& S = *reinterpret_cast<TopSmem*>(rt_raw);
   const int m = meta[0];
@@ -383,9 +394,34 @@ __global__ void __launch_bounds__(TOP_TPB) k_refit_top(const int* meta, int top_
   for (int k = threadIdx.x; k < m; k += TOP_TPB) {
     const int4 r = S.rec[k];
     nodes[r.x] = S.box[k];
-    const Box bl = r.z >= 0 ? S.box[r.z] : ld_box_cg(nodes + (-r.z - 1));
-    const Box br = r.w >= 0 ? S.box[r.w] : ld_box_cg(nodes + (-r.w - 1));
-    store_children(inner + r.x, bl, br);
+    const int ws = wslot[r.x];
+    if (ws >= 0) store_slot(wide, ws, S.box[k]);
+  }
+}
+
+// Build time: the topology of each four-wide node (children, leaf bounds,
+// empty slots) and the slot of every binary node whose box a four-wide node
+// keeps: a leaf child of a four-wide node, or a child of a folded node. The
+// caller sets wslot to -1 first (the root and the folded nodes keep it).
+__global__ void k_wide_topo(const LbvhInner* inner, const int* wflag, const int* widx, int n, LbvhWide* wide, int* wslot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1 || !wflag[i]) return;
+  const int leaf0 = n - 1, w = widx[i];
+  LbvhWide& W = wide[w];
+  const LbvhInner r = inner[i];
+  auto enc = [&](int c) { return c >= leaf0 ? -(c - leaf0) - 1 : widx[c]; };
+  for (int sd = 0; sd < 2; ++sd) {
+    const int c = sd ? r.rc : r.lc;
+    const int k = 2 * sd;
+    if (c >= leaf0) {
+      W.child[k] = enc(c); W.cmax[k] = sd ? r.rmax : r.lmax; wslot[c] = 4 * w + k;
+      for (int e = 0; e < 3; ++e) { W.box[k + 1][e] = FLT_MAX; W.box[k + 1][3 + e] = -FLT_MAX; }
+      W.child[k + 1] = 0; W.cmax[k + 1] = INT_MIN;
+    } else {
+      const LbvhInner g = inner[c];
+      W.child[k] = enc(g.lc); W.cmax[k] = g.lmax; wslot[g.lc] = 4 * w + k;
+      W.child[k + 1] = enc(g.rc); W.cmax[k + 1] = g.rmax; wslot[g.rc] = 4 * w + k + 1;
+    }
   }
 }
 
@@ -412,7 +448,7 @@ __device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, in
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
 // prims = edges, keep e1 < e2 without shared vertex.
 __global__ void k_query(const double* x, const double* x1, const int* qprims, const int* qorder, int kind, int nq, float pad, int n,
-                        const int4* leafv, const int* rank, const LbvhInner* inner, const Box* nodes, int2* out, int* count, int cap) {
+                        const int4* leafv, const int* rank, const LbvhWide* wide, const Box* nodes, int2* out, int* count, int cap) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < nq;
   const int q = active && qorder ? qorder[t] : t;
@@ -439,35 +475,30 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
       if (pad > 0.f) for (int k = 0; k < 3; ++k) { qb.lo[k] -= pad; qb.hi[k] += pad; }
     }
   }
-  // Depth-first traversal that tests both children of a node before
-  // descending (Karras 2012): an overlapping leaf child is reported at once,
-  // an overlapping internal child is entered, and the second of two
-  // overlapping internal children goes on the stack. With unique 64-bit keys
-  // the hierarchy is at most 64 levels deep, so 96 slots never overflow; an
-  // overflow would be reported through count[1] instead of dropping
-  // candidates silently.
+  // Depth-first traversal of the four-wide hierarchy: each step loads one
+  // 128-byte node and tests its (up to) four child boxes; an overlapping leaf
+  // child is reported at once, the first overlapping internal child is entered
+  // and the others go on the stack. The binary hierarchy is at most 64 levels
+  // deep with unique 64-bit keys, the four-wide one half that, so three
+  // pushes per level fit 96 slots; an overflow would be reported through
+  // count[1] instead of dropping candidates silently.
   //
   // The edge-edge query is a self query: each pair is found from the edge
-  // that comes first in the tree's sorted leaf order (subtrees whose leaves
+  // that comes first in the tree's sorted leaf order (children whose leaves
   // all come before the query's own position are skipped) and reported with
   // the lower edge index first, which is the set the q < prim rule of a full
   // query gives.
   constexpr int STACK = 96;
   int stack[STACK];
   int sp = 0;
-  const int leaf0 = n - 1;          // with one primitive the root (node 0) is its leaf
   const int qpos = active && kind == 1 ? rank[q] : -1;
-  int node = -1;
-  bool single = false;              // n == 1: test the root leaf once
-  if (active && n > 0) {
-    if (n == 1) single = true;
-    else if (overlap(qb, nodes[0])) node = 0;
-  }
-  auto accept = [&](int leaf) {
-    const int4 lv = leafv[leaf - leaf0];
+  const bool single = active && n == 1;  // one primitive: the root (node 0) is its leaf
+  int node = active && n > 1 ? 0 : -1;
+  auto accept = [&](int pos) {
+    const int4 lv = leafv[pos];
     bool hit;
     if (kind == 0) hit = lv.y != q && lv.z != q && lv.w != q;
-    else hit = leaf - leaf0 > qpos && lv.y != qa && lv.y != qc && lv.z != qa && lv.z != qc;
+    else hit = pos > qpos && lv.y != qa && lv.y != qc && lv.z != qa && lv.z != qc;
     return hit ? lv.x : -1;
   };
   auto emit_pair = [&](int prim) {  // (lower, higher) edge index for the self query
@@ -480,31 +511,30 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
     emit_pair(prim);
   }
   while (__any_sync(0xffffffffu, node >= 0)) {
-    int hl = -1, hr = -1;
+    int h[4] = {-1, -1, -1, -1};
     if (node >= 0) {
-      const float4* rec = reinterpret_cast<const float4*>(inner + node);
-      const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3];
-      Box bl, br;
-      bl.lo[0] = r0.x; bl.lo[1] = r0.y; bl.lo[2] = r0.z; bl.hi[0] = r0.w; bl.hi[1] = r1.x; bl.hi[2] = r1.y;
-      br.lo[0] = r1.z; br.lo[1] = r1.w; br.lo[2] = r2.x; br.hi[0] = r2.y; br.hi[1] = r2.z; br.hi[2] = r2.w;
-      const int l = __float_as_int(r3.x), r = __float_as_int(r3.y);
-      // self query: a subtree whose last leaf is at or before the query's position holds no new pair
-      bool ol = __float_as_int(r3.z) > qpos && overlap(qb, bl), orr = __float_as_int(r3.w) > qpos && overlap(qb, br);
-      bool ll = l >= leaf0, lr = r >= leaf0;
-      if (ol && ll) hl = accept(l);
-      if (orr && lr) hr = accept(r);
-      bool tl = ol && !ll, tr = orr && !lr;
-      if (!tl && !tr) node = sp > 0 ? stack[--sp] : -1;
-      else {
-        node = tl ? l : r;
-        if (tl && tr) {
-          if (sp < STACK) stack[sp++] = r;
-          else atomicAdd(count + 1, 1);
-        }
-      }
+      const float4* r = reinterpret_cast<const float4*>(wide + node);
+      const float4 f0 = __ldg(r), f1 = __ldg(r + 1), f2 = __ldg(r + 2), f3 = __ldg(r + 3), f4 = __ldg(r + 4), f5 = __ldg(r + 5);
+      const int4 ch = __ldg(reinterpret_cast<const int4*>(r) + 6), cm = __ldg(reinterpret_cast<const int4*>(r) + 7);
+      int next = -1;
+      auto slot = [&](float lox, float loy, float loz, float hix, float hiy, float hiz, int c, int m, int& hk) {
+        if (!(m > qpos && qb.lo[0] <= hix && qb.hi[0] >= lox && qb.lo[1] <= hiy && qb.hi[1] >= loy && qb.lo[2] <= hiz && qb.hi[2] >= loz))
+          return;
+        if (c < 0) hk = accept(-c - 1);
+        else if (next < 0) next = c;
+        else if (sp < STACK) stack[sp++] = c;
+        else atomicAdd(count + 1, 1);
+      };
+      slot(f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, ch.x, cm.x, h[0]);
+      slot(f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, ch.y, cm.y, h[1]);
+      slot(f3.x, f3.y, f3.z, f3.w, f4.x, f4.y, ch.z, cm.z, h[2]);
+      slot(f4.z, f4.w, f5.x, f5.y, f5.z, f5.w, ch.w, cm.w, h[3]);
+      node = next >= 0 ? next : (sp > 0 ? stack[--sp] : -1);
     }
-    emit_pair(hl);
-    emit_pair(hr);
+    emit_pair(h[0]);
+    emit_pair(h[1]);
+    emit_pair(h[2]);
+    emit_pair(h[3]);
   }
 }
 
@@ -575,6 +605,10 @@ cudaError_t Lbvh::reserve_prims(int n) {
   if ((e = parent.reserve(2 * N))) return e;
   if ((e = nodes.reserve(2 * N))) return e;
   if ((e = inner.reserve(N))) return e;
+  if ((e = wide.reserve(N))) return e;
+  if ((e = wflag.reserve(N))) return e;
+  if ((e = widx.reserve(N))) return e;
+  if ((e = wslot.reserve(2 * N))) return e;
   if ((e = rank.reserve(N))) return e;
   if ((e = arrive.reserve(N))) return e;
   if ((e = topo.reserve(N))) return e;
@@ -616,11 +650,20 @@ cudaError_t Lbvh::build(const double* x, const double* x1, const int* prims_, in
     if ((e = tmp.reserve(sb))) return e;
     if ((e = cub::DeviceScan::ExclusiveSum(tmp.p, sb, topflag.p, topnum.p, n - 1, s))) return e;
     k_top_records<<<nblk(n - 1), TPB, 0, s>>>(topo.p, inner.p, topnum.p, n, toprec.p, cuts.p);
-    launches += 2;
+    k_wide_flags<<<nblk(n - 1), TPB, 0, s>>>(topo.p, n, wflag.p);
+    sb = 0;
+    if ((e = cub::DeviceScan::ExclusiveSum(nullptr, sb, wflag.p, widx.p, n - 1, s))) return e;
+    if ((e = tmp.reserve(sb))) return e;
+    if ((e = cub::DeviceScan::ExclusiveSum(tmp.p, sb, wflag.p, widx.p, n - 1, s))) return e;
+    if ((e = cudaMemsetAsync(wslot.p, 0xff, sizeof(int) * (2 * n - 1), s))) return e;
+    k_wide_topo<<<nblk(n - 1), TPB, 0, s>>>(inner.p, wflag.p, widx.p, n, wide.p, wslot.p);
+    launches += 4;
+  } else {
+    if ((e = cudaMemsetAsync(wslot.p, 0xff, sizeof(int), s))) return e;  // the single leaf is the root
   }
   k_top_count<<<1, 1, 0, s>>>(topflag.p, topnum.p, n, meta.p, cuts.p);
   if ((e = launch_refit(x, x1, pad, s))) return e;
-  launches += (n > 1 ? 9 : 8) + (n > RF_CUT ? 1 : 0);
+  launches += (n > 1 ? 10 : 8) + (n > RF_CUT ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -658,8 +701,8 @@ cudaError_t Lbvh::launch_refit(const double* x, const double* x1, float pad, cud
   const int grid = std::max(1, std::min(3 * sms, 2 * ((n + 255) / 256)));
   const int cap = top_cap < 0 || top_cap > TOP_MAX ? TOP_MAX : top_cap;
   k_refit_cut<<<grid, RF_TPB, sizeof(RefitSmem), s>>>(x, x1, prims, arity, pad, order.p, n, parent.p, topo.p, cuts.p, meta.p, cap,
-                                                      nodes.p, arrive.p, inner.p);
-  if (n > RF_CUT) k_refit_top<<<1, TOP_TPB, sizeof(TopSmem), s>>>(meta.p, cap, toprec.p, nodes.p, inner.p);
+                                                      nodes.p, arrive.p, wslot.p, wide.p);
+  if (n > RF_CUT) k_refit_top<<<1, TOP_TPB, sizeof(TopSmem), s>>>(meta.p, cap, toprec.p, nodes.p, wslot.p, wide.p);
   return cudaGetLastError();
 }
 
@@ -683,7 +726,7 @@ cudaError_t run_query(Lbvh& B, const double* x, const double* x1, int kind, cons
   for (int attempt = 0; attempt < 2; ++attempt) {
     int cap = int(scratch.n);
     if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.n, B.leafv.p, B.rank.p, B.inner.p, B.nodes.p,
+    k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, B.qorder, kind, nq, pad, B.n, B.leafv.p, B.rank.p, B.wide.p, B.nodes.p,
                                      scratch.p, counter.p, cap);
     B.launches += 1;
     int cnt2[2] = {0, 0};
@@ -727,7 +770,7 @@ cudaError_t Lbvh::contacts_launch(const double* x, int kind, const int* qprims, 
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   if ((e = surv.reserve(scratch.n))) return e;
   const int cap = int(scratch.n);
-  k_query<<<nblk(nq), TPB, 0, s>>>(x, nullptr, qprims, qorder, kind, nq, pad, n, leafv.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, nullptr, qprims, qorder, kind, nq, pad, n, leafv.p, rank.p, wide.p, nodes.p, scratch.p, counter.p, cap);
   k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, gap, surv.p, counter.p + 2);
   launches += 2;
   return cudaGetLastError();
@@ -763,7 +806,7 @@ cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   const int cap = int(scratch.n);
   if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, n, leafv.p, rank.p, inner.p, nodes.p, scratch.p, counter.p, cap);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, n, leafv.p, rank.p, wide.p, nodes.p, scratch.p, counter.p, cap);
   k_pairs_toi<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, ext, eta_min, near, toi, overflow);
   launches += 2;
   return cudaGetLastError();

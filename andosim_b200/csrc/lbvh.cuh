@@ -9,10 +9,17 @@
 namespace ando {
 
 struct LbvhBox { float lo[3], hi[3]; };
-// Internal node as the traversal reads it: both children's boxes and indices
-// in one 64-byte record (one dependent load per level instead of two), and
-// the last sorted leaf position under each child (prunes the self-query).
-struct alignas(16) LbvhInner { float lbox[6], rbox[6]; int lc, rc, lmax, rmax; };
+// Internal node of the binary hierarchy: its children (internal index, or
+// n - 1 + sorted leaf position) and the last sorted leaf position under each.
+struct alignas(16) LbvhInner { int lc, rc, lmax, rmax; };
+// Four-wide node as the traversal reads it (128 bytes, one line): the binary
+// hierarchy with every other level folded into its parent. Slots 2s and
+// 2s + 1 hold side s of the binary node: its child when that is a leaf (slot
+// 2s + 1 then empty), else the child's two children. Per slot the box
+// (lo[3], hi[3]), the child (a four-wide node index >= 0, or a sorted leaf
+// position p as -(p + 1)) and the last sorted leaf position under it (prunes
+// the self query). An empty slot has an empty box and bound INT_MIN.
+struct alignas(128) LbvhWide { float box[4][6]; int child[4], cmax[4]; };
 
 struct Lbvh {
   int n = 0;                    // primitives
@@ -24,7 +31,10 @@ struct Lbvh {
   // 32 traversals of a warp on similar paths; results do not depend on it.
   const int* qorder = nullptr;
   DevBuf<LbvhBox> boxes, nodes; // primitive boxes; node boxes (internal [0,n-1), leaves [n-1, 2n-1))
-  DevBuf<LbvhInner> inner;      // n-1 internal nodes, child boxes packed (written by the refit)
+  DevBuf<LbvhInner> inner;      // n-1 internal nodes: children and their last leaves (the build's topology)
+  DevBuf<LbvhWide> wide;        // four-wide nodes: topology at build time, boxes by every refit
+  DevBuf<int> wflag, widx;      // per internal node: 1 at even depth (a four-wide node), its four-wide index
+  DevBuf<int> wslot;            // per node: 4 * four-wide index + slot where its box is kept, -1 if nowhere
   DevBuf<unsigned long long> keys, keys_sorted;
   DevBuf<int> idx, order, parent, arrive, bounds;
   DevBuf<int> rank;             // sorted leaf position of each primitive (inverse of order)
