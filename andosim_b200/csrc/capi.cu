@@ -166,6 +166,10 @@ struct ando_ctx_s {
 
   // broad phase (the LBVHs are rebuilt once per step, refit in between)
   long long bvh_epoch = 0;
+  // the time-of-impact candidate lists of the last line search (padded for
+  // contacts) hold every contact pair at the current positions: set by the
+  // line search, cleared by every entry point before it runs a step
+  bool cand_valid = false;
   DevBuf<int> edges;
   DevBuf<int> vorder, eorder;      // vertices / edges in Morton order of their rest positions (query order)
   int E = 0;
@@ -549,17 +553,31 @@ cudaError_t join_side(ando_ctx c) {
   return e == cudaSuccess ? cudaStreamWaitEvent(c->stream, c->ev_join, 0) : e;
 }
 
+// Pad of the boxes of the CORRECTED contact queries. Query and hierarchy
+// boxes are both inflated by it, so two primitives are candidates when their
+// boxes come closer than 2 pad. Half the activation distance is enough for
+// every pair closer than it (a box gap never exceeds the distance of what it
+// bounds); the 6.25 % and 1e-6 m on top cover the rounding of the FP32 boxes
+// for coordinates up to about 64 m. The narrow phase keeps the pairs whose
+// FP64 distance is below gap_max, so the contact set does not depend on it.
+float contact_pad(double gap_max) { return float(0.5 * gap_max * 1.0625 + 1e-6); }
+
 // Self-contact time of impact of the move x -> x1 (= x + ext), min-reduced
 // into toi: swept-box traversals of both trees, vertex-triangle on the main
-// stream and edge-edge on the side stream.
+// stream and edge-edge on the side stream. The swept boxes carry the contact
+// pad, so the candidate lists also hold every pair within the activation
+// distance at any position between x and x1, in particular where the line
+// search moves the vertices (the next contact set is filtered from them);
+// only pairs whose unpadded boxes overlap bound the step.
 int swept_toi(ando_ctx c, double eta_min, double near) {
   cudaStream_t s = c->stream;
+  const float pad = contact_pad(c->gap_max);
   CK(fork_side(c));
-  CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, 0.f, c->bvh_epoch, c->cub_tmp, s));
-  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, eta_min, near, c->toi.p, c->toi_scratch, c->pcount,
+  CK(c->bvh_tri.update(c->x.p, c->x1.p, c->tris.p, 3, c->T, pad, c->bvh_epoch, c->cub_tmp, s));
+  CK(c->bvh_tri.query_toi(c->x.p, c->x1.p, c->ext.p, 0, nullptr, c->V, pad, eta_min, near, c->toi.p, c->toi_scratch, c->pcount,
                           &c->ctrl.p->toi_overflow, s));
-  CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, 0.f, c->bvh_epoch, c->cub_tmp_side, c->side));
-  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, eta_min, near, c->toi.p, c->toi_scratch_ee, c->pcount_ee,
+  CK(c->bvh_edge.update(c->x.p, c->x1.p, c->edges.p, 2, c->E, pad, c->bvh_epoch, c->cub_tmp_side, c->side));
+  CK(c->bvh_edge.query_toi(c->x.p, c->x1.p, c->ext.p, 1, c->edges.p, c->E, pad, eta_min, near, c->toi.p, c->toi_scratch_ee, c->pcount_ee,
                            &c->ctrl.p->toi_overflow, c->side));
   CK(join_side(c));
   return ANDO_OK;
@@ -567,33 +585,37 @@ int swept_toi(ando_ctx c, double eta_min, double near) {
 
 // CORRECTED contact set at the current positions: LBVH vertex-triangle and
 // edge-edge candidates within the activation distance, then rigid contacts.
-int detect_corrected(ando_ctx c, int nb, double gap_max) {
+// With `reuse` the candidates are the last line search's lists (valid while
+// c->cand_valid): the vertices now sit where that line search moved them,
+// between its x and x1, and its boxes carried the contact pad, so the
+// filtered lists give the same contacts as new queries.
+int detect_corrected(ando_ctx c, int nb, double gap_max, bool reuse = false) {
   cudaStream_t s = c->stream;
   int nvt = 0, nee = 0;
-  // Query and hierarchy boxes are both inflated by `pad`, so two primitives
-  // are candidates when their boxes come closer than 2 pad. Half the
-  // activation distance is enough for every pair closer than it (a box gap
-  // never exceeds the distance of what it bounds); the 6.25 % and 1e-6 m on
-  // top cover the rounding of the FP32 boxes for coordinates up to about
-  // 64 m. The narrow phase keeps the pairs whose FP64 distance is below
-  // gap_max, so the contact set does not depend on the pad.
-  const float pad = float(0.5 * gap_max * 1.0625 + 1e-6);
+  const float pad = contact_pad(gap_max);
   {
     Phase ph(c, ANDO_PHASE_SETUP);
     long long b0 = c->bvh_tri.launches + c->bvh_edge.launches;
-    // both queries launched back to back, both counters read in one round trip
-    // the two queries on two streams (each is latency-bound), joined before the counts are read
+    // the two halves on two streams (each is latency-bound), joined before
+    // both counters are read in one round trip
     CK(fork_side(c));
-    CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, pad, c->bvh_epoch, c->cub_tmp, s));
-    CK(c->bvh_tri.contacts_launch(c->x.p, 0, nullptr, c->V, pad, gap_max, c->pair_scratch, c->pcount, s));
-    CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, pad, c->bvh_epoch, c->cub_tmp_side, c->side));
-    CK(c->bvh_edge.contacts_launch(c->x.p, 1, c->edges.p, c->E, pad, gap_max, c->pair_scratch_ee, c->pcount_ee, c->side));
+    if (reuse) {
+      CK(c->bvh_tri.contacts_from(c->x.p, 0, nullptr, gap_max, c->toi_scratch, c->pcount, s));
+      CK(c->bvh_edge.contacts_from(c->x.p, 1, c->edges.p, gap_max, c->toi_scratch_ee, c->pcount_ee, c->side));
+    } else {
+      CK(c->bvh_tri.update(c->x.p, nullptr, c->tris.p, 3, c->T, pad, c->bvh_epoch, c->cub_tmp, s));
+      CK(c->bvh_tri.contacts_launch(c->x.p, 0, nullptr, c->V, pad, gap_max, c->pair_scratch, c->pcount, s));
+      CK(c->bvh_edge.update(c->x.p, nullptr, c->edges.p, 2, c->E, pad, c->bvh_epoch, c->cub_tmp_side, c->side));
+      CK(c->bvh_edge.contacts_launch(c->x.p, 1, c->edges.p, c->E, pad, gap_max, c->pair_scratch_ee, c->pcount_ee, c->side));
+    }
     CK(join_side(c));
     int* h = c->counts_host;
     CK(cudaMemcpyAsync(h, c->pcount.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(h + 3, c->pcount_ee.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    for (int kind = 0; kind < 2; ++kind) {
+    if (reuse && (h[0] > int(c->toi_scratch.n) || h[3] > int(c->toi_scratch_ee.n)))
+      return fail(ANDO_ERR_STATE, "time-of-impact candidate lists incomplete");  // the line search grows and redoes an overflowed pass
+    for (int kind = 0; kind < 2 && !reuse; ++kind) {
       Lbvh& B = kind == 0 ? c->bvh_tri : c->bvh_edge;
       DevBuf<int2>& scr = kind == 0 ? c->pair_scratch : c->pair_scratch_ee;
       DevBuf<int>& cnt = kind == 0 ? c->pcount : c->pcount_ee;
@@ -677,7 +699,7 @@ int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, i
     launch_strain_face(m, c->x.p, sp, c->sflags.p, c->sv.p, c->ctrl.p, s);
     ph.launched();
   }
-  int rc = detect_corrected(c, nb, p.contact_gap_max);
+  int rc = detect_corrected(c, nb, p.contact_gap_max, c->cand_valid);
   if (rc) return rc;
   rc = prepare_contacts(c, sp, c->g_el_x.p, c->fixed.p);
   if (rc) return rc;
@@ -924,6 +946,7 @@ int inner_newton_corrected(ando_ctx c, const ando_params& p, const StepParams& s
       CK(cudaStreamSynchronize(s));
       c->collect();
     }
+    c->cand_valid = true;  // complete lists, x moved along them
     const Ctrl& h = *c->ctrl_host;
     if (h.pcg_status == PCG_TIMEOUT || h.bar_err) return fail(ANDO_ERR_TIMEOUT, "PCG grid barrier timed out");
     rc = learned_solve_stats(c, p, h, st);
@@ -1569,6 +1592,7 @@ int32_t ando_step(ando_ctx c, const ando_params* params, const ando_pin* pins, i
   if (rc) return rc;
   c->gap_max = p.contact_gap_max;
   c->bvh_epoch++;
+  c->cand_valid = false;
   c->val_valid = p.semantics == ANDO_SEMANTICS_REFERENCE || c->keep_system;
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
     rc = restore_start(c);
@@ -1691,6 +1715,7 @@ int32_t ando_eval_system(ando_ctx c, const ando_params* params, const ando_pin* 
   cudaStream_t s = c->stream;
   c->gap_max = p.contact_gap_max;
   c->bvh_epoch++;
+  c->cand_valid = false;
   c->val_valid = true;   // both semantics assemble the unscaled values here
   if (p.semantics == ANDO_SEMANTICS_CORRECTED) {
     rc = restore_start(c);
@@ -1755,6 +1780,7 @@ int32_t ando_compute_contacts_corrected(ando_ctx c, double gap_max, const ando_r
   if (rc) return rc;
   c->gap_max = gap_max;
   c->bvh_epoch++;
+  c->cand_valid = false;
   rc = detect_corrected(c, num_rigids, gap_max);
   if (rc) return rc;
   return contacts_out(c, out, capacity, num_out);

@@ -568,9 +568,14 @@ __global__ void k_pairs_gap(const int2* cand, const int* count, int cap, int kin
   }
 }
 
-// min over the candidates of the conservative time of impact along ext
+// min over the candidates of the conservative time of impact along ext. With
+// `pad` > 0 the traversal ran on boxes inflated by pad (so that the list also
+// holds every pair that can come within the contact distance at any position
+// on the way): only the pairs whose boxes overlap without the pad, built and
+// compared exactly as an unpadded traversal does, bound the step.
 __global__ void k_pairs_toi(const int2* cand, const int* count, int cap, int kind, const int* prims, const int* qprims, const double* x,
-                            const double* ext, double eta_min, double near, unsigned long long* toi, int* overflow) {
+                            const double* x1, const double* ext, float pad, double eta_min, double near, unsigned long long* toi,
+                            int* overflow) {
   if (count[0] > cap) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(overflow, count[0]);  // the capacity that is needed
     return;
@@ -578,8 +583,21 @@ __global__ void k_pairs_toi(const int2* cand, const int* count, int cap, int kin
   const int n = count[0];
   double t = 1.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int2 pr = cand[i];
+    if (pad > 0.f) {
+      Box qb;
+      if (kind == 0) {
+        const float3 p = xf(x, pr.x), p1 = xf(x1, pr.x);
+        const float e = 1e-4f;
+        qb.lo[0] = fminf(p.x - e, p1.x - e); qb.lo[1] = fminf(p.y - e, p1.y - e); qb.lo[2] = fminf(p.z - e, p1.z - e);
+        qb.hi[0] = fmaxf(p.x + e, p1.x + e); qb.hi[1] = fmaxf(p.y + e, p1.y + e); qb.hi[2] = fmaxf(p.z + e, p1.z + e);
+      } else {
+        qb = prim_box(x, x1, qprims, 2, pr.x, 0.f);
+      }
+      if (!overlap(qb, prim_box(x, x1, prims, kind == 0 ? 3 : 2, pr.y, 0.f))) continue;
+    }
     int id[4];
-    pair_ids(kind, cand[i], prims, qprims, id);
+    pair_ids(kind, pr, prims, qprims, id);
     t = fmin(t, pair_toi(kind, id, x, ext, eta_min, near));
   }
   t = warp_min(t);
@@ -797,18 +815,30 @@ cudaError_t Lbvh::contacts_finish(const int count[3], DevBuf<int2>& out, DevBuf<
   return cudaGetLastError();
 }
 
-cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, double eta_min,
-                            double near, unsigned long long* toi, DevBuf<int2>& scratch, DevBuf<int>& counter, int* overflow,
-                            cudaStream_t s) {
+cudaError_t Lbvh::query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, float pad,
+                            double eta_min, double near, unsigned long long* toi, DevBuf<int2>& scratch, DevBuf<int>& counter,
+                            int* overflow, cudaStream_t s) {
   if (n == 0 || nq == 0) return cudaSuccess;
   cudaError_t e;
   if ((e = counter.reserve(3))) return e;
   if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
   const int cap = int(scratch.n);
   if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
-  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, 0.f, n, leafv.p, rank.p, wide.p, nodes.p, scratch.p, counter.p, cap);
-  k_pairs_toi<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, ext, eta_min, near, toi, overflow);
+  k_query<<<nblk(nq), TPB, 0, s>>>(x, x1, qprims, qorder, kind, nq, pad, n, leafv.p, rank.p, wide.p, nodes.p, scratch.p, counter.p, cap);
+  k_pairs_toi<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, kind, prims, qprims, x, x1, ext, pad, eta_min, near, toi, overflow);
   launches += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t Lbvh::contacts_from(const double* x, int kind, const int* qprims, double gap, DevBuf<int2>& cand, DevBuf<int>& counter,
+                                cudaStream_t s) {
+  cudaError_t e;
+  if ((e = counter.reserve(3))) return e;
+  if (n == 0 || cand.n == 0) return cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s);
+  if ((e = cudaMemsetAsync(counter.p + 2, 0, sizeof(int), s))) return e;
+  if ((e = surv.reserve(cand.n))) return e;
+  k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(cand.p, counter.p, int(cand.n), kind, prims, qprims, x, gap, surv.p, counter.p + 2);
+  launches += 1;
   return cudaGetLastError();
 }
 

@@ -76,15 +76,26 @@ struct Lbvh {
                               DevBuf<int>& counter, cudaStream_t s);
   cudaError_t contacts_finish(const int count[3], DevBuf<int2>& out, DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1,
                               DevBuf<unsigned char>& tmp, int* npairs, cudaStream_t s);
-  // min over the swept-box candidates (x -> x1 = x + ext, no pad) of the
-  // pair's conservative time of impact, min-reduced into *toi (IEEE bits of a
+  // min over the swept-box candidates (x -> x1 = x + ext) of the pair's
+  // conservative time of impact, min-reduced into *toi (IEEE bits of a
   // non-negative double) on the device, with no host round trip: the
-  // candidate count stays on the device. When the candidates overflow
-  // `scratch`, *overflow is raised to the count needed and *toi is not
-  // lowered; the caller grows `scratch` and runs the pass again.
-  cudaError_t query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, double eta_min,
-                        double near, unsigned long long* toi, DevBuf<int2>& scratch, DevBuf<int>& counter, int* overflow,
+  // candidate count stays on the device. With pad > 0 the boxes are inflated
+  // by pad for the traversal (the list then also serves contacts_from at any
+  // position between x and x1) and only the pairs whose boxes overlap without
+  // it bound the step, so the result does not depend on the pad. When the
+  // candidates overflow `scratch`, *overflow is raised to the count needed and
+  // *toi is not lowered; the caller grows `scratch` and runs the pass again.
+  cudaError_t query_toi(const double* x, const double* x1, const double* ext, int kind, const int* qprims, int nq, float pad,
+                        double eta_min, double near, unsigned long long* toi, DevBuf<int2>& scratch, DevBuf<int>& counter, int* overflow,
                         cudaStream_t s);
+  // The first half of a contact query (contacts_launch) over the candidate
+  // list that a query_toi pass with the same counter left in `cand`: the
+  // pairs whose FP64 distance at x is below `gap`, counter[2] = how many;
+  // contacts_finish sorts them. Gives the contacts_launch result when every
+  // vertex at x lies between the pass's x and x1 and its pad is at least the
+  // contact query's.
+  cudaError_t contacts_from(const double* x, int kind, const int* qprims, double gap, DevBuf<int2>& cand, DevBuf<int>& counter,
+                            cudaStream_t s);
 };
 
 }  // namespace ando
