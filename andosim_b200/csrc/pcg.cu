@@ -617,12 +617,16 @@ int pcg_scaled_shapes(int device, int V, bool learned, PcgShape* out, int max) {
       if (grid > sms * per) grid = sms * per;
       out[n++] = PcgShape{tpb, grid, unroll};
     }
-    for (int t : {256, 512}) {
+    // fewer, larger CTAs: fewer arrivals at each grid barrier and fewer
+    // copies of the per-slice partials read after it; the last two
+    // candidates give every warp two slices
+    for (int t : {256, 512, 768, 1024}) {
       int p = occ(unroll, t);
       if (p < 1 || n >= max) continue;
       int grid = (ns + t / 32 - 1) / (t / 32);
       if (grid > sms * p) grid = sms * p;
       out[n++] = PcgShape{t, grid, unroll};
+      if (t >= 768 && grid > 1 && n < max) out[n++] = PcgShape{t, (grid + 1) / 2, unroll};
     }
   }
   return n;

@@ -249,6 +249,7 @@ def corrected_run(args, sc, local, flush, pg, precond, weights, profile=False, f
         total_ms += ms
     prof = S.profile()
     nnzb = S.system_size()[1]
+    shape = S.pcg_shape(precond == "learned")
     S.close()
     newton = sum(s["newton_iters"] for s in stats)
     pcg = sum(s["pcg_iters"] for s in stats)
@@ -256,6 +257,7 @@ def corrected_run(args, sc, local, flush, pg, precond, weights, profile=False, f
             "pcg_iters_per_newton": round(pcg / newton, 2) if newton else 0.0,
             "phase_ms_per_frame": {k: round(v / frames, 4) for k, v in prof["phase_ms"].items()},
             "pcg_us_per_iteration": round(prof["phase_ms"]["pcg"] * 1e3 / prof["pcg_iterations"], 2) if prof["pcg_iterations"] else None,
+            "pcg_launch_shape": {q: shape[q] for q in ("tpb", "grid", "unroll", "candidates")},
             "_prof": prof, "_nnzb": nnzb}
 
 
