@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--refresh", type=int, default=8,
                     help="Newton iterations between evaluations of the preconditioner network (8: about once per frame; in "
                          "between, S is rebuilt from each Newton system with the last coefficients)")
+    ap.add_argument("--pcg-shape", type=int, default=-1,
+                    help="learned scaled-PCG launch candidate of the timed contexts (-1: autotune on the first solve; "
+                         "a fixed candidate reproduces one shape, e.g. under a profiler)")
     ap.add_argument("--weights", default=None, help="learned preconditioner weights (.npy); default: the shipped C4 weights")
     ap.add_argument("--c3-frames", type=int, default=60, help="timed frames of the batched 64-scene comparison (0: skip)")
     ap.add_argument("--c2-frames", type=int, default=200, help="frames of the four-sheet stack (0: skip)")
@@ -197,9 +200,9 @@ def assembly_bytes(V, nnzb, learned=True):
 
 # DRAM bytes (read + write) per launch of the kernel on this workload, from one ncu capture (the summaries
 # under profiles/ give the command): the PCG's matrix and vectors come from DRAM once per launch and from L2
-# for every later iteration; the assembly's figure is k_assemble_scaled_slice alone.
-PCG_TRAFFIC = 45_572_352
-ASSEMBLY_TRAFFIC = 82_325_760
+# for every later iteration; the assembly's figure is k_diag_factor plus k_assemble_scaled_slice (44.9 + 27.9 MB).
+PCG_TRAFFIC = 53_985_536
+ASSEMBLY_TRAFFIC = 72_798_720
 
 
 class Timer:
@@ -231,6 +234,8 @@ def corrected_run(args, sc, local, flush, pg, precond, weights, profile=False, f
     S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
     if weights is not None:
         S.set_precond_weights(weights)
+    if args.pcg_shape >= 0:
+        S.select_pcg_shape(True, args.pcg_shape)
     params = abi.make_params(sc.params, semantics="corrected", precond=precond, precond_refresh=args.refresh)
     tm = Timer(torch, torch.cuda.ExternalStream(S.stream(), device=torch.device("cuda", local)), flush)
     for f in range(args.warmup):
@@ -273,6 +278,8 @@ def paired_run(args, sc, local, flush, pg, weights, steps=None, raw=False):
 
     S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
     S.set_precond_weights(weights)
+    if args.pcg_shape >= 0:
+        S.select_pcg_shape(True, args.pcg_shape)
     pl = abi.make_params(sc.params, semantics="corrected", precond="learned", precond_refresh=args.refresh)
     pj = abi.make_params(sc.params, semantics="corrected", precond="block_jacobi")
     tm = Timer(torch, torch.cuda.ExternalStream(S.stream(), device=torch.device("cuda", local)), flush)
