@@ -1447,11 +1447,13 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->x.reserve(3ull * V)); CK(c->v.reserve(3ull * V)); CK(c->x_prev.reserve(3ull * V)); CK(c->mass.reserve(V));
   CK(c->x_old.reserve(3ull * V)); CK(c->x_hat.reserve(3ull * V)); CK(c->g.reserve(3ull * V));
   CK(c->g_const.reserve(3ull * V)); CK(c->diag_const.reserve(9ull * V)); CK(c->diag_extra.reserve(9ull * V));
-  CK(c->b.reserve(3ull * V)); CK(c->d.reserve(3ull * V)); CK(c->r.reserve(3ull * V)); CK(c->z.reserve(3ull * V));
-  CK(c->p0.reserve(3ull * V)); CK(c->p1.reserve(3ull * V)); CK(c->Ap.reserve(3ull * V));
+  // r, z, p0, p1, Ap (and r2): one float4 per row for the scaled PCG, the
+  // first 3V for the REFERENCE PCG
+  CK(c->b.reserve(3ull * V)); CK(c->d.reserve(3ull * V)); CK(c->r.reserve(4ull * V)); CK(c->z.reserve(4ull * V));
+  CK(c->p0.reserve(4ull * V)); CK(c->p1.reserve(4ull * V)); CK(c->Ap.reserve(4ull * V));
   CK(c->val.reserve(9ull * nnzb)); CK(c->precond.reserve(9ull * V));
   CK(c->Linv.reserve(6ull * V)); CK(c->Lf.reserve(6ull * V)); CK(c->bhat.reserve(3ull * V)); CK(c->chol_ok.reserve(V));
-  CK(c->valh.reserve(9ull * nnzb)); CK(c->xh.reserve(3ull * V)); CK(c->r2.reserve(3ull * V));
+  CK(c->valh.reserve(9ull * nnzb)); CK(c->xh.reserve(3ull * V)); CK(c->r2.reserve(4ull * V));
   CK(c->sflags.reserve(std::max(T, 1))); CK(c->sv.reserve(2ull * std::max(T, 1)));
   {
     double sum = 0.0;

@@ -230,18 +230,39 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg(PcgArgs a) {
 // warp's 32 rows read every value and column load as one coalesced 128-byte
 // line, and 32 rows' gathers are in flight at once (sell_row_u below).
 
-struct GatherP {  // p = z + beta p_old
+// Row stride S of the scaled PCG's vectors r, r2, z, p0, p1 and Ap: 4 (one
+// float4 per row, the fourth lane unused, so a neighbour's entry is one
+// 16-byte load) in the block-Jacobi solve, 3 in the learned one, where the
+// larger vectors measured slower (19.5 against 18.7 us per iteration at
+// C4). Each solve initialises its vectors, so the two layouts share buffers
+// of 4V floats.
+template <int S> __device__ inline float4 ld4(const float* v, int j) {
+  if (S == 4) return reinterpret_cast<const float4*>(v)[j];
+  return make_float4(v[3 * j], v[3 * j + 1], v[3 * j + 2], 0.f);
+}
+template <int S> __device__ inline void st4(float* v, int j, float a, float b, float c) {
+  if (S == 4) reinterpret_cast<float4*>(v)[j] = make_float4(a, b, c, 0.f);
+  else { v[3 * j] = a; v[3 * j + 1] = b; v[3 * j + 2] = c; }
+}
+
+template <int S> struct GatherP {  // p = z + beta p_old
   const float* z; const float* pold; float beta; bool first;
-  __device__ void operator()(int j, float& q0, float& q1, float& q2) const { p_at(z, pold, beta, first, j, q0, q1, q2); }
+  __device__ void operator()(int j, float& q0, float& q1, float& q2) const {
+    const float4 zz = ld4<S>(z, j);
+    if (first) { q0 = zz.x; q1 = zz.y; q2 = zz.z; return; }
+    const float4 pp = ld4<S>(pold, j);
+    q0 = zz.x + beta * pp.x; q1 = zz.y + beta * pp.y; q2 = zz.z + beta * pp.z;
+  }
 };
 struct GatherV {  // plain vector
   const float* v;
   __device__ void operator()(int j, float& q0, float& q1, float& q2) const { q0 = v[3 * j]; q1 = v[3 * j + 1]; q2 = v[3 * j + 2]; }
 };
-struct GatherR {  // r - alpha Ap
+template <int S> struct GatherR {  // r - alpha Ap
   const float* r; const float* Ap; float alpha;
   __device__ void operator()(int j, float& q0, float& q1, float& q2) const {
-    q0 = r[3 * j] - alpha * Ap[3 * j]; q1 = r[3 * j + 1] - alpha * Ap[3 * j + 1]; q2 = r[3 * j + 2] - alpha * Ap[3 * j + 2];
+    const float4 rr = ld4<S>(r, j), aa = ld4<S>(Ap, j);
+    q0 = rr.x - alpha * aa.x; q1 = rr.y - alpha * aa.y; q2 = rr.z - alpha * aa.z;
   }
 };
 
@@ -399,6 +420,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
     if (blockIdx.x == 0 && threadIdx.x == 0) ctrl->fallback_ran = 1;
   }
   __shared__ RedSmem sh;
+  constexpr int S = LEARNED ? 3 : 4;  // row stride of r, z, p, Ap
   const int V = a.V, ns = (V + 31) >> 5;
   const unsigned nb = gridDim.x;
   const int lane = threadIdx.x & 31;
@@ -420,11 +442,11 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
       float b0 = a.bhat[3 * i], b1 = a.bhat[3 * i + 1], b2 = a.bhat[3 * i + 2];
       binf_loc = fmax(fabs(double(b0)), fmax(fabs(double(b1)), fabs(double(b2))));
       a.xh[3 * i] = 0.0; a.xh[3 * i + 1] = 0.0; a.xh[3 * i + 2] = 0.0;
-      r[3 * i] = b0; r[3 * i + 1] = b1; r[3 * i + 2] = b2;
+      st4<S>(r, i, b0, b1, b2);
       if (LEARNED) {
         float y0, y1, y2;
         sell_row_S<U>(i, a.chunk_off, a.sell_col, a.valh, a.coef, a.Sdiag, GatherV{a.bhat}, y0, y1, y2);
-        a.z[3 * i] = y0; a.z[3 * i + 1] = y1; a.z[3 * i + 2] = y2;
+        st4<S>(a.z, i, y0, y1, y2);
         rz_loc = double(b0) * y0 + double(b1) * y1 + double(b2) * y2;
       } else {
         rz_loc = double(b0) * b0 + double(b1) * b1 + double(b2) * b2;
@@ -456,7 +478,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
   int since = 0;
   for (int it = 0; ok && status == PCG_MAXIT && it < a.max_iters; ++it) {
     // ---- phase A: p_new = z + beta p_old, Ap = A^ p_new, p^T Ap
-    GatherP gp{zsrc, pold, beta, first};
+    GatherP<S> gp{zsrc, pold, beta, first};
     for (int sl = gw; sl < ns; sl += W) {
       const int row = 32 * sl + lane;
       double pap_loc = 0.0;
@@ -464,8 +486,8 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
         float y0, y1, y2;
         sell_row_u<U>(row, a.chunk_off, a.sell_col, a.valh, a.xbegin, a.xend, a.xcols, a.xvalh, gp, y0, y1, y2);
         float q0, q1, q2; gp(row, q0, q1, q2);
-        pnew[3 * row] = q0; pnew[3 * row + 1] = q1; pnew[3 * row + 2] = q2;
-        a.Ap[3 * row] = y0; a.Ap[3 * row + 1] = y1; a.Ap[3 * row + 2] = y2;
+        st4<S>(pnew, row, q0, q1, q2);
+        st4<S>(a.Ap, row, y0, y1, y2);
         pap_loc = double(q0) * y0 + double(q1) * y1 + double(q2) * y2;
       }
       pap_loc = warp_sum(pap_loc);
@@ -489,10 +511,11 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
         const int i = 32 * sl + lane;
         double rz_new_loc = 0.0, rinf_loc = 0.0;
         if (i < V) {
-          float p0 = pnew[3 * i], p1 = pnew[3 * i + 1], p2 = pnew[3 * i + 2];
+          const float4 pv = ld4<S>(pnew, i), rv = ld4<S>(r, i), av = ld4<S>(a.Ap, i);
+          const float p0 = pv.x, p1 = pv.y, p2 = pv.z;
           a.xh[3 * i] += double(alpha) * p0; a.xh[3 * i + 1] += double(alpha) * p1; a.xh[3 * i + 2] += double(alpha) * p2;
-          float r0 = r[3 * i] - alpha * a.Ap[3 * i], r1 = r[3 * i + 1] - alpha * a.Ap[3 * i + 1], r2 = r[3 * i + 2] - alpha * a.Ap[3 * i + 2];
-          r[3 * i] = r0; r[3 * i + 1] = r1; r[3 * i + 2] = r2;
+          float r0 = rv.x - alpha * av.x, r1 = rv.y - alpha * av.y, r2 = rv.z - alpha * av.z;
+          st4<S>(r, i, r0, r1, r2);
           if (sr) {
             sr[3 * i] = r0; sr[3 * i + 1] = r1; sr[3 * i + 2] = r2;
             sx[3 * i] = a.xh[3 * i]; sx[3 * i + 1] = a.xh[3 * i + 1]; sx[3 * i + 2] = a.xh[3 * i + 2];
@@ -505,7 +528,7 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
         if (lane == 0) { part_rz[sl] = rz_new_loc; part_rinf[sl] = rinf_loc; }
       }
     } else {
-      GatherR gr{r, a.Ap, alpha};
+      GatherR<S> gr{r, a.Ap, alpha};
       for (int sl = gw; sl < ns; sl += W) {
         const int row = 32 * sl + lane;
         double rz_new_loc = 0.0, rinf_loc = 0.0;
@@ -513,10 +536,11 @@ __global__ void __launch_bounds__(SCALED_MAX_TPB) k_pcg_scaled(PcgScaledArgs a) 
           float y0, y1, y2;
           sell_row_S<U>(row, a.chunk_off, a.sell_col, a.valh, a.coef, a.Sdiag, gr, y0, y1, y2);
           float r0, r1, r2; gr(row, r0, r1, r2);
-          a.xh[3 * row] += double(alpha) * pnew[3 * row]; a.xh[3 * row + 1] += double(alpha) * pnew[3 * row + 1];
-          a.xh[3 * row + 2] += double(alpha) * pnew[3 * row + 2];
-          rn[3 * row] = r0; rn[3 * row + 1] = r1; rn[3 * row + 2] = r2;
-          a.z[3 * row] = y0; a.z[3 * row + 1] = y1; a.z[3 * row + 2] = y2;
+          const float4 pv = ld4<S>(pnew, row);
+          a.xh[3 * row] += double(alpha) * pv.x; a.xh[3 * row + 1] += double(alpha) * pv.y;
+          a.xh[3 * row + 2] += double(alpha) * pv.z;
+          st4<S>(rn, row, r0, r1, r2);
+          st4<S>(a.z, row, y0, y1, y2);
           rz_new_loc = double(r0) * y0 + double(r1) * y1 + double(r2) * y2;
           rinf_loc = fmax(fabs(double(r0)), fmax(fabs(double(r1)), fabs(double(r2))));
         }
