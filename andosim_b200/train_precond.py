@@ -1,7 +1,7 @@
 """Train the learned preconditioner on the two-curtain workload and evaluate it.
 
     python -m andosim_b200.train_precond [--sets 256:0-14:1,64:0-239:4] [--train-seeds 0-7]
-        [--eval-seeds 8-11] [--steps 3000] [--out PATH] [--report PATH]
+        [--eval-seeds 8-11] [--steps 3000] [--out PATH] [--report PATH] [--evaluate WEIGHTS]
 
 Training data are the solver's own dumps: the first Newton system of the
 chosen frames of CORRECTED-semantics runs of scenes.c4 for the training seeds,
@@ -63,6 +63,8 @@ def main(argv=None):
     ap.add_argument("--refresh", type=int, default=1)
     ap.add_argument("--out", default=str(learned.DEFAULT_WEIGHTS))
     ap.add_argument("--report", default=None)
+    ap.add_argument("--evaluate", default=None,
+                    help="weights (.npy) to evaluate on the held-out seeds instead of training new ones")
     a = ap.parse_args(argv)
 
     sets = []
@@ -70,6 +72,11 @@ def main(argv=None):
         n, fr, ev = spec.split(":")
         f0, f1 = fr.split("-")
         sets.append((int(n), int(f0), int(f1), int(ev)))
+    if a.evaluate:
+        w = learned.load_weights(a.evaluate)
+        report = dict(sets=a.sets, weights=a.evaluate, eval=[])
+        run_eval(a, sets, w, report)
+        return
     t0 = time.time()
     trainer = abi.Trainer(abi.precond_init_weights(a.init_seed))
     n_sys = sum(learned.c4_training_set(trainer, seeds(a.train_seeds), n, range(f0, f1 + 1, ev)) for n, f0, f1, ev in sets)
@@ -85,6 +92,10 @@ def main(argv=None):
     report = dict(sets=a.sets, train_seeds=seeds(a.train_seeds), systems=n_sys, collect_s=t_collect, train_steps=a.steps,
                   train_s=t_train, loss_before=loss0, loss_after=loss1, weights=str(out), eval=[])
     print(json.dumps({k: v for k, v in report.items() if k != "eval"}), flush=True)
+    run_eval(a, sets, w, report)
+
+
+def run_eval(a, sets, w, report):
     for n, f0, f1, _ in sets:
         for sd in seeds(a.eval_seeds):
             sc = scenes.c4(seed=sd, n=n)
