@@ -28,6 +28,7 @@ EXPORTED = [
     "ando_eval_system",
     "ando_last_gradient", "ando_last_contact_blocks", "ando_profile_enable", "ando_profile_read", "ando_ctx_stream",
     "ando_broad_phase", "ando_pcg_solve_noalloc", "ando_ctx_keep_system",
+    "ando_collision_metrics", "ando_state_moments", "ando_edge_triangle_crossings",
 ]
 
 PHASES = ["setup", "strain", "gradient", "assemble", "pcg", "line_search", "finish", "precond"]
@@ -94,6 +95,22 @@ class Contact(C.Structure):
         ("gap", C.c_double), ("normal", C.c_double * 3), ("witness_p", C.c_double * 3), ("witness_q", C.c_double * 3),
         ("barycentric", C.c_double * 3), ("weights", C.c_double * 4),
     ]
+
+
+class Metrics(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("num_total_contacts", "num_point_triangle", "num_edge_edge", "num_wall",
+                                          "num_penetrations", "num_major_penetrations", "num_tunneling",
+                                          "num_ccd_contacts", "num_relative_velocities")] + \
+               [(n, C.c_double) for n in ("min_gap", "max_gap", "sum_gap", "max_penetration", "sum_penetration",
+                                          "max_relative_velocity", "sum_relative_velocity")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Moments(C.Structure):
+    _fields_ = [("kinetic_energy", C.c_double), ("linear_momentum", C.c_double * 3),
+                ("angular_momentum", C.c_double * 3), ("max_speed", C.c_double)]
 
 
 class Profile(C.Structure):
@@ -181,6 +198,9 @@ def lib() -> C.CDLL:
     L.ando_trainer_step.restype = I32; L.ando_trainer_step.argtypes = [P, C.c_float, pd]
     L.ando_trainer_get_weights.restype = I32; L.ando_trainer_get_weights.argtypes = [P, pf, I32]
     L.ando_trainer_set_weights.restype = I32; L.ando_trainer_set_weights.argtypes = [P, pf, I32]
+    L.ando_collision_metrics.restype = I32; L.ando_collision_metrics.argtypes = [P, D, I32, C.POINTER(Metrics)]
+    L.ando_state_moments.restype = I32; L.ando_state_moments.argtypes = [P, C.POINTER(Moments)]
+    L.ando_edge_triangle_crossings.restype = I32; L.ando_edge_triangle_crossings.argtypes = [P, C.POINTER(C.c_int64)]
     L.ando_pcg_solve_noalloc.restype = I32
     L.ando_pcg_solve_noalloc.argtypes = [I32, P, I32, P, P, P, P, P, P, C.c_int64, D, I32, pi, pi, pd]
     _lib = L
@@ -457,6 +477,25 @@ class Scene:
                "ando_last_scaled_system")
         return dict(rowptr=rowptr, cols=cols, valh=valh.reshape(-1, 3, 3), xrow=xr, xcol=xc,
                     xvalh=xvalh[:9 * len(xr)].reshape(-1, 3, 3), bhat=bhat, Lf=Lf.reshape(-1, 6), Linv=Linv.reshape(-1, 6))
+
+    def collision_metrics(self, gap_max: float, ccd: bool = True) -> dict:
+        """CollisionValidator sums over the context's current contact list, reduced on the device."""
+        m = Metrics()
+        _check(lib().ando_collision_metrics(self.ctx, float(gap_max), int(bool(ccd)), C.byref(m)), "ando_collision_metrics")
+        return m.as_dict()
+
+    def moments(self) -> dict:
+        """Kinetic energy, linear / angular momentum and largest speed of the device state."""
+        m = Moments()
+        _check(lib().ando_state_moments(self.ctx, C.byref(m)), "ando_state_moments")
+        return {"kinetic_energy": m.kinetic_energy, "linear_momentum": np.array(m.linear_momentum[:]),
+                "angular_momentum": np.array(m.angular_momentum[:]), "max_speed": m.max_speed}
+
+    def edge_triangle_crossings(self) -> int:
+        """Mesh edges passing through a triangle they share no vertex with, at the current positions."""
+        n = C.c_int64()
+        _check(lib().ando_edge_triangle_crossings(self.ctx, C.byref(n)), "ando_edge_triangle_crossings")
+        return int(n.value)
 
     def contacts(self, rigids: Optional[List[Rigid]] = None, semantics: str = "reference", gap_max: float = 1e-3) -> List[Contact]:
         """Contacts at the current state: the reference's query, or (semantics="corrected") the

@@ -18,7 +18,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "lib"
-CU_SOURCES = ["kernels.cu", "corrected.cu", "pcg.cu", "lbvh.cu", "learned.cu", "tc_gemm.cu", "capi.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "corrected.cu", "pcg.cu", "lbvh.cu", "learned.cu", "tc_gemm.cu", "capi.cu", "noalloc.cu", "diag.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 

@@ -229,6 +229,15 @@ struct State {
   ando_ctx ctx = nullptr;
   uint64_t topo = 0, verts = 0, weights = 0;
   bool dev_x = false, dev_v = false, start_stale = false, host_dirty = true, masses_dirty = true;
+  // The contact list the context holds on the device: its id (0: none, or
+  // replaced since) and length. compute_contacts stamps the Contact objects it
+  // returns with the id and their position, so CollisionValidator can reduce
+  // that list on the device instead of downloading the state.
+  uint64_t contact_list = 0;
+  size_t contact_count = 0;
+  static uint64_t next_contact_list() { static uint64_t n = 0; return ++n; }
+  // the device holds this state's current positions, velocities and masses
+  bool device_current() const { return ctx && !host_dirty && !masses_dirty; }
   ando_step_stats last{};
 
   State() = default;
@@ -287,6 +296,7 @@ struct State {
                              mesh.dm_inv.data(), &mt), "mesh upload");
       topo = mesh.topo_version; verts = mesh.vert_version;
       host_dirty = true; masses_dirty = true;
+      contact_list = 0;
     } else if (verts != mesh.vert_version) {
       std::vector<double> mv = flat(mesh.vertices);
       check(ando_mesh_set_vertices(ctx, mv.data(), int32_t(mesh.nv())), "mesh vertices");
@@ -296,6 +306,7 @@ struct State {
       std::vector<double> fx = flat(x), fv = flat(v), fp = flat(xp);
       check(ando_state_upload(ctx, fx.data(), fv.data(), fp.data(), m.data(), int32_t(nv())), "state upload");
       host_dirty = false; masses_dirty = false;
+      contact_list = 0;
       if (start.size() == nv()) {     // the upload made x the start; put the real one back
         std::vector<double> fs = flat(start);
         check(ando_state_set_start(ctx, fs.data(), int32_t(nv())), "state start");
@@ -312,7 +323,8 @@ struct Constraints {
 };
 
 enum class ContactType { POINT_TRIANGLE = 0, EDGE_EDGE = 1, WALL = 2, RIGID_POINT_TRIANGLE = 3 };
-struct Contact { ando_contact c{}; };
+// list / pos: which device contact list this contact was read from (State::contact_list) and where
+struct Contact { ando_contact c{}; uint64_t list = 0; int32_t pos = -1; };
 
 // --------------------------------------------------------------- diagnostics
 struct EnergyDiagnostics {
@@ -533,8 +545,11 @@ std::vector<Contact> compute_contacts(const Mesh& me, State& s, py::object rigid
     rc = query(buf.data(), n, &n);
   }
   check(rc, "compute_contacts");
+  const uint64_t id = State::next_contact_list();
+  s.contact_list = id;
+  s.contact_count = size_t(n);
   std::vector<Contact> out(static_cast<size_t>(n));
-  for (int32_t k = 0; k < n; ++k) out[size_t(k)].c = buf[size_t(k)];
+  for (int32_t k = 0; k < n; ++k) { out[size_t(k)].c = buf[size_t(k)]; out[size_t(k)].list = id; out[size_t(k)].pos = k; }
   return out;
 }
 
@@ -603,6 +618,43 @@ PYBIND11_MODULE(ando_barrier_core, m) {
 
   py::class_<Mesh>(m, "Mesh")
       .def(py::init<>())
+      // checkpoint / resume: current vertices, triangles, the rest state as
+      // computed at initialisation (kept, not recomputed) and the material
+      .def(py::pickle(
+          [](const Mesh& me) {
+            py::array_t<int32_t> tr(py::ssize_t(me.tris.size())), ed(py::ssize_t(me.edges.size()));
+            std::copy(me.tris.begin(), me.tris.end(), tr.mutable_data());
+            std::copy(me.edges.begin(), me.edges.end(), ed.mutable_data());
+            py::array_t<double> dm(py::ssize_t(me.dm_inv.size())), ar(py::ssize_t(me.areas.size()));
+            std::copy(me.dm_inv.begin(), me.dm_inv.end(), dm.mutable_data());
+            std::copy(me.areas.begin(), me.areas.end(), ar.mutable_data());
+            const Material& mt = me.material;
+            return py::make_tuple(v3_array64(me.vertices), tr, ed, dm, ar,
+                                  py::make_tuple(mt.youngs_modulus, mt.poisson_ratio, mt.density, mt.thickness, mt.bending_stiffness));
+          },
+          [](py::tuple t) {
+            if (t.size() != 6) throw std::runtime_error("Mesh: bad pickle");
+            Mesh me;
+            me.vertices = to_v3(t[0], "vertices");
+            auto tr = py::array_t<int32_t, py::array::c_style | py::array::forcecast>::ensure(t[1]);
+            auto ed = py::array_t<int32_t, py::array::c_style | py::array::forcecast>::ensure(t[2]);
+            auto dm = Arr<double>::ensure(t[3]);
+            auto ar = Arr<double>::ensure(t[4]);
+            if (!tr || !ed || !dm || !ar) throw std::runtime_error("Mesh: bad pickle arrays");
+            me.tris.assign(tr.data(), tr.data() + tr.size());
+            me.edges.assign(ed.data(), ed.data() + ed.size());
+            me.dm_inv.assign(dm.data(), dm.data() + dm.size());
+            me.areas.assign(ar.data(), ar.data() + ar.size());
+            if (me.tris.size() % 3 || me.dm_inv.size() != 4 * me.nt() || me.areas.size() != me.nt())
+              throw std::runtime_error("Mesh: inconsistent pickle");
+            for (int32_t q : me.tris) if (q < 0 || size_t(q) >= me.nv()) throw std::runtime_error("Mesh: triangle index out of range");
+            py::tuple mt = t[5].cast<py::tuple>();
+            me.material.youngs_modulus = mt[0].cast<Real>(); me.material.poisson_ratio = mt[1].cast<Real>();
+            me.material.density = mt[2].cast<Real>(); me.material.thickness = mt[3].cast<Real>();
+            me.material.bending_stiffness = mt[4].cast<Real>();
+            me.topo_version = Mesh::next_version(); me.vert_version = Mesh::next_version();
+            return me;
+          }))
       .def("initialize", [](Mesh& me, py::object v, py::object t, const Material& mt) {
         mesh_initialize(me, to_v3(v, "vertices"), to_tris(t, false), mt);
       }, py::arg("vertices"), py::arg("triangles"), py::arg("material"), "Initialize mesh from array-like vertex and triangle data")
@@ -680,10 +732,56 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         auto v = to_v3(p, "velocities");
         if (v.size() != s.nv()) throw py::value_error("velocities must have one row per vertex");
         s.sync_host(); s.v = v; s.host_dirty = true;
-      });
+      })
+      // checkpoint / resume (no reference counterpart: the reference saves no
+      // solver state): FP64 positions, velocities, previous positions, the
+      // CORRECTED step's start and the masses, downloaded if the device is
+      // newer. A restored state uploads them on its first GPU call, so the
+      // next steps continue the saved run.
+      .def(py::pickle(
+          [](State& s) {
+            s.sync_host();
+            py::array_t<double> mass(py::ssize_t(s.nv()));
+            std::copy(s.m.begin(), s.m.end(), mass.mutable_data());
+            return py::make_tuple(v3_array64(s.x), v3_array64(s.v), v3_array64(s.xp),
+                                  v3_array64(s.start.size() == s.nv() ? s.start : s.x), mass);
+          },
+          [](py::tuple t) {
+            if (t.size() != 5) throw std::runtime_error("State: bad pickle");
+            State s;
+            s.x = to_v3(t[0], "positions"); s.v = to_v3(t[1], "velocities"); s.xp = to_v3(t[2], "positions_prev");
+            s.start = to_v3(t[3], "start");
+            auto mass = Arr<double>::ensure(t[4]);
+            if (!mass || size_t(mass.size()) != s.x.size() || s.v.size() != s.x.size() || s.xp.size() != s.x.size() || s.start.size() != s.x.size())
+              throw std::runtime_error("State: inconsistent pickle");
+            s.m.assign(mass.data(), mass.data() + mass.size());
+            s.dev_x = s.dev_v = s.start_stale = false; s.host_dirty = true; s.masses_dirty = true;
+            return s;
+          }));
 
   py::class_<Constraints>(m, "Constraints")
       .def(py::init<>())
+      // checkpoint / resume: every pin and wall with its active flag, in order
+      .def(py::pickle(
+          [](const Constraints& c) {
+            py::list pins, walls;
+            for (auto& p : c.pins) pins.append(py::make_tuple(p.vertex, p.target.x, p.target.y, p.target.z, p.active));
+            for (auto& w : c.walls) walls.append(py::make_tuple(w.normal.x, w.normal.y, w.normal.z, w.offset, w.gap, w.active));
+            return py::make_tuple(pins, walls);
+          },
+          [](py::tuple t) {
+            if (t.size() != 2) throw std::runtime_error("Constraints: bad pickle");
+            Constraints c;
+            for (auto it : t[0].cast<py::list>()) {
+              py::tuple q = it.cast<py::tuple>();
+              c.pins.push_back({q[0].cast<int32_t>(), V3{q[1].cast<double>(), q[2].cast<double>(), q[3].cast<double>()}, q[4].cast<bool>()});
+            }
+            for (auto it : t[1].cast<py::list>()) {
+              py::tuple q = it.cast<py::tuple>();
+              c.walls.push_back({V3{q[0].cast<double>(), q[1].cast<double>(), q[2].cast<double>()}, q[3].cast<double>(), q[4].cast<double>(), q[5].cast<bool>()});
+            }
+            return c;
+          }))
       .def("add_pin", [](Constraints& c, int32_t i, py::object t) { c.pins.push_back({i, to_vec3(t, "pin target must be a 3D vector"), true}); })
       .def("add_wall", [](Constraints& c, py::object n, Real off, Real gap) {
         c.walls.push_back({normalized(to_vec3(n, "wall normal must be a 3D vector")), double(off), double(gap), true});
@@ -786,6 +884,7 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         std::vector<ando_rigid> ab;
         for (auto* b : h) ab.push_back(b->to_abi());
         int32_t rc;
+        s.contact_list = 0;               // the step replaces the device contact list
         {
           py::gil_scoped_release nogil;
           rc = ando_step(s.ctx, &ap, pins.data(), int32_t(pins.size()), walls.data(), int32_t(walls.size()),
@@ -823,19 +922,38 @@ PYBIND11_MODULE(ando_barrier_core, m) {
       .def_readonly("num_contacts", &EnergyDiagnostics::num_contacts).def_readonly("num_pins", &EnergyDiagnostics::num_pins)
       .def("update_drift", &EnergyDiagnostics::update_drift);
 
-  // energy_tracker.cpp:6-76 on the host copy of the state
+  // energy_tracker.cpp:6-76: reduced on the device when it holds the state
+  // (ando_state_moments, no download), else over the host copy
   struct EnergyTracker {};
-  auto ke = [](State& s) { s.sync_host(); double e = 0; for (size_t i = 0; i < s.nv(); ++i) e += 0.5 * s.m[i] * dot(s.v[i], s.v[i]); return e; };
-  auto lm = [](State& s) { s.sync_host(); V3 p{}; for (size_t i = 0; i < s.nv(); ++i) p = add(p, mul(s.v[i], s.m[i])); return p; };
-  auto am = [](State& s) { s.sync_host(); V3 a{}; for (size_t i = 0; i < s.nv(); ++i) a = add(a, cross(s.x[i], mul(s.v[i], s.m[i]))); return a; };
-  auto mvel = [](State& s) { s.sync_host(); double mv = 0; for (size_t i = 0; i < s.nv(); ++i) mv = std::max(mv, norm(s.v[i])); return mv; };
+  auto moments = [](State& s) {
+    ando_moments mo{};
+    if (s.device_current()) { check(ando_state_moments(s.ctx, &mo), "state moments"); return mo; }
+    s.sync_host();
+    double v2max = 0;
+    for (size_t i = 0; i < s.nv(); ++i) {
+      V3 p = mul(s.v[i], s.m[i]), L = cross(s.x[i], p);
+      mo.kinetic_energy += 0.5 * s.m[i] * dot(s.v[i], s.v[i]);
+      mo.linear_momentum[0] += p.x; mo.linear_momentum[1] += p.y; mo.linear_momentum[2] += p.z;
+      mo.angular_momentum[0] += L.x; mo.angular_momentum[1] += L.y; mo.angular_momentum[2] += L.z;
+      v2max = std::max(v2max, dot(s.v[i], s.v[i]));
+    }
+    mo.max_speed = std::sqrt(v2max);
+    return mo;
+  };
+  auto ke = [moments](State& s) { return moments(s).kinetic_energy; };
+  auto lm = [moments](State& s) { ando_moments mo = moments(s); return V3{mo.linear_momentum[0], mo.linear_momentum[1], mo.linear_momentum[2]}; };
+  auto am = [moments](State& s) { ando_moments mo = moments(s); return V3{mo.angular_momentum[0], mo.angular_momentum[1], mo.angular_momentum[2]}; };
+  auto mvel = [moments](State& s) { return moments(s).max_speed; };
   py::class_<EnergyTracker>(m, "EnergyTracker")
       .def(py::init<>())
-      .def_static("compute", [ke, lm, am, mvel](const Mesh& me, State& s, const Constraints& c, const SimParams&) {
+      .def_static("compute", [moments](const Mesh& me, State& s, const Constraints& c, const SimParams&) {
         EnergyDiagnostics d;
-        d.kinetic_energy = float(ke(s)); d.elastic_energy = float(elastic_energy(me)); d.barrier_energy = 0;
+        ando_moments mo = moments(s);
+        d.kinetic_energy = float(mo.kinetic_energy); d.elastic_energy = float(elastic_energy(me)); d.barrier_energy = 0;
         d.total_energy = d.kinetic_energy + d.elastic_energy + d.barrier_energy;
-        d.linear_momentum = lm(s); d.angular_momentum = am(s); d.max_velocity = float(mvel(s));
+        d.linear_momentum = V3{mo.linear_momentum[0], mo.linear_momentum[1], mo.linear_momentum[2]};
+        d.angular_momentum = V3{mo.angular_momentum[0], mo.angular_momentum[1], mo.angular_momentum[2]};
+        d.max_velocity = float(mo.max_speed);
         int nw = 0; for (auto& w : c.walls) nw += w.active;
         int np = 0; for (auto& p : c.pins) np += p.active;
         d.num_contacts = 0 * nw; d.num_pins = np;
@@ -862,7 +980,10 @@ PYBIND11_MODULE(ando_barrier_core, m) {
       .def_readonly("is_stable", &CollisionMetrics::is_stable)
       .def("quality_level", &CollisionMetrics::quality_level).def("quality_description", &CollisionMetrics::quality_description);
 
-  // collision_validator.cpp:7-221 on the host
+  // collision_validator.cpp:7-221. A list that compute_contacts returned for
+  // this state, unchanged and still the one the device holds, is reduced on
+  // the device (ando_collision_metrics: no contact or state download); any
+  // other list is read on the host, with the state's velocities downloaded.
   struct CollisionValidator {};
   py::class_<CollisionValidator>(m, "CollisionValidator")
       .def(py::init<>())
@@ -870,6 +991,26 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         CollisionMetrics M;
         M.ccd_enabled = ccd;
         M.num_total_contacts = int(cs.size());
+        bool on_device = !cs.empty() && s.device_current() && s.contact_list != 0 && cs.size() == s.contact_count;
+        for (size_t k = 0; on_device && k < cs.size(); ++k) on_device = cs[k].list == s.contact_list && cs[k].pos == int32_t(k);
+        if (on_device) {
+          ando_metrics d{};
+          check(ando_collision_metrics(s.ctx, double(gap_max), ccd ? 1 : 0, &d), "collision metrics");
+          const int n = d.num_total_contacts;
+          M.num_point_triangle = d.num_point_triangle; M.num_edge_edge = d.num_edge_edge; M.num_wall = d.num_wall;
+          M.min_gap = Real(d.min_gap); M.max_gap = Real(d.max_gap); M.avg_gap = Real(d.sum_gap / n);
+          M.num_penetrations = d.num_penetrations;
+          M.max_penetration = Real(d.max_penetration);
+          if (d.num_penetrations > 0) { M.avg_penetration = Real(d.sum_penetration / d.num_penetrations); M.is_stable = false; }
+          M.has_major_penetration = d.num_major_penetrations > 0; M.has_tunneling = d.num_tunneling > 0;
+          M.num_ccd_contacts = d.num_ccd_contacts; M.num_broad_phase_contacts = n - d.num_ccd_contacts;
+          M.ccd_effectiveness = (ccd && n > 0) ? Real(d.num_ccd_contacts) / Real(n) * 100.0f : 0.0f;
+          if (d.num_relative_velocities > 0) {
+            M.max_relative_velocity = Real(d.max_relative_velocity);
+            M.avg_relative_velocity = Real(d.sum_relative_velocity / d.num_relative_velocities);
+          }
+          return M;
+        }
         if (!cs.empty()) {
           M.min_gap = M.max_gap = float(cs[0].c.gap);
           Real sum_gap = 0, sum_pen = 0;
@@ -880,13 +1021,13 @@ PYBIND11_MODULE(ando_barrier_core, m) {
             M.min_gap = std::min(M.min_gap, g); M.max_gap = std::max(M.max_gap, g); sum_gap += g;
             if (g < 0) {
               M.num_penetrations++; Real pen = -g; M.max_penetration = std::max(M.max_penetration, pen); sum_pen += pen;
-              if (pen > 0.001f) M.has_major_penetration = true;
-              if (pen > 0.1f * gap_max) M.has_tunneling = true;
+              if (pen > 0.001) M.has_major_penetration = true;
+              if (pen > 0.1 * gap_max) M.has_tunneling = true;
             }
           }
           M.avg_gap = sum_gap / M.num_total_contacts;
           if (M.num_penetrations > 0) { M.avg_penetration = sum_pen / M.num_penetrations; M.is_stable = false; }
-          for (auto& C : cs) { if (ccd && float(C.c.gap) < gap_max * 0.5f) M.num_ccd_contacts++; else M.num_broad_phase_contacts++; }
+          for (auto& C : cs) { if (ccd && float(C.c.gap) < gap_max * 0.5) M.num_ccd_contacts++; else M.num_broad_phase_contacts++; }
           M.ccd_effectiveness = (ccd && M.num_total_contacts > 0) ? Real(M.num_ccd_contacts) / Real(M.num_total_contacts) * 100.0f : 0.0f;
           s.sync_host();
           std::vector<Real> rv;
@@ -909,6 +1050,14 @@ PYBIND11_MODULE(ando_barrier_core, m) {
         }
         return M;
       }, py::arg("mesh"), py::arg("state"), py::arg("contacts"), py::arg("gap_max"), py::arg("ccd_enabled"), "Compute comprehensive collision metrics")
+      // not in the reference's binding: the discrete check no contact list can give
+      .def_static("edge_triangle_crossings", [](const Mesh& me, State& s) {
+        s.bind(me);
+        int64_t n = 0;
+        check(ando_edge_triangle_crossings(s.ctx, &n), "edge_triangle_crossings");
+        return n;
+      }, py::arg("mesh"), py::arg("state"),
+         "Mesh edges whose segment passes through a triangle they share no vertex with (exact test on the GPU)")
       .def_static("has_penetrations", [](const std::vector<Contact>& cs) { for (auto& C : cs) if (C.c.gap < 0) return true; return false; })
       .def_static("max_penetration_depth", [](const std::vector<Contact>& cs) { Real m = 0; for (auto& C : cs) if (C.c.gap < 0) m = std::max(m, float(-C.c.gap)); return m; });
 
@@ -929,7 +1078,17 @@ PYBIND11_MODULE(ando_barrier_core, m) {
     Real r = float(std::sqrt(std::max(best, 0.0)));
     return std::isfinite(r) ? r : 0;
   };
+  // velocities: the reference's flat 3N array, or a State (its device
+  // velocities are reduced on the device, ando_state_moments)
   auto max_vel = [](py::object v) -> Real {
+    if (py::isinstance<State>(v)) {
+      State& st = v.cast<State&>();
+      if (st.device_current()) { ando_moments mo{}; check(ando_state_moments(st.ctx, &mo), "state moments"); return float(mo.max_speed); }
+      st.sync_v();
+      double mx = 0;
+      for (auto& q : st.v) mx = std::max(mx, double(float(q.x * q.x + q.y * q.y + q.z * q.z)));
+      return float(std::sqrt(mx));
+    }
     auto a = Arr<float>::ensure(v);
     double mx = 0; py::ssize_t n = a.size() / 3;
     for (py::ssize_t i = 0; i < n; ++i) { double x = a.data()[3 * i], y = a.data()[3 * i + 1], z = a.data()[3 * i + 2]; mx = std::max(mx, double(float(x * x + y * y + z * z))); }

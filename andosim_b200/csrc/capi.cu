@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <unordered_map>
 #include <unordered_set>
 #include <string>
 #include <vector>
@@ -25,6 +26,7 @@
 #include <thrust/iterator/counting_iterator.h>
 
 #include "../../include/ando_gpu.h"
+#include "diag.cuh"
 #include "kernels.cuh"
 #include "lbvh.cuh"
 #include "learned.cuh"
@@ -72,6 +74,8 @@ struct ando_ctx_s {
 
   DevBuf<int> tris, rowptr, cols, slot_row, diag_slot, face_slot, slot_cptr, slot_contrib, vf_ptr, vf;
   DevBuf<double> rest_area, dm_inv, mass, el_a, el_b, g_el, mesh_x;
+  DevBuf<double> bend_q;           // quadratic bending Hessian coefficient per slot (bending_stiffness > 0)
+  bool bending = false;
   DevBuf<double> x, v, x_prev, x_old, x_hat, g, g_const, diag_const, diag_extra;
   DevBuf<float> b, d, r, z, p0, p1, Ap, val, precond;
   DevBuf<unsigned char> sflags;
@@ -174,6 +178,15 @@ struct ando_ctx_s {
   DevBuf<int> vorder, eorder;      // vertices / edges in Morton order of their rest positions (query order)
   int E = 0;
   Lbvh bvh_tri, bvh_edge;
+  // diagnostics (diag.cu): per-block partials and totals of the validator
+  // metrics and state moments; a triangle hierarchy of its own for the
+  // crossing count, so the step's hierarchies and candidate lists stay valid
+  DevBuf<MetricSums> metric_parts, metric_out;
+  DevBuf<MomentSums> moment_parts, moment_out;
+  Lbvh bvh_check;
+  DevBuf<int2> cross_scratch;
+  DevBuf<int> cross_counter;
+  DevBuf<unsigned long long> cross_total;
   DevBuf<int2> pairs, pair_scratch, pair_scratch_ee;
   DevBuf<int2> toi_scratch, toi_scratch_ee;  // candidates of the time-of-impact passes (grown on overflow)
   DevBuf<unsigned long long> pk0, pk1;
@@ -216,6 +229,7 @@ struct ando_ctx_s {
     m.rowptr = rowptr.p; m.cols = cols.p; m.slot_row = slot_row.p; m.diag_slot = diag_slot.p;
     m.face_slot = face_slot.p; m.slot_cptr = slot_cptr.p; m.slot_contrib = slot_contrib.p;
     m.vf_ptr = vf_ptr.p; m.vf = vf.p; m.el_a = el_a.p; m.el_b = el_b.p; m.g_elastic = g_el.p;
+    m.bend_q = bending ? bend_q.p : nullptr;
     return m;
   }
 
@@ -270,6 +284,56 @@ struct Phase {
 }  // namespace
 
 namespace {
+
+// One interior edge of the quadratic bending energy: its ends, then the
+// vertex opposite it in each of its two faces; w the cotangent stencil over
+// them at rest; c = 6 k_b / (rest area of the two faces).
+struct Hinge { int v[4]; double w[4]; double c; };
+
+// Quadratic bending of CORRECTED semantics (no reference counterpart: the
+// reference declares Material::bending_stiffness, types.h:56, and never reads
+// it). For each edge shared by exactly two faces (ends i, j; opposite vertices
+// k, l) the rest-state stencil
+//   K = [cot a_j + cot b_j, cot a_i + cot b_i, -(cot a_i + cot a_j), -(cot b_i + cot b_j)]
+// (a_*: angles of the first face at i, j; b_*: of the second) annihilates
+// every affine map of a flat rest sheet, and E = k_b sum_e 3 / A_e |K_e x|^2
+// is the discrete-shell hinge energy k_b sum_e 3 |e|^2 / A_e t_e^2 of an
+// isometric fold t_e, to second order (Bergou, Wardetzky, Harmon, Zorin,
+// Grinspun, "A Quadratic Bending Model for Inextensible Surfaces", SGP
+// 2006). Its Hessian c K K^T (x) I3 is constant and positive semidefinite.
+// The rest shape is taken as flat; edges with a degenerate face are skipped.
+std::vector<Hinge> bending_hinges(const double* x, const int* tris, int T, const double* rest_areas, double kb) {
+  std::unordered_map<unsigned long long, std::vector<std::pair<int, int>>> faces_of;  // edge -> (face, opposite vertex)
+  std::vector<unsigned long long> order;                                            // edges in first-seen order
+  for (int f = 0; f < T; ++f)
+    for (int e = 0; e < 3; ++e) {
+      int a = tris[3 * f + e], b = tris[3 * f + (e + 1) % 3], o = tris[3 * f + (e + 2) % 3];
+      unsigned long long key = ((unsigned long long)(unsigned)std::min(a, b) << 32) | (unsigned)std::max(a, b);
+      auto& l = faces_of[key];
+      if (l.empty()) order.push_back(key);
+      l.push_back({f, o});
+    }
+  auto cot = [&](int at, int p, int q, bool& ok) {
+    double u[3], w[3];
+    for (int k = 0; k < 3; ++k) { u[k] = x[3ll * p + k] - x[3ll * at + k]; w[k] = x[3ll * q + k] - x[3ll * at + k]; }
+    double c0 = u[1] * w[2] - u[2] * w[1], c1 = u[2] * w[0] - u[0] * w[2], c2 = u[0] * w[1] - u[1] * w[0];
+    double s = std::sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    if (!(s > 0.0)) { ok = false; return 0.0; }
+    return (u[0] * w[0] + u[1] * w[1] + u[2] * w[2]) / s;
+  };
+  std::vector<Hinge> out;
+  for (unsigned long long key : order) {
+    const auto& l = faces_of[key];
+    if (l.size() != 2) continue;
+    int i = int(key >> 32), j = int(key & 0xffffffffu), k = l[0].second, m = l[1].second;
+    bool ok = true;
+    double ai = cot(i, j, k, ok), aj = cot(j, i, k, ok), bi = cot(i, j, m, ok), bj = cot(j, i, m, ok);
+    double area = rest_areas[l[0].first] + rest_areas[l[1].first];
+    if (!ok || !(area > 0.0)) continue;
+    out.push_back(Hinge{{i, j, k, m}, {aj + bj, ai + bi, -(ai + aj), -(bi + bj)}, 6.0 * kb / area});
+  }
+  return out;
+}
 
 // Indices of n points sorted by the 63-bit Morton code of their position in
 // the points' bounding box (ties by index).
@@ -1319,12 +1383,16 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
     return fail(ANDO_ERR_INVALID, "mesh arrays");
   for (long long k = 0; k < 3ll * T; ++k)
     if (tris[k] < 0 || tris[k] >= V) return fail(ANDO_ERR_INVALID, "triangle index out of range");
-  // Static block pattern: self blocks plus every (a, b) vertex pair of every face.
+  // Static block pattern: self blocks plus every (a, b) vertex pair of every
+  // face, and with bending the two vertices opposite each interior edge.
+  std::vector<Hinge> hinges;
+  if (mat->bending_stiffness > 0.0) hinges = bending_hinges(vertices, tris, T, rest_areas, mat->bending_stiffness);
   std::vector<std::vector<int>> adj(V);
   for (int i = 0; i < V; ++i) adj[i].push_back(i);
   for (int f = 0; f < T; ++f)
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) adj[tris[3 * f + a]].push_back(tris[3 * f + b]);
+  for (const Hinge& h : hinges) { adj[h.v[2]].push_back(h.v[3]); adj[h.v[3]].push_back(h.v[2]); }
   std::vector<int> rowptr(V + 1, 0), cols, slot_row, diag_slot(V);
   for (int i = 0; i < V; ++i) {
     auto& r = adj[i];
@@ -1375,6 +1443,11 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   std::vector<int> slotT(nnzb);
   for (int r = 0; r < V; ++r)
     for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) slotT[k] = slot_of(cols[k], r);
+  // bending Hessian per slot: q = sum over the hinges holding (a, b) of c w_a w_b
+  std::vector<double> bq(hinges.empty() ? 0 : nnzb, 0.0);
+  for (const Hinge& h : hinges)
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) bq[slot_of(h.v[a], h.v[b])] += h.c * h.w[a] * h.w[b];
   // SELL-32: chunks of 32 rows padded to the chunk's longest row
   const int nch = (V + 31) / 32;
   std::vector<int> choff(nch + 1, 0);
@@ -1421,6 +1494,8 @@ int32_t ando_mesh_upload(ando_ctx c, const double* vertices, int32_t V, const in
   CK(c->vf_ptr.upload(vfp.data(), V + 1, s));
   CK(c->vf.upload(vfl.data(), 3ull * T, s));
   CK(c->mesh_x.upload(vertices, 3ull * V, s));
+  c->bending = !hinges.empty();
+  if (c->bending) CK(c->bend_q.upload(bq.data(), nnzb, s));
   c->E = int(edges.size() / 2);
   CK(c->edges.upload(edges.data(), edges.size(), s));
   {
@@ -1786,6 +1861,67 @@ int32_t ando_compute_contacts_corrected(ando_ctx c, double gap_max, const ando_r
   rc = detect_corrected(c, num_rigids, gap_max);
   if (rc) return rc;
   return contacts_out(c, out, capacity, num_out);
+}
+
+int32_t ando_collision_metrics(ando_ctx c, double gap_max, int32_t ccd_enabled, ando_metrics* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out) return fail(ANDO_ERR_INVALID, "metrics output");
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  std::memset(out, 0, sizeof(*out));
+  if (c->ncontacts == 0) return ANDO_OK;
+  CK(c->metric_parts.reserve(DIAG_MAX_BLOCKS));
+  CK(c->metric_out.reserve(1));
+  launch_contact_metrics(c->contacts.p, c->ncontacts, c->v.p, gap_max, ccd_enabled ? 1 : 0, c->metric_parts.p, c->metric_out.p, c->stream);
+  CK(cudaGetLastError());
+  MetricSums h;
+  CK(cudaMemcpyAsync(&h, c->metric_out.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  out->num_total_contacts = h.n; out->num_point_triangle = h.n_pt; out->num_edge_edge = h.n_ee; out->num_wall = h.n_wall;
+  out->num_penetrations = h.n_pen; out->num_major_penetrations = h.n_major; out->num_tunneling = h.n_tunnel;
+  out->num_ccd_contacts = h.n_ccd; out->num_relative_velocities = h.n_rv;
+  out->min_gap = h.min_gap; out->max_gap = h.max_gap; out->sum_gap = h.sum_gap;
+  out->max_penetration = h.max_pen; out->sum_penetration = h.sum_pen;
+  out->max_relative_velocity = h.max_rv; out->sum_relative_velocity = h.sum_rv;
+  return ANDO_OK;
+}
+
+int32_t ando_state_moments(ando_ctx c, ando_moments* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out) return fail(ANDO_ERR_INVALID, "moments output");
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  CK(c->moment_parts.reserve(DIAG_MAX_BLOCKS));
+  CK(c->moment_out.reserve(1));
+  launch_state_moments(c->V, c->x.p, c->v.p, c->mass.p, c->moment_parts.p, c->moment_out.p, c->stream);
+  CK(cudaGetLastError());
+  MomentSums h;
+  CK(cudaMemcpyAsync(&h, c->moment_out.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  out->kinetic_energy = h.ke;
+  for (int k = 0; k < 3; ++k) { out->linear_momentum[k] = h.p[k]; out->angular_momentum[k] = h.L[k]; }
+  out->max_speed = std::sqrt(h.vmax2);
+  return ANDO_OK;
+}
+
+int32_t ando_edge_triangle_crossings(ando_ctx c, int64_t* crossings) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!crossings) return fail(ANDO_ERR_INVALID, "crossings output");
+  if (!c->mesh_ready || !c->state_ready) return fail(ANDO_ERR_STATE, "mesh/state not uploaded");
+  *crossings = 0;
+  if (c->T == 0 || c->E == 0) return ANDO_OK;
+  cudaStream_t s = c->stream;
+  // a fresh hierarchy over the triangles at x; edges query it in the Morton
+  // order of their rest midpoints. The 10 um pad only adds candidates: it
+  // covers the rounding of the single-precision boxes, and the exact test
+  // decides every pair.
+  CK(c->bvh_check.build(c->x.p, nullptr, c->tris.p, 3, c->T, 0.f, c->cub_tmp, s));
+  c->bvh_check.qorder = c->eorder.p;
+  long long n = 0;
+  CK(c->bvh_check.count_crossings(c->x.p, c->edges.p, c->E, 1e-5f, c->cross_scratch, c->cross_counter, c->cross_total, &n, s));
+  *crossings = n;
+  return ANDO_OK;
 }
 
 namespace {

@@ -99,6 +99,9 @@ struct MeshDev {
   const double* el_a;       // nnzb elastic in-plane coefficient of the diag(a,a,b) block
   const double* el_b;       // nnzb elastic third-axis coefficient
   const double* g_elastic;  // 3V  elastic gradient on the mesh vertices (constant)
+  // nnzb coefficient q of the quadratic bending Hessian q I3 per slot
+  // (CORRECTED semantics, bending_stiffness > 0; null without bending)
+  const double* bend_q;
 };
 
 // Strain-limit data of one face and one singular value.

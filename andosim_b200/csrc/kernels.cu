@@ -72,6 +72,9 @@ __global__ void k_elastic_slots(MeshDev m, double mu, double thickness, int sema
       A += c; B += c;
     }
   }
+  // CORRECTED: the constant Hessian of the quadratic bending energy joins the
+  // elastic blocks (and with them the elasticity-inclusive stiffnesses)
+  if (semantics != 0 && m.bend_q) { A += m.bend_q[s]; B += m.bend_q[s]; }
   el_a[s] = A; el_b[s] = B;
 }
 
@@ -469,6 +472,16 @@ __global__ void k_arap_gradient(MeshDev m, const double* X, double mu, double th
     d3 P0 = (F0 - R0) * tk, P1 = (F1 - R1) * tk;
     double G0 = a == 0 ? -(da + dc) : (a == 1 ? da : dc), G1 = a == 0 ? -(db + dd) : (a == 1 ? db : dd);
     acc = acc + P0 * G0 + P1 * G1;
+  }
+  // quadratic bending: row i of Q x, taken as sum_j q_ij (x_j - x_i) (the
+  // rows of Q sum to zero), which keeps the cancellation of a nearly flat
+  // sheet away from the absolute coordinates
+  if (m.bend_q) {
+    const d3 xi = ld3(X, i);
+    for (int k = m.rowptr[i]; k < m.rowptr[i + 1]; ++k) {
+      const double q = m.bend_q[k];
+      if (q != 0.0) acc = acc + (ld3(X, m.cols[k]) - xi) * q;
+    }
   }
   st3(g, i, acc);
 }

@@ -446,7 +446,8 @@ __device__ inline void emit(bool hit, int q, int prim, int2* out, int* count, in
 
 // One thread per query. kind 0: query = vertex (point box +-1e-4 inflated by
 // pad), prims = triangles, skip incident triangles. kind 1: query = edge,
-// prims = edges, keep e1 < e2 without shared vertex.
+// prims = edges, keep e1 < e2 without shared vertex. kind 2: query = edge,
+// prims = triangles, skip triangles that hold either end of the edge.
 __global__ void k_query(const double* x, const double* x1, const int* qprims, const int* qorder, int kind, int nq, float pad, int n,
                         const int4* leafv, const int* rank, const LbvhWide* wide, const Box* nodes, int2* out, int* count, int cap) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -498,6 +499,7 @@ __global__ void k_query(const double* x, const double* x1, const int* qprims, co
     const int4 lv = leafv[pos];
     bool hit;
     if (kind == 0) hit = lv.y != q && lv.z != q && lv.w != q;
+    else if (kind == 2) hit = lv.y != qa && lv.y != qc && lv.z != qa && lv.z != qc && lv.w != qa && lv.w != qc;
     else hit = pos > qpos && lv.y != qa && lv.y != qc && lv.z != qa && lv.z != qc;
     return hit ? lv.x : -1;
   };
@@ -602,6 +604,58 @@ __global__ void k_pairs_toi(const int2* cand, const int* count, int cap, int kin
   }
   t = warp_min(t);
   if ((threadIdx.x & 31) == 0 && t < 1.0) atomic_min_pos(toi, t);
+}
+
+// Exact segment-triangle crossing test in FP64: the segment's ends lie
+// strictly on opposite sides of the triangle's plane and the crossing point
+// has barycentric coordinates in [0, 1]. Every product, sum and quotient is
+// rounded on its own (no fused multiply-add), in the order written, so the
+// test takes the same decision as the same formula in plain IEEE double
+// arithmetic on the host.
+__device__ inline bool segment_crosses_triangle(const double* x, int p, int q, int a, int b, int c) {
+  auto mul = [](double u, double v) { return __dmul_rn(u, v); };
+  auto add = [](double u, double v) { return __dadd_rn(u, v); };
+  auto sub = [](double u, double v) { return __dsub_rn(u, v); };
+  double A[3], u[3], w[3], P[3], Q[3];
+  for (int k = 0; k < 3; ++k) {
+    A[k] = x[3 * a + k];
+    u[k] = sub(x[3 * b + k], A[k]);
+    w[k] = sub(x[3 * c + k], A[k]);
+    P[k] = x[3 * p + k];
+    Q[k] = x[3 * q + k];
+  }
+  const double n0 = sub(mul(u[1], w[2]), mul(u[2], w[1]));
+  const double n1 = sub(mul(u[2], w[0]), mul(u[0], w[2]));
+  const double n2 = sub(mul(u[0], w[1]), mul(u[1], w[0]));
+  const double s0 = add(add(mul(n0, sub(P[0], A[0])), mul(n1, sub(P[1], A[1]))), mul(n2, sub(P[2], A[2])));
+  const double s1 = add(add(mul(n0, sub(Q[0], A[0])), mul(n1, sub(Q[1], A[1]))), mul(n2, sub(Q[2], A[2])));
+  if (!((s0 > 0.0 && s1 < 0.0) || (s0 < 0.0 && s1 > 0.0))) return false;
+  const double t = __ddiv_rn(s0, sub(s0, s1));
+  double X[3];
+  for (int k = 0; k < 3; ++k) X[k] = sub(add(P[k], mul(t, sub(Q[k], P[k]))), A[k]);
+  auto dot3 = [&](const double* e, const double* f) { return add(add(mul(e[0], f[0]), mul(e[1], f[1])), mul(e[2], f[2])); };
+  const double uu = dot3(u, u), uw = dot3(u, w), ww = dot3(w, w), xu = dot3(X, u), xw = dot3(X, w);
+  const double den = sub(mul(uu, ww), mul(uw, uw));
+  if (!(fabs(den) > 0.0)) return false;
+  const double bv = __ddiv_rn(sub(mul(ww, xu), mul(uw, xw)), den);
+  const double bw = __ddiv_rn(sub(mul(uu, xw), mul(uw, xu)), den);
+  return bv >= 0.0 && bw >= 0.0 && add(bv, bw) <= 1.0;
+}
+
+// Crossings among the (edge, triangle) candidates of a kind-2 traversal,
+// summed into *crossings; nothing when the list overflowed its capacity (the
+// caller reads count[0], grows the list and runs again).
+__global__ void k_pairs_cross(const int2* cand, const int* count, int cap, const int* tris, const int* edges, const double* x,
+                              unsigned long long* crossings) {
+  if (count[0] > cap) return;
+  const int n = count[0];
+  unsigned long long mine = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int2 pr = cand[i];
+    mine += segment_crosses_triangle(x, edges[2 * pr.x], edges[2 * pr.x + 1], tris[3 * pr.y], tris[3 * pr.y + 1], tris[3 * pr.y + 2]);
+  }
+  for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(crossings, mine);
 }
 
 __global__ void k_pair_keys(const int2* pairs, int n, unsigned long long* keys) {
@@ -840,6 +894,38 @@ cudaError_t Lbvh::contacts_from(const double* x, int kind, const int* qprims, do
   k_pairs_gap<<<NARROW_GRID, TPB, 0, s>>>(cand.p, counter.p, int(cand.n), kind, prims, qprims, x, gap, surv.p, counter.p + 2);
   launches += 1;
   return cudaGetLastError();
+}
+
+// Edge-triangle crossings at x over this triangle hierarchy (built at x):
+// queries are the ne edges (their boxes inflated by pad, which only adds
+// candidates for the exact test). One host round trip per attempt; the
+// candidate list grows once if it overflowed.
+cudaError_t Lbvh::count_crossings(const double* x, const int* edges, int ne, float pad, DevBuf<int2>& scratch, DevBuf<int>& counter,
+                                  DevBuf<unsigned long long>& total, long long* crossings, cudaStream_t s) {
+  cudaError_t e;
+  *crossings = 0;
+  if (n == 0 || ne == 0) return cudaSuccess;
+  if ((e = counter.reserve(3))) return e;
+  if ((e = total.reserve(1))) return e;
+  if (scratch.n < 1024) if ((e = scratch.reserve(1024))) return e;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const int cap = int(scratch.n);
+    if ((e = cudaMemsetAsync(counter.p, 0, 3 * sizeof(int), s))) return e;
+    if ((e = cudaMemsetAsync(total.p, 0, sizeof(unsigned long long), s))) return e;
+    k_query<<<nblk(ne), TPB, 0, s>>>(x, nullptr, edges, qorder, 2, ne, pad, n, leafv.p, rank.p, wide.p, nodes.p, scratch.p, counter.p, cap);
+    k_pairs_cross<<<NARROW_GRID, TPB, 0, s>>>(scratch.p, counter.p, cap, prims, edges, x, total.p);
+    launches += 2;
+    int cnt2[2] = {0, 0};
+    unsigned long long got = 0;
+    if ((e = cudaMemcpyAsync(cnt2, counter.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaMemcpyAsync(&got, total.p, sizeof(got), cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaStreamSynchronize(s))) return e;
+    if (cnt2[1]) return cudaErrorLaunchOutOfResources;  // traversal stack overflow (cannot happen with unique keys)
+    if (cnt2[0] < 0 || cnt2[0] > (1 << 26)) return cudaErrorMemoryAllocation;
+    if (cnt2[0] <= cap) { *crossings = (long long)got; return cudaSuccess; }
+    if ((e = scratch.reserve(size_t(cnt2[0]) + size_t(cnt2[0]) / 4))) return e;
+  }
+  return cudaErrorMemoryAllocation;
 }
 
 }  // namespace ando

@@ -60,7 +60,8 @@ struct Lbvh {
   // full build once per caller epoch, refit otherwise
   cudaError_t update(const double* x, const double* x1, const int* prims, int arity, int n, float pad, long long epoch,
                      DevBuf<unsigned char>& tmp, cudaStream_t s);
-  // kind 0: vertices against triangles; kind 1: edges against edges.
+  // kind 0: vertices against triangles; kind 1: edges against edges; kind 2:
+  // edges against triangles (count_crossings).
   // Sorted candidate pairs (boxes overlap) in `out`, their number in *npairs.
   cudaError_t query(const double* x, const double* x1, int kind, const int* qprims, int nq, float pad, DevBuf<int2>& out, DevBuf<int2>& scratch,
                     DevBuf<unsigned long long>& k0, DevBuf<unsigned long long>& k1, DevBuf<int>& counter,
@@ -96,6 +97,12 @@ struct Lbvh {
   // contact query's.
   cudaError_t contacts_from(const double* x, int kind, const int* qprims, double gap, DevBuf<int2>& cand, DevBuf<int>& counter,
                             cudaStream_t s);
+  // Edge-triangle crossings at x (this hierarchy is over triangles, built at
+  // x): the (edge, triangle) pairs that share no vertex and where the edge's
+  // segment passes through the triangle, by an exact FP64 test of every
+  // candidate whose boxes (the edge's inflated by pad) overlap.
+  cudaError_t count_crossings(const double* x, const int* edges, int ne, float pad, DevBuf<int2>& scratch, DevBuf<int>& counter,
+                              DevBuf<unsigned long long>& total, long long* crossings, cudaStream_t s);
 };
 
 }  // namespace ando

@@ -312,10 +312,13 @@ def paired_run(args, sc, local, flush, pg, weights, steps=None, raw=False):
             r["launches"] += S.profile()["launches"] - n0
             outs[name] = S.download()[0]
         diffs.append(float(np.abs(outs["learned"] - outs["block_jacobi"]).max() / ext))
+    crossings = S.edge_triangle_crossings()       # untimed: the window's end state, exact test on the GPU
     S.close()
     if raw:
-        return res, diffs, steps
-    return summarize_pair(args, res, diffs, steps, pg)
+        return res, diffs, steps, crossings
+    out = summarize_pair(args, res, diffs, steps, pg)
+    out["edge_triangle_crossings_end"] = crossings
+    return out
 
 
 def summarize_pair(args, res, diffs, steps, pg):
@@ -478,7 +481,8 @@ def c3_run(args, local, seed=0):
 def c2_run(args, local, pg, seed=0):
     """The four-sheet stack (4 x 96 x 96, 200 frames: drop, land, stack), CORRECTED with block Jacobi,
     device-resident; contacts judged every 20 frames by the module's CollisionValidator on the CORRECTED
-    contact set, and the lowest vertex height."""
+    contact set (reduced on the device), the exact edge-triangle crossing count and the lowest vertex
+    height."""
     import torch
 
     from andosim_b200 import abi, ando_barrier_core as abc, scenes
@@ -493,7 +497,7 @@ def c2_run(args, local, pg, seed=0):
     for k, v in sc.params.items():
         setattr(p, k, v)
     p.semantics = "corrected"
-    ms, newton, pcg, contacts, penetrations, zmin, fails = 0.0, 0, 0, 0, 0, 1e9, 0
+    ms, newton, pcg, contacts, penetrations, zmin, fails, crossings = 0.0, 0, 0, 0, 0, 1e9, 0, 0
     c = abc.Constraints()
     for n, o, g in sc.walls:
         c.add_wall(n, o, g)
@@ -507,12 +511,14 @@ def c2_run(args, local, pg, seed=0):
             contacts = max(contacts, len(cs))
             met = abc.CollisionValidator.compute_metrics(m, st, cs, float(p.contact_gap_max), True)
             penetrations += int(met.num_penetrations)
+            crossings += int(abc.CollisionValidator.edge_triangle_crossings(m, st))
             zmin = min(zmin, float(st.get_positions64()[:, 2].min()))
     ms = dist_max(ms, pg)
     return {"workload": "c2_stack_4x96x96", "vertices": sc.num_vertices, "frames": args.c2_frames, "semantics": "CORRECTED",
             "preconditioner": "block_jacobi", "frames_per_s": round(args.c2_frames / (ms * 1e-3), 2),
             "newton_iters_per_frame": round(newton / args.c2_frames, 2), "pcg_iters_per_newton": round(pcg / max(newton, 1), 2),
-            "line_search_fail": fails, "contacts_max": contacts, "validator_penetrations": penetrations, "z_min": zmin,
+            "line_search_fail": fails, "contacts_max": contacts, "validator_penetrations": penetrations,
+            "edge_triangle_crossings": crossings, "z_min": zmin,
             "timing": "CUDA events of each step (device_ms), positions stay on the device",
             "waves": "2 mm (the configured 2 cm waves on sheets 5 mm apart start the stack self-intersecting)"}
 
@@ -536,9 +542,10 @@ def run_ours(args, rank, world, local, pg):
     clocks.start()
     # the paired window over several seeds of the workload: one trajectory's
     # iteration counts depend on which hard Newton systems its frames contain
-    res, diffs, nframes = None, [], 0
+    res, diffs, nframes, crossings = None, [], 0, []
     for sck in scs:
-        r, d, n = paired_run(args, sck, local, flush, pg, weights, raw=True)
+        r, d, n, cr = paired_run(args, sck, local, flush, pg, weights, raw=True)
+        crossings.append(cr)
         if res is None:
             res = r
         else:
@@ -562,7 +569,8 @@ def run_ours(args, rank, world, local, pg):
                 "jacobi": {k: v for k, v in pf["block_jacobi"].items() if k != "total_ms"},
                 "frames_per_s_ratio": round(pf["learned"]["frames_per_s"] / pf["block_jacobi"]["frames_per_s"], 3),
                 "pcg_iters_per_newton_ratio": round(pf["learned"]["pcg_iters_per_newton"] / max(pf["block_jacobi"]["pcg_iters_per_newton"], 1e-9), 3),
-                "step_position_diff_rel_extent": pf["step_position_diff_rel_extent"]}
+                "step_position_diff_rel_extent": pf["step_position_diff_rel_extent"],
+                "edge_triangle_crossings_end": pf["edge_triangle_crossings_end"]}
     prof, nnzb = lp.pop("_prof"), lp.pop("_nnzb")
     peaks = json.loads(PEAKS_FILE.read_text()) if PEAKS_FILE.exists() else {}
     hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
@@ -608,6 +616,9 @@ def run_ours(args, rank, world, local, pg):
                               "pcg_iters_per_newton_ratio": round(lrn["pcg_iters_per_newton"] / max(jac["pcg_iters_per_newton"], 1e-9), 3),
                               "paired": "each frame both preconditioners step from the same state",
                               "step_position_diff_rel_extent": pair["step_position_diff_rel_extent"]},
+        "edge_triangle_crossings": {"end_of_window_per_seed": crossings,
+                                    "check": "mesh edges through a triangle they share no vertex with, exact FP64 test on the GPU "
+                                             "(ando_edge_triangle_crossings), untimed"},
         "profiled_pass": lp,
         "full_length": full,
         "gpu_launches": lrn["gpu_launches"],

@@ -235,6 +235,48 @@ ANDO_API int32_t ando_compute_contacts(ando_ctx ctx, const ando_rigid* rigids, i
 ANDO_API int32_t ando_compute_contacts_corrected(ando_ctx ctx, double gap_max, const ando_rigid* rigids, int32_t num_rigids,
                                                  ando_contact* out, int32_t capacity, int32_t* num_out);
 
+/* CollisionMetrics (collision_validator.h) reduced on the device over the
+ * context's current contact list (the last ando_compute_contacts*, or the
+ * last Newton iteration of a step) and its velocities: counts, extremes and
+ * sums; the averages and flags follow from them (avg_gap = sum_gap /
+ * num_total_contacts, has_major_penetration = num_major_penetrations > 0, and
+ * so on). Gaps are compared in single precision like the reference's Real.
+ * With no contacts every field is zero. */
+typedef struct {
+  int32_t num_total_contacts, num_point_triangle, num_edge_edge, num_wall;
+  int32_t num_penetrations;        /* gap < 0 */
+  int32_t num_major_penetrations;  /* penetration > 1 mm */
+  int32_t num_tunneling;           /* penetration > 0.1 gap_max */
+  int32_t num_ccd_contacts;        /* ccd_enabled and gap < 0.5 gap_max */
+  int32_t num_relative_velocities; /* point-triangle, edge-edge and wall contacts */
+  double min_gap, max_gap, sum_gap, max_penetration, sum_penetration;
+  double max_relative_velocity, sum_relative_velocity;
+} ando_metrics;
+
+/* Replaces CollisionMetrics::compute_from_contacts and
+ * CollisionValidator::compute_metrics / compute_relative_velocities
+ * (collision_validator.cpp:7-111,133-157,179-221) for a contact list that is
+ * still on the device: no contact or state download. */
+ANDO_API int32_t ando_collision_metrics(ando_ctx ctx, double gap_max, int32_t ccd_enabled, ando_metrics* out);
+
+/* Moments of the device state: 1/2 sum m |v|^2, sum m v, sum x cross m v and
+ * max |v|. Replaces EnergyTracker::compute_kinetic_energy /
+ * compute_linear_momentum / compute_angular_momentum / compute_max_velocity
+ * (energy_tracker.cpp:7-42) and AdaptiveTimestep::compute_max_velocity
+ * (adaptive_timestep.cpp:132-149) without a state download. */
+typedef struct {
+  double kinetic_energy, linear_momentum[3], angular_momentum[3], max_speed;
+} ando_moments;
+ANDO_API int32_t ando_state_moments(ando_ctx ctx, ando_moments* out);
+
+/* Discrete intersection count at the current positions: mesh edges whose
+ * segment passes through a triangle they share no vertex with (exact FP64
+ * test over an LBVH of the triangles). No reference counterpart: the
+ * reference's CollisionValidator only reads a contact list and cannot see a
+ * crossing that no contact reports; this is the direct check that a
+ * trajectory stays intersection-free. */
+ANDO_API int32_t ando_edge_triangle_crossings(ando_ctx ctx, int64_t* crossings);
+
 /* Block-sparse (3x3 BSR) system of the most recent Newton iteration, for
  * inspection and for the preconditioner-training dump. Pass NULL pointers to
  * query sizes. rowptr: num_vertices+1; cols: nnzb; vals: 9*nnzb (row-major

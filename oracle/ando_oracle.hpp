@@ -201,6 +201,10 @@ template <class R> void sym_eigen3(const M3<R>& A, V3<R>& evals, M3<R>& evecs) {
 using Index = int32_t;
 struct Triangle { Index v[3] = {-1, -1, -1}; Triangle() = default; Triangle(Index a, Index b, Index c) { v[0] = a; v[1] = b; v[2] = c; } };
 struct Edge { Index v[2] = {-1, -1}; };
+// One interior edge of the quadratic bending energy (CORRECTED semantics):
+// v = the edge's ends, then the vertex opposite it in each of its two faces;
+// w = the cotangent stencil over v at rest; c = 6 / (rest area of the two faces).
+struct Hinge { Index v[4] = {-1, -1, -1, -1}; double w[4] = {0, 0, 0, 0}; double c = 0; };
 
 // types.h:51-57
 template <class R> struct Material {
@@ -228,6 +232,7 @@ template <class R> struct Mesh {
   std::vector<M2<R>> Dm_inv;
   std::vector<R> rest_areas;
   std::vector<std::vector<Index>> vertex_to_faces, vertex_to_edges;
+  std::vector<Hinge> hinges;
   Material<R> material;
 
   void initialize(const std::vector<V3<R>>& verts, const std::vector<Triangle>& tris, const Material<R>& mat) {
@@ -255,6 +260,53 @@ template <class R> struct Mesh {
       V3<R> nu = n / nl, t1 = e1 / std::sqrt(l1), t2 = nu.cross(t1);
       M2<R> Dm{e1.dot(t1), e2.dot(t1), e1.dot(t2), e2.dot(t2)};
       Dm_inv[i] = Dm.inverse();
+    }
+    compute_hinges();
+  }
+  // Quadratic bending (no reference counterpart: the reference declares
+  // Material::bending_stiffness, types.h:56, and never reads it). For every
+  // edge shared by exactly two faces (ends i, j; opposite vertices k in one
+  // face, l in the other) the stencil K over (i, j, k, l) at rest is
+  //   K = [cot a_j + cot b_j, cot a_i + cot b_i, -(cot a_i + cot a_j), -(cot b_i + cot b_j)]
+  // with a_i, a_j the rest angles of the first face at i and j and b_i, b_j
+  // those of the second. K annihilates every affine map of a flat rest sheet,
+  // and for an isometric fold by a dihedral angle t, |K x|^2 = |e|^2 (2 sin t/2)^2:
+  // E = k_b sum_e 3 / A_e |K_e x|^2 is the discrete-shell hinge energy
+  // k_b sum_e 3 |e|^2 / A_e t_e^2 to second order in t (A_e = rest area of the
+  // two faces), quadratic in x (Bergou, Wardetzky, Harmon, Zorin, Grinspun,
+  // "A Quadratic Bending Model for Inextensible Surfaces", SGP 2006). The rest
+  // shape is taken as flat. Edges with a degenerate face are skipped.
+  void compute_hinges() {
+    hinges.clear();
+    std::unordered_map<uint64_t, std::vector<std::pair<Index, Index>>> faces_of;  // edge key -> (face, opposite vertex)
+    for (size_t f = 0; f < triangles.size(); ++f)
+      for (int i = 0; i < 3; ++i) {
+        Index a = triangles[f].v[i], b = triangles[f].v[(i + 1) % 3], o = triangles[f].v[(i + 2) % 3];
+        Index lo = std::min(a, b), hi = std::max(a, b);
+        faces_of[(uint64_t(uint32_t(lo)) << 32) | uint64_t(uint32_t(hi))].push_back({Index(f), o});
+      }
+    auto cot = [&](Index at, Index p, Index q, bool& ok) {
+      double u[3], w[3];
+      for (int k = 0; k < 3; ++k) { u[k] = double(vertices[p][k]) - double(vertices[at][k]); w[k] = double(vertices[q][k]) - double(vertices[at][k]); }
+      double cr[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+      double s = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      if (!(s > 0.0)) { ok = false; return 0.0; }
+      return (u[0] * w[0] + u[1] * w[1] + u[2] * w[2]) / s;
+    };
+    for (const auto& e : edges) {
+      uint64_t key = (uint64_t(uint32_t(e.v[0])) << 32) | uint64_t(uint32_t(e.v[1]));
+      auto it = faces_of.find(key);
+      if (it == faces_of.end() || it->second.size() != 2) continue;
+      Index i = e.v[0], j = e.v[1], k = it->second[0].second, l = it->second[1].second;
+      bool ok = true;
+      double ai = cot(i, j, k, ok), aj = cot(j, i, k, ok), bi = cot(i, j, l, ok), bj = cot(j, i, l, ok);
+      double area = double(rest_areas[size_t(it->second[0].first)]) + double(rest_areas[size_t(it->second[1].first)]);
+      if (!ok || !(area > 0.0)) continue;
+      Hinge h;
+      h.v[0] = i; h.v[1] = j; h.v[2] = k; h.v[3] = l;
+      h.w[0] = aj + bj; h.w[1] = ai + bi; h.w[2] = -(ai + aj); h.w[3] = -(bi + bj);
+      h.c = 6.0 / area;
+      hinges.push_back(h);
     }
   }
   // mesh.cpp:77-98: unique edges in first-seen order over faces.
@@ -1648,6 +1700,26 @@ template <class R> void corrected_elastic_triplets(const Mesh<R>& mesh, std::vec
     R c[3][3]; corrected_face_coeffs(mesh, f, c);
     for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) for (int k = 0; k < 3; ++k) out.push_back({t.v[a] * 3 + k, t.v[b] * 3 + k, c[a][b]});
   }
+  // quadratic bending: its (constant) Hessian 2 k_b (3 / A_e) K K^T (x) I3 per hinge
+  const double kb = double(mesh.material.bending_stiffness);
+  if (kb > 0.0)
+    for (const auto& h : mesh.hinges)
+      for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) for (int k = 0; k < 3; ++k)
+        out.push_back({h.v[a] * 3 + k, h.v[b] * 3 + k, R(kb * h.c * h.w[a] * h.w[b])});
+}
+// Quadratic bending energy k_b sum_e (3 / A_e) |K_e x|^2 (Mesh::compute_hinges)
+// at X; adds its gradient 2 k_b (3 / A_e) K_e (K_e . x) to grad (3 per vertex).
+template <class R> double bending_at(const Mesh<R>& mesh, const std::vector<V3<R>>& X, std::vector<double>& grad) {
+  const double kb = double(mesh.material.bending_stiffness);
+  if (!(kb > 0.0)) return 0.0;
+  double E = 0.0;
+  for (const auto& h : mesh.hinges) {
+    double s[3] = {0, 0, 0};
+    for (int a = 0; a < 4; ++a) for (int q = 0; q < 3; ++q) s[q] += h.w[a] * double(X[size_t(h.v[a])][q]);
+    E += 0.5 * kb * h.c * (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    for (int a = 0; a < 4; ++a) for (int q = 0; q < 3; ++q) grad[3 * size_t(h.v[a]) + size_t(q)] += kb * h.c * h.w[a] * s[q];
+  }
+  return E;
 }
 // CORRECTED elasticity. The reference's membrane energy k |F - I|^2 is taken
 // in a frame aligned with edge e1, and its force formula (elasticity.cpp:18-61)
@@ -1693,13 +1765,15 @@ template <class R> void elastic_gradient_at(const Mesh<R>& mesh, const std::vect
     const auto& t = mesh.triangles[f];
     for (int a = 0; a < 3; ++a) for (int q = 0; q < 3; ++q) acc[3 * size_t(t.v[a]) + size_t(q)] += gr[a][q];
   }
+  bending_at(mesh, X, acc);
   g.assign(acc.size(), R(0));
   for (size_t i = 0; i < acc.size(); ++i) g[i] = R(acc[i]);
 }
 template <class R> double elastic_energy_at(const Mesh<R>& mesh, const std::vector<V3<R>>& X) {
   double e = 0.0;
   for (size_t f = 0; f < mesh.triangles.size(); ++f) { double gr[3][3] = {}; e += arap_face(mesh, X, f, gr); }
-  return e;
+  std::vector<double> unused(3 * X.size(), 0.0);
+  return e + bending_at(mesh, X, unused);
 }
 
 // Conservative time of impact of one pair along the motion x -> x + e: advance

@@ -276,6 +276,19 @@ template <class R> void bind(py::module_& m) {
   m.def("arap_energy", [](const MeshT& me, Arr<R> X) { return elastic_energy_at(me, to_v3<R>(X)); });
   m.def("arap_gradient", [](const MeshT& me, Arr<R> X) {
     std::vector<R> g; elastic_gradient_at(me, to_v3<R>(X), g); return py::array_t<R>(py::ssize_t(g.size()), g.data()); });
+  // quadratic bending of the CORRECTED step: energy and gradient at X, and the hinges
+  m.def("bending_energy", [](const MeshT& me, Arr<R> X) { std::vector<double> g(3 * me.vertices.size(), 0.0); return bending_at(me, to_v3<R>(X), g); });
+  m.def("bending_gradient", [](const MeshT& me, Arr<R> X) {
+    std::vector<double> g(3 * me.vertices.size(), 0.0); bending_at(me, to_v3<R>(X), g); return py::array_t<double>(py::ssize_t(g.size()), g.data()); });
+  m.def("bending_hinges", [](const MeshT& me) {
+    const py::ssize_t n = py::ssize_t(me.hinges.size());
+    py::array_t<int32_t> v({n, py::ssize_t(4)}); py::array_t<double> w({n, py::ssize_t(4)}); py::array_t<double> c(n);
+    auto vu = v.mutable_unchecked<2>(); auto wu = w.mutable_unchecked<2>(); auto cu = c.mutable_unchecked<1>();
+    for (py::ssize_t h = 0; h < n; ++h) {
+      for (int a = 0; a < 4; ++a) { vu(h, a) = me.hinges[size_t(h)].v[a]; wu(h, a) = me.hinges[size_t(h)].w[a]; }
+      cu(h) = me.hinges[size_t(h)].c;
+    }
+    return py::make_tuple(v, w, c); });
   m.def("pin_stiffness", [](R mass, R dt, py::object off, py::object H, R min_gap) {
     auto h = Arr<R>::ensure(H); M3<R> Hm; for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Hm(i, j) = h.at(i, j);
     return pin_stiffness(mass, dt, vec3<R>(off), Hm, min_gap); });
