@@ -16,7 +16,7 @@ from typing import Iterable, List, Optional, Sequence
 
 import numpy as np
 
-from . import abi, scenes
+from . import abi, dump, scenes
 
 WEIGHTS_DIR = Path(__file__).resolve().parent / "weights"
 DEFAULT_WEIGHTS = WEIGHTS_DIR / "precond_c4.npy"
@@ -38,19 +38,26 @@ def save_weights(w: np.ndarray, path: Optional[Path] = None) -> Path:
 
 
 def collect(trainer: abi.Trainer, sc: scenes.Scene, frames: Iterable[int], device: int = 0, max_probes: int = 6,
-            tol: float = 1e-6, params: Optional[dict] = None) -> int:
+            tol: float = 1e-6, params: Optional[dict] = None, dump_dir: Optional[Path] = None, seed: int = -1) -> int:
     """Step `sc` in CORRECTED semantics with block Jacobi and add the first
     Newton system of every frame in `frames` to the trainer. Returns how many
-    systems were added (frames whose system had already converged add none)."""
+    systems were added (frames whose system had already converged add none).
+    With `dump_dir` every evaluated system is also written there as an
+    ``.npz`` file (andosim_b200.dump)."""
     frames = sorted(set(frames))
     S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=device)
     p = abi.make_params(dict(sc.params, **(params or {})), semantics="corrected")
+    if dump_dir is not None:
+        S.keep_system()
     added = 0
     try:
         for f in range(frames[-1] + 1):
             S.apply_gravity(sc.gravity, p.dt)
             if f in frames:
                 S.eval_system(p, sc.pins_at(f), sc.walls)
+                if dump_dir is not None:
+                    dump.save_system(dump.frame_path(dump_dir, sc.name, seed, f), S, workload=sc.name, seed=seed, frame=f,
+                                     semantics="corrected", newton_iteration=0, pcg_tol=float(p.pcg_tol))
                 try:
                     trainer.add_system(S, max_probes=max_probes, tol=tol)
                     added += 1
@@ -81,9 +88,10 @@ def mean_loss(trainer: abi.Trainer) -> float:
     return float(np.mean([trainer.loss(i) for i in range(len(trainer))]))
 
 
-def c4_training_set(trainer: abi.Trainer, seeds: Sequence[int], n: int, frames: Iterable[int], device: int = 0) -> int:
+def c4_training_set(trainer: abi.Trainer, seeds: Sequence[int], n: int, frames: Iterable[int], device: int = 0,
+                    dump_dir: Optional[Path] = None) -> int:
     """Systems of the two-curtain workload (scenes.c4) for several seeds."""
     total = 0
     for sd in seeds:
-        total += collect(trainer, scenes.c4(seed=sd, n=n), frames, device=device)
+        total += collect(trainer, scenes.c4(seed=sd, n=n), frames, device=device, dump_dir=dump_dir, seed=sd)
     return total

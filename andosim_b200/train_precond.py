@@ -1,7 +1,7 @@
 """Train the learned preconditioner on the two-curtain workload and evaluate it.
 
     python -m andosim_b200.train_precond [--sets 256:0-14:1,64:0-239:4] [--train-seeds 0-7]
-        [--eval-seeds 8-11] [--steps 3000] [--out PATH] [--report PATH] [--evaluate WEIGHTS]
+        [--eval-seeds 8-11] [--steps 3000] [--out PATH] [--report PATH] [--evaluate WEIGHTS] [--dump DIR]
 
 Training data are the solver's own dumps: the first Newton system of the
 chosen frames of CORRECTED-semantics runs of scenes.c4 for the training seeds,
@@ -63,6 +63,7 @@ def main(argv=None):
     ap.add_argument("--refresh", type=int, default=1)
     ap.add_argument("--out", default=str(learned.DEFAULT_WEIGHTS))
     ap.add_argument("--report", default=None)
+    ap.add_argument("--dump", default=None, help="also write every training system as .npz into this directory")
     ap.add_argument("--evaluate", default=None,
                     help="weights (.npy) to evaluate on the held-out seeds instead of training new ones")
     a = ap.parse_args(argv)
@@ -79,7 +80,8 @@ def main(argv=None):
         return
     t0 = time.time()
     trainer = abi.Trainer(abi.precond_init_weights(a.init_seed))
-    n_sys = sum(learned.c4_training_set(trainer, seeds(a.train_seeds), n, range(f0, f1 + 1, ev)) for n, f0, f1, ev in sets)
+    n_sys = sum(learned.c4_training_set(trainer, seeds(a.train_seeds), n, range(f0, f1 + 1, ev), dump_dir=a.dump)
+                for n, f0, f1, ev in sets)
     t_collect = time.time() - t0
     loss0 = learned.mean_loss(trainer)
     t1 = time.time()
