@@ -24,6 +24,7 @@
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
 #include <thrust/iterator/counting_iterator.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/ando_gpu.h"
 #include "diag.cuh"
@@ -267,9 +268,15 @@ struct ando_ctx_s {
 namespace {
 
 // Times the launches issued while it is alive (one phase) and counts them.
+// Each phase is also an NVTX range (host-side, around its launches), so a
+// profiler's timeline and ncu's --nvtx filters see the step's phases; without
+// a tool attached the range calls do nothing.
+const char* const kPhaseNames[ANDO_PHASE_COUNT] = {"ando:setup", "ando:strain", "ando:gradient", "ando:assemble",
+                                                   "ando:pcg", "ando:line_search", "ando:finish", "ando:precond"};
 struct Phase {
   ando_ctx c; int phase; cudaEvent_t a = nullptr;
   Phase(ando_ctx c_, int ph) : c(c_), phase(ph) {
+    nvtxRangePushA(kPhaseNames[ph]);
     if (c->prof) { a = c->take_event(); cudaEventRecord(a, c->stream); }
   }
   void launched(int n = 1) { c->profile.launches += n; c->profile.phase_launches[phase] += n; }
@@ -279,6 +286,7 @@ struct Phase {
       cudaEventRecord(b, c->stream);
       c->pending.push_back({phase, a, b});
     }
+    nvtxRangePop();
   }
 };
 }  // namespace

@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--c2-frames", type=int, default=200, help="frames of the four-sheet stack (0: skip)")
     ap.add_argument("--seeds", type=int, default=3, help="seeds of the curtain workload in the paired learned/Jacobi window")
     ap.add_argument("--c5-frames", type=int, default=0, help="frames of the tablecloth over the box (0: skip)")
+    ap.add_argument("--heldout-frames", type=int, default=300,
+                    help="frames of the full-length learned runs of the curtains on the held-out seeds (0: skip)")
+    ap.add_argument("--heldout-seeds", default="8,9,10,11", help="held-out curtain seeds (the shipped weights trained on 0-7)")
     ap.add_argument("--c5-n", type=int, default=512, help="tablecloth grid side")
     return ap.parse_args()
 
@@ -525,6 +528,40 @@ def c2_run(args, local, pg, seed=0):
             "waves": "2 mm (the configured 2 cm waves on sheets 5 mm apart start the stack self-intersecting)"}
 
 
+def heldout_run(args, local, flush, pg, weights):
+    """The configured evaluation of the curtains: each held-out seed run for the full number of frames
+    with the learned preconditioner (refresh as in the timed window), device-resident; per seed the
+    frames/s, Newton and PCG counts, fallbacks, line-search failures, frames at the Newton cap, and
+    every 30 frames the exact edge-triangle crossing count (untimed)."""
+    import torch
+
+    from andosim_b200 import abi, scenes
+
+    out = []
+    for seed in [int(q) for q in args.heldout_seeds.split(",") if q.strip()]:
+        sc = scenes.c4(seed=seed, n=args.n, frames=args.heldout_frames)
+        S = abi.Scene(sc.vertices, sc.triangles, sc.material, device=local)
+        S.set_precond_weights(weights)
+        p = abi.make_params(sc.params, semantics="corrected", precond="learned", precond_refresh=args.refresh)
+        ms, newton, pcg, fb, fails, capped, crossings = 0.0, 0, 0, 0, 0, 0, 0
+        for f in range(args.heldout_frames):
+            S.apply_gravity(sc.gravity, p.dt)
+            st = S.step(p, sc.pins_at(f), sc.walls)
+            ms += st["device_ms"]; newton += st["newton_iters"]; pcg += st["pcg_iters"]
+            fb += st["precond_fallbacks"]; fails += st["line_search_fail"]
+            capped += int(st["newton_iters"] >= p.max_newton_steps * max(1, st["substeps"]))
+            if f % 30 == 29:
+                crossings += S.edge_triangle_crossings()
+        S.close()
+        ms = dist_max(ms, pg)
+        out.append({"seed": seed, "frames": args.heldout_frames, "frames_per_s": round(args.heldout_frames / (ms * 1e-3), 2),
+                    "newton_iters_per_frame": round(newton / args.heldout_frames, 2),
+                    "pcg_iters_per_newton": round(pcg / max(newton, 1), 2), "precond_fallbacks": fb,
+                    "line_search_fail": fails, "frames_at_newton_cap": capped, "edge_triangle_crossings": crossings})
+    return {"workload": f"c4_curtains_2x{args.n}x{args.n}", "preconditioner": "learned", "precond_refresh": args.refresh, "seeds": out,
+            "timing": "step device time (CUDA events inside ando_step), L2 not flushed, crossings checked every 30 frames"}
+
+
 def c5_run(args, local, pg, seed=0):
     """The tablecloth (n x n over a 3 m square) draped over the 12-triangle box (density 1e6, static in
     effect) on the ground, one edge row pulled at 1 m/s after frame 60: CORRECTED with block Jacobi
@@ -687,6 +724,8 @@ def run_ours(args, rank, world, local, pg):
         out["c2_stack"] = c2_run(args, local, pg, seed=rank)
     if args.c5_frames > 0:
         out["c5_tablecloth"] = c5_run(args, local, pg, seed=rank)
+    if args.heldout_frames > 0 and args.heldout_seeds:
+        out["heldout_full_length"] = heldout_run(args, local, flush, pg, weights)
     return out, sc, weights
 
 
