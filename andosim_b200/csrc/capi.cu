@@ -1936,6 +1936,7 @@ namespace {
 int contacts_out(ando_ctx c, ando_contact* out, int32_t capacity, int32_t* num_out) {
   *num_out = c->ncontacts;
   if (c->ncontacts == 0) return ANDO_OK;
+  if (capacity == 0) return fail(ANDO_ERR_CAPACITY, "contact buffer too small");  // a size query: nothing to copy
   std::vector<ContactDev> h(c->ncontacts);
   CK(cudaMemcpyAsync(h.data(), c->contacts.p, sizeof(ContactDev) * c->ncontacts, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
