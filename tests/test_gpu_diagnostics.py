@@ -144,7 +144,7 @@ def test_state_moments_match_host(abi):
     assert got["max_speed"] == np.sqrt((vel ** 2).sum(1).max())
 
 
-def test_module_validator_and_tracker_use_device_state(oracle, core):
+def test_module_validator_and_tracker_use_device_state(core):
     """After CORRECTED steps of two sheets in contact, the module's validator,
     energy tracker and adaptive time step (device reductions) agree with the
     same calls on a host-side copy of the contact list and velocities."""
