@@ -50,6 +50,7 @@ class Params(C.Structure):
         ("enable_strain_limiting", C.c_int32), ("strain_limit", C.c_double), ("strain_tau", C.c_double),
         ("strain_epsilon", C.c_double), ("strain_svd_epsilon", C.c_double), ("hessian_epsilon", C.c_double),
         ("min_gap", C.c_double), ("semantics", C.c_int32), ("precond", C.c_int32), ("precond_refresh", C.c_int32),
+        ("membrane_hessian", C.c_int32),
     ]
 
 
@@ -269,7 +270,7 @@ def make_params(params: dict, semantics: str = "reference", precond: str = "bloc
              contact_normal_epsilon=1e-8, barrier_tolerance=1e-12, enable_friction=0, friction_mu=0.1,
              friction_epsilon=1e-5, friction_tangent_threshold=1e-6, velocity_damping=0.0, contact_restitution=0.0,
              enable_strain_limiting=0, strain_limit=0.05, strain_tau=0.05, strain_epsilon=0.0, strain_svd_epsilon=1e-6,
-             hessian_epsilon=1e-8, min_gap=1e-8)
+             hessian_epsilon=1e-8, min_gap=1e-8, membrane_hessian=0)
     d.update({k: v for k, v in params.items()})
     p = Params()
     for name, typ in Params._fields_:

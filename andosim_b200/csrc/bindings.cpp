@@ -73,6 +73,7 @@ struct SimParams {
   std::string semantics = "reference";
   std::string preconditioner = "block_jacobi";
   int precond_refresh = 1;
+  std::string membrane_hessian = "fixed_rotation";   // CORRECTED: or "projected" (ando_params.membrane_hessian)
 };
 
 struct Triangle { int32_t v[3] = {-1, -1, -1}; };
@@ -516,6 +517,9 @@ ando_params to_abi(const SimParams& p) {
   else if (p.preconditioner == "learned") a.precond = ANDO_PRECOND_LEARNED;
   else throw py::value_error("preconditioner must be 'block_jacobi' or 'learned'");
   a.precond_refresh = p.precond_refresh;
+  if (p.membrane_hessian == "fixed_rotation") a.membrane_hessian = ANDO_MEMBRANE_FIXED_ROTATION;
+  else if (p.membrane_hessian == "projected") a.membrane_hessian = ANDO_MEMBRANE_PROJECTED;
+  else throw py::value_error("membrane_hessian must be 'fixed_rotation' or 'projected'");
   return a;
 }
 
@@ -608,6 +612,7 @@ PYBIND11_MODULE(ando_barrier_core, m) {
       .def_readwrite("hessian_epsilon", &SimParams::hessian_epsilon).def_readwrite("min_gap", &SimParams::min_gap)
       // GPU-only knobs
       .def_readwrite("semantics", &SimParams::semantics).def_readwrite("preconditioner", &SimParams::preconditioner)
+      .def_readwrite("membrane_hessian", &SimParams::membrane_hessian)
       .def_readwrite("precond_refresh", &SimParams::precond_refresh);
 
   py::class_<Triangle>(m, "Triangle")

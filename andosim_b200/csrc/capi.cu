@@ -77,6 +77,8 @@ struct ando_ctx_s {
   DevBuf<double> rest_area, dm_inv, mass, el_a, el_b, g_el, mesh_x;
   DevBuf<double> bend_q;           // quadratic bending Hessian coefficient per slot (bending_stiffness > 0)
   bool bending = false;
+  DevBuf<double> mface;            // per face: data of the projected exact membrane Hessian (MFACE doubles)
+  bool membrane_projected = false; // this step: CORRECTED with membrane_hessian = ANDO_MEMBRANE_PROJECTED
   DevBuf<double> x, v, x_prev, x_old, x_hat, g, g_const, diag_const, diag_extra;
   DevBuf<float> b, d, r, z, p0, p1, Ap, val, precond;
   DevBuf<unsigned char> sflags;
@@ -231,6 +233,7 @@ struct ando_ctx_s {
     m.face_slot = face_slot.p; m.slot_cptr = slot_cptr.p; m.slot_contrib = slot_contrib.p;
     m.vf_ptr = vf_ptr.p; m.vf = vf.p; m.el_a = el_a.p; m.el_b = el_b.p; m.g_elastic = g_el.p;
     m.bend_q = bending ? bend_q.p : nullptr;
+    m.mface = membrane_projected ? mface.p : nullptr;
     return m;
   }
 
@@ -765,6 +768,7 @@ int corrected_gradient(ando_ctx c, const ando_params& p, const StepParams& sp, i
     launch_ctrl_reset(c->ctrl.p, s);
     launch_arap_gradient(m, c->x.p, c->mu, c->thickness, c->g_el_x.p, s);
     ph.launched(2);
+    if (c->membrane_projected) { launch_membrane_face(m, c->x.p, c->mu, c->thickness, c->mface.p, s); ph.launched(); }
   }
   if (sp.enable_strain) {
     Phase ph(c, ANDO_PHASE_STRAIN);
@@ -1216,6 +1220,10 @@ std::vector<unsigned char> frame_key(ando_ctx c, const ando_params& p, const Ste
 int upload_constraints(ando_ctx c, const ando_params& p, const ando_pin* pins, int num_pins, const ando_wall* walls, int num_walls,
                        ando_rigid* rigids, int num_rigids, StepParams& sp) {
   cudaStream_t s = c->stream;
+  if (p.membrane_hessian != ANDO_MEMBRANE_FIXED_ROTATION && p.membrane_hessian != ANDO_MEMBRANE_PROJECTED)
+    return fail(ANDO_ERR_INVALID, "unknown membrane Hessian");
+  c->membrane_projected = p.semantics == ANDO_SEMANTICS_CORRECTED && p.membrane_hessian == ANDO_MEMBRANE_PROJECTED;
+  if (c->membrane_projected) CK(c->mface.reserve(size_t(MFACE) * std::max(c->T, 1)));
   if (c->el_semantics != p.semantics) {
     Phase ph(c, ANDO_PHASE_SETUP);
     launch_elastic_slots(c->mesh_dev(), c->mu, c->thickness, p.semantics, c->el_a.p, c->el_b.p, s);

@@ -102,7 +102,13 @@ struct MeshDev {
   // nnzb coefficient q of the quadratic bending Hessian q I3 per slot
   // (CORRECTED semantics, bending_stiffness > 0; null without bending)
   const double* bend_q;
+  // 13 per face (R0, R1, n, a_t, W00, W01, W11) of the projected exact membrane
+  // Hessian at the current positions (CORRECTED, membrane_hessian projected;
+  // null otherwise): the assembly subtracts its correction of the constant
+  // fixed-rotation blocks
+  const double* mface;
 };
+constexpr int MFACE = 13;
 
 // Strain-limit data of one face and one singular value.
 struct StrainSV { double J[9]; double dV, d2V; };

@@ -486,6 +486,35 @@ __global__ void k_arap_gradient(MeshDev m, const double* X, double mu, double th
   st3(g, i, acc);
 }
 
+// Per face: the data of the projected exact membrane Hessian at X (see
+// membrane_correction): R = U V^T, n = U0 x U1, a_t = 2k min(1, 2 / (s0 + s1))
+// and W = V diag(c0, c1) V^T with c_i = 2k min(1, 1 / s_i), from the thin SVD
+// of F = [x1 - x0, x2 - x0] Dm^-1. The Hessian of k |F - R|^2 in F has the
+// eigenvalues 2k (three symmetric in-plane modes), 2k (1 - 2 / (s0 + s1))
+// (the twist) and 2k (1 - 1 / s_i) (the flips n v_i^T); clamping them at zero
+// leaves 2k I minus a_t on the twist and c_i on the flips.
+__global__ void k_membrane_face(MeshDev m, const double* X, double mu, double thickness, double* out) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.T) return;
+  const int v0 = m.tris[3 * f], v1 = m.tris[3 * f + 1], v2 = m.tris[3 * f + 2];
+  const d3 e1 = ld3(X, v1) - ld3(X, v0), e2 = ld3(X, v2) - ld3(X, v0);
+  const double da = m.dm_inv[4 * f], db = m.dm_inv[4 * f + 1], dc = m.dm_inv[4 * f + 2], dd = m.dm_inv[4 * f + 3];
+  const d3 F0 = e1 * da + e2 * dc, F1 = e1 * db + e2 * dd;
+  const Svd32 s = svd32(F0, F1);
+  const d3 R0 = s.U0 * s.V00 + s.U1 * s.V01, R1 = s.U0 * s.V10 + s.U1 * s.V11;
+  const d3 n = normalized(cross(s.U0, s.U1));
+  const double k2 = 2.0 * m.rest_area[f] * thickness * mu;
+  const double at = k2 * fmin(1.0, 2.0 / (s.s0 + s.s1));
+  const double c0 = k2 * fmin(1.0, 1.0 / s.s0), c1 = k2 * fmin(1.0, 1.0 / s.s1);
+  double* q = out + (long long)MFACE * f;
+  q[0] = R0.x; q[1] = R0.y; q[2] = R0.z; q[3] = R1.x; q[4] = R1.y; q[5] = R1.z;
+  q[6] = n.x; q[7] = n.y; q[8] = n.z;
+  q[9] = at;
+  q[10] = s.V00 * c0 * s.V00 + s.V01 * c1 * s.V01;
+  q[11] = s.V00 * c0 * s.V10 + s.V01 * c1 * s.V11;
+  q[12] = s.V10 * c0 * s.V10 + s.V11 * c1 * s.V11;
+}
+
 __device__ inline int warp_sum_i(int v) { for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o); return v; }
 __device__ inline unsigned warp_and(unsigned v) { for (int o = 16; o; o >>= 1) v &= __shfl_xor_sync(0xffffffffu, v, o); return v; }
 __device__ inline double warp_max_d(double v) { for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o)); return v; }
@@ -711,10 +740,32 @@ __global__ void k_check(Ctrl* c, double tol) {
 // the strain-limit blocks of the faces sharing the slot (face order;
 // StrainLimiting::accumulate_hessian drop rules) and, for a diagonal slot, the
 // vertex's diagonal terms.
+// Projected exact membrane Hessian: the correction D_ab of face f's block
+// (a, b) (k_membrane_face), D_ab = a_t / 2 g_a g_b^T + w_ab n n^T with
+// g_a = G_a0 R1 - G_a1 R0 and w_ab = G_a W G_b^T, subtracted from H.
+__device__ inline void membrane_correction(const MeshDev& m, int f, int a, int b, double H[9]) {
+  const double* q = m.mface + (long long)MFACE * f;
+  const double da = m.dm_inv[4 * f], db = m.dm_inv[4 * f + 1], dc = m.dm_inv[4 * f + 2], dd = m.dm_inv[4 * f + 3];
+  const double Ga0 = a == 0 ? -(da + dc) : (a == 1 ? da : dc), Ga1 = a == 0 ? -(db + dd) : (a == 1 ? db : dd);
+  const double Gb0 = b == 0 ? -(da + dc) : (b == 1 ? da : dc), Gb1 = b == 0 ? -(db + dd) : (b == 1 ? db : dd);
+  const d3 R0 = mk(q[0], q[1], q[2]), R1 = mk(q[3], q[4], q[5]), n = mk(q[6], q[7], q[8]);
+  const double at = q[9], W00 = q[10], W01 = q[11], W11 = q[12];
+  const d3 ga = R1 * Ga0 - R0 * Ga1, gb = R1 * Gb0 - R0 * Gb1;
+  const double w = Ga0 * (W00 * Gb0 + W01 * Gb1) + Ga1 * (W01 * Gb0 + W11 * Gb1);
+  const double h = 0.5 * at;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) H[3 * r + c] -= h * comp(ga, r) * comp(gb, c) + w * comp(n, r) * comp(n, c);
+}
+
 __device__ inline void slot_block(const MeshDev& m, int s, int row, int col, const unsigned char* sflags, const StrainSV* sv,
                                   const double* diag_extra, int enable_strain, double H[9]) {
   for (int k = 0; k < 9; ++k) H[k] = 0.0;
   H[0] = H[4] = m.el_a[s]; H[8] = m.el_b[s];
+  if (m.mface)
+    for (int k = m.slot_cptr[s]; k < m.slot_cptr[s + 1]; ++k) {
+      const int e = m.slot_contrib[k];
+      membrane_correction(m, e / 9, (e % 9) / 3, e % 3, H);
+    }
   if (enable_strain) {
     for (int k = m.slot_cptr[s]; k < m.slot_cptr[s + 1]; ++k) {
       int e = m.slot_contrib[k];
@@ -1317,6 +1368,9 @@ void launch_elastic_slots(const MeshDev& m, double mu, double thickness, int sem
 }
 void launch_elastic_gradient(const MeshDev& m, const double* X, double mu, double thickness, double* g, cudaStream_t s) {
   if (m.V) k_elastic_gradient<<<nblk(m.V), TPB, 0, s>>>(m, X, mu, thickness, g);
+}
+void launch_membrane_face(const MeshDev& m, const double* X, double mu, double thickness, double* out, cudaStream_t s) {
+  if (m.T) k_membrane_face<<<nblk(m.T), TPB, 0, s>>>(m, X, mu, thickness, out);
 }
 void launch_arap_gradient(const MeshDev& m, const double* X, double mu, double thickness, double* g, cudaStream_t s) {
   if (m.V) k_arap_gradient<<<nblk(m.V), TPB, 0, s>>>(m, X, mu, thickness, g);

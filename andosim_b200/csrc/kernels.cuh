@@ -17,6 +17,8 @@ struct RigidDev {
 void launch_elastic_slots(const MeshDev& m, double mu, double thickness, int semantics, double* el_a, double* el_b, cudaStream_t s);
 void launch_elastic_gradient(const MeshDev& m, const double* mesh_vertices, double mu, double thickness, double* g_el, cudaStream_t s);
 void launch_arap_gradient(const MeshDev& m, const double* X, double mu, double thickness, double* g, cudaStream_t s);
+// per face: the data of the projected exact membrane Hessian at X (MFACE doubles each)
+void launch_membrane_face(const MeshDev& m, const double* X, double mu, double thickness, double* out, cudaStream_t s);
 
 // per step
 void launch_predict(int V, const double* x, const double* v, double dt, double* x_old, double* x_hat, cudaStream_t s);

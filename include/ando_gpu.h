@@ -85,7 +85,15 @@ typedef struct {
    * network (<= 1: every iteration). In between, S is rebuilt from the
    * current scaled system with the last coefficients (still SPD). */
   int32_t precond_refresh;
+  /* CORRECTED membrane Hessian in the Newton system: ANDO_MEMBRANE_FIXED_ROTATION
+   * (0, the constant 2k (G G^T) (x) I3) or ANDO_MEMBRANE_PROJECTED (1, the exact
+   * as-rigid-as-possible Hessian projected to positive semidefinite per face,
+   * rebuilt every Newton iteration: face rotations, such as a clamped sheet
+   * swinging down, are not resisted). */
+  int32_t membrane_hessian;
 } ando_params;
+
+typedef enum { ANDO_MEMBRANE_FIXED_ROTATION = 0, ANDO_MEMBRANE_PROJECTED = 1 } ando_membrane_hessian;
 
 /* PinConstraint (constraints.h:12-17). */
 typedef struct { int32_t vertex; int32_t active; double target[3]; } ando_pin;

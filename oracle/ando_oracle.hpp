@@ -222,6 +222,9 @@ template <class R> struct SimParams {
   R velocity_damping = R(0); R contact_restitution = R(0);
   bool enable_strain_limiting = false; R strain_limit = R(0.05); R strain_tau = R(0.05); R strain_epsilon = R(0); R strain_svd_epsilon = R(1e-6);
   R hessian_epsilon = R(1e-8); R min_gap = R(1e-8);
+  // CORRECTED only: 0 = the constant fixed-rotation membrane Hessian, 1 = the
+  // exact membrane Hessian projected to positive semidefinite per face
+  int membrane_hessian = 0;
 };
 
 // mesh.cpp:8-151
@@ -1757,6 +1760,63 @@ template <class R> double arap_face(const Mesh<R>& mesh, const std::vector<V3<R>
   for (int a = 0; a < 3; ++a) for (int q = 0; q < 3; ++q) grad[a][q] += P0[q] * G[a][0] + P1[q] * G[a][1];
   return k * E;
 }
+// Exact membrane Hessian, projected to positive semidefinite per face
+// (CORRECTED, membrane_hessian = 1). For E = k |F - R|^2 with F = U S V^T
+// (3 x 2, thin SVD), R = U V^T, n = U0 x U1, the Hessian in F is
+// 2k (I - dR/dF); its eigenpairs are 2k on the three symmetric in-plane modes,
+// 2k (1 - 2 / (s0 + s1)) on the twist R J / sqrt 2 (J the 2 x 2 rotation by
+// 90 degrees) and 2k (1 - 1 / s_i) on the flips n v_i^T. Clamping each at zero
+// gives H = 2k I - a_t t t^T - sum_i c_i f_i f_i^T with a_t = 2k min(1, 2 / (s0 + s1))
+// and c_i = 2k min(1, 1 / s_i): the fixed-rotation Hessian 2k I (the constant
+// elastic blocks) minus, per vertex pair (a, b) of the face,
+//   D_ab = a_t / 2 g_a g_b^T + w_ab n n^T,  g_a = G_a0 R1 - G_a1 R0,  w_ab = G_a W G_b^T,
+// W = V diag(c0, c1) V^T. Near rest (s = 1) the twist and flips, which are
+// the face's rotations, cost nothing, as the energy says. Writes D (FP64).
+template <class R> void membrane_correction_face(const Mesh<R>& mesh, const std::vector<V3<R>>& X, size_t f, double D[3][3][9]) {
+  const auto& t = mesh.triangles[f];
+  const double mu = double(mesh.material.youngs_modulus) / (2.0 * (1.0 + double(mesh.material.poisson_ratio)));
+  const double k = double(mesh.rest_areas[f]) * double(mesh.material.thickness) * mu;
+  const M2<R>& Dm = mesh.Dm_inv[f];
+  const double da = Dm.a, db = Dm.b, dc = Dm.c, dd = Dm.d;
+  double e1[3], e2[3], F0[3], F1[3];
+  for (int q = 0; q < 3; ++q) {
+    e1[q] = double(X[size_t(t.v[1])][q]) - double(X[size_t(t.v[0])][q]);
+    e2[q] = double(X[size_t(t.v[2])][q]) - double(X[size_t(t.v[0])][q]);
+    F0[q] = e1[q] * da + e2[q] * dc; F1[q] = e1[q] * db + e2[q] * dd;
+  }
+  V3<double> Fc[2] = {V3<double>(F0[0], F0[1], F0[2]), V3<double>(F1[0], F1[1], F1[2])};
+  Svd32<double> sv; svd32(Fc, sv);
+  const V3<double> R0 = sv.U[0] * sv.V[0][0] + sv.U[1] * sv.V[0][1], R1 = sv.U[0] * sv.V[1][0] + sv.U[1] * sv.V[1][1];
+  V3<double> n = sv.U[0].cross(sv.U[1]);
+  const double nl = n.norm();
+  if (nl > 0.0) n = n / nl;
+  const double s0 = double(sv.sigma[0]), s1 = double(sv.sigma[1]);
+  const double at = 2.0 * k * std::min(1.0, 2.0 / (s0 + s1));
+  const double c0 = 2.0 * k * std::min(1.0, 1.0 / s0), c1 = 2.0 * k * std::min(1.0, 1.0 / s1);
+  double W[2][2];
+  for (int p2 = 0; p2 < 2; ++p2)
+    for (int q2 = 0; q2 < 2; ++q2) W[p2][q2] = sv.V[p2][0] * c0 * sv.V[q2][0] + sv.V[p2][1] * c1 * sv.V[q2][1];
+  const double G[3][2] = {{-(da + dc), -(db + dd)}, {da, db}, {dc, dd}};
+  V3<double> g[3];
+  for (int a = 0; a < 3; ++a) g[a] = R1 * G[a][0] - R0 * G[a][1];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double w = 0.0;
+      for (int p2 = 0; p2 < 2; ++p2) for (int q2 = 0; q2 < 2; ++q2) w += G[a][p2] * W[p2][q2] * G[b][q2];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) D[a][b][3 * r + c] = 0.5 * at * g[a][r] * g[b][c] + w * n[r] * n[c];
+    }
+}
+// The projection's correction of every face at X as triplets (subtracted).
+template <class R> void membrane_correction_triplets(const Mesh<R>& mesh, const std::vector<V3<R>>& X, std::vector<Triplet<R>>& out) {
+  for (size_t f = 0; f < mesh.triangles.size(); ++f) {
+    double D[3][3][9];
+    membrane_correction_face(mesh, X, f, D);
+    const auto& t = mesh.triangles[f];
+    for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c)
+      out.push_back({t.v[a] * 3 + r, t.v[b] * 3 + c, R(-D[a][b][3 * r + c])});
+  }
+}
 template <class R> void elastic_gradient_at(const Mesh<R>& mesh, const std::vector<V3<R>>& X, std::vector<R>& g) {
   std::vector<double> acc(3 * X.size(), 0.0);
   for (size_t f = 0; f < mesh.triangles.size(); ++f) {
@@ -2030,6 +2090,7 @@ template <class R> class CorrectedIntegrator {
     R dinv = R(1) / (dt * dt);
     for (Index row = 0; row < 3 * n; ++row) { R v = st.masses[size_t(row / 3)] * dinv; if (v != R(0)) tr.push_back({row, row, v}); }
     corrected_elastic_triplets(mesh, tr);
+    if (p.membrane_hessian) membrane_correction_triplets(mesh, st.positions, tr);
     if (p.enable_strain_limiting) strain_hessian(mesh, st, C, p, tr);
     for (const auto& c : contacts) {
       R kb = corrected_contact_stiffness(c, st.masses, H_el, p.min_gap);

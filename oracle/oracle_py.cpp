@@ -109,7 +109,7 @@ template <class R> void bind(py::module_& m) {
       .def_readwrite("velocity_damping", &ParT::velocity_damping).def_readwrite("contact_restitution", &ParT::contact_restitution)
       .def_readwrite("enable_strain_limiting", &ParT::enable_strain_limiting).def_readwrite("strain_limit", &ParT::strain_limit)
       .def_readwrite("strain_tau", &ParT::strain_tau).def_readwrite("strain_epsilon", &ParT::strain_epsilon)
-      .def_readwrite("strain_svd_epsilon", &ParT::strain_svd_epsilon).def_readwrite("hessian_epsilon", &ParT::hessian_epsilon)
+      .def_readwrite("strain_svd_epsilon", &ParT::strain_svd_epsilon).def_readwrite("hessian_epsilon", &ParT::hessian_epsilon).def_readwrite("membrane_hessian", &ParT::membrane_hessian)
       .def_readwrite("min_gap", &ParT::min_gap);
 
   py::class_<MeshT>(m, "Mesh")

@@ -34,3 +34,22 @@ def test_elasticity_compute_hessian_matches_oracle(core, oracle):
     Ho = dense(O.Integrator.base_matrices(mo, so, p)["H_elastic"], n)
     assert np.abs(H - Ho).max() <= 1e-6 * np.abs(Ho).max()
     assert len(core.Elasticity.compute_hessian(m, st)) == len(trip)
+
+
+def test_unknown_gpu_knobs_are_refused_before_any_device_call(core):
+    """SimParams' GPU-only string fields are checked when a step converts them,
+    before a context exists: a typo raises ValueError, never a silent default."""
+    import pytest
+
+    sc = scenes.c1(n=4)
+    m = core.Mesh()
+    m.initialize(sc.vertices, sc.triangles, core.Material(**sc.material))
+    st = core.State()
+    st.initialize(m)
+    for field, bad in (("semantics", "corected"), ("preconditioner", "jacobi"), ("membrane_hessian", "exact")):
+        p = core.SimParams()
+        setattr(p, field, bad)
+        with pytest.raises(ValueError, match=field):
+            core.Integrator.step(m, st, core.Constraints(), p)
+    p = core.SimParams()
+    assert (p.semantics, p.preconditioner, p.membrane_hessian) == ("reference", "block_jacobi", "fixed_rotation")
