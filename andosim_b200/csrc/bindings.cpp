@@ -815,6 +815,22 @@ PYBIND11_MODULE(ando_barrier_core, m) {
 
   py::class_<Contact>(m, "Contact")
       .def(py::init<>())
+      // not in the reference's binding: a contact built by hand (its fields stay
+      // read-only), so a caller can judge its own contact list with
+      // CollisionValidator; such a list is always read on the host
+      .def(py::init([](ContactType type, int32_t idx0, int32_t idx1, int32_t idx2, int32_t idx3, double gap, py::object normal,
+                       int32_t rigid_body_index) {
+             Contact c;
+             c.c.type = int32_t(type); c.c.idx0 = idx0; c.c.idx1 = idx1; c.c.idx2 = idx2; c.c.idx3 = idx3;
+             c.c.rigid_body_index = rigid_body_index; c.c.gap = gap;
+             if (!normal.is_none()) {
+               V3 n = to_vec3(normal, "normal must be a 3D vector");
+               c.c.normal[0] = n.x; c.c.normal[1] = n.y; c.c.normal[2] = n.z;
+             }
+             return c;
+           }),
+           py::arg("type"), py::arg("idx0") = -1, py::arg("idx1") = -1, py::arg("idx2") = -1, py::arg("idx3") = -1,
+           py::arg("gap") = 0.0, py::arg("normal") = py::none(), py::arg("rigid_body_index") = -1)
       .def_property_readonly("type", [](const Contact& c) { return ContactType(c.c.type); })
       .def_property_readonly("idx0", [](const Contact& c) { return c.c.idx0; })
       .def_property_readonly("idx1", [](const Contact& c) { return c.c.idx1; })
