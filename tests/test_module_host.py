@@ -53,3 +53,28 @@ def test_unknown_gpu_knobs_are_refused_before_any_device_call(core):
             core.Integrator.step(m, st, core.Constraints(), p)
     p = core.SimParams()
     assert (p.semantics, p.preconditioner, p.membrane_hessian) == ("reference", "block_jacobi", "fixed_rotation")
+
+
+def test_module_barrier_functions_meet_the_reference_expectations(core):
+    """The module's barrier_energy / gradient / hessian (bindings.cpp:421-442 of
+    the reference) against tests/test_barrier_derivatives.cpp:21-236: closed
+    forms at g = 5 mm, g_max = 10 mm, k = 1000, central differences, the
+    domain edges and the force direction, in the reference's FP32 Real."""
+    import pytest
+
+    g, gm, k = 0.005, 0.01, 1000.0
+    assert core.barrier_energy(g, gm, k) == pytest.approx(6.25e-3, rel=1e-5)
+    assert core.barrier_gradient(g, gm, k) == pytest.approx(-3.75, rel=1e-5)
+    assert core.barrier_hessian(g, gm, k) == pytest.approx(1500.0, rel=1e-5)
+    assert core.barrier_energy(0.015, gm, k) == 0.0 and core.barrier_energy(gm, gm, k) == 0.0
+    assert core.barrier_energy(-0.001, gm, k) > 0.0
+    assert core.barrier_gradient(gm, gm, k) == 0.0 and core.barrier_hessian(gm, gm, k) == 0.0
+    g1, g2, g3 = (core.barrier_gradient(x, gm, k) for x in (0.002, 0.005, 0.009))
+    assert g1 < 0 and g2 < 0 and g3 < 0 and abs(g1) > abs(g2) > abs(g3)
+    h = 1e-4                                  # FP32 arithmetic: a larger step than the FP64 oracle's
+    for i in range(1, 10):
+        x = i / 10.0 * gm
+        fd_g = (core.barrier_energy(x + h, gm, k) - core.barrier_energy(x - h, gm, k)) / (2 * h)
+        fd_h = (core.barrier_gradient(x + h, gm, k) - core.barrier_gradient(x - h, gm, k)) / (2 * h)
+        assert abs(core.barrier_gradient(x, gm, k) - fd_g) / (abs(fd_g) + 1e-10) < 1e-2
+        assert abs(core.barrier_hessian(x, gm, k) - fd_h) / (abs(fd_h) + 1e-10) < 1e-2
