@@ -276,6 +276,18 @@ template <class R> void bind(py::module_& m) {
   m.def("arap_energy", [](const MeshT& me, Arr<R> X) { return elastic_energy_at(me, to_v3<R>(X)); });
   m.def("arap_gradient", [](const MeshT& me, Arr<R> X) {
     std::vector<R> g; elastic_gradient_at(me, to_v3<R>(X), g); return py::array_t<R>(py::ssize_t(g.size()), g.data()); });
+  // thin SVD of one 3 x 2 matrix (the strain limits' and the membrane's svd32): U (3 x 2), sigma, V (2 x 2)
+  m.def("svd32", [](py::object Fo) {
+    auto F = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(Fo);
+    if (!F || F.ndim() != 2 || F.shape(0) != 3 || F.shape(1) != 2) throw py::value_error("F must be 3 x 2");
+    V3<double> c[2] = {V3<double>(F.at(0, 0), F.at(1, 0), F.at(2, 0)), V3<double>(F.at(0, 1), F.at(1, 1), F.at(2, 1))};
+    Svd32<double> s; bool ok = svd32(c, s);
+    py::array_t<double> U({py::ssize_t(3), py::ssize_t(2)}), S(2), V({py::ssize_t(2), py::ssize_t(2)});
+    auto u = U.mutable_unchecked<2>(); auto v = V.mutable_unchecked<2>();
+    for (int r = 0; r < 3; ++r) for (int q = 0; q < 2; ++q) u(r, q) = s.U[q][r];
+    for (int r = 0; r < 2; ++r) for (int q = 0; q < 2; ++q) v(r, q) = s.V[r][q];
+    S.mutable_data()[0] = s.sigma[0]; S.mutable_data()[1] = s.sigma[1];
+    return py::make_tuple(U, S, V, ok); });
   // quadratic bending of the CORRECTED step: energy and gradient at X, and the hinges
   m.def("bending_energy", [](const MeshT& me, Arr<R> X) { std::vector<double> g(3 * me.vertices.size(), 0.0); return bending_at(me, to_v3<R>(X), g); });
   m.def("bending_gradient", [](const MeshT& me, Arr<R> X) {
