@@ -276,6 +276,18 @@ template <class R> void bind(py::module_& m) {
   m.def("arap_energy", [](const MeshT& me, Arr<R> X) { return elastic_energy_at(me, to_v3<R>(X)); });
   m.def("arap_gradient", [](const MeshT& me, Arr<R> X) {
     std::vector<R> g; elastic_gradient_at(me, to_v3<R>(X), g); return py::array_t<R>(py::ssize_t(g.size()), g.data()); });
+  // sparse assembly from triplets with duplicates summed (what the reference leaves to setFromTriplets)
+  m.def("csr_from_triplets", [](Index n, py::object ro, py::object co, py::object vo) {
+    auto r = py::array_t<int64_t, py::array::c_style | py::array::forcecast>::ensure(ro);
+    auto c = py::array_t<int64_t, py::array::c_style | py::array::forcecast>::ensure(co);
+    auto v = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(vo);
+    if (!r || !c || !v || r.size() != c.size() || r.size() != v.size()) throw py::value_error("triplet arrays");
+    std::vector<Triplet<R>> t(size_t(r.size()));
+    for (py::ssize_t k = 0; k < r.size(); ++k) {
+      if (r.data()[k] < 0 || r.data()[k] >= n || c.data()[k] < 0 || c.data()[k] >= n) throw py::value_error("triplet index out of range");
+      t[size_t(k)] = {Index(r.data()[k]), Index(c.data()[k]), R(v.data()[k])};
+    }
+    return csr_dict(Csr<R>::from_triplets(n, t)); });
   // thin SVD of one 3 x 2 matrix (the strain limits' and the membrane's svd32): U (3 x 2), sigma, V (2 x 2)
   m.def("svd32", [](py::object Fo) {
     auto F = py::array_t<double, py::array::c_style | py::array::forcecast>::ensure(Fo);

@@ -85,3 +85,26 @@ def test_svd32_values_and_polar_factor(oracle, kind):
         np.testing.assert_allclose(U @ np.diag(s) @ V.T, F, rtol=0, atol=1e-11 * scale)
         # the polar factor R = U V^T, unique for a full-rank F
         np.testing.assert_allclose(U @ V.T, Un @ Vtn, rtol=0, atol=1e-9 * scale / sn[1])
+
+
+def test_triplet_assembly_sums_duplicates_like_scipy(oracle):
+    """Sparse assembly from triplets (the reference's SparseMatrix::setFromTriplets
+    in matrix_assembly.cpp): duplicates summed, columns sorted per row, against
+    scipy's COO -> CSR conversion of the same triplets."""
+    import scipy.sparse as sp
+
+    O = oracle.f64
+    rng = np.random.default_rng(3)
+    n = 60
+    k = 4000                                               # about one duplicate per entry
+    rows = rng.integers(0, n, k)
+    cols = rng.integers(0, n, k)
+    vals = rng.normal(size=k) * 10.0 ** rng.uniform(-6, 6, k)
+    A = O.csr_from_triplets(n, rows, cols, vals)
+    B = sp.coo_matrix((vals, (rows, cols)), shape=(n, n)).tocsr()
+    B.sum_duplicates()
+    B.sort_indices()
+    np.testing.assert_array_equal(np.asarray(A["rowptr"]), B.indptr)
+    np.testing.assert_array_equal(np.asarray(A["cols"]), B.indices)
+    scale = np.abs(vals).max()
+    np.testing.assert_allclose(np.asarray(A["vals"]), B.data, rtol=1e-12, atol=1e-15 * scale)
