@@ -2,14 +2,17 @@
 
 The reference tests its pybind11 surface from Python (tests/test_adaptive_timestep.py:
 CFL time step, minimum edge length, velocity scan and smoothing;
-tests/test_state_constraints.py: State and Constraints accessors, pins, walls).
+tests/test_state_constraints.py: State and Constraints accessors, pins, walls;
+tests/test_e2e.py: gravity fall, pins, the adaptive time step workflow, ground
+approach, multi-frame stability and energy trends, all through
+State.apply_gravity, which runs on the host while a state has no device
+context).
 Where a checkout of the reference sits beside this container's repository,
 each of those test functions is imported from the reference's file with
 `ando_barrier_core` resolved to this repository's module and called as is: the
 drop-in must pass the reference's checks unchanged. Nothing is copied; without
-the checkout (the GPU box has none) the test is skipped. test_e2e.py steps
-cloth and needs the GPU, test_heatmap_colors.py tests the add-on's overlay
-colours: neither is run here.
+the checkout (the GPU box has none) the test is skipped. test_heatmap_colors.py
+tests the add-on's overlay colours and is not run.
 """
 from __future__ import annotations
 
@@ -20,7 +23,7 @@ from pathlib import Path
 import pytest
 
 REFERENCE_TESTS = Path("/root/reference/tests")
-SUITES = ["test_adaptive_timestep.py", "test_state_constraints.py"]
+SUITES = ["test_adaptive_timestep.py", "test_state_constraints.py", "test_e2e.py"]
 
 
 def reference_tests(name):
