@@ -104,3 +104,27 @@ def test_elasticity_energy_and_gradient_match_oracle(core, oracle):
     assert np.abs(go).max() > 0 and eo > 0
     assert np.abs(g - go).max() <= 1e-5 * np.abs(go).max()
     assert abs(e - eo) <= 1e-5 * eo
+
+
+def test_energy_tracker_on_the_host_copy(core):
+    """EnergyTracker (energy_tracker.cpp:7-76) on a state that has no device
+    context yet: kinetic energy, momenta and the largest speed from the host
+    arrays, against numpy."""
+    sc = scenes.c1(n=5)
+    m = core.Mesh()
+    m.initialize(sc.vertices, sc.triangles, core.Material(**sc.material))
+    st = core.State()
+    st.initialize(m)
+    rng = np.random.default_rng(9)
+    v = rng.normal(size=sc.vertices.shape)
+    st.set_velocities64(v)
+    mass = np.asarray(st.get_masses(), dtype=np.float64)
+    x = st.get_positions64()
+    p = mass[:, None] * v
+    ke = 0.5 * (mass * (v ** 2).sum(1)).sum()
+    assert abs(core.EnergyTracker.compute_kinetic_energy(st) - ke) <= 1e-6 * ke
+    np.testing.assert_allclose(core.EnergyTracker.compute_linear_momentum(st), p.sum(0), rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(core.EnergyTracker.compute_angular_momentum(st), np.cross(x, p).sum(0), rtol=1e-5, atol=1e-7)
+    assert abs(core.EnergyTracker.compute_max_velocity(st) - np.linalg.norm(v, axis=1).max()) <= 1e-6 * np.linalg.norm(v, axis=1).max()
+    d = core.EnergyTracker.compute(m, st, core.Constraints(), core.SimParams())
+    assert abs(d.kinetic_energy - ke) <= 1e-6 * ke and d.total_energy >= d.kinetic_energy
