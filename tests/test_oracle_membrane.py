@@ -98,3 +98,26 @@ def test_clamped_strip_swings_with_the_projected_hessian(oracle):
     creep, swing = sag(0), sag(1)
     assert creep < 5e-3, creep
     assert swing > 5e-2, swing                   # 8 cm in 10 frames against free fall's 13.6 cm
+
+
+def test_projected_hessian_with_bending_is_the_exact_jacobian(oracle):
+    """With bending on as well, the assembled elastic Hessian (projected membrane
+    plus the constant bending Hessian) is the central-difference Jacobian of the
+    whole elastic gradient where no membrane eigenvalue is clamped."""
+    O = oracle.f64
+    v = scenes.grid_plane(4, 0.03)
+    v[:, 2] = 0.3
+    mat = dict(youngs_modulus=1e5, poisson_ratio=0.3, density=200.0, thickness=1e-3, bending_stiffness=2e-4)
+    sc = scenes.Scene("membrane_bending", v, scenes.grid_triangles(4, 4), mat, scenes.cloth_params(enable_strain_limiting=False), [], [])
+    x = v.copy()
+    x[:, :2] *= 1.08                            # every face stretched both ways: nothing clamped
+    x += np.random.default_rng(4).normal(scale=2e-4, size=x.shape)
+    m, Hp = elastic_hessian(O, sc, x, 1)
+    J = np.zeros_like(Hp)
+    flat = x.ravel()
+    for i in range(flat.size):
+        xp = flat.copy(); xp[i] += H
+        xm = flat.copy(); xm[i] -= H
+        J[:, i] = (O.arap_gradient(m, xp.reshape(x.shape)) - O.arap_gradient(m, xm.reshape(x.shape))) / (2 * H)
+    assert np.abs(O.bending_gradient(m, x)).max() > 0
+    assert np.abs(Hp - J).max() <= 1e-6 * np.abs(J).max()
