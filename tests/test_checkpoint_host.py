@@ -56,3 +56,34 @@ def test_corrupt_state_pickle_is_rejected(core):
     s2 = core.State.__new__(core.State)
     with pytest.raises(RuntimeError, match="inconsistent"):
         s2.__setstate__(bad)
+
+
+def test_npz_checkpoint_round_trip(core, tmp_path):
+    """andosim_b200.checkpoint writes the pickled arrays as a plain .npz and
+    rebuilds objects equal field for field."""
+    from andosim_b200 import checkpoint
+
+    sc = scenes.c1(n=7)
+    m = core.Mesh()
+    m.initialize(sc.vertices, sc.triangles, core.Material(**sc.material, bending_stiffness=1e-3))
+    st = core.State()
+    st.initialize(m)
+    rng = np.random.default_rng(2)
+    st.set_positions64(sc.vertices + rng.normal(scale=1e-3, size=sc.vertices.shape))
+    st.set_velocities64(rng.normal(size=sc.vertices.shape))
+    c = core.Constraints()
+    for i, t in sc.pins:
+        c.add_pin(int(i), t)
+    c.add_wall(np.array([0.0, 0.0, 1.0]), 0.0, 1e-3)
+    path = checkpoint.save(tmp_path / "run.npz", m, st, c, frame=42, workload="c1")
+    assert checkpoint.restart_frame(path) == 42
+    m2, st2, c2, frame, meta = checkpoint.load(path, core)
+    assert frame == 42 and meta == {"workload": "c1"}
+    with np.load(path, allow_pickle=False) as z:           # plain arrays, no pickled objects
+        assert z["positions"].dtype == np.float64 and z["pins"].shape == (len(sc.pins), 5)
+    np.testing.assert_array_equal(m2.get_vertices(), m.get_vertices())
+    np.testing.assert_array_equal(st2.get_positions64(), st.get_positions64())
+    np.testing.assert_array_equal(st2.get_velocities64(), st.get_velocities64())
+    np.testing.assert_array_equal(st2.get_masses(), st.get_masses())
+    assert sorted(c2._pins) == sorted(c._pins) and len(c2._walls) == 1
+    assert m2.__getstate__()[5] == m.__getstate__()[5]      # material, bending stiffness included
